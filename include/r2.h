@@ -1,0 +1,170 @@
+/*
+ * r2.h — C ABI of the B200-native Renderer2 hot paths (SGGX mesh-to-volume LOD
+ * filter and wavefront path tracer).
+ *
+ * Every entry point returns an r2_status; no C++ exception crosses this
+ * boundary.  Pointers are plain host pointers unless a parameter name starts
+ * with `d_` (device memory on the current CUDA device).  Matrices are glm
+ * column-major mat4x3 (12 floats: four columns of xyz).
+ *
+ * Reference interfaces replaced (paths inside FrederikBoehm/Renderer2):
+ *   CConfigLoader::loadConfig        raytracer/include/backend/config_loader.hpp:36-40
+ *   filter::CFilter / runFiltering   raytracer/filter.hpp:13-44, raytracer/filter.cu:20-123
+ *   rt::Raytracer::renderFrame       raytracer/raytracer.hpp:29-72, raytracer/raytracer.cu:161-210
+ *   CPipeline / main                 raytracer/pipeline.hpp:5-17, raytracer/main.cu:4-18
+ */
+#ifndef R2_H
+#define R2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum r2_status {
+  R2_OK = 0,
+  R2_ERR_INVALID_ARGUMENT = 1,
+  R2_ERR_INVALID_CONFIG = 2,
+  R2_ERR_IO = 3,
+  R2_ERR_OUT_OF_MEMORY = 4,
+  R2_ERR_ADMISSION_REJECTED = 5,
+  R2_ERR_DEVICE_TIMEOUT = 6,
+  R2_ERR_DEVICE = 7,
+  R2_ERR_UNSUPPORTED = 8,
+  R2_ERR_NO_DEVICE = 9
+} r2_status;
+
+/* Human-readable name of a status code (static string). */
+const char* r2_status_string(r2_status s);
+/* Message of the last failing call on this thread ("" if none). */
+const char* r2_last_error(void);
+/* ABI version: major * 10000 + minor * 100 + patch. */
+int r2_version(void);
+
+/* Voxel payload, 32 bytes, byte-identical to the reference's
+ * filter::SFilteredDataCompact (raytracer/include/filtering/filtered_data.hpp:33-61),
+ * which is stored in the NanoVDB Vec4d grid (openvdb_backend.cpp:27). */
+typedef struct r2_voxel {
+  float density;
+  uint16_t sigma_x, sigma_y, sigma_z; /* [0,1] -> [0,65535] */
+  uint16_t r_xy, r_xz, r_yz;          /* [-1,1] -> [0,65535] */
+  uint8_t diffuse[3];
+  uint8_t specular[3];
+  uint16_t normal[3];                 /* [-1,1] -> [0,65535] */
+  uint16_t ior;                       /* IEEE half bits */
+  uint16_t pad;
+} r2_voxel;
+
+/* Surface material of a mesh: the reference's CMaterial built from MTL keys
+ * (raytracer/src/material/material.cu:80-148): Kd, Ks, alpha = sqrt(2/(Ns+2)),
+ * ior = Ni (1.5 when Ni == 1), Oren-Nayar roughness 0 for OBJ materials. */
+typedef struct r2_material {
+  float diffuse[3];
+  float specular[3];
+  float alpha_x, alpha_y;     /* GGX roughness */
+  float eta_i, eta_t;         /* Fresnel indices (eta_t is the ior) */
+  float diffuse_roughness;    /* Oren-Nayar sigma */
+  float pad;
+} r2_material;
+
+/* Filter parameters: the "Filtering" block of config.json
+ * (raytracer/src/backend/config_loader.cu:75-100) plus build options. */
+typedef struct r2_filter_params {
+  float min_voxel_size;        /* MinVoxelSize */
+  uint32_t lods;               /* LODs (voxel size doubles per LOD) */
+  uint32_t samples_per_voxel;  /* SamplesPerVoxel (<= 1024) */
+  float sigma_t;               /* SigmaT */
+  uint32_t estimation_iterations; /* EstimationIterations */
+  float alpha;                 /* Alpha */
+  uint32_t clip_rays;          /* ClipRays */
+  uint32_t seed;               /* Philox key word 1 */
+} r2_filter_params;
+
+/* Grid of one LOD: COpenvdbBackend::setupGrid (openvdb_backend.cpp:71-106). */
+typedef struct r2_filter_grid {
+  int32_t num_voxels[3];
+  float index_to_model[12];
+  float model_to_index[12];
+  float model_to_world[12];
+  float world_to_model[12];
+  float world_bb_min[3];
+  float world_bb_max[3];
+  float voxel_size;            /* LOD voxel size (file-name suffix) */
+} r2_filter_grid;
+
+/* ------------------------------------------------------------------------ */
+/* Mesh filter on host arrays (one FILTER-masked mesh, one material).
+ *
+ * Replaces the body of CFilter::runFiltering for one LOD
+ * (raytracer/filter.cu:84-99: setupGrid, optixLaunch(nx,ny,nz), D2H copy).
+ * positions: 3*nverts floats (model space); indices: 3*ntris;
+ * normals: 3*nverts (model space vertex normals);
+ * model_to_world: the object's T*R*S transform (12 floats);
+ * voxel_size: this LOD's voxel size; out: nx*ny*nz payloads (host), indexed
+ * x + y*nx + z*nx*ny.  grid_out (nullable) receives the grid.
+ * wide_out (nullable): 20 floats per voxel (density, Sxx Syy Szz Sxy Sxz Syz,
+ * diffuse rgb, specular rgb, normal xyz, ior, hits, mean ray length) before
+ * quantisation — the parity surface against the FP64 oracle. */
+r2_status r2_filter_mesh(const float* positions, uint32_t nverts, const uint32_t* indices,
+                         uint32_t ntris, const float* normals, const r2_material* material,
+                         const float* model_to_world, const r2_filter_params* params,
+                         float voxel_size, r2_filter_grid* grid_out, r2_voxel* out,
+                         float* wide_out, size_t out_capacity);
+
+/* Grid setup only (host): world BB union, ceil(extent/vs - 0.001), transforms. */
+r2_status r2_filter_setup_grid(const float* model_bb_min, const float* model_bb_max,
+                               const float* model_to_world, float voxel_size,
+                               r2_filter_grid* grid_out);
+
+/* ------------------------------------------------------------------------ */
+/* Device-resident filter scene (inputs stay in HBM between launches). */
+typedef struct r2_filter_scene r2_filter_scene;
+
+r2_status r2_filter_scene_create(const float* positions, uint32_t nverts,
+                                 const uint32_t* indices, uint32_t ntris, const float* normals,
+                                 const r2_material* material, const float* model_to_world,
+                                 r2_filter_scene** out);
+r2_status r2_filter_scene_destroy(r2_filter_scene* scene);
+/* Grid for a voxel size over this scene's bounds. */
+r2_status r2_filter_scene_grid(const r2_filter_scene* scene, float voxel_size,
+                               r2_filter_grid* grid_out);
+/* Filter one LOD into device memory.  d_out: nx*ny*nz r2_voxel; d_wide
+ * (nullable): 20 floats per voxel; d_fp16 (nullable): 8 halves per voxel
+ * (density, Sxx, Syy, Szz, Sxy, Sxz, Syz, 0).  stream: cudaStream_t or NULL.
+ * stats_out (nullable, host): [0]=voxels, [1]=voxels with candidate geometry,
+ * [2]=kernel milliseconds of the per-voxel sampling kernel. */
+r2_status r2_filter_scene_run(r2_filter_scene* scene, const r2_filter_grid* grid,
+                              const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
+                              uint16_t* d_fp16, void* stream, double* stats_out);
+
+/* BVH of a filter scene, downloaded for bit-exact comparison with the oracle:
+ * nodes: (ntris-1 or 1) * 16 words; tri_order: ntris original indices. */
+r2_status r2_filter_scene_bvh(const r2_filter_scene* scene, int32_t* nodes, size_t node_words,
+                              uint32_t* tri_order, size_t ntris, uint32_t* nnodes_out,
+                              uint32_t* height_out);
+
+/* ------------------------------------------------------------------------ */
+/* Synthetic inputs (seeded), used by the configs in the benchmark plan. */
+
+/* Icosphere of subdivision level `subdiv` (20*4^subdiv triangles) of radius 1,
+ * displaced radially by 1 + amplitude*valuenoise(4 p) with seed `seed`.
+ * Capacities are in elements; counts are returned. Smooth area-weighted normals. */
+r2_status r2_gen_icosphere(uint32_t subdiv, float amplitude, uint32_t seed, float* positions,
+                           size_t pos_capacity, uint32_t* indices, size_t idx_capacity,
+                           float* normals, uint32_t* nverts_out, uint32_t* ntris_out);
+
+/* Leaf quads in the unit cube: n_quads quads (2 triangles each), a fraction
+ * `clustered` Gaussian (sigma 0.02) around n_branches cubic Bezier curves,
+ * random orientation, edge ~ U[0.005, 0.02]. */
+r2_status r2_gen_foliage(uint32_t n_quads, uint32_t n_branches, float clustered, uint32_t seed,
+                         float* positions, size_t pos_capacity, uint32_t* indices,
+                         size_t idx_capacity, float* normals, uint32_t* nverts_out,
+                         uint32_t* ntris_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* R2_H */

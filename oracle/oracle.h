@@ -1,0 +1,100 @@
+/*
+ * CPU oracle for the Renderer2 hot paths — TEST INFRASTRUCTURE ONLY.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / reference
+ * arm may load this library, and only as the checker or the timed CPU
+ * baseline; the product path never calls it.
+ *
+ * It restates, in plain C, the reference algorithms of FrederikBoehm/Renderer2:
+ *   - per-voxel SGGX filtering, CMeshFilter::run / estimateDensity
+ *     (raytracer/include/filtering/mesh_filter.hpp:51-122, 182-226);
+ *   - the 32-byte payload encode, SFilteredDataCompact(const SFilteredData&)
+ *     (raytracer/include/filtering/filtered_data.hpp:91-107);
+ *   - SGGX S construction, buildS (raytracer/include/medium/sggx_phase_function.hpp:95-105);
+ *   - the bounding-sphere clip, Sphere::intersect (raytracer/include/shapes/sphere.hpp:33-90);
+ *   - grid setup, COpenvdbBackend::setupGrid (raytracer/src/filtering/openvdb_backend.cpp:71-106);
+ * driven by the same Philox4x32-10 streams as the GPU kernels, over its own
+ * LBVH built with the same deterministic algorithm (bit-exact leaf assignment).
+ * Geometry (ray generation, traversal, hit normals) is FP32 with the same
+ * operation order as the device code; accumulation, the density fit and the
+ * mean normal are FP64 (the "FP64 rebuild").
+ *
+ * Parity pinning: the reference has no tests or golden vectors, and its own
+ * RNG (cuRAND XORWOW) and OptiX traversal cannot run here.  The math functions
+ * this oracle restates are pinned against the reference's own headers compiled
+ * for the host (oracle/ref_kat.cpp -> oracle/_ref/libr2ref.so) through the
+ * golden vectors in tests/golden/.
+ */
+#ifndef R2_ORACLE_H
+#define R2_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void orc_sincos_turns(float u, float* s, float* c);
+
+/* LBVH identical to the GPU builder.  nodes_out: (ntris > 1 ? ntris-1 : 1) * 16
+ * int32 words (BvhNode layout), order_out: ntris.  Returns the tree height or
+ * -1 on error. */
+int orc_build_bvh(const float* world_pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris,
+                  int32_t* nodes_out, uint32_t* order_out, float* tris_out /* 12*ntris or NULL */);
+
+/* Closest hit: returns BVH-order triangle or -1; t/b1/b2 out. */
+int orc_trace(const int32_t* nodes, const float* tris, float ox, float oy, float oz, float dx, float dy,
+              float dz, float tmax, float* t, float* b1, float* b2);
+
+typedef struct orc_material {
+  float diffuse[3];
+  float specular[3];
+  float alpha_x, alpha_y, eta_i, eta_t, diffuse_roughness, pad;
+} orc_material;
+
+typedef struct orc_filter_params {
+  float min_voxel_size;
+  uint32_t lods;
+  uint32_t samples_per_voxel;
+  float sigma_t;
+  uint32_t estimation_iterations;
+  float alpha;
+  uint32_t clip_rays;
+  uint32_t seed;
+} orc_filter_params;
+
+typedef struct orc_grid {
+  int32_t num_voxels[3];
+  float index_to_model[12];
+  float model_to_index[12];
+  float model_to_world[12];
+  float world_to_model[12];
+  float world_bb_min[3];
+  float world_bb_max[3];
+  float voxel_size;
+} orc_grid;
+
+/* Grid setup from the model bounds and the object's model_to_world. */
+void orc_setup_grid(const float* model_lo, const float* model_hi, const float* model_to_world, float voxel_size,
+                    orc_grid* g);
+
+/* Filters voxels [v0, v1) of the grid.  wide_out: 20 doubles per voxel of the
+ * range (density, S xx yy zz xy xz yz, diffuse, specular, normal, ior, hits,
+ * mean ray length, mean roughness); compact_out: 32 bytes per voxel of the
+ * range (nullable).  threads: worker threads (0 = all cores).  The mesh is in
+ * model space; positions and hit normals use obj_model_to_world (the
+ * object's own transform), voxel centres the grid's model_to_world.  lod is
+ * the Philox counter word of the LOD. */
+int orc_filter(const float* positions, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* normals,
+               const orc_material* mat, const float* obj_model_to_world, const orc_grid* g,
+               const orc_filter_params* p, uint32_t lod, uint64_t v0, uint64_t v1, double* wide_out,
+               uint8_t* compact_out, int threads);
+
+/* Encode a wide (double) record to the 32-byte payload (FP64 arithmetic). */
+void orc_encode(const double* wide, uint8_t* out32);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

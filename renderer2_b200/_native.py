@@ -1,0 +1,103 @@
+"""ctypes binding of the C ABI declared in include/r2.h.
+
+The native library is required: importing this module raises if
+``_lib/librenderer2.so`` is missing (there is no Python or CPU fallback for
+the hot paths).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "librenderer2.so")
+
+
+class R2Error(RuntimeError):
+    def __init__(self, status: int, name: str, message: str):
+        super().__init__(f"{name}: {message}")
+        self.status = status
+        self.name = name
+
+
+class Voxel(C.Structure):
+    _fields_ = [("density", C.c_float), ("sigma", C.c_uint16 * 3), ("r", C.c_uint16 * 3),
+                ("diffuse", C.c_uint8 * 3), ("specular", C.c_uint8 * 3), ("normal", C.c_uint16 * 3),
+                ("ior", C.c_uint16), ("pad", C.c_uint16)]
+
+
+VOXEL_DTYPE = np.dtype([("density", "<f4"), ("sigma", "<u2", 3), ("r", "<u2", 3), ("diffuse", "u1", 3),
+                        ("specular", "u1", 3), ("normal", "<u2", 3), ("ior", "<u2"), ("pad", "<u2")])
+assert VOXEL_DTYPE.itemsize == 32
+
+
+class Material(C.Structure):
+    _fields_ = [("diffuse", C.c_float * 3), ("specular", C.c_float * 3), ("alpha_x", C.c_float),
+                ("alpha_y", C.c_float), ("eta_i", C.c_float), ("eta_t", C.c_float),
+                ("diffuse_roughness", C.c_float), ("pad", C.c_float)]
+
+
+class FilterParams(C.Structure):
+    _fields_ = [("min_voxel_size", C.c_float), ("lods", C.c_uint32), ("samples_per_voxel", C.c_uint32),
+                ("sigma_t", C.c_float), ("estimation_iterations", C.c_uint32), ("alpha", C.c_float),
+                ("clip_rays", C.c_uint32), ("seed", C.c_uint32)]
+
+
+class FilterGrid(C.Structure):
+    _fields_ = [("num_voxels", C.c_int32 * 3), ("index_to_model", C.c_float * 12),
+                ("model_to_index", C.c_float * 12), ("model_to_world", C.c_float * 12),
+                ("world_to_model", C.c_float * 12), ("world_bb_min", C.c_float * 3),
+                ("world_bb_max", C.c_float * 3), ("voxel_size", C.c_float)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"native library missing: {LIB_PATH} (run __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    u32, i32, f32, sz = C.c_uint32, C.c_int32, C.c_float, C.c_size_t
+    sigs = {
+        "r2_status_string": (C.c_char_p, [C.c_int]),
+        "r2_last_error": (C.c_char_p, []),
+        "r2_version": (C.c_int, []),
+        "r2_gen_icosphere": (C.c_int, [u32, f32, u32, P, sz, P, sz, P, P, P]),
+        "r2_gen_foliage": (C.c_int, [u32, u32, f32, u32, P, sz, P, sz, P, P, P]),
+        "r2_filter_setup_grid": (C.c_int, [P, P, P, f32, P]),
+        "r2_filter_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, f32, P, P, P, sz]),
+        "r2_filter_scene_create": (C.c_int, [P, u32, P, u32, P, P, P, P]),
+        "r2_filter_scene_destroy": (C.c_int, [P]),
+        "r2_filter_scene_grid": (C.c_int, [P, f32, P]),
+        "r2_filter_scene_run": (C.c_int, [P, P, P, P, P, P, P, P]),
+        "r2_filter_scene_bvh": (C.c_int, [P, P, sz, P, sz, P, P]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int) -> None:
+    if status != 0:
+        name = lib.r2_status_string(status).decode()
+        msg = lib.r2_last_error().decode()
+        raise R2Error(status, name, msg)
+
+
+def ptr(a):
+    """Host pointer of a contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    assert a.flags["C_CONTIGUOUS"], "array must be C-contiguous"
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def identity43() -> np.ndarray:
+    m = np.zeros(12, np.float32)
+    m[0] = m[4] = m[8] = 1.0
+    return m

@@ -1,0 +1,207 @@
+// Triangle BVH that replaces the reference's OptiX GAS/IAS
+// (raytracer/src/mesh/mesh.cu:140-168, raytracer/src/scene/scene.cu:188-256)
+// and its optixTrace closest-hit query (include/scene/device_scene_impl.hpp:12-31).
+//
+// Layout in HBM (all arrays 16-byte aligned, read with 128-bit loads):
+//   nodes[n-1]  BvhNode, 64 B each: both children's boxes live in the parent so
+//               one 64-byte fetch decides which children a ray enters.
+//   tris[3n]    float4 per vertex in BVH (Morton) order: v0.xyz|w=orig index,
+//               v1.xyz|w=0, v2.xyz|w=0 — the watertight test needs raw vertices.
+// Child encoding: c >= 0 is an internal node; c < 0 is a leaf reference
+// ~(first | count << 26) (see bvh_leaf_ref).  ch.z holds the node's parent and
+// ch.w its depth (build bookkeeping; traversal ignores them).
+#pragma once
+#include "r2_core.h"
+
+namespace r2 {
+
+struct __align__(16) BvhNode {
+  float4 b0;  // child0 lo.x hi.x lo.y hi.y
+  float4 b1;  // child1 lo.x hi.x lo.y hi.y
+  float4 bz;  // child0 lo.z hi.z, child1 lo.z hi.z
+  int4 ch;    // child0, child1, parent, depth
+};
+static_assert(sizeof(BvhNode) == 64, "BvhNode must be 64 bytes");
+
+// Marker for an absent second child (a BVH over a single leaf).
+#define R2_BVH_NONE ((int)0x80000000)
+
+struct BvhView {
+  const BvhNode* nodes;
+  const float4* tris;  // 3 per triangle, BVH order
+  uint32_t ntris;
+};
+
+struct Hit {
+  float t;
+  float b1, b2;  // barycentric weights of v1 and v2 (OptiX convention)
+  int tri;       // BVH-order triangle index, -1 = miss
+};
+
+// Per-ray constants of the watertight ray/triangle test (Woop, Benthin, Wald,
+// "Watertight Ray/Triangle Intersection", JCGT 2013).
+struct RayPre {
+  V3 o, d, invd;
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+};
+
+R2_HD RayPre make_ray_pre(V3 o, V3 d) {
+  RayPre r;
+  r.o = o;
+  r.d = d;
+  r.invd = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  V3 ad = vabs(d);
+  int kz = (ad.x > ad.y) ? ((ad.x > ad.z) ? 0 : 2) : ((ad.y > ad.z) ? 1 : 2);
+  int kx = kz + 1; if (kx == 3) kx = 0;
+  int ky = kx + 1; if (ky == 3) ky = 0;
+  if (comp(d, kz) < 0.0f) { int t = kx; kx = ky; ky = t; }
+  r.kx = kx; r.ky = ky; r.kz = kz;
+  float dz = comp(d, kz);
+  r.Sx = comp(d, kx) / dz;
+  r.Sy = comp(d, ky) / dz;
+  r.Sz = 1.0f / dz;
+  return r;
+}
+
+// Robust slab test (Ize, "Robust BVH Ray Traversal", JCGT 2013): the far
+// distance is scaled by 1 + 2*gamma(3) so boxes are never missed by rounding.
+R2_HD bool slab(const RayPre& r, float lox, float hix, float loy, float hiy, float loz,
+                float hiz, float tmax, float* tentry) {
+  float tx0 = (lox - r.o.x) * r.invd.x, tx1 = (hix - r.o.x) * r.invd.x;
+  float ty0 = (loy - r.o.y) * r.invd.y, ty1 = (hiy - r.o.y) * r.invd.y;
+  float tz0 = (loz - r.o.z) * r.invd.z, tz1 = (hiz - r.o.z) * r.invd.z;
+  float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+  float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+  tf = tf * 1.00000024f;  // 1 + 2*gamma(3) rounded up
+  *tentry = tn;
+  return tn <= tf;
+}
+
+// Watertight test.  Accepts 0 < t and (t, tri) lexicographically below the
+// current best (t, tri) so the closest hit is independent of visiting order.
+R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, Hit* best) {
+  V3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
+  float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
+  float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
+  float Bx = comp(B, r.kx) - r.Sx * Bz0, By = comp(B, r.ky) - r.Sy * Bz0;
+  float Cx = comp(C, r.kx) - r.Sx * Cz0, Cy = comp(C, r.ky) - r.Sy * Cz0;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    double CxBy = (double)Cx * (double)By, CyBx = (double)Cy * (double)Bx;
+    U = (float)(CxBy - CyBx);
+    double AxCy = (double)Ax * (double)Cy, AyCx = (double)Ay * (double)Cx;
+    V = (float)(AxCy - AyCx);
+    double BxAy = (double)Bx * (double)Ay, ByAx = (double)By * (double)Ax;
+    W = (float)(BxAy - ByAx);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = U + V + W;
+  if (det == 0.0f) return false;
+  float Az = r.Sz * Az0, Bz = r.Sz * Bz0, Cz = r.Sz * Cz0;
+  float T = U * Az + V * Bz + W * Cz;
+  float rcp = 1.0f / det;
+  float t = T * rcp;
+  if (!(t > 0.0f)) return false;
+  if (t < best->t || (t == best->t && tri < best->tri)) {
+    best->t = t;
+    best->b1 = V * rcp;
+    best->b2 = W * rcp;
+    best->tri = tri;
+    return true;
+  }
+  return false;
+}
+
+#define R2_BVH_STACK 96
+#define R2_LEAF_MAX 16
+
+// Leaf reference: ~(first | count << 26); first < 2^26, count <= 31.
+R2_HD int bvh_leaf_ref(int first, int count) { return ~(first | (count << 26)); }
+R2_HD int bvh_leaf_first(int ref) { return (~ref) & 0x03FFFFFF; }
+R2_HD int bvh_leaf_count(int ref) { return ((~ref) >> 26) & 0x1F; }
+
+// Closest hit in (0, tmax] (kAnyHit: first hit found).  `tri` of the result is
+// the BVH-order index, -1 on a miss.  Stack entries hold child references with
+// their entry distance; leaves are tested when reached.  The builder bounds the
+// tree depth by R2_BVH_STACK so the stack cannot overflow.
+template <bool kAnyHit>
+R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax) {
+  Hit best;
+  best.t = tmax;
+  best.b1 = best.b2 = 0.0f;
+  best.tri = 0x7FFFFFFF;
+  const RayPre r = make_ray_pre(o, d);
+  int stack[R2_BVH_STACK];
+  float stackT[R2_BVH_STACK];
+  int sp = 0;
+  int cur = 0;  // root is internal node 0
+  bool found = false;
+  while (true) {
+    if (cur >= 0) {
+#if defined(__CUDA_ARCH__)
+      const float4 b0 = __ldg(&bvh.nodes[cur].b0);
+      const float4 b1 = __ldg(&bvh.nodes[cur].b1);
+      const float4 bz = __ldg(&bvh.nodes[cur].bz);
+      const int4 ch = __ldg(&bvh.nodes[cur].ch);
+#else
+      const float4 b0 = bvh.nodes[cur].b0;
+      const float4 b1 = bvh.nodes[cur].b1;
+      const float4 bz = bvh.nodes[cur].bz;
+      const int4 ch = bvh.nodes[cur].ch;
+#endif
+      float t0 = 0.0f, t1 = 0.0f;
+      const bool h0 = slab(r, b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, best.t, &t0);
+      const bool h1 = (ch.y != R2_BVH_NONE) && slab(r, b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, best.t, &t1);
+      if (h0 && h1) {
+        int nearC = ch.x, farC = ch.y;
+        float farT = t1;
+        if (t1 < t0) { nearC = ch.y; farC = ch.x; farT = t0; }
+        stack[sp] = farC;
+        stackT[sp] = farT;
+        ++sp;
+        cur = nearC;
+        continue;
+      } else if (h0) {
+        cur = ch.x;
+        continue;
+      } else if (h1) {
+        cur = ch.y;
+        continue;
+      }
+    } else {
+      const int first = bvh_leaf_first(cur);
+      const int count = bvh_leaf_count(cur);
+      for (int i = 0; i < count; ++i) {
+        const int tri = first + i;
+#if defined(__CUDA_ARCH__)
+        const float4 a = __ldg(&bvh.tris[3 * tri + 0]);
+        const float4 b = __ldg(&bvh.tris[3 * tri + 1]);
+        const float4 c = __ldg(&bvh.tris[3 * tri + 2]);
+#else
+        const float4 a = bvh.tris[3 * tri + 0];
+        const float4 b = bvh.tris[3 * tri + 1];
+        const float4 c = bvh.tris[3 * tri + 2];
+#endif
+        if (tri_test(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &best)) {
+          found = true;
+          if (kAnyHit) return best;
+        }
+      }
+    }
+    // pop the next child whose entry distance is not beyond the closest hit
+    while (true) {
+      if (sp == 0) {
+        if (!found) best.tri = -1;
+        return best;
+      }
+      --sp;
+      if (stackT[sp] <= best.t) break;
+    }
+    cur = stack[sp];
+  }
+}
+
+}  // namespace r2

@@ -1,0 +1,36 @@
+// GPU LBVH builder (host interface).  See bvh_build.cu.
+#pragma once
+#include "bvh.h"
+#include "runtime.h"
+
+namespace r2 {
+
+// SAH constants of the leaf-collapse pass: cost(leaf) = kSahTri * n,
+// cost(inner) = kSahNode + (A_l cost_l + A_r cost_r) / A.
+constexpr float kSahNode = 1.2f;
+constexpr float kSahTri = 1.0f;
+constexpr int kLeafMax = 8;
+
+// A triangle BVH resident in device memory.
+struct DeviceBvh {
+  DBuf<BvhNode> nodes;     // max(ntris-1, 1) nodes
+  DBuf<float4> tris;       // 3 per triangle in BVH order
+  DBuf<uint32_t> order;    // BVH position -> original triangle index
+  uint32_t ntris = 0;
+  uint32_t nnodes = 0;
+  uint32_t height = 0;     // levels of inner nodes on the longest root-leaf path
+  BvhView view() const {
+    BvhView v;
+    v.nodes = nodes.get();
+    v.tris = tris.get();
+    v.ntris = ntris;
+    return v;
+  }
+};
+
+// Builds the BVH over triangles (d_pos: 3 floats per vertex, d_idx: 3 per
+// triangle, both device).  Deterministic: the result depends only on the input.
+void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out,
+               cudaStream_t stream);
+
+}  // namespace r2

@@ -1,0 +1,303 @@
+// SGGX mesh-to-volume filter kernels for sm_100a.
+//
+// Reference path: __raygen__filtering (raytracer/src/backend/shaders.optix.cu:258-284)
+// launches one OptiX thread per voxel running CMeshFilter::run
+// (raytracer/include/filtering/mesh_filter.hpp:51-122) and estimateDensity (182-204).
+//
+// B200 design:
+//  * k_filter_classify: one thread per voxel tests the voxel's bounding sphere
+//    (radius 1.1 * |voxelSize| / 2, inflated by 0.1%) against the BVH boxes.
+//    Every filter ray starts inside the voxel and ends inside that sphere, so a
+//    voxel whose sphere touches no triangle box has zero hits for certain: it
+//    gets the empty payload here.  The others are appended to a work list with
+//    warp-aggregated atomics (ballot + popc).
+//  * k_filter_sample: a persistent kernel; each warp pops one voxel at a time
+//    from the work list and its 32 lanes trace the voxel's samples (lane l owns
+//    samples l, l+32, ...), so a warp's rays share one BVH neighbourhood.  Hit
+//    ray lengths live in shared memory (no 4 KB per-thread local array).  Sums
+//    are compensated per lane and across the warp (TwoSum butterfly).  The
+//    density fit runs its iterations as warp reductions.
+#include "filter.cuh"
+#include "filter_math.h"
+
+namespace r2 {
+namespace {
+
+constexpr int kSampleWarps = 4;  // warps per block of the sampling kernel
+
+__device__ __forceinline__ V3 voxel_center(const FilterLaunch& L, int x, int y, int z) {
+  V3 pm = xform_point(L.indexToModel, v3((float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f));
+  return xform_point(L.modelToWorld, pm);
+}
+
+__device__ __forceinline__ bool box_overlap(float lox, float hix, float loy, float hiy, float loz,
+                                            float hiz, V3 qlo, V3 qhi) {
+  return !(lox > qhi.x || hix < qlo.x || loy > qhi.y || hiy < qlo.y || loz > qhi.z || hiz < qlo.z);
+}
+
+// Does any triangle box overlap the query box?
+__device__ bool bvh_any_box(const BvhView& bvh, V3 qlo, V3 qhi) {
+  int stack[R2_BVH_STACK];
+  int sp = 0;
+  int cur = 0;
+  while (true) {
+    if (cur >= 0) {
+      const BvhNode* nd = &bvh.nodes[cur];
+      float4 b0 = __ldg(&nd->b0), b1 = __ldg(&nd->b1), bz = __ldg(&nd->bz);
+      int4 ch = __ldg(&nd->ch);
+      bool h0 = box_overlap(b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, qlo, qhi);
+      bool h1 = ch.y != R2_BVH_NONE && box_overlap(b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, qlo, qhi);
+      if (h0 && h1) {
+        stack[sp++] = ch.y;
+        cur = ch.x;
+        continue;
+      } else if (h0) {
+        cur = ch.x;
+        continue;
+      } else if (h1) {
+        cur = ch.y;
+        continue;
+      }
+    } else {
+      int first = bvh_leaf_first(cur), count = bvh_leaf_count(cur);
+      for (int i = 0; i < count; ++i) {
+        int t = first + i;
+        float4 a = __ldg(&bvh.tris[3 * t]), b = __ldg(&bvh.tris[3 * t + 1]), c = __ldg(&bvh.tris[3 * t + 2]);
+        float lx = fminf(fminf(a.x, b.x), c.x), hx = fmaxf(fmaxf(a.x, b.x), c.x);
+        float ly = fminf(fminf(a.y, b.y), c.y), hy = fmaxf(fmaxf(a.y, b.y), c.y);
+        float lz = fminf(fminf(a.z, b.z), c.z), hz = fmaxf(fmaxf(a.z, b.z), c.z);
+        if (box_overlap(lx, hx, ly, hy, lz, hz, qlo, qhi)) return true;
+      }
+    }
+    if (sp == 0) return false;
+    cur = stack[--sp];
+  }
+}
+
+__device__ __forceinline__ void write_voxel(r2_voxel* out, size_t vid, const r2_voxel& v) {
+  const uint4* src = reinterpret_cast<const uint4*>(&v);
+  uint4* dst = reinterpret_cast<uint4*>(out + vid);
+  dst[0] = src[0];
+  dst[1] = src[1];
+}
+
+__device__ __forceinline__ void write_empty(const FilterLaunch& L, size_t vid) {
+  write_voxel(L.out, vid, empty_voxel());
+  if (L.wide) {
+    float* w = L.wide + vid * kWideFloats;
+    for (int k = 0; k < kWideFloats; ++k) w[k] = 0.0f;
+    w[16] = 1.0f;
+  }
+  if (L.fp16) {
+    uint4* f = reinterpret_cast<uint4*>(L.fp16 + vid * 8);
+    *f = make_uint4(0, 0, 0, 0);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_filter_classify(FilterLaunch L) {
+  const size_t nvox = (size_t)L.nx * L.ny * L.nz;
+  const float radius = 1.1f * length(L.voxelSize) / 2.0f;
+  const float rq = radius * 1.001f + 1e-6f;
+  const int lane = threadIdx.x & 31;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t base = (size_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < nvox; base += stride) {
+    size_t vid = base + lane;
+    bool valid = vid < nvox;
+    bool cand = false;
+    if (valid) {
+      int x = (int)(vid % L.nx), y = (int)((vid / L.nx) % L.ny), z = (int)(vid / ((size_t)L.nx * L.ny));
+      V3 c = voxel_center(L, x, y, z);
+      cand = bvh_any_box(L.bvh, c - v3(rq), c + v3(rq));
+      if (!cand) write_empty(L, vid);
+    }
+    unsigned m = __ballot_sync(0xFFFFFFFFu, cand);
+    if (m) {
+      uint32_t slot = 0;
+      int leader = __ffs(m) - 1;
+      if (lane == leader) slot = atomicAdd(&L.counters[0], (uint32_t)__popc(m));
+      slot = __shfl_sync(0xFFFFFFFFu, slot, leader);
+      if (cand) L.work[slot + __popc(m & ((1u << lane) - 1u))] = (uint32_t)vid;
+    }
+  }
+}
+
+__device__ __forceinline__ CSum warp_csum(CSum v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    CSum o;
+    o.s = __shfl_xor_sync(0xFFFFFFFFu, v.s, off);
+    o.c = __shfl_xor_sync(0xFFFFFFFFu, v.c, off);
+    v = ccombine(v, o);
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunch L) {
+  __shared__ float ts[kSampleWarps][kFilterMaxSpv];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* myTs = ts[warp];
+  const uint32_t ncand = *(volatile uint32_t*)&L.counters[0];
+  const float radius = 1.1f * length(L.voxelSize) / 2.0f;
+  const float tMaxFixed = L.voxelSize.x;
+  while (true) {
+    uint32_t w = 0;
+    if (lane == 0) w = atomicAdd(&L.counters[1], 1u);
+    w = __shfl_sync(0xFFFFFFFFu, w, 0);
+    if (w >= ncand) break;
+    const uint32_t vid = L.work[w];
+    const int x = (int)(vid % (uint32_t)L.nx);
+    const int y = (int)((vid / (uint32_t)L.nx) % (uint32_t)L.ny);
+    const int z = (int)(vid / ((uint32_t)L.nx * (uint32_t)L.ny));
+    const V3 center = voxel_center(L, x, y, z);
+    const V3 cv = v3((float)x, (float)y, (float)z);
+
+    CSum S[6], nrm[3], dist;
+    float dif[3] = {0.f, 0.f, 0.f}, spe[3] = {0.f, 0.f, 0.f}, rough = 0.f, ior = 0.f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) S[k] = csum0();
+#pragma unroll
+    for (int k = 0; k < 3; ++k) nrm[k] = csum0();
+    dist = csum0();
+    uint32_t hits = 0;
+
+    for (uint32_t s = lane; s < L.spv; s += 32) {
+      const U4 r0 = philox4x32_10(u4(s, 0u, L.lod, 0u), vid, L.seed);
+      const U4 r1 = philox4x32_10(u4(s, 1u, L.lod, 0u), vid, L.seed);
+      const V3 oi = cv + v3(u01(r0.x), u01(r0.y), u01(r0.z));
+      const V3 o = xform_point(L.indexToWorld, oi);
+      const V3 d = uniform_sample_sphere(u01(r0.w), u01(r1.x));
+      const float tmax = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
+      const Hit h = bvh_trace<false>(L.bvh, o, d, tmax);
+      float tsv = -1.0f;
+      if (h.tri >= 0) {
+        const float4 n0 = __ldg(&L.triN[3 * h.tri]);
+        const float4 n1 = __ldg(&L.triN[3 * h.tri + 1]);
+        const float4 n2 = __ldg(&L.triN[3 * h.tri + 2]);
+        const float b0 = (1.0f - h.b1) - h.b2;
+        V3 gn = v3(n0.x, n0.y, n0.z) * b0 + v3(n1.x, n1.y, n1.z) * h.b1 + v3(n2.x, n2.y, n2.z) * h.b2;
+        gn = normalize(gn);
+        const V3 n = normalize(xform_vector(L.objModelToWorld, gn));
+        const r2_material& m = L.mats[__ldg(&L.triMat[h.tri])];
+        float bs[6];
+        build_s(n, m.alpha_x, bs);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) cadd(S[k], bs[k]);
+        cadd(nrm[0], n.x);
+        cadd(nrm[1], n.y);
+        cadd(nrm[2], n.z);
+        cadd(dist, tmax);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          dif[k] += m.diffuse[k];
+          spe[k] += m.specular[k];
+        }
+        rough += m.alpha_x;
+        ior += m.eta_t;
+        ++hits;
+        tsv = tmax;
+      }
+      myTs[s] = tsv;
+    }
+
+    // warp reductions (butterfly: every lane ends with the same totals)
+#pragma unroll
+    for (int k = 0; k < 6; ++k) S[k] = warp_csum(S[k]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) nrm[k] = warp_csum(nrm[k]);
+    dist = warp_csum(dist);
+    CSum cd[3], cs[3], cr, ci;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      cd[k].s = dif[k]; cd[k].c = 0.f; cd[k] = warp_csum(cd[k]);
+      cs[k].s = spe[k]; cs[k].c = 0.f; cs[k] = warp_csum(cs[k]);
+    }
+    cr.s = rough; cr.c = 0.f; cr = warp_csum(cr);
+    ci.s = ior; ci.c = 0.f; ci = warp_csum(ci);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) hits += __shfl_xor_sync(0xFFFFFFFFu, hits, off);
+
+    float wv[kWideFloats];
+#pragma unroll
+    for (int k = 0; k < kWideFloats; ++k) wv[k] = 0.0f;
+    if (hits > 0) {
+      // estimateDensity (mesh_filter.hpp:182-204)
+      const float avgDist = cvalue(dist) / (float)hits;
+      const float pMesh = (float)hits / (float)L.spv;
+      float density = -logf(1.0f - pMesh) / (avgDist * L.sigma_t);
+      const float nAlpha = L.alpha / L.sigma_t;
+      for (uint32_t it = 0; it < L.iters; ++it) {
+        float pVol;
+        if (L.clip) {
+          CSum p = csum0();
+          for (uint32_t s = lane; s < L.spv; s += 32) {
+            float t = myTs[s];
+            if (t >= 0.0f) cadd(p, expf(-density * L.sigma_t * t));
+          }
+          p = warp_csum(p);
+          pVol = 1.0f - cvalue(p) / (float)hits;
+        } else {
+          pVol = 1.0f - expf(-density * L.sigma_t * tMaxFixed);
+        }
+        density = density - nAlpha * (pVol - pMesh);
+      }
+      const float inv = 1.0f / (float)hits;
+      wv[0] = density;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) wv[1 + k] = cvalue(S[k]) * inv;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        wv[7 + k] = cvalue(cd[k]) * inv;
+        wv[10 + k] = cvalue(cs[k]) * inv;
+      }
+      const V3 nm = normalize(xform_vector(L.worldToModel, v3(cvalue(nrm[0]), cvalue(nrm[1]), cvalue(nrm[2])) * inv));
+      wv[13] = nm.x;
+      wv[14] = nm.y;
+      wv[15] = nm.z;
+      wv[16] = cvalue(ci) * inv;
+      wv[17] = (float)hits;
+      wv[18] = avgDist;
+      wv[19] = cvalue(cr) * inv;
+    } else {
+      wv[16] = 1.0f;
+    }
+    if (lane == 0) {
+      write_voxel(L.out, vid, hits > 0 ? encode_voxel(wv) : empty_voxel());
+      if (L.fp16) {
+        uint16_t h[8];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) h[k] = f32_to_f16_bits(wv[k]);
+        h[7] = 0;
+        *reinterpret_cast<uint4*>(L.fp16 + (size_t)vid * 8) = *reinterpret_cast<const uint4*>(h);
+      }
+    }
+    if (L.wide && lane < kWideFloats) {
+      float val = wv[0];
+#pragma unroll
+      for (int k = 1; k < kWideFloats; ++k) if (lane == k) val = wv[k];
+      L.wide[(size_t)vid * kWideFloats + lane] = val;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+void launch_filter_classify(const FilterLaunch& L, cudaStream_t s) {
+  const size_t nvox = (size_t)L.nx * L.ny * L.nz;
+  int blocks = (int)std::min<size_t>((nvox + 255) / 256, (size_t)sm_count() * 16);
+  if (blocks < 1) blocks = 1;
+  k_filter_classify<<<blocks, 256, 0, s>>>(L);
+  R2_CUDA(cudaGetLastError());
+}
+
+void launch_filter_sample(const FilterLaunch& L, cudaStream_t s) {
+  static int perSm = 0;
+  if (perSm == 0) {
+    R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_filter_sample, kSampleWarps * 32, 0));
+    if (perSm < 1) perSm = 1;
+  }
+  k_filter_sample<<<sm_count() * perSm, kSampleWarps * 32, 0, s>>>(L);
+  R2_CUDA(cudaGetLastError());
+}
+
+}  // namespace r2

@@ -1,0 +1,144 @@
+"""ctypes view of the CPU oracle (oracle/_build/liboracle.so) — the checker.
+
+Only tests, __graft_entry__.smoke() and bench.py's CPU-baseline legs use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+
+
+def ensure_built() -> str:
+    if not os.path.exists(ORACLE_LIB) or any(
+            os.path.getmtime(os.path.join(ORACLE_DIR, f)) > os.path.getmtime(ORACLE_LIB)
+            for f in os.listdir(ORACLE_DIR) if f.endswith((".c", ".h"))):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+    return ORACLE_LIB
+
+
+class Grid(C.Structure):
+    _fields_ = [("num_voxels", C.c_int32 * 3), ("index_to_model", C.c_float * 12),
+                ("model_to_index", C.c_float * 12), ("model_to_world", C.c_float * 12),
+                ("world_to_model", C.c_float * 12), ("world_bb_min", C.c_float * 3),
+                ("world_bb_max", C.c_float * 3), ("voxel_size", C.c_float)]
+
+
+class Material(C.Structure):
+    _fields_ = [("diffuse", C.c_float * 3), ("specular", C.c_float * 3), ("alpha_x", C.c_float),
+                ("alpha_y", C.c_float), ("eta_i", C.c_float), ("eta_t", C.c_float),
+                ("diffuse_roughness", C.c_float), ("pad", C.c_float)]
+
+
+class Params(C.Structure):
+    _fields_ = [("min_voxel_size", C.c_float), ("lods", C.c_uint32), ("samples_per_voxel", C.c_uint32),
+                ("sigma_t", C.c_float), ("estimation_iterations", C.c_uint32), ("alpha", C.c_float),
+                ("clip_rays", C.c_uint32), ("seed", C.c_uint32)]
+
+
+def _load():
+    lib = C.CDLL(ensure_built())
+    P = C.c_void_p
+    lib.orc_philox4x32_10.argtypes = [P, P, P]
+    lib.orc_sincos_turns.argtypes = [C.c_float, P, P]
+    lib.orc_build_bvh.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P]
+    lib.orc_build_bvh.restype = C.c_int
+    lib.orc_trace.argtypes = [P, P] + [C.c_float] * 7 + [P, P, P]
+    lib.orc_trace.restype = C.c_int
+    lib.orc_setup_grid.argtypes = [P, P, P, C.c_float, P]
+    lib.orc_filter.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, P, P, C.c_uint32, C.c_uint64, C.c_uint64, P,
+                               P, C.c_int]
+    lib.orc_filter.restype = C.c_int
+    lib.orc_encode.argtypes = [P, P]
+    return lib
+
+
+lib = _load()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def philox(ctr, key):
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib.orc_philox4x32_10(_p(c), _p(k), _p(out))
+    return out
+
+
+def sincos_turns(u):
+    s = C.c_float()
+    c = C.c_float()
+    lib.orc_sincos_turns(C.c_float(u), C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+def build_bvh(world_pos, idx):
+    pos = np.ascontiguousarray(world_pos, np.float32)
+    ix = np.ascontiguousarray(idx, np.uint32)
+    n = ix.shape[0]
+    nodes = np.zeros((max(n - 1, 1), 16), np.int32)
+    order = np.zeros(n, np.uint32)
+    tris = np.zeros((n, 12), np.float32)
+    h = lib.orc_build_bvh(_p(pos), pos.shape[0], _p(ix), n, _p(nodes), _p(order), _p(tris))
+    return nodes, order, tris, h
+
+
+def trace(nodes, tris, o, d, tmax):
+    t = C.c_float()
+    b1 = C.c_float()
+    b2 = C.c_float()
+    tri = lib.orc_trace(_p(nodes), _p(tris), *[float(x) for x in o], *[float(x) for x in d], float(tmax),
+                        C.byref(t), C.byref(b1), C.byref(b2))
+    return tri, t.value, b1.value, b2.value
+
+
+def setup_grid(lo, hi, m2w, vs):
+    g = Grid()
+    lo = np.ascontiguousarray(lo, np.float32)
+    hi = np.ascontiguousarray(hi, np.float32)
+    m = np.ascontiguousarray(m2w, np.float32)
+    lib.orc_setup_grid(_p(lo), _p(hi), _p(m), C.c_float(vs), C.byref(g))
+    return g
+
+
+def material_from(native_mat) -> Material:
+    m = Material()
+    C.memmove(C.byref(m), C.byref(native_mat), C.sizeof(Material))
+    return m
+
+
+def params_from(native_params) -> Params:
+    p = Params()
+    C.memmove(C.byref(p), C.byref(native_params), C.sizeof(Params))
+    return p
+
+
+def grid_from(native_grid) -> Grid:
+    g = Grid()
+    C.memmove(C.byref(g), C.byref(native_grid), C.sizeof(Grid))
+    return g
+
+
+def filter_voxels(mesh, mat, m2w, grid, prm, v0=0, v1=None, lod=0, threads=0):
+    """Oracle filter of voxels [v0, v1): (wide float64 (n, 20), compact uint8 (n, 32))."""
+    nvox = int(np.prod(np.array(grid.num_voxels[:], np.int64)))
+    v1 = nvox if v1 is None else v1
+    pos = np.ascontiguousarray(mesh.positions, np.float32)
+    idx = np.ascontiguousarray(mesh.indices, np.uint32)
+    nrm = np.ascontiguousarray(mesh.normals, np.float32)
+    m2w = np.ascontiguousarray(m2w, np.float32)
+    wide = np.zeros((v1 - v0, 20), np.float64)
+    comp = np.zeros((v1 - v0, 32), np.uint8)
+    r = lib.orc_filter(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), C.byref(mat), _p(m2w),
+                       C.byref(grid), C.byref(prm), lod, v0, v1, _p(wide), _p(comp), threads)
+    assert r >= 0, f"oracle filter failed ({r})"
+    return wide, comp
