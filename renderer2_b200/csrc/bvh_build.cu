@@ -190,7 +190,7 @@ __global__ void k_bottom_up(int n, const uint32_t* __restrict__ order, const flo
   leafLo[i] = triLo[prim];
   leafHi[i] = triHi[prim];
   int p = leafParent[i];
-  while (p >= 0) {
+  while (p >= 0 && p < n - 1) {
     __threadfence();
     if (atomicAdd(&flags[p], 1) == 0) return;  // sibling not finished yet
     __threadfence();
@@ -314,6 +314,9 @@ void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, Device
   }
   const int ni = n - 1;
   DBuf<int> left(ni), right(ni), first(ni), last(ni), nodeParent(ni), leafParent(n);
+  // parents default to -1 so a malformed hierarchy ends the bottom-up walk
+  R2_CUDA(cudaMemsetAsync(nodeParent.get(), 0xFF, sizeof(int) * ni, s));
+  R2_CUDA(cudaMemsetAsync(leafParent.get(), 0xFF, sizeof(int) * n, s));
   k_karras<<<(ni + 255) / 256, 256, 0, s>>>(keysSorted.get(), n, left.get(), right.get(), first.get(),
                                             last.get(), nodeParent.get(), leafParent.get());
   DBuf<float4> leafLo(n), leafHi(n), nodeLo(ni), nodeHi(ni);
