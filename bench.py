@@ -1,15 +1,19 @@
 """Benchmark of the Renderer2 hot paths on B200.
 
-Default workload (N=1): the SGGX mesh filter of config "filter at scale":
-500k seeded leaf quads (1M triangles, 70% clustered on 20 branch curves) in
-the unit cube, filtered to a 256^3 grid with 256 samples/voxel and 20
-estimation iterations.  A step is one full LOD filter (classification +
-persistent per-voxel sampling kernel) over device-resident inputs.
+Headline (N=1 workload, config "surface path tracing"): 8x8 grid of displaced
+icospheres (327,680 triangles, per-object GGX roughness U[0.05,1], albedo
+U[0.2,0.9]) lit by a 512x256 lognormal(0,1.5) HDR environment, 1024x1024,
+64 spp, max depth 8.  A step is one frame (64 waves of 1M paths) over a
+device-resident scene; metric paths/s.
+
+Second leg (config "filter at scale"): 500k leaf quads (1M tris) filtered to
+256^3 with 256 samples/voxel and 20 iterations; metric filtered voxels/s,
+reported in the "filter" object of the same line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl native|reference]
 
-Prints one JSON line (rank 0).  --impl reference times the CPU oracle port of
-the reference's per-voxel algorithm on the host cores (bounded sample).
+--impl reference times the CPU oracle port of the reference's integrator and
+filter on the host cores (bounded samples of the same workloads).
 """
 from __future__ import annotations
 
@@ -29,11 +33,18 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_PATH = os.path.join(ROOT, "profiles", "traffic.json")
 FALLBACK_HBM_GBS = 6650.0
 
+RENDER_CFG = dict(width=1024, height=1024, spp=64, depth=8, seed=0)
 FILTER_CFG = dict(n_quads=500_000, n_branches=20, clustered=0.7, seed=4, grid=256, spv=256, iters=20)
-# Algorithmic bytes per filtered voxel: 32 B payload write + 4 B work-list
-# traffic (write on classification, read on pop).  Rays live in registers.
+# Algorithmic bytes (SoA traffic a kernel must move; BVH nodes/triangles are
+# excluded as L2-resident by design):
+#   k_extend: queue id 4 + ray origin 16 + direction 16 + hit record 16 = 52 B per path segment
+#   k_shadow: record origin 16 + direction 16 + visibility 1 = 33 B per shadow slot (2 per segment)
+#   k_filter_sample: payload 32 + work-list id 4 = 36 B per filtered voxel
+EXTEND_BYTES_PER_SEGMENT = 52.0
+SHADOW_BYTES_PER_SLOT = 33.0
 FILTER_BYTES_PER_VOXEL = 36.0
 
 
@@ -44,6 +55,16 @@ def _peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def _traffic(kernel: str):
+    """DRAM bytes per work unit of a kernel from the committed ncu summary."""
+    try:
+        with open(TRAFFIC_PATH) as f:
+            t = json.load(f)
+        return t.get(kernel)
+    except Exception:
+        return None
 
 
 class ClockSampler:
@@ -80,7 +101,7 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
+        sm, mx, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
@@ -89,6 +110,7 @@ class ClockSampler:
             try:
                 sm.append(float(parts[1]))
                 mx = float(parts[2])
+                power.append(float(parts[3]))
             except ValueError:
                 continue
             for n, v in zip(names, parts[5:9]):
@@ -97,14 +119,12 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "power_w_max": max(power) if power else None}
 
 
 def _dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    return int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
 
 
 def _max_over_ranks(x: float, world: int) -> float:
@@ -123,6 +143,18 @@ def _barrier(world: int):
         dist.barrier()
 
 
+# ------------------------------------------------------------------ workloads
+
+def render_workload():
+    from renderer2_b200 import render_scenes as RS
+    from renderer2_b200 import raytracer as R
+    desc, cam = RS.c2_scene()
+    c = RENDER_CFG
+    cam = R.camera(c["width"], c["height"], 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+    prm = R.params(c["spp"], c["depth"], c["seed"])
+    return desc, cam, prm
+
+
 def filter_workload():
     from renderer2_b200 import filter as F
     from renderer2_b200 import scenes
@@ -134,40 +166,204 @@ def filter_workload():
     return mesh, mat, prm, vs
 
 
-def cpu_filter_sample(mesh, mat, prm, vs, budget_s: float = 15.0):
-    """Oracle (FP32 geometry + FP64 fit, all host threads) on contiguous z-slices
-    around the grid's centre; BVH build time is measured and subtracted."""
+def _input_bytes(desc):
+    b = desc["env"].nbytes
+    for mesh, _, _ in desc["meshes"]:
+        b += mesh.positions.nbytes + mesh.indices.nbytes + mesh.normals.nbytes
+    return b
+
+
+# ------------------------------------------------------------------ CPU baselines (oracle port)
+
+def cpu_render_sample(desc, cam, prm, budget_s=15.0, threads=0):
+    """Oracle paths/s on full-spp row bands at the frame centre."""
+    import oracle_lib as O
+    cores = threads or os.cpu_count() or 1
+    W, H = cam.width, cam.height
+    row = H // 2
+    rows, done, t_work = 2, 0, 0.0
+    while True:
+        p0, p1 = row * W, min((row + rows) * W, W * H)
+        t0 = time.perf_counter()
+        O.render(desc, cam, prm.spp, prm.max_depth, prm.seed, p0, p1, threads=cores)
+        t_work += time.perf_counter() - t0
+        done += (p1 - p0)
+        row += rows
+        if t_work >= budget_s or row >= H:
+            break
+        rate = done / t_work
+        rows = max(1, min(int((budget_s - t_work) * rate / W), H - row))
+    paths = done * prm.spp
+    return {"value": paths / t_work, "unit": "paths/s", "cores": cores, "kind": "port",
+            "sample": f"{done // W} rows x {W} px x {prm.spp} spp at the frame centre ({paths} paths), "
+                      f"BVH build included per call"}
+
+
+def cpu_filter_sample(mesh, mat, prm, vs, budget_s=15.0, threads=0):
+    """Oracle voxels/s on contiguous z-slices at the grid centre (BVH build subtracted)."""
     import oracle_lib as O
     from renderer2_b200 import _native as N
-    import ctypes as C
     m2w = N.identity43()
-    lo = mesh.positions.min(0).astype(np.float32)
-    hi = mesh.positions.max(0).astype(np.float32)
-    g = O.setup_grid(lo, hi, m2w, vs)
+    g = O.setup_grid(mesh.positions.min(0).astype(np.float32), mesh.positions.max(0).astype(np.float32), m2w, vs)
     nx, ny, nz = g.num_voxels[:]
     slab = nx * ny
-    cores = os.cpu_count() or 1
+    cores = threads or os.cpu_count() or 1
     t0 = time.perf_counter()
     O.filter_voxels(mesh, O.material_from(mat), m2w, g, O.params_from(prm), 0, 0, 0, cores)
     t_build = time.perf_counter() - t0
-    z = nz // 2
-    done_vox, t_work = 0, 0.0
-    nslices = 1
+    z, done, t_work, nsl = nz // 2, 0, 0.0, 1
     while True:
-        v0, v1 = z * slab, min((z + nslices) * slab, nx * ny * nz)
+        v0, v1 = z * slab, min((z + nsl) * slab, nx * ny * nz)
         t0 = time.perf_counter()
         O.filter_voxels(mesh, O.material_from(mat), m2w, g, O.params_from(prm), v0, v1, 0, cores)
-        dt = time.perf_counter() - t0 - t_build
-        done_vox += v1 - v0
-        t_work += max(dt, 1e-9)
-        z += nslices
+        t_work += max(time.perf_counter() - t0 - t_build, 1e-9)
+        done += v1 - v0
+        z += nsl
         if t_work >= budget_s or z >= nz:
             break
-        rate = done_vox / t_work
-        nslices = max(1, min(int((budget_s - t_work) * rate / slab), nz - z))
-    return {"value": done_vox / t_work, "unit": "voxels/s", "cores": cores, "kind": "port",
-            "sample": f"{done_vox} voxels ({done_vox // slab} z-slices of {nx}x{ny} at the grid centre), "
-                      f"{FILTER_CFG['spv']} spv, BVH build ({t_build:.2f}s) excluded"}
+        nsl = max(1, min(int((budget_s - t_work) * (done / t_work) / slab), nz - z))
+    return {"value": done / t_work, "unit": "voxels/s", "cores": cores, "kind": "port",
+            "sample": f"{done // slab} z-slices of {nx}x{ny} at the grid centre, {FILTER_CFG['spv']} spv, "
+                      f"BVH build ({t_build:.2f}s) excluded"}
+
+
+# ------------------------------------------------------------------ native legs
+
+def bench_render(args, world, local):
+    import torch
+    from renderer2_b200 import render_scenes as RS
+    desc, cam, prm = render_workload()
+    sc = RS.build_scene(desc)
+    npix = cam.width * cam.height
+    frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup):
+        sc.render_device(cam, prm, frame.data_ptr(), stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    _barrier(world)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    st = np.zeros(8)
+    stats = []
+    ev0.record()
+    for _ in range(args.steps):
+        # inputs (BVH 21 MB nodes + 16 MB tris + state ~200 MB per wave) exceed L2; no flush needed
+        sc.render_device(cam, prm, frame.data_ptr(), stream, stats=st)
+        stats.append(st.copy())
+    ev1.record()
+    torch.cuda.synchronize()
+    _barrier(world)
+    ck = clocks.stop()
+    total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
+    paths = npix * prm.spp
+    value = world * paths * args.steps / (total_ms / 1e3)
+    st = np.mean(np.array(stats), axis=0)
+    seg, shadow = st[2], st[3]
+    ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
+    # dominant kernel over the frame: per-wave ms x spp
+    seg_wave, sh_wave = seg / prm.spp, 2.0 * seg / prm.spp
+    dom = "extend" if ms_wave["extend"] >= ms_wave["shadow"] else "shadow"
+    peak, peak_kind = _peaks()
+    if dom == "extend":
+        alg = EXTEND_BYTES_PER_SEGMENT * seg_wave
+        kname = "k_extend"
+    else:
+        alg = SHADOW_BYTES_PER_SLOT * sh_wave
+        kname = "k_shadow"
+    kms = ms_wave[dom]
+    launches = prm.max_depth
+    achieved = alg / (kms / 1e3) / 1e9
+    tr = _traffic(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tr["bytes_per_unit"] * (seg_wave if dom == "extend" else sh_wave) / launches)
+                if tr else None,
+                "alg_bytes_per_launch": alg / launches, "avg_launch_ms": kms / launches,
+                "note": "per-launch figures averaged over the bounces of the timed middle wave; "
+                        "traversal is L2/issue bound, see rays_per_s",
+                "rays_per_s": (seg + shadow) / (st[1] / 1e3), "kernel_ms_per_wave": ms_wave}
+    # end to end through the public API with host buffers: scene upload + BVH build + render + frame download
+    from renderer2_b200 import render_scenes as RS2
+    h2d = _input_bytes(desc)
+    e2e_ms = []
+    for _ in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = RS2.build_scene(desc)
+        s2.render(cam, prm)
+        s2.close()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    e2e = {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms}
+    sc.close()
+    launches_per_step = prm.spp * (2 + 4 * prm.max_depth)
+    return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths,
+                segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
+                desc=desc, cam=cam, prm=prm)
+
+
+def bench_filter(args, world, local):
+    import torch
+    from renderer2_b200 import filter as F
+    mesh, mat, prm, vs = filter_workload()
+    sc = F.FilterScene(mesh, mat)
+    g = sc.grid(vs)
+    nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+    out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    st = np.zeros(3)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
+    torch.cuda.synchronize()
+    _barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_ms, kernel_ms, cand = 0.0, [], []
+    for _ in range(args.steps):
+        flush.fill_(1)  # 256 MiB write evicts L2 between steps
+        ev0.record()
+        sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
+        ev1.record()
+        torch.cuda.synchronize()
+        step_ms += ev0.elapsed_time(ev1)
+        kernel_ms.append(st[2])
+        cand.append(st[1])
+    _barrier(world)
+    total_ms = _max_over_ranks(step_ms, world)
+    value = world * nvox * args.steps / (total_ms / 1e3)
+    h2d = mesh.positions.nbytes + mesh.indices.nbytes + mesh.normals.nbytes
+    e2e_ms = []
+    for _ in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        F.filter_mesh(mesh, mat, prm, vs)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    kms = float(np.mean(kernel_ms))
+    peak, peak_kind = _peaks()
+    alg = FILTER_BYTES_PER_VOXEL * nvox
+    achieved = alg / (kms / 1e3) / 1e9
+    tr = _traffic("k_filter_sample")
+    rays = float(np.mean(cand)) * FILTER_CFG["spv"]
+    sc.close()
+    return {"metric": "filtered voxels/s", "value": value, "unit": "voxels/s", "ms_per_step": total_ms / args.steps,
+            "config": {"workload": "filter at scale: 500k leaf quads (1M tris), 256^3, 256 spv, 20 iters",
+                       "voxels": nvox, "candidate_voxels": float(np.mean(cand)),
+                       "l2": "256 MiB flush write between steps"},
+            "roofline": {"bound": "hbm", "kernel": "k_filter_sample", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": tr["bytes_per_unit"] * float(np.mean(cand)) if tr else None,
+                         "kernel_ms": kms, "rays_per_s": rays / (kms / 1e3),
+                         "note": "36 B/voxel algorithmic; traversal/issue bound"},
+            "e2e": {"value": world * nvox / (e2e_ms / 1e3), "unit": "voxels/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(nvox * 32), "ms_per_step": e2e_ms},
+            "gpu_launches": 2 * args.steps, "_mesh": (mesh, mat, prm, vs)}
 
 
 def run_native(args):
@@ -180,81 +376,29 @@ def run_native(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     else:
         torch.cuda.set_device(0)
-    from renderer2_b200 import _native as N
-    from renderer2_b200 import filter as F
+    import renderer2_b200  # noqa: F401  (loads the native library)
 
-    mesh, mat, prm, vs = filter_workload()
-    sc = F.FilterScene(mesh, mat)
-    g = sc.grid(vs)
-    nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
-    out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream().cuda_stream
-    st = np.zeros(3)
-    kernel_ms = []
-    cand = []
-    for _ in range(args.warmup):
-        flush.fill_(1)
-        sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
-    torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
-    _barrier(world)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    step_ms = 0.0
-    for _ in range(args.steps):
-        flush.fill_(1)  # 256 MiB write evicts L2 between steps
-        ev0.record()
-        sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
-        ev1.record()
-        torch.cuda.synchronize()
-        step_ms += ev0.elapsed_time(ev1)
-        kernel_ms.append(st[2])
-        cand.append(st[1])
-    torch.cuda.synchronize()
-    _barrier(world)
-    ck = clocks.stop()
-    total_ms = _max_over_ranks(step_ms, world)
-    value = world * nvox * args.steps / (total_ms / 1e3)
-
-    # end to end through the host-buffer entry point (upload, BVH build, filter, download)
-    e2e_ms = []
-    h2d = mesh.positions.nbytes + mesh.indices.nbytes + mesh.normals.nbytes
-    for i in range(max(1, min(args.steps, 3))):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        F.filter_mesh(mesh, mat, prm, vs)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
-    e2e = {"value": world * nvox / (e2e_ms / 1e3), "unit": "voxels/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(nvox * 32), "ms_per_step": e2e_ms}
-
-    kms = float(np.mean(kernel_ms))
-    peak, peak_kind = _peaks()
-    alg_bytes = FILTER_BYTES_PER_VOXEL * nvox
-    achieved = alg_bytes / (kms / 1e3) / 1e9
-    rays = float(np.mean(cand)) * FILTER_CFG["spv"]
-    roofline = {"bound": "hbm", "kernel": "k_filter_sample", "achieved": achieved, "peak": peak,
-                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None, "kernel_ms": kms,
-                "note": "36 B/voxel algorithmic; the kernel is traversal/issue bound, rays/s below",
-                "rays_per_s": rays / (kms / 1e3)}
+    r = bench_render(args, world, local)
+    f = bench_filter(args, world, local) if not args.skip_filter else None
     if rank == 0:
-        cpu = cpu_filter_sample(mesh, mat, prm, vs, budget_s=args.cpu_budget) if world == 1 else None
-        line = {"metric": "filtered voxels/s", "value": value, "unit": "voxels/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded generators)",
-                "config": {"workload": "filter at scale: 500k leaf quads (1M tris), 256^3, 256 spv, 20 iters",
-                           "grid": [int(x) for x in g.num_voxels[:]], "voxels": nvox,
-                           "candidate_voxels": float(np.mean(cand)), "l2": "256 MiB flush write between steps",
-                           "parallelism": f"replicas x{world}"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 2 * args.steps,
-                "clocks": ck}
+        cpu = cpu_render_sample(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
+        line = {"metric": "paths/s", "value": r["value"], "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+                "config": {"workload": "surface path tracing: 8x8 displaced icospheres (327,680 tris), 512x256 "
+                                       "lognormal(0,1.5) env, 1024x1024, 64 spp, max depth 8",
+                           "paths_per_step": r["paths"], "segments_per_step": r["segments_per_frame"],
+                           "shadow_rays_per_step": r["shadow_rays_per_frame"],
+                           "l2": "inputs + wave state larger than L2", "parallelism": f"replicas x{world}"},
+                "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
+                "clocks": r["clocks"]}
+        if f is not None:
+            mesh, mat, prm, vs = f.pop("_mesh")
+            if world == 1:
+                f["cpu_baseline"] = cpu_filter_sample(mesh, mat, prm, vs, budget_s=args.cpu_budget)
+            line["filter"] = f
+            line["gpu_launches"] += f["gpu_launches"]
         print(json.dumps(line), flush=True)
-    sc.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -264,31 +408,36 @@ def run_reference(args):
     world, rank, _ = _dist_setup()
     if rank != 0:
         return
-    mesh, mat, prm, vs = filter_workload()
-    vals = []
+    desc, cam, prm = render_workload()
     for _ in range(args.warmup):
-        cpu_filter_sample(mesh, mat, prm, vs, budget_s=2.0)
-    for _ in range(args.steps):
-        vals.append(cpu_filter_sample(mesh, mat, prm, vs, budget_s=args.cpu_budget / max(1, args.steps)))
+        cpu_render_sample(desc, cam, prm, budget_s=1.0)
+    vals = [cpu_render_sample(desc, cam, prm, budget_s=args.cpu_budget / max(1, args.steps))
+            for _ in range(args.steps)]
     v = float(np.median([x["value"] for x in vals]))
     cpu = dict(vals[-1])
     cpu["value"] = v
-    line = {"impl": "reference", "metric": "filtered voxels/s", "value": v, "unit": "voxels/s", "n_gpus": world,
+    line = {"impl": "reference", "metric": "paths/s", "value": v, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-            "config": {"workload": "filter at scale: 500k leaf quads (1M tris), 256^3, 256 spv, 20 iters"},
-            "cpu_baseline": cpu, "e2e": {"value": v, "unit": "voxels/s", "h2d_bytes_per_step": 0,
-                                         "d2h_bytes_per_step": 0}}
+            "config": {"workload": "surface path tracing: 8x8 displaced icospheres (327,680 tris), 512x256 "
+                                   "lognormal(0,1.5) env, 1024x1024, 64 spp, max depth 8"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.skip_filter:
+        mesh, mat, fprm, vs = filter_workload()
+        fc = cpu_filter_sample(mesh, mat, fprm, vs, budget_s=max(5.0, args.cpu_budget / 2))
+        line["filter"] = {"metric": "filtered voxels/s", "value": fc["value"], "unit": "voxels/s", "cpu_baseline": fc}
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--skip-filter", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

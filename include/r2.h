@@ -146,6 +146,66 @@ r2_status r2_filter_scene_bvh(const r2_filter_scene* scene, int32_t* nodes, size
                               uint32_t* height_out);
 
 /* ------------------------------------------------------------------------ */
+/* Path tracer.
+ *
+ * Replaces rt::Raytracer (raytracer/raytracer.hpp:29-72): construction
+ * (raytracer.cu:129-152: scene upload, acceleration structure, samplers) and
+ * renderFrame (raytracer.cu:161-210: clear, one launch per sample of
+ * CPathIntegrator::Li, include/integrators/path_integrator_impl.hpp:120-247).
+ * The acceleration structure is this library's LBVH (no OptiX).  The frame
+ * is the linear, pre-tonemap radiance buffer of SFrame::data
+ * (common/frame.hpp:6-12): 3 floats per pixel, row 0 at the bottom. */
+typedef struct r2_scene r2_scene;
+
+/* CCamera(sensorWidth, sensorHeight, fov, pos, lookAt, up)
+ * (raytracer/include/camera/camera.hpp:27): fov is the horizontal FOV in degrees. */
+typedef struct r2_camera {
+  uint32_t width, height;
+  float fov_deg;
+  float pos[3];
+  float look_at[3];
+  float up[3];
+} r2_camera;
+
+typedef struct r2_render_params {
+  uint32_t spp;        /* "Samples" of config.json */
+  uint32_t max_depth;  /* bounce cap (the reference hard-codes 50) */
+  uint32_t seed;       /* Philox key word 1 */
+  uint32_t flags;      /* reserved, 0 */
+} r2_render_params;
+
+/* Object masks (raytracer/include/scene/sceneobject_mask.hpp:6-11). */
+#define R2_MASK_FILTER 1u
+#define R2_MASK_RENDER 2u
+#define R2_MASK_ALL 255u
+
+/* Analytic shapes of scenedescription.json (Type "Sphere" / "Circle"). */
+#define R2_SHAPE_SPHERE 0
+#define R2_SHAPE_CIRCLE 1
+
+r2_status r2_scene_create(r2_scene** out);
+r2_status r2_scene_destroy(r2_scene* scene);
+/* Adds a triangle mesh (model space) with one material and its T*R*S transform. */
+r2_status r2_scene_add_mesh(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
+                            uint32_t ntris, const float* normals, const r2_material* material,
+                            const float* model_to_world, uint32_t mask);
+r2_status r2_scene_add_shape(r2_scene* scene, int shape_type, const float* center, float radius,
+                             const float* normal, const r2_material* material, uint32_t mask);
+/* Environment map: width*height RGB float texels, row 0 = top (+Y). */
+r2_status r2_scene_set_envmap(r2_scene* scene, const float* rgb, uint32_t width, uint32_t height);
+/* Uploads the scene and builds the BVH (device-resident until destroyed). */
+r2_status r2_scene_commit(r2_scene* scene);
+/* Renders one frame into device memory d_rgb (width*height*3 floats).
+ * stats_out (nullable, 8 doubles): [0] paths, [1] milliseconds of the frame on
+ * the stream, [2] path segments traced, [3] shadow rays traced, [4..7]
+ * milliseconds of the extend / shade / shadow / accumulate kernels of one
+ * (the middle) wave. */
+r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* d_rgb,
+                           void* stream, double* stats_out);
+/* Same through host memory: commits if needed, renders, copies the frame to rgb. */
+r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* rgb);
+
+/* ------------------------------------------------------------------------ */
 /* Synthetic inputs (seeded), used by the configs in the benchmark plan. */
 
 /* Icosphere of subdivision level `subdiv` (20*4^subdiv triangles) of radius 1,

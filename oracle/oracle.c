@@ -4,6 +4,7 @@
  * expression rounds like the device code (which is built with -fmad=false).
  */
 #include "oracle.h"
+#include "oracle_internal.h"
 
 #include <math.h>
 #include <pthread.h>
@@ -29,7 +30,7 @@ void orc_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key[2], uint32_t
   out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-static float u01(uint32_t b) { return (float)(b >> 8) * (1.0f / 16777216.0f); }
+#define u01 oi_u01
 
 /* sin/cos of u turns: Taylor series on [-pi/4, pi/4] after exact quadrant
  * reduction; the same operation sequence as the device code. */
@@ -55,27 +56,6 @@ void orc_sincos_turns(float u, float* s, float* c) {
 }
 
 /* ---------------------------------------------------------------- vectors */
-
-typedef struct { float x, y, z; } f3;
-static f3 F3(float x, float y, float z) { f3 r = {x, y, z}; return r; }
-static f3 add3(f3 a, f3 b) { return F3(a.x + b.x, a.y + b.y, a.z + b.z); }
-static f3 sub3(f3 a, f3 b) { return F3(a.x - b.x, a.y - b.y, a.z - b.z); }
-static f3 mul3s(f3 a, float s) { return F3(a.x * s, a.y * s, a.z * s); }
-static float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-static f3 norm3(f3 a) { return mul3s(a, 1.0f / sqrtf(dot3(a, a))); }
-static float comp3(f3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
-
-/* glm mat4x3 * vec4(p, 1) / vec4(v, 0), left-to-right accumulation. */
-static f3 xpoint(const float* m, f3 p) {
-  return F3(m[0] * p.x + m[3] * p.y + m[6] * p.z + m[9] * 1.0f,
-            m[1] * p.x + m[4] * p.y + m[7] * p.z + m[10] * 1.0f,
-            m[2] * p.x + m[5] * p.y + m[8] * p.z + m[11] * 1.0f);
-}
-static f3 xvec(const float* m, f3 v) {
-  return F3(m[0] * v.x + m[3] * v.y + m[6] * v.z + m[9] * 0.0f,
-            m[1] * v.x + m[4] * v.y + m[7] * v.z + m[10] * 0.0f,
-            m[2] * v.x + m[5] * v.y + m[8] * v.z + m[11] * 0.0f);
-}
 
 /* ---------------------------------------------------------------- LBVH */
 
@@ -386,7 +366,6 @@ static int slab(const rpre_t* r, const float* b, int slot, float tmax, float* te
   return tn <= tf;
 }
 
-typedef struct { float t, b1, b2; int tri; } hit_t;
 
 static int tri_test(const rpre_t* r, f3 p0, f3 p1, f3 p2, int tri, hit_t* best) {
   f3 A = sub3(p0, r->o), B = sub3(p1, r->o), C = sub3(p2, r->o);
@@ -423,7 +402,7 @@ static int tri_test(const rpre_t* r, f3 p0, f3 p1, f3 p2, int tri, hit_t* best) 
   return 0;
 }
 
-static hit_t trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax) {
+hit_t oi_trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, int any_hit) {
   hit_t best;
   best.t = tmax;
   best.b1 = best.b2 = 0.0f;
@@ -455,8 +434,10 @@ static hit_t trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tm
       for (int i = 0; i < count; ++i) {
         int tri = first + i;
         const float* tv = &tris[12 * (size_t)tri];
-        if (tri_test(&r, F3(tv[0], tv[1], tv[2]), F3(tv[4], tv[5], tv[6]), F3(tv[8], tv[9], tv[10]), tri, &best))
+        if (tri_test(&r, F3(tv[0], tv[1], tv[2]), F3(tv[4], tv[5], tv[6]), F3(tv[8], tv[9], tv[10]), tri, &best)) {
           found = 1;
+          if (any_hit) return best;
+        }
       }
     }
     for (;;) {
@@ -473,7 +454,7 @@ static hit_t trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tm
 
 int orc_trace(const int32_t* nodes, const float* tris, float ox, float oy, float oz, float dx, float dy, float dz,
               float tmax, float* t, float* b1, float* b2) {
-  hit_t h = trace(nodes, tris, F3(ox, oy, oz), F3(dx, dy, dz), tmax);
+  hit_t h = oi_trace(nodes, tris, F3(ox, oy, oz), F3(dx, dy, dz), tmax, 0);
   *t = h.t;
   *b1 = h.b1;
   *b2 = h.b2;
@@ -482,15 +463,14 @@ int orc_trace(const int32_t* nodes, const float* tris, float ox, float oy, float
 
 /* ---------------------------------------------------------------- grid setup */
 
-typedef struct { float m[4][4]; } m4_t; /* m[col][row] */
 
-static m4_t m4_id(void) {
+m4_t oi_m4_id(void) {
   m4_t r;
   memset(&r, 0, sizeof(r));
   for (int i = 0; i < 4; ++i) r.m[i][i] = 1.0f;
   return r;
 }
-static m4_t m4_mul(m4_t a, m4_t b) {
+m4_t oi_m4_mul(m4_t a, m4_t b) {
   m4_t r;
   for (int j = 0; j < 4; ++j)
     for (int i = 0; i < 4; ++i) {
@@ -502,7 +482,7 @@ static m4_t m4_mul(m4_t a, m4_t b) {
     }
   return r;
 }
-static m4_t m4_inv(m4_t a) {
+m4_t oi_m4_inv(m4_t a) {
   double A[4][8];
   for (int r = 0; r < 4; ++r) {
     for (int c = 0; c < 4; ++c) A[r][c] = a.m[c][r];
@@ -515,7 +495,7 @@ static m4_t m4_inv(m4_t a) {
     if (piv != c)
       for (int k = 0; k < 8; ++k) { double t = A[c][k]; A[c][k] = A[piv][k]; A[piv][k] = t; }
     double p = A[c][c];
-    if (p == 0.0) return m4_id();
+    if (p == 0.0) return oi_m4_id();
     for (int k = 0; k < 8; ++k) A[c][k] /= p;
     for (int r = 0; r < 4; ++r) {
       if (r == c) continue;
@@ -537,7 +517,7 @@ static m4_t m4_from43(const float* f) {
   }
   return r;
 }
-static void m4_to43(m4_t a, float* f) {
+void oi_m4_to43(m4_t a, float* f) {
   for (int c = 0; c < 4; ++c) { f[3 * c] = a.m[c][0]; f[3 * c + 1] = a.m[c][1]; f[3 * c + 2] = a.m[c][2]; }
 }
 
@@ -547,28 +527,28 @@ void orc_setup_grid(const float* mlo, const float* mhi, const float* m2w, float 
   f3 a = xpoint(m2w, F3(mlo[0], mlo[1], mlo[2])), b = xpoint(m2w, F3(mhi[0], mhi[1], mhi[2]));
   f3 wlo = F3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z));
   f3 whi = F3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z));
-  m4_t w2m = m4_inv(m4_from43(m2w));
+  m4_t w2m = oi_m4_inv(m4_from43(m2w));
   f3 ext = sub3(whi, wlo);
   int nv[3] = {(int)ceilf(ext.x / vs - 0.001f), (int)ceilf(ext.y / vs - 0.001f), (int)ceilf(ext.z / vs - 0.001f)};
   for (int k = 0; k < 3; ++k) g->num_voxels[k] = nv[k];
-  m4_t T = m4_id(), S1 = m4_id(), S2 = m4_id();
+  m4_t T = oi_m4_id(), S1 = oi_m4_id(), S2 = oi_m4_id();
   T.m[3][0] = wlo.x; T.m[3][1] = wlo.y; T.m[3][2] = wlo.z;
   S1.m[0][0] = ext.x; S1.m[1][1] = ext.y; S1.m[2][2] = ext.z;
   S2.m[0][0] = 1.0f / (float)nv[0]; S2.m[1][1] = 1.0f / (float)nv[1]; S2.m[2][2] = 1.0f / (float)nv[2];
-  m4_t i2m = m4_mul(m4_mul(m4_mul(w2m, T), S1), S2);
-  m4_t m2i = m4_inv(i2m);
-  m4_t m2wI = m4_inv(w2m);
-  m4_t i2w = m4_mul(m2wI, i2m);
+  m4_t i2m = oi_m4_mul(oi_m4_mul(oi_m4_mul(w2m, T), S1), S2);
+  m4_t m2i = oi_m4_inv(i2m);
+  m4_t m2wI = oi_m4_inv(w2m);
+  m4_t i2w = oi_m4_mul(m2wI, i2m);
   float i2w43[12];
-  m4_to43(i2w, i2w43);
+  oi_m4_to43(i2w, i2w43);
   f3 p0 = xpoint(i2w43, F3(0.0f, 0.0f, 0.0f));
   f3 p1 = xpoint(i2w43, F3((float)nv[0], (float)nv[1], (float)nv[2]));
   g->world_bb_min[0] = fminf(p0.x, p1.x); g->world_bb_min[1] = fminf(p0.y, p1.y); g->world_bb_min[2] = fminf(p0.z, p1.z);
   g->world_bb_max[0] = fmaxf(p0.x, p1.x); g->world_bb_max[1] = fmaxf(p0.y, p1.y); g->world_bb_max[2] = fmaxf(p0.z, p1.z);
-  m4_to43(i2m, g->index_to_model);
-  m4_to43(m2i, g->model_to_index);
-  m4_to43(m2wI, g->model_to_world);
-  m4_to43(w2m, g->world_to_model);
+  oi_m4_to43(i2m, g->index_to_model);
+  oi_m4_to43(m2i, g->model_to_index);
+  oi_m4_to43(m2wI, g->model_to_world);
+  oi_m4_to43(w2m, g->world_to_model);
   g->voxel_size = vs;
 }
 
@@ -676,7 +656,7 @@ static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
   int x = (int)(vid % (uint64_t)nx), y = (int)((vid / (uint64_t)nx) % (uint64_t)ny),
       z = (int)(vid / ((uint64_t)nx * (uint64_t)ny));
   float i2w[12];
-  m4_to43(m4_mul(m4_from43(g->model_to_world), m4_from43(g->index_to_model)), i2w);
+  oi_m4_to43(oi_m4_mul(m4_from43(g->model_to_world), m4_from43(g->index_to_model)), i2w);
   f3 wlo = F3(g->world_bb_min[0], g->world_bb_min[1], g->world_bb_min[2]);
   f3 whi = F3(g->world_bb_max[0], g->world_bb_max[1], g->world_bb_max[2]);
   f3 ext = sub3(whi, wlo);
@@ -704,7 +684,7 @@ static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
     orc_sincos_turns(u01(r1[0]), &sn, &cs);
     f3 d = F3(rr * cs, rr * sn, zz);
     float tmax = p->clip_rays ? sphere_exit(o, d, center, radius) : tmaxFixed;
-    hit_t h = trace(J->nodes, J->tris, o, d, tmax);
+    hit_t h = oi_trace(J->nodes, J->tris, o, d, tmax, 0);
     if (h.tri < 0) continue;
     uint32_t prim = J->order[h.tri];
     const uint32_t* tv = &J->idx[3 * (size_t)prim];

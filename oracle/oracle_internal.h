@@ -1,0 +1,53 @@
+/*
+ * Internal helpers shared by the oracle's translation units (test
+ * infrastructure only).  Float expressions keep the device code's order.
+ */
+#ifndef R2_ORACLE_INTERNAL_H
+#define R2_ORACLE_INTERNAL_H
+#include <math.h>
+#include <stdint.h>
+
+typedef struct { float x, y, z; } f3;
+static inline f3 F3(float x, float y, float z) { f3 r = {x, y, z}; return r; }
+static inline f3 add3(f3 a, f3 b) { return F3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline f3 sub3(f3 a, f3 b) { return F3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline f3 mul3(f3 a, f3 b) { return F3(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline f3 mul3s(f3 a, float s) { return F3(a.x * s, a.y * s, a.z * s); }
+static inline f3 div3s(f3 a, float s) { return F3(a.x / s, a.y / s, a.z / s); }
+static inline f3 neg3(f3 a) { return F3(-a.x, -a.y, -a.z); }
+static inline float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline f3 cross3(f3 a, f3 b) {
+  return F3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+static inline float len3(f3 a) { return sqrtf(dot3(a, a)); }
+static inline f3 norm3(f3 a) { return mul3s(a, 1.0f / sqrtf(dot3(a, a))); }
+static inline float comp3(f3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+static inline f3 abs3(f3 a) { return F3(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+
+/* glm mat4x3 * vec4(p, 1) / vec4(v, 0), left-to-right accumulation. */
+static inline f3 xpoint(const float* m, f3 p) {
+  return F3(m[0] * p.x + m[3] * p.y + m[6] * p.z + m[9] * 1.0f,
+            m[1] * p.x + m[4] * p.y + m[7] * p.z + m[10] * 1.0f,
+            m[2] * p.x + m[5] * p.y + m[8] * p.z + m[11] * 1.0f);
+}
+static inline f3 xvec(const float* m, f3 v) {
+  return F3(m[0] * v.x + m[3] * v.y + m[6] * v.z + m[9] * 0.0f,
+            m[1] * v.x + m[4] * v.y + m[7] * v.z + m[10] * 0.0f,
+            m[2] * v.x + m[5] * v.y + m[8] * v.z + m[11] * 0.0f);
+}
+
+typedef struct { float t, b1, b2; int tri; } hit_t;
+
+/* Closest (any_hit = 0) or first found (any_hit = 1) hit in (0, tmax]. */
+hit_t oi_trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, int any_hit);
+
+static inline float oi_u01(uint32_t b) { return (float)(b >> 8) * (1.0f / 16777216.0f); }
+
+/* 4x4 helpers (m[col][row]) */
+typedef struct { float m[4][4]; } m4_t;
+m4_t oi_m4_id(void);
+m4_t oi_m4_mul(m4_t a, m4_t b);
+m4_t oi_m4_inv(m4_t a);
+void oi_m4_to43(m4_t a, float* f);
+
+#endif

@@ -1,0 +1,64 @@
+/*
+ * CPU oracle of the path tracer — TEST INFRASTRUCTURE ONLY (see oracle.h for
+ * who may call it).
+ *
+ * Restates CPathIntegrator::Li and direct()
+ * (raytracer/include/integrators/path_integrator_impl.hpp:23-247) for surface
+ * scenes lit by the environment map, with the reference's materials
+ * (material.hpp:67-100, microfacet_brdf.hpp:57-100, microfacet_distribution.hpp:40-141,
+ * oren_nayar_brdf.hpp:36-81, fresnel.hpp:28-54), environment sampling
+ * (environmentmap.hpp:28-55, distribution_1d.hpp:54-122, distribution_2d.hpp:50-84,
+ * environmentmap.cu:16-29) and camera (camera.cu:20-37, pixel_sampler.hpp:36-47),
+ * one path at a time, with the same Philox streams as the GPU wavefront.
+ */
+#ifndef R2_RENDER_ORACLE_H
+#define R2_RENDER_ORACLE_H
+#include <stdint.h>
+
+#include "oracle.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_mesh {
+  const float* positions; /* model space, 3 per vertex */
+  uint32_t nverts;
+  const uint32_t* indices;
+  uint32_t ntris;
+  const float* normals;
+  float model_to_world[12];
+  orc_material material;
+} orc_mesh;
+
+typedef struct orc_shape {
+  int type; /* 0 sphere, 1 circle */
+  float center[3];
+  float radius;
+  float normal[3];
+  orc_material material;
+} orc_shape;
+
+typedef struct orc_camera {
+  uint32_t width, height;
+  float fov_deg;
+  float pos[3], look_at[3], up[3];
+} orc_camera;
+
+/* Renders pixels [p0, p1) (row-major, row 0 = bottom) with spp samples.
+ * rgb_out: 3 floats per pixel, the frame accumulation sum_s L_s / spp;
+ * var_out (nullable): per pixel and channel, the unbiased sample variance of
+ * L_s.  Returns 0 on success. */
+int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes, uint32_t nshapes,
+               const float* env_rgb, int env_w, int env_h, const orc_camera* cam, uint32_t spp, uint32_t max_depth,
+               uint32_t seed, uint32_t p0, uint32_t p1, float* rgb_out, double* var_out, int threads);
+
+/* Environment sampling primitives, exposed for unit tests. */
+int orc_env_sample(const float* env_rgb, int env_w, int env_h, float u0, float u1, float* dir_out, float* pdf_out,
+                   float* le_out);
+int orc_env_le(const float* env_rgb, int env_w, int env_h, const float* dir, float* pdf_out, float* le_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -71,6 +71,14 @@ def _load():
         "r2_filter_scene_grid": (C.c_int, [P, f32, P]),
         "r2_filter_scene_run": (C.c_int, [P, P, P, P, P, P, P, P]),
         "r2_filter_scene_bvh": (C.c_int, [P, P, sz, P, sz, P, P]),
+        "r2_scene_create": (C.c_int, [P]),
+        "r2_scene_destroy": (C.c_int, [P]),
+        "r2_scene_add_mesh": (C.c_int, [P, P, u32, P, u32, P, P, P, u32]),
+        "r2_scene_add_shape": (C.c_int, [P, C.c_int, P, f32, P, P, u32]),
+        "r2_scene_set_envmap": (C.c_int, [P, P, u32, u32]),
+        "r2_scene_commit": (C.c_int, [P]),
+        "r2_render_device": (C.c_int, [P, P, P, P, P, P]),
+        "r2_render_host": (C.c_int, [P, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -1,0 +1,85 @@
+// C ABI: path tracer scene and frame entry points.
+#include <memory>
+
+#include "capi_util.h"
+#include "render_host.h"
+
+struct r2_scene {
+  std::unique_ptr<r2::RenderScene> impl;
+};
+
+extern "C" {
+
+r2_status r2_scene_create(r2_scene** out) {
+  R2_API_BEGIN
+  R2_REQUIRE(out, R2_ERR_INVALID_ARGUMENT, "null argument");
+  r2::require_device();
+  auto sc = new r2_scene;
+  try {
+    sc->impl.reset(new r2::RenderScene());
+  } catch (...) {
+    delete sc;
+    throw;
+  }
+  *out = sc;
+  R2_API_END
+}
+
+r2_status r2_scene_destroy(r2_scene* scene) {
+  R2_API_BEGIN
+  delete scene;
+  R2_API_END
+}
+
+r2_status r2_scene_add_mesh(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
+                            uint32_t ntris, const float* normals, const r2_material* material,
+                            const float* model_to_world, uint32_t mask) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && material, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->add_mesh(positions, nverts, indices, ntris, normals, *material, model_to_world, mask);
+  R2_API_END
+}
+
+r2_status r2_scene_add_shape(r2_scene* scene, int shape_type, const float* center, float radius, const float* normal,
+                             const r2_material* material, uint32_t mask) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && material && center, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->add_shape(shape_type, center, radius, normal, *material, mask);
+  R2_API_END
+}
+
+r2_status r2_scene_set_envmap(r2_scene* scene, const float* rgb, uint32_t width, uint32_t height) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->set_envmap(rgb, (int)width, (int)height);
+  R2_API_END
+}
+
+r2_status r2_scene_commit(r2_scene* scene) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->commit();
+  R2_API_END
+}
+
+r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* d_rgb,
+                           void* stream, double* stats_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && camera && params && d_rgb, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->render(*camera, *params, d_rgb, (cudaStream_t)stream, stats_out);
+  R2_API_END
+}
+
+r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* rgb) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && camera && params && rgb, R2_ERR_INVALID_ARGUMENT, "null argument");
+  size_t n = (size_t)camera->width * camera->height * 3;
+  r2::DBuf<float> d(n);
+  cudaStream_t s = scene->impl->stream();
+  scene->impl->render(*camera, *params, d.get(), s, nullptr);
+  d.download(rgb, n, s);
+  R2_CUDA(cudaStreamSynchronize(s));
+  R2_API_END
+}
+
+}  // extern "C"

@@ -96,7 +96,10 @@ __device__ __forceinline__ void write_empty(const FilterLaunch& L, size_t vid) {
 
 __global__ void __launch_bounds__(256) k_filter_classify(FilterLaunch L) {
   const size_t nvox = (size_t)L.nx * L.ny * L.nz;
-  const float radius = 1.1f * length(L.voxelSize) / 2.0f;
+  // Reach of a filter ray from the voxel centre: with ClipRays the ray ends on
+  // the bounding sphere; otherwise it starts anywhere in the voxel and runs
+  // voxelSize.x (mesh_filter.hpp:72-82).
+  const float radius = L.clip ? 1.1f * length(L.voxelSize) / 2.0f : length(L.voxelSize) / 2.0f + L.voxelSize.x;
   const float rq = radius * 1.001f + 1e-6f;
   const int lane = threadIdx.x & 31;
   const size_t stride = (size_t)gridDim.x * blockDim.x;

@@ -1,0 +1,76 @@
+// Wavefront path tracer: launch description shared by the kernels (render.cu)
+// and the host runtime (render_host.cu).
+#pragma once
+#include "bvh_build.cuh"
+#include "shading.h"
+
+namespace r2 {
+
+// Analytic scene objects of the reference's scene description (Circle,
+// Sphere; include/shapes/circle.hpp:35-60, sphere.hpp:33-90).
+enum ShapeType : int { kShapeSphere = 0, kShapeCircle = 1 };
+
+struct Shape {
+  int type;
+  int material;
+  float radius;
+  float pad;
+  V3 center;
+  V3 normal;
+};
+
+// Device view of a committed scene.
+struct SceneView {
+  BvhView bvh;
+  const float4* triN;      // 3 per BVH-order triangle: world-space vertex normals
+  const uint32_t* triMat;  // per BVH-order triangle: material index
+  const Material* mats;
+  const Shape* shapes;
+  int nshapes;
+  int hasTris;
+  EnvMap env;
+};
+
+// Per-path SoA state of one wave (one sample of every pixel).
+struct PathState {
+  float4* rayO;     // origin
+  float4* rayD;     // direction
+  float4* T;        // throughput
+  float4* L;        // radiance
+  float4* hit;      // t, b1, b2, prim code (as int bits: >=0 tri, <= -2 shape, -1 miss)
+  uint32_t* q[2];   // ping-pong queues of live path ids
+  uint32_t* counts; // [bounce] live path count entering the bounce
+  // shadow records, two per queue slot (0: light sample, 1: BSDF sample)
+  float4* shO;      // origin.xyz, pdf (0 = no ray)
+  float4* shD;      // direction.xyz, unused
+  float4* shPre;    // (mis * f) * Le
+  float4* shT;      // throughput at the bounce (one per slot pair)
+  uint8_t* vis;     // visibility of each shadow ray
+};
+
+struct RenderLaunch {
+  SceneView scene;
+  Camera cam;
+  PathState st;
+  float* frame;       // W*H*3 linear RGB, row 0 = bottom (SFrame layout)
+  uint32_t npix;
+  uint32_t sample;    // sample index of the wave
+  uint32_t spp;
+  uint32_t maxDepth;
+  uint32_t seed;
+  uint32_t bounce;
+  unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
+};
+
+// Optional per-kernel timing of one wave: events recorded after each launch;
+// kind: -1 start, 0 camera, 1 extend, 2 shade, 3 shadow, 4 accum, 5 finish.
+struct WaveTimer {
+  static constexpr int kMax = 6 + 4 * 64;
+  cudaEvent_t ev[kMax];
+  int kind[kMax];
+  int n = 0;
+};
+
+void launch_render_wave(const RenderLaunch& L, int nblocks, cudaStream_t s, WaveTimer* tm = nullptr);
+
+}  // namespace r2

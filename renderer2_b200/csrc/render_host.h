@@ -1,0 +1,73 @@
+// Host side of the path tracer: scene assembly (meshes flattened to world
+// space, analytic shapes, environment map with the reference's distributions),
+// camera setup and the per-sample wave loop.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "render.cuh"
+
+namespace r2 {
+
+// CCamera (raytracer/src/camera/camera.cu:20-37): 10 um pixels, near plane
+// from the horizontal field of view, view matrix glm::lookAt.
+Camera make_camera(const r2_camera& c);
+
+// Environment map distributions built exactly like CEnvironmentMap
+// (src/scene/environmentmap.cu:11-29) and CDistribution1D/2D
+// (src/sampling/distribution_1d.cu:6-39, distribution_2d.cu:7-14, .hpp:59-71).
+struct EnvHost {
+  int W = 0, H = 0;
+  std::vector<float4> tex;
+  std::vector<float> margFunc, margCdf, rowFunc, rowCdf, rowFuncInt;
+  float margFuncInt = 0.0f;
+};
+void build_env(const float* rgb, int W, int H, EnvHost* e);
+
+class RenderScene {
+ public:
+  RenderScene();
+  ~RenderScene();
+  RenderScene(const RenderScene&) = delete;
+  RenderScene& operator=(const RenderScene&) = delete;
+
+  void add_mesh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
+                const r2_material& mat, const float* modelToWorld, uint32_t mask);
+  void add_shape(int type, const float* center, float radius, const float* normal, const r2_material& mat,
+                 uint32_t mask);
+  void set_envmap(const float* rgb, int W, int H);
+  void commit();
+  // One frame: `spp` waves accumulated into d_frame (W*H*3 floats, cleared here).
+  void render(const r2_camera& cam, const r2_render_params& p, float* d_frame, cudaStream_t s, double* stats);
+  cudaStream_t stream() const { return stream_; }
+  uint32_t ntris() const { return (uint32_t)(hIdx_.size() / 3); }
+  const DeviceBvh& bvh() const { return bvh_; }
+
+ private:
+  void ensure_state(uint32_t npix);
+  cudaStream_t stream_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  bool committed_ = false;
+  std::vector<float> hPos_, hNrm_;
+  std::vector<uint32_t> hIdx_, hTriMat_;
+  std::vector<Material> hMats_;
+  std::vector<Shape> hShapes_;
+  EnvHost env_;
+  DeviceBvh bvh_;
+  DBuf<float4> triN_;
+  DBuf<uint32_t> triMat_;
+  DBuf<Material> mats_;
+  DBuf<Shape> shapes_;
+  DBuf<float4> envTex_;
+  DBuf<float> envBuf_;
+  SceneView view_;
+  // wave state
+  uint32_t cap_ = 0;
+  DBuf<float4> rayO_, rayD_, T_, L_, hit_, shO_, shD_, shPre_, shT_;
+  DBuf<uint32_t> q0_, q1_, counts_;
+  DBuf<uint8_t> vis_;
+  DBuf<unsigned long long> statBuf_;
+  std::unique_ptr<WaveTimer> timer_;
+};
+
+}  // namespace r2

@@ -1,0 +1,96 @@
+"""Python view of the path tracer entry points (C ABI in include/r2.h).
+
+Mirrors rt::Raytracer (raytracer/raytracer.hpp:29-72): a scene is committed
+once (LBVH built on the device) and renderFrame produces the linear radiance
+buffer of SFrame::data (3 floats per pixel, row 0 = bottom) before tonemapping.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class Camera(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov_deg", C.c_float), ("pos", C.c_float * 3),
+                ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("spp", C.c_uint32), ("max_depth", C.c_uint32), ("seed", C.c_uint32), ("flags", C.c_uint32)]
+
+
+def camera(width, height, fov_deg=45.0, pos=(0, 0, 3), look_at=(0, 0, 0), up=(0, 1, 0)) -> Camera:
+    c = Camera()
+    c.width, c.height, c.fov_deg = int(width), int(height), float(fov_deg)
+    c.pos[:] = list(map(float, pos))
+    c.look_at[:] = list(map(float, look_at))
+    c.up[:] = list(map(float, up))
+    return c
+
+
+def params(spp=16, max_depth=8, seed=0) -> RenderParams:
+    p = RenderParams()
+    p.spp, p.max_depth, p.seed, p.flags = int(spp), int(max_depth), int(seed), 0
+    return p
+
+
+SPHERE, CIRCLE = 0, 1
+
+
+class Scene:
+    """Device-resident render scene (r2_scene_*)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        N.check(N.lib.r2_scene_create(C.byref(h)))
+        self.handle = h
+        self._keep = []
+
+    def close(self):
+        if self.handle:
+            N.check(N.lib.r2_scene_destroy(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_mesh(self, mesh, material, model_to_world=None, mask=255):
+        pos = np.ascontiguousarray(mesh.positions, np.float32)
+        idx = np.ascontiguousarray(mesh.indices, np.uint32)
+        nrm = np.ascontiguousarray(mesh.normals, np.float32)
+        m2w = np.ascontiguousarray(N.identity43() if model_to_world is None else model_to_world, np.float32)
+        N.check(N.lib.r2_scene_add_mesh(self.handle, N.ptr(pos), pos.shape[0], N.ptr(idx), idx.shape[0], N.ptr(nrm),
+                                        C.byref(material), N.ptr(m2w), mask))
+
+    def add_shape(self, kind, center, radius, normal, material, mask=255):
+        c = np.ascontiguousarray(center, np.float32)
+        n = np.ascontiguousarray(normal, np.float32)
+        N.check(N.lib.r2_scene_add_shape(self.handle, int(kind), N.ptr(c), float(radius), N.ptr(n), C.byref(material),
+                                         mask))
+
+    def set_envmap(self, rgb: np.ndarray):
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w, _ = rgb.shape
+        N.check(N.lib.r2_scene_set_envmap(self.handle, N.ptr(rgb), w, h))
+
+    def commit(self):
+        N.check(N.lib.r2_scene_commit(self.handle))
+
+    def render_device(self, cam: Camera, prm: RenderParams, d_rgb: int, stream: int = 0, stats=None):
+        st = np.zeros(8, np.float64)
+        N.check(N.lib.r2_render_device(self.handle, C.byref(cam), C.byref(prm), C.c_void_p(d_rgb),
+                                       C.c_void_p(stream or None), N.ptr(st)))
+        if stats is not None:
+            stats[:] = st
+        return st
+
+    def render(self, cam: Camera, prm: RenderParams) -> np.ndarray:
+        out = np.zeros((cam.height, cam.width, 3), np.float32)
+        N.check(N.lib.r2_render_host(self.handle, C.byref(cam), C.byref(prm), N.ptr(out)))
+        return out

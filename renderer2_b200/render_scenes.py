@@ -1,0 +1,64 @@
+"""Seeded synthetic render scenes of the benchmark configurations."""
+from __future__ import annotations
+
+import numpy as np
+
+from . import filter as F
+from . import raytracer as R
+from . import scenes
+
+
+def white_env(w: int = 4, h: int = 2) -> np.ndarray:
+    """Constant white environment (radiance 1 in every direction)."""
+    return np.ones((h, w, 3), np.float32)
+
+
+def lognormal_env(w: int = 512, h: int = 256, sigma: float = 1.5, seed: int = 3) -> np.ndarray:
+    """Procedural HDR map: every channel of every texel ~ lognormal(0, sigma)."""
+    rng = np.random.default_rng(seed)
+    return rng.lognormal(0.0, sigma, size=(h, w, 3)).astype(np.float32)
+
+
+def translate43(x, y, z):
+    m = np.zeros(12, np.float32)
+    m[0] = m[4] = m[8] = 1.0
+    m[9:12] = (x, y, z)
+    return m
+
+
+def c1_scene():
+    """Config 1: icosphere sub 4 (5,120 tris), GGX roughness 0.3 albedo 0.8, constant white env;
+    camera (0,0,3) -> origin, fov 45."""
+    mesh = scenes.icosphere(4, 0.05, 1)
+    mat = F.material(diffuse=(0.8, 0.8, 0.8), specular=(1.0, 1.0, 1.0), alpha=0.3, ior=1.5)
+    desc = {"meshes": [(mesh, mat, translate43(0, 0, 0))], "shapes": [], "env": white_env()}
+    cam = R.camera(256, 256, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
+    return desc, cam
+
+
+def c2_scene():
+    """Config 2: 8x8 grid of displaced icospheres (64 x 5,120 = 327,680 tris), per-object GGX
+    roughness U[0.05, 1] and albedo U[0.2, 0.9] (seed 2), lognormal(0, 1.5) 512x256 env (seed 3)."""
+    rng = np.random.default_rng(2)
+    meshes = []
+    for k in range(64):
+        i, j = k % 8, k // 8
+        mesh = scenes.icosphere(4, 0.05, k + 1)
+        a = float(rng.uniform(0.05, 1.0))
+        alb = float(rng.uniform(0.2, 0.9))
+        mat = F.material(diffuse=(alb, alb, alb), specular=(1.0, 1.0, 1.0), alpha=a, ior=1.5)
+        meshes.append((mesh, mat, translate43(-8.75 + 2.5 * i, -8.75 + 2.5 * j, 0.0)))
+    desc = {"meshes": meshes, "shapes": [], "env": lognormal_env()}
+    cam = R.camera(1024, 1024, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+    return desc, cam
+
+
+def build_scene(desc) -> R.Scene:
+    sc = R.Scene()
+    for mesh, mat, m2w in desc.get("meshes", []):
+        sc.add_mesh(mesh, mat, m2w)
+    for kind, c, r, n, mat in desc.get("shapes", []):
+        sc.add_shape(kind, c, r, n, mat)
+    sc.set_envmap(desc["env"])
+    sc.commit()
+    return sc

@@ -142,3 +142,65 @@ def filter_voxels(mesh, mat, m2w, grid, prm, v0=0, v1=None, lod=0, threads=0):
                        C.byref(grid), C.byref(prm), lod, v0, v1, _p(wide), _p(comp), threads)
     assert r >= 0, f"oracle filter failed ({r})"
     return wide, comp
+
+
+# ---------------------------------------------------------------- path tracer oracle
+
+class OMesh(C.Structure):
+    _fields_ = [("positions", C.c_void_p), ("nverts", C.c_uint32), ("indices", C.c_void_p), ("ntris", C.c_uint32),
+                ("normals", C.c_void_p), ("model_to_world", C.c_float * 12), ("material", Material)]
+
+
+class OShape(C.Structure):
+    _fields_ = [("type", C.c_int), ("center", C.c_float * 3), ("radius", C.c_float), ("normal", C.c_float * 3),
+                ("material", Material)]
+
+
+class OCamera(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fov_deg", C.c_float), ("pos", C.c_float * 3),
+                ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
+
+
+lib.orc_render.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                           C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+lib.orc_render.restype = C.c_int
+lib.orc_env_sample.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
+lib.orc_env_le.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+
+
+def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want_var=False):
+    """scene_desc: dict(meshes=[(Mesh, native material, m2w)], shapes=[(kind, center, radius, normal, material)],
+    env=(H, W, 3) float32).  Returns rgb (n, 3) [, var (n, 3)] for pixels [p0, p1)."""
+    keep = []
+    meshes = (OMesh * max(1, len(scene_desc.get("meshes", []))))()
+    for i, (mesh, mat, m2w) in enumerate(scene_desc.get("meshes", [])):
+        pos = np.ascontiguousarray(mesh.positions, np.float32)
+        idx = np.ascontiguousarray(mesh.indices, np.uint32)
+        nrm = np.ascontiguousarray(mesh.normals, np.float32)
+        keep += [pos, idx, nrm]
+        meshes[i].positions = pos.ctypes.data
+        meshes[i].nverts = pos.shape[0]
+        meshes[i].indices = idx.ctypes.data
+        meshes[i].ntris = idx.shape[0]
+        meshes[i].normals = nrm.ctypes.data
+        meshes[i].model_to_world[:] = [float(x) for x in np.asarray(m2w, np.float32)]
+        meshes[i].material = material_from(mat)
+    shapes = (OShape * max(1, len(scene_desc.get("shapes", []))))()
+    for i, (kind, c, r, n, mat) in enumerate(scene_desc.get("shapes", [])):
+        shapes[i].type = kind
+        shapes[i].center[:] = list(map(float, c))
+        shapes[i].radius = float(r)
+        shapes[i].normal[:] = list(map(float, n))
+        shapes[i].material = material_from(mat)
+    env = np.ascontiguousarray(scene_desc["env"], np.float32)
+    oc = OCamera()
+    C.memmove(C.byref(oc), C.byref(cam), C.sizeof(OCamera))
+    npix = cam.width * cam.height
+    p1 = npix if p1 is None else p1
+    rgb = np.zeros((p1 - p0, 3), np.float32)
+    var = np.zeros((p1 - p0, 3), np.float64) if want_var else None
+    r = lib.orc_render(C.addressof(meshes), len(scene_desc.get("meshes", [])), C.addressof(shapes),
+                       len(scene_desc.get("shapes", [])), env.ctypes.data, env.shape[1], env.shape[0], C.byref(oc),
+                       spp, max_depth, seed, p0, p1, rgb.ctypes.data, _p(var), threads)
+    assert r == 0, f"oracle render failed ({r})"
+    return (rgb, var) if want_var else rgb

@@ -1,0 +1,119 @@
+"""GPU parity of the wavefront path tracer against the CPU oracle.
+
+The oracle runs each path start to finish (like the reference's megakernel)
+with the same Philox streams, so the GPU frame must match it pixel for pixel
+up to the rounding of acos/atan2/sin inside the environment lookup; and a
+low-spp GPU frame must lie within 3 sigma of a high-spp oracle estimate.
+"""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from renderer2_b200 import filter as F  # noqa: E402
+from renderer2_b200 import raytracer as R  # noqa: E402
+from renderer2_b200 import render_scenes as RS  # noqa: E402
+from renderer2_b200 import scenes  # noqa: E402
+
+PIX_REL = 1e-4   # per-pixel relative tolerance (libm vs CUDA acos/atan2/sin in the env lookup)
+PIX_FRAC = 0.999  # fraction of pixels that must meet it
+
+
+def _gpu_frame(desc, cam, spp, depth, seed):
+    sc = RS.build_scene(desc)
+    img = sc.render(cam, R.params(spp, depth, seed))
+    sc.close()
+    return img.reshape(-1, 3)
+
+
+def _agree(g, o):
+    tol = PIX_REL * np.maximum(1.0, np.abs(o))
+    ok = np.all(np.abs(g - o) <= tol, axis=1)
+    return ok.mean()
+
+
+def test_c1_small_matches_oracle():
+    desc, _ = RS.c1_scene()
+    cam = R.camera(64, 64, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
+    g = _gpu_frame(desc, cam, 8, 8, 0)
+    o = O.render(desc, cam, 8, 8, 0)
+    assert np.isfinite(g).all()
+    frac = _agree(g, o)
+    assert frac >= PIX_FRAC, f"only {frac:.4f} of pixels agree"
+    assert np.abs(g.mean(0) - o.mean(0)).max() < 1e-4
+
+
+def test_shapes_and_lognormal_env_match_oracle():
+    mesh = scenes.icosphere(3, 0.05, 7)
+    desc = {
+        "meshes": [(mesh, F.material(diffuse=(0.7, 0.4, 0.2), specular=(1, 1, 1), alpha=0.15, ior=1.5),
+                    RS.translate43(0.0, 0.2, 0.0))],
+        "shapes": [(R.SPHERE, (1.6, 0.0, -0.5), 0.6, (1, 0, 0),
+                    F.material(diffuse=(0.2, 0.8, 0.3), specular=(0.5, 0.5, 0.5), alpha=0.6, ior=1.33,
+                               diffuse_roughness=0.5)),
+                   (R.CIRCLE, (0.0, -1.1, 0.0), 3.4e38, (0, 1, 0),
+                    F.material(diffuse=(0.3, 0.3, 0.3), specular=(0.9, 0.9, 0.9), alpha=0.99, ior=1.2,
+                               diffuse_roughness=0.99))],
+        "env": RS.lognormal_env(64, 32, 1.5, 9),
+    }
+    cam = R.camera(48, 40, 60.0, (0.5, 1.0, 4.0), (0.0, 0.0, 0.0), (0, 1, 0))
+    g = _gpu_frame(desc, cam, 6, 6, 5)
+    o = O.render(desc, cam, 6, 6, 5)
+    frac = _agree(g, o)
+    assert frac >= PIX_FRAC, f"only {frac:.4f} of pixels agree"
+
+
+def test_deep_paths_rr_match_oracle():
+    # depth > 4 exercises Russian roulette; albedo near 1 keeps paths alive
+    mesh = scenes.icosphere(2, 0.3, 3)
+    desc = {"meshes": [(mesh, F.material(diffuse=(0.95, 0.95, 0.95), specular=(1, 1, 1), alpha=0.5, ior=1.5),
+                        RS.translate43(0, 0, 0))],
+            "shapes": [(R.CIRCLE, (0.0, -1.2, 0.0), 50.0, (0, 1, 0), F.material(diffuse=(0.9, 0.9, 0.9), alpha=0.3))],
+            "env": RS.lognormal_env(32, 16, 0.5, 1)}
+    cam = R.camera(32, 32, 50.0, (0, 0.5, 3.5), (0, 0, 0), (0, 1, 0))
+    g = _gpu_frame(desc, cam, 4, 12, 3)
+    o = O.render(desc, cam, 4, 12, 3)
+    assert _agree(g, o) >= PIX_FRAC
+
+
+def test_three_sigma_against_high_spp_oracle():
+    desc, _ = RS.c1_scene()
+    desc = dict(desc)
+    desc["env"] = RS.lognormal_env(32, 16, 1.0, 4)
+    cam = R.camera(24, 24, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
+    spp_g, spp_o = 64, 2048
+    g = _gpu_frame(desc, cam, spp_g, 8, 101)
+    o, var = O.render(desc, cam, spp_o, 8, 7, want_var=True)
+    sigma = np.sqrt(var / spp_g + var / spp_o) + 1e-7
+    z = np.abs(g - o) / sigma
+    within = (z <= 3.0).mean()
+    assert within >= 0.98, f"{within:.4f} of pixel channels within 3 sigma"
+
+
+def test_device_entry_matches_host_entry_and_is_deterministic():
+    desc, _ = RS.c1_scene()
+    cam = R.camera(40, 30, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
+    sc = RS.build_scene(desc)
+    a = sc.render(cam, R.params(4, 8, 2))
+    buf = torch.empty(40 * 30 * 3, dtype=torch.float32, device="cuda")
+    st = sc.render_device(cam, R.params(4, 8, 2), buf.data_ptr())
+    torch.cuda.synchronize()
+    b = buf.cpu().numpy().reshape(30, 40, 3)
+    c = sc.render(cam, R.params(4, 8, 2))
+    sc.close()
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+    assert st[0] == 40 * 30 * 4
+
+
+def test_render_rejects_bad_arguments():
+    desc, _ = RS.c1_scene()
+    sc = RS.build_scene(desc)
+    from renderer2_b200 import _native as N
+    with pytest.raises(N.R2Error):
+        sc.render(R.camera(8, 8), R.params(0, 8, 0))
+    with pytest.raises(N.R2Error):
+        sc.render(R.camera(8, 8), R.params(1, 100, 0))
+    sc.close()
