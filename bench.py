@@ -430,6 +430,39 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_case(args):
+    """Small single-GPU cases for kernel profiling (a few hundred MB on the device)."""
+    import torch
+    torch.cuda.set_device(0)
+    if args.case == "render-small":
+        from renderer2_b200 import render_scenes as RS
+        from renderer2_b200 import raytracer as R
+        desc, _ = RS.c2_scene()
+        cam = R.camera(256, 256, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+        sc = RS.build_scene(desc)
+        frame = torch.empty(256 * 256 * 3, dtype=torch.float32, device="cuda")
+        st = sc.render_device(cam, R.params(2, 8, 0), frame.data_ptr())
+        torch.cuda.synchronize()
+        sc.close()
+        print(json.dumps({"case": args.case, "paths": st[0], "ms": st[1]}))
+    elif args.case == "filter-small":
+        from renderer2_b200 import filter as F
+        from renderer2_b200 import scenes
+        mesh = scenes.foliage(100_000, 20, 0.7, 4)
+        mat = F.material(diffuse=(0.1, 0.6, 0.1), specular=(0.04, 0.04, 0.04), alpha=0.5, ior=1.5)
+        sc = F.FilterScene(mesh, mat)
+        g = sc.grid(scenes.voxel_size_for(mesh, 64))
+        nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+        out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+        st = np.zeros(3)
+        sc.run(g, F.params(samples_per_voxel=256, iterations=20), out.data_ptr(), stats=st)
+        torch.cuda.synchronize()
+        sc.close()
+        print(json.dumps({"case": args.case, "voxels": st[0], "candidates": st[1], "ms": st[2]}))
+    else:
+        raise SystemExit(f"unknown case {args.case}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -438,8 +471,11 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--skip-filter", action="store_true")
+    ap.add_argument("--case", default=None, help="profiling case: render-small | filter-small")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.case:
+        run_case(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_native(args)
