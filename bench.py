@@ -378,6 +378,19 @@ def run_native(args):
         torch.cuda.set_device(0)
     import renderer2_b200  # noqa: F401  (loads the native library)
 
+    if args.skip_render:
+        f = bench_filter(args, world, local)
+        if rank == 0:
+            mesh, mat, prm, vs = f.pop("_mesh")
+            f.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)"})
+            if world == 1:
+                f["cpu_baseline"] = cpu_filter_sample(mesh, mat, prm, vs, budget_s=args.cpu_budget)
+            print(json.dumps(f), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     r = bench_render(args, world, local)
     f = bench_filter(args, world, local) if not args.skip_filter else None
     if rank == 0:
@@ -471,6 +484,7 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--skip-filter", action="store_true")
+    ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
     ap.add_argument("--case", default=None, help="profiling case: render-small | filter-small")
     args = ap.parse_args()
     if args.case:

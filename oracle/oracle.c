@@ -800,3 +800,16 @@ int orc_filter(const float* positions, uint32_t nverts, const uint32_t* idx, uin
   free(jobs); free(th); free(wpos); free(nodes); free(order); free(tris);
   return height;
 }
+
+/* Unit hook for the golden-vector tests: buildS in FP64 as accumulated by the
+ * filter oracle (xx yy zz xy xz yz). */
+void orc_t_build_s(const float* n, float sigma, double* out) {
+  double x = n[0], y = n[1], z = n[2], a = sigma;
+  double xx = x * x, xy = x * y, xz = x * z, yy = y * y, yz = y * z, zz = z * z;
+  out[0] = xx + a * (yy + zz);
+  out[1] = yy + a * (xx + zz);
+  out[2] = zz + a * (xx + yy);
+  out[3] = xy - a * xy;
+  out[4] = xz - a * xz;
+  out[5] = yz - a * yz;
+}

@@ -739,3 +739,98 @@ int orc_env_le(const float* env_rgb, int W, int H, const float* dir, float* pdf,
   env_free(&e);
   return 0;
 }
+
+/* ------------------------------------------------------------ unit hooks for the golden-vector tests */
+
+static f3 L3(const float* p) { return F3(p[0], p[1], p[2]); }
+static void P3(float* o, f3 v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
+
+float orc_t_fresnel(float etaI, float etaT, float c) { return fresnel(etaI, etaT, c); }
+
+void orc_t_microfacet(float ax, float ay, float etaI, float etaT, const float* wo, const float* wi, float* out) {
+  orc_material om;
+  memset(&om, 0, sizeof(om));
+  om.alpha_x = ax; om.alpha_y = ay; om.eta_i = etaI; om.eta_t = etaT;
+  mat_t m = make_mat(&om);
+  out[0] = mf_f(&m, L3(wo), L3(wi));
+  out[1] = mf_pdf(&m, L3(wo), L3(wi));
+}
+
+void orc_t_microfacet_sample(float ax, float ay, float etaI, float etaT, const float* wo, float u1, float u2,
+                             float* out) {
+  orc_material om;
+  memset(&om, 0, sizeof(om));
+  om.alpha_x = ax; om.alpha_y = ay; om.eta_i = etaI; om.eta_t = etaT;
+  mat_t m = make_mat(&om);
+  f3 wi = F3(0.0f, 0.0f, 0.0f);
+  float pdf = 0.0f;
+  float f = mf_sample_f(&m, L3(wo), u1, u2, &wi, &pdf);
+  P3(out, wi);
+  out[3] = pdf;
+  out[4] = f;
+}
+
+void orc_t_ggx_sample_h(float ax, float ay, const float* wo, float u1, float u2, float* out) {
+  ggx_t g = {ax, ay};
+  P3(out, ggx_sample_h(g, L3(wo), u1, u2));
+}
+
+void orc_t_oren_nayar(float roughness, const float* wo, const float* wi, float* out) {
+  orc_material om;
+  memset(&om, 0, sizeof(om));
+  om.diffuse_roughness = roughness;
+  mat_t m = make_mat(&om);
+  out[0] = on_f(&m, L3(wo), L3(wi));
+  out[1] = on_pdf(L3(wo), L3(wi));
+}
+
+void orc_t_oren_nayar_sample(float roughness, const float* wo, float u1, float u2, float* out) {
+  orc_material om;
+  memset(&om, 0, sizeof(om));
+  om.diffuse_roughness = roughness;
+  mat_t m = make_mat(&om);
+  f3 wi;
+  float pdf = 0.0f;
+  float f = on_sample_f(&m, L3(wo), u1, u2, &wi, &pdf);
+  P3(out, wi);
+  out[3] = pdf;
+  out[4] = f;
+}
+
+void orc_t_warps(float u1, float u2, float* out) {
+  float zz = 1.0f - 2.0f * u1, r = sqrtf(fmaxf(0.0f, 1.0f - zz * zz)), s, c;
+  orc_sincos_turns(u2, &s, &c);
+  P3(out + 0, F3(r * c, r * s, zz));
+  float rh = sqrtf(fmaxf(0.0f, 1.0f - u1 * u1));
+  P3(out + 3, F3(rh * c, rh * s, u1));
+  f3 d = cosine_hemisphere(u1, u2);
+  P3(out + 6, F3(d.x, d.y, 0.0f));
+  P3(out + 9, d);
+}
+
+void orc_t_frame(const float* n, const float* v, float* out) {
+  frame_t f = frame_from_normal(L3(n));
+  P3(out, f.T);
+  P3(out + 3, f.B);
+  P3(out + 6, to_local(&f, L3(v)));
+}
+
+void orc_t_offset(const float* p, const float* d, float* out) { P3(out, offset_origin(L3(p), L3(d))); }
+
+int orc_t_find_interval(const float* cdf, int size, float u) { return find_interval(cdf, size, u); }
+
+void orc_t_sphere(const float* c, float r, const float* o, const float* d, float tmax, float* out) {
+  orc_shape sh;
+  memset(&sh, 0, sizeof(sh));
+  sh.type = 0;
+  sh.center[0] = c[0]; sh.center[1] = c[1]; sh.center[2] = c[2];
+  sh.radius = r;
+  rscene_t S;
+  memset(&S, 0, sizeof(S));
+  S.shapes = &sh;
+  S.nshapes = 1;
+  float t, b1, b2;
+  int code = scene_closest(&S, L3(o), L3(d), tmax, &t, &b1, &b2);
+  out[0] = code == -2 ? 1.0f : 0.0f;
+  out[1] = code == -2 ? t : 0.0f;
+}

@@ -1,0 +1,226 @@
+"""Generates tests/golden/ref_math.json from the reference's own headers.
+
+Builds oracle/_ref/libr2ref.so (the reference's math headers compiled for the
+host from the reference tree, see oracle/ref_kat.cpp) and evaluates it on
+seeded inputs.  Run in the build container, where the reference tree is
+mounted:
+
+    python tests/golden/make_golden.py [/path/to/reference/raytracer/include]
+
+The JSON holds inputs and reference outputs; tests/test_golden.py checks the
+oracle's restatement against it without needing the reference.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+ORACLE = os.path.join(ROOT, "oracle")
+LIB = os.path.join(ORACLE, "_ref", "libr2ref.so")
+OUT = os.path.join(HERE, "ref_math.json")
+
+
+def build(ref_include: str) -> C.CDLL:
+    subprocess.run(["make", "-s", "-C", ORACLE, "ref", f"REF={ref_include}"], check=True)
+    lib = C.CDLL(LIB)
+    P = C.c_void_p
+    f = C.c_float
+    lib.ref_u01.restype = f
+    lib.ref_u01.argtypes = [f]
+    lib.ref_fresnel.restype = f
+    lib.ref_fresnel.argtypes = [f, f, f]
+    lib.ref_warps.argtypes = [P, P]
+    lib.ref_build_s.argtypes = [P, f, P]
+    lib.ref_encode.argtypes = [P, P]
+    lib.ref_decode.argtypes = [P, P]
+    lib.ref_microfacet.argtypes = [f, f, f, f, P, P, P]
+    lib.ref_microfacet_sample.argtypes = [f, f, f, f, P, P, P]
+    lib.ref_ggx_sample_h.argtypes = [f, f, P, f, f, P]
+    lib.ref_oren_nayar.argtypes = [f, P, P, P]
+    lib.ref_oren_nayar_sample.argtypes = [f, P, P, P]
+    lib.ref_frame.argtypes = [P, P, P]
+    lib.ref_offset.argtypes = [P, P, P]
+    lib.ref_sphere.argtypes = [P, f, P, P, P, f, P]
+    lib.ref_find_interval.restype = C.c_int
+    lib.ref_find_interval.argtypes = [P, C.c_int, f]
+    lib.ref_sggx.argtypes = [P, P, P, P, f, f, P]
+    lib.ref_sggx_sample.argtypes = [P, P, f, P, P, C.c_int, P]
+    lib.ref_get_rotation.argtypes = [P, P]
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _f32(x):
+    return np.ascontiguousarray(x, np.float32)
+
+
+def unit(rng, n):
+    v = rng.normal(size=(n, 3))
+    return _f32(v / np.linalg.norm(v, axis=1, keepdims=True))
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/raytracer/include"
+    lib = build(ref)
+    rng = np.random.default_rng(20261203)
+    g = {"vec2_arg_order": lib.ref_vec2_arg_order()}
+
+    # cuRAND value -> uniformSample01
+    cs = _f32(np.concatenate([rng.uniform(1e-7, 1.0, 64), [1.0, 0.5, 1e-7]]))
+    g["u01"] = {"c": cs.tolist(), "u": [lib.ref_u01(float(c)) for c in cs]}
+
+    # sampling warps, driven by two draws
+    rows = []
+    for _ in range(256):
+        c = _f32(rng.uniform(1e-6, 1.0, 2))
+        out = np.zeros(12, np.float32)
+        lib.ref_warps(_p(c), _p(out))
+        u = [lib.ref_u01(float(c[0])), lib.ref_u01(float(c[1]))]
+        rows.append({"u": u, "out": out.tolist()})
+    g["warps"] = rows
+
+    rows = []
+    for n, s in zip(unit(rng, 128), rng.uniform(0.0, 1.0, 128)):
+        out = np.zeros(6, np.float32)
+        lib.ref_build_s(_p(n), float(s), _p(out))
+        rows.append({"n": n.tolist(), "sigma": float(s), "S": out.tolist()})
+    g["build_s"] = rows
+
+    rows = []
+    for i in range(256):
+        n = unit(rng, 1)[0]
+        a = float(rng.uniform(0.02, 1.0))
+        S = np.outer(n, n) + a * (np.eye(3) - np.outer(n, n))
+        w = np.zeros(17, np.float32)
+        w[0] = rng.lognormal(0, 2)
+        w[1:7] = [S[0, 0], S[1, 1], S[2, 2], S[0, 1], S[0, 2], S[1, 2]]
+        w[7:13] = rng.uniform(0, 1, 6)
+        w[13:16] = unit(rng, 1)[0]
+        w[16] = rng.uniform(1.0, 2.0)
+        if i == 0:
+            w[:] = 0.0
+            w[16] = 1.0  # voxel without hits
+        out = np.zeros(32, np.uint8)
+        lib.ref_encode(_p(w), _p(out))
+        dec = np.zeros(17, np.float32)
+        lib.ref_decode(_p(out), _p(dec))
+        rows.append({"in": w.tolist(), "bytes": out.tolist(), "decoded": dec.tolist()})
+    g["payload"] = rows
+
+    rows = []
+    for _ in range(256):
+        etaI, etaT = 1.0, float(rng.uniform(1.0, 2.5))
+        c = float(rng.uniform(-1.0, 1.0))
+        rows.append({"etaI": etaI, "etaT": etaT, "cos": c, "F": lib.ref_fresnel(etaI, etaT, c)})
+    g["fresnel"] = rows
+
+    def hemi(n, sign=1.0):
+        v = unit(rng, n)
+        v[:, 2] = np.abs(v[:, 2]) * sign
+        return _f32(v)
+
+    rows = []
+    for wo, wi in zip(hemi(256), unit(rng, 256)):
+        ax, ay = float(rng.uniform(0.05, 1.0)), float(rng.uniform(0.05, 1.0))
+        etaT = float(rng.uniform(1.1, 2.0))
+        out = np.zeros(2, np.float32)
+        lib.ref_microfacet(ax, ay, 1.0, etaT, _p(wo), _p(wi), _p(out))
+        c = _f32(rng.uniform(1e-6, 1.0, 2))
+        so = np.zeros(5, np.float32)
+        lib.ref_microfacet_sample(ax, ay, 1.0, etaT, _p(wo), _p(c), _p(so))
+        h = np.zeros(3, np.float32)
+        u1, u2 = float(rng.uniform(0, 1)), float(rng.uniform(0, 1))
+        lib.ref_ggx_sample_h(ax, ay, _p(wo), u1, u2, _p(h))
+        rows.append({"ax": ax, "ay": ay, "etaT": etaT, "wo": wo.tolist(), "wi": wi.tolist(), "f_pdf": out.tolist(),
+                     "draw_u": [lib.ref_u01(float(c[0])), lib.ref_u01(float(c[1]))], "sample": so.tolist(),
+                     "h_u": [u1, u2], "h": h.tolist()})
+    g["microfacet"] = rows
+
+    rows = []
+    for wo, wi in zip(unit(rng, 256), unit(rng, 256)):
+        r = float(rng.uniform(0.0, 1.0))
+        out = np.zeros(2, np.float32)
+        lib.ref_oren_nayar(r, _p(wo), _p(wi), _p(out))
+        c = _f32(rng.uniform(1e-6, 1.0, 2))
+        so = np.zeros(5, np.float32)
+        lib.ref_oren_nayar_sample(r, _p(wo), _p(c), _p(so))
+        rows.append({"roughness": r, "wo": wo.tolist(), "wi": wi.tolist(), "f_pdf": out.tolist(),
+                     "draw_u": [lib.ref_u01(float(c[0])), lib.ref_u01(float(c[1]))], "sample": so.tolist()})
+    g["oren_nayar"] = rows
+
+    rows = []
+    for n, v in zip(unit(rng, 128), unit(rng, 128)):
+        out = np.zeros(9, np.float32)
+        lib.ref_frame(_p(n), _p(v), _p(out))
+        rows.append({"n": n.tolist(), "v": v.tolist(), "out": out.tolist()})
+    g["frame"] = rows
+
+    rows = []
+    for _ in range(128):
+        p = _f32(rng.uniform(-10, 10, 3))
+        d = unit(rng, 1)[0]
+        out = np.zeros(3, np.float32)
+        lib.ref_offset(_p(p), _p(d), _p(out))
+        rows.append({"p": p.tolist(), "d": d.tolist(), "out": out.tolist()})
+    g["offset"] = rows
+
+    rows = []
+    for _ in range(256):
+        c = _f32(rng.uniform(-1, 1, 3))
+        r = float(rng.uniform(0.1, 2.0))
+        o = _f32(c + rng.uniform(-1.5, 1.5, 3) * r)
+        d = unit(rng, 1)[0]
+        out = np.zeros(2, np.float32)
+        nrm = _f32([0.0, 1.0, 0.0])
+        lib.ref_sphere(_p(c), r, _p(nrm), _p(o), _p(d), 1e12, _p(out))
+        rows.append({"c": c.tolist(), "r": r, "o": o.tolist(), "d": d.tolist(), "out": out.tolist()})
+    g["sphere"] = rows
+
+    rows = []
+    for _ in range(128):
+        n = int(rng.integers(2, 40))
+        f = rng.uniform(0, 1, n - 1)
+        cdf = _f32(np.concatenate([[0.0], np.cumsum(f) / f.sum()]))
+        u = float(rng.uniform(0, 1))
+        rows.append({"cdf": cdf.tolist(), "u": u, "k": lib.ref_find_interval(_p(cdf), n, u)})
+    g["find_interval"] = rows
+
+    rows = []
+    for _ in range(128):
+        n = unit(rng, 1)[0]
+        a = float(rng.uniform(0.05, 1.0))
+        S = np.outer(n, n) + a * (np.eye(3) - np.outer(n, n))
+        S6 = _f32([S[0, 0], S[1, 1], S[2, 2], S[0, 1], S[0, 2], S[1, 2]])
+        wo, wi = unit(rng, 1)[0], unit(rng, 1)[0]
+        u1, u2 = float(rng.uniform(0, 1)), float(rng.uniform(0, 1))
+        out = np.zeros(6, np.float32)
+        lib.ref_sggx(_p(S6), _p(n), _p(wo), _p(wi), u1, u2, _p(out))
+        rows.append({"S": S6.tolist(), "n": n.tolist(), "wo": wo.tolist(), "wi": wi.tolist(), "u": [u1, u2],
+                     "out": out.tolist()})
+    g["sggx"] = rows
+
+    rows = []
+    for n in [unit(rng, 1)[0] for _ in range(32)] + [_f32([0, 1, 0]), _f32([0, -1, 0]), _f32([1, 0, 0]),
+                                                       _f32([0, 0, 1])]:
+        out = np.zeros(16, np.float32)
+        lib.ref_get_rotation(_p(n), _p(out))
+        rows.append({"n": n.tolist(), "m": out.tolist()})
+    g["get_rotation"] = rows
+
+    with open(OUT, "w") as fh:
+        json.dump(g, fh)
+    print(f"wrote {OUT}")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,160 @@
+"""The oracle against golden vectors produced by the reference's own headers
+compiled for the host (tests/golden/make_golden.py, oracle/ref_kat.cpp).
+
+The reference ships no tests or fixtures; these vectors are its own functions
+evaluated on seeded inputs: payload encode (filtered_data.hpp:91-107),
+buildS (sggx_phase_function.hpp:95-105), Fresnel (fresnel.hpp:28-54), GGX
+microfacet BRDF and VNDF sampling (microfacet_brdf.hpp:57-100,
+microfacet_distribution.hpp:40-141), Oren-Nayar (oren_nayar_brdf.hpp:36-81),
+CSampler warps (sampler.hpp:39-94), CCoordinateFrame::fromNormal
+(objects.hpp:28-40), CRay::offsetRayOrigin (ray.hpp:73-85), Sphere::intersect
+(sphere.hpp:33-90) and findInterval (functions.hpp:10-27).
+
+Tolerances: exact where the oracle performs the same float operations;
+a few float ulps where the oracle evaluates sampled angles with its own
+sin/cos (the reference rounds 2*pi*u to float first) or uses the transposed
+frame instead of glm::inverse.
+"""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+
+G = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "ref_math.json")))
+L = O.lib
+P, f = C.c_void_p, C.c_float
+L.orc_t_fresnel.restype = f
+L.orc_t_fresnel.argtypes = [f, f, f]
+L.orc_t_microfacet.argtypes = [f, f, f, f, P, P, P]
+L.orc_t_microfacet_sample.argtypes = [f, f, f, f, P, f, f, P]
+L.orc_t_ggx_sample_h.argtypes = [f, f, P, f, f, P]
+L.orc_t_oren_nayar.argtypes = [f, P, P, P]
+L.orc_t_oren_nayar_sample.argtypes = [f, P, f, f, P]
+L.orc_t_warps.argtypes = [f, f, P]
+L.orc_t_frame.argtypes = [P, P, P]
+L.orc_t_offset.argtypes = [P, P, P]
+L.orc_t_find_interval.restype = C.c_int
+L.orc_t_find_interval.argtypes = [P, C.c_int, f]
+L.orc_t_sphere.argtypes = [P, f, P, P, f, P]
+L.orc_t_build_s.argtypes = [P, f, P]
+
+
+def a32(x):
+    return np.ascontiguousarray(x, np.float32)
+
+
+def p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def close(a, b, rtol, atol):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.all(np.abs(a - b) <= atol + rtol * np.abs(b))
+
+
+def test_payload_encode_matches_reference():
+    for r in G["payload"]:
+        w = np.asarray(r["in"], np.float64)
+        wide = np.zeros(20, np.float64)
+        wide[:17] = w
+        out = np.zeros(32, np.uint8)
+        L.orc_encode(p(wide), p(out))
+        ref = np.asarray(r["bytes"], np.uint8)
+        assert out[:4].tobytes() == ref[:4].tobytes()          # density float
+        a16 = np.frombuffer(out[4:16].tobytes(), np.uint16).astype(int)
+        r16 = np.frombuffer(ref[4:16].tobytes(), np.uint16).astype(int)
+        assert np.abs(a16 - r16).max() <= 1                      # sigma, r: one LSB (FP64 vs FP32)
+        assert np.abs(out[16:22].astype(int) - ref[16:22].astype(int)).max() <= 1
+        n16 = np.frombuffer(out[22:28].tobytes(), np.uint16).astype(int)
+        rn16 = np.frombuffer(ref[22:28].tobytes(), np.uint16).astype(int)
+        assert np.abs(n16 - rn16).max() <= 1
+        assert out[28:30].tobytes() == ref[28:30].tobytes()      # ior half
+
+
+def test_empty_payload_is_background():
+    r = G["payload"][0]
+    assert r["bytes"] == [0] * 29 + [60, 0, 0]
+
+
+def test_build_s_matches_reference():
+    for r in G["build_s"]:
+        out = np.zeros(6, np.float64)
+        L.orc_t_build_s(p(a32(r["n"])), r["sigma"], p(out))
+        assert close(out, r["S"], 1e-6, 1e-7)
+
+
+def test_fresnel_matches_reference():
+    for r in G["fresnel"]:
+        assert L.orc_t_fresnel(r["etaI"], r["etaT"], r["cos"]) == np.float32(r["F"])
+
+
+def test_warps_match_reference():
+    for r in G["warps"]:
+        out = np.zeros(12, np.float32)
+        L.orc_t_warps(r["u"][0], r["u"][1], p(out))
+        assert close(out, r["out"], 0.0, 2e-6)
+
+
+def test_microfacet_matches_reference():
+    order = G["vec2_arg_order"]
+    for r in G["microfacet"]:
+        out = np.zeros(2, np.float32)
+        L.orc_t_microfacet(r["ax"], r["ay"], 1.0, r["etaT"], p(a32(r["wo"])), p(a32(r["wi"])), p(out))
+        assert close(out, r["f_pdf"], 1e-5, 1e-7)
+        h = np.zeros(3, np.float32)
+        L.orc_t_ggx_sample_h(r["ax"], r["ay"], p(a32(r["wo"])), r["h_u"][0], r["h_u"][1], p(h))
+        assert close(h, r["h"], 1e-5, 2e-6)
+        # sampleF draws glm::vec2(u(), u()); this build evaluates the arguments in `order`
+        d = r["draw_u"]
+        u1, u2 = (d[0], d[1]) if order == 0 else (d[1], d[0])
+        so = np.zeros(5, np.float32)
+        L.orc_t_microfacet_sample(r["ax"], r["ay"], 1.0, r["etaT"], p(a32(r["wo"])), u1, u2, p(so))
+        ref = np.asarray(r["sample"], np.float32)
+        if ref[3] == 0.0:
+            assert so[3] == 0.0
+        else:
+            assert close(so, ref, 1e-4, 1e-6)
+
+
+def test_oren_nayar_matches_reference():
+    for r in G["oren_nayar"]:
+        out = np.zeros(2, np.float32)
+        L.orc_t_oren_nayar(r["roughness"], p(a32(r["wo"])), p(a32(r["wi"])), p(out))
+        assert close(out, r["f_pdf"], 1e-6, 1e-8)
+        so = np.zeros(5, np.float32)
+        L.orc_t_oren_nayar_sample(r["roughness"], p(a32(r["wo"])), r["draw_u"][0], r["draw_u"][1], p(so))
+        assert close(so, r["sample"], 1e-5, 2e-6)
+
+
+def test_frame_matches_reference():
+    for r in G["frame"]:
+        out = np.zeros(9, np.float32)
+        L.orc_t_frame(p(a32(r["n"])), p(a32(r["v"])), p(out))
+        assert close(out[:6], r["out"][:6], 0.0, 0.0)  # tangent and bitangent: same operations
+        assert close(out[6:], r["out"][6:], 0.0, 1e-6)  # transpose vs glm::inverse
+
+
+def test_offset_matches_reference():
+    for r in G["offset"]:
+        out = np.zeros(3, np.float32)
+        L.orc_t_offset(p(a32(r["p"])), p(a32(r["d"])), p(out))
+        assert np.array_equal(out, np.asarray(r["out"], np.float32))
+
+
+def test_sphere_matches_reference():
+    for r in G["sphere"]:
+        out = np.zeros(2, np.float32)
+        L.orc_t_sphere(p(a32(r["c"])), r["r"], p(a32(r["o"])), p(a32(r["d"])), 1e12, p(out))
+        assert out[0] == r["out"][0]
+        if out[0]:
+            assert close(out[1], r["out"][1], 1e-5, 1e-6)
+
+
+def test_find_interval_matches_reference():
+    for r in G["find_interval"]:
+        cdf = a32(r["cdf"])
+        assert L.orc_t_find_interval(p(cdf), len(cdf), r["u"]) == r["k"]
