@@ -139,6 +139,25 @@ r2_status r2_filter_scene_run(r2_filter_scene* scene, const r2_filter_grid* grid
                               const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
                               uint16_t* d_fp16, void* stream, double* stats_out);
 
+/* Same as r2_filter_scene_run, for callers that must not allocate device
+ * memory during the call: frame loops that run under a fixed memory budget
+ * with no allocation after start-up, applications that own every device
+ * allocation through their own pool, and latency-bound callers that cannot
+ * afford the device-wide synchronisation cudaMalloc/cudaFree may imply.
+ * It allocates nothing: the voxel work list and queue counters live in a
+ * fixed scratch array inside the library (4 MiB, held by every GPU that loads
+ * the library until the process exits), so grids above 2^20 voxels are
+ * rejected with R2_ERR_UNSUPPORTED.  The scene is created beforehand with
+ * r2_filter_scene_create.  The first call on a device resolves the scratch
+ * array's device address (set-up done once per device) and should come
+ * before any stream capture.  All calls share the one scratch array and it
+ * keeps the last call's contents: calls that overlap on the GPU race and must
+ * be serialised by the caller.
+ * This entry point has no counterpart in the reference. */
+r2_status r2_filter_scene_run_static(r2_filter_scene* scene, const r2_filter_grid* grid,
+                                     const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
+                                     uint16_t* d_fp16, void* stream);
+
 /* BVH of a filter scene, downloaded for bit-exact comparison with the oracle:
  * nodes: (ntris-1 or 1) * 16 words; tri_order: ntris original indices. */
 r2_status r2_filter_scene_bvh(const r2_filter_scene* scene, int32_t* nodes, size_t node_words,

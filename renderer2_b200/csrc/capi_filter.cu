@@ -181,3 +181,6 @@ r2_status r2_filter_mesh(const float* positions, uint32_t nverts, const uint32_t
 }
 
 }  // extern "C"
+
+// Accessor for the allocation-free entry point (filter_static.cu).
+r2::FilterScene* r2_filter_scene_impl(r2_filter_scene* scene) { return scene->impl.get(); }
