@@ -158,6 +158,33 @@ r2_status r2_filter_scene_run_static(r2_filter_scene* scene, const r2_filter_gri
                                      const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
                                      uint16_t* d_fp16, void* stream);
 
+/* All LODs with the reference's file outputs (CFilter::runFiltering,
+ * raytracer/filter.cu:74-123): voxel size min_voxel_size * 2^lod; per LOD
+ * <out_root>/<model_name>/filtered_mesh_<std::to_string(vs)>.nvdb (NanoVDB
+ * Vec4d grid, active = density > 0 or a grid corner, openvdb_backend.cpp:108-157)
+ * and .brickgrid (density bricks + majorant mips, host_grid_brick.cpp:61-152),
+ * and <out_root>/volume_description.json (volume_description_manager.cpp:50-144).
+ * The object transform is T(pos3) * getRotation(orientation3) * S(scaling3)
+ * (src/scene/sceneobject.cu:375-377).  stats_out (nullable, 4 doubles): LODs,
+ * voxels, active voxels, sampling-kernel milliseconds. */
+r2_status r2_filter_run_mesh(const float* positions, uint32_t nverts, const uint32_t* indices, uint32_t ntris,
+                             const float* normals, const r2_material* material, const float* pos3,
+                             const float* orientation3, const float* scaling3, const r2_filter_params* params,
+                             const char* out_root, const char* model_name, double* stats_out);
+
+/* NanoVDB file written by the filter: counts4 = leaves, lower nodes, upper
+ * nodes, active voxels; index_bbox6 = active index box (inclusive);
+ * world_bbox6; index_to_model12 = the grid map as a glm mat4x3. */
+r2_status r2_nvdb_info(const char* path, uint64_t* counts4, int32_t* index_bbox6, double* world_bbox6,
+                       float* index_to_model12);
+/* Payloads and active flags at n index coordinates (3 int32 each). */
+r2_status r2_nvdb_lookup(const char* path, const int32_t* coords, uint32_t n, r2_voxel* out, uint8_t* active);
+/* Brick grid file: dims7 = bricks xyz, atlas voxels xyz, non-constant bricks;
+ * minmaj2 = density minorant/majorant; indirection/range (nullable) receive
+ * the per-brick words (capacity in elements). */
+r2_status r2_brickgrid_info(const char* path, uint32_t* dims7, float* minmaj2, uint32_t* indirection,
+                            uint32_t* range, size_t capacity);
+
 /* BVH of a filter scene, downloaded for bit-exact comparison with the oracle:
  * nodes: (ntris-1 or 1) * 16 words; tri_order: ntris original indices. */
 r2_status r2_filter_scene_bvh(const r2_filter_scene* scene, int32_t* nodes, size_t node_words,
