@@ -217,8 +217,13 @@ typedef struct r2_render_params {
   uint32_t spp;        /* "Samples" of config.json */
   uint32_t max_depth;  /* bounce cap (the reference hard-codes 50) */
   uint32_t seed;       /* Philox key word 1 */
-  uint32_t flags;      /* reserved, 0 */
+  uint32_t flags;      /* R2_RENDER_* bits */
 } r2_render_params;
+
+/* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA
+ * (CNVDBMedium::sampleDDA / trDDA, nvdb_medium_impl.hpp:139-187, 248-294)
+ * instead of the global majorant (sampleInternal / trInternal, 94-137, 203-239). */
+#define R2_RENDER_BRICK_GRID 1u
 
 /* Object masks (raytracer/include/scene/sceneobject_mask.hpp:6-11). */
 #define R2_MASK_FILTER 1u
@@ -239,16 +244,28 @@ r2_status r2_scene_add_shape(r2_scene* scene, int shape_type, const float* cente
                              const float* normal, const r2_material* material, uint32_t mask);
 /* Environment map: width*height RGB float texels, row 0 = top (+Y). */
 r2_status r2_scene_set_envmap(r2_scene* scene, const float* rgb, uint32_t width, uint32_t height);
+/* Heterogeneous SGGX medium of scenedescription.json (Type "Medium"): loads
+ * <path>.nvdb and <path>.brickgrid (path without extension, ending in the
+ * filter voxel size "\d+.\d+"), placed with T(pos) R(orientation) S(scaling).
+ * Replaces CNVDBMedium(path, sigma_a, sigma_s) (raytracer/src/medium/nvdb_medium.cu:45-61,
+ * 130-173) inside CHostSceneobject(medium, pos, orientation, scaling, mask)
+ * (raytracer/src/scene/sceneobject.cu:50-65). */
+r2_status r2_scene_add_medium(r2_scene* scene, const char* path, const float* sigma_a, const float* sigma_s,
+                              const float* pos, const float* orientation, const float* scaling, uint32_t mask);
 /* Uploads the scene and builds the BVH (device-resident until destroyed). */
 r2_status r2_scene_commit(r2_scene* scene);
 /* Renders one frame into device memory d_rgb (width*height*3 floats).
  * stats_out (nullable, 8 doubles): [0] paths, [1] milliseconds of the frame on
  * the stream, [2] path segments traced, [3] shadow rays traced, [4..7]
  * milliseconds of the extend / shade / shadow / accumulate kernels of one
- * (the middle) wave. */
+ * (the middle) wave.  With stats_out the call waits for the frame and returns
+ * R2_ERR_DEVICE_TIMEOUT (frame still written) if a loop bound ended any path:
+ * 2^20 tracking steps, 64 medium boundaries within a bounce, 256 along a
+ * shadow ray (the reference's loops have no bound). */
 r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* d_rgb,
                            void* stream, double* stats_out);
-/* Same through host memory: commits if needed, renders, copies the frame to rgb. */
+/* Same through host memory: commits if needed, renders, copies the frame to
+ * rgb; loop bounds are reported as in r2_render_device. */
 r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* rgb);
 
 /* ------------------------------------------------------------------------ */

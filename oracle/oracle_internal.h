@@ -50,4 +50,32 @@ m4_t oi_m4_mul(m4_t a, m4_t b);
 m4_t oi_m4_inv(m4_t a);
 void oi_m4_to43(m4_t a, float* f);
 
+/* NanoVDB Vec4d grid file (volume_reader.c). */
+typedef struct {
+  uint8_t* buf; /* grid buffer */
+  uint64_t size;
+  float matF[9], vecF[3];   /* map, row-major */
+  double worldBBox[6];
+  int32_t indexBBox[6];     /* root bbox (inclusive) */
+  uint64_t voxelCount;
+  uint64_t rootOff, leafOff;
+  uint32_t leafCount, tableSize;
+  uint8_t background[32];
+} oi_nvdb;
+int oi_nvdb_read(const char* path, oi_nvdb* g);
+void oi_nvdb_free(oi_nvdb* g);
+/* ReadAccessor::getValue by a root/upper/lower/leaf walk (32-byte payload). */
+void oi_nvdb_value(const oi_nvdb* g, int x, int y, int z, uint8_t out[32]);
+float oi_nvdb_max_density(const oi_nvdb* g);
+
+/* ".brickgrid" file of the library. */
+typedef struct {
+  uint32_t nb[3], ad[3], count;
+  float minorant, majorant;
+  uint32_t *ind, *range, *mips[3];
+  uint8_t* atlas;
+} oi_bricks;
+int oi_bricks_read(const char* path, oi_bricks* b);
+void oi_bricks_free(oi_bricks* b);
+
 #endif

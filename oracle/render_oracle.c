@@ -8,6 +8,7 @@
 
 #include <float.h>
 #include <pthread.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include <unistd.h>
@@ -403,6 +404,593 @@ static f3 env_le(const env_t* e, f3 d, float* pdf) {
   return env_lookup(e, x, y);
 }
 
+/* ------------------------------------------------------------ media
+ * CNVDBMedium / CMediumInstance / SGGX phase function restated from
+ * nvdb_medium_impl.hpp:28-320, medium_instance_impl.hpp:7-45,
+ * sggx_phase_function.hpp:89-233, device_grid_brick_impl.hpp:9-33 and the
+ * bounding-box program shaders.optix.cu:192-236. */
+#define MEDIUM_CODE_BASE (-1000000)
+#define EV_SCATTER (-2147483647)
+#define EV_DEAD (-2147483646)
+#define MAX_TRACKING_STEPS (1 << 20)
+#define MAX_PASS_THROUGH 64
+#define MAX_SHADOW_SEGMENTS 256
+#define PURPOSE_MEDIUM 0x10u
+#define PURPOSE_SCATTER 0x100u
+#define PURPOSE_SHADOW_TR 0x200u
+
+/* log x (x > 0 normal): x = m 2^e with m in [sqrt(1/2), sqrt(2)), then
+ * log m = 2 atanh(s) = 2 (s + s^3/3 + ... + s^11/11), s = (m - 1)/(m + 1)
+ * (Cody and Waite's reduction); e ln 2 added as 0.693145751953125 + 1.42860682e-6. */
+static float oi_log(float x) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  int e = (int)((b >> 23) & 0xFFu) - 127;
+  uint32_t mb = (b & 0x7FFFFFu) | 0x3F800000u;
+  float m;
+  memcpy(&m, &mb, 4);
+  if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float s2 = s * s;
+  float p = fmaf(s2, 1.0f / 11.0f, 1.0f / 9.0f);
+  p = fmaf(s2, p, 1.0f / 7.0f);
+  p = fmaf(s2, p, 1.0f / 5.0f);
+  p = fmaf(s2, p, 1.0f / 3.0f);
+  const float twoS = 2.0f * s;
+  const float lm = fmaf(twoS * s2, p, twoS);
+  const float fe = (float)e;
+  return fmaf(fe, 0.693145751953125f, fmaf(fe, 1.42860682e-6f, lm));
+}
+
+/* Sequential uniforms: draw i = word i&3 of Philox((sample, bounce, i>>2, purpose), (pixel, seed)). */
+typedef struct { uint32_t k0, k1, c0, c1, purpose, idx; uint32_t buf[4]; } rng_t;
+static rng_t rng_make(uint32_t pixel, uint32_t seed, uint32_t sample, uint32_t bounce, uint32_t purpose) {
+  rng_t r;
+  memset(&r, 0, sizeof(r));
+  r.k0 = pixel; r.k1 = seed; r.c0 = sample; r.c1 = bounce; r.purpose = purpose;
+  return r;
+}
+static float rng_next(rng_t* r) {
+  const uint32_t w = r->idx & 3u;
+  if (w == 0) {
+    uint32_t ctr[4] = {r->c0, r->c1, r->idx >> 2, r->purpose}, key[2] = {r->k0, r->k1};
+    orc_philox4x32_10(ctr, key, r->buf);
+  }
+  r->idx++;
+  return oi_u01(r->buf[w]);
+}
+
+typedef struct { f3 o, d; float tmax; } ray_t;
+static ray_t mkray(f3 o, f3 d, float t) { ray_t r; r.o = o; r.d = d; r.tmax = t; return r; }
+/* CRay::transform (direction renormalised) and transform2 (kept). */
+static ray_t ray_xf(ray_t r, const float* M) {
+  f3 o = xpoint(M, r.o), e = xpoint(M, add3(r.o, mul3s(r.d, r.tmax)));
+  return mkray(o, norm3(xvec(M, r.d)), len3(sub3(e, o)));
+}
+static ray_t ray_xf2(ray_t r, const float* M) {
+  f3 o = xpoint(M, r.o), e = xpoint(M, add3(r.o, mul3s(r.d, r.tmax)));
+  f3 d = xvec(M, r.d);
+  return mkray(o, d, len3(sub3(e, o)) / len3(d));
+}
+/* CRay::offsetRayOrigin(dir): the origin moves, the end point stays. */
+static ray_t ray_off(ray_t r, f3 dir) {
+  f3 end = add3(r.o, mul3s(r.d, r.tmax));
+  f3 o = offset_origin(r.o, dir);
+  return mkray(o, r.d, len3(sub3(end, o)));
+}
+
+typedef struct {
+  float m2w[12], w2m[12];
+  f3 bbMin, bbMax;
+  float ratio;
+  float i2m[12], m2i[12], u2s[12], s2m[12];
+  int ibbMin[3], size[3];
+  f3 sigmaS;
+  float sigmaT, invMax;
+  oi_nvdb g;
+  oi_bricks b;
+} med_t;
+
+typedef struct {
+  float density;
+  float S[6];
+  f3 diffuse, specular, normal;
+  float ior;
+} fdat;
+
+static float half_to_float(uint16_t h) {
+  const int e = (h >> 10) & 0x1F, m = h & 0x3FF;
+  float v;
+  if (e == 0) v = ldexpf((float)m, -24);
+  else if (e == 31) v = m ? NAN : INFINITY;
+  else v = ldexpf((float)(m | 0x400), e - 25);
+  return (h & 0x8000) ? -v : v;
+}
+
+/* SFilteredData(const SFilteredDataCompact&) of a 32-byte payload. */
+static fdat fd_decode(const uint8_t* c) {
+  const float inv16 = 1.0f / 65535.0f, inv8 = 1.0f / 255.0f;
+  uint16_t u[6], nn[3], ior;
+  fdat d;
+  memcpy(&d.density, c, 4);
+  memcpy(u, c + 4, 12);
+  memcpy(nn, c + 22, 6);
+  memcpy(&ior, c + 28, 2);
+  const float sx = u[0] * inv16, sy = u[1] * inv16, sz = u[2] * inv16;
+  const float rxy = 2.0f * (u[3] * inv16) - 1.0f, rxz = 2.0f * (u[4] * inv16) - 1.0f, ryz = 2.0f * (u[5] * inv16) - 1.0f;
+  d.S[0] = sx * sx; d.S[1] = sy * sy; d.S[2] = sz * sz;
+  d.S[3] = rxy * sx * sy; d.S[4] = rxz * sx * sz; d.S[5] = ryz * sy * sz;
+  d.diffuse = mul3s(F3((float)c[16], (float)c[17], (float)c[18]), inv8);
+  d.specular = mul3s(F3((float)c[19], (float)c[20], (float)c[21]), inv8);
+  d.normal = norm3(sub3(mul3s(mul3s(F3((float)nn[0], (float)nn[1], (float)nn[2]), 2.0f), inv16), F3(1.0f, 1.0f, 1.0f)));
+  d.ior = half_to_float(ior);
+  return d;
+}
+
+static fdat fd_lerp(float t, const fdat* a, const fdat* b) {
+  const float u = 1.0f - t;
+  fdat r;
+  r.density = u * a->density + t * b->density;
+  for (int k = 0; k < 6; ++k) r.S[k] = u * a->S[k] + t * b->S[k];
+  r.diffuse = add3(mul3s(a->diffuse, u), mul3s(b->diffuse, t));
+  r.specular = add3(mul3s(a->specular, u), mul3s(b->specular, t));
+  r.normal = norm3(add3(mul3s(norm3(a->normal), u), mul3s(norm3(b->normal), t)));
+  r.ior = u * a->ior + t * b->ior;
+  return r;
+}
+
+static fdat med_voxel(const med_t* m, int x, int y, int z) {
+  uint8_t v[32];
+  oi_nvdb_value(&m->g, x, y, z, v);
+  return fd_decode(v);
+}
+
+/* CNVDBMedium::filteredData: trilinear over 8 payloads at p (unit box). */
+static fdat med_filtered(const med_t* m, f3 p) {
+  const f3 ps = F3(p.x * (float)m->size[0] + (float)m->ibbMin[0] - 0.5f, p.y * (float)m->size[1] + (float)m->ibbMin[1] - 0.5f,
+                   p.z * (float)m->size[2] + (float)m->ibbMin[2] - 0.5f);
+  const int ix = (int)floorf(ps.x), iy = (int)floorf(ps.y), iz = (int)floorf(ps.z);
+  const f3 d = F3(ps.x - (float)ix, ps.y - (float)iy, ps.z - (float)iz);
+  fdat a, b;
+  a = med_voxel(m, ix, iy, iz); b = med_voxel(m, ix + 1, iy, iz);
+  const fdat d00 = fd_lerp(d.x, &a, &b);
+  a = med_voxel(m, ix, iy + 1, iz); b = med_voxel(m, ix + 1, iy + 1, iz);
+  const fdat d10 = fd_lerp(d.x, &a, &b);
+  a = med_voxel(m, ix, iy, iz + 1); b = med_voxel(m, ix + 1, iy, iz + 1);
+  const fdat d01 = fd_lerp(d.x, &a, &b);
+  a = med_voxel(m, ix, iy + 1, iz + 1); b = med_voxel(m, ix + 1, iy + 1, iz + 1);
+  const fdat d11 = fd_lerp(d.x, &a, &b);
+  const fdat d0 = fd_lerp(d.y, &d00, &d10);
+  const fdat d1 = fd_lerp(d.y, &d01, &d11);
+  return fd_lerp(d.z, &d0, &d1);
+}
+
+/* nanovdb::Ray::intersects on the world box; exit t when the origin is strictly inside. */
+static float med_box_hit(const med_t* m, f3 o, f3 d) {
+  float t0 = 0.0f, t1 = DEFAULT_TMAX;
+  const f3 inv = F3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  for (int i = 0; i < 3; ++i) {
+    float a = comp3(m->bbMin, i), b = comp3(m->bbMax, i);
+    if (a >= b) return -1.0f;
+    a = (a - comp3(o, i)) * comp3(inv, i);
+    b = (b - comp3(o, i)) * comp3(inv, i);
+    if (a > b) { float t = a; a = b; b = t; }
+    if (a > t0) t0 = a;
+    if (b < t1) t1 = b;
+    if (t0 > t1) return -1.0f;
+  }
+  if (!(t1 < DEFAULT_TMAX)) return -1.0f;
+  const int inside = o.x > m->bbMin.x && o.y > m->bbMin.y && o.z > m->bbMin.z && o.x < m->bbMax.x &&
+                     o.y < m->bbMax.y && o.z < m->bbMax.z;
+  return inside ? t1 : t0;
+}
+
+static uint32_t brick_word(const uint32_t* a, int nx, int ny, int nz, int x, int y, int z) {
+  if (x < 0 || y < 0 || z < 0 || x >= nx || y >= ny || z >= nz) return 0u;
+  return a[(size_t)x + (size_t)y * nx + (size_t)z * nx * ny];
+}
+static float brick_majorant(const med_t* m, f3 ip, int mip) {
+  const int bx = (int)floorf(ip.x) >> 3, by = (int)floorf(ip.y) >> 3, bz = (int)floorf(ip.z) >> 3;
+  const int nx = (int)m->b.nb[0], ny = (int)m->b.nb[1], nz = (int)m->b.nb[2];
+  uint32_t w;
+  if (mip <= 0) w = brick_word(m->b.range, nx, ny, nz, bx, by, bz);
+  else w = brick_word(m->b.mips[mip - 1], nx >> mip, ny >> mip, nz >> mip, bx >> mip, by >> mip, bz >> mip);
+  return half_to_float((uint16_t)(w >> 16));
+}
+static float brick_density(const med_t* m, f3 ip) {
+  const int ix = (int)floorf(ip.x), iy = (int)floorf(ip.y), iz = (int)floorf(ip.z);
+  const int nx = (int)m->b.nb[0], ny = (int)m->b.nb[1], nz = (int)m->b.nb[2];
+  const uint32_t ptr = brick_word(m->b.ind, nx, ny, nz, ix >> 3, iy >> 3, iz >> 3);
+  const uint32_t rw = brick_word(m->b.range, nx, ny, nz, ix >> 3, iy >> 3, iz >> 3);
+  const int ax = (int)((ptr >> 22) & 1023u) * 8 + (ix & 7);
+  const int ay = (int)((ptr >> 12) & 1023u) * 8 + (iy & 7);
+  const int az = (int)((ptr >> 2) & 1023u) * 8 + (iz & 7);
+  uint8_t v = 0;
+  if (ax < (int)m->b.ad[0] && ay < (int)m->b.ad[1] && az < (int)m->b.ad[2])
+    v = m->b.atlas[(size_t)ax + (size_t)ay * m->b.ad[0] + (size_t)az * m->b.ad[0] * m->b.ad[1]];
+  const float lo = half_to_float((uint16_t)(rw & 0xFFFFu)), hi = half_to_float((uint16_t)(rw >> 16));
+  return lo + (float)v * (1.0f / 255.0f) * (hi - lo);
+}
+static float step_dda(f3 pos, f3 inv, int mip) {
+  const float dim = (float)(8 << mip);
+  const float ox = inv.x >= 0.0f ? dim + 0.5f : -0.5f;
+  const float oy = inv.y >= 0.0f ? dim + 0.5f : -0.5f;
+  const float oz = inv.z >= 0.0f ? dim + 0.5f : -0.5f;
+  const float tx = (floorf(pos.x * (1.0f / dim)) * dim + ox - pos.x) * inv.x;
+  const float ty = (floorf(pos.y * (1.0f / dim)) * dim + oy - pos.y) * inv.y;
+  const float tz = (floorf(pos.z * (1.0f / dim)) * dim + oz - pos.z) * inv.z;
+  return fminf(tx, fminf(ty, tz));
+}
+
+typedef struct { int hit; f3 pos, normal; float S[6]; float ior; } mev_t;
+
+static f3 scatter_albedo(const med_t* m, const fdat* fd, f3 dirModel) {
+  const f3 n = norm3(fd->normal);
+  const float w = fresnel(1.0f, fd->ior, fabsf(dot3(norm3(neg3(dirModel)), n)));
+  const f3 a = add3(mul3s(fd->diffuse, 1.0f - w), mul3s(fd->specular, w));
+  return F3(a.x * m->sigmaS.x / m->sigmaT, a.y * m->sigmaS.y / m->sigmaT, a.z * m->sigmaS.z / m->sigmaT);
+}
+static void fill_event(mev_t* ev, ray_t w, const fdat* fd) {
+  ev->hit = 1;
+  ev->pos = add3(w.o, mul3s(w.d, w.tmax));
+  ev->normal = norm3(fd->normal);
+  for (int k = 0; k < 6; ++k) ev->S[k] = fd->S[k];
+  ev->ior = fd->ior;
+}
+static float inv_majorant(const med_t* m) { return 1.0f / (m->ratio / m->invMax); }
+
+static f3 med_sample_internal(const med_t* m, ray_t rm, rng_t* rng, mev_t* ev, int* err) {
+  ray_t ray = ray_xf2(rm, m->m2i);
+  const float invMax = inv_majorant(m);
+  if (!(invMax < INFINITY)) return F3(1.0f, 1.0f, 1.0f);
+  float t = 0.0f;
+  for (int it = 0; it < MAX_TRACKING_STEPS; ++it) {
+    t -= oi_log(1.0f - rng_next(rng)) * invMax / m->sigmaT;
+    if (t >= ray.tmax) return F3(1.0f, 1.0f, 1.0f);
+    const fdat fd = med_filtered(m, add3(ray.o, mul3s(ray.d, t)));
+    if (m->ratio * fd.density * invMax > rng_next(rng)) {
+      ray.tmax = t;
+      const ray_t w = ray_xf2(ray, m->i2m);
+      fill_event(ev, w, &fd);
+      return scatter_albedo(m, &fd, w.d);
+    }
+  }
+  *err = 1;
+  return F3(0.0f, 0.0f, 0.0f);
+}
+
+static f3 med_sample_dda(const med_t* m, ray_t rm, rng_t* rng, mev_t* ev, int* err) {
+  ray_t iray = ray_xf2(rm, m->u2s);
+  const f3 ri = F3(1.0f / iray.d.x, 1.0f / iray.d.y, 1.0f / iray.d.z);
+  float t = 0.0f;
+  float tau = -oi_log(1.0f - rng_next(rng));
+  float mip = 3.0f;
+  for (int it = 0; it < MAX_TRACKING_STEPS; ++it) {
+    if (!(t < iray.tmax)) return F3(1.0f, 1.0f, 1.0f);
+    const f3 curr = add3(iray.o, mul3s(iray.d, t));
+    const int mi = (int)roundf(mip);
+    const float majorant = m->ratio * brick_majorant(m, curr, mi);
+    const float dt = step_dda(curr, ri, mi);
+    const float prevT = t;
+    t += dt / m->sigmaT;
+    if (t == prevT) return F3(1.0f, 1.0f, 1.0f);
+    tau -= majorant * dt;
+    mip = fminf(mip + 0.25f, 3.0f);
+    if (tau > 0.0f) continue;
+    t += tau / (majorant * m->sigmaT);
+    if (t >= iray.tmax) return F3(1.0f, 1.0f, 1.0f);
+    const float jx = rng_next(rng);
+    const float jy = rng_next(rng);
+    const float jz = rng_next(rng);
+    const float d = brick_density(m, sub3(add3(add3(iray.o, mul3s(iray.d, t)), F3(jx, jy, jz)), F3(0.5f, 0.5f, 0.5f)));
+    if (rng_next(rng) * majorant < d * m->ratio) {
+      iray.tmax = t;
+      const f3 ip = add3(iray.o, mul3s(iray.d, t));
+      const f3 pos = F3((ip.x - (float)m->ibbMin[0]) / (float)m->size[0], (ip.y - (float)m->ibbMin[1]) / (float)m->size[1],
+                        (ip.z - (float)m->ibbMin[2]) / (float)m->size[2]);
+      const fdat fd = med_filtered(m, pos);
+      const ray_t w = ray_xf2(iray, m->s2m);
+      fill_event(ev, w, &fd);
+      return scatter_albedo(m, &fd, w.d);
+    }
+    tau = -oi_log(1.0f - rng_next(rng));
+    mip = fmaxf(0.0f, mip - 2.0f);
+  }
+  *err = 1;
+  return F3(0.0f, 0.0f, 0.0f);
+}
+
+static float med_tr_internal(const med_t* m, ray_t rm, rng_t* rng, int* err) {
+  const ray_t ray = ray_xf2(rm, m->m2i);
+  const float invMax = inv_majorant(m);
+  if (!(invMax < INFINITY)) return 1.0f;
+  float tr = 1.0f, t = 0.0f;
+  for (int it = 0; it < MAX_TRACKING_STEPS; ++it) {
+    t -= oi_log(1.0f - rng_next(rng)) * invMax / m->sigmaT;
+    if (t >= ray.tmax) return tr;
+    const float d = med_filtered(m, add3(ray.o, mul3s(ray.d, t))).density;
+    tr *= 1.0f - fmaxf(0.0f, m->ratio * d * invMax);
+    if (tr < 1.0f) {
+      const float p = 1.0f - tr;
+      if (rng_next(rng) < p) return 0.0f;
+      tr /= 1.0f - p;
+    }
+  }
+  *err = 1;
+  return 0.0f;
+}
+
+static float med_tr_dda(const med_t* m, ray_t rm, rng_t* rng, int* err) {
+  const ray_t iray = ray_xf2(rm, m->u2s);
+  const f3 ri = F3(1.0f / iray.d.x, 1.0f / iray.d.y, 1.0f / iray.d.z);
+  float tr = 1.0f, t = 0.0f;
+  const float volMajorant = 1.0f / inv_majorant(m);
+  float tau = -oi_log(1.0f - rng_next(rng));
+  float mip = 3.0f;
+  for (int it = 0; it < MAX_TRACKING_STEPS; ++it) {
+    if (!(t < iray.tmax)) return tr;
+    const f3 curr = add3(iray.o, mul3s(iray.d, t));
+    const int mi = (int)roundf(mip);
+    const float majorant = m->ratio * brick_majorant(m, curr, mi);
+    const float dt = step_dda(curr, ri, mi);
+    const float prevT = t;
+    t += dt / m->sigmaT;
+    if (t == prevT) return tr;
+    tau -= majorant * dt;
+    mip = fminf(mip + 0.25f, 3.0f);
+    if (tau > 0.0f) continue;
+    t += tau / (majorant * m->sigmaT);
+    if (t >= iray.tmax) return tr;
+    const float jx = rng_next(rng);
+    const float jy = rng_next(rng);
+    const float jz = rng_next(rng);
+    const float d = brick_density(m, sub3(add3(add3(iray.o, mul3s(iray.d, t)), F3(jx, jy, jz)), F3(0.5f, 0.5f, 0.5f)));
+    if (rng_next(rng) * majorant < d * m->ratio) {
+      tr *= fmaxf(0.0f, 1.0f - volMajorant / majorant);
+      if (tr < 0.1f) {
+        const float prob = 1.0f - tr;
+        if (rng_next(rng) < prob) return 0.0f;
+        tr /= 1.0f - prob;
+      }
+    }
+    tau = -oi_log(1.0f - rng_next(rng));
+    mip = fmaxf(0.0f, mip - 2.0f);
+  }
+  *err = 1;
+  return 0.0f;
+}
+
+static f3 inst_sample(const med_t* m, ray_t rw, int dda, rng_t* rng, mev_t* ev, int* err) {
+  const ray_t rm = ray_xf2(rw, m->w2m);
+  ev->hit = 0;
+  const f3 a = dda ? med_sample_dda(m, rm, rng, ev, err) : med_sample_internal(m, rm, rng, ev, err);
+  if (ev->hit) {
+    ev->pos = xpoint(m->m2w, ev->pos);
+    ev->normal = norm3(xvec(m->m2w, ev->normal));
+  }
+  return a;
+}
+static float inst_tr(const med_t* m, ray_t rw, int dda, rng_t* rng, int* err) {
+  const ray_t rm = ray_xf2(rw, m->w2m);
+  return dda ? med_tr_dda(m, rm, rng, err) : med_tr_internal(m, rm, rng, err);
+}
+
+/* CNVDBMedium::moveToVoxelBorder and CMediumInstance::moveToVoxelBorder. */
+static ray_t med_move(const med_t* m, ray_t rm) {
+  const ray_t ri = ray_xf(rm, m->m2i);
+  const f3 ibb = F3((float)m->ibbMin[0], (float)m->ibbMin[1], (float)m->ibbMin[2]);
+  const f3 sz = F3((float)m->size[0], (float)m->size[1], (float)m->size[2]);
+  const f3 ip = F3(ri.o.x * sz.x + ibb.x, ri.o.y * sz.y + ibb.y, ri.o.z * sz.z + ibb.z);
+  const f3 vlo = F3((floorf(ip.x) - ibb.x) / sz.x, (floorf(ip.y) - ibb.y) / sz.y, (floorf(ip.z) - ibb.z) / sz.z);
+  const f3 vhi = F3((ceilf(ip.x) - ibb.x) / sz.x, (ceilf(ip.y) - ibb.y) / sz.y, (ceilf(ip.z) - ibb.z) / sz.z);
+  const float eps = FLT_EPSILON;
+  const float gamma = (3.0f * eps) / (1.0f - 3.0f * eps);
+  float t1 = ri.tmax;
+  for (int i = 0; i < 3; ++i) {
+    const float inv = 1.0f / comp3(ri.d, i);
+    float tn = (comp3(vlo, i) - comp3(ri.o, i)) * inv;
+    float tf = (comp3(vhi, i) - comp3(ri.o, i)) * inv;
+    if (tn > tf) { float tt = tn; tn = tf; tf = tt; }
+    tf *= 1.0f + 2.0f * gamma;
+    t1 = tf < t1 ? tf : t1;
+  }
+  t1 *= (1.0f - RAY_OFFSET);
+  const ray_t moved = mkray(add3(ri.o, mul3s(ri.d, t1)), ri.d, ri.tmax - t1);
+  return ray_off(ray_xf(moved, m->i2m), neg3(rm.d));
+}
+static ray_t inst_move(const med_t* m, ray_t rw) {
+  const ray_t rm = ray_xf(rw, m->w2m);
+  const ray_t moved = med_move(m, rm);
+  return ray_off(ray_xf(moved, m->m2w), neg3(rw.d));
+}
+
+/* SGGX microflake distribution and phase function. */
+typedef struct { float S[6]; float inv[9]; f3 normal; } sggx_t;
+static float s_at(const float* S, int r, int c) {
+  if (r == c) return S[r];
+  const int a = r < c ? r : c, b = r < c ? c : r;
+  return (a == 0 && b == 1) ? S[3] : ((a == 0) ? S[4] : S[5]);
+}
+static float det3s(const float* S) {
+  return s_at(S, 0, 0) * (s_at(S, 1, 1) * s_at(S, 2, 2) - s_at(S, 2, 1) * s_at(S, 1, 2)) -
+         s_at(S, 1, 0) * (s_at(S, 0, 1) * s_at(S, 2, 2) - s_at(S, 2, 1) * s_at(S, 0, 2)) +
+         s_at(S, 2, 0) * (s_at(S, 0, 1) * s_at(S, 1, 2) - s_at(S, 1, 1) * s_at(S, 0, 2));
+}
+static f3 smul(const float* S, f3 w) {
+  return F3(s_at(S, 0, 0) * w.x + s_at(S, 1, 0) * w.y + s_at(S, 2, 0) * w.z,
+            s_at(S, 0, 1) * w.x + s_at(S, 1, 1) * w.y + s_at(S, 2, 1) * w.z,
+            s_at(S, 0, 2) * w.x + s_at(S, 1, 2) * w.y + s_at(S, 2, 2) * w.z);
+}
+static sggx_t make_sggx(const float* S, f3 n) {
+  sggx_t g;
+  float m[3][3];
+  for (int k = 0; k < 6; ++k) g.S[k] = S[k];
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) m[c][r] = s_at(S, r, c);
+  const float o = 1.0f / (m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]) -
+                          m[1][0] * (m[0][1] * m[2][2] - m[2][1] * m[0][2]) +
+                          m[2][0] * (m[0][1] * m[1][2] - m[1][1] * m[0][2]));
+  g.inv[0] = +(m[1][1] * m[2][2] - m[2][1] * m[1][2]) * o;
+  g.inv[3] = -(m[1][0] * m[2][2] - m[2][0] * m[1][2]) * o;
+  g.inv[6] = +(m[1][0] * m[2][1] - m[2][0] * m[1][1]) * o;
+  g.inv[1] = -(m[0][1] * m[2][2] - m[2][1] * m[0][2]) * o;
+  g.inv[4] = +(m[0][0] * m[2][2] - m[2][0] * m[0][2]) * o;
+  g.inv[7] = -(m[0][0] * m[2][1] - m[2][0] * m[0][1]) * o;
+  g.inv[2] = +(m[0][1] * m[1][2] - m[1][1] * m[0][2]) * o;
+  g.inv[5] = -(m[0][0] * m[1][2] - m[1][0] * m[0][2]) * o;
+  g.inv[8] = +(m[0][0] * m[1][1] - m[1][0] * m[0][1]) * o;
+  g.normal = n;
+  return g;
+}
+static float sggx_D(const sggx_t* g, f3 w) {
+  const f3 iw = F3(g->inv[0] * w.x + g->inv[3] * w.y + g->inv[6] * w.z, g->inv[1] * w.x + g->inv[4] * w.y + g->inv[7] * w.z,
+                   g->inv[2] * w.x + g->inv[5] * w.y + g->inv[8] * w.z);
+  const float v = dot3(w, iw);
+  return (float)(1.0 / (PI_D * (double)sqrtf(fabsf(det3s(g->S))) * (double)v * (double)v));
+}
+static float sggx_sigma(const sggx_t* g, f3 w) { return sqrtf(fmaxf(dot3(w, smul(g->S, w)), 0.0f)); }
+static f3 sggx_vndf(const sggx_t* g, float u1, float u2) {
+  const f3 N = g->normal;
+  f3 T, B;
+  if (N.z < -0.9999999f) {
+    T = F3(0.0f, -1.0f, 0.0f);
+    B = F3(-1.0f, 0.0f, 0.0f);
+  } else {
+    const float a = 1.0f / (1.0f + N.z);
+    const float b = -N.x * N.y * a;
+    T = norm3(F3(1.0f - N.x * N.x * a, b, -N.x));
+    B = norm3(F3(b, 1.0f - N.y * N.y * a, -N.y));
+  }
+  const f3 wk = B, wj = T, wi = N;
+  const float Skk = dot3(wk, smul(g->S, wk)), Skj = dot3(wk, smul(g->S, wj)), Ski = dot3(wk, smul(g->S, wi));
+  const float Sjj = dot3(wj, smul(g->S, wj)), Sji = dot3(wj, smul(g->S, wi)), Sii = dot3(wi, smul(g->S, wi));
+  const float P[6] = {Skk, Sjj, Sii, Skj, Ski, Sji};
+  const float temp = sqrtf(Sjj * Sii - Sji * Sji);
+  const f3 Mk = F3(sqrtf(fabsf(det3s(P))) / temp, 0.0f, 0.0f);
+  const float scaling = 1.0f / sqrtf(Sii);
+  const f3 Mj = mul3s(F3(-(Ski * Sji - Skj * Sii) / temp, temp, 0.0f), scaling);
+  const f3 Mi = mul3s(F3(Ski, Sji, Sii), scaling);
+  const float sq = sqrtf(u1);
+  float sn, cs;
+  orc_sincos_turns(u2, &sn, &cs);
+  const float u = sq * cs, v = sq * sn;
+  const float w = sqrtf(1.0f - u * u - v * v);
+  const f3 wm = norm3(add3(add3(mul3s(Mk, u), mul3s(Mj, v)), mul3s(Mi, w)));
+  return norm3(add3(add3(mul3s(wk, wm.x), mul3s(wj, wm.y)), mul3s(wi, wm.z)));
+}
+static float sggx_p_spec(const sggx_t* g, f3 wo, f3 wi) {
+  const f3 wh = norm3(add3(wi, wo));
+  return sggx_D(g, wh) / (4.0f * sggx_sigma(g, wo));
+}
+static float sggx_p(const sggx_t* g, float ior, f3 wo, f3 wi, rng_t* rng) {
+  const float w = fresnel(1.0f, ior, fabsf(dot3(norm3(wo), g->normal)));
+  const float a = rng_next(rng);
+  const float b = rng_next(rng);
+  const f3 wm = sggx_vndf(g, a, b);
+  const float pd = (float)((double)fmaxf(dot3(wi, wm), 0.0f) / PI_D);
+  return pd * (1.0f - w) + sggx_p_spec(g, wo, wi) * w;
+}
+static float sggx_sample_p(const sggx_t* g, float ior, f3 wo, f3* wi, rng_t* rng) {
+  const float w = fresnel(1.0f, ior, fabsf(dot3(norm3(wo), g->normal)));
+  if (rng_next(rng) < w) {
+    const float a = rng_next(rng);
+    const float b = rng_next(rng);
+    const f3 wm = sggx_vndf(g, a, b);
+    *wi = reflect3(neg3(wo), wm);
+    return sggx_p_spec(g, wo, *wi);
+  }
+  const float a = rng_next(rng);
+  const float b = rng_next(rng);
+  const f3 wn = sggx_vndf(g, a, b);
+  const frame_t fr = frame_from_normal(wn);
+  const float c1 = rng_next(rng);
+  const float c2 = rng_next(rng);
+  *wi = norm3(to_world(&fr, cosine_hemisphere(c1, c2)));
+  return (float)((double)fmaxf(dot3(*wi, wn), 0.0f) / PI_D);
+}
+
+/* getRotation (functions.hpp:128-142): +Y to `n`, entries rounded. */
+static m4_t rot_from_normal(f3 n) {
+  m4_t r = oi_m4_id();
+  const float c = dot3(n, F3(0.0f, 1.0f, 0.0f));
+  if (c == 1.0f) return r;
+  if (c == -1.0f) { r.m[0][0] = r.m[1][1] = r.m[2][2] = -1.0f; return r; }
+  const float angle = acosf(c);
+  const f3 ax = norm3(cross3(n, F3(0.0f, 1.0f, 0.0f)));
+  const float cs = cosf(angle), sn = sinf(angle);
+  const f3 tp = mul3s(ax, 1.0f - cs);
+  r.m[0][0] = cs + tp.x * ax.x; r.m[0][1] = tp.x * ax.y + sn * ax.z; r.m[0][2] = tp.x * ax.z - sn * ax.y;
+  r.m[1][0] = tp.y * ax.x - sn * ax.z; r.m[1][1] = cs + tp.y * ax.y; r.m[1][2] = tp.y * ax.z + sn * ax.x;
+  r.m[2][0] = tp.z * ax.x + sn * ax.y; r.m[2][1] = tp.z * ax.y - sn * ax.x; r.m[2][2] = cs + tp.z * ax.z;
+  for (int c2 = 0; c2 < 4; ++c2)
+    for (int i = 0; i < 4; ++i) r.m[c2][i] = roundf(r.m[c2][i]);
+  return r;
+}
+static m4_t affine4(m4_t a) {
+  for (int c = 0; c < 4; ++c) a.m[c][3] = c == 3 ? 1.0f : 0.0f;
+  return a;
+}
+
+/* CNVDBMedium::getVoxelSizeFiltering: trailing \d+\.\d+ of the path. */
+static int voxel_size_from_path(const char* path, float* out) {
+  size_t n = strlen(path), i = n;
+  while (i > 0 && path[i - 1] >= '0' && path[i - 1] <= '9') --i;
+  if (i == n || i == 0 || path[i - 1] != '.') return -1;
+  size_t k = i - 1;
+  while (k > 0 && path[k - 1] >= '0' && path[k - 1] <= '9') --k;
+  if (k == i - 1) return -1;
+  *out = strtof(path + k, NULL);
+  return 0;
+}
+
+static int med_load(med_t* m, const orc_medium* om) {
+  memset(m, 0, sizeof(*m));
+  char buf[4096];
+  float vsF;
+  if (voxel_size_from_path(om->path, &vsF)) return -1;
+  snprintf(buf, sizeof(buf), "%s.nvdb", om->path);
+  if (oi_nvdb_read(buf, &m->g)) return -2;
+  snprintf(buf, sizeof(buf), "%s.brickgrid", om->path);
+  if (oi_bricks_read(buf, &m->b)) { oi_nvdb_free(&m->g); return -3; }
+  for (int k = 0; k < 3; ++k) {
+    const int lo = m->g.voxelCount == 0 ? 0 : m->g.indexBBox[k];
+    const int hi = m->g.voxelCount == 0 ? 0 : m->g.indexBBox[3 + k];
+    m->ibbMin[k] = lo;
+    m->size[k] = hi - lo + 1;
+  }
+  m4_t nano = oi_m4_id(), toNano = oi_m4_id();
+  for (int c = 0; c < 3; ++c)
+    for (int r = 0; r < 3; ++r) nano.m[c][r] = m->g.matF[3 * r + c];
+  for (int r = 0; r < 3; ++r) nano.m[3][r] = m->g.vecF[r];
+  for (int k = 0; k < 3; ++k) { toNano.m[k][k] = (float)m->size[k]; toNano.m[3][k] = (float)m->ibbMin[k]; }
+  const m4_t i2m = affine4(oi_m4_mul(nano, toNano));
+  const m4_t m2i = affine4(oi_m4_inv(i2m));
+  const m4_t s2i = affine4(oi_m4_inv(toNano));
+  oi_m4_to43(i2m, m->i2m);
+  oi_m4_to43(m2i, m->m2i);
+  oi_m4_to43(oi_m4_mul(toNano, m2i), m->u2s);
+  oi_m4_to43(oi_m4_mul(i2m, s2i), m->s2m);
+  m->sigmaS = F3(om->sigma_s[0], om->sigma_s[1], om->sigma_s[2]);
+  m->sigmaT = fmaxf(om->sigma_a[0] + om->sigma_s[0], fmaxf(om->sigma_a[1] + om->sigma_s[1], om->sigma_a[2] + om->sigma_s[2]));
+  m->invMax = 1.0f / oi_nvdb_max_density(&m->g);
+  m4_t T = oi_m4_id(), Sc = oi_m4_id();
+  for (int k = 0; k < 3; ++k) { T.m[3][k] = om->pos[k]; Sc.m[k][k] = om->scaling[k]; }
+  const m4_t m2w = oi_m4_mul(oi_m4_mul(T, rot_from_normal(F3(om->orientation[0], om->orientation[1], om->orientation[2]))), Sc);
+  oi_m4_to43(m2w, m->m2w);
+  oi_m4_to43(oi_m4_inv(m2w), m->w2m);
+  const f3 bmin = F3((float)m->g.worldBBox[0], (float)m->g.worldBBox[1], (float)m->g.worldBBox[2]);
+  const f3 bmax = F3((float)m->g.worldBBox[3], (float)m->g.worldBBox[4], (float)m->g.worldBBox[5]);
+  const f3 a = xpoint(m->m2w, bmin), b = xpoint(m->m2w, bmax);
+  m->bbMin = F3(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z);
+  m->bbMax = F3(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z);
+  m->ratio = vsF / ((m->bbMax.x - m->bbMin.x) / (float)m->size[0]);
+  return 0;
+}
+static void med_free(med_t* m) {
+  oi_nvdb_free(&m->g);
+  oi_bricks_free(&m->b);
+}
+
 /* ------------------------------------------------------------ scene */
 typedef struct {
   int32_t* nodes;
@@ -416,6 +1004,9 @@ typedef struct {
   const orc_shape* shapes;
   mat_t* shapeMats;
   uint32_t nshapes;
+  med_t* media;
+  uint32_t nmedia;
+  int dda;
   env_t env;
   /* camera */
   float v2w[12];
@@ -464,9 +1055,23 @@ static int scene_closest(const rscene_t* S, f3 o, f3 d, float tmax, float* tOut,
         }
       }
     }
-    if (ts > 0.0f && ts < t) { t = ts; code = -2 - (int)i; }
+    if (ts > 0.0f && ts < t) { t = ts; *b1 = *b2 = 0.0f; code = -2 - (int)i; }
   }
   *tOut = t;
+  return code;
+}
+
+/* closest including the medium boxes: code MEDIUM_CODE_BASE - m for medium m */
+static int scene_closest_media(const rscene_t* S, f3 o, f3 d, float tmax, float* tOut, float* b1, float* b2) {
+  int code = scene_closest(S, o, d, tmax, tOut, b1, b2);
+  for (uint32_t m = 0; m < S->nmedia; ++m) {
+    const float tm = med_box_hit(&S->media[m], o, d);
+    if (tm >= 0.0f && tm <= tmax && tm < *tOut) {
+      *tOut = tm;
+      *b1 = *b2 = 0.0f;
+      code = MEDIUM_CODE_BASE - (int)m;
+    }
+  }
   return code;
 }
 
@@ -489,6 +1094,77 @@ static void philox_u(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_
   orc_philox4x32_10(ctr, key, out);
 }
 
+/* intersectTr as direct() uses it: 0 when the walk ends on a surface, else
+ * the product of the media's ratio-tracking estimates along the segments. */
+static float shadow_tr(const rscene_t* S, f3 o, f3 d, float tmax, int med, rng_t* rng, int* err) {
+  if (scene_occluded(S, o, d, tmax)) return 0.0f;
+  float tr = 1.0f;
+  if (S->nmedia == 0) return tr;
+  f3 p0 = o;
+  const f3 p1 = add3(o, mul3s(d, tmax));
+  int cur = med;
+  for (int k = 0; k < MAX_SHADOW_SEGMENTS; ++k) {
+    const f3 off = offset_origin(p0, norm3(sub3(p1, p0)));
+    const float tl = len3(sub3(p1, off));
+    const f3 dir = div3s(sub3(p1, p0), tl);
+    float best = tl;
+    int hitM = -1;
+    for (uint32_t m = 0; m < S->nmedia; ++m) {
+      const float tm = med_box_hit(&S->media[m], off, dir);
+      if (tm >= 0.0f && tm <= tl && tm < best) { best = tm; hitM = (int)m; }
+    }
+    if (hitM < 0) return tr;
+    if (cur >= 0 && hitM == cur) tr *= inst_tr(&S->media[cur], mkray(off, dir, best), S->dda, rng, err);
+    p0 = add3(off, mul3s(dir, best));
+    cur = cur < 0 ? hitM : -1;
+  }
+  *err = 1;
+  return 0.0f;
+}
+
+/* The medium part of Li (path_integrator_impl.hpp:127-192) up to the event
+ * the bounce shades; updates the ray, its medium, and the throughput. */
+static int extend_media(const rscene_t* S, uint32_t p, uint32_t s, uint32_t b, f3* o, f3* d, int* med, float* tmax,
+                        f3* T, float* tHit, float* hb1, float* hb2, mev_t* ev, int* evMed, int* err) {
+  int j;
+  for (j = 0; j < MAX_PASS_THROUGH; ++j) {
+    const int c = scene_closest_media(S, *o, *d, *tmax, tHit, hb1, hb2);
+    int dead = 0;
+    ev->hit = 0;
+    if (c <= MEDIUM_CODE_BASE) {
+      const int mi = MEDIUM_CODE_BASE - c;
+      rng_t rs = rng_make(p, S->seed, s, b, PURPOSE_MEDIUM + (uint32_t)j);
+      if (*med >= 0) {
+        if (mi != *med) dead = 1;
+        else { *T = mul3(*T, inst_sample(&S->media[*med], mkray(*o, *d, *tHit), S->dda, &rs, ev, err)); *evMed = *med; }
+      } else {
+        const ray_t mr = ray_off(mkray(add3(*o, mul3s(*d, *tHit)), norm3(*d), DEFAULT_TMAX), *d);
+        float te, e1, e2;
+        const int ce = scene_closest_media(S, mr.o, mr.d, mr.tmax, &te, &e1, &e2);
+        if (ce != -1) {
+          if (ce <= MEDIUM_CODE_BASE && MEDIUM_CODE_BASE - ce != mi) dead = 1;
+          else { *T = mul3(*T, inst_sample(&S->media[mi], mkray(mr.o, mr.d, te), S->dda, &rs, ev, err)); *evMed = mi; }
+        }
+      }
+      if (*err) dead = 1;
+      if (!dead && (T->x == 0.0f || T->y == 0.0f || T->z == 0.0f)) dead = 1;
+    }
+    if (dead) return EV_DEAD;
+    if (ev->hit) return EV_SCATTER;
+    if (c <= MEDIUM_CODE_BASE) {
+      const ray_t nr = ray_off(mkray(add3(*o, mul3s(*d, *tHit)), norm3(*d), DEFAULT_TMAX), *d);
+      *o = nr.o;
+      *d = nr.d;
+      *tmax = nr.tmax;
+      *med = *med < 0 ? MEDIUM_CODE_BASE - c : -1;
+      continue;
+    }
+    return c;
+  }
+  *err = 1;
+  return EV_DEAD;
+}
+
 static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
   const int px = (int)(p % (uint32_t)S->W), py = (int)(p / (uint32_t)S->W);
   uint32_t r[4];
@@ -500,9 +1176,15 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
   f3 o = xpoint(S->v2w, F3(0.0f, 0.0f, 0.0f));
   f3 d = norm3(xvec(S->v2w, dv));
   f3 T = F3(1.0f, 1.0f, 1.0f), L = F3(0.0f, 0.0f, 0.0f);
+  int med = -1;
+  float tmax = DEFAULT_TMAX;
   for (uint32_t b = 0; b < S->maxDepth; ++b) {
     float t, hb1, hb2;
-    int code = scene_closest(S, o, d, DEFAULT_TMAX, &t, &hb1, &hb2);
+    int code;
+    mev_t ev;
+    int evMed = -1, err = 0;
+    if (S->nmedia == 0) code = scene_closest(S, o, d, DEFAULT_TMAX, &t, &hb1, &hb2);
+    else code = extend_media(S, p, s, b, &o, &d, &med, &tmax, &T, &t, &hb1, &hb2, &ev, &evMed, &err);
     if (code == -1) {
       if (b == 0) {
         float lp;
@@ -510,6 +1192,69 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
         L = add3(L, mul3(le, T));
       }
       break;
+    }
+    if (code == EV_DEAD) break;
+    if (code == EV_SCATTER) {
+      /* direct() with the phase function, then the phase-sampled continuation */
+      const med_t* M = &S->media[evMed];
+      const sggx_t g = make_sggx(ev.S, ev.normal);
+      const f3 wo = neg3(d);
+      rng_t rs = rng_make(p, S->seed, s, b, PURPOSE_SCATTER);
+      f3 dl = F3(0.0f, 0.0f, 0.0f);
+      int anyShadow = 0;
+      {
+        f3 ldir;
+        float lpdf = 0.0f;
+        const float u0 = rng_next(&rs);
+        const float u1 = rng_next(&rs);
+        const f3 Le = env_sample(&S->env, u0, u1, &ldir, &lpdf);
+        if (lpdf > 0.0f) {
+          ldir = norm3(ldir);
+          const ray_t lr = inst_move(M, ray_off(mkray(ev.pos, ldir, DEFAULT_TMAX), ev.normal));
+          const float sp = sggx_p(&g, ev.ior, wo, ldir, &rs);
+          const float mis = (1.0f * lpdf) / (1.0f * lpdf + 1.0f * sp);
+          const f3 pre = mul3(mul3s(F3(sp, sp, sp), mis), Le);
+          rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 0u);
+          const float tr = shadow_tr(S, lr.o, lr.d, lr.tmax, evMed, &rt, &err);
+          dl = add3(dl, div3s(mul3s(pre, tr), lpdf));
+          anyShadow = 1;
+        }
+      }
+      {
+        f3 wi = F3(0.0f, 0.0f, 0.0f);
+        const float sp = sggx_sample_p(&g, ev.ior, wo, &wi, &rs);
+        if (sp > 0.0f) {
+          wi = norm3(wi);
+          const ray_t br = inst_move(M, ray_off(mkray(ev.pos, wi, DEFAULT_TMAX), ev.normal));
+          float lpdf;
+          const f3 Le = env_le(&S->env, wi, &lpdf);
+          const float mis = (1.0f * sp) / (1.0f * sp + 1.0f * lpdf);
+          const f3 pre = mul3(mul3s(F3(sp, sp, sp), mis), Le);
+          rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 1u);
+          const float tr = shadow_tr(S, br.o, br.d, br.tmax, evMed, &rt, &err);
+          dl = add3(dl, div3s(mul3s(pre, tr), sp));
+          anyShadow = 1;
+        }
+      }
+      if (anyShadow) L = add3(L, mul3(dl, T));
+      f3 wc = F3(0.0f, 0.0f, 0.0f);
+      sggx_sample_p(&g, ev.ior, wo, &wc, &rs);
+      const ray_t cr = inst_move(M, ray_off(mkray(ev.pos, norm3(wc), DEFAULT_TMAX), wc));
+      f3 Tn = T;
+      if (b > 3) {
+        uint32_t rC[4];
+        philox_u(s, b, 2u, 1u, p, S->seed, rC);
+        float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
+        if (oi_u01(rC[0]) <= prr) break;
+        Tn = div3s(Tn, 1.0f - prr);
+      }
+      if (b + 1 >= S->maxDepth) break;
+      o = cr.o;
+      d = cr.d;
+      tmax = cr.tmax;
+      med = evMed;
+      T = Tn;
+      continue;
     }
     f3 pos = add3(o, mul3s(d, t));
     f3 n;
@@ -549,7 +1294,14 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
         float spdf = mat_pdf(m, woT, lT);
         float mis = (1.0f * lpdf) / (1.0f * lpdf + 1.0f * spdf);
         f3 pre = mul3(mul3s(f, mis), Le);
-        float tr = scene_occluded(S, offO, ldir, DEFAULT_TMAX) ? 0.0f : 1.0f;
+        float tr;
+        if (S->nmedia == 0) {
+          tr = scene_occluded(S, offO, ldir, DEFAULT_TMAX) ? 0.0f : 1.0f;
+        } else {
+          const ray_t lr = ray_off(mkray(pos, ldir, DEFAULT_TMAX), n);
+          rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 0u);
+          tr = shadow_tr(S, offO, ldir, lr.tmax, med, &rt, &err);
+        }
         dl = add3(dl, div3s(mul3s(pre, tr), lpdf));
         anyShadow = 1;
       }
@@ -566,7 +1318,14 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
         f3 Le = env_le(&S->env, wi, &lpdf);
         float mis = (1.0f * spdf) / (1.0f * spdf + 1.0f * lpdf);
         f3 pre = mul3(mul3s(f, mis), Le);
-        float tr = scene_occluded(S, offO, wi, DEFAULT_TMAX) ? 0.0f : 1.0f;
+        float tr;
+        if (S->nmedia == 0) {
+          tr = scene_occluded(S, offO, wi, DEFAULT_TMAX) ? 0.0f : 1.0f;
+        } else {
+          const ray_t br = ray_off(mkray(pos, wi, DEFAULT_TMAX), n);
+          rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 1u);
+          tr = shadow_tr(S, offO, wi, br.tmax, med, &rt, &err);
+        }
         dl = add3(dl, div3s(mul3s(pre, tr), spdf));
         anyShadow = 1;
       }
@@ -589,6 +1348,7 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
       Tn = div3s(Tn, 1.0f - prr);
     }
     if (b + 1 >= S->maxDepth) break;
+    tmax = S->nmedia == 0 ? DEFAULT_TMAX : ray_off(mkray(pos, dirW, DEFAULT_TMAX), n).tmax;
     o = offO;
     d = dirW;
     T = Tn;
@@ -658,8 +1418,20 @@ static void make_cam(rscene_t* S, const orc_camera* c) {
 
 int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes, uint32_t nshapes, const float* env_rgb,
                int env_w, int env_h, const orc_camera* cam, uint32_t spp, uint32_t max_depth, uint32_t seed, uint32_t p0,
-               uint32_t p1, float* rgb_out, double* var_out, int threads) {
+               uint32_t p1, float* rgb_out, double* var_out, int threads, const orc_medium* media, uint32_t nmedia,
+               uint32_t flags) {
   if (env_w < 2 || env_h < 2 || spp == 0 || max_depth == 0) return -1;
+  med_t* meds = NULL;
+  if (nmedia > 0) {
+    meds = (med_t*)calloc(nmedia, sizeof(med_t));
+    for (uint32_t i = 0; i < nmedia; ++i) {
+      if (med_load(&meds[i], &media[i]) != 0) {
+        for (uint32_t k = 0; k < i; ++k) med_free(&meds[k]);
+        free(meds);
+        return -3;
+      }
+    }
+  }
   rscene_t S;
   memset(&S, 0, sizeof(S));
   uint32_t nv = 0, nt = 0;
@@ -703,6 +1475,9 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   S.spp = spp;
   S.maxDepth = max_depth;
   S.seed = seed;
+  S.media = meds;
+  S.nmedia = nmedia;
+  S.dda = (flags & 1u) ? 1 : 0;
   if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
   if (threads < 1) threads = 1;
   rjob_t* jobs = (rjob_t*)malloc(sizeof(rjob_t) * (size_t)threads);
@@ -717,8 +1492,12 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   env_free(&S.env);
   free(wpos); free(S.wnrm); free(S.idx); free(S.triMat); free(S.mats); free(S.shapeMats);
   if (nt > 0) { free(S.nodes); free(S.order); free(S.tris); }
+  for (uint32_t i = 0; i < nmedia; ++i) med_free(&meds[i]);
+  free(meds);
   return 0;
 }
+
+float orc_t_log(float x) { return oi_log(x); }
 
 int orc_env_sample(const float* env_rgb, int W, int H, float u0, float u1, float* dir, float* pdf, float* le) {
   env_t e;

@@ -39,6 +39,14 @@ typedef struct orc_shape {
   orc_material material;
 } orc_shape;
 
+/* Medium of a filtered LOD: <path>.nvdb + <path>.brickgrid, placed with
+ * T(pos) R(orientation) S(scaling) (sceneobject.cu:50-65). */
+typedef struct orc_medium {
+  const char* path;
+  float sigma_a[3], sigma_s[3];
+  float pos[3], orientation[3], scaling[3];
+} orc_medium;
+
 typedef struct orc_camera {
   uint32_t width, height;
   float fov_deg;
@@ -48,10 +56,15 @@ typedef struct orc_camera {
 /* Renders pixels [p0, p1) (row-major, row 0 = bottom) with spp samples.
  * rgb_out: 3 floats per pixel, the frame accumulation sum_s L_s / spp;
  * var_out (nullable): per pixel and channel, the unbiased sample variance of
- * L_s.  Returns 0 on success. */
+ * L_s.  media (nullable): heterogeneous SGGX media; flags bit 0 selects the
+ * brick-grid DDA tracking.  Returns 0 on success. */
 int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes, uint32_t nshapes,
                const float* env_rgb, int env_w, int env_h, const orc_camera* cam, uint32_t spp, uint32_t max_depth,
-               uint32_t seed, uint32_t p0, uint32_t p1, float* rgb_out, double* var_out, int threads);
+               uint32_t seed, uint32_t p0, uint32_t p1, float* rgb_out, double* var_out, int threads,
+               const orc_medium* media, uint32_t nmedia, uint32_t flags);
+
+/* Natural logarithm of the tracking code (exposed for unit tests). */
+float orc_t_log(float x);
 
 /* Environment sampling primitives, exposed for unit tests. */
 int orc_env_sample(const float* env_rgb, int env_w, int env_h, float u0, float u1, float* dir_out, float* pdf_out,

@@ -76,6 +76,8 @@ def _load():
         "r2_scene_add_mesh": (C.c_int, [P, P, u32, P, u32, P, P, P, u32]),
         "r2_scene_add_shape": (C.c_int, [P, C.c_int, P, f32, P, P, u32]),
         "r2_scene_set_envmap": (C.c_int, [P, P, u32, u32]),
+        "r2_scene_add_medium": (C.c_int, [P, C.c_char_p, P, P, P, P, P, u32]),
+        "r2_filter_run_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, P, P, C.c_char_p, C.c_char_p, P]),
         "r2_scene_commit": (C.c_int, [P]),
         "r2_render_device": (C.c_int, [P, P, P, P, P, P]),
         "r2_render_host": (C.c_int, [P, P, P, P]),

@@ -55,6 +55,14 @@ r2_status r2_scene_set_envmap(r2_scene* scene, const float* rgb, uint32_t width,
   R2_API_END
 }
 
+r2_status r2_scene_add_medium(r2_scene* scene, const char* path, const float* sigma_a, const float* sigma_s,
+                              const float* pos, const float* orientation, const float* scaling, uint32_t mask) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->add_medium(path, sigma_a, sigma_s, pos, orientation, scaling, mask);
+  R2_API_END
+}
+
 r2_status r2_scene_commit(r2_scene* scene) {
   R2_API_BEGIN
   R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
@@ -67,6 +75,10 @@ r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_re
   R2_API_BEGIN
   R2_REQUIRE(scene && camera && params && d_rgb, R2_ERR_INVALID_ARGUMENT, "null argument");
   scene->impl->render(*camera, *params, d_rgb, (cudaStream_t)stream, stats_out);
+  if (stats_out) {
+    const uint32_t b = scene->impl->bound_hits((cudaStream_t)stream);
+    R2_REQUIRE(b == 0, R2_ERR_DEVICE_TIMEOUT, std::to_string(b) + " paths or shadow rays ended by a loop bound");
+  }
   R2_API_END
 }
 
@@ -79,6 +91,8 @@ r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_rend
   scene->impl->render(*camera, *params, d.get(), s, nullptr);
   d.download(rgb, n, s);
   R2_CUDA(cudaStreamSynchronize(s));
+  const uint32_t b = scene->impl->bound_hits(s);
+  R2_REQUIRE(b == 0, R2_ERR_DEVICE_TIMEOUT, std::to_string(b) + " paths or shadow rays ended by a loop bound");
   R2_API_END
 }
 

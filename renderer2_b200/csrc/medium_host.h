@@ -1,0 +1,38 @@
+// Loading of a filtered medium for rendering: the NanoVDB grid (leaves copied
+// to the device with a flat leaf index), the brick grid and the transforms of
+// CNVDBMedium::init (raytracer/src/medium/nvdb_medium.cu:130-173,
+// getIndexToModelTransformation / getMaxValue) and of the medium's scene
+// object (raytracer/src/scene/sceneobject.cu:50-65, getFilterRenderRatio 108-114).
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "media.cuh"
+#include "runtime.h"
+#include "volume.h"
+
+namespace r2 {
+
+// CNVDBMedium::getVoxelSizeFiltering (nvdb_medium.cu:180-188): the trailing
+// "\d+\.\d+" of the path (without extension), as std::stof reads it.
+float voxel_size_from_path(const std::string& path);
+
+struct MediumHost {
+  MediumView view;  // device pointers are filled in by upload()
+  std::vector<uint8_t> leaves;
+  std::vector<int32_t> leafIndex;
+  BrickGridHost bricks;
+  DBuf<uint8_t> dLeaves, dAtlas;
+  DBuf<int32_t> dLeafIndex;
+  DBuf<uint32_t> dIndirection, dRange, dMips[3];
+  void upload(cudaStream_t s);
+  size_t device_bytes() const;
+};
+
+// Loads <path>.nvdb and <path>.brickgrid for a medium placed with
+// T(pos) R(orientation) S(scaling).
+std::unique_ptr<MediumHost> load_medium(const std::string& path, const float sigmaA[3], const float sigmaS[3],
+                                        V3 pos, V3 orientation, V3 scaling);
+
+}  // namespace r2

@@ -152,6 +152,39 @@ R2_HD void sincos_turns(float u, float* s, float* c) {
   else { *s = -cs; *c = sn; }
 }
 
+// ---------------------------------------------------------------------------
+// Natural logarithm of a positive normal float, written from the series
+// log m = 2 atanh(s) = 2 (s + s^3/3 + s^5/5 + ...), s = (m - 1)/(m + 1), after
+// the classical reduction x = m 2^e with m in [sqrt(1/2), sqrt(2)) (Cody and
+// Waite, "Software Manual for the Elementary Functions", 1980).  |s| <= 0.1716,
+// the series stops after s^11 (truncation below 1e-10 relative), and e ln 2 is
+// added in two parts (0.693145751953125 + 1.42860682e-6).  Every step is an
+// IEEE operation or an explicit fmaf, so host and device give identical bits.
+// Used for the free-flight distances of delta and ratio tracking.
+// ---------------------------------------------------------------------------
+R2_HD float log_r2(float x) {
+  uint32_t b;
+  memcpy(&b, &x, 4);
+  int e = (int)((b >> 23) & 0xFFu) - 127;
+  uint32_t mb = (b & 0x7FFFFFu) | 0x3F800000u;
+  float m;
+  memcpy(&m, &mb, 4);
+  if (m > 1.41421354f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float s2 = s * s;
+  float p = fmaf(s2, 1.0f / 11.0f, 1.0f / 9.0f);
+  p = fmaf(s2, p, 1.0f / 7.0f);
+  p = fmaf(s2, p, 1.0f / 5.0f);
+  p = fmaf(s2, p, 1.0f / 3.0f);
+  const float twoS = 2.0f * s;
+  const float lm = fmaf(twoS * s2, p, twoS);
+  const float fe = (float)e;
+  return fmaf(fe, 0.693145751953125f, fmaf(fe, 1.42860682e-6f, lm));
+}
+
 // CSampler::uniformSampleSphere (sampler.hpp:86-94): z = 1 - 2u1, phi = 2 pi u2.
 R2_HD V3 uniform_sample_sphere(float u1, float u2) {
   float z = 1.0f - 2.0f * u1;

@@ -2,7 +2,7 @@
 // and the host runtime (render_host.cu).
 #pragma once
 #include "bvh_build.cuh"
-#include "shading.h"
+#include "media.cuh"
 
 namespace r2 {
 
@@ -28,16 +28,19 @@ struct SceneView {
   const Shape* shapes;
   int nshapes;
   int hasTris;
+  const MediumView* media;  // medium instances (device array), nullable
+  int nmedia;
   EnvMap env;
 };
 
 // Per-path SoA state of one wave (one sample of every pixel).
 struct PathState {
-  float4* rayO;     // origin
-  float4* rayD;     // direction
+  float4* rayO;     // origin, .w = current medium index as int bits (-1: none)
+  float4* rayD;     // direction, .w = ray tmax
   float4* T;        // throughput
   float4* L;        // radiance
-  float4* hit;      // t, b1, b2, prim code (as int bits: >=0 tri, <= -2 shape, -1 miss)
+  float4* hit;      // t, b1, b2, event code (int bits: >= 0 triangle, -1 miss, -2 - i shape i,
+                    // kEventScatter medium collision, kEventDead path ended by a medium rule)
   uint32_t* q[2];   // ping-pong queues of live path ids
   uint32_t* counts; // [bounce] live path count entering the bounce
   // shadow records, two per queue slot (0: light sample, 1: BSDF sample)
@@ -45,8 +48,17 @@ struct PathState {
   float4* shD;      // direction.xyz, unused
   float4* shPre;    // (mis * f) * Le
   float4* shT;      // throughput at the bounce (one per slot pair)
-  uint8_t* vis;     // visibility of each shadow ray
+  float* shTr;      // transmittance of each shadow ray (0 or 1 without media)
+  // media scenes only
+  float2* shX;      // shadow ray tmax, medium index (int bits)
+  float4* evA;      // collision position, ior
+  float4* evB;      // collision normal, medium index (int bits)
+  float4* evC;      // SGGX S xx yy zz xy
+  float2* evD;      // SGGX S xz yz
 };
+
+constexpr int kEventScatter = -2147483647;  // INT_MIN + 1
+constexpr int kEventDead = -2147483646;     // INT_MIN + 2
 
 struct RenderLaunch {
   SceneView scene;
@@ -59,7 +71,9 @@ struct RenderLaunch {
   uint32_t maxDepth;
   uint32_t seed;
   uint32_t bounce;
+  uint32_t dda;       // brick-grid DDA tracking (UseBrickGrid) instead of the global majorant
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
+  unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };
 
 // Optional per-kernel timing of one wave: events recorded after each launch;

@@ -153,6 +153,17 @@ void RenderScene::set_envmap(const float* rgb, int W, int H) {
   committed_ = false;
 }
 
+void RenderScene::add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
+                             const float* orientation, const float* scaling, uint32_t mask) {
+  R2_REQUIRE(path && sigmaA && sigmaS && pos && orientation && scaling, R2_ERR_INVALID_ARGUMENT, "null medium argument");
+  R2_REQUIRE(media_.size() < 4096, R2_ERR_UNSUPPORTED, "too many media in one scene");
+  (void)mask;
+  media_.push_back(load_medium(path, sigmaA, sigmaS, v3(pos[0], pos[1], pos[2]),
+                               v3(orientation[0], orientation[1], orientation[2]),
+                               v3(scaling[0], scaling[1], scaling[2])));
+  committed_ = false;
+}
+
 void RenderScene::commit() {
   R2_REQUIRE(env_.W > 0, R2_ERR_INVALID_CONFIG, "scene has no environment map");
   cudaStream_t s = stream_;
@@ -189,6 +200,16 @@ void RenderScene::commit() {
   if (!hShapes_.empty()) shapes_.upload(hShapes_.data(), hShapes_.size(), s);
   view_.shapes = shapes_.get();
   view_.nshapes = (int)hShapes_.size();
+  if (!media_.empty()) {
+    std::vector<MediumView> mv;
+    for (auto& m : media_) {
+      m->upload(s);
+      mv.push_back(m->view);
+    }
+    mediaViews_.upload(mv.data(), mv.size(), s);
+  }
+  view_.media = mediaViews_.get();
+  view_.nmedia = (int)media_.size();
   // environment: texels + one float buffer for all distribution arrays
   envTex_.upload(env_.tex.data(), env_.tex.size(), s);
   std::vector<float> buf;
@@ -214,12 +235,19 @@ void RenderScene::commit() {
 }
 
 void RenderScene::ensure_state(uint32_t n) {
-  if (n <= cap_) return;
-  rayO_.alloc(n); rayD_.alloc(n); T_.alloc(n); L_.alloc(n); hit_.alloc(n);
-  shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
-  q0_.alloc(n); q1_.alloc(n); vis_.alloc(2 * (size_t)n);
-  counts_.alloc(64);
-  cap_ = n;
+  if (n > cap_) {
+    rayO_.alloc(n); rayD_.alloc(n); T_.alloc(n); L_.alloc(n); hit_.alloc(n);
+    shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
+    q0_.alloc(n); q1_.alloc(n); shTr_.alloc(2 * (size_t)n);
+    counts_.alloc(64);
+    bound_.alloc(1);
+    cap_ = n;
+  }
+  if (!media_.empty() && n > mediaCap_) {
+    shX_.alloc(2 * (size_t)n);
+    evA_.alloc(n); evB_.alloc(n); evC_.alloc(n); evD_.alloc(n);
+    mediaCap_ = n;
+  }
 }
 
 void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d_frame, cudaStream_t s,
@@ -228,6 +256,7 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
   R2_REQUIRE(c.width > 0 && c.height > 0, R2_ERR_INVALID_ARGUMENT, "empty frame");
   R2_REQUIRE(p.spp > 0, R2_ERR_INVALID_ARGUMENT, "spp must be positive");
   R2_REQUIRE(p.max_depth > 0 && p.max_depth <= 60, R2_ERR_UNSUPPORTED, "max_depth must be in [1, 60]");
+  R2_REQUIRE((p.flags & ~R2_RENDER_BRICK_GRID) == 0, R2_ERR_INVALID_ARGUMENT, "unknown render flags");
   if (!committed_) commit();
   if (!s) s = stream_;
   const uint32_t npix = c.width * c.height;
@@ -239,12 +268,19 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
   L.st.rayO = rayO_.get(); L.st.rayD = rayD_.get(); L.st.T = T_.get(); L.st.L = L_.get(); L.st.hit = hit_.get();
   L.st.q[0] = q0_.get(); L.st.q[1] = q1_.get(); L.st.counts = counts_.get();
   L.st.shO = shO_.get(); L.st.shD = shD_.get(); L.st.shPre = shPre_.get(); L.st.shT = shT_.get();
-  L.st.vis = vis_.get();
+  L.st.shTr = shTr_.get();
+  if (!media_.empty()) {
+    L.st.shX = shX_.get();
+    L.st.evA = evA_.get(); L.st.evB = evB_.get(); L.st.evC = evC_.get(); L.st.evD = evD_.get();
+  }
   L.frame = d_frame;
   L.npix = npix;
   L.spp = p.spp;
   L.maxDepth = p.max_depth;
   L.seed = p.seed;
+  L.dda = (p.flags & R2_RENDER_BRICK_GRID) ? 1u : 0u;
+  L.bound = bound_.get();
+  R2_CUDA(cudaMemsetAsync(bound_.get(), 0, sizeof(unsigned int), s));
   int nblocks = std::max(1, std::min((int)((npix + 255) / 256), sm_count() * 8));
   R2_CUDA(cudaMemsetAsync(d_frame, 0, sizeof(float) * 3 * (size_t)npix, s));
   if (stats) {
@@ -282,6 +318,14 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
     stats[3] = (double)cnt[1];
     for (int k = 1; k <= 4; ++k) stats[3 + k] = kms[k];  // one wave: extend, shade, shadow, accum
   }
+}
+
+uint32_t RenderScene::bound_hits(cudaStream_t s) {
+  if (!bound_.get()) return 0;
+  unsigned int b = 0;
+  bound_.download(&b, 1, s ? s : stream_);
+  R2_CUDA(cudaStreamSynchronize(s ? s : stream_));
+  return b;
 }
 
 }  // namespace r2

@@ -5,6 +5,7 @@
 #include <memory>
 #include <vector>
 
+#include "medium_host.h"
 #include "render.cuh"
 
 namespace r2 {
@@ -36,9 +37,14 @@ class RenderScene {
   void add_shape(int type, const float* center, float radius, const float* normal, const r2_material& mat,
                  uint32_t mask);
   void set_envmap(const float* rgb, int W, int H);
+  // Medium of a filtered LOD: <path>.nvdb + <path>.brickgrid placed with T(pos) R(orientation) S(scaling).
+  void add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
+                  const float* orientation, const float* scaling, uint32_t mask);
   void commit();
   // One frame: `spp` waves accumulated into d_frame (W*H*3 floats, cleared here).
   void render(const r2_camera& cam, const r2_render_params& p, float* d_frame, cudaStream_t s, double* stats);
+  // Paths and shadow rays of the last frame that a loop bound ended (waits for the stream).
+  uint32_t bound_hits(cudaStream_t s);
   cudaStream_t stream() const { return stream_; }
   uint32_t ntris() const { return (uint32_t)(hIdx_.size() / 3); }
   const DeviceBvh& bvh() const { return bvh_; }
@@ -52,6 +58,8 @@ class RenderScene {
   std::vector<uint32_t> hIdx_, hTriMat_;
   std::vector<Material> hMats_;
   std::vector<Shape> hShapes_;
+  std::vector<std::unique_ptr<MediumHost>> media_;
+  DBuf<MediumView> mediaViews_;
   EnvHost env_;
   DeviceBvh bvh_;
   DBuf<float4> triN_;
@@ -65,7 +73,11 @@ class RenderScene {
   uint32_t cap_ = 0;
   DBuf<float4> rayO_, rayD_, T_, L_, hit_, shO_, shD_, shPre_, shT_;
   DBuf<uint32_t> q0_, q1_, counts_;
-  DBuf<uint8_t> vis_;
+  DBuf<float> shTr_;
+  uint32_t mediaCap_ = 0;
+  DBuf<float2> shX_, evD_;
+  DBuf<float4> evA_, evB_, evC_;
+  DBuf<unsigned int> bound_;
   DBuf<unsigned long long> statBuf_;
   std::unique_ptr<WaveTimer> timer_;
 };

@@ -8,6 +8,7 @@ SFilteredDataCompact layout indexed x + y*nx + z*nx*ny.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass
 
 import numpy as np
@@ -129,3 +130,25 @@ def filter_mesh(mesh: Mesh, mat, prm, voxel_size: float, model_to_world=None, wi
                                  N.ptr(m2w), C.byref(prm), float(voxel_size), C.byref(g), N.ptr(out), N.ptr(w),
                                  nvox))
     return (g, out, w) if wide else (g, out)
+
+
+def run_filtering(mesh: Mesh, mat, prm, out_root, model, pos=(0, 0, 0), orientation=(0, 1, 0), scaling=(1, 1, 1)):
+    """All LODs of one FILTER object with file outputs (CFilter::runFiltering,
+    filter.cu:74-123): <out_root>/<model>/filtered_mesh_<vs>.nvdb and
+    .brickgrid per LOD plus <out_root>/volume_description.json.  Returns the
+    medium paths (without extension) and the stats
+    [lods, voxels, active voxels, kernel ms]."""
+    p = _c(mesh.positions, np.float32)
+    ix = _c(mesh.indices, np.uint32)
+    nr = _c(mesh.normals, np.float32)
+    pos3, ori3, sc3 = (_c(v, np.float32) for v in (pos, orientation, scaling))
+    st = np.zeros(4)
+    N.check(N.lib.r2_filter_run_mesh(N.ptr(p), mesh.nverts, N.ptr(ix), mesh.ntris, N.ptr(nr), C.byref(mat),
+                                     N.ptr(pos3), N.ptr(ori3), N.ptr(sc3), C.byref(prm), str(out_root).encode(),
+                                     str(model).encode(), N.ptr(st)))
+    vs = np.float32(prm.min_voxel_size)
+    paths = []
+    for _ in range(int(st[0])):
+        paths.append(os.path.join(str(out_root), str(model), "filtered_mesh_%f" % float(vs)))
+        vs = np.float32(vs * np.float32(2.0))
+    return paths, st

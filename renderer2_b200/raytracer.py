@@ -31,9 +31,13 @@ def camera(width, height, fov_deg=45.0, pos=(0, 0, 3), look_at=(0, 0, 0), up=(0,
     return c
 
 
-def params(spp=16, max_depth=8, seed=0) -> RenderParams:
+BRICK_GRID = 1  # R2_RENDER_BRICK_GRID ("UseBrickGrid")
+
+
+def params(spp=16, max_depth=8, seed=0, brick_grid=False) -> RenderParams:
     p = RenderParams()
-    p.spp, p.max_depth, p.seed, p.flags = int(spp), int(max_depth), int(seed), 0
+    p.spp, p.max_depth, p.seed = int(spp), int(max_depth), int(seed)
+    p.flags = BRICK_GRID if brick_grid else 0
     return p
 
 
@@ -73,6 +77,11 @@ class Scene:
         n = np.ascontiguousarray(normal, np.float32)
         N.check(N.lib.r2_scene_add_shape(self.handle, int(kind), N.ptr(c), float(radius), N.ptr(n), C.byref(material),
                                          mask))
+
+    def add_medium(self, path, sigma_a, sigma_s, pos=(0, 0, 0), orientation=(0, 1, 0), scaling=(1, 1, 1), mask=255):
+        """Medium "Path" of scenedescription.json: loads <path>.nvdb and <path>.brickgrid."""
+        arrs = [np.ascontiguousarray(v, np.float32) for v in (sigma_a, sigma_s, pos, orientation, scaling)]
+        N.check(N.lib.r2_scene_add_medium(self.handle, str(path).encode(), *[N.ptr(a) for a in arrs], mask))
 
     def set_envmap(self, rgb: np.ndarray):
         rgb = np.ascontiguousarray(rgb, np.float32)

@@ -161,17 +161,36 @@ class OCamera(C.Structure):
                 ("look_at", C.c_float * 3), ("up", C.c_float * 3)]
 
 
+class OMedium(C.Structure):
+    _fields_ = [("path", C.c_char_p), ("sigma_a", C.c_float * 3), ("sigma_s", C.c_float * 3), ("pos", C.c_float * 3),
+                ("orientation", C.c_float * 3), ("scaling", C.c_float * 3)]
+
+
 lib.orc_render.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
-                           C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int]
+                           C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_int,
+                           C.c_void_p, C.c_uint32, C.c_uint32]
 lib.orc_render.restype = C.c_int
+lib.orc_t_log.argtypes = [C.c_float]
+lib.orc_t_log.restype = C.c_float
 lib.orc_env_sample.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
 lib.orc_env_le.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
 
 
-def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want_var=False):
+def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want_var=False, flags=0):
     """scene_desc: dict(meshes=[(Mesh, native material, m2w)], shapes=[(kind, center, radius, normal, material)],
-    env=(H, W, 3) float32).  Returns rgb (n, 3) [, var (n, 3)] for pixels [p0, p1)."""
+    media=[(path, sigma_a, sigma_s, pos, orientation, scaling)], env=(H, W, 3) float32).
+    Returns rgb (n, 3) [, var (n, 3)] for pixels [p0, p1)."""
     keep = []
+    media = (OMedium * max(1, len(scene_desc.get("media", []))))()
+    for i, (path, sa, ss, pos, ori, sc) in enumerate(scene_desc.get("media", [])):
+        pb = str(path).encode()
+        keep.append(pb)
+        media[i].path = pb
+        media[i].sigma_a[:] = list(map(float, sa))
+        media[i].sigma_s[:] = list(map(float, ss))
+        media[i].pos[:] = list(map(float, pos))
+        media[i].orientation[:] = list(map(float, ori))
+        media[i].scaling[:] = list(map(float, sc))
     meshes = (OMesh * max(1, len(scene_desc.get("meshes", []))))()
     for i, (mesh, mat, m2w) in enumerate(scene_desc.get("meshes", [])):
         pos = np.ascontiguousarray(mesh.positions, np.float32)
@@ -201,6 +220,7 @@ def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want
     var = np.zeros((p1 - p0, 3), np.float64) if want_var else None
     r = lib.orc_render(C.addressof(meshes), len(scene_desc.get("meshes", [])), C.addressof(shapes),
                        len(scene_desc.get("shapes", [])), env.ctypes.data, env.shape[1], env.shape[0], C.byref(oc),
-                       spp, max_depth, seed, p0, p1, rgb.ctypes.data, _p(var), threads)
+                       spp, max_depth, seed, p0, p1, rgb.ctypes.data, _p(var), threads, C.addressof(media),
+                       len(scene_desc.get("media", [])), flags)
     assert r == 0, f"oracle render failed ({r})"
     return (rgb, var) if want_var else rgb

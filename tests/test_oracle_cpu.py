@@ -41,6 +41,22 @@ def test_sincos_turns_accuracy():
         assert abs(c - math.cos(x)) < 3e-7
 
 
+def test_tracking_log_accuracy():
+    # the free-flight logarithm of delta/ratio tracking, over every argument
+    # 1 - u that the 24-bit uniforms produce, stays within 2 ulp of log
+    rng = np.random.default_rng(5)
+    ks = np.concatenate([np.arange(1, 4096), rng.integers(1, 1 << 24, 20000), [1 << 23, (1 << 24) - 1, 1 << 24]])
+    worst = 0.0
+    for k in ks:
+        x = np.float32(int(k) * 2.0 ** -24)
+        got = O.lib.orc_t_log(float(x))
+        ref = math.log(float(x))
+        ulp = float(np.spacing(np.float32(abs(ref)))) if ref != 0.0 else 2.0 ** -149
+        worst = max(worst, abs(got - ref) / ulp)
+    assert O.lib.orc_t_log(1.0) == 0.0
+    assert worst <= 2.0, worst
+
+
 def _random_mesh(n, seed):
     rng = np.random.default_rng(seed)
     pos = rng.uniform(-1, 1, size=(3 * n, 3)).astype(np.float32)
