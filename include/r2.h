@@ -252,6 +252,11 @@ r2_status r2_scene_set_envmap(r2_scene* scene, const float* rgb, uint32_t width,
  * (raytracer/src/scene/sceneobject.cu:50-65). */
 r2_status r2_scene_add_medium(r2_scene* scene, const char* path, const float* sigma_a, const float* sigma_s,
                               const float* pos, const float* orientation, const float* scaling, uint32_t mask);
+/* Same with the Henyey-Greenstein phase function of asymmetry g (Medium with a
+ * "G" key; CNVDBMedium(path, sigma_a, sigma_s, g), nvdb_medium.cu:27-43). */
+r2_status r2_scene_add_medium_hg(r2_scene* scene, const char* path, const float* sigma_a, const float* sigma_s,
+                                 float g, const float* pos, const float* orientation, const float* scaling,
+                                 uint32_t mask);
 /* Uploads the scene and builds the BVH (device-resident until destroyed). */
 r2_status r2_scene_commit(r2_scene* scene);
 /* Renders one frame into device memory d_rgb (width*height*3 floats).
@@ -267,6 +272,65 @@ r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_re
 /* Same through host memory: commits if needed, renders, copies the frame to
  * rgb; loop bounds are reported as in r2_render_device. */
 r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* rgb);
+
+/* ------------------------------------------------------------------------ */
+/* Pipeline: config.json + scenedescription.json.
+ *
+ * Replaces CConfigLoader::loadConfig (raytracer/include/backend/config_loader.hpp:36-40,
+ * raytracer/src/backend/config_loader.cu:340-368) and CPipeline(configPath) / run()
+ * (raytracer/pipeline.hpp:5-17, pipeline.cu:18-90).  Loading parses both JSON
+ * files (comments allowed), reads the Radiance .hdr environment map and the
+ * OBJ/MTL meshes; media are read at the first render.  Relative paths resolve
+ * against the working directory, as in the reference. */
+typedef struct r2_config r2_config;
+
+typedef struct r2_config_info {
+  uint32_t frame_width, frame_height, channels, samples;  /* General */
+  float gamma;
+  uint32_t use_brick_grid;
+  uint32_t filter_active;                                  /* Filtering.Active */
+  r2_filter_params filter;                                 /* Filtering (seed 0) */
+  r2_camera camera;                                        /* Camera */
+  uint32_t env_width, env_height;                          /* Scene.Envmap */
+  uint32_t n_shapes, n_meshes, n_media;                    /* n_meshes counts OBJ submeshes */
+  uint32_t n_triangles;
+} r2_config_info;
+
+typedef struct r2_render_opts {
+  uint32_t spp;        /* 0: General.Samples */
+  uint32_t max_depth;  /* 0: 50, the reference's bounce cap */
+  uint32_t seed;
+  uint32_t flags;      /* reserved, 0 */
+} r2_render_opts;
+
+r2_status r2_config_load(const char* config_json_path, r2_config** out);
+r2_status r2_config_free(r2_config* cfg);
+r2_status r2_config_info_get(const r2_config* cfg, r2_config_info* out);
+/* CFilter(config).runFiltering() (raytracer/filter.hpp:183-214, filter.cu:20-123):
+ * the FILTER-masked mesh (one OBJ file, all its submeshes) filtered for every
+ * LOD into <out_root>/<mesh name>/filtered_mesh_<vs>.{nvdb,brickgrid} and
+ * <out_root>/volume_description.json; out_root NULL means "./filtering".
+ * Without FILTER objects nothing is written (R2_OK).  stats_out (nullable, 4
+ * doubles): LODs, voxels, active voxels, kernel milliseconds. */
+r2_status r2_filter_run(r2_config* cfg, const char* out_root, double* stats_out);
+/* Raytracer(config).renderFrame() (raytracer/raytracer.hpp:29-72,
+ * raytracer.cu:161-210): the scene stays resident on the device across calls.
+ * out_linear_rgb (nullable): W*H*3 pre-tonemap radiance, row 0 at the bottom;
+ * out_bytes (nullable): W*H*3 bytes after the log-average tonemap and gamma
+ * (SFrame::dataBytes). */
+r2_status r2_render(r2_config* cfg, const r2_render_opts* opts, float* out_linear_rgb, uint8_t* out_bytes);
+/* Output stage on host buffers (raytracer.cu:33-127): L = exp(sum log(r+g+b+FLT_MIN)
+ * / (3WH)) - WH FLT_MIN; c / (c + L); ^(1/gamma); bytes = round(255 c). */
+r2_status r2_tonemap(const float* linear_rgb, uint32_t width, uint32_t height, float gamma, float* out_rgb,
+                     uint8_t* out_bytes);
+/* Image files: 8-bit RGB PNG (flip_vertical as the reference's writer does for
+ * bottom-up frames) and Radiance RGBE .hdr (row 0 = top). */
+r2_status r2_write_png(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical);
+r2_status r2_read_hdr(const char* path, float* rgb, size_t capacity, uint32_t* width, uint32_t* height);
+r2_status r2_write_hdr(const char* path, const float* rgb, uint32_t width, uint32_t height);
+/* OBJ/MTL import summary (CAssetManager::loadWithAssimp, asset_manager.cu:25-84). */
+r2_status r2_obj_info(const char* directory, const char* filename, uint32_t* n_submeshes, uint32_t* n_vertices,
+                      uint32_t* n_triangles, r2_material* first_material);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic inputs (seeded), used by the configs in the benchmark plan. */

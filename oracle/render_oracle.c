@@ -487,6 +487,8 @@ typedef struct {
   int ibbMin[3], size[3];
   f3 sigmaS;
   float sigmaT, invMax;
+  int hg;
+  float hgG;
   oi_nvdb g;
   oi_bricks b;
 } med_t;
@@ -909,6 +911,31 @@ static float sggx_sample_p(const sggx_t* g, float ior, f3 wo, f3* wi, rng_t* rng
   return (float)((double)fmaxf(dot3(*wi, wn), 0.0f) / PI_D);
 }
 
+/* Henyey-Greenstein (henyey_greenstein_phase_function.hpp:22-50). */
+static float phase_hg(float cosTheta, float g) {
+  const float denom = 1.0f + g * g + 2.0f * g * cosTheta;
+  return (float)((double)(1.0f - g * g) / (4.0 * PI_D * (double)denom * (double)sqrtf(denom)));
+}
+static float hg_sample_p(float g, f3 wo, f3* wi, rng_t* rng) {
+  const float u1 = rng_next(rng);
+  const float u2 = rng_next(rng);
+  float cosTheta;
+  if (fabsf(g) < 1e-3f) {
+    cosTheta = 1.0f - 2.0f * u1;
+  } else {
+    const float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+    cosTheta = (1.0f + g * g - sq * sq) / (2.0f * g);
+  }
+  const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+  float s, c;
+  orc_sincos_turns(u2, &s, &c);
+  const f3 v1 = fabsf(wo.x) > fabsf(wo.y) ? div3s(F3(-wo.z, 0.0f, wo.x), sqrtf(wo.x * wo.x + wo.z * wo.z))
+                                          : div3s(F3(0.0f, wo.z, -wo.y), sqrtf(wo.y * wo.y + wo.z * wo.z));
+  const f3 v2 = cross3(wo, v1);
+  *wi = add3(add3(mul3s(v1, sinTheta * c), mul3s(v2, sinTheta * s)), mul3s(neg3(wo), cosTheta));
+  return phase_hg(-cosTheta, g);
+}
+
 /* getRotation (functions.hpp:128-142): +Y to `n`, entries rounded. */
 static m4_t rot_from_normal(f3 n) {
   m4_t r = oi_m4_id();
@@ -970,6 +997,8 @@ static int med_load(med_t* m, const orc_medium* om) {
   oi_m4_to43(m2i, m->m2i);
   oi_m4_to43(oi_m4_mul(toNano, m2i), m->u2s);
   oi_m4_to43(oi_m4_mul(i2m, s2i), m->s2m);
+  m->hg = om->hg;
+  m->hgG = om->g;
   m->sigmaS = F3(om->sigma_s[0], om->sigma_s[1], om->sigma_s[2]);
   m->sigmaT = fmaxf(om->sigma_a[0] + om->sigma_s[0], fmaxf(om->sigma_a[1] + om->sigma_s[1], om->sigma_a[2] + om->sigma_s[2]));
   m->invMax = 1.0f / oi_nvdb_max_density(&m->g);
@@ -1211,7 +1240,7 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
         if (lpdf > 0.0f) {
           ldir = norm3(ldir);
           const ray_t lr = inst_move(M, ray_off(mkray(ev.pos, ldir, DEFAULT_TMAX), ev.normal));
-          const float sp = sggx_p(&g, ev.ior, wo, ldir, &rs);
+          const float sp = M->hg ? phase_hg(dot3(wo, ldir), M->hgG) : sggx_p(&g, ev.ior, wo, ldir, &rs);
           const float mis = (1.0f * lpdf) / (1.0f * lpdf + 1.0f * sp);
           const f3 pre = mul3(mul3s(F3(sp, sp, sp), mis), Le);
           rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 0u);
@@ -1222,7 +1251,7 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
       }
       {
         f3 wi = F3(0.0f, 0.0f, 0.0f);
-        const float sp = sggx_sample_p(&g, ev.ior, wo, &wi, &rs);
+        const float sp = M->hg ? hg_sample_p(M->hgG, wo, &wi, &rs) : sggx_sample_p(&g, ev.ior, wo, &wi, &rs);
         if (sp > 0.0f) {
           wi = norm3(wi);
           const ray_t br = inst_move(M, ray_off(mkray(ev.pos, wi, DEFAULT_TMAX), ev.normal));
@@ -1238,7 +1267,8 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
       }
       if (anyShadow) L = add3(L, mul3(dl, T));
       f3 wc = F3(0.0f, 0.0f, 0.0f);
-      sggx_sample_p(&g, ev.ior, wo, &wc, &rs);
+      if (M->hg) hg_sample_p(M->hgG, wo, &wc, &rs);
+      else sggx_sample_p(&g, ev.ior, wo, &wc, &rs);
       const ray_t cr = inst_move(M, ray_off(mkray(ev.pos, norm3(wc), DEFAULT_TMAX), wc));
       f3 Tn = T;
       if (b > 3) {
@@ -1498,6 +1528,30 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
 }
 
 float orc_t_log(float x) { return oi_log(x); }
+
+/* Raytracer's output stage (raytracer.cu:33-127): column sums of
+ * log(r+g+b+FLT_MIN)/(3WH) in row order, their sum in column order,
+ * L = exp(sum) - WH FLT_MIN, c/(c+L), ^(1/gamma), round(255 c). */
+void orc_tonemap(const float* rgb, uint32_t W, uint32_t H, float gamma, float* out, uint8_t* bytes) {
+  const float divisor = (float)(H * W * 3);
+  float total = 0.0f;
+  for (uint32_t x = 0; x < W; ++x) {
+    float acc = 0.0f;
+    for (uint32_t y = 0; y < H; ++y) {
+      const float* p = rgb + 3 * ((size_t)y * W + x);
+      acc += logf(p[0] + p[1] + p[2] + FLT_MIN) / divisor;
+    }
+    total += acc;
+  }
+  const float L = expf(total) - (float)(W * H) * FLT_MIN;
+  const float invGamma = 1.0f / gamma;
+  for (size_t i = 0; i < (size_t)W * H * 3; ++i) {
+    const float c = rgb[i];
+    const float t = powf(c / (c + L), invGamma);
+    if (out) out[i] = t;
+    if (bytes) bytes[i] = (uint8_t)roundf(t * 255.0f);
+  }
+}
 
 int orc_env_sample(const float* env_rgb, int W, int H, float u0, float u1, float* dir, float* pdf, float* le) {
   env_t e;

@@ -45,6 +45,8 @@ typedef struct orc_medium {
   const char* path;
   float sigma_a[3], sigma_s[3];
   float pos[3], orientation[3], scaling[3];
+  int hg;  /* 1: Henyey-Greenstein phase function with asymmetry g instead of SGGX */
+  float g;
 } orc_medium;
 
 typedef struct orc_camera {
@@ -65,6 +67,9 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
 
 /* Natural logarithm of the tracking code (exposed for unit tests). */
 float orc_t_log(float x);
+
+/* Log-average tonemap, gamma and bytes of a linear W*H*3 frame (either output nullable). */
+void orc_tonemap(const float* rgb, uint32_t W, uint32_t H, float gamma, float* out, uint8_t* bytes);
 
 /* Environment sampling primitives, exposed for unit tests. */
 int orc_env_sample(const float* env_rgb, int env_w, int env_h, float u0, float u1, float* dir_out, float* pdf_out,

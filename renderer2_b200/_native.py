@@ -77,10 +77,21 @@ def _load():
         "r2_scene_add_shape": (C.c_int, [P, C.c_int, P, f32, P, P, u32]),
         "r2_scene_set_envmap": (C.c_int, [P, P, u32, u32]),
         "r2_scene_add_medium": (C.c_int, [P, C.c_char_p, P, P, P, P, P, u32]),
+        "r2_scene_add_medium_hg": (C.c_int, [P, C.c_char_p, P, P, f32, P, P, P, u32]),
         "r2_filter_run_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, P, P, C.c_char_p, C.c_char_p, P]),
         "r2_scene_commit": (C.c_int, [P]),
         "r2_render_device": (C.c_int, [P, P, P, P, P, P]),
         "r2_render_host": (C.c_int, [P, P, P, P]),
+        "r2_config_load": (C.c_int, [C.c_char_p, P]),
+        "r2_config_free": (C.c_int, [P]),
+        "r2_config_info_get": (C.c_int, [P, P]),
+        "r2_filter_run": (C.c_int, [P, C.c_char_p, P]),
+        "r2_render": (C.c_int, [P, P, P, P]),
+        "r2_tonemap": (C.c_int, [P, u32, u32, f32, P, P]),
+        "r2_write_png": (C.c_int, [C.c_char_p, P, u32, u32, C.c_int]),
+        "r2_read_hdr": (C.c_int, [C.c_char_p, P, sz, P, P]),
+        "r2_write_hdr": (C.c_int, [C.c_char_p, P, u32, u32]),
+        "r2_obj_info": (C.c_int, [C.c_char_p, C.c_char_p, P, P, P, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -63,6 +63,15 @@ r2_status r2_scene_add_medium(r2_scene* scene, const char* path, const float* si
   R2_API_END
 }
 
+r2_status r2_scene_add_medium_hg(r2_scene* scene, const char* path, const float* sigma_a, const float* sigma_s,
+                                 float g, const float* pos, const float* orientation, const float* scaling,
+                                 uint32_t mask) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->add_medium(path, sigma_a, sigma_s, pos, orientation, scaling, mask, true, g);
+  R2_API_END
+}
+
 r2_status r2_scene_commit(r2_scene* scene) {
   R2_API_BEGIN
   R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");

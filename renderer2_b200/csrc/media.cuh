@@ -56,6 +56,8 @@ struct MediumView {
   V3 sigmaS;
   float sigmaT;         // max over channels of sigma_a + sigma_s
   float invMaxDensity;  // 1 / max density of the grid
+  int hg;               // phase function: 0 SGGX (payload S), 1 Henyey-Greenstein with g
+  float g;
   // NanoVDB leaves (16544 B each, payloads at byte 160) and the flat index
   const uint8_t* leaves;
   const int32_t* leafIndex;
@@ -603,6 +605,34 @@ R2_HD float sggx_sample_p(const Sggx& g, float ior, V3 wo, V3* wi, RngStream& rn
   const float c2 = rng.next();
   *wi = normalize(to_world(fr, cosine_sample_hemisphere(c1, c2)));
   return (float)((double)fmaxf(dot(*wi, wn), 0.0f) / kPiD);
+}
+
+// ---------------------------------------------------------------- Henyey-Greenstein
+// (include/medium/henyey_greenstein_phase_function.hpp:22-50, coordinateSystem
+// and sphericalDirection of include/utility/functions.hpp:29-47); the media of
+// scene objects with a "G" key use it instead of the SGGX lobes.
+R2_HD float phase_hg(float cosTheta, float g) {
+  const float denom = 1.0f + g * g + 2.0f * g * cosTheta;
+  return (float)((double)(1.0f - g * g) / (4.0 * kPiD * (double)denom * (double)sqrtf(denom)));
+}
+R2_HD float hg_sample_p(float g, V3 wo, V3* wi, RngStream& rng) {
+  const float u1 = rng.next();
+  const float u2 = rng.next();
+  float cosTheta;
+  if (fabsf(g) < 1e-3f) {
+    cosTheta = 1.0f - 2.0f * u1;
+  } else {
+    const float sq = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+    cosTheta = (1.0f + g * g - sq * sq) / (2.0f * g);
+  }
+  const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+  float s, c;
+  sincos_turns(u2, &s, &c);  // phi = 2 pi u2
+  const V3 v1 = fabsf(wo.x) > fabsf(wo.y) ? v3(-wo.z, 0.0f, wo.x) / sqrtf(wo.x * wo.x + wo.z * wo.z)
+                                          : v3(0.0f, wo.z, -wo.y) / sqrtf(wo.y * wo.y + wo.z * wo.z);
+  const V3 v2 = cross(wo, v1);
+  *wi = v1 * (sinTheta * c) + v2 * (sinTheta * s) + (-wo) * cosTheta;
+  return phase_hg(-cosTheta, g);
 }
 
 }  // namespace r2

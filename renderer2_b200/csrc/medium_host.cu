@@ -27,10 +27,12 @@ float voxel_size_from_path(const std::string& path) {
 static M4 affine(const M4& a) { return m43_to_m4(m4_to_m43(a)); }
 
 std::unique_ptr<MediumHost> load_medium(const std::string& path, const float sigmaA[3], const float sigmaS[3],
-                                        V3 pos, V3 orientation, V3 scaling) {
+                                        V3 pos, V3 orientation, V3 scaling, bool hg, float hgG) {
   std::unique_ptr<MediumHost> mh(new MediumHost());
   MediumView& v = mh->view;
   memset(&v, 0, sizeof(v));
+  v.hg = hg ? 1 : 0;
+  v.g = hgG;
   const std::vector<uint8_t> g = nvdb::read_file(path + ".nvdb");
   const nvdb::GridData* G = nvdb::grid_data(g.data());
   const nvdb::TreeData* T = nvdb::tree_data(g.data());

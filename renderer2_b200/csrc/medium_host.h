@@ -31,8 +31,10 @@ struct MediumHost {
 };
 
 // Loads <path>.nvdb and <path>.brickgrid for a medium placed with
-// T(pos) R(orientation) S(scaling).
+// T(pos) R(orientation) S(scaling); hg selects the Henyey-Greenstein phase
+// function with asymmetry g (CNVDBMedium(path, sigma_a, sigma_s, g),
+// nvdb_medium.cu:27-43) instead of the SGGX one (45-61).
 std::unique_ptr<MediumHost> load_medium(const std::string& path, const float sigmaA[3], const float sigmaS[3],
-                                        V3 pos, V3 orientation, V3 scaling);
+                                        V3 pos, V3 orientation, V3 scaling, bool hg = false, float g = 0.0f);
 
 }  // namespace r2

@@ -398,7 +398,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
     if (lpdf > 0.0f) {
       ldir = normalize(ldir);
       const Ray lr = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, ldir, kDefaultTmax), n));
-      const float sp = sggx_p(g, ior, wo, ldir, rs);
+      const float sp = M.hg ? phase_hg(dot(wo, ldir), M.g) : sggx_p(g, ior, wo, ldir, rs);
       const float mis = balance_heuristic(lpdf, sp);
       shO0 = f4(lr.o, lpdf);
       shD0 = f4(lr.d, 0.0f);
@@ -408,7 +408,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   }
   {
     V3 wi = v3(0.0f);
-    const float sp = sggx_sample_p(g, ior, wo, &wi, rs);
+    const float sp = M.hg ? hg_sample_p(M.g, wo, &wi, rs) : sggx_sample_p(g, ior, wo, &wi, rs);
     if (sp > 0.0f) {
       wi = normalize(wi);
       const Ray br = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, wi, kDefaultTmax), n));
@@ -429,7 +429,8 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   L.st.shPre[2 * i + 1] = pre1;
   L.st.shT[i] = f4(T, 0.0f);
   V3 wi = v3(0.0f);
-  sggx_sample_p(g, ior, wo, &wi, rs);
+  if (M.hg) hg_sample_p(M.g, wo, &wi, rs);
+  else sggx_sample_p(g, ior, wo, &wi, rs);
   const Ray cr = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, normalize(wi), kDefaultTmax), wi));
   V3 Tn = T;
   if (L.bounce > 3) {

@@ -110,7 +110,9 @@ void RenderScene::add_mesh(const float* pos, uint32_t nverts, const uint32_t* id
                            const r2_material& mat, const float* m2w, uint32_t mask) {
   R2_REQUIRE(pos && idx && nrm && m2w, R2_ERR_INVALID_ARGUMENT, "null mesh array");
   R2_REQUIRE(nverts > 0 && ntris > 0, R2_ERR_INVALID_ARGUMENT, "empty mesh");
-  (void)mask;  // rendering traces every object (visibility mask 255)
+  // render rays carry visibility mask 255 (device_scene.hpp:17): every object
+  // with a nonzero mask is visible, FILTER-only ones included
+  if (mask == 0) return;
   M43 M = m43_from_floats(m2w);
   uint32_t base = (uint32_t)(hPos_.size() / 3);
   uint32_t matId = (uint32_t)hMats_.size();
@@ -134,7 +136,7 @@ void RenderScene::add_mesh(const float* pos, uint32_t nverts, const uint32_t* id
 void RenderScene::add_shape(int type, const float* center, float radius, const float* normal, const r2_material& mat,
                             uint32_t mask) {
   R2_REQUIRE(type == kShapeSphere || type == kShapeCircle, R2_ERR_INVALID_ARGUMENT, "unknown shape type");
-  (void)mask;
+  if (mask == 0) return;
   Shape s;
   memset(&s, 0, sizeof(s));
   s.type = type;
@@ -154,13 +156,14 @@ void RenderScene::set_envmap(const float* rgb, int W, int H) {
 }
 
 void RenderScene::add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
-                             const float* orientation, const float* scaling, uint32_t mask) {
+                             const float* orientation, const float* scaling, uint32_t mask, bool hg, float g) {
   R2_REQUIRE(path && sigmaA && sigmaS && pos && orientation && scaling, R2_ERR_INVALID_ARGUMENT, "null medium argument");
   R2_REQUIRE(media_.size() < 4096, R2_ERR_UNSUPPORTED, "too many media in one scene");
-  (void)mask;
-  media_.push_back(load_medium(path, sigmaA, sigmaS, v3(pos[0], pos[1], pos[2]),
-                               v3(orientation[0], orientation[1], orientation[2]),
-                               v3(scaling[0], scaling[1], scaling[2])));
+  std::unique_ptr<MediumHost> m = load_medium(path, sigmaA, sigmaS, v3(pos[0], pos[1], pos[2]),
+                                              v3(orientation[0], orientation[1], orientation[2]),
+                                              v3(scaling[0], scaling[1], scaling[2]), hg, g);
+  if (mask == 0) return;  // render rays (mask 255) never see objects with mask NONE
+  media_.push_back(std::move(m));
   committed_ = false;
 }
 

@@ -39,7 +39,7 @@ class RenderScene {
   void set_envmap(const float* rgb, int W, int H);
   // Medium of a filtered LOD: <path>.nvdb + <path>.brickgrid placed with T(pos) R(orientation) S(scaling).
   void add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
-                  const float* orientation, const float* scaling, uint32_t mask);
+                  const float* orientation, const float* scaling, uint32_t mask, bool hg = false, float g = 0.0f);
   void commit();
   // One frame: `spp` waves accumulated into d_frame (W*H*3 floats, cleared here).
   void render(const r2_camera& cam, const r2_render_params& p, float* d_frame, cudaStream_t s, double* stats);

@@ -78,10 +78,17 @@ class Scene:
         N.check(N.lib.r2_scene_add_shape(self.handle, int(kind), N.ptr(c), float(radius), N.ptr(n), C.byref(material),
                                          mask))
 
-    def add_medium(self, path, sigma_a, sigma_s, pos=(0, 0, 0), orientation=(0, 1, 0), scaling=(1, 1, 1), mask=255):
-        """Medium "Path" of scenedescription.json: loads <path>.nvdb and <path>.brickgrid."""
+    def add_medium(self, path, sigma_a, sigma_s, pos=(0, 0, 0), orientation=(0, 1, 0), scaling=(1, 1, 1), mask=255,
+                   g=None):
+        """Medium "Path" of scenedescription.json: loads <path>.nvdb and <path>.brickgrid.
+        g (the "G" key) selects the Henyey-Greenstein phase function."""
         arrs = [np.ascontiguousarray(v, np.float32) for v in (sigma_a, sigma_s, pos, orientation, scaling)]
-        N.check(N.lib.r2_scene_add_medium(self.handle, str(path).encode(), *[N.ptr(a) for a in arrs], mask))
+        p = [N.ptr(a) for a in arrs]
+        if g is None:
+            N.check(N.lib.r2_scene_add_medium(self.handle, str(path).encode(), *p, mask))
+        else:
+            N.check(N.lib.r2_scene_add_medium_hg(self.handle, str(path).encode(), p[0], p[1], float(g), p[2], p[3],
+                                                 p[4], mask))
 
     def set_envmap(self, rgb: np.ndarray):
         rgb = np.ascontiguousarray(rgb, np.float32)

@@ -59,8 +59,10 @@ def build_scene(desc) -> R.Scene:
         sc.add_mesh(mesh, mat, m2w)
     for kind, c, r, n, mat in desc.get("shapes", []):
         sc.add_shape(kind, c, r, n, mat)
-    for path, sa, ss, pos, ori, scl in desc.get("media", []):
-        sc.add_medium(path, sa, ss, pos, ori, scl)
+    for med in desc.get("media", []):
+        path, sa, ss, pos, ori, scl = med[:6]
+        g = med[6] if len(med) > 6 else None
+        sc.add_medium(path, sa, ss, pos, ori, scl, g=g)
     sc.set_envmap(desc["env"])
     sc.commit()
     return sc

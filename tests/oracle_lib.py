@@ -163,7 +163,7 @@ class OCamera(C.Structure):
 
 class OMedium(C.Structure):
     _fields_ = [("path", C.c_char_p), ("sigma_a", C.c_float * 3), ("sigma_s", C.c_float * 3), ("pos", C.c_float * 3),
-                ("orientation", C.c_float * 3), ("scaling", C.c_float * 3)]
+                ("orientation", C.c_float * 3), ("scaling", C.c_float * 3), ("hg", C.c_int), ("g", C.c_float)]
 
 
 lib.orc_render.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
@@ -182,7 +182,11 @@ def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want
     Returns rgb (n, 3) [, var (n, 3)] for pixels [p0, p1)."""
     keep = []
     media = (OMedium * max(1, len(scene_desc.get("media", []))))()
-    for i, (path, sa, ss, pos, ori, sc) in enumerate(scene_desc.get("media", [])):
+    for i, med in enumerate(scene_desc.get("media", [])):
+        path, sa, ss, pos, ori, sc = med[:6]
+        if len(med) > 6 and med[6] is not None:  # Henyey-Greenstein asymmetry g
+            media[i].hg = 1
+            media[i].g = float(med[6])
         pb = str(path).encode()
         keep.append(pb)
         media[i].path = pb
@@ -224,3 +228,16 @@ def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want
                        len(scene_desc.get("media", [])), flags)
     assert r == 0, f"oracle render failed ({r})"
     return (rgb, var) if want_var else rgb
+
+
+lib.orc_tonemap.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]
+lib.orc_tonemap.restype = None
+
+
+def tonemap(linear, gamma):
+    """Oracle output stage: (tonemapped floats, bytes) of an (H, W, 3) frame."""
+    lin = np.ascontiguousarray(linear, np.float32)
+    out = np.zeros_like(lin)
+    by = np.zeros(lin.shape, np.uint8)
+    lib.orc_tonemap(lin.ctypes.data, lin.shape[1], lin.shape[0], float(gamma), out.ctypes.data, by.ctypes.data)
+    return out, by

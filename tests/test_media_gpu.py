@@ -90,6 +90,18 @@ def test_medium_instance_transform_and_coarse_lod_match_oracle(lods):
         assert frac >= PIX_FRAC, f"dda={dda}: only {frac:.4f} of pixels agree"
 
 
+@pytest.mark.parametrize("g", [0.0, 0.45, -0.6])
+def test_medium_henyey_greenstein_matches_oracle(lods, g):
+    # a Medium with a "G" key: Henyey-Greenstein phase function, SGGX payload albedo
+    desc = _desc(lods[0])
+    desc["media"] = [desc["media"][0] + (g,)]
+    cam = R.camera(32, 32, 50.0, (0.3, 0.6, 3.2), (0.0, 0.0, 0.0), (0, 1, 0))
+    gi = _gpu(desc, cam, 3, 6, 21, True)
+    o = O.render(desc, cam, 3, 6, 21, flags=1)
+    frac = _agree(gi, o)
+    assert frac >= PIX_FRAC, f"g={g}: only {frac:.4f} of pixels agree"
+
+
 def test_medium_three_sigma_against_high_spp_oracle(lods):
     desc = _desc(lods[0], ground=False)
     cam = R.camera(16, 16, 45.0, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0, 1, 0))
