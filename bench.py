@@ -46,6 +46,14 @@ FILTER_CFG = dict(n_quads=500_000, n_branches=20, clustered=0.7, seed=4, grid=25
 EXTEND_BYTES_PER_SEGMENT = 52.0
 SHADOW_BYTES_PER_SLOT = 33.0
 FILTER_BYTES_PER_VOXEL = 36.0
+# media scenes:
+#   k_extend_media: queue id 4 + ray in/out 64 + throughput in/out 32 + hit record 16 = 116 B per segment
+#   k_shadow<true>: record origin 16 + direction 16 + tmax/medium 8 + queue id 4 + transmittance 4 = 48 B per slot
+#   k_shade<true>: hit 16 + ray 32 + throughput 16 + radiance 16 + 2 records x 64 + continuation 48 = 256 B per segment
+VOLUME_EXTEND_BYTES_PER_SEGMENT = 116.0
+SHADOW_MEDIA_BYTES_PER_SLOT = 48.0
+SHADE_BYTES_PER_SEGMENT = 256.0
+VOLUME_CFG = dict(grid=256, n_quads=200_000, ico_subdiv=6, width=1920, height=1080, spp=16, depth=16, seed=0)
 
 
 def _peaks():
@@ -185,7 +193,7 @@ def cpu_render_sample(desc, cam, prm, budget_s=15.0, threads=0):
     while True:
         p0, p1 = row * W, min((row + rows) * W, W * H)
         t0 = time.perf_counter()
-        O.render(desc, cam, prm.spp, prm.max_depth, prm.seed, p0, p1, threads=cores)
+        O.render(desc, cam, prm.spp, prm.max_depth, prm.seed, p0, p1, threads=cores, flags=prm.flags)
         t_work += time.perf_counter() - t0
         done += (p1 - p0)
         row += rows
@@ -366,6 +374,86 @@ def bench_filter(args, world, local):
             "gpu_launches": 2 * args.steps, "_mesh": (mesh, mat, prm, vs)}
 
 
+def bench_volume(args, world, local):
+    """Config 4 leg: one batched-volume scene (filtered 256^3 foliage medium +
+    81,920-tri mesh), 1920x1080, depth 16, brick-grid DDA tracking."""
+    import tempfile
+
+    import torch
+    from renderer2_b200 import raytracer as R
+    from renderer2_b200 import render_scenes as RS
+    c = VOLUME_CFG
+    work = tempfile.mkdtemp(prefix="r2vol")
+    desc, cam = RS.volume_scene(work, 0, grid=c["grid"], n_quads=c["n_quads"], ico_subdiv=c["ico_subdiv"],
+                                width=c["width"], height=c["height"])
+    prm = R.params(c["spp"], c["depth"], c["seed"], brick_grid=True)
+    sc = RS.build_scene(desc)
+    npix = cam.width * cam.height
+    frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup):
+        sc.render_device(cam, prm, frame.data_ptr(), stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    st = np.zeros(8)
+    stats = []
+    ev0.record()
+    for _ in range(args.steps):
+        # wave state (~1 GB at 1080p) and grid leaves exceed L2; no flush needed
+        sc.render_device(cam, prm, frame.data_ptr(), stream, stats=st)
+        stats.append(st.copy())
+    ev1.record()
+    torch.cuda.synchronize()
+    _barrier(world)
+    total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
+    paths = npix * prm.spp
+    st = np.mean(np.array(stats), axis=0)
+    seg, shadow = st[2], st[3]
+    ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
+    seg_wave = seg / prm.spp
+    dom = max(("extend", "shadow", "shade"), key=lambda k: ms_wave[k])
+    per_unit = {"extend": (VOLUME_EXTEND_BYTES_PER_SEGMENT, seg_wave, "k_extend_media"),
+                "shadow": (SHADOW_MEDIA_BYTES_PER_SLOT, 2.0 * seg_wave, "k_shadow<true>"),
+                "shade": (SHADE_BYTES_PER_SEGMENT, seg_wave, "k_shade<true>")}[dom]
+    alg = per_unit[0] * per_unit[1]
+    kms = ms_wave[dom]
+    peak, peak_kind = _peaks()
+    achieved = alg / (kms / 1e3) / 1e9
+    tr = _traffic(per_unit[2])
+    launches = prm.max_depth
+    roofline = {"bound": "hbm", "kernel": per_unit[2], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": tr["bytes_per_unit"] * per_unit[1] / launches if tr else None,
+                "alg_bytes_per_launch": alg / launches, "avg_launch_ms": kms / launches,
+                "note": "delta/ratio tracking is latency bound on dependent grid lookups",
+                "kernel_ms_per_wave": ms_wave}
+    h2d = _input_bytes(desc) + sum(os.path.getsize(m[0] + e) for m in desc["media"] for e in (".nvdb", ".brickgrid"))
+    e2e_ms = []
+    for _ in range(1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = RS.build_scene(desc)
+        s2.render(cam, prm)
+        s2.close()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    sc.close()
+    out = {"metric": "paths/s", "value": world * paths * args.steps / (total_ms / 1e3), "unit": "paths/s",
+           "ms_per_step": total_ms / args.steps,
+           "config": {"workload": f"batched volume scene 0: foliage {c['n_quads']} quads filtered to "
+                                  f"{c['grid']}^3 (SGGX medium, brick-grid DDA) + {20 * 4 ** c['ico_subdiv']}-tri "
+                                  f"mesh, {c['width']}x{c['height']}, {c['spp']} spp per step, depth {c['depth']}",
+                      "paths_per_step": paths, "segments_per_step": seg, "shadow_rays_per_step": shadow,
+                      "l2": "wave state larger than L2"},
+           "roofline": roofline,
+           "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
+                   "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms},
+           "gpu_launches": prm.spp * (2 + 4 * prm.max_depth) * args.steps}
+    return out, (desc, cam, prm)
+
+
 def run_native(args):
     import torch
     world, rank, local = _dist_setup()
@@ -393,6 +481,7 @@ def run_native(args):
         return
     r = bench_render(args, world, local)
     f = bench_filter(args, world, local) if not args.skip_filter else None
+    vol = bench_volume(args, world, local) if not args.skip_volume else None
     if rank == 0:
         cpu = cpu_render_sample(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
         line = {"metric": "paths/s", "value": r["value"], "unit": "paths/s", "n_gpus": world, "steps": args.steps,
@@ -411,6 +500,12 @@ def run_native(args):
                 f["cpu_baseline"] = cpu_filter_sample(mesh, mat, prm, vs, budget_s=args.cpu_budget)
             line["filter"] = f
             line["gpu_launches"] += f["gpu_launches"]
+        if vol is not None:
+            v, (vdesc, vcam, vprm) = vol
+            if world == 1:
+                v["cpu_baseline"] = cpu_render_sample(vdesc, vcam, vprm, budget_s=max(5.0, args.cpu_budget / 2))
+            line["volume"] = v
+            line["gpu_launches"] += v["gpu_launches"]
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -472,6 +567,20 @@ def run_case(args):
         torch.cuda.synchronize()
         sc.close()
         print(json.dumps({"case": args.case, "voxels": st[0], "candidates": st[1], "ms": st[2]}))
+    elif args.case == "volume-small":
+        import tempfile
+
+        from renderer2_b200 import raytracer as R
+        from renderer2_b200 import render_scenes as RS
+        desc, cam = RS.volume_scene(tempfile.mkdtemp(prefix="r2vol"), 0, grid=128, n_quads=50_000, ico_subdiv=4,
+                                    width=480, height=270)
+        sc = RS.build_scene(desc)
+        frame = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
+        st = sc.render_device(cam, R.params(2, 16, 0, brick_grid=True), frame.data_ptr())
+        torch.cuda.synchronize()
+        sc.close()
+        print(json.dumps({"case": args.case, "paths": st[0], "ms": st[1], "extend_ms": st[4], "shade_ms": st[5],
+                          "shadow_ms": st[6]}))
     else:
         raise SystemExit(f"unknown case {args.case}")
 
@@ -484,6 +593,7 @@ def main():
     ap.add_argument("--impl", default="native", choices=["native", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--skip-filter", action="store_true")
+    ap.add_argument("--skip-volume", action="store_true")
     ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
     ap.add_argument("--case", default=None, help="profiling case: render-small | filter-small")
     args = ap.parse_args()

@@ -53,6 +53,35 @@ def c2_scene():
     return desc, cam
 
 
+def volume_scene(work_dir, index: int = 0, grid: int = 256, n_quads: int = 200_000, ico_subdiv: int = 6,
+                 width: int = 1920, height: int = 1080, filter_spv: int = 64, filter_iters: int = 10):
+    """Config 4 scene `index` (seed 5 + index): a foliage grid filtered on the GPU
+    (LOD 0 NanoVDB + brick grid written under work_dir, grid^3 voxels) as an
+    SGGX medium scaled to a 4-unit cube, a displaced icosphere (20 * 4^ico_subdiv
+    triangles) beside it, a ground disc and a lognormal(0, 1.5) environment;
+    1920x1080 camera, fov 60.  sigma_s = 10 (the filter's SigmaT), sigma_a = 0."""
+    seed = 5 + index
+    leaves = scenes.foliage(n_quads, 20, 0.7, seed)
+    mat = F.material(diffuse=(0.15, 0.55, 0.1), specular=(0.05, 0.05, 0.05), alpha=0.45, ior=1.5)
+    prm = F.params(samples_per_voxel=filter_spv, iterations=filter_iters,
+                   min_voxel_size=scenes.voxel_size_for(leaves, grid), lods=1)
+    paths, _ = F.run_filtering(leaves, mat, prm, work_dir, f"foliage{index}")
+    ico = scenes.icosphere(ico_subdiv, 0.08, seed)
+    m2w = np.zeros(12, np.float32)
+    m2w[0] = m2w[4] = m2w[8] = 1.5
+    m2w[9:12] = (6.5, 1.5, 2.0)
+    desc = {
+        "meshes": [(ico, F.material(diffuse=(0.7, 0.6, 0.5), specular=(1, 1, 1), alpha=0.25, ior=1.5), m2w)],
+        "shapes": [(R.CIRCLE, (0.0, -0.01, 0.0), 1000.0, (0, 1, 0),
+                    F.material(diffuse=(0.4, 0.35, 0.3), specular=(0.2, 0.2, 0.2), alpha=0.8, ior=1.3,
+                               diffuse_roughness=0.5))],
+        "media": [(paths[0], (0.0, 0.0, 0.0), (10.0, 10.0, 10.0), (0.0, 0.0, 0.0), (0.0, 1.0, 0.0), (4.0, 4.0, 4.0))],
+        "env": lognormal_env(512, 256, 1.5, seed),
+    }
+    cam = R.camera(width, height, 60.0, (3.0, 3.0, 13.0), (3.5, 1.8, 2.0), (0, 1, 0))
+    return desc, cam
+
+
 def build_scene(desc) -> R.Scene:
     sc = R.Scene()
     for mesh, mat, m2w in desc.get("meshes", []):
