@@ -163,6 +163,41 @@ R2_HD FData medium_filtered(const MediumView& m, V3 p) {
   return fdata_lerp(d.z, d0, d1);
 }
 
+// Density at p alone: the density term of medium_filtered with the same
+// operations (4-byte loads instead of 32-byte payloads).
+R2_HD float voxel_density(const MediumView& m, int x, int y, int z) {
+  const int bx = (x - m.leafOrigin[0]) >> 3, by = (y - m.leafOrigin[1]) >> 3, bz = (z - m.leafOrigin[2]) >> 3;
+  if (x >= m.leafOrigin[0] && y >= m.leafOrigin[1] && z >= m.leafOrigin[2] && bx < m.L[0] && by < m.L[1] &&
+      bz < m.L[2]) {
+    const int li = m.leafIndex[(size_t)bx + (size_t)by * m.L[0] + (size_t)bz * m.L[0] * m.L[1]];
+    if (li >= 0) {
+      const size_t off = (size_t)li * 16544 + 160 + (size_t)(((x & 7) << 6) | ((y & 7) << 3) | (z & 7)) * 32;
+#if defined(__CUDA_ARCH__)
+      return __ldg(reinterpret_cast<const float*>(m.leaves + off));
+#else
+      float v;
+      memcpy(&v, m.leaves + off, 4);
+      return v;
+#endif
+    }
+  }
+  return 0.0f;
+}
+R2_HD float medium_density(const MediumView& m, V3 p) {
+  const V3 ps = v3(p.x * (float)m.size[0] + (float)m.ibbMin[0] - 0.5f, p.y * (float)m.size[1] + (float)m.ibbMin[1] - 0.5f,
+                   p.z * (float)m.size[2] + (float)m.ibbMin[2] - 0.5f);
+  const int ix = (int)floorf(ps.x), iy = (int)floorf(ps.y), iz = (int)floorf(ps.z);
+  const float dx = ps.x - (float)ix, dy = ps.y - (float)iy, dz = ps.z - (float)iz;
+  const float ux = 1.0f - dx, uy = 1.0f - dy, uz = 1.0f - dz;
+  const float d00 = ux * voxel_density(m, ix, iy, iz) + dx * voxel_density(m, ix + 1, iy, iz);
+  const float d10 = ux * voxel_density(m, ix, iy + 1, iz) + dx * voxel_density(m, ix + 1, iy + 1, iz);
+  const float d01 = ux * voxel_density(m, ix, iy, iz + 1) + dx * voxel_density(m, ix + 1, iy, iz + 1);
+  const float d11 = ux * voxel_density(m, ix, iy + 1, iz + 1) + dx * voxel_density(m, ix + 1, iy + 1, iz + 1);
+  const float d0 = uy * d00 + dy * d10;
+  const float d1 = uy * d01 + dy * d11;
+  return uz * d0 + dz * d1;
+}
+
 // ---------------------------------------------------------------- rays (ray.hpp:41-91)
 struct Ray {
   V3 o, d;
@@ -310,8 +345,9 @@ R2_HD V3 medium_sample_internal(const MediumView& m, const Ray& rayModel, RngStr
   for (int it = 0; it < kMaxTrackingSteps; ++it) {
     t -= log_r2(1.0f - rng.next()) * invMax / m.sigmaT;
     if (t >= ray.tmax) return v3(1.0f);
-    const FData fd = medium_filtered(m, ray.o + ray.d * t);
-    if (m.filterRenderRatio * fd.density * invMax > rng.next()) {
+    const V3 pt = ray.o + ray.d * t;
+    if (m.filterRenderRatio * medium_density(m, pt) * invMax > rng.next()) {
+      const FData fd = medium_filtered(m, pt);
       ray.tmax = t;
       const Ray w = ray_transform2(ray, m.indexToModel);
       fill_event(ev, w, fd);
@@ -374,7 +410,7 @@ R2_HD float medium_tr_internal(const MediumView& m, const Ray& rayModel, RngStre
   for (int it = 0; it < kMaxTrackingSteps; ++it) {
     t -= log_r2(1.0f - rng.next()) * invMax / m.sigmaT;
     if (t >= ray.tmax) return tr;
-    const float d = medium_filtered(m, ray.o + ray.d * t).density;
+    const float d = medium_density(m, ray.o + ray.d * t);
     tr *= 1.0f - fmaxf(0.0f, m.filterRenderRatio * d * invMax);
     if (tr < 1.0f) {
       const float p = 1.0f - tr;
@@ -605,6 +641,129 @@ R2_HD float sggx_sample_p(const Sggx& g, float ior, V3 wo, V3* wi, RngStream& rn
   const float c2 = rng.next();
   *wi = normalize(to_world(fr, cosine_sample_hemisphere(c1, c2)));
   return (float)((double)fmaxf(dot(*wi, wn), 0.0f) / kPiD);
+}
+
+// ---------------------------------------------------------------- resumable tracking
+// The four tracking loops above, cut into single steps so that a warp can
+// interleave many segments of different lengths (a lane whose segment ends
+// takes the next one from a queue).  Each step is one loop iteration of the
+// corresponding function with the same operations and random draws, so a
+// segment tracked step by step gives the same result as the loop.
+enum TrackStatus : int { kTrackRunning = 0, kTrackDone = 1, kTrackCollide = 2, kTrackError = 3 };
+
+struct TrackState {
+  V3 o, d, ri;  // ray in the tracking space (unit box, or scaled index box for the DDA), 1/d
+  float tmax, t, tau, mip, tr, invMax;
+  int steps;
+  RngStream rng;
+};
+
+// Start of sampleInternal / sampleDDA (kSample) or trInternal / trDDA for a
+// world-space ray through the instance.
+template <bool kDDA, bool kSample>
+R2_HD int track_init(const MediumView& m, const Ray& rayWorld, TrackState* s) {
+  const Ray rm = ray_transform2(rayWorld, m.worldToModel);
+  s->t = 0.0f;
+  s->tr = 1.0f;
+  s->steps = 0;
+  if (kDDA) {
+    const Ray iray = ray_transform2(rm, m.unitToScaled);
+    s->o = iray.o;
+    s->d = iray.d;
+    s->tmax = iray.tmax;
+    s->ri = v3(1.0f / iray.d.x, 1.0f / iray.d.y, 1.0f / iray.d.z);
+    if (!kSample) s->invMax = 1.0f / inv_majorant(m);  // the volume majorant of trDDA
+    s->tau = -log_r2(1.0f - s->rng.next());
+    s->mip = 3.0f;
+  } else {
+    const Ray ray = ray_transform2(rm, m.modelToIndex);
+    s->o = ray.o;
+    s->d = ray.d;
+    s->tmax = ray.tmax;
+    s->invMax = inv_majorant(m);
+    if (!(s->invMax < INFINITY)) return kTrackDone;
+  }
+  return kTrackRunning;
+}
+
+// One iteration.  kSample: kTrackCollide fills ev (world space) and albedo.
+// Transmittance: kTrackDone leaves the estimate in s.tr.
+template <bool kDDA, bool kSample>
+R2_HD int track_step(const MediumView& m, TrackState& s, MediumEvent* ev, V3* albedo) {
+  if (s.steps >= kMaxTrackingSteps) return kTrackError;
+  ++s.steps;
+  if (kDDA) {
+    if (!(s.t < s.tmax)) return kTrackDone;
+    const V3 curr = s.o + s.d * s.t;
+    const int mi = (int)roundf(s.mip);
+    const float majorant = m.filterRenderRatio * brick_majorant(m, curr, mi);
+    const float dt = step_dda(curr, s.ri, mi);
+    const float prevT = s.t;
+    s.t += dt / m.sigmaT;
+    if (s.t == prevT) return kTrackDone;
+    s.tau -= majorant * dt;
+    s.mip = fminf(s.mip + 0.25f, 3.0f);
+    if (s.tau > 0.0f) return kTrackRunning;
+    s.t += s.tau / (majorant * m.sigmaT);
+    if (s.t >= s.tmax) return kTrackDone;
+    const float jx = s.rng.next();
+    const float jy = s.rng.next();
+    const float jz = s.rng.next();
+    const float d = brick_density(m, s.o + s.d * s.t + v3(jx, jy, jz) - v3(0.5f));
+    if (s.rng.next() * majorant < d * m.filterRenderRatio) {
+      if (kSample) {
+        const V3 ip = s.o + s.d * s.t;
+        const V3 pos = v3((ip.x - (float)m.ibbMin[0]) / (float)m.size[0], (ip.y - (float)m.ibbMin[1]) / (float)m.size[1],
+                          (ip.z - (float)m.ibbMin[2]) / (float)m.size[2]);
+        const FData fd = medium_filtered(m, pos);
+        const Ray w = ray_transform2(make_ray(s.o, s.d, s.t), m.scaledToModel);
+        fill_event(ev, w, fd);
+        *albedo = scatter_albedo(m, fd, w.d);
+        ev->pos = xform_point(m.modelToWorld, ev->pos);
+        ev->normal = normalize(xform_vector(m.modelToWorld, ev->normal));
+        return kTrackCollide;
+      }
+      s.tr *= fmaxf(0.0f, 1.0f - s.invMax / majorant);
+      if (s.tr < 0.1f) {
+        const float prob = 1.0f - s.tr;
+        if (s.rng.next() < prob) {
+          s.tr = 0.0f;
+          return kTrackDone;
+        }
+        s.tr /= 1.0f - prob;
+      }
+    }
+    s.tau = -log_r2(1.0f - s.rng.next());
+    s.mip = fmaxf(0.0f, s.mip - 2.0f);
+    return kTrackRunning;
+  } else {
+    s.t -= log_r2(1.0f - s.rng.next()) * s.invMax / m.sigmaT;
+    if (s.t >= s.tmax) return kTrackDone;
+    const V3 pt = s.o + s.d * s.t;
+    const float dens = medium_density(m, pt);
+    if (kSample) {
+      if (m.filterRenderRatio * dens * s.invMax > s.rng.next()) {
+        const FData fd = medium_filtered(m, pt);
+        const Ray w = ray_transform2(make_ray(s.o, s.d, s.t), m.indexToModel);
+        fill_event(ev, w, fd);
+        *albedo = scatter_albedo(m, fd, w.d);
+        ev->pos = xform_point(m.modelToWorld, ev->pos);
+        ev->normal = normalize(xform_vector(m.modelToWorld, ev->normal));
+        return kTrackCollide;
+      }
+      return kTrackRunning;
+    }
+    s.tr *= 1.0f - fmaxf(0.0f, m.filterRenderRatio * dens * s.invMax);
+    if (s.tr < 1.0f) {
+      const float p = 1.0f - s.tr;
+      if (s.rng.next() < p) {
+        s.tr = 0.0f;
+        return kTrackDone;
+      }
+      s.tr /= 1.0f - p;
+    }
+    return kTrackRunning;
+  }
 }
 
 // ---------------------------------------------------------------- Henyey-Greenstein

@@ -22,6 +22,8 @@
 // wave is a fixed launch sequence (graph-capturable, no host round trips).
 // Random numbers: Philox4x32-10 keyed by (pixel, seed), counter (sample,
 // bounce, block, purpose) — independent of queue position and batching.
+#include <algorithm>
+
 #include "render.cuh"
 
 namespace r2 {
@@ -32,7 +34,14 @@ constexpr uint32_t kPurposeMedium = 0x10u;     // + pass-through index within th
 constexpr uint32_t kPurposeScatter = 0x100u;   // phase-function and light draws at a collision
 constexpr uint32_t kPurposeShadowTr = 0x200u;  // + shadow slot (0 light, 1 BSDF)
 constexpr int kMaxPassThrough = 64;            // medium boundaries crossed within one bounce
-constexpr int kMaxShadowSegments = 256;        // medium boundaries along one shadow ray
+constexpr int kMaxShadowSegments = 256;        // medium boundaries along one shadow ray (per round)
+constexpr int kMediaRounds = 2;                // queued tracking rounds per bounce before the inline round
+constexpr int kTrackSteps = 8;                 // tracking steps a lane takes between refills
+// Media counters of a bounce (PathState::mc): [3r] segments queued in round r,
+// [3r+1] segments taken, [3r+2] entries of list r + 1; path extension at 0,
+// shadows at kShadowCounters.
+constexpr int kCountersPerBounce = 16;
+constexpr int kShadowCounters = 6;
 
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
@@ -115,42 +124,6 @@ __device__ __forceinline__ bool scene_occluded(const SceneView& S, V3 o, V3 d, f
   return false;
 }
 
-// CDeviceScene::intersectTr seen from direct(): the result is 0 when the walk
-// ends on a surface (materials do not emit), else the product of the media's
-// ratio-tracking estimates.  A surface anywhere on the ray ends the walk
-// there, so the any-hit test decides that case; without one the walk visits
-// only medium boxes, segment by segment through CRay::spawnRay towards the
-// fixed far point p1, multiplying Tr when a segment leaves the current medium.
-__device__ float shadow_transmittance(const SceneView& S, V3 o, V3 d, float tmax, int med, bool dda, RngStream& rng,
-                                      int* err) {
-  if (scene_occluded(S, o, d, tmax)) return 0.0f;
-  float tr = 1.0f;
-  if (S.nmedia == 0) return tr;
-  V3 p0 = o;
-  const V3 p1 = o + d * tmax;
-  int cur = med;
-  for (int k = 0; k < kMaxShadowSegments; ++k) {
-    const V3 off = offset_ray_origin(p0, normalize(p1 - p0));
-    const float tl = length(p1 - off);
-    const V3 dir = (p1 - p0) / tl;
-    float best = tl;
-    int hitM = -1;
-    for (int m = 0; m < S.nmedia; ++m) {
-      const float tm = medium_box_hit(S.media[m], off, dir);
-      if (tm >= 0.0f && tm <= tl && tm < best) {
-        best = tm;
-        hitM = m;
-      }
-    }
-    if (hitM < 0) return tr;
-    if (cur >= 0 && hitM == cur) tr *= instance_tr(S.media[cur], make_ray(off, dir, best), dda, rng, err);
-    p0 = off + dir * best;
-    cur = cur < 0 ? hitM : -1;
-  }
-  *err = 1;
-  return 0.0f;
-}
-
 __device__ __forceinline__ uint32_t push_queue(uint32_t* q, uint32_t* count, bool pred, uint32_t value) {
   const unsigned full = __activemask();
   const unsigned m = __ballot_sync(full, pred);
@@ -191,87 +164,260 @@ __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
   }
 }
 
+// ------------------------------------------------------------------ media: path extension
 // The medium part of Li (path_integrator_impl.hpp:127-192) up to the event
 // that the bounce shades: a surface hit, a medium collision, a miss, or the
-// end of the path by a medium rule.
-__global__ void __launch_bounds__(128) k_extend_media(RenderLaunch L) {
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = L.st.q[L.bounce & 1];
-  const uint32_t stride = gridDim.x * blockDim.x;
+// end of the path by a medium rule; material-less medium hits are passed
+// through without counting a bounce (the reference's `--bounces; continue`).
+//
+// Tracking runs apart from the closest-hit work: a resolve round takes a path
+// up to its first segment that needs tracking and queues that segment; the
+// persistent k_track resolves queued segments, refilling a lane as soon as its
+// segment ends, and either ends the path's bounce (collision, dead path) or
+// passes the path to the next round, which continues from the segment's far
+// boundary.  The last round tracks inline.  Every segment draws from its own
+// stream (purpose kPurposeMedium + j, j = medium boundaries met in the bounce)
+// and the steps repeat the loop's operations, so the split changes no result.
+
+// Reserves one slot per calling lane of a warp-aggregated counter.
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t* counter) {
+  const unsigned m = __activemask();
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+}
+
+// A stream positioned at draw idx.
+__device__ __forceinline__ RngStream rng_resume(uint32_t pixel, uint32_t seed, uint32_t sample, uint32_t bounce,
+                                                uint32_t purpose, uint32_t idx) {
+  RngStream r = rng_stream(pixel, seed, sample, bounce, purpose);
+  r.idx = idx;
+  if (idx & 3u) r.buf = philox4x32_10(u4(sample, bounce, idx >> 2, purpose), pixel, seed);
+  return r;
+}
+
+template <bool kInline>
+__device__ __forceinline__ void resolve_path(const RenderLaunch& L, uint32_t p, bool fresh, uint32_t* jobCounter) {
   const SceneView& S = L.scene;
-  const bool dda = L.dda != 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const uint32_t p = q[i];
-    const float4 ro = L.st.rayO[p], rd = L.st.rayD[p];
-    V3 o = xyz(ro), d = xyz(rd);
-    int med = __float_as_int(ro.w);
-    float tmax = rd.w;
-    V3 T = xyz(L.st.T[p]);
-    float4 hr = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(kEventDead));
-    int err = 0;
-    int j = 0;
-    for (; j < kMaxPassThrough; ++j) {
-      hr = scene_closest<true>(S, o, d, tmax);
-      const int c = __float_as_int(hr.w);
-      MediumEvent ev;
-      ev.hit = 0;
-      int evMed = -1;
-      bool dead = false;
-      if (c <= kMediumCodeBase) {
-        const int mi = kMediumCodeBase - c;
-        RngStream rs = rng_stream(p, L.seed, L.sample, L.bounce, kPurposeMedium + (uint32_t)j);
-        if (med >= 0) {  // origin inside a medium: track to the hit
-          if (mi != med) {
+  const float4 ro = L.st.rayO[p], rd = L.st.rayD[p];
+  V3 o = xyz(ro), d = xyz(rd);
+  int med = __float_as_int(ro.w);
+  float tmax = rd.w;
+  V3 T = xyz(L.st.T[p]);
+  int j = 0;
+  if (!fresh) {  // k_track passed the segment that ends at the pending boundary hit
+    const float4 h = L.st.hit[p];
+    const int mi = kMediumCodeBase - __float_as_int(h.w);
+    const Ray nr = ray_offset(make_ray(o + d * h.x, normalize(d), kDefaultTmax), d);
+    o = nr.o;
+    d = nr.d;
+    tmax = nr.tmax;
+    med = med < 0 ? mi : -1;
+    j = (int)L.st.pj[p] + 1;
+  }
+  float4 hr = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(kEventDead));
+  int err = 0;
+  for (; j < kMaxPassThrough; ++j) {
+    hr = scene_closest<true>(S, o, d, tmax);
+    const int c = __float_as_int(hr.w);
+    MediumEvent ev;
+    ev.hit = 0;
+    int evMed = -1;
+    bool dead = false;
+    if (c <= kMediumCodeBase) {
+      const int mi = kMediumCodeBase - c;
+      Ray seg = make_ray(o, d, hr.x);
+      int segMed = -1;
+      if (med >= 0) {  // origin inside a medium: track to the hit
+        if (mi != med) dead = true;
+        else segMed = med;
+      } else {  // entering: find the far side, track through
+        const Ray mr = ray_offset(make_ray(o + d * hr.x, normalize(d), kDefaultTmax), d);
+        const float4 he = scene_closest<true>(S, mr.o, mr.d, mr.tmax);
+        const int ce = __float_as_int(he.w);
+        if (ce != -1) {
+          if (ce <= kMediumCodeBase && kMediumCodeBase - ce != mi) {
             dead = true;
           } else {
-            T = T * instance_sample(S.media[med], make_ray(o, d, hr.x), dda, rs, &ev, &err);
-            evMed = med;
-          }
-        } else {  // entering: find the far side, track through
-          const Ray mr = ray_offset(make_ray(o + d * hr.x, normalize(d), kDefaultTmax), d);
-          const float4 he = scene_closest<true>(S, mr.o, mr.d, mr.tmax);
-          const int ce = __float_as_int(he.w);
-          if (ce != -1) {
-            if (ce <= kMediumCodeBase && kMediumCodeBase - ce != mi) {
-              dead = true;
-            } else {
-              T = T * instance_sample(S.media[mi], make_ray(mr.o, mr.d, he.x), dda, rs, &ev, &err);
-              evMed = mi;
-            }
+            seg = make_ray(mr.o, mr.d, he.x);
+            segMed = mi;
           }
         }
-        if (err) dead = true;
-        if (!dead && (T.x == 0.0f || T.y == 0.0f || T.z == 0.0f)) dead = true;
       }
-      if (dead) {
-        hr.w = __int_as_float(kEventDead);
-        break;
+      if (segMed >= 0) {
+        if (kInline) {
+          RngStream rs = rng_stream(p, L.seed, L.sample, L.bounce, kPurposeMedium + (uint32_t)j);
+          T = T * instance_sample(S.media[segMed], seg, L.dda != 0, rs, &ev, &err);
+          evMed = segMed;
+          if (err) dead = true;
+        } else {  // queue the segment; the path waits at this boundary hit
+          const uint32_t k = warp_reserve(jobCounter);
+          L.st.jO[k] = f4(seg.o, seg.tmax);
+          L.st.jD[k] = f4(seg.d, __int_as_float(segMed));
+          L.st.jM[k] = make_uint2(p, (uint32_t)j);
+          L.st.rayO[p] = f4(o, __int_as_float(med));
+          L.st.rayD[p] = f4(d, tmax);
+          L.st.hit[p] = hr;
+          L.st.pj[p] = (uint32_t)j;
+          return;
+        }
       }
-      if (ev.hit) {
-        L.st.evA[p] = f4(ev.pos, ev.ior);
-        L.st.evB[p] = f4(ev.normal, __int_as_float(evMed));
-        L.st.evC[p] = make_float4(ev.S[0], ev.S[1], ev.S[2], ev.S[3]);
-        L.st.evD[p] = make_float2(ev.S[4], ev.S[5]);
-        hr.w = __int_as_float(kEventScatter);
-        break;
-      }
-      if (c <= kMediumCodeBase) {  // material-less hit: continue from it without counting a bounce
-        const Ray nr = ray_offset(make_ray(o + d * hr.x, normalize(d), kDefaultTmax), d);
-        o = nr.o;
-        d = nr.d;
-        tmax = nr.tmax;
-        med = med < 0 ? kMediumCodeBase - c : -1;
-        hr.w = __int_as_float(kEventDead);  // stays so if the pass-through bound is reached
-        continue;
-      }
-      break;  // surface hit or miss
+      if (!dead && (T.x == 0.0f || T.y == 0.0f || T.z == 0.0f)) dead = true;
     }
-    if (j == kMaxPassThrough) err = 1;
-    if (err) atomicAdd(L.bound, 1u);
-    L.st.rayO[p] = f4(o, __int_as_float(med));
-    L.st.rayD[p] = f4(d, tmax);
+    if (dead) {
+      hr.w = __int_as_float(kEventDead);
+      break;
+    }
+    if (ev.hit) {
+      L.st.evA[p] = f4(ev.pos, ev.ior);
+      L.st.evB[p] = f4(ev.normal, __int_as_float(evMed));
+      L.st.evC[p] = make_float4(ev.S[0], ev.S[1], ev.S[2], ev.S[3]);
+      L.st.evD[p] = make_float2(ev.S[4], ev.S[5]);
+      hr.w = __int_as_float(kEventScatter);
+      break;
+    }
+    if (c <= kMediumCodeBase) {  // material-less hit: continue from it without counting a bounce
+      const Ray nr = ray_offset(make_ray(o + d * hr.x, normalize(d), kDefaultTmax), d);
+      o = nr.o;
+      d = nr.d;
+      tmax = nr.tmax;
+      med = med < 0 ? kMediumCodeBase - c : -1;
+      hr.w = __int_as_float(kEventDead);  // stays so if the pass-through bound is reached
+      continue;
+    }
+    break;  // surface hit or miss
+  }
+  if (j == kMaxPassThrough) err = 1;
+  if (err) atomicAdd(L.bound, 1u);
+  L.st.rayO[p] = f4(o, __int_as_float(med));
+  L.st.rayD[p] = f4(d, tmax);
+  L.st.T[p] = f4(T, 0.0f);
+  L.st.hit[p] = hr;
+}
+
+// Round `round` of path extension: round 0 takes the bounce's live paths,
+// later rounds the paths k_track passed; kInline tracks instead of queueing.
+template <bool kFirst, bool kInline>
+__global__ void __launch_bounds__(128) k_resolve(RenderLaunch L, int round) {
+  uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce;
+  const uint32_t n = kFirst ? *(volatile uint32_t*)&L.st.counts[L.bounce] : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
+  const uint32_t* list = kFirst ? L.st.q[L.bounce & 1] : L.st.rl[round - 1];
+  uint32_t* jobs = &mc[3 * round];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) resolve_path<kInline>(L, list[i], kFirst, jobs);
+}
+
+// End of a tracked path segment.
+__device__ __forceinline__ void finish_sample(const RenderLaunch& L, uint32_t p, int st, int med, const MediumEvent& ev,
+                                              V3 albedo, uint32_t* nextCount, uint32_t* nextList) {
+  V3 T = xyz(L.st.T[p]);
+  bool dead = false;
+  if (st == kTrackError) {
+    atomicAdd(L.bound, 1u);
+    dead = true;
+  } else if (st == kTrackCollide) {
+    T = T * albedo;
     L.st.T[p] = f4(T, 0.0f);
-    L.st.hit[p] = hr;
+  }
+  if (!dead && (T.x == 0.0f || T.y == 0.0f || T.z == 0.0f)) dead = true;
+  if (dead) {
+    float4 h = L.st.hit[p];
+    h.w = __int_as_float(kEventDead);
+    L.st.hit[p] = h;
+  } else if (st == kTrackCollide) {
+    L.st.evA[p] = f4(ev.pos, ev.ior);
+    L.st.evB[p] = f4(ev.normal, __int_as_float(med));
+    L.st.evC[p] = make_float4(ev.S[0], ev.S[1], ev.S[2], ev.S[3]);
+    L.st.evD[p] = make_float2(ev.S[4], ev.S[5]);
+    float4 h = L.st.hit[p];
+    h.w = __int_as_float(kEventScatter);
+    L.st.hit[p] = h;
+  } else {
+    nextList[warp_reserve(nextCount)] = p;
+  }
+}
+
+// End of a tracked shadow segment: the walk's transmittance absorbs it.
+__device__ __forceinline__ void finish_tr(const RenderLaunch& L, uint32_t slot, int st, const TrackState& s,
+                                          uint32_t* nextCount, uint32_t* nextList) {
+  if (st == kTrackError) {
+    atomicAdd(L.bound, 1u);
+    L.st.shTr[slot] = 0.0f;
+    return;
+  }
+  const float4 w = L.st.swP[slot];
+  const float tr = w.w * s.tr;
+  if (tr == 0.0f) {
+    L.st.shTr[slot] = 0.0f;
+    return;
+  }
+  L.st.swP[slot] = make_float4(w.x, w.y, w.z, tr);
+  L.st.swM[slot] = make_int2(L.st.swM[slot].x, (int)s.rng.idx);
+  nextList[warp_reserve(nextCount)] = slot;
+}
+
+// Persistent tracking of the queued segments of round `round`: every lane
+// holds one segment, advances it kTrackSteps steps at a time, and takes the
+// next queued segment as soon as its own ends.
+template <bool kDDA, bool kSample>
+__global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
+  uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce + (kSample ? 0 : kShadowCounters);
+  const uint32_t njobs = *(volatile uint32_t*)&mc[3 * round];
+  uint32_t* taken = &mc[3 * round + 1];
+  uint32_t* nextCount = &mc[3 * round + 2];
+  uint32_t* nextList = kSample ? L.st.rl[round] : L.st.sl[round];
+  const int lane = threadIdx.x & 31;
+  TrackState s;
+  uint32_t owner = 0;
+  int med = 0;
+  bool active = false, drained = false;
+  for (;;) {
+    const bool need = !active && !drained;
+    const unsigned want = __ballot_sync(0xffffffffu, need);
+    if (want) {
+      const int leader = __ffs(want) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(taken, (uint32_t)__popc(want));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (base + (uint32_t)__popc(want) >= njobs) drained = true;  // warp-uniform
+      if (need) {
+        const uint32_t k = base + (uint32_t)__popc(want & ((1u << lane) - 1u));
+        if (k < njobs) {
+          const float4 jo = L.st.jO[k], jd = L.st.jD[k];
+          const uint2 jm = L.st.jM[k];
+          owner = jm.x;
+          med = __float_as_int(jd.w);
+          if (kSample) s.rng = rng_stream(owner, L.seed, L.sample, L.bounce, kPurposeMedium + jm.y);
+          else s.rng = rng_resume(L.st.q[L.bounce & 1][owner >> 1], L.seed, L.sample, L.bounce,
+                                  kPurposeShadowTr + (owner & 1u), jm.y);
+          const int st = track_init<kDDA, kSample>(L.scene.media[med], make_ray(xyz(jo), xyz(jd), jo.w), &s);
+          if (st == kTrackRunning) {
+            active = true;
+          } else if (kSample) {
+            MediumEvent ev;
+            finish_sample(L, owner, st, med, ev, v3(1.0f), nextCount, nextList);
+          } else {
+            finish_tr(L, owner, st, s, nextCount, nextList);
+          }
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) {
+      if (drained) break;
+      continue;
+    }
+    for (int k = 0; k < kTrackSteps && active; ++k) {
+      MediumEvent ev;
+      V3 albedo = v3(1.0f);
+      const int st = track_step<kDDA, kSample>(L.scene.media[med], s, &ev, &albedo);
+      if (st != kTrackRunning) {
+        if (kSample) finish_sample(L, owner, st, med, ev, albedo, nextCount, nextList);
+        else finish_tr(L, owner, st, s, nextCount, nextList);
+        active = false;
+      }
+    }
   }
 }
 
@@ -484,27 +630,15 @@ __global__ void __launch_bounds__(128) k_shade(RenderLaunch L) {
   }
 }
 
-template <bool kMedia>
-__global__ void __launch_bounds__(128) k_shadow(RenderLaunch L) {
+// Visibility of every shadow record of a scene without media.
+__global__ void __launch_bounds__(128) k_shadow_surfaces(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = L.st.q[L.bounce & 1];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += stride) {
     const float4 o = L.st.shO[j];
     float tr = 0.0f;
     const bool traced = o.w > 0.0f;
-    if (traced) {
-      const float4 d = L.st.shD[j];
-      if (kMedia) {
-        const float2 x = L.st.shX[j];
-        RngStream rs = rng_stream(q[j >> 1], L.seed, L.sample, L.bounce, kPurposeShadowTr + (j & 1u));
-        int err = 0;
-        tr = shadow_transmittance(L.scene, xyz(o), xyz(d), x.x, __float_as_int(x.y), L.dda != 0, rs, &err);
-        if (err) atomicAdd(L.bound, 1u);
-      } else {
-        tr = scene_occluded(L.scene, xyz(o), xyz(d), kDefaultTmax) ? 0.0f : 1.0f;
-      }
-    }
+    if (traced) tr = scene_occluded(L.scene, xyz(o), xyz(L.st.shD[j]), kDefaultTmax) ? 0.0f : 1.0f;
     L.st.shTr[j] = tr;
     if (L.stats) {
       const unsigned m = __ballot_sync(__activemask(), traced);
@@ -513,6 +647,112 @@ __global__ void __launch_bounds__(128) k_shadow(RenderLaunch L) {
     }
   }
   if (L.stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)n);
+}
+
+// ------------------------------------------------------------------ media: shadow transmittance
+// CDeviceScene::intersectTr as direct() uses it: 0 when the walk ends on a
+// surface (materials do not emit), else the product of the media's
+// ratio-tracking estimates.  A surface anywhere on the ray ends the walk there,
+// so the any-hit test decides that case; without one the walk visits only
+// medium boxes, segment by segment through CRay::spawnRay towards the fixed
+// far point p1, multiplying Tr when a segment leaves the current medium.  As
+// for path extension, segments that need tracking are queued for k_track and
+// the walk resumes after them; the last round tracks inline.  The slot's
+// stream (purpose kPurposeShadowTr + slot parity) continues across segments.
+template <bool kInline>
+__device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot, bool fresh, uint32_t* jobCounter) {
+  const SceneView& S = L.scene;
+  const float4 o4 = L.st.shO[slot], d4 = L.st.shD[slot];
+  const float2 x = L.st.shX[slot];
+  const V3 o = xyz(o4), d = xyz(d4);
+  V3 p0;
+  int cur;
+  float tr;
+  uint32_t idx;
+  if (fresh) {
+    if (scene_occluded(S, o, d, x.x)) {
+      L.st.shTr[slot] = 0.0f;
+      return;
+    }
+    p0 = o;
+    cur = __float_as_int(x.y);
+    tr = 1.0f;
+    idx = 0;
+  } else {
+    const float4 w = L.st.swP[slot];
+    const int2 m = L.st.swM[slot];
+    p0 = xyz(w);
+    tr = w.w;
+    cur = m.x;
+    idx = (uint32_t)m.y;
+  }
+  const V3 p1 = o + d * x.x;
+  RngStream rs;
+  if (kInline)
+    rs = rng_resume(L.st.q[L.bounce & 1][slot >> 1], L.seed, L.sample, L.bounce, kPurposeShadowTr + (slot & 1u), idx);
+  int err = 0;
+  for (int k = 0; k < kMaxShadowSegments; ++k) {
+    const V3 off = offset_ray_origin(p0, normalize(p1 - p0));
+    const float tl = length(p1 - off);
+    const V3 dir = (p1 - p0) / tl;
+    float best = tl;
+    int hitM = -1;
+    for (int m = 0; m < S.nmedia; ++m) {
+      const float tm = medium_box_hit(S.media[m], off, dir);
+      if (tm >= 0.0f && tm <= tl && tm < best) {
+        best = tm;
+        hitM = m;
+      }
+    }
+    if (hitM < 0) {
+      L.st.shTr[slot] = tr;
+      if (err) atomicAdd(L.bound, 1u);
+      return;
+    }
+    if (cur >= 0 && hitM == cur) {
+      if (kInline) {
+        tr *= instance_tr(S.media[cur], make_ray(off, dir, best), L.dda != 0, rs, &err);
+      } else {
+        const uint32_t k2 = warp_reserve(jobCounter);
+        L.st.jO[k2] = f4(off, best);
+        L.st.jD[k2] = f4(dir, __int_as_float(cur));
+        L.st.jM[k2] = make_uint2(slot, idx);
+        L.st.swP[slot] = f4(off + dir * best, tr);
+        L.st.swM[slot] = make_int2(-1, (int)idx);
+        return;
+      }
+    }
+    p0 = off + dir * best;
+    cur = cur < 0 ? hitM : -1;
+  }
+  atomicAdd(L.bound, 1u);
+  L.st.shTr[slot] = 0.0f;
+}
+
+template <bool kFirst, bool kInline>
+__global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int round) {
+  uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce + kShadowCounters;
+  const uint32_t n = kFirst ? 2 * *(volatile uint32_t*)&L.st.counts[L.bounce] : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
+  const uint32_t* list = kFirst ? nullptr : L.st.sl[round - 1];
+  uint32_t* jobs = &mc[3 * round];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t slot = kFirst ? i : list[i];
+    if (kFirst) {
+      const bool traced = L.st.shO[slot].w > 0.0f;
+      if (L.stats) {
+        const unsigned m = __ballot_sync(__activemask(), traced);
+        if ((threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1) && m)
+          atomicAdd(&L.stats[1], (unsigned long long)__popc(m));
+      }
+      if (!traced) {
+        L.st.shTr[slot] = 0.0f;
+        continue;
+      }
+    }
+    shadow_walk<kInline>(L, slot, kFirst, jobs);
+  }
+  if (kFirst && L.stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)(n / 2));
 }
 
 __global__ void __launch_bounds__(256) k_accum(RenderLaunch L) {
@@ -543,6 +783,30 @@ __global__ void __launch_bounds__(256) k_finish(RenderLaunch L) {
   }
 }
 
+template <typename K>
+int resident_blocks(K kernel, int threads) {
+  int n = 0;
+  R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0));
+  return std::max(1, n) * sm_count();
+}
+
+void launch_track(const RenderLaunch& L, bool sample, int round, cudaStream_t s) {
+  static int b[4] = {0, 0, 0, 0};
+  const int which = (L.dda ? 1 : 0) + (sample ? 2 : 0);
+  if (b[which] == 0) {
+    b[0] = resident_blocks(k_track<false, false>, 128);
+    b[1] = resident_blocks(k_track<true, false>, 128);
+    b[2] = resident_blocks(k_track<false, true>, 128);
+    b[3] = resident_blocks(k_track<true, true>, 128);
+  }
+  switch (which) {
+    case 0: k_track<false, false><<<b[0], 128, 0, s>>>(L, round); break;
+    case 1: k_track<true, false><<<b[1], 128, 0, s>>>(L, round); break;
+    case 2: k_track<false, true><<<b[2], 128, 0, s>>>(L, round); break;
+    default: k_track<true, true><<<b[3], 128, 0, s>>>(L, round); break;
+  }
+}
+
 }  // namespace
 
 void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, WaveTimer* tm) {
@@ -556,23 +820,34 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
     ++ev;
   };
   R2_CUDA(cudaMemsetAsync(L.st.counts, 0, sizeof(uint32_t) * (L.maxDepth + 2), s));
+  if (media) R2_CUDA(cudaMemsetAsync(L.st.mc, 0, sizeof(uint32_t) * kCountersPerBounce * L.maxDepth, s));
   mark(-1);
   k_camera<<<nblocks, 256, 0, s>>>(L);
   mark(0);
   for (uint32_t b = 0; b < L.maxDepth; ++b) {
     L.bounce = b;
     if (media) {
-      k_extend_media<<<nblocks * 2, 128, 0, s>>>(L);
+      k_resolve<true, false><<<nblocks * 2, 128, 0, s>>>(L, 0);
+      for (int r = 0; r < kMediaRounds; ++r) {
+        launch_track(L, true, r, s);
+        if (r + 1 < kMediaRounds) k_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
+        else k_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
+      }
       mark(1);
       k_shade<true><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
-      k_shadow<true><<<nblocks * 2, 128, 0, s>>>(L);
+      k_shadow_resolve<true, false><<<nblocks * 2, 128, 0, s>>>(L, 0);
+      for (int r = 0; r < kMediaRounds; ++r) {
+        launch_track(L, false, r, s);
+        if (r + 1 < kMediaRounds) k_shadow_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
+        else k_shadow_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
+      }
     } else {
       k_extend<<<nblocks * 2, 128, 0, s>>>(L);
       mark(1);
       k_shade<false><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
-      k_shadow<false><<<nblocks * 2, 128, 0, s>>>(L);
+      k_shadow_surfaces<<<nblocks * 2, 128, 0, s>>>(L);
     }
     mark(3);
     k_accum<<<nblocks, 256, 0, s>>>(L);

@@ -55,6 +55,15 @@ struct PathState {
   float4* evB;      // collision normal, medium index (int bits)
   float4* evC;      // SGGX S xx yy zz xy
   float2* evD;      // SGGX S xz yz
+  uint32_t* mc;     // per-bounce counters of the tracking rounds
+  uint32_t* pj;     // per path: medium boundaries met in the bounce when its segment was queued
+  float4* jO;       // queued segments: origin, tmax
+  float4* jD;       //                  direction, medium (int bits)
+  uint2* jM;        //                  owner (path or shadow slot), stream purpose / draw index
+  uint32_t* rl[2];  // paths resumed in rounds 1, 2
+  uint32_t* sl[2];  // shadow slots resumed in rounds 1, 2
+  float4* swP;      // shadow walk: next origin, transmittance so far
+  int2* swM;        // shadow walk: current medium, draw index of the slot's stream
 };
 
 constexpr int kEventScatter = -2147483647;  // INT_MIN + 1

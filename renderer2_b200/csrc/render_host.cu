@@ -249,6 +249,11 @@ void RenderScene::ensure_state(uint32_t n) {
   if (!media_.empty() && n > mediaCap_) {
     shX_.alloc(2 * (size_t)n);
     evA_.alloc(n); evB_.alloc(n); evC_.alloc(n); evD_.alloc(n);
+    mc_.alloc(16 * 64);
+    pj_.alloc(n); rl0_.alloc(n); rl1_.alloc(n);
+    sl0_.alloc(2 * (size_t)n); sl1_.alloc(2 * (size_t)n);
+    jO_.alloc(2 * (size_t)n); jD_.alloc(2 * (size_t)n); jM_.alloc(2 * (size_t)n);
+    swP_.alloc(2 * (size_t)n); swM_.alloc(2 * (size_t)n);
     mediaCap_ = n;
   }
 }
@@ -275,6 +280,10 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
   if (!media_.empty()) {
     L.st.shX = shX_.get();
     L.st.evA = evA_.get(); L.st.evB = evB_.get(); L.st.evC = evC_.get(); L.st.evD = evD_.get();
+    L.st.mc = mc_.get(); L.st.pj = pj_.get();
+    L.st.rl[0] = rl0_.get(); L.st.rl[1] = rl1_.get(); L.st.sl[0] = sl0_.get(); L.st.sl[1] = sl1_.get();
+    L.st.jO = jO_.get(); L.st.jD = jD_.get(); L.st.jM = jM_.get();
+    L.st.swP = swP_.get(); L.st.swM = swM_.get();
   }
   L.frame = d_frame;
   L.npix = npix;

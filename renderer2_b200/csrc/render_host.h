@@ -77,6 +77,10 @@ class RenderScene {
   uint32_t mediaCap_ = 0;
   DBuf<float2> shX_, evD_;
   DBuf<float4> evA_, evB_, evC_;
+  DBuf<uint32_t> mc_, pj_, rl0_, rl1_, sl0_, sl1_;
+  DBuf<float4> jO_, jD_, swP_;
+  DBuf<uint2> jM_;
+  DBuf<int2> swM_;
   DBuf<unsigned int> bound_;
   DBuf<unsigned long long> statBuf_;
   std::unique_ptr<WaveTimer> timer_;
