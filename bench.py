@@ -567,16 +567,20 @@ def run_case(args):
         torch.cuda.synchronize()
         sc.close()
         print(json.dumps({"case": args.case, "voxels": st[0], "candidates": st[1], "ms": st[2]}))
-    elif args.case == "volume-small":
+    elif args.case in ("volume-small", "volume-mid"):
         import tempfile
 
         from renderer2_b200 import raytracer as R
         from renderer2_b200 import render_scenes as RS
-        desc, cam = RS.volume_scene(tempfile.mkdtemp(prefix="r2vol"), 0, grid=128, n_quads=50_000, ico_subdiv=4,
-                                    width=480, height=270)
+        if args.case == "volume-small":
+            desc, cam = RS.volume_scene(tempfile.mkdtemp(prefix="r2vol"), 0, grid=128, n_quads=50_000, ico_subdiv=4,
+                                        width=480, height=270)
+        else:  # the bench scene at a quarter of the pixels, one wave
+            desc, cam = RS.volume_scene(tempfile.mkdtemp(prefix="r2vol"), 0, width=960, height=540)
         sc = RS.build_scene(desc)
         frame = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
-        st = sc.render_device(cam, R.params(2, 16, 0, brick_grid=True), frame.data_ptr())
+        spp = 2 if args.case == "volume-small" else 1
+        st = sc.render_device(cam, R.params(spp, 16, 0, brick_grid=True), frame.data_ptr())
         torch.cuda.synchronize()
         sc.close()
         print(json.dumps({"case": args.case, "paths": st[0], "ms": st[1], "extend_ms": st[4], "shade_ms": st[5],

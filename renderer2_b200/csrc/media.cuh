@@ -30,6 +30,25 @@ struct RngStream {
     ++idx;
     return u01(w == 0 ? buf.x : (w == 1 ? buf.y : (w == 2 ? buf.z : buf.w)));
   }
+  // The next five draws without consuming them, from the two blocks that hold
+  // them (computed together, so lanes of a warp that reach this point compute
+  // them at once instead of at different draws); advance() consumes n <= 5.
+  R2_HD void peek5(float* u, U4* w0, U4* w1) const {
+    const uint32_t b = idx >> 2;
+    *w0 = philox4x32_10(u4(c0, c1, b, purpose), k0, k1);
+    *w1 = philox4x32_10(u4(c0, c1, b + 1u, purpose), k0, k1);
+    for (uint32_t i = 0; i < 5u; ++i) {
+      const uint32_t j = (idx & 3u) + i;
+      const U4& w = j < 4u ? *w0 : *w1;
+      const uint32_t k = j & 3u;
+      u[i] = u01(k == 0 ? w.x : (k == 1 ? w.y : (k == 2 ? w.z : w.w)));
+    }
+  }
+  R2_HD void advance(uint32_t n, const U4& w0, const U4& w1) {
+    const uint32_t b = idx >> 2;
+    idx += n;
+    buf = (idx >> 2) == b ? w0 : w1;  // next() recomputes when idx reaches a new block
+  }
 };
 R2_HD RngStream rng_stream(uint32_t pixel, uint32_t seed, uint32_t sample, uint32_t bounce, uint32_t purpose) {
   RngStream r;
@@ -686,10 +705,34 @@ R2_HD int track_init(const MediumView& m, const Ray& rayWorld, TrackState* s) {
   return kTrackRunning;
 }
 
-// One iteration.  kSample: kTrackCollide fills ev (world space) and albedo.
-// Transmittance: kTrackDone leaves the estimate in s.tr.
+// The collision at parameter t of the tracking-space ray (o, d) of a sampled
+// segment: the event in world space and the albedo weight, as sampleInternal /
+// sampleDDA compute them when their test accepts.
+template <bool kDDA>
+R2_HD V3 track_collision(const MediumView& m, V3 o, V3 d, float t, MediumEvent* ev) {
+  FData fd;
+  Ray w;
+  if (kDDA) {
+    const V3 ip = o + d * t;
+    const V3 pos = v3((ip.x - (float)m.ibbMin[0]) / (float)m.size[0], (ip.y - (float)m.ibbMin[1]) / (float)m.size[1],
+                      (ip.z - (float)m.ibbMin[2]) / (float)m.size[2]);
+    fd = medium_filtered(m, pos);
+    w = ray_transform2(make_ray(o, d, t), m.scaledToModel);
+  } else {
+    fd = medium_filtered(m, o + d * t);
+    w = ray_transform2(make_ray(o, d, t), m.indexToModel);
+  }
+  fill_event(ev, w, fd);
+  const V3 albedo = scatter_albedo(m, fd, w.d);
+  ev->pos = xform_point(m.modelToWorld, ev->pos);
+  ev->normal = normalize(xform_vector(m.modelToWorld, ev->normal));
+  return albedo;
+}
+
+// One iteration.  kSample: kTrackCollide leaves the collision at s.t (see
+// track_collision).  Transmittance: kTrackDone leaves the estimate in s.tr.
 template <bool kDDA, bool kSample>
-R2_HD int track_step(const MediumView& m, TrackState& s, MediumEvent* ev, V3* albedo) {
+R2_HD int track_step(const MediumView& m, TrackState& s) {
   if (s.steps >= kMaxTrackingSteps) return kTrackError;
   ++s.steps;
   if (kDDA) {
@@ -706,34 +749,34 @@ R2_HD int track_step(const MediumView& m, TrackState& s, MediumEvent* ev, V3* al
     if (s.tau > 0.0f) return kTrackRunning;
     s.t += s.tau / (majorant * m.sigmaT);
     if (s.t >= s.tmax) return kTrackDone;
-    const float jx = s.rng.next();
-    const float jy = s.rng.next();
-    const float jz = s.rng.next();
-    const float d = brick_density(m, s.o + s.d * s.t + v3(jx, jy, jz) - v3(0.5f));
-    if (s.rng.next() * majorant < d * m.filterRenderRatio) {
+    // draws: jitter x, y, z, acceptance, then the roulette (transmittance
+    // only, after a real collision that drops tr below 0.1) and the next
+    // free-flight sample, in that order
+    float u[5];
+    U4 w0, w1;
+    s.rng.peek5(u, &w0, &w1);
+    const float d = brick_density(m, s.o + s.d * s.t + v3(u[0], u[1], u[2]) - v3(0.5f));
+    if (u[3] * majorant < d * m.filterRenderRatio) {
       if (kSample) {
-        const V3 ip = s.o + s.d * s.t;
-        const V3 pos = v3((ip.x - (float)m.ibbMin[0]) / (float)m.size[0], (ip.y - (float)m.ibbMin[1]) / (float)m.size[1],
-                          (ip.z - (float)m.ibbMin[2]) / (float)m.size[2]);
-        const FData fd = medium_filtered(m, pos);
-        const Ray w = ray_transform2(make_ray(s.o, s.d, s.t), m.scaledToModel);
-        fill_event(ev, w, fd);
-        *albedo = scatter_albedo(m, fd, w.d);
-        ev->pos = xform_point(m.modelToWorld, ev->pos);
-        ev->normal = normalize(xform_vector(m.modelToWorld, ev->normal));
+        s.rng.advance(4, w0, w1);
         return kTrackCollide;
       }
       s.tr *= fmaxf(0.0f, 1.0f - s.invMax / majorant);
       if (s.tr < 0.1f) {
         const float prob = 1.0f - s.tr;
-        if (s.rng.next() < prob) {
+        s.rng.advance(5, w0, w1);
+        if (u[4] < prob) {
           s.tr = 0.0f;
           return kTrackDone;
         }
         s.tr /= 1.0f - prob;
+        s.tau = -log_r2(1.0f - s.rng.next());
+        s.mip = fmaxf(0.0f, s.mip - 2.0f);
+        return kTrackRunning;
       }
     }
-    s.tau = -log_r2(1.0f - s.rng.next());
+    s.rng.advance(5, w0, w1);
+    s.tau = -log_r2(1.0f - u[4]);
     s.mip = fmaxf(0.0f, s.mip - 2.0f);
     return kTrackRunning;
   } else {
@@ -741,18 +784,7 @@ R2_HD int track_step(const MediumView& m, TrackState& s, MediumEvent* ev, V3* al
     if (s.t >= s.tmax) return kTrackDone;
     const V3 pt = s.o + s.d * s.t;
     const float dens = medium_density(m, pt);
-    if (kSample) {
-      if (m.filterRenderRatio * dens * s.invMax > s.rng.next()) {
-        const FData fd = medium_filtered(m, pt);
-        const Ray w = ray_transform2(make_ray(s.o, s.d, s.t), m.indexToModel);
-        fill_event(ev, w, fd);
-        *albedo = scatter_albedo(m, fd, w.d);
-        ev->pos = xform_point(m.modelToWorld, ev->pos);
-        ev->normal = normalize(xform_vector(m.modelToWorld, ev->normal));
-        return kTrackCollide;
-      }
-      return kTrackRunning;
-    }
+    if (kSample) return m.filterRenderRatio * dens * s.invMax > s.rng.next() ? kTrackCollide : kTrackRunning;
     s.tr *= 1.0f - fmaxf(0.0f, m.filterRenderRatio * dens * s.invMax);
     if (s.tr < 1.0f) {
       const float p = 1.0f - s.tr;

@@ -260,6 +260,11 @@ R2_HD uint16_t f32_to_f16_bits(float f) {
 }
 
 R2_HD float f16_bits_to_f32(uint16_t h) {
+#if defined(__CUDA_ARCH__)
+  float f;  // half -> float is exact: the conversion instruction gives the same bits
+  asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(h));
+  return f;
+#else
   uint32_t sign = ((uint32_t)h & 0x8000u) << 16;
   uint32_t e = (h >> 10) & 0x1Fu;
   uint32_t m = h & 0x3FFu;
@@ -281,6 +286,7 @@ R2_HD float f16_bits_to_f32(uint16_t h) {
   float f;
   memcpy(&f, &x, 4);
   return f;
+#endif
 }
 
 }  // namespace r2

@@ -36,12 +36,13 @@ constexpr uint32_t kPurposeShadowTr = 0x200u;  // + shadow slot (0 light, 1 BSDF
 constexpr int kMaxPassThrough = 64;            // medium boundaries crossed within one bounce
 constexpr int kMaxShadowSegments = 256;        // medium boundaries along one shadow ray (per round)
 constexpr int kMediaRounds = 2;                // queued tracking rounds per bounce before the inline round
-constexpr int kTrackSteps = 8;                 // tracking steps a lane takes between refills
+constexpr uint32_t kDefaultTrackSteps = 8;     // tracking steps a lane takes between refills
 // Media counters of a bounce (PathState::mc): [3r] segments queued in round r,
 // [3r+1] segments taken, [3r+2] entries of list r + 1; path extension at 0,
 // shadows at kShadowCounters.
 constexpr int kCountersPerBounce = 16;
 constexpr int kShadowCounters = 6;
+constexpr int kCollideCounter = 12;  // entries of the collision list
 
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
@@ -309,33 +310,59 @@ __global__ void __launch_bounds__(128) k_resolve(RenderLaunch L, int round) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) resolve_path<kInline>(L, list[i], kFirst, jobs);
 }
 
-// End of a tracked path segment.
-__device__ __forceinline__ void finish_sample(const RenderLaunch& L, uint32_t p, int st, int med, const MediumEvent& ev,
-                                              V3 albedo, uint32_t* nextCount, uint32_t* nextList) {
-  V3 T = xyz(L.st.T[p]);
+// End of a tracked path segment without a collision: a pass (or an error).
+__device__ __forceinline__ void finish_pass(const RenderLaunch& L, uint32_t p, int st, uint32_t* nextCount,
+                                            uint32_t* nextList) {
+  const V3 T = xyz(L.st.T[p]);
   bool dead = false;
   if (st == kTrackError) {
     atomicAdd(L.bound, 1u);
     dead = true;
-  } else if (st == kTrackCollide) {
-    T = T * albedo;
-    L.st.T[p] = f4(T, 0.0f);
   }
   if (!dead && (T.x == 0.0f || T.y == 0.0f || T.z == 0.0f)) dead = true;
   if (dead) {
     float4 h = L.st.hit[p];
     h.w = __int_as_float(kEventDead);
     L.st.hit[p] = h;
-  } else if (st == kTrackCollide) {
-    L.st.evA[p] = f4(ev.pos, ev.ior);
-    L.st.evB[p] = f4(ev.normal, __int_as_float(med));
-    L.st.evC[p] = make_float4(ev.S[0], ev.S[1], ev.S[2], ev.S[3]);
-    L.st.evD[p] = make_float2(ev.S[4], ev.S[5]);
-    float4 h = L.st.hit[p];
-    h.w = __int_as_float(kEventScatter);
-    L.st.hit[p] = h;
   } else {
     nextList[warp_reserve(nextCount)] = p;
+  }
+}
+
+// A collision: the tracking-space ray and parameter are parked in evA/evB and
+// the path joins the collision list that k_collide resolves.
+__device__ __forceinline__ void finish_collide(const RenderLaunch& L, uint32_t p, int med, const TrackState& s) {
+  uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce;
+  L.st.evA[p] = f4(s.o, s.t);
+  L.st.evB[p] = f4(s.d, __int_as_float(med));
+  L.st.cl[warp_reserve(&mc[kCollideCounter])] = p;
+}
+
+// Collision events of the bounce's queued segments (sampleInternal /
+// sampleDDA on acceptance), the albedo weight, and the dead-path rule.
+template <bool kDDA>
+__global__ void __launch_bounds__(128) k_collide(RenderLaunch L) {
+  const uint32_t n = *(volatile uint32_t*)&L.st.mc[kCountersPerBounce * L.bounce + kCollideCounter];
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t p = L.st.cl[i];
+    const float4 a = L.st.evA[p], b = L.st.evB[p];
+    const int med = __float_as_int(b.w);
+    MediumEvent ev;
+    const V3 albedo = track_collision<kDDA>(L.scene.media[med], xyz(a), xyz(b), a.w, &ev);
+    const V3 T = xyz(L.st.T[p]) * albedo;
+    L.st.T[p] = f4(T, 0.0f);
+    float4 h = L.st.hit[p];
+    if (T.x == 0.0f || T.y == 0.0f || T.z == 0.0f) {
+      h.w = __int_as_float(kEventDead);
+    } else {
+      L.st.evA[p] = f4(ev.pos, ev.ior);
+      L.st.evB[p] = f4(ev.normal, __int_as_float(med));
+      L.st.evC[p] = make_float4(ev.S[0], ev.S[1], ev.S[2], ev.S[3]);
+      L.st.evD[p] = make_float2(ev.S[4], ev.S[5]);
+      h.w = __int_as_float(kEventScatter);
+    }
+    L.st.hit[p] = h;
   }
 }
 
@@ -359,7 +386,7 @@ __device__ __forceinline__ void finish_tr(const RenderLaunch& L, uint32_t slot, 
 }
 
 // Persistent tracking of the queued segments of round `round`: every lane
-// holds one segment, advances it kTrackSteps steps at a time, and takes the
+// holds one segment, advances it L.trackSteps steps at a time, and takes the
 // next queued segment as soon as its own ends.
 template <bool kDDA, bool kSample>
 __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
@@ -396,8 +423,7 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
           if (st == kTrackRunning) {
             active = true;
           } else if (kSample) {
-            MediumEvent ev;
-            finish_sample(L, owner, st, med, ev, v3(1.0f), nextCount, nextList);
+            finish_pass(L, owner, st, nextCount, nextList);
           } else {
             finish_tr(L, owner, st, s, nextCount, nextList);
           }
@@ -408,12 +434,11 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
       if (drained) break;
       continue;
     }
-    for (int k = 0; k < kTrackSteps && active; ++k) {
-      MediumEvent ev;
-      V3 albedo = v3(1.0f);
-      const int st = track_step<kDDA, kSample>(L.scene.media[med], s, &ev, &albedo);
+    for (uint32_t k = 0; k < L.trackSteps && active; ++k) {
+      const int st = track_step<kDDA, kSample>(L.scene.media[med], s);
       if (st != kTrackRunning) {
-        if (kSample) finish_sample(L, owner, st, med, ev, albedo, nextCount, nextList);
+        if (kSample && st == kTrackCollide) finish_collide(L, owner, med, s);
+        else if (kSample) finish_pass(L, owner, st, nextCount, nextList);
         else finish_tr(L, owner, st, s, nextCount, nextList);
         active = false;
       }
@@ -811,6 +836,7 @@ void launch_track(const RenderLaunch& L, bool sample, int round, cudaStream_t s)
 
 void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, WaveTimer* tm) {
   RenderLaunch L = L0;
+  if (L.trackSteps == 0) L.trackSteps = kDefaultTrackSteps;
   const bool media = L.scene.nmedia > 0;
   int ev = 0;
   auto mark = [&](int kind) {
@@ -833,6 +859,8 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
         if (r + 1 < kMediaRounds) k_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
         else k_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
+      if (L.dda) k_collide<true><<<nblocks * 2, 128, 0, s>>>(L);
+      else k_collide<false><<<nblocks * 2, 128, 0, s>>>(L);
       mark(1);
       k_shade<true><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);

@@ -62,6 +62,7 @@ struct PathState {
   uint2* jM;        //                  owner (path or shadow slot), stream purpose / draw index
   uint32_t* rl[2];  // paths resumed in rounds 1, 2
   uint32_t* sl[2];  // shadow slots resumed in rounds 1, 2
+  uint32_t* cl;     // paths whose queued segment ended in a collision
   float4* swP;      // shadow walk: next origin, transmittance so far
   int2* swM;        // shadow walk: current medium, draw index of the slot's stream
 };
@@ -81,6 +82,7 @@ struct RenderLaunch {
   uint32_t seed;
   uint32_t bounce;
   uint32_t dda;       // brick-grid DDA tracking (UseBrickGrid) instead of the global majorant
+  uint32_t trackSteps;  // tracking steps a lane takes between refills (tuning, >= 1)
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

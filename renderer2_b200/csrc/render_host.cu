@@ -1,5 +1,6 @@
 // Host side of the wavefront path tracer.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -95,6 +96,7 @@ RenderScene::RenderScene() {
   R2_CUDA(cudaEventCreate(&ev0_));
   R2_CUDA(cudaEventCreate(&ev1_));
   memset(&view_, 0, sizeof(view_));
+  if (const char* e = getenv("R2_TRACK_STEPS")) trackSteps_ = (uint32_t)std::max(1l, std::min(1024l, atol(e)));
 }
 
 RenderScene::~RenderScene() {
@@ -250,7 +252,7 @@ void RenderScene::ensure_state(uint32_t n) {
     shX_.alloc(2 * (size_t)n);
     evA_.alloc(n); evB_.alloc(n); evC_.alloc(n); evD_.alloc(n);
     mc_.alloc(16 * 64);
-    pj_.alloc(n); rl0_.alloc(n); rl1_.alloc(n);
+    pj_.alloc(n); rl0_.alloc(n); rl1_.alloc(n); cl_.alloc(n);
     sl0_.alloc(2 * (size_t)n); sl1_.alloc(2 * (size_t)n);
     jO_.alloc(2 * (size_t)n); jD_.alloc(2 * (size_t)n); jM_.alloc(2 * (size_t)n);
     swP_.alloc(2 * (size_t)n); swM_.alloc(2 * (size_t)n);
@@ -281,7 +283,7 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
     L.st.shX = shX_.get();
     L.st.evA = evA_.get(); L.st.evB = evB_.get(); L.st.evC = evC_.get(); L.st.evD = evD_.get();
     L.st.mc = mc_.get(); L.st.pj = pj_.get();
-    L.st.rl[0] = rl0_.get(); L.st.rl[1] = rl1_.get(); L.st.sl[0] = sl0_.get(); L.st.sl[1] = sl1_.get();
+    L.st.rl[0] = rl0_.get(); L.st.rl[1] = rl1_.get(); L.st.cl = cl_.get(); L.st.sl[0] = sl0_.get(); L.st.sl[1] = sl1_.get();
     L.st.jO = jO_.get(); L.st.jD = jD_.get(); L.st.jM = jM_.get();
     L.st.swP = swP_.get(); L.st.swM = swM_.get();
   }
@@ -291,6 +293,7 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
   L.maxDepth = p.max_depth;
   L.seed = p.seed;
   L.dda = (p.flags & R2_RENDER_BRICK_GRID) ? 1u : 0u;
+  L.trackSteps = trackSteps_;
   L.bound = bound_.get();
   R2_CUDA(cudaMemsetAsync(bound_.get(), 0, sizeof(unsigned int), s));
   int nblocks = std::max(1, std::min((int)((npix + 255) / 256), sm_count() * 8));

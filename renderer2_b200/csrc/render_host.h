@@ -75,9 +75,10 @@ class RenderScene {
   DBuf<uint32_t> q0_, q1_, counts_;
   DBuf<float> shTr_;
   uint32_t mediaCap_ = 0;
+  uint32_t trackSteps_ = 0;  // 0: the kernels' default; R2_TRACK_STEPS overrides
   DBuf<float2> shX_, evD_;
   DBuf<float4> evA_, evB_, evC_;
-  DBuf<uint32_t> mc_, pj_, rl0_, rl1_, sl0_, sl1_;
+  DBuf<uint32_t> mc_, pj_, rl0_, rl1_, sl0_, sl1_, cl_;
   DBuf<float4> jO_, jD_, swP_;
   DBuf<uint2> jM_;
   DBuf<int2> swM_;
