@@ -33,7 +33,8 @@ typedef enum r2_status {
   R2_ERR_DEVICE_TIMEOUT = 6,
   R2_ERR_DEVICE = 7,
   R2_ERR_UNSUPPORTED = 8,
-  R2_ERR_NO_DEVICE = 9
+  R2_ERR_NO_DEVICE = 9,
+  R2_ERR_PENDING = 10  /* a served job did not finish within the wait */
 } r2_status;
 
 /* Human-readable name of a status code (static string). */
@@ -331,6 +332,39 @@ r2_status r2_write_hdr(const char* path, const float* rgb, uint32_t width, uint3
 /* OBJ/MTL import summary (CAssetManager::loadWithAssimp, asset_manager.cu:25-84). */
 r2_status r2_obj_info(const char* directory, const char* filename, uint32_t* n_submeshes, uint32_t* n_vertices,
                       uint32_t* n_triangles, r2_material* first_material);
+
+/* ------------------------------------------------------------------------ */
+/* Serving: a request loop that overlaps jobs on the device (continuous
+ * batching).  This has no counterpart in the reference, which renders one
+ * frame at a time (raytracer/pipeline.cu:24-90).
+ *
+ * Jobs wait in a FIFO queue; the loop admits the head as soon as one of
+ * `slots` slots is free and the job's device memory (wave state and frame, or
+ * voxel output and work list) fits in what `hbm_budget_bytes` leaves.  Each
+ * slot has its own stream and buffers; scenes stay resident and must stay
+ * alive and unmodified (committed) while their jobs run.  Each result is the
+ * same alone and in any mix (random streams depend on pixel, sample and seed
+ * only).  A job's output is written to the caller's buffer before r2_server_wait
+ * reports it. */
+typedef struct r2_server r2_server;
+r2_status r2_server_create(uint32_t slots, uint64_t hbm_budget_bytes, r2_server** out);
+/* Finishes admitted and queued jobs, then releases the server. */
+r2_status r2_server_destroy(r2_server* server);
+/* A frame of a committed scene into rgb_out (W*H*3 floats, row 0 at the bottom).
+ * R2_ERR_ADMISSION_REJECTED if the job alone exceeds the budget. */
+r2_status r2_server_submit_render(r2_server* server, r2_scene* scene, const r2_camera* camera,
+                                  const r2_render_params* params, float* rgb_out, uint64_t* job_id);
+/* One LOD of a filter scene into out (nx*ny*nz payloads). */
+r2_status r2_server_submit_filter(r2_server* server, r2_filter_scene* scene, const r2_filter_grid* grid,
+                                  const r2_filter_params* params, uint32_t lod, r2_voxel* out, uint64_t* job_id);
+/* Waits up to timeout_s seconds (< 0: forever).  Returns R2_ERR_PENDING if the
+ * job is not done yet (it can be waited for again), else the job's own status;
+ * times_out (nullable, 3 doubles): submit, start and end times in seconds on the
+ * server's clock.  A finished job is forgotten once waited for. */
+r2_status r2_server_wait(r2_server* server, uint64_t job_id, double timeout_s, double* times_out);
+/* stats_out (5 doubles): jobs done, jobs queued, jobs running, device bytes
+ * admitted, seconds since the server started. */
+r2_status r2_server_stats(r2_server* server, double* stats_out);
 
 /* ------------------------------------------------------------------------ */
 /* Synthetic inputs (seeded), used by the configs in the benchmark plan. */

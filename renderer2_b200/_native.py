@@ -82,6 +82,12 @@ def _load():
         "r2_scene_commit": (C.c_int, [P]),
         "r2_render_device": (C.c_int, [P, P, P, P, P, P]),
         "r2_render_host": (C.c_int, [P, P, P, P]),
+        "r2_server_create": (C.c_int, [u32, C.c_uint64, P]),
+        "r2_server_destroy": (C.c_int, [P]),
+        "r2_server_submit_render": (C.c_int, [P, P, P, P, P, P]),
+        "r2_server_submit_filter": (C.c_int, [P, P, P, P, u32, P, P]),
+        "r2_server_wait": (C.c_int, [P, C.c_uint64, C.c_double, P]),
+        "r2_server_stats": (C.c_int, [P, P]),
         "r2_config_load": (C.c_int, [C.c_char_p, P]),
         "r2_config_free": (C.c_int, [P]),
         "r2_config_info_get": (C.c_int, [P, P]),

@@ -36,6 +36,7 @@ const char* r2_status_string(r2_status s) {
     case R2_ERR_DEVICE: return "R2_ERR_DEVICE";
     case R2_ERR_UNSUPPORTED: return "R2_ERR_UNSUPPORTED";
     case R2_ERR_NO_DEVICE: return "R2_ERR_NO_DEVICE";
+    case R2_ERR_PENDING: return "R2_ERR_PENDING";
   }
   return "R2_ERR_UNKNOWN";
 }

@@ -8,6 +8,8 @@ struct r2_scene {
   std::unique_ptr<r2::RenderScene> impl;
 };
 
+r2::RenderScene* r2_scene_impl(r2_scene* scene) { return scene->impl.get(); }
+
 extern "C" {
 
 r2_status r2_scene_create(r2_scene** out) {

@@ -45,6 +45,11 @@ constexpr int kShadowCounters = 6;
 constexpr int kCollideCounter = 12;  // entries of the collision list
 
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+// Sample index of the wave: a kernel parameter, or the device counter of a
+// captured wave that is replayed once per sample.
+__device__ __forceinline__ uint32_t wave_sample(const RenderLaunch& L) {
+  return L.sampleDev ? *(volatile const uint32_t*)L.sampleDev : L.sample;
+}
 __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
 
 // Closest hit over triangles, analytic shapes and (kMedia) medium boxes.
@@ -142,7 +147,7 @@ __global__ void __launch_bounds__(256) k_camera(RenderLaunch L) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < L.npix; p += stride) {
     const int px = (int)(p % (uint32_t)L.cam.W), py = (int)(p / (uint32_t)L.cam.W);
-    const U4 r = philox4x32_10(u4(L.sample, kPurposeCamera, 0u, 0u), p, L.seed);
+    const U4 r = philox4x32_10(u4(wave_sample(L), kPurposeCamera, 0u, 0u), p, L.seed);
     V3 o, d;
     camera_ray(L.cam, px, py, u01(r.x), &o, &d);
     L.st.rayO[p] = f4(o, __int_as_float(-1));
@@ -249,7 +254,7 @@ __device__ __forceinline__ void resolve_path(const RenderLaunch& L, uint32_t p, 
       }
       if (segMed >= 0) {
         if (kInline) {
-          RngStream rs = rng_stream(p, L.seed, L.sample, L.bounce, kPurposeMedium + (uint32_t)j);
+          RngStream rs = rng_stream(p, L.seed, wave_sample(L), L.bounce, kPurposeMedium + (uint32_t)j);
           T = T * instance_sample(S.media[segMed], seg, L.dda != 0, rs, &ev, &err);
           evMed = segMed;
           if (err) dead = true;
@@ -416,8 +421,8 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
           const uint2 jm = L.st.jM[k];
           owner = jm.x;
           med = __float_as_int(jd.w);
-          if (kSample) s.rng = rng_stream(owner, L.seed, L.sample, L.bounce, kPurposeMedium + jm.y);
-          else s.rng = rng_resume(L.st.q[L.bounce & 1][owner >> 1], L.seed, L.sample, L.bounce,
+          if (kSample) s.rng = rng_stream(owner, L.seed, wave_sample(L), L.bounce, kPurposeMedium + jm.y);
+          else s.rng = rng_resume(L.st.q[L.bounce & 1][owner >> 1], L.seed, wave_sample(L), L.bounce,
                                   kPurposeShadowTr + (owner & 1u), jm.y);
           const int st = track_init<kDDA, kSample>(L.scene.media[med], make_ray(xyz(jo), xyz(jd), jo.w), &s);
           if (st == kTrackRunning) {
@@ -467,8 +472,8 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
     n = sh.type == kShapeCircle ? normalize(sh.normal) : normalize(pos - sh.center);
     m = L.scene.mats[sh.material];
   }
-  const U4 rA = philox4x32_10(u4(L.sample, L.bounce, 0u, 1u), p, L.seed);
-  const U4 rB = philox4x32_10(u4(L.sample, L.bounce, 1u, 1u), p, L.seed);
+  const U4 rA = philox4x32_10(u4(wave_sample(L), L.bounce, 0u, 1u), p, L.seed);
+  const U4 rB = philox4x32_10(u4(wave_sample(L), L.bounce, 1u, 1u), p, L.seed);
   const Frame fr = frame_from_normal(n);
   const V3 wo = -d;
   const V3 woT = to_local(fr, wo);
@@ -532,7 +537,7 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   const float cosine = fabsf(dot(n, dirW));
   V3 Tn = T * ((f * cosine) / pdf);
   if (L.bounce > 3) {
-    const U4 rC = philox4x32_10(u4(L.sample, L.bounce, 2u, 1u), p, L.seed);
+    const U4 rC = philox4x32_10(u4(wave_sample(L), L.bounce, 2u, 1u), p, L.seed);
     const float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
     if (u01(rC.x) <= prr) return false;
     Tn = Tn / (1.0f - prr);
@@ -558,7 +563,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   const float S[6] = {c.x, c.y, c.z, c.w, e.x, e.y};
   const Sggx g = make_sggx(S, n);
   const V3 wo = -d;
-  RngStream rs = rng_stream(p, L.seed, L.sample, L.bounce, kPurposeScatter);
+  RngStream rs = rng_stream(p, L.seed, wave_sample(L), L.bounce, kPurposeScatter);
   float4 shO0 = make_float4(0, 0, 0, 0), shO1 = shO0, shD0 = shO0, shD1 = shO0, pre0 = shO0, pre1 = shO0;
   {
     V3 ldir;
@@ -605,7 +610,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   const Ray cr = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, normalize(wi), kDefaultTmax), wi));
   V3 Tn = T;
   if (L.bounce > 3) {
-    const U4 rC = philox4x32_10(u4(L.sample, L.bounce, 2u, 1u), p, L.seed);
+    const U4 rC = philox4x32_10(u4(wave_sample(L), L.bounce, 2u, 1u), p, L.seed);
     const float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
     if (u01(rC.x) <= prr) return false;
     Tn = Tn / (1.0f - prr);
@@ -714,7 +719,7 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
   const V3 p1 = o + d * x.x;
   RngStream rs;
   if (kInline)
-    rs = rng_resume(L.st.q[L.bounce & 1][slot >> 1], L.seed, L.sample, L.bounce, kPurposeShadowTr + (slot & 1u), idx);
+    rs = rng_resume(L.st.q[L.bounce & 1][slot >> 1], L.seed, wave_sample(L), L.bounce, kPurposeShadowTr + (slot & 1u), idx);
   int err = 0;
   for (int k = 0; k < kMaxShadowSegments; ++k) {
     const V3 off = offset_ray_origin(p0, normalize(p1 - p0));
@@ -815,15 +820,22 @@ int resident_blocks(K kernel, int threads) {
   return std::max(1, n) * sm_count();
 }
 
+int g_trackBlocks[4] = {0, 0, 0, 0};  // resident blocks of k_track<dda, sample>, by dda + 2 sample
+
+void query_track_blocks() {
+  if (g_trackBlocks[0] != 0) return;
+  g_trackBlocks[1] = resident_blocks(k_track<true, false>, 128);
+  g_trackBlocks[2] = resident_blocks(k_track<false, true>, 128);
+  g_trackBlocks[3] = resident_blocks(k_track<true, true>, 128);
+  g_trackBlocks[0] = resident_blocks(k_track<false, false>, 128);
+}
+
+__global__ void k_advance_sample(uint32_t* sample) { *sample += 1u; }
+
 void launch_track(const RenderLaunch& L, bool sample, int round, cudaStream_t s) {
-  static int b[4] = {0, 0, 0, 0};
+  query_track_blocks();
   const int which = (L.dda ? 1 : 0) + (sample ? 2 : 0);
-  if (b[which] == 0) {
-    b[0] = resident_blocks(k_track<false, false>, 128);
-    b[1] = resident_blocks(k_track<true, false>, 128);
-    b[2] = resident_blocks(k_track<false, true>, 128);
-    b[3] = resident_blocks(k_track<true, true>, 128);
-  }
+  const int* b = g_trackBlocks;
   switch (which) {
     case 0: k_track<false, false><<<b[0], 128, 0, s>>>(L, round); break;
     case 1: k_track<true, false><<<b[1], 128, 0, s>>>(L, round); break;
@@ -883,8 +895,14 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
   }
   k_finish<<<nblocks, 256, 0, s>>>(L);
   mark(5);
+  if (L.sampleDev) k_advance_sample<<<1, 1, 0, s>>>(L.sampleDev);
   if (tm) tm->n = ev;
   R2_CUDA(cudaGetLastError());
+}
+
+void prepare_render_launches() {
+  query_track_blocks();
+  sm_count();
 }
 
 }  // namespace r2

@@ -77,6 +77,7 @@ struct RenderLaunch {
   float* frame;       // W*H*3 linear RGB, row 0 = bottom (SFrame layout)
   uint32_t npix;
   uint32_t sample;    // sample index of the wave
+  uint32_t* sampleDev;  // nullable: device sample counter of a captured wave (read instead of `sample`)
   uint32_t spp;
   uint32_t maxDepth;
   uint32_t seed;
@@ -96,6 +97,10 @@ struct WaveTimer {
   int n = 0;
 };
 
+// One wave (one sample of every pixel).  With L.sampleDev the last launch
+// advances the device sample counter, so a captured wave replays as the next sample.
 void launch_render_wave(const RenderLaunch& L, int nblocks, cudaStream_t s, WaveTimer* tm = nullptr);
+// Occupancy queries of the persistent kernels, done before any capture.
+void prepare_render_launches();
 
 }  // namespace r2

@@ -91,22 +91,29 @@ void build_env(const float* rgb, int W, int H, EnvHost* e) {
     dist1d(&rad[(size_t)y * W], W, &e->rowFunc[(size_t)y * W], &e->rowCdf[(size_t)y * (W + 1)], &e->rowFuncInt[y]);
 }
 
+RenderContext::RenderContext() {
+  R2_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  R2_CUDA(cudaEventCreate(&ev0));
+  R2_CUDA(cudaEventCreate(&ev1));
+  bound.alloc(1);
+  sampleDev.alloc(1);
+}
+
+RenderContext::~RenderContext() {
+  if (stream) cudaStreamSynchronize(stream);
+  if (timer)
+    for (int i = 0; i < WaveTimer::kMax; ++i) cudaEventDestroy(timer->ev[i]);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (stream) cudaStreamDestroy(stream);
+}
+
 RenderScene::RenderScene() {
-  R2_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  R2_CUDA(cudaEventCreate(&ev0_));
-  R2_CUDA(cudaEventCreate(&ev1_));
   memset(&view_, 0, sizeof(view_));
   if (const char* e = getenv("R2_TRACK_STEPS")) trackSteps_ = (uint32_t)std::max(1l, std::min(1024l, atol(e)));
 }
 
-RenderScene::~RenderScene() {
-  if (stream_) cudaStreamSynchronize(stream_);
-  if (timer_)
-    for (int i = 0; i < WaveTimer::kMax; ++i) cudaEventDestroy(timer_->ev[i]);
-  if (ev0_) cudaEventDestroy(ev0_);
-  if (ev1_) cudaEventDestroy(ev1_);
-  if (stream_) cudaStreamDestroy(stream_);
-}
+RenderScene::~RenderScene() {}
 
 void RenderScene::add_mesh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
                            const r2_material& mat, const float* m2w, uint32_t mask) {
@@ -171,7 +178,7 @@ void RenderScene::add_medium(const char* path, const float* sigmaA, const float*
 
 void RenderScene::commit() {
   R2_REQUIRE(env_.W > 0, R2_ERR_INVALID_CONFIG, "scene has no environment map");
-  cudaStream_t s = stream_;
+  cudaStream_t s = ctx_.stream;
   uint32_t nt = (uint32_t)(hIdx_.size() / 3);
   memset(&view_, 0, sizeof(view_));
   if (nt > 0) {
@@ -239,16 +246,15 @@ void RenderScene::commit() {
   committed_ = true;
 }
 
-void RenderScene::ensure_state(uint32_t n) {
+void RenderContext::ensure(uint32_t n, bool media) {
   if (n > cap_) {
     rayO_.alloc(n); rayD_.alloc(n); T_.alloc(n); L_.alloc(n); hit_.alloc(n);
     shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
     q0_.alloc(n); q1_.alloc(n); shTr_.alloc(2 * (size_t)n);
     counts_.alloc(64);
-    bound_.alloc(1);
     cap_ = n;
   }
-  if (!media_.empty() && n > mediaCap_) {
+  if (media && n > mediaCap_) {
     shX_.alloc(2 * (size_t)n);
     evA_.alloc(n); evB_.alloc(n); evC_.alloc(n); evD_.alloc(n);
     mc_.alloc(16 * 64);
@@ -260,71 +266,105 @@ void RenderScene::ensure_state(uint32_t n) {
   }
 }
 
-void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d_frame, cudaStream_t s,
-                         double* stats) {
+size_t RenderContext::bytes_for(uint32_t n, bool media) {
+  // per path: 5 float4 state + 3 x 2 float4 records + float4 throughput + 2 queue ids + 2 transmittances
+  size_t b = (size_t)n * (5 * 16 + 6 * 16 + 16 + 8 + 8) + 64 * 4;
+  // media: records (4 float4 + float2), shadow tmax/medium, round queues and walk state
+  if (media) b += (size_t)n * (16 + 48 + 8 + 16 + 16 + 64 + 16 + 32 + 16) + 16 * 64 * 4;
+  return b + (size_t)n * 12;  // frame
+}
+
+void RenderContext::fill(PathState* st) const {
+  st->rayO = rayO_.get(); st->rayD = rayD_.get(); st->T = T_.get(); st->L = L_.get(); st->hit = hit_.get();
+  st->q[0] = q0_.get(); st->q[1] = q1_.get(); st->counts = counts_.get();
+  st->shO = shO_.get(); st->shD = shD_.get(); st->shPre = shPre_.get(); st->shT = shT_.get();
+  st->shTr = shTr_.get();
+  if (mediaCap_ > 0) {
+    st->shX = shX_.get();
+    st->evA = evA_.get(); st->evB = evB_.get(); st->evC = evC_.get(); st->evD = evD_.get();
+    st->mc = mc_.get(); st->pj = pj_.get();
+    st->rl[0] = rl0_.get(); st->rl[1] = rl1_.get(); st->cl = cl_.get();
+    st->sl[0] = sl0_.get(); st->sl[1] = sl1_.get();
+    st->jO = jO_.get(); st->jD = jD_.get(); st->jM = jM_.get();
+    st->swP = swP_.get(); st->swM = swM_.get();
+  }
+}
+
+uint32_t RenderContext::bound_hits(cudaStream_t s) {
+  unsigned int b = 0;
+  bound.download(&b, 1, s);
+  R2_CUDA(cudaStreamSynchronize(s));
+  return b;
+}
+
+void RenderScene::check_params(const r2_camera& c, const r2_render_params& p, const float* d_frame) {
   R2_REQUIRE(d_frame, R2_ERR_INVALID_ARGUMENT, "null frame");
   R2_REQUIRE(c.width > 0 && c.height > 0, R2_ERR_INVALID_ARGUMENT, "empty frame");
+  R2_REQUIRE((uint64_t)c.width * c.height < (1ull << 31), R2_ERR_UNSUPPORTED, "frame too large");
   R2_REQUIRE(p.spp > 0, R2_ERR_INVALID_ARGUMENT, "spp must be positive");
   R2_REQUIRE(p.max_depth > 0 && p.max_depth <= 60, R2_ERR_UNSUPPORTED, "max_depth must be in [1, 60]");
   R2_REQUIRE((p.flags & ~R2_RENDER_BRICK_GRID) == 0, R2_ERR_INVALID_ARGUMENT, "unknown render flags");
-  if (!committed_) commit();
-  if (!s) s = stream_;
-  const uint32_t npix = c.width * c.height;
-  ensure_state(npix);
+}
+
+RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera& c, const r2_render_params& p,
+                                      float* d_frame) {
   RenderLaunch L;
   memset(&L, 0, sizeof(L));
   L.scene = view_;
   L.cam = make_camera(c);
-  L.st.rayO = rayO_.get(); L.st.rayD = rayD_.get(); L.st.T = T_.get(); L.st.L = L_.get(); L.st.hit = hit_.get();
-  L.st.q[0] = q0_.get(); L.st.q[1] = q1_.get(); L.st.counts = counts_.get();
-  L.st.shO = shO_.get(); L.st.shD = shD_.get(); L.st.shPre = shPre_.get(); L.st.shT = shT_.get();
-  L.st.shTr = shTr_.get();
-  if (!media_.empty()) {
-    L.st.shX = shX_.get();
-    L.st.evA = evA_.get(); L.st.evB = evB_.get(); L.st.evC = evC_.get(); L.st.evD = evD_.get();
-    L.st.mc = mc_.get(); L.st.pj = pj_.get();
-    L.st.rl[0] = rl0_.get(); L.st.rl[1] = rl1_.get(); L.st.cl = cl_.get(); L.st.sl[0] = sl0_.get(); L.st.sl[1] = sl1_.get();
-    L.st.jO = jO_.get(); L.st.jD = jD_.get(); L.st.jM = jM_.get();
-    L.st.swP = swP_.get(); L.st.swM = swM_.get();
-  }
+  ctx.fill(&L.st);
   L.frame = d_frame;
-  L.npix = npix;
+  L.npix = c.width * c.height;
   L.spp = p.spp;
   L.maxDepth = p.max_depth;
   L.seed = p.seed;
   L.dda = (p.flags & R2_RENDER_BRICK_GRID) ? 1u : 0u;
   L.trackSteps = trackSteps_;
-  L.bound = bound_.get();
-  R2_CUDA(cudaMemsetAsync(bound_.get(), 0, sizeof(unsigned int), s));
-  int nblocks = std::max(1, std::min((int)((npix + 255) / 256), sm_count() * 8));
+  L.bound = ctx.bound.get();
+  return L;
+}
+
+static int wave_blocks(uint32_t npix) { return std::max(1, std::min((int)((npix + 255) / 256), sm_count() * 8)); }
+
+void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d_frame, cudaStream_t s,
+                         double* stats) {
+  check_params(c, p, d_frame);
+  if (!committed_) commit();
+  RenderContext& ctx = ctx_;
+  if (!s) s = ctx.stream;
+  const uint32_t npix = c.width * c.height;
+  ctx.ensure(npix, !media_.empty());
+  RenderLaunch L = make_launch(ctx, c, p, d_frame);
+  R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
+  const int nblocks = wave_blocks(npix);
   R2_CUDA(cudaMemsetAsync(d_frame, 0, sizeof(float) * 3 * (size_t)npix, s));
   if (stats) {
-    statBuf_.reserve(2);
-    R2_CUDA(cudaMemsetAsync(statBuf_.get(), 0, 2 * sizeof(unsigned long long), s));
-    L.stats = statBuf_.get();
-    if (!timer_) {
-      timer_.reset(new WaveTimer());
-      for (int i = 0; i < WaveTimer::kMax; ++i) R2_CUDA(cudaEventCreate(&timer_->ev[i]));
+    ctx.statBuf.reserve(2);
+    R2_CUDA(cudaMemsetAsync(ctx.statBuf.get(), 0, 2 * sizeof(unsigned long long), s));
+    L.stats = ctx.statBuf.get();
+    if (!ctx.timer) {
+      ctx.timer.reset(new WaveTimer());
+      for (int i = 0; i < WaveTimer::kMax; ++i) R2_CUDA(cudaEventCreate(&ctx.timer->ev[i]));
     }
   }
-  R2_CUDA(cudaEventRecord(ev0_, s));
+  R2_CUDA(cudaEventRecord(ctx.ev0, s));
   for (uint32_t smp = 0; smp < p.spp; ++smp) {
     L.sample = smp;
     // the middle wave of a frame is timed kernel by kernel when statistics are requested
-    launch_render_wave(L, nblocks, s, (stats && smp == p.spp / 2) ? timer_.get() : nullptr);
+    launch_render_wave(L, nblocks, s, (stats && smp == p.spp / 2) ? ctx.timer.get() : nullptr);
   }
-  R2_CUDA(cudaEventRecord(ev1_, s));
+  R2_CUDA(cudaEventRecord(ctx.ev1, s));
   if (stats) {
-    R2_CUDA(cudaEventSynchronize(ev1_));
+    R2_CUDA(cudaEventSynchronize(ctx.ev1));
     float ms = 0.0f;
-    R2_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+    R2_CUDA(cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1));
     unsigned long long cnt[2] = {0, 0};
-    R2_CUDA(cudaMemcpy(cnt, statBuf_.get(), sizeof(cnt), cudaMemcpyDeviceToHost));
+    R2_CUDA(cudaMemcpy(cnt, ctx.statBuf.get(), sizeof(cnt), cudaMemcpyDeviceToHost));
     double kms[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = 1; i < timer_->n; ++i) {
+    for (int i = 1; i < ctx.timer->n; ++i) {
       float d = 0.0f;
-      R2_CUDA(cudaEventElapsedTime(&d, timer_->ev[i - 1], timer_->ev[i]));
-      int k = timer_->kind[i];
+      R2_CUDA(cudaEventElapsedTime(&d, ctx.timer->ev[i - 1], ctx.timer->ev[i]));
+      int k = ctx.timer->kind[i];
       if (k >= 0 && k < 6) kms[k] += d;
     }
     stats[0] = (double)npix * p.spp;
@@ -335,12 +375,45 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
   }
 }
 
-uint32_t RenderScene::bound_hits(cudaStream_t s) {
-  if (!bound_.get()) return 0;
-  unsigned int b = 0;
-  bound_.download(&b, 1, s ? s : stream_);
-  R2_CUDA(cudaStreamSynchronize(s ? s : stream_));
-  return b;
+void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame,
+                               cudaStream_t s) {
+  check_params(c, p, d_frame);
+  R2_REQUIRE(committed_, R2_ERR_INVALID_ARGUMENT, "scene not committed");
+  const uint32_t npix = c.width * c.height;
+  ctx.ensure(npix, !media_.empty());
+  RenderLaunch L = make_launch(ctx, c, p, d_frame);
+  L.sampleDev = ctx.sampleDev.get();
+  R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
+  R2_CUDA(cudaMemsetAsync(ctx.sampleDev.get(), 0, sizeof(uint32_t), s));
+  R2_CUDA(cudaMemsetAsync(d_frame, 0, sizeof(float) * 3 * (size_t)npix, s));
+  prepare_render_launches();  // occupancy queries stay outside the capture
+  // one wave (reading its sample index from the device counter, which its
+  // last node advances), captured once and replayed per sample
+  cudaStream_t cap = nullptr;
+  R2_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  struct Guard {
+    cudaStream_t s;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t e = nullptr;
+    ~Guard() {
+      if (e) cudaGraphExecDestroy(e);
+      if (g) cudaGraphDestroy(g);
+      cudaStreamDestroy(s);
+    }
+  } guard{cap};
+  R2_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+  try {
+    launch_render_wave(L, wave_blocks(npix), cap, nullptr);
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(cap, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  R2_CUDA(cudaStreamEndCapture(cap, &guard.g));
+  R2_CUDA(cudaGraphInstantiate(&guard.e, guard.g, 0));
+  for (uint32_t smp = 0; smp < p.spp; ++smp) R2_CUDA(cudaGraphLaunch(guard.e, s));
+  // the executable graph may be destroyed while its launches are pending
 }
 
 }  // namespace r2

@@ -1,6 +1,6 @@
 // Host side of the path tracer: scene assembly (meshes flattened to world
-// space, analytic shapes, environment map with the reference's distributions),
-// camera setup and the per-sample wave loop.
+// space, analytic shapes, media, environment map with the reference's
+// distributions), camera setup, per-render state and the per-sample wave loop.
 #pragma once
 #include <memory>
 #include <vector>
@@ -25,6 +25,44 @@ struct EnvHost {
 };
 void build_env(const float* rgb, int W, int H, EnvHost* e);
 
+// The state of one render in flight: wave buffers (grown on demand), the
+// device sample counter of captured waves, the loop-bound counter, statistics
+// buffers and timers.  Renders that run concurrently use separate contexts.
+class RenderContext {
+ public:
+  RenderContext();
+  ~RenderContext();
+  RenderContext(const RenderContext&) = delete;
+  RenderContext& operator=(const RenderContext&) = delete;
+
+  // Buffers for npix paths (media: the tracking-round state too).
+  void ensure(uint32_t npix, bool media);
+  void fill(PathState* st) const;
+  // Device bytes a render of npix paths needs (buffers + frame).
+  static size_t bytes_for(uint32_t npix, bool media);
+  // Paths and shadow rays of the last render that a loop bound ended (waits for s).
+  uint32_t bound_hits(cudaStream_t s);
+
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DBuf<unsigned int> bound;
+  DBuf<uint32_t> sampleDev;
+  DBuf<unsigned long long> statBuf;
+  std::unique_ptr<WaveTimer> timer;
+
+ private:
+  uint32_t cap_ = 0, mediaCap_ = 0;
+  DBuf<float4> rayO_, rayD_, T_, L_, hit_, shO_, shD_, shPre_, shT_;
+  DBuf<uint32_t> q0_, q1_, counts_;
+  DBuf<float> shTr_;
+  DBuf<float2> shX_, evD_;
+  DBuf<float4> evA_, evB_, evC_;
+  DBuf<uint32_t> mc_, pj_, rl0_, rl1_, sl0_, sl1_, cl_;
+  DBuf<float4> jO_, jD_, swP_;
+  DBuf<uint2> jM_;
+  DBuf<int2> swM_;
+};
+
 class RenderScene {
  public:
   RenderScene();
@@ -41,18 +79,25 @@ class RenderScene {
   void add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
                   const float* orientation, const float* scaling, uint32_t mask, bool hg = false, float g = 0.0f);
   void commit();
-  // One frame: `spp` waves accumulated into d_frame (W*H*3 floats, cleared here).
+  bool committed() const { return committed_; }
+  bool has_media() const { return !media_.empty(); }
+  // One frame: `spp` waves accumulated into d_frame (W*H*3 floats, cleared here),
+  // on the scene's own context.
   void render(const r2_camera& cam, const r2_render_params& p, float* d_frame, cudaStream_t s, double* stats);
-  // Paths and shadow rays of the last frame that a loop bound ended (waits for the stream).
-  uint32_t bound_hits(cudaStream_t s);
-  cudaStream_t stream() const { return stream_; }
+  // The same frame on a caller's context and stream, one wave captured as a
+  // CUDA graph and replayed once per sample (the scene must be committed).
+  void render_graph(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame,
+                    cudaStream_t s);
+  // Paths and shadow rays of the last render() that a loop bound ended (waits for the stream).
+  uint32_t bound_hits(cudaStream_t s) { return ctx_.bound_hits(s ? s : ctx_.stream); }
+  cudaStream_t stream() const { return ctx_.stream; }
   uint32_t ntris() const { return (uint32_t)(hIdx_.size() / 3); }
   const DeviceBvh& bvh() const { return bvh_; }
 
  private:
-  void ensure_state(uint32_t npix);
-  cudaStream_t stream_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  RenderLaunch make_launch(const RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame);
+  static void check_params(const r2_camera& c, const r2_render_params& p, const float* d_frame);
+  RenderContext ctx_;
   bool committed_ = false;
   std::vector<float> hPos_, hNrm_;
   std::vector<uint32_t> hIdx_, hTriMat_;
@@ -69,22 +114,7 @@ class RenderScene {
   DBuf<float4> envTex_;
   DBuf<float> envBuf_;
   SceneView view_;
-  // wave state
-  uint32_t cap_ = 0;
-  DBuf<float4> rayO_, rayD_, T_, L_, hit_, shO_, shD_, shPre_, shT_;
-  DBuf<uint32_t> q0_, q1_, counts_;
-  DBuf<float> shTr_;
-  uint32_t mediaCap_ = 0;
   uint32_t trackSteps_ = 0;  // 0: the kernels' default; R2_TRACK_STEPS overrides
-  DBuf<float2> shX_, evD_;
-  DBuf<float4> evA_, evB_, evC_;
-  DBuf<uint32_t> mc_, pj_, rl0_, rl1_, sl0_, sl1_, cl_;
-  DBuf<float4> jO_, jD_, swP_;
-  DBuf<uint2> jM_;
-  DBuf<int2> swM_;
-  DBuf<unsigned int> bound_;
-  DBuf<unsigned long long> statBuf_;
-  std::unique_ptr<WaveTimer> timer_;
 };
 
 }  // namespace r2
