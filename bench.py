@@ -54,6 +54,7 @@ VOLUME_EXTEND_BYTES_PER_SEGMENT = 116.0
 SHADOW_MEDIA_BYTES_PER_SLOT = 48.0
 SHADE_BYTES_PER_SEGMENT = 256.0
 VOLUME_CFG = dict(grid=256, n_quads=200_000, ico_subdiv=6, width=1920, height=1080, spp=16, depth=16, seed=0)
+SERVE_CFG = dict(jobs=60, rate=40.0, slots=6, budget=40 << 30)
 
 
 def _peaks():
@@ -454,6 +455,130 @@ def bench_volume(args, world, local):
     return out, (desc, cam, prm)
 
 
+def serving_jobs(seed=11):
+    """Config 5 scaled to a bench step: 60 jobs, Poisson arrivals at SERVE_CFG['rate'] per second;
+    70% renders (256^2 .. 1280x720, spp log-uniform in [4, 64], depth 8, on the config-1 and
+    config-2 scenes), 30% filter jobs (64^3 .. 192^3 over foliage of 20k .. 200k triangles, 64 spv,
+    10 iterations)."""
+    rng = np.random.default_rng(seed)
+    c = SERVE_CFG
+    t = 0.0
+    jobs = []
+    sizes = [(256, 256), (384, 384), (512, 512), (1280, 720)]
+    for k in range(c["jobs"]):
+        t += float(rng.exponential(1.0 / c["rate"]))
+        if rng.uniform() < 0.7:
+            w, h = sizes[int(rng.integers(len(sizes)))]
+            spp = int(round(np.exp(rng.uniform(np.log(4), np.log(64)))))
+            jobs.append(("render", t, int(rng.integers(2)), w, h, spp, int(rng.integers(1 << 30))))
+        else:
+            jobs.append(("filter", t, int(rng.integers(3)), int(rng.choice([64, 96, 128, 192])), int(rng.integers(1 << 30))))
+    return jobs
+
+
+def bench_serving(args):
+    """Served (request loop, SERVE_CFG['slots'] slots) against one job at a time on the same GPU."""
+    import threading as th
+
+    import torch
+    from renderer2_b200 import filter as F
+    from renderer2_b200 import raytracer as R
+    from renderer2_b200 import render_scenes as RS
+    from renderer2_b200 import scenes
+    from renderer2_b200 import serving as S
+    c = SERVE_CFG
+    d1, _ = RS.c1_scene()
+    d2, _ = RS.c2_scene()
+    rscenes = [RS.build_scene(d1), RS.build_scene(d2)]
+    cams = [((0, 0, 3), (0, 0, 0)), ((0, 0, 24), (0, 0, 0))]
+    fmat = F.material(diffuse=(0.1, 0.6, 0.1), specular=(0.04, 0.04, 0.04), alpha=0.5, ior=1.5)
+    meshes = [scenes.foliage(n, 10, 0.7, 20 + i) for i, n in enumerate((10_000, 40_000, 100_000))]
+    fscenes = [F.FilterScene(m, fmat) for m in meshes]
+    jobs = serving_jobs()
+
+    def spec(j):
+        if j[0] == "render":
+            _, _, si, w, h, spp, seed = j
+            pos, at = cams[si]
+            return rscenes[si], R.camera(w, h, 45.0, pos, at, (0, 1, 0)), R.params(spp, 8, seed)
+        _, _, fi, n, seed = j
+        return fscenes[fi], fscenes[fi].grid(scenes.voxel_size_for(meshes[fi], n)), \
+            F.params(samples_per_voxel=64, iterations=10, seed=seed)
+
+    specs = [spec(j) for j in jobs]
+    work = [(s[1].width * s[1].height * s[2].spp, 0) if j[0] == "render" else
+            (0, int(np.prod(np.array(s[1].num_voxels[:], np.int64)))) for j, s in zip(jobs, specs)]
+    paths, voxels = sum(w[0] for w in work), sum(w[1] for w in work)
+    arrivals = np.array([j[1] for j in jobs])
+
+    def run_alone(k):
+        s = specs[k]
+        if jobs[k][0] == "render":
+            s[0].render(s[1], s[2])
+        else:
+            nvox = work[k][1]
+            out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+            s[0].run(s[1], s[2], out.data_ptr())
+            out.cpu()
+        torch.cuda.synchronize()
+
+    for k in range(min(4, len(jobs))):  # warm-up (BVH and graph code paths, allocations)
+        run_alone(k)
+    # one job at a time: FIFO on one queue, each job alone on the GPU
+    t0 = time.perf_counter()
+    done_alone = []
+    for k in range(len(jobs)):
+        now = time.perf_counter() - t0
+        if now < arrivals[k]:
+            time.sleep(arrivals[k] - now)
+        run_alone(k)
+        done_alone.append(time.perf_counter() - t0)
+    span_alone = done_alone[-1] - arrivals[0]
+    lat_alone = np.array(done_alone) - arrivals
+    # served: submit at the arrival times, wait for all
+    srv = S.Server(slots=c["slots"], hbm_budget=c["budget"])
+    handles = [None] * len(jobs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for k in range(len(jobs)):
+            now = time.perf_counter() - t0
+            if now < arrivals[k]:
+                time.sleep(arrivals[k] - now)
+            s = specs[k]
+            handles[k] = srv.submit_render(*s) if jobs[k][0] == "render" else srv.submit_filter(*s)
+
+    th_sub = th.Thread(target=submitter)
+    th_sub.start()
+    done_srv = [0.0] * len(jobs)
+    th_sub.join()
+    for k in range(len(jobs)):
+        srv.wait(handles[k], 600.0)
+        done_srv[k] = handles[k].times[2] - handles[k].times[0] + arrivals[k]
+    srv.close()
+    span_srv = max(done_srv) - arrivals[0]
+    lat_srv = np.array(done_srv) - arrivals
+    for sc in rscenes:
+        sc.close()
+    for fs in fscenes:
+        fs.close()
+
+    def pct(a, q):
+        return float(np.percentile(a, q))
+
+    return {"metric": "served paths/s & filtered voxels/s", "unit": "paths/s, voxels/s",
+            "config": {"workload": f"{len(jobs)} jobs, Poisson arrivals at {c['rate']}/s: 70% renders (256^2..1280x720, "
+                                   "spp log-uniform 4..64, depth 8, config-1/config-2 scenes), 30% filters "
+                                   "(64^3..192^3, foliage 10k..100k quads, 64 spv, 10 iterations)",
+                       "slots": c["slots"], "hbm_budget_bytes": c["budget"], "paths": paths, "voxels": voxels},
+            "served": {"paths_per_s": paths / span_srv, "voxels_per_s": voxels / span_srv, "makespan_s": span_srv,
+                       "p50_latency_s": pct(lat_srv, 50), "p99_latency_s": pct(lat_srv, 99)},
+            "one_at_a_time": {"paths_per_s": paths / span_alone, "voxels_per_s": voxels / span_alone,
+                              "makespan_s": span_alone, "p50_latency_s": pct(lat_alone, 50),
+                              "p99_latency_s": pct(lat_alone, 99)},
+            "speedup_makespan": span_alone / span_srv}
+
+
 def run_native(args):
     import torch
     world, rank, local = _dist_setup()
@@ -482,6 +607,7 @@ def run_native(args):
     r = bench_render(args, world, local)
     f = bench_filter(args, world, local) if not args.skip_filter else None
     vol = bench_volume(args, world, local) if not args.skip_volume else None
+    serve = bench_serving(args) if (not args.skip_serving and world == 1) else None
     if rank == 0:
         cpu = cpu_render_sample(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
         line = {"metric": "paths/s", "value": r["value"], "unit": "paths/s", "n_gpus": world, "steps": args.steps,
@@ -506,6 +632,8 @@ def run_native(args):
                 v["cpu_baseline"] = cpu_render_sample(vdesc, vcam, vprm, budget_s=max(5.0, args.cpu_budget / 2))
             line["volume"] = v
             line["gpu_launches"] += v["gpu_launches"]
+        if serve is not None:
+            line["serving"] = serve
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -567,6 +695,9 @@ def run_case(args):
         torch.cuda.synchronize()
         sc.close()
         print(json.dumps({"case": args.case, "voxels": st[0], "candidates": st[1], "ms": st[2]}))
+    elif args.case == "serving":
+        import renderer2_b200  # noqa: F401
+        print(json.dumps(bench_serving(args)))
     elif args.case in ("volume-small", "volume-mid"):
         import tempfile
 
@@ -598,6 +729,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--skip-filter", action="store_true")
     ap.add_argument("--skip-volume", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
     ap.add_argument("--case", default=None, help="profiling case: render-small | filter-small")
     args = ap.parse_args()
