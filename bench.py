@@ -47,13 +47,15 @@ EXTEND_BYTES_PER_SEGMENT = 52.0
 SHADOW_BYTES_PER_SLOT = 33.0
 FILTER_BYTES_PER_VOXEL = 36.0
 # media scenes:
-#   k_extend_media: queue id 4 + ray in/out 64 + throughput in/out 32 + hit record 16 = 116 B per segment
-#   k_shadow<true>: record origin 16 + direction 16 + tmax/medium 8 + queue id 4 + transmittance 4 = 48 B per slot
+#   extend phase (k_resolve rounds, k_track, k_collide): queue id 4 + ray in/out 64 + throughput in/out 32 + hit record 16 = 116 B per segment
+#   shadow phase (k_shadow_resolve rounds, k_track): record origin 16 + direction 16 + tmax/medium 8 + queue id 4 + transmittance 4 = 48 B per slot
 #   k_shade<true>: hit 16 + ray 32 + throughput 16 + radiance 16 + 2 records x 64 + continuation 48 = 256 B per segment
 VOLUME_EXTEND_BYTES_PER_SEGMENT = 116.0
 SHADOW_MEDIA_BYTES_PER_SLOT = 48.0
 SHADE_BYTES_PER_SEGMENT = 256.0
 VOLUME_CFG = dict(grid=256, n_quads=200_000, ico_subdiv=6, width=1920, height=1080, spp=16, depth=16, seed=0)
+VOLUME_BATCH_CFG = dict(scenes=16, grids=(128, 192, 256, 160), quads=(50_000, 150_000, 300_000), ico=(6, 7),
+                        width=1920, height=1080, spp=2, depth=16)
 SERVE_CFG = dict(jobs=60, rate=40.0, slots=6, budget=40 << 30)
 
 
@@ -157,7 +159,7 @@ def _barrier(world: int):
 def render_workload():
     from renderer2_b200 import render_scenes as RS
     from renderer2_b200 import raytracer as R
-    desc, cam = RS.c2_scene()
+    desc, cam = RS.icosphere_grid_scene()
     c = RENDER_CFG
     cam = R.camera(c["width"], c["height"], 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
     prm = R.params(c["spp"], c["depth"], c["seed"])
@@ -243,6 +245,7 @@ def bench_render(args, world, local):
     from renderer2_b200 import render_scenes as RS
     desc, cam, prm = render_workload()
     sc = RS.build_scene(desc)
+    tuning = sc.autotune(cam, prm).as_tuple()  # set-up: launch tuning of this frame (never changes the image)
     npix = cam.width * cam.height
     frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
@@ -281,7 +284,7 @@ def bench_render(args, world, local):
         kname = "k_extend"
     else:
         alg = SHADOW_BYTES_PER_SLOT * sh_wave
-        kname = "k_shadow"
+        kname = "k_shadow_surfaces"
     kms = ms_wave[dom]
     launches = prm.max_depth
     achieved = alg / (kms / 1e3) / 1e9
@@ -310,7 +313,7 @@ def bench_render(args, world, local):
            "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms}
     sc.close()
     launches_per_step = prm.spp * (2 + 4 * prm.max_depth)
-    return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths,
+    return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths, tuning=tuning,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
                 desc=desc, cam=cam, prm=prm)
 
@@ -376,7 +379,7 @@ def bench_filter(args, world, local):
 
 
 def bench_volume(args, world, local):
-    """Config 4 leg: one batched-volume scene (filtered 256^3 foliage medium +
+    """Volume leg: one batched-volume scene (filtered 256^3 foliage medium +
     81,920-tri mesh), 1920x1080, depth 16, brick-grid DDA tracking."""
     import tempfile
 
@@ -389,6 +392,7 @@ def bench_volume(args, world, local):
                                 width=c["width"], height=c["height"])
     prm = R.params(c["spp"], c["depth"], c["seed"], brick_grid=True)
     sc = RS.build_scene(desc)
+    tuning = sc.autotune(cam, prm).as_tuple()
     npix = cam.width * cam.height
     frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
@@ -415,8 +419,8 @@ def bench_volume(args, world, local):
     ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
     seg_wave = seg / prm.spp
     dom = max(("extend", "shadow", "shade"), key=lambda k: ms_wave[k])
-    per_unit = {"extend": (VOLUME_EXTEND_BYTES_PER_SEGMENT, seg_wave, "k_extend_media"),
-                "shadow": (SHADOW_MEDIA_BYTES_PER_SLOT, 2.0 * seg_wave, "k_shadow<true>"),
+    per_unit = {"extend": (VOLUME_EXTEND_BYTES_PER_SEGMENT, seg_wave, "extend phase"),
+                "shadow": (SHADOW_MEDIA_BYTES_PER_SLOT, 2.0 * seg_wave, "shadow phase"),
                 "shade": (SHADE_BYTES_PER_SEGMENT, seg_wave, "k_shade<true>")}[dom]
     alg = per_unit[0] * per_unit[1]
     kms = ms_wave[dom]
@@ -447,18 +451,103 @@ def bench_volume(args, world, local):
                                   f"{c['grid']}^3 (SGGX medium, brick-grid DDA) + {20 * 4 ** c['ico_subdiv']}-tri "
                                   f"mesh, {c['width']}x{c['height']}, {c['spp']} spp per step, depth {c['depth']}",
                       "paths_per_step": paths, "segments_per_step": seg, "shadow_rays_per_step": shadow,
-                      "l2": "wave state larger than L2"},
+                      "l2": "wave state larger than L2",
+                      "tuning": dict(zip(("track_steps", "trav_visits", "trav_refill"), tuning))},
            "roofline": roofline,
            "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms},
-           "gpu_launches": prm.spp * (2 + 4 * prm.max_depth) * args.steps}
+           # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, shade, 3 shadow resolve, accum
+           "gpu_launches": prm.spp * (2 + 13 * prm.max_depth) * args.steps}
     return out, (desc, cam, prm)
 
 
+def bench_volume_batch(args, world, local):
+    """Batched volume leg: VOLUME_BATCH_CFG['scenes'] scenes (foliage grids of uneven size and
+    occupancy filtered on the GPU, icosphere meshes of 82k or 328k triangles), 1920x1080, depth 16,
+    brick-grid DDA, all rendered by one captured CUDA graph (a wave of every scene per replay);
+    against the same frames rendered one scene after the other."""
+    import shutil
+    import tempfile
+
+    import torch
+    from renderer2_b200 import raytracer as R
+    from renderer2_b200 import render_scenes as RS
+    c = VOLUME_BATCH_CFG
+    work = tempfile.mkdtemp(prefix="r2vb")
+    descs, cams, prms = [], [], []
+    for i in range(c["scenes"]):
+        d, cam = RS.volume_scene(work, 100 + i, grid=c["grids"][i % len(c["grids"])],
+                                 n_quads=c["quads"][(i // 2) % len(c["quads"])], ico_subdiv=c["ico"][i % 2],
+                                 width=c["width"], height=c["height"])
+        descs.append(d)
+        cams.append(cam)
+        prms.append(R.params(c["spp"], c["depth"], i, brick_grid=True))
+    scs = [RS.build_scene(d) for d in descs]
+    tuned = scs[0].autotune(cams[0], prms[0])  # one scene's choice applies to all
+    for sc in scs[1:]:
+        sc.set_tuning(tuned)
+    npix = [cm.width * cm.height for cm in cams]
+    frames = [torch.empty(n * 3, dtype=torch.float32, device="cuda") for n in npix]
+    batch = R.RenderBatch(scs, cams, prms, [f.data_ptr() for f in frames])
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup):
+        batch.run(stream, timing=False)
+        for sc, cm, p, f in zip(scs, cams, prms, frames):
+            sc.render_device(cm, p, f.data_ptr(), stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ev[0].record()
+    for _ in range(args.steps):
+        # 16 scenes' wave state (~1 GB each) and media exceed L2; no flush needed
+        batch.run(stream, timing=False)
+    ev[1].record()
+    for _ in range(args.steps):
+        for sc, cm, p, f in zip(scs, cams, prms, frames):
+            sc.render_device(cm, p, f.data_ptr(), stream)
+    ev[2].record()
+    torch.cuda.synchronize()
+    _barrier(world)
+    ms_batch = _max_over_ranks(ev[0].elapsed_time(ev[1]), world)
+    ms_seq = _max_over_ranks(ev[1].elapsed_time(ev[2]), world)
+    paths = sum(npix) * c["spp"]
+    # end to end: upload every scene (media read from their files), one batch, frames back to the host
+    h2d = sum(_input_bytes(d) + sum(os.path.getsize(m[0] + e) for m in d["media"] for e in (".nvdb", ".brickgrid"))
+              for d in descs)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = [RS.build_scene(d) for d in descs]
+    b2 = R.RenderBatch(s2, cams, prms, [f.data_ptr() for f in frames])
+    b2.run(stream, timing=False)
+    host = [f.cpu().numpy() for f in frames]
+    e2e_ms = _max_over_ranks((time.perf_counter() - t0) * 1e3, world)
+    b2.close()
+    for s in s2:
+        s.close()
+    batch.close()
+    for s in scs:
+        s.close()
+    del host
+    shutil.rmtree(work, ignore_errors=True)
+    return {"metric": "paths/s", "value": world * paths * args.steps / (ms_batch / 1e3), "unit": "paths/s",
+            "ms_per_step": ms_batch / args.steps,
+            "config": {"workload": f"{c['scenes']} batched volume scenes: foliage grids {c['grids']}^3 of "
+                                   f"{c['quads']} quads (SGGX media, brick-grid DDA) + icosphere meshes "
+                                   f"(81,920 / 327,680 tris), {c['width']}x{c['height']}, {c['spp']} spp per step, "
+                                   f"depth {c['depth']}, one captured graph per sample",
+                       "paths_per_step": paths, "l2": "wave state larger than L2"},
+            "one_scene_at_a_time": {"value": world * paths * args.steps / (ms_seq / 1e3),
+                                    "ms_per_step": ms_seq / args.steps},
+            "speedup_vs_one_at_a_time": ms_seq / ms_batch,
+            "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(sum(npix) * 12), "ms_per_step": e2e_ms},
+            "gpu_launches": c["spp"] * c["scenes"] * (3 + 13 * c["depth"]) * args.steps}
+
+
 def serving_jobs(seed=11):
-    """Config 5 scaled to a bench step: 60 jobs, Poisson arrivals at SERVE_CFG['rate'] per second;
-    70% renders (256^2 .. 1280x720, spp log-uniform in [4, 64], depth 8, on the config-1 and
-    config-2 scenes), 30% filter jobs (64^3 .. 192^3 over foliage of 20k .. 200k triangles, 64 spv,
+    """The serving mix scaled to a bench step: 60 jobs, Poisson arrivals at SERVE_CFG['rate'] per second;
+    70% renders (256^2 .. 1280x720, spp log-uniform in [4, 64], depth 8, on the small icosphere and
+    the icosphere-grid scenes), 30% filter jobs (64^3 .. 192^3 over foliage of 20k .. 200k triangles, 64 spv,
     10 iterations)."""
     rng = np.random.default_rng(seed)
     c = SERVE_CFG
@@ -487,8 +576,8 @@ def bench_serving(args):
     from renderer2_b200 import scenes
     from renderer2_b200 import serving as S
     c = SERVE_CFG
-    d1, _ = RS.c1_scene()
-    d2, _ = RS.c2_scene()
+    d1, _ = RS.icosphere_scene()
+    d2, _ = RS.icosphere_grid_scene()
     rscenes = [RS.build_scene(d1), RS.build_scene(d2)]
     cams = [((0, 0, 3), (0, 0, 0)), ((0, 0, 24), (0, 0, 0))]
     fmat = F.material(diffuse=(0.1, 0.6, 0.1), specular=(0.04, 0.04, 0.04), alpha=0.5, ior=1.5)
@@ -568,7 +657,7 @@ def bench_serving(args):
 
     return {"metric": "served paths/s & filtered voxels/s", "unit": "paths/s, voxels/s",
             "config": {"workload": f"{len(jobs)} jobs, Poisson arrivals at {c['rate']}/s: 70% renders (256^2..1280x720, "
-                                   "spp log-uniform 4..64, depth 8, config-1/config-2 scenes), 30% filters "
+                                   "spp log-uniform 4..64, depth 8, icosphere / icosphere-grid scenes), 30% filters "
                                    "(64^3..192^3, foliage 10k..100k quads, 64 spv, 10 iterations)",
                        "slots": c["slots"], "hbm_budget_bytes": c["budget"], "paths": paths, "voxels": voxels},
             "served": {"paths_per_s": paths / span_srv, "voxels_per_s": voxels / span_srv, "makespan_s": span_srv,
@@ -607,6 +696,7 @@ def run_native(args):
     r = bench_render(args, world, local)
     f = bench_filter(args, world, local) if not args.skip_filter else None
     vol = bench_volume(args, world, local) if not args.skip_volume else None
+    vbatch = bench_volume_batch(args, world, local) if not args.skip_volume else None
     serve = bench_serving(args) if (not args.skip_serving and world == 1) else None
     if rank == 0:
         cpu = cpu_render_sample(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
@@ -617,7 +707,8 @@ def run_native(args):
                                        "lognormal(0,1.5) env, 1024x1024, 64 spp, max depth 8",
                            "paths_per_step": r["paths"], "segments_per_step": r["segments_per_frame"],
                            "shadow_rays_per_step": r["shadow_rays_per_frame"],
-                           "l2": "inputs + wave state larger than L2", "parallelism": f"replicas x{world}"},
+                           "l2": "inputs + wave state larger than L2", "parallelism": f"replicas x{world}",
+                           "tuning": dict(zip(("track_steps", "trav_visits", "trav_refill"), r["tuning"]))},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"]}
         if f is not None:
@@ -632,6 +723,9 @@ def run_native(args):
                 v["cpu_baseline"] = cpu_render_sample(vdesc, vcam, vprm, budget_s=max(5.0, args.cpu_budget / 2))
             line["volume"] = v
             line["gpu_launches"] += v["gpu_launches"]
+        if vbatch is not None:
+            line["volume_batch"] = vbatch
+            line["gpu_launches"] += vbatch["gpu_launches"]
         if serve is not None:
             line["serving"] = serve
         print(json.dumps(line), flush=True)
@@ -673,7 +767,7 @@ def run_case(args):
     if args.case == "render-small":
         from renderer2_b200 import render_scenes as RS
         from renderer2_b200 import raytracer as R
-        desc, _ = RS.c2_scene()
+        desc, _ = RS.icosphere_grid_scene()
         cam = R.camera(256, 256, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
         sc = RS.build_scene(desc)
         frame = torch.empty(256 * 256 * 3, dtype=torch.float32, device="cuda")
@@ -681,6 +775,17 @@ def run_case(args):
         torch.cuda.synchronize()
         sc.close()
         print(json.dumps({"case": args.case, "paths": st[0], "ms": st[1]}))
+    elif args.case == "render-wave":
+        # one wave of the headline frame: the same launches (1M paths per bounce) as a bench step
+        desc, cam, prm = render_workload()
+        from renderer2_b200 import render_scenes as RS
+        from renderer2_b200 import raytracer as R
+        sc = RS.build_scene(desc)
+        frame = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
+        st = sc.render_device(cam, R.params(1, prm.max_depth, 0), frame.data_ptr())
+        torch.cuda.synchronize()
+        sc.close()
+        print(json.dumps({"case": args.case, "paths": st[0], "segments": st[2], "shadow_rays": st[3], "ms": st[1]}))
     elif args.case == "filter-small":
         from renderer2_b200 import filter as F
         from renderer2_b200 import scenes
@@ -698,6 +803,10 @@ def run_case(args):
     elif args.case == "serving":
         import renderer2_b200  # noqa: F401
         print(json.dumps(bench_serving(args)))
+    elif args.case == "volume-batch":
+        import renderer2_b200  # noqa: F401
+        args.steps, args.warmup = 1, 1
+        print(json.dumps(bench_volume_batch(args, 1, 0)))
     elif args.case in ("volume-small", "volume-mid"):
         import tempfile
 

@@ -221,6 +221,15 @@ typedef struct r2_render_params {
   uint32_t flags;      /* R2_RENDER_* bits */
 } r2_render_params;
 
+/* Launch tuning of a scene's renders.  No image depends on it: every setting
+ * gives the same frames bit for bit.  0 selects the built-in default. */
+typedef struct r2_render_tuning {
+  uint32_t track_steps; /* media: tracking steps a lane of the persistent tracker takes between refills (1..1024) */
+  uint32_t trav_visits; /* BVH node/leaf visits a lane takes between refill checks of the surface kernels */
+  uint32_t trav_refill; /* finished lanes of a warp (1..32) that make it take new rays */
+  uint32_t reserved;    /* 0 */
+} r2_render_tuning;
+
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA
  * (CNVDBMedium::sampleDDA / trDDA, nvdb_medium_impl.hpp:139-187, 248-294)
  * instead of the global majorant (sampleInternal / trInternal, 94-137, 203-239). */
@@ -273,6 +282,37 @@ r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_re
 /* Same through host memory: commits if needed, renders, copies the frame to
  * rgb; loop bounds are reported as in r2_render_device. */
 r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* rgb);
+
+/* The scene's launch tuning (initially the defaults, or the environment's
+ * R2_TRACK_STEPS / R2_TRAV_VISITS / R2_TRAV_REFILL). */
+r2_status r2_scene_set_tuning(r2_scene* scene, const r2_render_tuning* tuning);
+r2_status r2_scene_get_tuning(r2_scene* scene, r2_render_tuning* tuning);
+/* Autotuner: times one wave of this frame for each candidate value of one
+ * setting at a time (scenes without media: refill lanes, then visits; with
+ * media: tracking steps), keeps a candidate that is faster by more than 2 %,
+ * and stores the result as the scene's tuning (also written to tuning_out,
+ * nullable).  Commits the scene if needed; waits. */
+r2_status r2_scene_autotune(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
+                            r2_render_tuning* tuning_out);
+
+/* Frames of n committed scenes (a scene may appear more than once) rendered
+ * together by one captured CUDA graph holding one wave of every frame, each on
+ * a branch of its own so that their kernels overlap; the graph is replayed
+ * once per sample.  The reference renders one scene per process
+ * (CPipeline::run, pipeline.cu:18-90); a batch is how many scenes share one
+ * GPU.  Every frame equals r2_render_device's with the same arguments.
+ * Cameras, parameters (all with the same spp) and device frames d_rgb[i]
+ * (width*height*3 floats) are fixed at creation; the scenes must outlive the
+ * batch. */
+typedef struct r2_render_batch r2_render_batch;
+r2_status r2_render_batch_create(r2_scene* const* scenes, const r2_camera* cameras, const r2_render_params* params,
+                                 float* const* d_rgb, uint32_t n, r2_render_batch** out);
+r2_status r2_render_batch_destroy(r2_render_batch* batch);
+/* Clears and renders every frame on stream (null: the default stream).  With
+ * ms_out the call waits, stores the device milliseconds of all samples and
+ * returns R2_ERR_DEVICE_TIMEOUT (frames still written) if a loop bound ended
+ * any path, as r2_render_device does. */
+r2_status r2_render_batch_run(r2_render_batch* batch, void* stream, double* ms_out);
 
 /* ------------------------------------------------------------------------ */
 /* Pipeline: config.json + scenedescription.json.

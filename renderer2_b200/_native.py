@@ -82,6 +82,12 @@ def _load():
         "r2_scene_commit": (C.c_int, [P]),
         "r2_render_device": (C.c_int, [P, P, P, P, P, P]),
         "r2_render_host": (C.c_int, [P, P, P, P]),
+        "r2_scene_set_tuning": (C.c_int, [P, P]),
+        "r2_scene_get_tuning": (C.c_int, [P, P]),
+        "r2_scene_autotune": (C.c_int, [P, P, P, P]),
+        "r2_render_batch_create": (C.c_int, [P, P, P, P, u32, P]),
+        "r2_render_batch_destroy": (C.c_int, [P]),
+        "r2_render_batch_run": (C.c_int, [P, P, P]),
         "r2_server_create": (C.c_int, [u32, C.c_uint64, P]),
         "r2_server_destroy": (C.c_int, [P]),
         "r2_server_submit_render": (C.c_int, [P, P, P, P, P, P]),

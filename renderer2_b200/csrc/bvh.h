@@ -123,23 +123,38 @@ R2_HD int bvh_leaf_ref(int first, int count) { return ~(first | (count << 26)); 
 R2_HD int bvh_leaf_first(int ref) { return (~ref) & 0x03FFFFFF; }
 R2_HD int bvh_leaf_count(int ref) { return ((~ref) >> 26) & 0x1F; }
 
-// Closest hit in (0, tmax] (kAnyHit: first hit found).  `tri` of the result is
-// the BVH-order index, -1 on a miss.  Stack entries hold child references with
-// their entry distance; leaves are tested when reached.  The builder bounds the
-// tree depth by R2_BVH_STACK so the stack cannot overflow.
-template <bool kAnyHit>
-R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax) {
+// A ray's traversal that can stop after any node or leaf and resume later:
+// the per-ray constants, the best hit so far, the node to visit next and the
+// depth of the caller-held stack.
+struct TraceState {
+  RayPre r;
   Hit best;
-  best.t = tmax;
-  best.b1 = best.b2 = 0.0f;
-  best.tri = 0x7FFFFFFF;
-  const RayPre r = make_ray_pre(o, d);
-  int stack[R2_BVH_STACK];
-  float stackT[R2_BVH_STACK];
-  int sp = 0;
-  int cur = 0;  // root is internal node 0
-  bool found = false;
-  while (true) {
+  int cur;
+  int sp;
+  int found;
+};
+
+R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax) {
+  s.r = make_ray_pre(o, d);
+  s.best.t = tmax;
+  s.best.b1 = s.best.b2 = 0.0f;
+  s.best.tri = 0x7FFFFFFF;
+  s.cur = 0;  // root is internal node 0
+  s.sp = 0;
+  s.found = 0;
+}
+
+// Visits up to maxVisits nodes or leaves; true when the query has finished
+// (closest hit in (0, tmax], kAnyHit: the first hit found) with s.best.tri the
+// BVH-order index, -1 on a miss.  Stack entries hold child references with
+// their entry distance; leaves are tested when reached.  The builder bounds the
+// tree depth by R2_BVH_STACK so the stack cannot overflow.  The visiting order
+// does not depend on where the visits are split, and the closest hit does not
+// depend on the visiting order.
+template <bool kAnyHit>
+R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* stackT, int maxVisits) {
+  for (int v = 0; v < maxVisits; ++v) {
+    const int cur = s.cur;
     if (cur >= 0) {
 #if defined(__CUDA_ARCH__)
       const float4 b0 = __ldg(&bvh.nodes[cur].b0);
@@ -153,22 +168,22 @@ R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax) {
       const int4 ch = bvh.nodes[cur].ch;
 #endif
       float t0 = 0.0f, t1 = 0.0f;
-      const bool h0 = slab(r, b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, best.t, &t0);
-      const bool h1 = (ch.y != R2_BVH_NONE) && slab(r, b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, best.t, &t1);
+      const bool h0 = slab(s.r, b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, s.best.t, &t0);
+      const bool h1 = (ch.y != R2_BVH_NONE) && slab(s.r, b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, s.best.t, &t1);
       if (h0 && h1) {
         int nearC = ch.x, farC = ch.y;
         float farT = t1;
         if (t1 < t0) { nearC = ch.y; farC = ch.x; farT = t0; }
-        stack[sp] = farC;
-        stackT[sp] = farT;
-        ++sp;
-        cur = nearC;
+        stack[s.sp] = farC;
+        stackT[s.sp] = farT;
+        ++s.sp;
+        s.cur = nearC;
         continue;
       } else if (h0) {
-        cur = ch.x;
+        s.cur = ch.x;
         continue;
       } else if (h1) {
-        cur = ch.y;
+        s.cur = ch.y;
         continue;
       }
     } else {
@@ -185,23 +200,36 @@ R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax) {
         const float4 b = bvh.tris[3 * tri + 1];
         const float4 c = bvh.tris[3 * tri + 2];
 #endif
-        if (tri_test(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &best)) {
-          found = true;
-          if (kAnyHit) return best;
+        if (tri_test(s.r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &s.best)) {
+          s.found = 1;
+          if (kAnyHit) return true;
         }
       }
     }
     // pop the next child whose entry distance is not beyond the closest hit
     while (true) {
-      if (sp == 0) {
-        if (!found) best.tri = -1;
-        return best;
+      if (s.sp == 0) {
+        if (!s.found) s.best.tri = -1;
+        return true;
       }
-      --sp;
-      if (stackT[sp] <= best.t) break;
+      --s.sp;
+      if (stackT[s.sp] <= s.best.t) break;
     }
-    cur = stack[sp];
+    s.cur = stack[s.sp];
   }
+  return false;
+}
+
+// The whole query at once.
+template <bool kAnyHit>
+R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax) {
+  TraceState s;
+  trace_begin(s, o, d, tmax);
+  int stack[R2_BVH_STACK];
+  float stackT[R2_BVH_STACK];
+  while (!trace_advance<kAnyHit>(bvh, s, stack, stackT, 1 << 30)) {
+  }
+  return s.best;
 }
 
 }  // namespace r2

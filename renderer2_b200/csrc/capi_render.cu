@@ -8,6 +8,10 @@ struct r2_scene {
   std::unique_ptr<r2::RenderScene> impl;
 };
 
+struct r2_render_batch {
+  std::unique_ptr<r2::RenderBatch> impl;
+};
+
 r2::RenderScene* r2_scene_impl(r2_scene* scene) { return scene->impl.get(); }
 
 extern "C" {
@@ -104,6 +108,71 @@ r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_rend
   R2_CUDA(cudaStreamSynchronize(s));
   const uint32_t b = scene->impl->bound_hits(s);
   R2_REQUIRE(b == 0, R2_ERR_DEVICE_TIMEOUT, std::to_string(b) + " paths or shadow rays ended by a loop bound");
+  R2_API_END
+}
+
+r2_status r2_scene_set_tuning(r2_scene* scene, const r2_render_tuning* tuning) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && tuning, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->set_tuning(*tuning);
+  R2_API_END
+}
+
+r2_status r2_scene_get_tuning(r2_scene* scene, r2_render_tuning* tuning) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && tuning, R2_ERR_INVALID_ARGUMENT, "null argument");
+  *tuning = scene->impl->tuning();
+  R2_API_END
+}
+
+r2_status r2_scene_autotune(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
+                            r2_render_tuning* tuning_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && camera && params, R2_ERR_INVALID_ARGUMENT, "null argument");
+  const r2_render_tuning t = scene->impl->autotune(*camera, *params);
+  if (tuning_out) *tuning_out = t;
+  R2_API_END
+}
+
+r2_status r2_render_batch_create(r2_scene* const* scenes, const r2_camera* cameras, const r2_render_params* params,
+                                 float* const* d_rgb, uint32_t n, r2_render_batch** out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scenes && cameras && params && d_rgb && out, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(n > 0, R2_ERR_INVALID_ARGUMENT, "empty batch");
+  std::vector<r2::RenderScene*> sc(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    R2_REQUIRE(scenes[i], R2_ERR_INVALID_ARGUMENT, "null scene in batch");
+    sc[i] = scenes[i]->impl.get();
+  }
+  auto b = new r2_render_batch;
+  try {
+    b->impl.reset(new r2::RenderBatch(sc, std::vector<r2_camera>(cameras, cameras + n),
+                                      std::vector<r2_render_params>(params, params + n),
+                                      std::vector<float*>(d_rgb, d_rgb + n)));
+  } catch (...) {
+    delete b;
+    throw;
+  }
+  *out = b;
+  R2_API_END
+}
+
+r2_status r2_render_batch_destroy(r2_render_batch* batch) {
+  R2_API_BEGIN
+  delete batch;
+  R2_API_END
+}
+
+r2_status r2_render_batch_run(r2_render_batch* batch, void* stream, double* ms_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(batch, R2_ERR_INVALID_ARGUMENT, "null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  const double ms = batch->impl->run(s, ms_out != nullptr);
+  if (ms_out) {
+    *ms_out = ms;
+    const uint32_t b = batch->impl->bound_hits(s);
+    R2_REQUIRE(b == 0, R2_ERR_DEVICE_TIMEOUT, std::to_string(b) + " paths or shadow rays ended by a loop bound");
+  }
   R2_API_END
 }
 

@@ -36,7 +36,6 @@ constexpr uint32_t kPurposeShadowTr = 0x200u;  // + shadow slot (0 light, 1 BSDF
 constexpr int kMaxPassThrough = 64;            // medium boundaries crossed within one bounce
 constexpr int kMaxShadowSegments = 256;        // medium boundaries along one shadow ray (per round)
 constexpr int kMediaRounds = 2;                // queued tracking rounds per bounce before the inline round
-constexpr uint32_t kDefaultTrackSteps = 8;     // tracking steps a lane takes between refills
 // Media counters of a bounce (PathState::mc): [3r] segments queued in round r,
 // [3r+1] segments taken, [3r+2] entries of list r + 1; path extension at 0,
 // shadows at kShadowCounters.
@@ -54,18 +53,16 @@ __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
 
 // Closest hit over triangles, analytic shapes and (kMedia) medium boxes.
 // Code: >= 0 triangle, -1 miss, -2 - i shape i, kMediumCodeBase - m medium m.
+// scene_closest_after finishes the query from the triangles' result h.
 template <bool kMedia>
-__device__ __forceinline__ float4 scene_closest(const SceneView& S, V3 o, V3 d, float tmax) {
+__device__ __forceinline__ float4 scene_closest_after(const SceneView& S, V3 o, V3 d, float tmax, const Hit& h) {
   float t = tmax, b1 = 0.0f, b2 = 0.0f;
   int code = -1;
-  if (S.hasTris) {
-    Hit h = bvh_trace<false>(S.bvh, o, d, tmax);
-    if (h.tri >= 0) {
-      t = h.t;
-      b1 = h.b1;
-      b2 = h.b2;
-      code = h.tri;
-    }
+  if (h.tri >= 0) {
+    t = h.t;
+    b1 = h.b1;
+    b2 = h.b2;
+    code = h.tri;
   }
   for (int i = 0; i < S.nshapes; ++i) {
     const Shape& sh = S.shapes[i];
@@ -115,6 +112,14 @@ __device__ __forceinline__ float4 scene_closest(const SceneView& S, V3 o, V3 d, 
   return make_float4(t, b1, b2, __int_as_float(code));
 }
 
+template <bool kMedia>
+__device__ __forceinline__ float4 scene_closest(const SceneView& S, V3 o, V3 d, float tmax) {
+  Hit h;
+  h.tri = -1;
+  if (S.hasTris) h = bvh_trace<false>(S.bvh, o, d, tmax);
+  return scene_closest_after<kMedia>(S, o, d, tmax, h);
+}
+
 // Any surface (triangle or shape) along the ray.
 __device__ __forceinline__ bool scene_occluded(const SceneView& S, V3 o, V3 d, float tmax) {
   if (S.hasTris) {
@@ -159,15 +164,76 @@ __global__ void __launch_bounds__(256) k_camera(RenderLaunch L) {
   if (blockIdx.x == 0 && threadIdx.x == 0) L.st.counts[0] = L.npix;
 }
 
+// Persistent BVH traversal with dynamic ray fetch (Aila and Laine,
+// "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009): the
+// lanes of a warp run their rays in rounds of `visits` node/leaf visits, and
+// as soon as `refill` lanes have finished (or all of them) the warp takes as
+// many new items from the queue with one atomic, so that lanes do not idle
+// behind the warp's longest ray.  begin(k, s, &item) starts item k (false: it
+// needed no traversal and is done); end(item, s) consumes a finished query.
+// Results do not depend on visits or refill.
+template <bool kAnyHit, class Begin, class End>
+__device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n, uint32_t* taken, int visits,
+                                                 int refill, Begin begin, End end) {
+  int stack[R2_BVH_STACK];
+  float stackT[R2_BVH_STACK];
+  TraceState s;
+  uint32_t item = 0;
+  bool active = false;
+  bool more = true;  // warp-uniform: the queue may still hold items
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    if (more) {
+      const unsigned idle = __ballot_sync(0xffffffffu, !active);
+      const int nIdle = __popc(idle);
+      if (nIdle >= refill || idle == 0xffffffffu) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(taken, (uint32_t)nIdle);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base + (uint32_t)nIdle >= n) more = false;
+        if (!active) {
+          const uint32_t k = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
+          if (k < n) active = begin(k, s, &item);
+        }
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0) {
+      if (!more) break;
+      continue;
+    }
+    if (active && trace_advance<kAnyHit>(bvh, s, stack, stackT, visits)) {
+      end(item, s);
+      active = false;
+    }
+  }
+}
+
+__device__ __forceinline__ int trav_visits(const RenderLaunch& L) { return (int)max(1u, L.travVisits); }
+__device__ __forceinline__ int trav_refill(const RenderLaunch& L) { return (int)min(32u, max(1u, L.travRefill)); }
+
+// Closest hit of every live path (scenes without media).
 __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
   const uint32_t* q = L.st.q[L.bounce & 1];
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    const uint32_t p = q[i];
-    const V3 o = xyz(L.st.rayO[p]), d = xyz(L.st.rayD[p]);
-    L.st.hit[p] = scene_closest<false>(L.scene, o, d, kDefaultTmax);
+  if (!L.scene.hasTris) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+      const uint32_t p = q[i];
+      L.st.hit[p] = scene_closest<false>(L.scene, xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), kDefaultTmax);
+    }
+    return;
   }
+  auto begin = [&](uint32_t k, TraceState& s, uint32_t* item) {
+    const uint32_t p = q[k];
+    *item = p;
+    trace_begin(s, xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), kDefaultTmax);
+    return true;
+  };
+  auto end = [&](uint32_t p, const TraceState& s) {
+    L.st.hit[p] = scene_closest_after<false>(L.scene, s.r.o, s.r.d, kDefaultTmax, s.best);
+  };
+  trace_persistent<false>(L.scene.bvh, n, &L.st.counts[kTravCounters + 2 * L.bounce], trav_visits(L),
+                          trav_refill(L), begin, end);
 }
 
 // ------------------------------------------------------------------ media: path extension
@@ -663,20 +729,49 @@ __global__ void __launch_bounds__(128) k_shade(RenderLaunch L) {
 // Visibility of every shadow record of a scene without media.
 __global__ void __launch_bounds__(128) k_shadow_surfaces(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += stride) {
-    const float4 o = L.st.shO[j];
-    float tr = 0.0f;
-    const bool traced = o.w > 0.0f;
-    if (traced) tr = scene_occluded(L.scene, xyz(o), xyz(L.st.shD[j]), kDefaultTmax) ? 0.0f : 1.0f;
-    L.st.shTr[j] = tr;
-    if (L.stats) {
-      const unsigned m = __ballot_sync(__activemask(), traced);
-      if ((threadIdx.x & 31) == (unsigned)(__ffs(__activemask()) - 1) && m)
-        atomicAdd(&L.stats[1], (unsigned long long)__popc(m));
+  uint32_t traced = 0;
+  if (!L.scene.hasTris) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += stride) {
+      const float4 o = L.st.shO[j];
+      float tr = 0.0f;
+      if (o.w > 0.0f) {
+        tr = scene_occluded(L.scene, xyz(o), xyz(L.st.shD[j]), kDefaultTmax) ? 0.0f : 1.0f;
+        ++traced;
+      }
+      L.st.shTr[j] = tr;
     }
+  } else {
+    auto begin = [&](uint32_t j, TraceState& s, uint32_t* item) {
+      const float4 o = L.st.shO[j];
+      *item = j;
+      if (!(o.w > 0.0f)) {  // no ray for this record
+        L.st.shTr[j] = 0.0f;
+        return false;
+      }
+      ++traced;
+      trace_begin(s, xyz(o), xyz(L.st.shD[j]), kDefaultTmax);
+      return true;
+    };
+    auto end = [&](uint32_t j, const TraceState& s) {
+      bool occluded = s.best.tri >= 0;
+      if (!occluded && L.scene.nshapes > 0) {
+        SceneView noTris = L.scene;
+        noTris.hasTris = 0;
+        Hit none;
+        none.tri = -1;
+        occluded = __float_as_int(scene_closest_after<false>(noTris, s.r.o, s.r.d, kDefaultTmax, none).w) != -1;
+      }
+      L.st.shTr[j] = occluded ? 0.0f : 1.0f;
+    };
+    trace_persistent<true>(L.scene.bvh, 2 * n, &L.st.counts[kTravCounters + 2 * L.bounce + 1], trav_visits(L),
+                           trav_refill(L), begin, end);
   }
-  if (L.stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)n);
+  if (L.stats) {
+    for (int o = 16; o > 0; o >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, o);
+    if ((threadIdx.x & 31) == 0 && traced) atomicAdd(&L.stats[1], (unsigned long long)traced);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)n);
+  }
 }
 
 // ------------------------------------------------------------------ media: shadow transmittance
@@ -822,8 +917,12 @@ int resident_blocks(K kernel, int threads) {
 
 int g_trackBlocks[4] = {0, 0, 0, 0};  // resident blocks of k_track<dda, sample>, by dda + 2 sample
 
+int g_travBlocks[2] = {0, 0};  // resident blocks of k_extend, k_shadow_surfaces
+
 void query_track_blocks() {
   if (g_trackBlocks[0] != 0) return;
+  g_travBlocks[0] = resident_blocks(k_extend, 128);
+  g_travBlocks[1] = resident_blocks(k_shadow_surfaces, 128);
   g_trackBlocks[1] = resident_blocks(k_track<true, false>, 128);
   g_trackBlocks[2] = resident_blocks(k_track<false, true>, 128);
   g_trackBlocks[3] = resident_blocks(k_track<true, true>, 128);
@@ -849,6 +948,9 @@ void launch_track(const RenderLaunch& L, bool sample, int round, cudaStream_t s)
 void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, WaveTimer* tm) {
   RenderLaunch L = L0;
   if (L.trackSteps == 0) L.trackSteps = kDefaultTrackSteps;
+  if (L.travVisits == 0) L.travVisits = kDefaultTravVisits;
+  if (L.travRefill == 0) L.travRefill = kDefaultTravRefill;
+  query_track_blocks();
   const bool media = L.scene.nmedia > 0;
   int ev = 0;
   auto mark = [&](int kind) {
@@ -857,7 +959,7 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
     tm->kind[ev] = kind;
     ++ev;
   };
-  R2_CUDA(cudaMemsetAsync(L.st.counts, 0, sizeof(uint32_t) * (L.maxDepth + 2), s));
+  R2_CUDA(cudaMemsetAsync(L.st.counts, 0, sizeof(uint32_t) * (kTravCounters + 2 * L.maxDepth), s));
   if (media) R2_CUDA(cudaMemsetAsync(L.st.mc, 0, sizeof(uint32_t) * kCountersPerBounce * L.maxDepth, s));
   mark(-1);
   k_camera<<<nblocks, 256, 0, s>>>(L);
@@ -883,11 +985,11 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
         else k_shadow_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
     } else {
-      k_extend<<<nblocks * 2, 128, 0, s>>>(L);
+      k_extend<<<std::min(nblocks * 2, g_travBlocks[0]), 128, 0, s>>>(L);
       mark(1);
       k_shade<false><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
-      k_shadow_surfaces<<<nblocks * 2, 128, 0, s>>>(L);
+      k_shadow_surfaces<<<std::min(nblocks * 2, g_travBlocks[1]), 128, 0, s>>>(L);
     }
     mark(3);
     k_accum<<<nblocks, 256, 0, s>>>(L);

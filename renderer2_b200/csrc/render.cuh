@@ -42,7 +42,8 @@ struct PathState {
   float4* hit;      // t, b1, b2, event code (int bits: >= 0 triangle, -1 miss, -2 - i shape i,
                     // kEventScatter medium collision, kEventDead path ended by a medium rule)
   uint32_t* q[2];   // ping-pong queues of live path ids
-  uint32_t* counts; // [bounce] live path count entering the bounce
+  uint32_t* counts; // [bounce] live path count entering the bounce; from kTravCounters on,
+                    // per bounce the rays taken by the persistent surface traversals
   // shadow records, two per queue slot (0: light sample, 1: BSDF sample)
   float4* shO;      // origin.xyz, pdf (0 = no ray)
   float4* shD;      // direction.xyz, unused
@@ -67,6 +68,17 @@ struct PathState {
   int2* swM;        // shadow walk: current medium, draw index of the slot's stream
 };
 
+// Launch tuning defaults (RenderLaunch::trackSteps, travVisits, travRefill);
+// no result depends on them.
+constexpr uint32_t kDefaultTrackSteps = 8;   // tracking steps a lane takes between refills
+constexpr uint32_t kDefaultTravVisits = 32;  // BVH visits between refill checks
+constexpr uint32_t kDefaultTravRefill = 8;   // finished lanes that trigger a refill
+
+// PathState::counts layout: [0, 64) live paths per bounce, then two counters
+// per bounce (extension rays taken, shadow records taken).
+constexpr int kTravCounters = 64;
+constexpr int kCountsSize = kTravCounters + 2 * 64;
+
 constexpr int kEventScatter = -2147483647;  // INT_MIN + 1
 constexpr int kEventDead = -2147483646;     // INT_MIN + 2
 
@@ -84,6 +96,8 @@ struct RenderLaunch {
   uint32_t bounce;
   uint32_t dda;       // brick-grid DDA tracking (UseBrickGrid) instead of the global majorant
   uint32_t trackSteps;  // tracking steps a lane takes between refills (tuning, >= 1)
+  uint32_t travVisits;  // BVH visits a lane takes between refill checks of the surface kernels (tuning, >= 1)
+  uint32_t travRefill;  // finished lanes of a warp that trigger a refill (tuning, 1..32)
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

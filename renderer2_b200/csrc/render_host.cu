@@ -110,7 +110,13 @@ RenderContext::~RenderContext() {
 
 RenderScene::RenderScene() {
   memset(&view_, 0, sizeof(view_));
-  if (const char* e = getenv("R2_TRACK_STEPS")) trackSteps_ = (uint32_t)std::max(1l, std::min(1024l, atol(e)));
+  auto env = [](const char* name, long lo, long hi) -> uint32_t {
+    const char* e = getenv(name);
+    return e ? (uint32_t)std::max(lo, std::min(hi, atol(e))) : 0u;
+  };
+  tuning_.track_steps = env("R2_TRACK_STEPS", 1, 1024);
+  tuning_.trav_visits = env("R2_TRAV_VISITS", 1, 1 << 20);
+  tuning_.trav_refill = env("R2_TRAV_REFILL", 1, 32);
 }
 
 RenderScene::~RenderScene() {}
@@ -251,7 +257,7 @@ void RenderContext::ensure(uint32_t n, bool media) {
     rayO_.alloc(n); rayD_.alloc(n); T_.alloc(n); L_.alloc(n); hit_.alloc(n);
     shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
     q0_.alloc(n); q1_.alloc(n); shTr_.alloc(2 * (size_t)n);
-    counts_.alloc(64);
+    counts_.alloc(kCountsSize);
     cap_ = n;
   }
   if (media && n > mediaCap_) {
@@ -268,7 +274,7 @@ void RenderContext::ensure(uint32_t n, bool media) {
 
 size_t RenderContext::bytes_for(uint32_t n, bool media) {
   // per path: 5 float4 state + 3 x 2 float4 records + float4 throughput + 2 queue ids + 2 transmittances
-  size_t b = (size_t)n * (5 * 16 + 6 * 16 + 16 + 8 + 8) + 64 * 4;
+  size_t b = (size_t)n * (5 * 16 + 6 * 16 + 16 + 8 + 8) + kCountsSize * 4;
   // media: records (4 float4 + float2), shadow tmax/medium, round queues and walk state
   if (media) b += (size_t)n * (16 + 48 + 8 + 16 + 16 + 64 + 16 + 32 + 16) + 16 * 64 * 4;
   return b + (size_t)n * 12;  // frame
@@ -319,7 +325,9 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   L.maxDepth = p.max_depth;
   L.seed = p.seed;
   L.dda = (p.flags & R2_RENDER_BRICK_GRID) ? 1u : 0u;
-  L.trackSteps = trackSteps_;
+  L.trackSteps = tuning_.track_steps;
+  L.travVisits = tuning_.trav_visits;
+  L.travRefill = tuning_.trav_refill;
   L.bound = ctx.bound.get();
   return L;
 }
@@ -377,12 +385,8 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
 
 void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame,
                                cudaStream_t s) {
-  check_params(c, p, d_frame);
-  R2_REQUIRE(committed_, R2_ERR_INVALID_ARGUMENT, "scene not committed");
+  RenderLaunch L = prepare(ctx, c, p, d_frame);
   const uint32_t npix = c.width * c.height;
-  ctx.ensure(npix, !media_.empty());
-  RenderLaunch L = make_launch(ctx, c, p, d_frame);
-  L.sampleDev = ctx.sampleDev.get();
   R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
   R2_CUDA(cudaMemsetAsync(ctx.sampleDev.get(), 0, sizeof(uint32_t), s));
   R2_CUDA(cudaMemsetAsync(d_frame, 0, sizeof(float) * 3 * (size_t)npix, s));
@@ -414,6 +418,167 @@ void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_
   R2_CUDA(cudaGraphInstantiate(&guard.e, guard.g, 0));
   for (uint32_t smp = 0; smp < p.spp; ++smp) R2_CUDA(cudaGraphLaunch(guard.e, s));
   // the executable graph may be destroyed while its launches are pending
+}
+
+RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame) {
+  check_params(c, p, d_frame);
+  R2_REQUIRE(committed_, R2_ERR_INVALID_ARGUMENT, "scene not committed");
+  ctx.ensure(c.width * c.height, !media_.empty());
+  RenderLaunch L = make_launch(ctx, c, p, d_frame);
+  L.sampleDev = ctx.sampleDev.get();
+  return L;
+}
+
+void RenderScene::set_tuning(const r2_render_tuning& t) {
+  R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.reserved == 0, R2_ERR_INVALID_ARGUMENT,
+             "tuning out of range (track_steps <= 1024, trav_refill <= 32, reserved 0)");
+  tuning_ = t;
+}
+
+r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_params& p) {
+  R2_REQUIRE(c.width > 0 && c.height > 0 && (uint64_t)c.width * c.height < (1ull << 31), R2_ERR_INVALID_ARGUMENT,
+             "frame size out of range");
+  const uint32_t npix = c.width * c.height;
+  DBuf<float> frame((size_t)npix * 3);  // the tuner's own frame
+  check_params(c, p, frame.get());
+  if (!committed_) commit();
+  RenderContext& ctx = ctx_;
+  cudaStream_t s = ctx.stream;
+  r2_render_params p1 = p;
+  p1.spp = 1;
+  RenderLaunch L = prepare(ctx, c, p1, frame.get());
+  prepare_render_launches();
+  const int nblocks = wave_blocks(npix);
+  // one wave of sample 0 per setting, the faster of two runs
+  auto time_wave = [&](const r2_render_tuning& t) {
+    L.trackSteps = t.track_steps;
+    L.travVisits = t.trav_visits;
+    L.travRefill = t.trav_refill;
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      R2_CUDA(cudaEventRecord(ctx.ev0, s));
+      launch_render_wave(L, nblocks, s, nullptr);
+      R2_CUDA(cudaEventRecord(ctx.ev1, s));
+      R2_CUDA(cudaEventSynchronize(ctx.ev1));
+      float ms = 0.0f;
+      R2_CUDA(cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1));
+      best = std::min(best, ms);
+    }
+    return best;
+  };
+  r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, 0};
+  R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
+  time_wave(cur);  // warm-up
+  float curMs = time_wave(cur);
+  static const uint32_t refills[] = {2, 4, 16, 32};
+  static const uint32_t visits[] = {8, 16, 64, 256};
+  static const uint32_t steps[] = {2, 4, 16, 32};
+  auto sweep = [&](uint32_t r2_render_tuning::*field, const uint32_t* cand, int n) {
+    const r2_render_tuning base = cur;
+    for (int i = 0; i < n; ++i) {
+      r2_render_tuning t = base;
+      t.*field = cand[i];
+      const float ms = time_wave(t);
+      if (ms < curMs * 0.98f) {
+        cur = t;
+        curMs = ms;
+      }
+    }
+  };
+  if (media_.empty()) {  // the persistent surface traversals run in scenes without media
+    sweep(&r2_render_tuning::trav_refill, refills, 4);
+    sweep(&r2_render_tuning::trav_visits, visits, 4);
+  } else {
+    sweep(&r2_render_tuning::track_steps, steps, 4);
+  }
+  tuning_ = cur;
+  return cur;
+}
+
+RenderBatch::RenderBatch(const std::vector<RenderScene*>& scenes, const std::vector<r2_camera>& cams,
+                         const std::vector<r2_render_params>& params, const std::vector<float*>& frames) {
+  const size_t n = scenes.size();
+  R2_REQUIRE(n > 0 && cams.size() == n && params.size() == n && frames.size() == n, R2_ERR_INVALID_ARGUMENT,
+             "batch arrays must have one entry per frame");
+  spp_ = params[0].spp;
+  std::vector<RenderLaunch> Ls;
+  for (size_t i = 0; i < n; ++i) {
+    R2_REQUIRE(scenes[i], R2_ERR_INVALID_ARGUMENT, "null scene in batch");
+    R2_REQUIRE(params[i].spp == spp_, R2_ERR_INVALID_ARGUMENT, "all frames of a batch share the sample count");
+    ctx_.emplace_back(new RenderContext());
+    Ls.push_back(scenes[i]->prepare(*ctx_.back(), cams[i], params[i], frames[i]));
+    frames_.push_back(frames[i]);
+    npix_.push_back((size_t)cams[i].width * cams[i].height);
+  }
+  prepare_render_launches();  // occupancy queries stay outside the capture
+  R2_CUDA(cudaEventCreate(&ev0_));
+  R2_CUDA(cudaEventCreate(&ev1_));
+  // one wave of every frame: the capture stream forks into the contexts'
+  // streams (each frame a branch of its own) and joins them again
+  cudaStream_t cap = nullptr;
+  R2_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  std::vector<cudaEvent_t> evs(n + 1, nullptr);
+  struct Guard {
+    cudaStream_t s;
+    std::vector<cudaEvent_t>& evs;
+    ~Guard() {
+      for (cudaEvent_t e : evs)
+        if (e) cudaEventDestroy(e);
+      cudaStreamDestroy(s);
+    }
+  } guard{cap, evs};
+  for (auto& e : evs) R2_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  R2_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+  try {
+    R2_CUDA(cudaEventRecord(evs[n], cap));
+    for (size_t i = 0; i < n; ++i) {
+      cudaStream_t b = ctx_[i]->stream;
+      R2_CUDA(cudaStreamWaitEvent(b, evs[n], 0));
+      launch_render_wave(Ls[i], wave_blocks((uint32_t)npix_[i]), b, nullptr);
+      R2_CUDA(cudaEventRecord(evs[i], b));
+      R2_CUDA(cudaStreamWaitEvent(cap, evs[i], 0));
+    }
+  } catch (...) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(cap, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  R2_CUDA(cudaStreamEndCapture(cap, &graph_));
+  R2_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+}
+
+RenderBatch::~RenderBatch() {
+  if (ev1_) cudaEventSynchronize(ev1_);  // the last run's samples, before the buffers go
+  if (exec_) cudaGraphExecDestroy(exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+}
+
+double RenderBatch::run(cudaStream_t s, bool timing) {
+  for (size_t i = 0; i < ctx_.size(); ++i) {
+    R2_CUDA(cudaMemsetAsync(ctx_[i]->bound.get(), 0, sizeof(unsigned int), s));
+    R2_CUDA(cudaMemsetAsync(ctx_[i]->sampleDev.get(), 0, sizeof(uint32_t), s));
+    R2_CUDA(cudaMemsetAsync(frames_[i], 0, sizeof(float) * 3 * npix_[i], s));
+  }
+  R2_CUDA(cudaEventRecord(ev0_, s));
+  for (uint32_t smp = 0; smp < spp_; ++smp) R2_CUDA(cudaGraphLaunch(exec_, s));
+  R2_CUDA(cudaEventRecord(ev1_, s));
+  if (!timing) return 0.0;
+  R2_CUDA(cudaEventSynchronize(ev1_));
+  float ms = 0.0f;
+  R2_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+  return ms;
+}
+
+uint32_t RenderBatch::bound_hits(cudaStream_t s) {
+  std::vector<unsigned int> b(ctx_.size(), 0);
+  for (size_t i = 0; i < ctx_.size(); ++i) ctx_[i]->bound.download(&b[i], 1, s);
+  R2_CUDA(cudaStreamSynchronize(s));
+  uint32_t t = 0;
+  for (unsigned int v : b) t += v;
+  return t;
 }
 
 }  // namespace r2

@@ -88,6 +88,12 @@ class RenderScene {
   // CUDA graph and replayed once per sample (the scene must be committed).
   void render_graph(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame,
                     cudaStream_t s);
+  // The launch description of a frame on ctx (its buffers grown to fit).
+  RenderLaunch prepare(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame);
+  // Launch tuning (0 fields: the defaults) and the autotuner that sets it.
+  void set_tuning(const r2_render_tuning& t);
+  r2_render_tuning tuning() const { return tuning_; }
+  r2_render_tuning autotune(const r2_camera& cam, const r2_render_params& p);
   // Paths and shadow rays of the last render() that a loop bound ended (waits for the stream).
   uint32_t bound_hits(cudaStream_t s) { return ctx_.bound_hits(s ? s : ctx_.stream); }
   cudaStream_t stream() const { return ctx_.stream; }
@@ -114,7 +120,34 @@ class RenderScene {
   DBuf<float4> envTex_;
   DBuf<float> envBuf_;
   SceneView view_;
-  uint32_t trackSteps_ = 0;  // 0: the kernels' default; R2_TRACK_STEPS overrides
+  r2_render_tuning tuning_{0, 0, 0, 0};  // 0 fields: the kernels' defaults
+};
+
+// Frames of several committed scenes rendered by one captured CUDA graph: the
+// graph holds one wave of every scene, each on its own branch (forked capture
+// streams), and is replayed once per sample.  Frames, cameras and parameters
+// are fixed at construction; all entries share the sample count.
+class RenderBatch {
+ public:
+  RenderBatch(const std::vector<RenderScene*>& scenes, const std::vector<r2_camera>& cams,
+              const std::vector<r2_render_params>& params, const std::vector<float*>& frames);
+  ~RenderBatch();
+  RenderBatch(const RenderBatch&) = delete;
+  RenderBatch& operator=(const RenderBatch&) = delete;
+  // All frames (cleared first); returns the device milliseconds between the
+  // first clear and the last wave when timing is requested (waits).
+  double run(cudaStream_t s, bool timing);
+  // Paths and shadow rays of the last run that a loop bound ended (waits for s).
+  uint32_t bound_hits(cudaStream_t s);
+
+ private:
+  std::vector<std::unique_ptr<RenderContext>> ctx_;
+  std::vector<float*> frames_;
+  std::vector<size_t> npix_;
+  uint32_t spp_ = 0;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
 };
 
 }  // namespace r2

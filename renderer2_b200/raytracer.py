@@ -44,6 +44,19 @@ def params(spp=16, max_depth=8, seed=0, brick_grid=False) -> RenderParams:
 SPHERE, CIRCLE = 0, 1
 
 
+class Tuning(C.Structure):
+    """Launch tuning (r2_render_tuning); 0 fields select the defaults; images never depend on it."""
+    _fields_ = [("track_steps", C.c_uint32), ("trav_visits", C.c_uint32), ("trav_refill", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+    def as_tuple(self):
+        return (self.track_steps, self.trav_visits, self.trav_refill)
+
+
+def tuning(track_steps=0, trav_visits=0, trav_refill=0) -> Tuning:
+    return Tuning(track_steps, trav_visits, trav_refill, 0)
+
+
 class Scene:
     """Device-resident render scene (r2_scene_*)."""
 
@@ -106,7 +119,53 @@ class Scene:
             stats[:] = st
         return st
 
+    def set_tuning(self, t: Tuning):
+        N.check(N.lib.r2_scene_set_tuning(self.handle, C.byref(t)))
+
+    def get_tuning(self) -> Tuning:
+        t = Tuning()
+        N.check(N.lib.r2_scene_get_tuning(self.handle, C.byref(t)))
+        return t
+
+    def autotune(self, cam: Camera, prm: RenderParams) -> Tuning:
+        """Times one wave of this frame per candidate setting and keeps the fastest (see r2_scene_autotune)."""
+        t = Tuning()
+        N.check(N.lib.r2_scene_autotune(self.handle, C.byref(cam), C.byref(prm), C.byref(t)))
+        return t
+
     def render(self, cam: Camera, prm: RenderParams) -> np.ndarray:
         out = np.zeros((cam.height, cam.width, 3), np.float32)
         N.check(N.lib.r2_render_host(self.handle, C.byref(cam), C.byref(prm), N.ptr(out)))
         return out
+
+
+class RenderBatch:
+    """Frames of several committed scenes rendered by one captured CUDA graph
+    (r2_render_batch_*); frames are device pointers of width*height*3 floats."""
+
+    def __init__(self, scenes, cams, prms, d_frames):
+        n = len(scenes)
+        assert len(cams) == n and len(prms) == n and len(d_frames) == n and n > 0
+        self._keep = (list(scenes), (Camera * n)(*cams), (RenderParams * n)(*prms))
+        sh = (C.c_void_p * n)(*[s.handle for s in scenes])
+        fr = (C.c_void_p * n)(*[int(p) for p in d_frames])
+        h = C.c_void_p()
+        N.check(N.lib.r2_render_batch_create(sh, self._keep[1], self._keep[2], fr, n, C.byref(h)))
+        self.handle = h
+
+    def run(self, stream: int = 0, timing: bool = True) -> float:
+        """Renders every frame; with timing, waits and returns the device milliseconds."""
+        ms = C.c_double(0.0)
+        N.check(N.lib.r2_render_batch_run(self.handle, C.c_void_p(stream or None), C.byref(ms) if timing else None))
+        return ms.value
+
+    def close(self):
+        if self.handle:
+            N.check(N.lib.r2_render_batch_destroy(self.handle))
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -26,8 +26,8 @@ def translate43(x, y, z):
     return m
 
 
-def c1_scene():
-    """Config 1: icosphere sub 4 (5,120 tris), GGX roughness 0.3 albedo 0.8, constant white env;
+def icosphere_scene():
+    """Small plain scene: icosphere sub 4 (5,120 tris), GGX roughness 0.3 albedo 0.8, constant white env;
     camera (0,0,3) -> origin, fov 45."""
     mesh = scenes.icosphere(4, 0.05, 1)
     mat = F.material(diffuse=(0.8, 0.8, 0.8), specular=(1.0, 1.0, 1.0), alpha=0.3, ior=1.5)
@@ -36,8 +36,8 @@ def c1_scene():
     return desc, cam
 
 
-def c2_scene():
-    """Config 2: 8x8 grid of displaced icospheres (64 x 5,120 = 327,680 tris), per-object GGX
+def icosphere_grid_scene():
+    """Surface path-tracing scene: 8x8 grid of displaced icospheres (64 x 5,120 = 327,680 tris), per-object GGX
     roughness U[0.05, 1] and albedo U[0.2, 0.9] (seed 2), lognormal(0, 1.5) 512x256 env (seed 3)."""
     rng = np.random.default_rng(2)
     meshes = []
@@ -55,7 +55,7 @@ def c2_scene():
 
 def volume_scene(work_dir, index: int = 0, grid: int = 256, n_quads: int = 200_000, ico_subdiv: int = 6,
                  width: int = 1920, height: int = 1080, filter_spv: int = 64, filter_iters: int = 10):
-    """Config 4 scene `index` (seed 5 + index): a foliage grid filtered on the GPU
+    """Batched-volume scene `index` (seed 5 + index): a foliage grid filtered on the GPU
     (LOD 0 NanoVDB + brick grid written under work_dir, grid^3 voxels) as an
     SGGX medium scaled to a 4-unit cube, a displaced icosphere (20 * 4^ico_subdiv
     triangles) beside it, a ground disc and a lognormal(0, 1.5) environment;

@@ -113,8 +113,8 @@ def test_bvh_bit_exact(mesh_kind):
     assert np.array_equal(nodes, onodes)
 
 
-def test_filter_c1_parity():
-    """Config 1: icosphere sub 4 (5,120 tris), 32^3, 64 samples/voxel, 10 iterations."""
+def test_filter_small_icosphere_parity():
+    """Plain small case: icosphere sub 4 (5,120 tris), 32^3, 64 samples/voxel, 10 iterations."""
     mesh = scenes.icosphere(4, 0.05, 1)
     mat = F.material()
     prm = F.params(samples_per_voxel=64, iterations=10)

@@ -124,3 +124,18 @@ def test_medium_loading_errors(lods, tmp_path):
     with pytest.raises(N.R2Error):
         sc.add_medium(lods[0], (0, 0, 0), (0, 0, 0))  # sigma_t = 0
     sc.close()
+
+
+def test_medium_tracking_tuning_never_changes_the_frame(lods):
+    desc = _desc(lods[0])
+    cam = R.camera(32, 28, 50.0, (0.3, 0.6, 3.2), (0.0, 0.0, 0.0), (0, 1, 0))
+    sc = RS.build_scene(desc)
+    prm = R.params(3, 8, 17, brick_grid=True)
+    ref = sc.render(cam, prm)
+    for steps, visits, refill in [(1, 2, 1), (64, 7, 32)]:
+        sc.set_tuning(R.tuning(steps, visits, refill))
+        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill)
+    t = sc.autotune(cam, prm)
+    assert t.track_steps >= 1
+    assert np.array_equal(sc.render(cam, prm), ref)
+    sc.close()

@@ -35,8 +35,8 @@ def _agree(g, o):
     return ok.mean()
 
 
-def test_c1_small_matches_oracle():
-    desc, _ = RS.c1_scene()
+def test_small_icosphere_matches_oracle():
+    desc, _ = RS.icosphere_scene()
     cam = R.camera(64, 64, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
     g = _gpu_frame(desc, cam, 8, 8, 0)
     o = O.render(desc, cam, 8, 8, 0)
@@ -80,7 +80,7 @@ def test_deep_paths_rr_match_oracle():
 
 
 def test_three_sigma_against_high_spp_oracle():
-    desc, _ = RS.c1_scene()
+    desc, _ = RS.icosphere_scene()
     desc = dict(desc)
     desc["env"] = RS.lognormal_env(32, 16, 1.0, 4)
     cam = R.camera(24, 24, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
@@ -94,7 +94,7 @@ def test_three_sigma_against_high_spp_oracle():
 
 
 def test_device_entry_matches_host_entry_and_is_deterministic():
-    desc, _ = RS.c1_scene()
+    desc, _ = RS.icosphere_scene()
     cam = R.camera(40, 30, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
     sc = RS.build_scene(desc)
     a = sc.render(cam, R.params(4, 8, 2))
@@ -109,11 +109,33 @@ def test_device_entry_matches_host_entry_and_is_deterministic():
 
 
 def test_render_rejects_bad_arguments():
-    desc, _ = RS.c1_scene()
+    desc, _ = RS.icosphere_scene()
     sc = RS.build_scene(desc)
     from renderer2_b200 import _native as N
     with pytest.raises(N.R2Error):
         sc.render(R.camera(8, 8), R.params(0, 8, 0))
     with pytest.raises(N.R2Error):
         sc.render(R.camera(8, 8), R.params(1, 100, 0))
+    sc.close()
+
+
+def test_launch_tuning_never_changes_the_frame():
+    """Refill thresholds and visit rounds of the persistent traversals (and the
+    autotuner's choice) give the same frame bit for bit."""
+    desc, _ = RS.icosphere_grid_scene()
+    cam = R.camera(96, 80, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+    prm = R.params(2, 8, 5)
+    sc = RS.build_scene(desc)
+    ref = sc.render(cam, prm)
+    for visits, refill in [(1, 1), (3, 32), (1000, 5), (64, 16)]:
+        sc.set_tuning(R.tuning(trav_visits=visits, trav_refill=refill))
+        assert sc.get_tuning().as_tuple() == (0, visits, refill)
+        assert np.array_equal(sc.render(cam, prm), ref), (visits, refill)
+    t = sc.autotune(cam, prm)
+    assert 1 <= t.trav_refill <= 32 and t.trav_visits >= 1
+    assert sc.get_tuning().as_tuple() == t.as_tuple()
+    assert np.array_equal(sc.render(cam, prm), ref)
+    from renderer2_b200 import _native as N
+    with pytest.raises(N.R2Error):
+        sc.set_tuning(R.tuning(trav_refill=33))
     sc.close()

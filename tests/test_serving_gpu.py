@@ -18,7 +18,7 @@ from renderer2_b200 import serving as S  # noqa: E402
 
 @pytest.fixture(scope="module")
 def world(tmp_path_factory):
-    desc1, _ = RS.c1_scene()
+    desc1, _ = RS.icosphere_scene()
     desc1 = dict(desc1)
     desc1["env"] = RS.lognormal_env(64, 32, 1.0, 2)
     sc1 = RS.build_scene(desc1)
@@ -115,3 +115,31 @@ def test_wait_timeout_reports_pending(world):
     assert srv.wait(h, 300.0)
     assert np.isfinite(h.out).all() and h.out.mean() > 0
     srv.close()
+
+
+def test_render_batch_matches_single_frames(world):
+    """One captured graph holding a wave of every frame (the same scene twice
+    with other cameras, a media scene with both tracking modes) gives every
+    frame bit for bit, run twice."""
+    cams = [R.camera(64, 48, 45.0, (0, 0, 3)), R.camera(96, 96, 50.0, (0.5, 0.3, 3.2)),
+            R.camera(40, 30, 60.0, (0.3, 0.6, 3.2)), R.camera(48, 64, 40.0, (0.2, 0.1, 3.0))]
+    scs = [world["sc1"], world["sc2"], world["sc1"], world["sc2"]]
+    prms = [R.params(3, 6, 11), R.params(3, 8, 12, brick_grid=True), R.params(3, 5, 13), R.params(3, 8, 14)]
+    refs = [s.render(c, p) for s, c, p in zip(scs, cams, prms)]
+    frames = [torch.empty((c.height, c.width, 3), dtype=torch.float32, device="cuda") for c in cams]
+    b = R.RenderBatch(scs, cams, prms, [f.data_ptr() for f in frames])
+    for _ in range(2):
+        ms = b.run()
+        assert ms > 0
+        for f, ref in zip(frames, refs):
+            assert np.array_equal(f.cpu().numpy(), ref)
+    b.close()
+
+
+def test_render_batch_rejects_mixed_sample_counts(world):
+    cam = R.camera(16, 16)
+    f = torch.empty((16, 16, 3), dtype=torch.float32, device="cuda")
+    with pytest.raises(N.R2Error) as e:
+        R.RenderBatch([world["sc1"], world["sc1"]], [cam, cam], [R.params(2), R.params(3)],
+                      [f.data_ptr(), f.data_ptr()])
+    assert e.value.name == "R2_ERR_INVALID_ARGUMENT"
