@@ -245,7 +245,7 @@ def bench_render(args, world, local):
     from renderer2_b200 import render_scenes as RS
     desc, cam, prm = render_workload()
     sc = RS.build_scene(desc)
-    tuning = sc.autotune(cam, prm).as_tuple()  # set-up: launch tuning of this frame (never changes the image)
+    tuning = sc.autotune(cam, prm).as_dict()  # set-up: launch tuning of this frame (never changes the image)
     npix = cam.width * cam.height
     frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
@@ -275,8 +275,9 @@ def bench_render(args, world, local):
     st = np.mean(np.array(stats), axis=0)
     seg, shadow = st[2], st[3]
     ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
-    # dominant kernel over the frame: per-wave ms x spp
-    seg_wave, sh_wave = seg / prm.spp, 2.0 * seg / prm.spp
+    # dominant kernel over the frame; a wave renders S samples of every pixel
+    S = sc.wave_samples(cam, prm)
+    seg_wave, sh_wave = seg * S / prm.spp, 2.0 * seg * S / prm.spp
     dom = "extend" if ms_wave["extend"] >= ms_wave["shadow"] else "shadow"
     peak, peak_kind = _peaks()
     if dom == "extend":
@@ -294,6 +295,7 @@ def bench_render(args, world, local):
                 "traffic": (tr["bytes_per_unit"] * (seg_wave if dom == "extend" else sh_wave) / launches)
                 if tr else None,
                 "alg_bytes_per_launch": alg / launches, "avg_launch_ms": kms / launches,
+                "samples_per_wave": S,
                 "note": "per-launch figures averaged over the bounces of the timed middle wave; "
                         "traversal is L2/issue bound, see rays_per_s",
                 "rays_per_s": (seg + shadow) / (st[1] / 1e3), "kernel_ms_per_wave": ms_wave}
@@ -312,7 +314,7 @@ def bench_render(args, world, local):
     e2e = {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms}
     sc.close()
-    launches_per_step = prm.spp * (2 + 4 * prm.max_depth)
+    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth)
     return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths, tuning=tuning,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
                 desc=desc, cam=cam, prm=prm)
@@ -392,7 +394,7 @@ def bench_volume(args, world, local):
                                 width=c["width"], height=c["height"])
     prm = R.params(c["spp"], c["depth"], c["seed"], brick_grid=True)
     sc = RS.build_scene(desc)
-    tuning = sc.autotune(cam, prm).as_tuple()
+    tuning = sc.autotune(cam, prm).as_dict()
     npix = cam.width * cam.height
     frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
@@ -417,7 +419,8 @@ def bench_volume(args, world, local):
     st = np.mean(np.array(stats), axis=0)
     seg, shadow = st[2], st[3]
     ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
-    seg_wave = seg / prm.spp
+    S = sc.wave_samples(cam, prm)
+    seg_wave = seg * S / prm.spp
     dom = max(("extend", "shadow", "shade"), key=lambda k: ms_wave[k])
     per_unit = {"extend": (VOLUME_EXTEND_BYTES_PER_SEGMENT, seg_wave, "extend phase"),
                 "shadow": (SHADOW_MEDIA_BYTES_PER_SLOT, 2.0 * seg_wave, "shadow phase"),
@@ -452,12 +455,12 @@ def bench_volume(args, world, local):
                                   f"mesh, {c['width']}x{c['height']}, {c['spp']} spp per step, depth {c['depth']}",
                       "paths_per_step": paths, "segments_per_step": seg, "shadow_rays_per_step": shadow,
                       "l2": "wave state larger than L2",
-                      "tuning": dict(zip(("track_steps", "trav_visits", "trav_refill"), tuning))},
+                      "tuning": tuning},
            "roofline": roofline,
            "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms},
            # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, shade, 3 shadow resolve, accum
-           "gpu_launches": prm.spp * (2 + 13 * prm.max_depth) * args.steps}
+           "gpu_launches": (prm.spp // S) * (2 + 13 * prm.max_depth) * args.steps}
     return out, (desc, cam, prm)
 
 
@@ -708,7 +711,7 @@ def run_native(args):
                            "paths_per_step": r["paths"], "segments_per_step": r["segments_per_frame"],
                            "shadow_rays_per_step": r["shadow_rays_per_frame"],
                            "l2": "inputs + wave state larger than L2", "parallelism": f"replicas x{world}",
-                           "tuning": dict(zip(("track_steps", "trav_visits", "trav_refill"), r["tuning"]))},
+                           "tuning": r["tuning"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"]}
         if f is not None:
@@ -776,16 +779,19 @@ def run_case(args):
         sc.close()
         print(json.dumps({"case": args.case, "paths": st[0], "ms": st[1]}))
     elif args.case == "render-wave":
-        # one wave of the headline frame: the same launches (1M paths per bounce) as a bench step
+        # one wave of the headline frame: --case-spp samples of every pixel in one wave
         desc, cam, prm = render_workload()
         from renderer2_b200 import render_scenes as RS
         from renderer2_b200 import raytracer as R
         sc = RS.build_scene(desc)
         frame = torch.empty(cam.width * cam.height * 3, dtype=torch.float32, device="cuda")
-        st = sc.render_device(cam, R.params(1, prm.max_depth, 0), frame.data_ptr())
+        n = args.case_spp
+        sc.set_tuning(R.tuning(wave_paths=cam.width * cam.height * n))
+        st = sc.render_device(cam, R.params(n, prm.max_depth, 0), frame.data_ptr())
         torch.cuda.synchronize()
         sc.close()
-        print(json.dumps({"case": args.case, "paths": st[0], "segments": st[2], "shadow_rays": st[3], "ms": st[1]}))
+        print(json.dumps({"case": args.case, "paths": st[0], "segments": st[2], "shadow_rays": st[3], "ms": st[1],
+                          "ms_per_wave": {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}}))
     elif args.case == "filter-small":
         from renderer2_b200 import filter as F
         from renderer2_b200 import scenes
@@ -840,7 +846,9 @@ def main():
     ap.add_argument("--skip-volume", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
-    ap.add_argument("--case", default=None, help="profiling case: render-small | filter-small")
+    ap.add_argument("--case", default=None,
+                    help="profiling case: render-wave | filter-small | volume-small | volume-mid | volume-batch | serving")
+    ap.add_argument("--case-spp", type=int, default=1, help="render-wave: samples per pixel, all in one wave")
     args = ap.parse_args()
     if args.case:
         run_case(args)

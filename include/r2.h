@@ -227,7 +227,8 @@ typedef struct r2_render_tuning {
   uint32_t track_steps; /* media: tracking steps a lane of the persistent tracker takes between refills (1..1024) */
   uint32_t trav_visits; /* BVH node/leaf visits a lane takes between refill checks of the surface kernels */
   uint32_t trav_refill; /* finished lanes of a warp (1..32) that make it take new rays */
-  uint32_t reserved;    /* 0 */
+  uint32_t wave_paths;  /* paths per wave: a wave renders the largest divisor of spp samples of every
+                           pixel that keeps width*height*samples within it (at least one sample) */
 } r2_render_tuning;
 
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA
@@ -273,7 +274,8 @@ r2_status r2_scene_commit(r2_scene* scene);
  * stats_out (nullable, 8 doubles): [0] paths, [1] milliseconds of the frame on
  * the stream, [2] path segments traced, [3] shadow rays traced, [4..7]
  * milliseconds of the extend / shade / shadow / accumulate kernels of one
- * (the middle) wave.  With stats_out the call waits for the frame and returns
+ * (the middle) wave, which renders r2_scene_wave_samples samples of every
+ * pixel.  With stats_out the call waits for the frame and returns
  * R2_ERR_DEVICE_TIMEOUT (frame still written) if a loop bound ended any path:
  * 2^20 tracking steps, 64 medium boundaries within a bounce, 256 along a
  * shadow ray (the reference's loops have no bound). */
@@ -287,6 +289,10 @@ r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_rend
  * R2_TRACK_STEPS / R2_TRAV_VISITS / R2_TRAV_REFILL). */
 r2_status r2_scene_set_tuning(r2_scene* scene, const r2_render_tuning* tuning);
 r2_status r2_scene_get_tuning(r2_scene* scene, r2_render_tuning* tuning);
+/* Samples of every pixel that one wave of this frame renders under the
+ * scene's tuning (stats_out[4..7] of r2_render_device time one such wave). */
+r2_status r2_scene_wave_samples(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
+                                uint32_t* samples_out);
 /* Autotuner: times one wave of this frame for each candidate value of one
  * setting at a time (scenes without media: refill lanes, then visits; with
  * media: tracking steps), keeps a candidate that is faster by more than 2 %,

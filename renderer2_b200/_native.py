@@ -85,6 +85,7 @@ def _load():
         "r2_scene_set_tuning": (C.c_int, [P, P]),
         "r2_scene_get_tuning": (C.c_int, [P, P]),
         "r2_scene_autotune": (C.c_int, [P, P, P, P]),
+        "r2_scene_wave_samples": (C.c_int, [P, P, P, P]),
         "r2_render_batch_create": (C.c_int, [P, P, P, P, u32, P]),
         "r2_render_batch_destroy": (C.c_int, [P]),
         "r2_render_batch_run": (C.c_int, [P, P, P]),

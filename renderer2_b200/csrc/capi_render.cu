@@ -125,6 +125,15 @@ r2_status r2_scene_get_tuning(r2_scene* scene, r2_render_tuning* tuning) {
   R2_API_END
 }
 
+r2_status r2_scene_wave_samples(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
+                                uint32_t* samples_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && camera && params && samples_out, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(params->spp > 0, R2_ERR_INVALID_ARGUMENT, "spp must be positive");
+  *samples_out = scene->impl->wave_spp(camera->width * camera->height, params->spp);
+  R2_API_END
+}
+
 r2_status r2_scene_autotune(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
                             r2_render_tuning* tuning_out) {
   R2_API_BEGIN

@@ -49,6 +49,13 @@ __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.
 __device__ __forceinline__ uint32_t wave_sample(const RenderLaunch& L) {
   return L.sampleDev ? *(volatile const uint32_t*)L.sampleDev : L.sample;
 }
+// Pixel and sample of path p of the wave (waves group consecutive samples).
+__device__ __forceinline__ uint32_t path_pixel(const RenderLaunch& L, uint32_t p) {
+  return L.waveSpp == 1u ? p : p % L.npix;
+}
+__device__ __forceinline__ uint32_t path_sample(const RenderLaunch& L, uint32_t p) {
+  return wave_sample(L) + (L.waveSpp == 1u ? 0u : p / L.npix);
+}
 __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
 
 // Closest hit over triangles, analytic shapes and (kMedia) medium boxes.
@@ -150,9 +157,10 @@ __device__ __forceinline__ uint32_t push_queue(uint32_t* q, uint32_t* count, boo
 
 __global__ void __launch_bounds__(256) k_camera(RenderLaunch L) {
   const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < L.npix; p += stride) {
-    const int px = (int)(p % (uint32_t)L.cam.W), py = (int)(p / (uint32_t)L.cam.W);
-    const U4 r = philox4x32_10(u4(wave_sample(L), kPurposeCamera, 0u, 0u), p, L.seed);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < L.wavePaths; p += stride) {
+    const uint32_t pix = path_pixel(L, p);
+    const int px = (int)(pix % (uint32_t)L.cam.W), py = (int)(pix / (uint32_t)L.cam.W);
+    const U4 r = philox4x32_10(u4(path_sample(L, p), kPurposeCamera, 0u, 0u), pix, L.seed);
     V3 o, d;
     camera_ray(L.cam, px, py, u01(r.x), &o, &d);
     L.st.rayO[p] = f4(o, __int_as_float(-1));
@@ -161,7 +169,7 @@ __global__ void __launch_bounds__(256) k_camera(RenderLaunch L) {
     L.st.L[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     L.st.q[0][p] = p;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) L.st.counts[0] = L.npix;
+  if (blockIdx.x == 0 && threadIdx.x == 0) L.st.counts[0] = L.wavePaths;
 }
 
 // Persistent BVH traversal with dynamic ray fetch (Aila and Laine,
@@ -320,7 +328,8 @@ __device__ __forceinline__ void resolve_path(const RenderLaunch& L, uint32_t p, 
       }
       if (segMed >= 0) {
         if (kInline) {
-          RngStream rs = rng_stream(p, L.seed, wave_sample(L), L.bounce, kPurposeMedium + (uint32_t)j);
+          RngStream rs = rng_stream(path_pixel(L, p), L.seed, path_sample(L, p), L.bounce,
+                                    kPurposeMedium + (uint32_t)j);
           T = T * instance_sample(S.media[segMed], seg, L.dda != 0, rs, &ev, &err);
           evMed = segMed;
           if (err) dead = true;
@@ -487,9 +496,13 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
           const uint2 jm = L.st.jM[k];
           owner = jm.x;
           med = __float_as_int(jd.w);
-          if (kSample) s.rng = rng_stream(owner, L.seed, wave_sample(L), L.bounce, kPurposeMedium + jm.y);
-          else s.rng = rng_resume(L.st.q[L.bounce & 1][owner >> 1], L.seed, wave_sample(L), L.bounce,
-                                  kPurposeShadowTr + (owner & 1u), jm.y);
+          if (kSample) {
+            s.rng = rng_stream(path_pixel(L, owner), L.seed, path_sample(L, owner), L.bounce, kPurposeMedium + jm.y);
+          } else {
+            const uint32_t op = L.st.q[L.bounce & 1][owner >> 1];
+            s.rng = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce,
+                               kPurposeShadowTr + (owner & 1u), jm.y);
+          }
           const int st = track_init<kDDA, kSample>(L.scene.media[med], make_ray(xyz(jo), xyz(jd), jo.w), &s);
           if (st == kTrackRunning) {
             active = true;
@@ -538,8 +551,9 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
     n = sh.type == kShapeCircle ? normalize(sh.normal) : normalize(pos - sh.center);
     m = L.scene.mats[sh.material];
   }
-  const U4 rA = philox4x32_10(u4(wave_sample(L), L.bounce, 0u, 1u), p, L.seed);
-  const U4 rB = philox4x32_10(u4(wave_sample(L), L.bounce, 1u, 1u), p, L.seed);
+  const uint32_t pix = path_pixel(L, p), smp = path_sample(L, p);
+  const U4 rA = philox4x32_10(u4(smp, L.bounce, 0u, 1u), pix, L.seed);
+  const U4 rB = philox4x32_10(u4(smp, L.bounce, 1u, 1u), pix, L.seed);
   const Frame fr = frame_from_normal(n);
   const V3 wo = -d;
   const V3 woT = to_local(fr, wo);
@@ -603,7 +617,7 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   const float cosine = fabsf(dot(n, dirW));
   V3 Tn = T * ((f * cosine) / pdf);
   if (L.bounce > 3) {
-    const U4 rC = philox4x32_10(u4(wave_sample(L), L.bounce, 2u, 1u), p, L.seed);
+    const U4 rC = philox4x32_10(u4(smp, L.bounce, 2u, 1u), pix, L.seed);
     const float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
     if (u01(rC.x) <= prr) return false;
     Tn = Tn / (1.0f - prr);
@@ -629,7 +643,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   const float S[6] = {c.x, c.y, c.z, c.w, e.x, e.y};
   const Sggx g = make_sggx(S, n);
   const V3 wo = -d;
-  RngStream rs = rng_stream(p, L.seed, wave_sample(L), L.bounce, kPurposeScatter);
+  RngStream rs = rng_stream(path_pixel(L, p), L.seed, path_sample(L, p), L.bounce, kPurposeScatter);
   float4 shO0 = make_float4(0, 0, 0, 0), shO1 = shO0, shD0 = shO0, shD1 = shO0, pre0 = shO0, pre1 = shO0;
   {
     V3 ldir;
@@ -676,7 +690,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   const Ray cr = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, normalize(wi), kDefaultTmax), wi));
   V3 Tn = T;
   if (L.bounce > 3) {
-    const U4 rC = philox4x32_10(u4(wave_sample(L), L.bounce, 2u, 1u), p, L.seed);
+    const U4 rC = philox4x32_10(u4(path_sample(L, p), L.bounce, 2u, 1u), path_pixel(L, p), L.seed);
     const float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
     if (u01(rC.x) <= prr) return false;
     Tn = Tn / (1.0f - prr);
@@ -813,8 +827,10 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
   }
   const V3 p1 = o + d * x.x;
   RngStream rs;
-  if (kInline)
-    rs = rng_resume(L.st.q[L.bounce & 1][slot >> 1], L.seed, wave_sample(L), L.bounce, kPurposeShadowTr + (slot & 1u), idx);
+  if (kInline) {
+    const uint32_t op = L.st.q[L.bounce & 1][slot >> 1];
+    rs = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce, kPurposeShadowTr + (slot & 1u), idx);
+  }
   int err = 0;
   for (int k = 0; k < kMaxShadowSegments; ++k) {
     const V3 off = offset_ray_origin(p0, normalize(p1 - p0));
@@ -896,15 +912,23 @@ __global__ void __launch_bounds__(256) k_accum(RenderLaunch L) {
   }
 }
 
+// Adds the wave's samples to the frame pixel by pixel in sample order, the
+// same additions as one wave per sample.
 __global__ void __launch_bounds__(256) k_finish(RenderLaunch L) {
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < L.npix; p += stride) {
-    V3 v = xyz(L.st.L[p]);
-    if (isnan(v.x) || isnan(v.y) || isnan(v.z) || isinf(v.x) || isinf(v.y) || isinf(v.z)) v = v3(0.0f);
-    else v = v / (float)L.spp;
-    L.frame[3 * p] += v.x;
-    L.frame[3 * p + 1] += v.y;
-    L.frame[3 * p + 2] += v.z;
+    float fx = L.frame[3 * p], fy = L.frame[3 * p + 1], fz = L.frame[3 * p + 2];
+    for (uint32_t k = 0; k < L.waveSpp; ++k) {
+      V3 v = xyz(L.st.L[p + k * L.npix]);
+      if (isnan(v.x) || isnan(v.y) || isnan(v.z) || isinf(v.x) || isinf(v.y) || isinf(v.z)) v = v3(0.0f);
+      else v = v / (float)L.spp;
+      fx += v.x;
+      fy += v.y;
+      fz += v.z;
+    }
+    L.frame[3 * p] = fx;
+    L.frame[3 * p + 1] = fy;
+    L.frame[3 * p + 2] = fz;
   }
 }
 
@@ -929,7 +953,7 @@ void query_track_blocks() {
   g_trackBlocks[0] = resident_blocks(k_track<false, false>, 128);
 }
 
-__global__ void k_advance_sample(uint32_t* sample) { *sample += 1u; }
+__global__ void k_advance_sample(uint32_t* sample, uint32_t n) { *sample += n; }
 
 void launch_track(const RenderLaunch& L, bool sample, int round, cudaStream_t s) {
   query_track_blocks();
@@ -997,7 +1021,7 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
   }
   k_finish<<<nblocks, 256, 0, s>>>(L);
   mark(5);
-  if (L.sampleDev) k_advance_sample<<<1, 1, 0, s>>>(L.sampleDev);
+  if (L.sampleDev) k_advance_sample<<<1, 1, 0, s>>>(L.sampleDev, L.waveSpp);
   if (tm) tm->n = ev;
   R2_CUDA(cudaGetLastError());
 }

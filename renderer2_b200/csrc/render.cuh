@@ -73,6 +73,7 @@ struct PathState {
 constexpr uint32_t kDefaultTrackSteps = 8;   // tracking steps a lane takes between refills
 constexpr uint32_t kDefaultTravVisits = 32;  // BVH visits between refill checks
 constexpr uint32_t kDefaultTravRefill = 8;   // finished lanes that trigger a refill
+constexpr uint32_t kDefaultWavePaths = 1u << 22;  // paths per wave a frame's samples are grouped to
 
 // PathState::counts layout: [0, 64) live paths per bounce, then two counters
 // per bounce (extension rays taken, shadow records taken).
@@ -87,8 +88,10 @@ struct RenderLaunch {
   Camera cam;
   PathState st;
   float* frame;       // W*H*3 linear RGB, row 0 = bottom (SFrame layout)
-  uint32_t npix;
-  uint32_t sample;    // sample index of the wave
+  uint32_t npix;      // pixels of the frame
+  uint32_t waveSpp;   // samples per wave (>= 1): path p is pixel p % npix, sample `sample` + p / npix
+  uint32_t wavePaths; // npix * waveSpp
+  uint32_t sample;    // first sample index of the wave
   uint32_t* sampleDev;  // nullable: device sample counter of a captured wave (read instead of `sample`)
   uint32_t spp;
   uint32_t maxDepth;
@@ -111,8 +114,9 @@ struct WaveTimer {
   int n = 0;
 };
 
-// One wave (one sample of every pixel).  With L.sampleDev the last launch
-// advances the device sample counter, so a captured wave replays as the next sample.
+// One wave (L.waveSpp consecutive samples of every pixel).  With L.sampleDev
+// the last launch advances the device sample counter by L.waveSpp, so a
+// captured wave replays as the next samples.
 void launch_render_wave(const RenderLaunch& L, int nblocks, cudaStream_t s, WaveTimer* tm = nullptr);
 // Occupancy queries of the persistent kernels, done before any capture.
 void prepare_render_launches();

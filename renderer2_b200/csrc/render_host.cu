@@ -312,8 +312,16 @@ void RenderScene::check_params(const r2_camera& c, const r2_render_params& p, co
   R2_REQUIRE((p.flags & ~R2_RENDER_BRICK_GRID) == 0, R2_ERR_INVALID_ARGUMENT, "unknown render flags");
 }
 
+uint32_t RenderScene::wave_spp(uint32_t npix, uint32_t spp) const {
+  const uint64_t target = tuning_.wave_paths ? tuning_.wave_paths : kDefaultWavePaths;
+  uint32_t best = 1;
+  for (uint32_t k = 2; k <= spp; ++k)
+    if (spp % k == 0 && (uint64_t)k * npix <= target && (uint64_t)k * npix < (1ull << 31)) best = k;
+  return best;
+}
+
 RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera& c, const r2_render_params& p,
-                                      float* d_frame) {
+                                      float* d_frame, uint32_t waveSpp) {
   RenderLaunch L;
   memset(&L, 0, sizeof(L));
   L.scene = view_;
@@ -321,6 +329,8 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   ctx.fill(&L.st);
   L.frame = d_frame;
   L.npix = c.width * c.height;
+  L.waveSpp = waveSpp;
+  L.wavePaths = L.npix * waveSpp;
   L.spp = p.spp;
   L.maxDepth = p.max_depth;
   L.seed = p.seed;
@@ -341,10 +351,11 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
   RenderContext& ctx = ctx_;
   if (!s) s = ctx.stream;
   const uint32_t npix = c.width * c.height;
-  ctx.ensure(npix, !media_.empty());
-  RenderLaunch L = make_launch(ctx, c, p, d_frame);
+  const uint32_t S = wave_spp(npix, p.spp);
+  ctx.ensure(npix * S, !media_.empty());
+  RenderLaunch L = make_launch(ctx, c, p, d_frame, S);
   R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
-  const int nblocks = wave_blocks(npix);
+  const int nblocks = wave_blocks(npix * S);
   R2_CUDA(cudaMemsetAsync(d_frame, 0, sizeof(float) * 3 * (size_t)npix, s));
   if (stats) {
     ctx.statBuf.reserve(2);
@@ -356,10 +367,11 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
     }
   }
   R2_CUDA(cudaEventRecord(ctx.ev0, s));
-  for (uint32_t smp = 0; smp < p.spp; ++smp) {
+  for (uint32_t smp = 0; smp < p.spp; smp += S) {
     L.sample = smp;
     // the middle wave of a frame is timed kernel by kernel when statistics are requested
-    launch_render_wave(L, nblocks, s, (stats && smp == p.spp / 2) ? ctx.timer.get() : nullptr);
+    const bool timed = stats && smp <= p.spp / 2 && p.spp / 2 < smp + S;
+    launch_render_wave(L, nblocks, s, timed ? ctx.timer.get() : nullptr);
   }
   R2_CUDA(cudaEventRecord(ctx.ev1, s));
   if (stats) {
@@ -385,14 +397,15 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
 
 void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame,
                                cudaStream_t s) {
-  RenderLaunch L = prepare(ctx, c, p, d_frame);
   const uint32_t npix = c.width * c.height;
+  const uint32_t S = wave_spp(npix, p.spp);
+  RenderLaunch L = prepare(ctx, c, p, d_frame, S);
   R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
   R2_CUDA(cudaMemsetAsync(ctx.sampleDev.get(), 0, sizeof(uint32_t), s));
   R2_CUDA(cudaMemsetAsync(d_frame, 0, sizeof(float) * 3 * (size_t)npix, s));
   prepare_render_launches();  // occupancy queries stay outside the capture
-  // one wave (reading its sample index from the device counter, which its
-  // last node advances), captured once and replayed per sample
+  // one wave (reading its first sample index from the device counter, which
+  // its last node advances), captured once and replayed spp / S times
   cudaStream_t cap = nullptr;
   R2_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   struct Guard {
@@ -407,7 +420,7 @@ void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_
   } guard{cap};
   R2_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
   try {
-    launch_render_wave(L, wave_blocks(npix), cap, nullptr);
+    launch_render_wave(L, wave_blocks(npix * S), cap, nullptr);
   } catch (...) {
     cudaGraph_t g = nullptr;
     cudaStreamEndCapture(cap, &g);
@@ -416,22 +429,24 @@ void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_
   }
   R2_CUDA(cudaStreamEndCapture(cap, &guard.g));
   R2_CUDA(cudaGraphInstantiate(&guard.e, guard.g, 0));
-  for (uint32_t smp = 0; smp < p.spp; ++smp) R2_CUDA(cudaGraphLaunch(guard.e, s));
+  for (uint32_t smp = 0; smp < p.spp; smp += S) R2_CUDA(cudaGraphLaunch(guard.e, s));
   // the executable graph may be destroyed while its launches are pending
 }
 
-RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame) {
+RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame,
+                                  uint32_t waveSpp) {
   check_params(c, p, d_frame);
   R2_REQUIRE(committed_, R2_ERR_INVALID_ARGUMENT, "scene not committed");
-  ctx.ensure(c.width * c.height, !media_.empty());
-  RenderLaunch L = make_launch(ctx, c, p, d_frame);
+  R2_REQUIRE(waveSpp >= 1 && p.spp % waveSpp == 0, R2_ERR_INVALID_ARGUMENT, "samples per wave must divide spp");
+  ctx.ensure(c.width * c.height * waveSpp, !media_.empty());
+  RenderLaunch L = make_launch(ctx, c, p, d_frame, waveSpp);
   L.sampleDev = ctx.sampleDev.get();
   return L;
 }
 
 void RenderScene::set_tuning(const r2_render_tuning& t) {
-  R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.reserved == 0, R2_ERR_INVALID_ARGUMENT,
-             "tuning out of range (track_steps <= 1024, trav_refill <= 32, reserved 0)");
+  R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31), R2_ERR_INVALID_ARGUMENT,
+             "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31)");
   tuning_ = t;
 }
 
@@ -444,52 +459,64 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
   if (!committed_) commit();
   RenderContext& ctx = ctx_;
   cudaStream_t s = ctx.stream;
-  r2_render_params p1 = p;
-  p1.spp = 1;
-  RenderLaunch L = prepare(ctx, c, p1, frame.get());
   prepare_render_launches();
-  const int nblocks = wave_blocks(npix);
-  // one wave of sample 0 per setting, the faster of two runs
+  const r2_render_tuning saved = tuning_;
+  // milliseconds per path of the frame's first wave under tuning t, the faster of two runs
   auto time_wave = [&](const r2_render_tuning& t) {
-    L.trackSteps = t.track_steps;
-    L.travVisits = t.trav_visits;
-    L.travRefill = t.trav_refill;
+    tuning_ = t;
+    const uint32_t S = wave_spp(npix, p.spp);
+    RenderLaunch L = prepare(ctx, c, p, frame.get(), S);
+    L.sampleDev = nullptr;
+    L.sample = 0;
     float best = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {
       R2_CUDA(cudaEventRecord(ctx.ev0, s));
-      launch_render_wave(L, nblocks, s, nullptr);
+      launch_render_wave(L, wave_blocks(npix * S), s, nullptr);
       R2_CUDA(cudaEventRecord(ctx.ev1, s));
       R2_CUDA(cudaEventSynchronize(ctx.ev1));
       float ms = 0.0f;
       R2_CUDA(cudaEventElapsedTime(&ms, ctx.ev0, ctx.ev1));
       best = std::min(best, ms);
     }
-    return best;
+    return best / ((float)S * (float)npix);
   };
-  r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, 0};
-  R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
-  time_wave(cur);  // warm-up
-  float curMs = time_wave(cur);
-  static const uint32_t refills[] = {2, 4, 16, 32};
-  static const uint32_t visits[] = {8, 16, 64, 256};
-  static const uint32_t steps[] = {2, 4, 16, 32};
-  auto sweep = [&](uint32_t r2_render_tuning::*field, const uint32_t* cand, int n) {
-    const r2_render_tuning base = cur;
-    for (int i = 0; i < n; ++i) {
-      r2_render_tuning t = base;
-      t.*field = cand[i];
-      const float ms = time_wave(t);
-      if (ms < curMs * 0.98f) {
-        cur = t;
-        curMs = ms;
+  r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths};
+  try {
+    R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
+    time_wave(cur);  // warm-up
+    float curT = time_wave(cur);
+    auto sweep = [&](uint32_t r2_render_tuning::*field, const uint32_t* cand, int n) {
+      const r2_render_tuning base = cur;
+      for (int i = 0; i < n; ++i) {
+        r2_render_tuning t = base;
+        t.*field = cand[i];
+        if (field == &r2_render_tuning::wave_paths) {  // skip settings that give the same waves
+          tuning_ = t;
+          const uint32_t S = wave_spp(npix, p.spp);
+          tuning_ = cur;
+          if (S == wave_spp(npix, p.spp)) continue;
+        }
+        const float ms = time_wave(t);
+        if (ms < curT * 0.98f) {
+          cur = t;
+          curT = ms;
+        }
       }
+    };
+    static const uint32_t wavePaths[] = {1u << 20, 1u << 21, 1u << 23, 1u << 24};
+    static const uint32_t refills[] = {2, 4, 16, 32};
+    static const uint32_t visits[] = {8, 16, 64, 256};
+    static const uint32_t steps[] = {2, 4, 16, 32};
+    sweep(&r2_render_tuning::wave_paths, wavePaths, 4);
+    if (media_.empty()) {  // the persistent surface traversals run in scenes without media
+      sweep(&r2_render_tuning::trav_refill, refills, 4);
+      sweep(&r2_render_tuning::trav_visits, visits, 4);
+    } else {
+      sweep(&r2_render_tuning::track_steps, steps, 4);
     }
-  };
-  if (media_.empty()) {  // the persistent surface traversals run in scenes without media
-    sweep(&r2_render_tuning::trav_refill, refills, 4);
-    sweep(&r2_render_tuning::trav_visits, visits, 4);
-  } else {
-    sweep(&r2_render_tuning::track_steps, steps, 4);
+  } catch (...) {
+    tuning_ = saved;
+    throw;
   }
   tuning_ = cur;
   return cur;
@@ -506,7 +533,8 @@ RenderBatch::RenderBatch(const std::vector<RenderScene*>& scenes, const std::vec
     R2_REQUIRE(scenes[i], R2_ERR_INVALID_ARGUMENT, "null scene in batch");
     R2_REQUIRE(params[i].spp == spp_, R2_ERR_INVALID_ARGUMENT, "all frames of a batch share the sample count");
     ctx_.emplace_back(new RenderContext());
-    Ls.push_back(scenes[i]->prepare(*ctx_.back(), cams[i], params[i], frames[i]));
+    // one sample per wave: the batch's frames together fill the GPU
+    Ls.push_back(scenes[i]->prepare(*ctx_.back(), cams[i], params[i], frames[i], 1));
     frames_.push_back(frames[i]);
     npix_.push_back((size_t)cams[i].width * cams[i].height);
   }

@@ -81,15 +81,20 @@ class RenderScene {
   void commit();
   bool committed() const { return committed_; }
   bool has_media() const { return !media_.empty(); }
-  // One frame: `spp` waves accumulated into d_frame (W*H*3 floats, cleared here),
-  // on the scene's own context.
+  // One frame: spp / wave_spp waves accumulated into d_frame (W*H*3 floats,
+  // cleared here), on the scene's own context.
   void render(const r2_camera& cam, const r2_render_params& p, float* d_frame, cudaStream_t s, double* stats);
   // The same frame on a caller's context and stream, one wave captured as a
-  // CUDA graph and replayed once per sample (the scene must be committed).
+  // CUDA graph and replayed spp / wave_spp times (the scene must be committed).
   void render_graph(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame,
                     cudaStream_t s);
-  // The launch description of a frame on ctx (its buffers grown to fit).
-  RenderLaunch prepare(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame);
+  // The launch description of a frame on ctx with waveSpp samples per wave
+  // (a divisor of p.spp; the context's buffers grown to fit).
+  RenderLaunch prepare(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame,
+                       uint32_t waveSpp);
+  // Samples per wave of a frame: the largest divisor of spp whose wave stays
+  // within the tuning's paths per wave (at least one).
+  uint32_t wave_spp(uint32_t npix, uint32_t spp) const;
   // Launch tuning (0 fields: the defaults) and the autotuner that sets it.
   void set_tuning(const r2_render_tuning& t);
   r2_render_tuning tuning() const { return tuning_; }
@@ -101,7 +106,8 @@ class RenderScene {
   const DeviceBvh& bvh() const { return bvh_; }
 
  private:
-  RenderLaunch make_launch(const RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame);
+  RenderLaunch make_launch(const RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame,
+                           uint32_t waveSpp);
   static void check_params(const r2_camera& c, const r2_render_params& p, const float* d_frame);
   RenderContext ctx_;
   bool committed_ = false;
@@ -125,7 +131,8 @@ class RenderScene {
 
 // Frames of several committed scenes rendered by one captured CUDA graph: the
 // graph holds one wave of every scene, each on its own branch (forked capture
-// streams), and is replayed once per sample.  Frames, cameras and parameters
+// streams), and is replayed once per sample (waves of one sample: the frames
+// together fill the GPU).  Frames, cameras and parameters
 // are fixed at construction; all entries share the sample count.
 class RenderBatch {
  public:

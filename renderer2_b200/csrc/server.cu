@@ -73,7 +73,7 @@ uint64_t Server::submit(std::unique_ptr<ServerJob> job) {
     R2_REQUIRE(npix > 0 && j->rp.spp > 0 && j->rp.max_depth > 0 && j->rp.max_depth <= 60, R2_ERR_INVALID_ARGUMENT,
                "bad render job");
     j->outBytes = (size_t)npix * 12;
-    j->bytes = RenderContext::bytes_for(npix, j->scene->has_media());
+    j->bytes = RenderContext::bytes_for(npix * j->scene->wave_spp(npix, j->rp.spp), j->scene->has_media());
   } else {
     R2_REQUIRE(j->fscene, R2_ERR_INVALID_ARGUMENT, "filter job needs a filter scene");
     const size_t nvox = (size_t)j->grid.num_voxels[0] * j->grid.num_voxels[1] * j->grid.num_voxels[2];

@@ -47,14 +47,18 @@ SPHERE, CIRCLE = 0, 1
 class Tuning(C.Structure):
     """Launch tuning (r2_render_tuning); 0 fields select the defaults; images never depend on it."""
     _fields_ = [("track_steps", C.c_uint32), ("trav_visits", C.c_uint32), ("trav_refill", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("wave_paths", C.c_uint32)]
+    NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths")
 
     def as_tuple(self):
-        return (self.track_steps, self.trav_visits, self.trav_refill)
+        return tuple(getattr(self, n) for n in self.NAMES)
+
+    def as_dict(self):
+        return dict(zip(self.NAMES, self.as_tuple()))
 
 
-def tuning(track_steps=0, trav_visits=0, trav_refill=0) -> Tuning:
-    return Tuning(track_steps, trav_visits, trav_refill, 0)
+def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0) -> Tuning:
+    return Tuning(track_steps, trav_visits, trav_refill, wave_paths)
 
 
 class Scene:
@@ -126,6 +130,12 @@ class Scene:
         t = Tuning()
         N.check(N.lib.r2_scene_get_tuning(self.handle, C.byref(t)))
         return t
+
+    def wave_samples(self, cam: Camera, prm: RenderParams) -> int:
+        """Samples of every pixel one wave of this frame renders (r2_scene_wave_samples)."""
+        n = C.c_uint32()
+        N.check(N.lib.r2_scene_wave_samples(self.handle, C.byref(cam), C.byref(prm), C.byref(n)))
+        return n.value
 
     def autotune(self, cam: Camera, prm: RenderParams) -> Tuning:
         """Times one wave of this frame per candidate setting and keeps the fastest (see r2_scene_autotune)."""

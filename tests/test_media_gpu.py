@@ -132,9 +132,10 @@ def test_medium_tracking_tuning_never_changes_the_frame(lods):
     sc = RS.build_scene(desc)
     prm = R.params(3, 8, 17, brick_grid=True)
     ref = sc.render(cam, prm)
-    for steps, visits, refill in [(1, 2, 1), (64, 7, 32)]:
-        sc.set_tuning(R.tuning(steps, visits, refill))
-        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill)
+    for steps, visits, refill, wave in [(1, 2, 1, 32 * 28), (64, 7, 32, 3 * 32 * 28)]:
+        sc.set_tuning(R.tuning(steps, visits, refill, wave))
+        assert sc.wave_samples(cam, prm) == wave // (32 * 28)
+        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill, wave)
     t = sc.autotune(cam, prm)
     assert t.track_steps >= 1
     assert np.array_equal(sc.render(cam, prm), ref)

@@ -126,11 +126,13 @@ def test_launch_tuning_never_changes_the_frame():
     cam = R.camera(96, 80, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
     prm = R.params(2, 8, 5)
     sc = RS.build_scene(desc)
+    sc.set_tuning(R.tuning(wave_paths=96 * 80))  # one sample per wave
     ref = sc.render(cam, prm)
-    for visits, refill in [(1, 1), (3, 32), (1000, 5), (64, 16)]:
-        sc.set_tuning(R.tuning(trav_visits=visits, trav_refill=refill))
-        assert sc.get_tuning().as_tuple() == (0, visits, refill)
-        assert np.array_equal(sc.render(cam, prm), ref), (visits, refill)
+    for visits, refill, wave in [(1, 1, 0), (3, 32, 96 * 80), (1000, 5, 2 * 96 * 80), (64, 16, 1 << 24)]:
+        sc.set_tuning(R.tuning(trav_visits=visits, trav_refill=refill, wave_paths=wave))
+        assert sc.get_tuning().as_tuple() == (0, visits, refill, wave)
+        assert sc.wave_samples(cam, prm) == (2 if wave != 96 * 80 else 1)
+        assert np.array_equal(sc.render(cam, prm), ref), (visits, refill, wave)
     t = sc.autotune(cam, prm)
     assert 1 <= t.trav_refill <= 32 and t.trav_visits >= 1
     assert sc.get_tuning().as_tuple() == t.as_tuple()
