@@ -57,6 +57,11 @@ __device__ __forceinline__ uint32_t path_sample(const RenderLaunch& L, uint32_t 
   return wave_sample(L) + (L.waveSpp == 1u ? 0u : p / L.npix);
 }
 __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
+// Entries of the kernel parameter's pointer pairs, picked with selects: a
+// dynamic index into an array inside the parameter makes the compiler copy the
+// whole launch description to local memory.
+__device__ __forceinline__ uint32_t* pick(uint32_t* const (&a)[2], uint32_t i) { return i ? a[1] : a[0]; }
+__device__ __forceinline__ uint32_t* path_queue(const RenderLaunch& L, uint32_t b) { return pick(L.st.q, b & 1u); }
 
 // Closest hit over triangles, analytic shapes and (kMedia) medium boxes.
 // Code: >= 0 triangle, -1 miss, -2 - i shape i, kMediumCodeBase - m medium m.
@@ -222,7 +227,7 @@ __device__ __forceinline__ int trav_refill(const RenderLaunch& L) { return (int)
 // Closest hit of every live path (scenes without media).
 __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = L.st.q[L.bounce & 1];
+  const uint32_t* q = path_queue(L, L.bounce);
   if (!L.scene.hasTris) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -384,7 +389,7 @@ template <bool kFirst, bool kInline>
 __global__ void __launch_bounds__(128) k_resolve(RenderLaunch L, int round) {
   uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce;
   const uint32_t n = kFirst ? *(volatile uint32_t*)&L.st.counts[L.bounce] : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
-  const uint32_t* list = kFirst ? L.st.q[L.bounce & 1] : L.st.rl[round - 1];
+  const uint32_t* list = kFirst ? path_queue(L, L.bounce) : pick(L.st.rl, (uint32_t)(round - 1));
   uint32_t* jobs = &mc[3 * round];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) resolve_path<kInline>(L, list[i], kFirst, jobs);
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
   const uint32_t njobs = *(volatile uint32_t*)&mc[3 * round];
   uint32_t* taken = &mc[3 * round + 1];
   uint32_t* nextCount = &mc[3 * round + 2];
-  uint32_t* nextList = kSample ? L.st.rl[round] : L.st.sl[round];
+  uint32_t* nextList = kSample ? pick(L.st.rl, (uint32_t)round) : pick(L.st.sl, (uint32_t)round);
   const int lane = threadIdx.x & 31;
   TrackState s;
   uint32_t owner = 0;
@@ -499,7 +504,7 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
           if (kSample) {
             s.rng = rng_stream(path_pixel(L, owner), L.seed, path_sample(L, owner), L.bounce, kPurposeMedium + jm.y);
           } else {
-            const uint32_t op = L.st.q[L.bounce & 1][owner >> 1];
+            const uint32_t op = path_queue(L, L.bounce)[owner >> 1];
             s.rng = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce,
                                kPurposeShadowTr + (owner & 1u), jm.y);
           }
@@ -532,6 +537,55 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
 
 // Surface shading: direct() at a surface and the sampleF continuation
 // (path_integrator_impl.hpp:23-118, 196-222).
+// Out-of-line copies of the large shading routines.  k_shade's lanes diverge
+// between lobes and events, and with every routine inlined at each call site
+// the kernel's code outgrew the instruction cache (warps stalled on
+// instruction fetch); one copy of each keeps the working set small.  The
+// arithmetic is the same, so results do not change.
+struct BsdfSample {
+  V3 f, wi;
+  float pdf;
+};
+__device__ __noinline__ BsdfSample bsdf_sample_nc(Material m, V3 wo, float uSel, float u1, float u2) {
+  BsdfSample r;
+  r.wi = v3(0.0f);
+  r.pdf = 0.0f;
+  r.f = mat_sample_f(m, wo, uSel, u1, u2, &r.wi, &r.pdf);
+  return r;
+}
+struct BsdfEval {
+  V3 f;
+  float pdf;
+};
+__device__ __noinline__ BsdfEval bsdf_eval_nc(Material m, V3 wo, V3 wi) {
+  BsdfEval r;
+  r.f = mat_f(m, wo, wi);
+  r.pdf = mat_pdf(m, wo, wi);
+  return r;
+}
+struct EnvSample {
+  V3 Le, dir;
+  float pdf;
+};
+__device__ __noinline__ EnvSample env_sample_nc(EnvMap e, float u0, float u1) {
+  EnvSample r;
+  r.dir = v3(0.0f);
+  r.pdf = 0.0f;
+  r.Le = env_sample(e, u0, u1, &r.dir, &r.pdf);
+  return r;
+}
+struct EnvEval {
+  V3 Le;
+  float pdf;
+};
+__device__ __noinline__ EnvEval env_le_nc(EnvMap e, V3 d) {
+  EnvEval r;
+  r.pdf = 0.0f;
+  r.Le = env_le(e, d, &r.pdf);
+  return r;
+}
+__device__ __noinline__ U4 philox_nc(U4 ctr, uint32_t k0, uint32_t k1) { return philox4x32_10(ctr, k0, k1); }
+
 template <bool kMedia>
 __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i, uint32_t p, int code, float4 hr,
                                               V3 o, V3 d, int med, V3 T) {
@@ -552,8 +606,8 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
     m = L.scene.mats[sh.material];
   }
   const uint32_t pix = path_pixel(L, p), smp = path_sample(L, p);
-  const U4 rA = philox4x32_10(u4(smp, L.bounce, 0u, 1u), pix, L.seed);
-  const U4 rB = philox4x32_10(u4(smp, L.bounce, 1u, 1u), pix, L.seed);
+  const U4 rA = philox_nc(u4(smp, L.bounce, 0u, 1u), pix, L.seed);
+  const U4 rB = philox_nc(u4(smp, L.bounce, 1u, 1u), pix, L.seed);
   const Frame fr = frame_from_normal(n);
   const V3 wo = -d;
   const V3 woT = to_local(fr, wo);
@@ -561,14 +615,15 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   float4 shO0 = make_float4(0, 0, 0, 0), shO1 = shO0, shD0 = shO0, shD1 = shO0, pre0 = shO0, pre1 = shO0;
   // --- direct(): light sample (path_integrator_impl.hpp:31-71)
   {
-    V3 ldir;
-    float lpdf = 0.0f;
-    const V3 Le = env_sample(L.scene.env, u01(rA.x), u01(rA.y), &ldir, &lpdf);
+    const EnvSample es = env_sample_nc(L.scene.env, u01(rA.x), u01(rA.y));
+    const V3 Le = es.Le;
+    const float lpdf = es.pdf;
     if (lpdf > 0.0f) {
-      ldir = normalize(ldir);
+      const V3 ldir = normalize(es.dir);
       const V3 lT = normalize(to_local(fr, ldir));
-      const V3 f = mat_f(m, woT, lT) * fabsf(dot(n, ldir));
-      const float spdf = mat_pdf(m, woT, lT);
+      const BsdfEval be = bsdf_eval_nc(m, woT, lT);
+      const V3 f = be.f * fabsf(dot(n, ldir));
+      const float spdf = be.pdf;
       const float mis = balance_heuristic(lpdf, spdf);
       shO0 = f4(offO, lpdf);
       shD0 = f4(ldir, 0.0f);
@@ -581,15 +636,15 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   }
   // --- direct(): BSDF sample (path_integrator_impl.hpp:74-113)
   {
-    V3 wiT = v3(0.0f);
-    float spdf = 0.0f;
-    V3 f = mat_sample_f(m, woT, u01(rA.z), u01(rA.w), u01(rB.x), &wiT, &spdf);
-    V3 wi = normalize(to_world(fr, wiT));
-    f = f * fabsf(dot(n, wi));
+    const BsdfSample bs = bsdf_sample_nc(m, woT, u01(rA.z), u01(rA.w), u01(rB.x));
+    const float spdf = bs.pdf;
+    V3 wi = normalize(to_world(fr, bs.wi));
+    const V3 f = bs.f * fabsf(dot(n, wi));
     if (spdf > 0.0f) {
       wi = normalize(wi);
-      float lpdf;
-      const V3 Le = env_le(L.scene.env, wi, &lpdf);
+      const EnvEval ee = env_le_nc(L.scene.env, wi);
+      const V3 Le = ee.Le;
+      const float lpdf = ee.pdf;
       const float mis = balance_heuristic(spdf, lpdf);
       shO1 = f4(offO, spdf);
       shD1 = f4(wi, 0.0f);
@@ -609,15 +664,15 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   L.st.shT[i] = f4(T, 0.0f);
   // --- continuation (path_integrator_impl.hpp:200-232)
   const V3 dT = normalize(to_local(fr, d));
-  V3 wi = v3(0.0f);
-  float pdf = 0.0f;
-  const V3 f = mat_sample_f(m, -dT, u01(rB.y), u01(rB.z), u01(rB.w), &wi, &pdf);
+  const BsdfSample cs = bsdf_sample_nc(m, -dT, u01(rB.y), u01(rB.z), u01(rB.w));
+  const V3 wi = cs.wi, f = cs.f;
+  const float pdf = cs.pdf;
   if (pdf == 0.0f) return false;
   const V3 dirW = normalize(to_world(fr, wi));
   const float cosine = fabsf(dot(n, dirW));
   V3 Tn = T * ((f * cosine) / pdf);
   if (L.bounce > 3) {
-    const U4 rC = philox4x32_10(u4(smp, L.bounce, 2u, 1u), pix, L.seed);
+    const U4 rC = philox_nc(u4(smp, L.bounce, 2u, 1u), pix, L.seed);
     const float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
     if (u01(rC.x) <= prr) return false;
     Tn = Tn / (1.0f - prr);
@@ -703,10 +758,10 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
 }
 
 template <bool kMedia>
-__global__ void __launch_bounds__(128) k_shade(RenderLaunch L) {
+__global__ void __launch_bounds__(128, 5) k_shade(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = L.st.q[L.bounce & 1];
-  uint32_t* qn = L.st.q[(L.bounce + 1) & 1];
+  const uint32_t* q = path_queue(L, L.bounce);
+  uint32_t* qn = path_queue(L, L.bounce + 1);
   uint32_t* cn = &L.st.counts[L.bounce + 1];
   const uint32_t stride = gridDim.x * blockDim.x;
   // uniform trip count per warp so the ballot below sees the whole warp
@@ -723,8 +778,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderLaunch L) {
       const V3 T = xyz(L.st.T[p]);
       if (code == -1 || code == kEventDead) {
         if (code == -1 && L.bounce == 0) {
-          float lp;
-          const V3 le = env_le(L.scene.env, d, &lp);
+          const V3 le = env_le_nc(L.scene.env, d).Le;
           L.st.L[p] = f4(xyz(L.st.L[p]) + le * T, 0.0f);
         }
         const float4 z = make_float4(0, 0, 0, 0);
@@ -828,7 +882,7 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
   const V3 p1 = o + d * x.x;
   RngStream rs;
   if (kInline) {
-    const uint32_t op = L.st.q[L.bounce & 1][slot >> 1];
+    const uint32_t op = path_queue(L, L.bounce)[slot >> 1];
     rs = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce, kPurposeShadowTr + (slot & 1u), idx);
   }
   int err = 0;
@@ -874,7 +928,7 @@ template <bool kFirst, bool kInline>
 __global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int round) {
   uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce + kShadowCounters;
   const uint32_t n = kFirst ? 2 * *(volatile uint32_t*)&L.st.counts[L.bounce] : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
-  const uint32_t* list = kFirst ? nullptr : L.st.sl[round - 1];
+  const uint32_t* list = kFirst ? nullptr : pick(L.st.sl, (uint32_t)(round - 1));
   uint32_t* jobs = &mc[3 * round];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -898,7 +952,7 @@ __global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int roun
 
 __global__ void __launch_bounds__(256) k_accum(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = L.st.q[L.bounce & 1];
+  const uint32_t* q = path_queue(L, L.bounce);
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const float4 o0 = L.st.shO[2 * i], o1 = L.st.shO[2 * i + 1];
