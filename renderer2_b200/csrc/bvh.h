@@ -124,15 +124,18 @@ R2_HD int bvh_leaf_first(int ref) { return (~ref) & 0x03FFFFFF; }
 R2_HD int bvh_leaf_count(int ref) { return ((~ref) >> 26) & 0x1F; }
 
 // A ray's traversal that can stop after any node or leaf and resume later:
-// the per-ray constants, the best hit so far, the node to visit next and the
-// depth of the caller-held stack.
+// the per-ray constants, the best hit so far, the node to visit next (or
+// kTraceDone), a postponed leaf (0: none) and the depth of the caller-held stack.
 struct TraceState {
   RayPre r;
   Hit best;
   int cur;
+  int leaf;
   int sp;
   int found;
 };
+
+constexpr int kTraceDone = 0x7FFFFFFF;  // no node left to visit (never a node index)
 
 R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax) {
   s.r = make_ray_pre(o, d);
@@ -140,22 +143,47 @@ R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax) {
   s.best.b1 = s.best.b2 = 0.0f;
   s.best.tri = 0x7FFFFFFF;
   s.cur = 0;  // root is internal node 0
+  s.leaf = 0;
   s.sp = 0;
   s.found = 0;
 }
 
-// Visits up to maxVisits nodes or leaves; true when the query has finished
-// (closest hit in (0, tmax], kAnyHit: the first hit found) with s.best.tri the
-// BVH-order index, -1 on a miss.  Stack entries hold child references with
-// their entry distance; leaves are tested when reached.  The builder bounds the
-// tree depth by R2_BVH_STACK so the stack cannot overflow.  The visiting order
-// does not depend on where the visits are split, and the closest hit does not
-// depend on the visiting order.
+// Next stacked child whose entry distance is not beyond the closest hit.
+R2_HD int trace_pop(TraceState& s, const int* stack, const float* stackT) {
+  while (s.sp > 0) {
+    --s.sp;
+    if (stackT[s.sp] <= s.best.t) return stack[s.sp];
+  }
+  return kTraceDone;
+}
+
+// True when every lane of the warp running this loop holds a postponed leaf.
+R2_HD bool trace_all_have_leaf(bool mine) {
+#if defined(__CUDA_ARCH__)
+  return !__any_sync(__activemask(), !mine);
+#else
+  return mine;
+#endif
+}
+
+// Visits about maxVisits nodes and triangles; true when the query has
+// finished (closest hit in (0, tmax], kAnyHit: the first hit found) with
+// s.best.tri the BVH-order index, -1 on a miss.  Speculative while-while
+// traversal (Aila and Laine, "Understanding the Efficiency of Ray Traversal on
+// GPUs", HPG 2009): inner nodes are visited until every lane of the warp has
+// met a leaf, which is postponed while traversal continues; then the lanes
+// test their leaves together.  Stack entries hold child references with their
+// entry distance.  The builder bounds the tree depth by R2_BVH_STACK so the
+// stack cannot overflow.  The closest hit does not depend on the visiting
+// order (ties go to the lower triangle index).
 template <bool kAnyHit>
 R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* stackT, int maxVisits) {
-  for (int v = 0; v < maxVisits; ++v) {
-    const int cur = s.cur;
-    if (cur >= 0) {
+  int budget = maxVisits;
+  while (budget > 0) {
+    // inner nodes, the first leaf met postponed
+    while (s.cur >= 0 && s.cur != kTraceDone && budget > 0) {
+      --budget;
+      const int cur = s.cur;
 #if defined(__CUDA_ARCH__)
       const float4 b0 = __ldg(&bvh.nodes[cur].b0);
       const float4 b1 = __ldg(&bvh.nodes[cur].b1);
@@ -178,17 +206,24 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
         stackT[s.sp] = farT;
         ++s.sp;
         s.cur = nearC;
-        continue;
       } else if (h0) {
         s.cur = ch.x;
-        continue;
       } else if (h1) {
         s.cur = ch.y;
-        continue;
+      } else {
+        s.cur = trace_pop(s, stack, stackT);
       }
-    } else {
-      const int first = bvh_leaf_first(cur);
-      const int count = bvh_leaf_count(cur);
+      if (s.cur < 0 && s.leaf == 0) {
+        s.leaf = s.cur;
+        s.cur = trace_pop(s, stack, stackT);
+      }
+      if (trace_all_have_leaf(s.leaf != 0)) break;
+    }
+    // postponed leaves, and a leaf met right after one
+    while (s.leaf < 0) {
+      const int first = bvh_leaf_first(s.leaf);
+      const int count = bvh_leaf_count(s.leaf);
+      budget -= count;
       for (int i = 0; i < count; ++i) {
         const int tri = first + i;
 #if defined(__CUDA_ARCH__)
@@ -202,20 +237,23 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
 #endif
         if (tri_test(s.r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &s.best)) {
           s.found = 1;
-          if (kAnyHit) return true;
+          if (kAnyHit) {
+            s.leaf = 0;
+            s.cur = kTraceDone;
+            return true;
+          }
         }
       }
-    }
-    // pop the next child whose entry distance is not beyond the closest hit
-    while (true) {
-      if (s.sp == 0) {
-        if (!s.found) s.best.tri = -1;
-        return true;
+      s.leaf = 0;
+      if (s.cur < 0) {
+        s.leaf = s.cur;
+        s.cur = trace_pop(s, stack, stackT);
       }
-      --s.sp;
-      if (stackT[s.sp] <= s.best.t) break;
     }
-    s.cur = stack[s.sp];
+    if (s.cur == kTraceDone) {
+      if (!s.found) s.best.tri = -1;
+      return true;
+    }
   }
   return false;
 }

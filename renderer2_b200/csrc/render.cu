@@ -185,13 +185,18 @@ __global__ void __launch_bounds__(256) k_camera(RenderLaunch L) {
 // behind the warp's longest ray.  begin(k, s, &item) starts item k (false: it
 // needed no traversal and is done); end(item, s) consumes a finished query.
 // Results do not depend on visits or refill.
+// A ray still unfinished after kMaxTraceVisits visits (a correct traversal
+// visits each node at most once) is ended as a miss and counted in *bound.
+constexpr int kMaxTraceVisits = 1 << 26;
+
 template <bool kAnyHit, class Begin, class End>
 __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n, uint32_t* taken, int visits,
-                                                 int refill, Begin begin, End end) {
+                                                 int refill, unsigned int* bound, Begin begin, End end) {
   int stack[R2_BVH_STACK];
   float stackT[R2_BVH_STACK];
   TraceState s;
   uint32_t item = 0;
+  int spent = 0;  // visits of the lane's current ray
   bool active = false;
   bool more = true;  // warp-uniform: the queue may still hold items
   const int lane = threadIdx.x & 31;
@@ -206,7 +211,10 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
         if (base + (uint32_t)nIdle >= n) more = false;
         if (!active) {
           const uint32_t k = base + (uint32_t)__popc(idle & ((1u << lane) - 1u));
-          if (k < n) active = begin(k, s, &item);
+          if (k < n) {
+            active = begin(k, s, &item);
+            spent = 0;
+          }
         }
       }
     }
@@ -214,9 +222,18 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
       if (!more) break;
       continue;
     }
-    if (active && trace_advance<kAnyHit>(bvh, s, stack, stackT, visits)) {
-      end(item, s);
-      active = false;
+    if (active) {
+      bool done = trace_advance<kAnyHit>(bvh, s, stack, stackT, visits);
+      spent += visits;
+      if (!done && spent >= kMaxTraceVisits) {
+        s.best.tri = -1;
+        atomicAdd(bound, 1u);
+        done = true;
+      }
+      if (done) {
+        end(item, s);
+        active = false;
+      }
     }
   }
 }
@@ -246,7 +263,7 @@ __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
     L.st.hit[p] = scene_closest_after<false>(L.scene, s.r.o, s.r.d, kDefaultTmax, s.best);
   };
   trace_persistent<false>(L.scene.bvh, n, &L.st.counts[kTravCounters + 2 * L.bounce], trav_visits(L),
-                          trav_refill(L), begin, end);
+                          trav_refill(L), L.bound, begin, end);
 }
 
 // ------------------------------------------------------------------ media: path extension
@@ -585,6 +602,31 @@ __device__ __noinline__ EnvEval env_le_nc(EnvMap e, V3 d) {
   return r;
 }
 __device__ __noinline__ U4 philox_nc(U4 ctr, uint32_t k0, uint32_t k1) { return philox4x32_10(ctr, k0, k1); }
+// Phase functions of a medium collision (SGGX, or Henyey-Greenstein for media
+// with "G"); the stream is passed through by value.
+struct PhaseEval {
+  float p;
+  RngStream rs;
+};
+__device__ __noinline__ PhaseEval phase_eval_nc(const MediumView* M, Sggx g, float ior, V3 wo, V3 wi, RngStream rs) {
+  PhaseEval r;
+  r.p = M->hg ? phase_hg(dot(wo, wi), M->g) : sggx_p(g, ior, wo, wi, rs);
+  r.rs = rs;
+  return r;
+}
+struct PhaseSample {
+  V3 wi;
+  float p;
+  RngStream rs;
+};
+__device__ __noinline__ PhaseSample phase_sample_nc(const MediumView* M, Sggx g, float ior, V3 wo, RngStream rs) {
+  PhaseSample r;
+  r.wi = v3(0.0f);
+  r.p = M->hg ? hg_sample_p(M->g, wo, &r.wi, rs) : sggx_sample_p(g, ior, wo, &r.wi, rs);
+  r.rs = rs;
+  return r;
+}
+__device__ __noinline__ Ray voxel_border_nc(const MediumView* M, Ray r) { return instance_move_to_voxel_border(*M, r); }
 
 template <bool kMedia>
 __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i, uint32_t p, int code, float4 hr,
@@ -701,15 +743,17 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   RngStream rs = rng_stream(path_pixel(L, p), L.seed, path_sample(L, p), L.bounce, kPurposeScatter);
   float4 shO0 = make_float4(0, 0, 0, 0), shO1 = shO0, shD0 = shO0, shD1 = shO0, pre0 = shO0, pre1 = shO0;
   {
-    V3 ldir;
-    float lpdf = 0.0f;
     const float u0 = rs.next();
     const float u1 = rs.next();
-    const V3 Le = env_sample(L.scene.env, u0, u1, &ldir, &lpdf);
+    const EnvSample es = env_sample_nc(L.scene.env, u0, u1);
+    const V3 Le = es.Le;
+    const float lpdf = es.pdf;
     if (lpdf > 0.0f) {
-      ldir = normalize(ldir);
-      const Ray lr = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, ldir, kDefaultTmax), n));
-      const float sp = M.hg ? phase_hg(dot(wo, ldir), M.g) : sggx_p(g, ior, wo, ldir, rs);
+      const V3 ldir = normalize(es.dir);
+      const Ray lr = voxel_border_nc(&M, ray_offset(make_ray(pos, ldir, kDefaultTmax), n));
+      const PhaseEval pe = phase_eval_nc(&M, g, ior, wo, ldir, rs);
+      rs = pe.rs;
+      const float sp = pe.p;
       const float mis = balance_heuristic(lpdf, sp);
       shO0 = f4(lr.o, lpdf);
       shD0 = f4(lr.d, 0.0f);
@@ -718,13 +762,15 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
     }
   }
   {
-    V3 wi = v3(0.0f);
-    const float sp = M.hg ? hg_sample_p(M.g, wo, &wi, rs) : sggx_sample_p(g, ior, wo, &wi, rs);
+    const PhaseSample ps = phase_sample_nc(&M, g, ior, wo, rs);
+    rs = ps.rs;
+    const float sp = ps.p;
     if (sp > 0.0f) {
-      wi = normalize(wi);
-      const Ray br = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, wi, kDefaultTmax), n));
-      float lpdf;
-      const V3 Le = env_le(L.scene.env, wi, &lpdf);
+      const V3 wi = normalize(ps.wi);
+      const Ray br = voxel_border_nc(&M, ray_offset(make_ray(pos, wi, kDefaultTmax), n));
+      const EnvEval ee = env_le_nc(L.scene.env, wi);
+      const V3 Le = ee.Le;
+      const float lpdf = ee.pdf;
       const float mis = balance_heuristic(sp, lpdf);
       shO1 = f4(br.o, sp);
       shD1 = f4(br.d, 0.0f);
@@ -739,13 +785,11 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   L.st.shPre[2 * i] = pre0;
   L.st.shPre[2 * i + 1] = pre1;
   L.st.shT[i] = f4(T, 0.0f);
-  V3 wi = v3(0.0f);
-  if (M.hg) hg_sample_p(M.g, wo, &wi, rs);
-  else sggx_sample_p(g, ior, wo, &wi, rs);
-  const Ray cr = instance_move_to_voxel_border(M, ray_offset(make_ray(pos, normalize(wi), kDefaultTmax), wi));
+  const V3 wi = phase_sample_nc(&M, g, ior, wo, rs).wi;
+  const Ray cr = voxel_border_nc(&M, ray_offset(make_ray(pos, normalize(wi), kDefaultTmax), wi));
   V3 Tn = T;
   if (L.bounce > 3) {
-    const U4 rC = philox4x32_10(u4(path_sample(L, p), L.bounce, 2u, 1u), path_pixel(L, p), L.seed);
+    const U4 rC = philox_nc(u4(path_sample(L, p), L.bounce, 2u, 1u), path_pixel(L, p), L.seed);
     const float prr = 1.0f - (Tn.x + Tn.y + Tn.z) / 3.0f;
     if (u01(rC.x) <= prr) return false;
     Tn = Tn / (1.0f - prr);
@@ -758,7 +802,7 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
 }
 
 template <bool kMedia>
-__global__ void __launch_bounds__(128, 5) k_shade(RenderLaunch L) {
+__global__ void __launch_bounds__(128, kMedia ? 4 : 5) k_shade(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
   const uint32_t* q = path_queue(L, L.bounce);
   uint32_t* qn = path_queue(L, L.bounce + 1);
@@ -833,7 +877,7 @@ __global__ void __launch_bounds__(128) k_shadow_surfaces(RenderLaunch L) {
       L.st.shTr[j] = occluded ? 0.0f : 1.0f;
     };
     trace_persistent<true>(L.scene.bvh, 2 * n, &L.st.counts[kTravCounters + 2 * L.bounce + 1], trav_visits(L),
-                           trav_refill(L), begin, end);
+                           trav_refill(L), L.bound, begin, end);
   }
   if (L.stats) {
     for (int o = 16; o > 0; o >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, o);
