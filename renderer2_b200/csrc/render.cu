@@ -177,6 +177,80 @@ __global__ void __launch_bounds__(256) k_camera(RenderLaunch L) {
   if (blockIdx.x == 0 && threadIdx.x == 0) L.st.counts[0] = L.wavePaths;
 }
 
+// Out-of-line copies of the large shading routines.  k_shade's lanes diverge
+// between lobes and events, and with every routine inlined at each call site
+// the kernel's code outgrew the instruction cache (warps stalled on
+// instruction fetch); one copy of each keeps the working set small.  The
+// arithmetic is the same, so results do not change.
+struct BsdfSample {
+  V3 f, wi;
+  float pdf;
+};
+__device__ __noinline__ BsdfSample bsdf_sample_nc(Material m, V3 wo, float uSel, float u1, float u2) {
+  BsdfSample r;
+  r.wi = v3(0.0f);
+  r.pdf = 0.0f;
+  r.f = mat_sample_f(m, wo, uSel, u1, u2, &r.wi, &r.pdf);
+  return r;
+}
+struct BsdfEval {
+  V3 f;
+  float pdf;
+};
+__device__ __noinline__ BsdfEval bsdf_eval_nc(Material m, V3 wo, V3 wi) {
+  BsdfEval r;
+  r.f = mat_f(m, wo, wi);
+  r.pdf = mat_pdf(m, wo, wi);
+  return r;
+}
+struct EnvSample {
+  V3 Le, dir;
+  float pdf;
+};
+__device__ __noinline__ EnvSample env_sample_nc(EnvMap e, float u0, float u1) {
+  EnvSample r;
+  r.dir = v3(0.0f);
+  r.pdf = 0.0f;
+  r.Le = env_sample(e, u0, u1, &r.dir, &r.pdf);
+  return r;
+}
+struct EnvEval {
+  V3 Le;
+  float pdf;
+};
+__device__ __noinline__ EnvEval env_le_nc(EnvMap e, V3 d) {
+  EnvEval r;
+  r.pdf = 0.0f;
+  r.Le = env_le(e, d, &r.pdf);
+  return r;
+}
+__device__ __noinline__ U4 philox_nc(U4 ctr, uint32_t k0, uint32_t k1) { return philox4x32_10(ctr, k0, k1); }
+// Phase functions of a medium collision (SGGX, or Henyey-Greenstein for media
+// with "G"); the stream is passed through by value.
+struct PhaseEval {
+  float p;
+  RngStream rs;
+};
+__device__ __noinline__ PhaseEval phase_eval_nc(const MediumView* M, Sggx g, float ior, V3 wo, V3 wi, RngStream rs) {
+  PhaseEval r;
+  r.p = M->hg ? phase_hg(dot(wo, wi), M->g) : sggx_p(g, ior, wo, wi, rs);
+  r.rs = rs;
+  return r;
+}
+struct PhaseSample {
+  V3 wi;
+  float p;
+  RngStream rs;
+};
+__device__ __noinline__ PhaseSample phase_sample_nc(const MediumView* M, Sggx g, float ior, V3 wo, RngStream rs) {
+  PhaseSample r;
+  r.wi = v3(0.0f);
+  r.p = M->hg ? hg_sample_p(M->g, wo, &r.wi, rs) : sggx_sample_p(g, ior, wo, &r.wi, rs);
+  r.rs = rs;
+  return r;
+}
+__device__ __noinline__ Ray voxel_border_nc(const MediumView* M, Ray r) { return instance_move_to_voxel_border(*M, r); }
+
 // Persistent BVH traversal with dynamic ray fetch (Aila and Laine,
 // "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009): the
 // lanes of a warp run their rays in rounds of `visits` node/leaf visits, and
@@ -241,7 +315,22 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
 __device__ __forceinline__ int trav_visits(const RenderLaunch& L) { return (int)max(1u, L.travVisits); }
 __device__ __forceinline__ int trav_refill(const RenderLaunch& L) { return (int)min(32u, max(1u, L.travRefill)); }
 
-// Closest hit of every live path (scenes without media).
+// Closest hit of every live path (scenes without media).  A path that hits a
+// surface goes to the bounce's hit queue (shading, shadow rays and
+// accumulation then run over hits only); a miss ends the path here with the
+// environment term of the first bounce (k_shade's miss rule).
+__device__ __forceinline__ void extend_result(const RenderLaunch& L, uint32_t p, V3 d, float4 h) {
+  if (__float_as_int(h.w) == -1) {
+    if (L.bounce == 0) {
+      const V3 le = env_le_nc(L.scene.env, d).Le;
+      L.st.L[p] = f4(xyz(L.st.L[p]) + le * xyz(L.st.T[p]), 0.0f);
+    }
+  } else {
+    L.st.hit[p] = h;
+  }
+  push_queue(L.st.qh, &L.st.counts[kHitCounters + L.bounce], __float_as_int(h.w) != -1, p);
+}
+
 __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
   const uint32_t* q = path_queue(L, L.bounce);
@@ -249,7 +338,8 @@ __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
       const uint32_t p = q[i];
-      L.st.hit[p] = scene_closest<false>(L.scene, xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), kDefaultTmax);
+      const V3 d = xyz(L.st.rayD[p]);
+      extend_result(L, p, d, scene_closest<false>(L.scene, xyz(L.st.rayO[p]), d, kDefaultTmax));
     }
     return;
   }
@@ -260,7 +350,7 @@ __global__ void __launch_bounds__(128) k_extend(RenderLaunch L) {
     return true;
   };
   auto end = [&](uint32_t p, const TraceState& s) {
-    L.st.hit[p] = scene_closest_after<false>(L.scene, s.r.o, s.r.d, kDefaultTmax, s.best);
+    extend_result(L, p, s.r.d, scene_closest_after<false>(L.scene, s.r.o, s.r.d, kDefaultTmax, s.best));
   };
   trace_persistent<false>(L.scene.bvh, n, &L.st.counts[kTravCounters + 2 * L.bounce], trav_visits(L),
                           trav_refill(L), L.bound, begin, end);
@@ -554,80 +644,6 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
 
 // Surface shading: direct() at a surface and the sampleF continuation
 // (path_integrator_impl.hpp:23-118, 196-222).
-// Out-of-line copies of the large shading routines.  k_shade's lanes diverge
-// between lobes and events, and with every routine inlined at each call site
-// the kernel's code outgrew the instruction cache (warps stalled on
-// instruction fetch); one copy of each keeps the working set small.  The
-// arithmetic is the same, so results do not change.
-struct BsdfSample {
-  V3 f, wi;
-  float pdf;
-};
-__device__ __noinline__ BsdfSample bsdf_sample_nc(Material m, V3 wo, float uSel, float u1, float u2) {
-  BsdfSample r;
-  r.wi = v3(0.0f);
-  r.pdf = 0.0f;
-  r.f = mat_sample_f(m, wo, uSel, u1, u2, &r.wi, &r.pdf);
-  return r;
-}
-struct BsdfEval {
-  V3 f;
-  float pdf;
-};
-__device__ __noinline__ BsdfEval bsdf_eval_nc(Material m, V3 wo, V3 wi) {
-  BsdfEval r;
-  r.f = mat_f(m, wo, wi);
-  r.pdf = mat_pdf(m, wo, wi);
-  return r;
-}
-struct EnvSample {
-  V3 Le, dir;
-  float pdf;
-};
-__device__ __noinline__ EnvSample env_sample_nc(EnvMap e, float u0, float u1) {
-  EnvSample r;
-  r.dir = v3(0.0f);
-  r.pdf = 0.0f;
-  r.Le = env_sample(e, u0, u1, &r.dir, &r.pdf);
-  return r;
-}
-struct EnvEval {
-  V3 Le;
-  float pdf;
-};
-__device__ __noinline__ EnvEval env_le_nc(EnvMap e, V3 d) {
-  EnvEval r;
-  r.pdf = 0.0f;
-  r.Le = env_le(e, d, &r.pdf);
-  return r;
-}
-__device__ __noinline__ U4 philox_nc(U4 ctr, uint32_t k0, uint32_t k1) { return philox4x32_10(ctr, k0, k1); }
-// Phase functions of a medium collision (SGGX, or Henyey-Greenstein for media
-// with "G"); the stream is passed through by value.
-struct PhaseEval {
-  float p;
-  RngStream rs;
-};
-__device__ __noinline__ PhaseEval phase_eval_nc(const MediumView* M, Sggx g, float ior, V3 wo, V3 wi, RngStream rs) {
-  PhaseEval r;
-  r.p = M->hg ? phase_hg(dot(wo, wi), M->g) : sggx_p(g, ior, wo, wi, rs);
-  r.rs = rs;
-  return r;
-}
-struct PhaseSample {
-  V3 wi;
-  float p;
-  RngStream rs;
-};
-__device__ __noinline__ PhaseSample phase_sample_nc(const MediumView* M, Sggx g, float ior, V3 wo, RngStream rs) {
-  PhaseSample r;
-  r.wi = v3(0.0f);
-  r.p = M->hg ? hg_sample_p(M->g, wo, &r.wi, rs) : sggx_sample_p(g, ior, wo, &r.wi, rs);
-  r.rs = rs;
-  return r;
-}
-__device__ __noinline__ Ray voxel_border_nc(const MediumView* M, Ray r) { return instance_move_to_voxel_border(*M, r); }
-
 template <bool kMedia>
 __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i, uint32_t p, int code, float4 hr,
                                               V3 o, V3 d, int med, V3 T) {
@@ -803,8 +819,9 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
 
 template <bool kMedia>
 __global__ void __launch_bounds__(128, kMedia ? 4 : 5) k_shade(RenderLaunch L) {
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = path_queue(L, L.bounce);
+  // scenes without media shade the bounce's surface hits (k_extend ended the misses)
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[kMedia ? L.bounce : kHitCounters + L.bounce];
+  const uint32_t* q = kMedia ? path_queue(L, L.bounce) : L.st.qh;
   uint32_t* qn = path_queue(L, L.bounce + 1);
   uint32_t* cn = &L.st.counts[L.bounce + 1];
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -840,7 +857,7 @@ __global__ void __launch_bounds__(128, kMedia ? 4 : 5) k_shade(RenderLaunch L) {
 
 // Visibility of every shadow record of a scene without media.
 __global__ void __launch_bounds__(128) k_shadow_surfaces(RenderLaunch L) {
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[kHitCounters + L.bounce];
   uint32_t traced = 0;
   if (!L.scene.hasTris) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -882,7 +899,7 @@ __global__ void __launch_bounds__(128) k_shadow_surfaces(RenderLaunch L) {
   if (L.stats) {
     for (int o = 16; o > 0; o >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, o);
     if ((threadIdx.x & 31) == 0 && traced) atomicAdd(&L.stats[1], (unsigned long long)traced);
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)L.st.counts[L.bounce]);
   }
 }
 
@@ -995,8 +1012,9 @@ __global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int roun
 }
 
 __global__ void __launch_bounds__(256) k_accum(RenderLaunch L) {
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
-  const uint32_t* q = path_queue(L, L.bounce);
+  const bool hitsOnly = L.scene.nmedia == 0;  // shadow records of the hit queue
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[hitsOnly ? kHitCounters + L.bounce : L.bounce];
+  const uint32_t* q = hitsOnly ? L.st.qh : path_queue(L, L.bounce);
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const float4 o0 = L.st.shO[2 * i], o1 = L.st.shO[2 * i + 1];
@@ -1081,7 +1099,7 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
     tm->kind[ev] = kind;
     ++ev;
   };
-  R2_CUDA(cudaMemsetAsync(L.st.counts, 0, sizeof(uint32_t) * (kTravCounters + 2 * L.maxDepth), s));
+  R2_CUDA(cudaMemsetAsync(L.st.counts, 0, sizeof(uint32_t) * kCountsSize, s));
   if (media) R2_CUDA(cudaMemsetAsync(L.st.mc, 0, sizeof(uint32_t) * kCountersPerBounce * L.maxDepth, s));
   mark(-1);
   k_camera<<<nblocks, 256, 0, s>>>(L);
