@@ -3,8 +3,8 @@
 Headline (N=1 workload, config "surface path tracing"): 8x8 grid of displaced
 icospheres (327,680 triangles, per-object GGX roughness U[0.05,1], albedo
 U[0.2,0.9]) lit by a 512x256 lognormal(0,1.5) HDR environment, 1024x1024,
-64 spp, max depth 8.  A step is one frame (64 waves of 1M paths) over a
-device-resident scene; metric paths/s.
+64 spp, max depth 8.  A step is one frame (64 spp in waves of several samples
+per pixel, the wave size autotuned) over a device-resident scene; metric paths/s.
 
 Second leg (config "filter at scale"): 500k leaf quads (1M tris) filtered to
 256^3 with 256 samples/voxel and 20 iterations; metric filtered voxels/s,
@@ -41,10 +41,10 @@ FILTER_CFG = dict(n_quads=500_000, n_branches=20, clustered=0.7, seed=4, grid=25
 # Algorithmic bytes (SoA traffic a kernel must move; BVH nodes/triangles are
 # excluded as L2-resident by design):
 #   k_extend: queue id 4 + ray origin 16 + direction 16 + hit record 16 = 52 B per path segment
-#   k_shadow: record origin 16 + direction 16 + visibility 1 = 33 B per shadow slot (2 per segment)
+#   k_shadow_surfaces: record origin 16 + direction 16 + visibility 1 = 33 B per traced shadow ray
 #   k_filter_sample: payload 32 + work-list id 4 = 36 B per filtered voxel
 EXTEND_BYTES_PER_SEGMENT = 52.0
-SHADOW_BYTES_PER_SLOT = 33.0
+SHADOW_BYTES_PER_RAY = 33.0
 FILTER_BYTES_PER_VOXEL = 36.0
 # media scenes:
 #   extend phase (k_resolve rounds, k_track, k_collide): queue id 4 + ray in/out 64 + throughput in/out 32 + hit record 16 = 116 B per segment
@@ -277,14 +277,14 @@ def bench_render(args, world, local):
     ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
     # dominant kernel over the frame; a wave renders S samples of every pixel
     S = sc.wave_samples(cam, prm)
-    seg_wave, sh_wave = seg * S / prm.spp, 2.0 * seg * S / prm.spp
+    seg_wave, sh_wave = seg * S / prm.spp, shadow * S / prm.spp
     dom = "extend" if ms_wave["extend"] >= ms_wave["shadow"] else "shadow"
     peak, peak_kind = _peaks()
     if dom == "extend":
         alg = EXTEND_BYTES_PER_SEGMENT * seg_wave
         kname = "k_extend"
     else:
-        alg = SHADOW_BYTES_PER_SLOT * sh_wave
+        alg = SHADOW_BYTES_PER_RAY * sh_wave
         kname = "k_shadow_surfaces"
     kms = ms_wave[dom]
     launches = prm.max_depth

@@ -373,6 +373,10 @@ r2_status r2_tonemap(const float* linear_rgb, uint32_t width, uint32_t height, f
 /* Image files: 8-bit RGB PNG (flip_vertical as the reference's writer does for
  * bottom-up frames) and Radiance RGBE .hdr (row 0 = top). */
 r2_status r2_write_png(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical);
+/* Baseline JPEG (4:4:4, standard tables, quality 1..100): the output.jpg of
+ * CImageWriter::writeToFile (visualisation/src/image_writer.cpp:13-17, quality 100). */
+r2_status r2_write_jpg(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical,
+                       int quality);
 r2_status r2_read_hdr(const char* path, float* rgb, size_t capacity, uint32_t* width, uint32_t* height);
 r2_status r2_write_hdr(const char* path, const float* rgb, uint32_t width, uint32_t height);
 /* OBJ/MTL import summary (CAssetManager::loadWithAssimp, asset_manager.cu:25-84). */

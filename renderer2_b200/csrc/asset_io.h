@@ -13,7 +13,8 @@
 // mantissa * 2^(e - 136).
 //
 // PNG: 8-bit RGB with stored (uncompressed) deflate blocks, optionally flipped
-// vertically like the reference's writer (visualisation/src/image_writer.cpp:7-24).
+// vertically like the reference's writer (visualisation/src/image_writer.cpp:7-24);
+// JPEG: see jpeg_writer.cpp.
 #pragma once
 #include <stdint.h>
 
@@ -43,5 +44,8 @@ RgbImage read_hdr(const std::string& path);
 void write_hdr(const std::string& path, const float* rgb, uint32_t width, uint32_t height);
 
 void write_png(const std::string& path, const uint8_t* rgb, uint32_t width, uint32_t height, bool flipVertical);
+// Baseline JPEG, 4:4:4, quality 1..100 (the reference writes quality 100); jpeg_writer.cpp.
+void write_jpg(const std::string& path, const uint8_t* rgb, uint32_t width, uint32_t height, bool flipVertical,
+               int quality);
 
 }  // namespace r2

@@ -220,6 +220,15 @@ r2_status r2_tonemap(const float* linear_rgb, uint32_t width, uint32_t height, f
   R2_API_END
 }
 
+r2_status r2_write_jpg(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical,
+                       int quality) {
+  R2_API_BEGIN
+  R2_REQUIRE(path && rgb, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(quality >= 1 && quality <= 100, R2_ERR_INVALID_ARGUMENT, "JPEG quality must be in [1, 100]");
+  r2::write_jpg(path, rgb, width, height, flip_vertical != 0, quality);
+  R2_API_END
+}
+
 r2_status r2_write_png(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical) {
   R2_API_BEGIN
   R2_REQUIRE(path && rgb, R2_ERR_INVALID_ARGUMENT, "null argument");

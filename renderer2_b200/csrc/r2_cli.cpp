@@ -49,6 +49,8 @@ int main(int argc, char** argv) {
   if (s != R2_OK) return fail(s, "render");
   std::chrono::duration<double> d = std::chrono::steady_clock::now() - t0;
   printf("Rendering took %f s\n", d.count());
+  s = r2_write_jpg("./output.jpg", bytes.data(), info.frame_width, info.frame_height, 1, 100);
+  if (s != R2_OK) return fail(s, "output.jpg");
   s = r2_write_png("./output.png", bytes.data(), info.frame_width, info.frame_height, 1);
   if (s != R2_OK) return fail(s, "output.png");
   // the frame's row 0 is the bottom; .hdr files start at the top

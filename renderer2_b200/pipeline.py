@@ -83,6 +83,12 @@ def write_png(path, rgb: np.ndarray, flip_vertical=False):
     N.check(N.lib.r2_write_png(str(path).encode(), N.ptr(a), a.shape[1], a.shape[0], int(flip_vertical)))
 
 
+def write_jpg(path, rgb: np.ndarray, flip_vertical=False, quality=100):
+    a = np.ascontiguousarray(rgb, np.uint8)
+    N.check(N.lib.r2_write_jpg(str(path).encode(), N.ptr(a), a.shape[1], a.shape[0], int(flip_vertical),
+                               int(quality)))
+
+
 def read_hdr(path) -> np.ndarray:
     w, h = C.c_uint32(), C.c_uint32()
     N.check(N.lib.r2_read_hdr(str(path).encode(), None, 0, C.byref(w), C.byref(h)))

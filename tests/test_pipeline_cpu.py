@@ -124,6 +124,32 @@ def test_png_writer_decodes(tmp_path):
     assert np.array_equal(rows[:, 1:].reshape(37, 300, 3), rgb[::-1])
 
 
+@pytest.mark.parametrize("w,h", [(64, 48), (37, 29)])
+def test_jpg_writer_decodes(tmp_path, w, h):
+    """output.jpg as the reference writes it (quality 100, flipped): a baseline
+    JPEG that an independent decoder (Pillow) reads back to within JPEG's
+    rounding of the original, on a smooth image and on noise, also when the
+    size is not a multiple of the 8x8 block."""
+    Image = pytest.importorskip("PIL.Image")
+    yy, xx = np.mgrid[0:h, 0:w]
+    smooth = np.stack([xx * 255 // max(w - 1, 1), yy * 255 // max(h - 1, 1), (xx + yy) % 256], -1).astype(np.uint8)
+    noise = np.random.default_rng(3).integers(0, 256, (h, w, 3), dtype=np.uint8)
+    for img, tol in ((smooth, 3.0), (noise, 6.0)):
+        P.write_jpg(tmp_path / "o.jpg", img, flip_vertical=True, quality=100)
+        with Image.open(tmp_path / "o.jpg") as im:
+            assert im.format == "JPEG" and im.size == (w, h) and im.mode == "RGB"
+            back = np.asarray(im.convert("RGB")).astype(np.float64)
+        err = np.abs(back - img[::-1].astype(np.float64))
+        assert err.mean() < tol / 3 and err.max() <= 8 * tol, (err.mean(), err.max())
+    # lower quality: coarser but still close on the smooth image
+    P.write_jpg(tmp_path / "q50.jpg", smooth, quality=50)
+    with Image.open(tmp_path / "q50.jpg") as im:
+        back = np.asarray(im.convert("RGB")).astype(np.float64)
+    assert np.abs(back - smooth).mean() < 6.0
+    with pytest.raises(N.R2Error):
+        P.write_jpg(tmp_path / "bad.jpg", smooth, quality=0)
+
+
 def _pipeline_files(tmp_path, mesh_mask=("RENDER",), filter_active=False):
     mesh = scenes.icosphere(2, 0.05, 1)
     P.write_obj(tmp_path / "assets", "sphere", [(mesh, (0.8, 0.8, 0.8), (1, 1, 1), 2.0 / 0.3 ** 2 - 2.0, 1.5)])

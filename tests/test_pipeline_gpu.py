@@ -112,3 +112,7 @@ def test_cli_writes_the_frame(tmp_path):
     hdr = P.read_hdr(tmp_path / "output.hdr")
     m = lin[::-1].max(axis=2, keepdims=True)
     assert np.all(np.abs(hdr - lin[::-1]) <= m / 128.0 + 1e-30)
+    Image = pytest.importorskip("PIL.Image")
+    with Image.open(tmp_path / "output.jpg") as im:  # quality 100, as the reference writes it
+        jpg = np.asarray(im.convert("RGB")).astype(np.float64)
+    assert jpg.shape == img.shape and np.abs(jpg - img).mean() < 3.0
