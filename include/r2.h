@@ -139,6 +139,12 @@ r2_status r2_filter_scene_grid(const r2_filter_scene* scene, float voxel_size,
 r2_status r2_filter_scene_run(r2_filter_scene* scene, const r2_filter_grid* grid,
                               const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
                               uint16_t* d_fp16, void* stream, double* stats_out);
+/* The same LOD through the counting build of the sampling kernel (same
+ * payloads, slower): counts_out[0] rays traced, [1] inner BVH nodes visited,
+ * [2] triangles tested -- the operation counts behind the filter's
+ * arithmetic roofline.  Waits for the result. */
+r2_status r2_filter_scene_count(r2_filter_scene* scene, const r2_filter_grid* grid,
+                                const r2_filter_params* params, r2_voxel* d_out, uint64_t* counts_out);
 
 /* Same as r2_filter_scene_run, for callers that must not allocate device
  * memory during the call: frame loops that run under a fixed memory budget
@@ -402,6 +408,10 @@ r2_status r2_server_create(uint32_t slots, uint64_t hbm_budget_bytes, r2_server*
 r2_status r2_server_destroy(r2_server* server);
 /* A frame of a committed scene into rgb_out (W*H*3 floats, row 0 at the bottom).
  * R2_ERR_ADMISSION_REJECTED if the job alone exceeds the budget. */
+/* Device bytes a render job of this scene, camera and parameters is admitted
+ * with (checked against the budget; plan budgets with it). */
+r2_status r2_server_render_bytes(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
+                                 uint64_t* bytes_out);
 r2_status r2_server_submit_render(r2_server* server, r2_scene* scene, const r2_camera* camera,
                                   const r2_render_params* params, float* rgb_out, uint64_t* job_id);
 /* One LOD of a filter scene into out (nx*ny*nz payloads). */

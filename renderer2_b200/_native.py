@@ -70,6 +70,7 @@ def _load():
         "r2_filter_scene_destroy": (C.c_int, [P]),
         "r2_filter_scene_grid": (C.c_int, [P, f32, P]),
         "r2_filter_scene_run": (C.c_int, [P, P, P, P, P, P, P, P]),
+        "r2_filter_scene_count": (C.c_int, [P, P, P, P, P]),
         "r2_filter_scene_bvh": (C.c_int, [P, P, sz, P, sz, P, P]),
         "r2_scene_create": (C.c_int, [P]),
         "r2_scene_destroy": (C.c_int, [P]),
@@ -92,6 +93,7 @@ def _load():
         "r2_server_create": (C.c_int, [u32, C.c_uint64, P]),
         "r2_server_destroy": (C.c_int, [P]),
         "r2_server_submit_render": (C.c_int, [P, P, P, P, P, P]),
+        "r2_server_render_bytes": (C.c_int, [P, P, P, P]),
         "r2_server_submit_filter": (C.c_int, [P, P, P, P, u32, P, P]),
         "r2_server_wait": (C.c_int, [P, C.c_uint64, C.c_double, P]),
         "r2_server_stats": (C.c_int, [P, P]),

@@ -133,6 +133,7 @@ struct TraceState {
   int leaf;
   int sp;
   int found;
+  uint32_t nodes, tris;  // visits counted by the counting instantiation (kCount)
 };
 
 constexpr int kTraceDone = 0x7FFFFFFF;  // no node left to visit (never a node index)
@@ -146,6 +147,7 @@ R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax) {
   s.leaf = 0;
   s.sp = 0;
   s.found = 0;
+  s.nodes = s.tris = 0;
 }
 
 // Next stacked child whose entry distance is not beyond the closest hit.
@@ -176,13 +178,14 @@ R2_HD bool trace_all_have_leaf(bool mine) {
 // entry distance.  The builder bounds the tree depth by R2_BVH_STACK so the
 // stack cannot overflow.  The closest hit does not depend on the visiting
 // order (ties go to the lower triangle index).
-template <bool kAnyHit>
+template <bool kAnyHit, bool kCount = false>
 R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* stackT, int maxVisits) {
   int budget = maxVisits;
   while (budget > 0) {
     // inner nodes, the first leaf met postponed
     while (s.cur >= 0 && s.cur != kTraceDone && budget > 0) {
       --budget;
+      if (kCount) ++s.nodes;
       const int cur = s.cur;
 #if defined(__CUDA_ARCH__)
       const float4 b0 = __ldg(&bvh.nodes[cur].b0);
@@ -224,6 +227,7 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
       const int first = bvh_leaf_first(s.leaf);
       const int count = bvh_leaf_count(s.leaf);
       budget -= count;
+      if (kCount) s.tris += (uint32_t)count;
       for (int i = 0; i < count; ++i) {
         const int tri = first + i;
 #if defined(__CUDA_ARCH__)
@@ -258,14 +262,20 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
   return false;
 }
 
-// The whole query at once.
-template <bool kAnyHit>
-R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax) {
+// The whole query at once; the counting instantiation adds the inner nodes
+// visited and the triangles tested to *nodes and *tris.
+template <bool kAnyHit, bool kCount = false>
+R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax, uint32_t* nodes = nullptr,
+                    uint32_t* tris = nullptr) {
   TraceState s;
   trace_begin(s, o, d, tmax);
   int stack[R2_BVH_STACK];
   float stackT[R2_BVH_STACK];
-  while (!trace_advance<kAnyHit>(bvh, s, stack, stackT, 1 << 30)) {
+  while (!trace_advance<kAnyHit, kCount>(bvh, s, stack, stackT, 1 << 30)) {
+  }
+  if (kCount) {
+    *nodes += s.nodes;
+    *tris += s.tris;
   }
   return s.best;
 }

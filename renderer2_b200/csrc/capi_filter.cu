@@ -129,6 +129,21 @@ r2_status r2_filter_scene_grid(const r2_filter_scene* scene, float voxel_size, r
   R2_API_END
 }
 
+r2_status r2_filter_scene_count(r2_filter_scene* scene, const r2_filter_grid* grid, const r2_filter_params* params,
+                                r2_voxel* d_out, uint64_t* counts_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && grid && params && d_out && counts_out, R2_ERR_INVALID_ARGUMENT, "null argument");
+  r2::DBuf<unsigned long long> ops(3);
+  cudaStream_t s = scene->impl->stream();
+  R2_CUDA(cudaMemsetAsync(ops.get(), 0, 3 * sizeof(unsigned long long), s));
+  scene->impl->run(*grid, *params, 0, d_out, nullptr, nullptr, s, nullptr, nullptr, nullptr, ops.get());
+  unsigned long long h[3] = {0, 0, 0};
+  ops.download(h, 3, s);
+  R2_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < 3; ++k) counts_out[k] = h[k];
+  R2_API_END
+}
+
 r2_status r2_filter_scene_run(r2_filter_scene* scene, const r2_filter_grid* grid, const r2_filter_params* params,
                               r2_voxel* d_out, float* d_wide, uint16_t* d_fp16, void* stream, double* stats_out) {
   R2_API_BEGIN

@@ -31,6 +31,15 @@ r2_status r2_server_destroy(r2_server* server) {
   R2_API_END
 }
 
+r2_status r2_server_render_bytes(r2_scene* scene, const r2_camera* camera, const r2_render_params* params,
+                                 uint64_t* bytes_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && camera && params && bytes_out, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(camera->width > 0 && camera->height > 0 && params->spp > 0, R2_ERR_INVALID_ARGUMENT, "empty job");
+  *bytes_out = r2::Server::render_bytes(*r2_scene_impl(scene), *camera, *params);
+  R2_API_END
+}
+
 r2_status r2_server_submit_render(r2_server* server, r2_scene* scene, const r2_camera* camera,
                                   const r2_render_params* params, float* rgb_out, uint64_t* job_id) {
   R2_API_BEGIN

@@ -135,6 +135,7 @@ __device__ __forceinline__ CSum warp_csum(CSum v) {
   return v;
 }
 
+template <bool kCount>
 __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunch L) {
   __shared__ float ts[kSampleWarps][kFilterMaxSpv];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -142,6 +143,7 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
   const uint32_t ncand = *(volatile uint32_t*)&L.counters[0];
   const float radius = 1.1f * length(L.voxelSize) / 2.0f;
   const float tMaxFixed = L.voxelSize.x;
+  uint32_t cRays = 0, cNodes = 0, cTris = 0;  // counting build only
   while (true) {
     uint32_t w = 0;
     if (lane == 0) w = atomicAdd(&L.counters[1], 1u);
@@ -170,7 +172,8 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
       const V3 o = xform_point(L.indexToWorld, oi);
       const V3 d = uniform_sample_sphere(u01(r0.w), u01(r1.x));
       const float tmax = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
-      const Hit h = bvh_trace<false>(L.bvh, o, d, tmax);
+      const Hit h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris);
+      if (kCount) ++cRays;
       float tsv = -1.0f;
       if (h.tri >= 0) {
         const float4 n0 = __ldg(&L.triN[3 * h.tri]);
@@ -281,6 +284,20 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
     }
     __syncwarp();
   }
+  if (kCount) {
+    unsigned long long r = cRays, n = cNodes, t = cTris;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      r += __shfl_xor_sync(0xFFFFFFFFu, r, off);
+      n += __shfl_xor_sync(0xFFFFFFFFu, n, off);
+      t += __shfl_xor_sync(0xFFFFFFFFu, t, off);
+    }
+    if (lane == 0) {
+      atomicAdd(&L.ops[0], r);
+      atomicAdd(&L.ops[1], n);
+      atomicAdd(&L.ops[2], t);
+    }
+  }
 }
 
 }  // namespace
@@ -294,12 +311,16 @@ void launch_filter_classify(const FilterLaunch& L, cudaStream_t s) {
 }
 
 void launch_filter_sample(const FilterLaunch& L, cudaStream_t s) {
-  static int perSm = 0;
-  if (perSm == 0) {
-    R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, k_filter_sample, kSampleWarps * 32, 0));
-    if (perSm < 1) perSm = 1;
+  static int perSm[2] = {0, 0};
+  const int c = L.ops ? 1 : 0;
+  if (perSm[c] == 0) {
+    int n = 0;
+    if (c) R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<true>, kSampleWarps * 32, 0));
+    else R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<false>, kSampleWarps * 32, 0));
+    perSm[c] = n < 1 ? 1 : n;
   }
-  k_filter_sample<<<sm_count() * perSm, kSampleWarps * 32, 0, s>>>(L);
+  if (c) k_filter_sample<true><<<sm_count() * perSm[c], kSampleWarps * 32, 0, s>>>(L);
+  else k_filter_sample<false><<<sm_count() * perSm[c], kSampleWarps * 32, 0, s>>>(L);
   R2_CUDA(cudaGetLastError());
 }
 

@@ -28,6 +28,7 @@ struct FilterLaunch {
   uint16_t* fp16;            // nullable
   uint32_t* work;            // candidate voxel ids
   uint32_t* counters;        // [0] candidates, [1] queue head
+  unsigned long long* ops;   // nullable: counting build, [0] rays, [1] inner nodes visited, [2] triangles tested
 };
 
 // Host launchers.  `classify` writes the empty payload for voxels whose

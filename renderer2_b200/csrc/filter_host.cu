@@ -124,7 +124,7 @@ r2_filter_grid FilterScene::grid(float voxelSize) const {
 
 void FilterScene::run(const r2_filter_grid& g, const r2_filter_params& p, uint32_t lod, r2_voxel* d_out,
                       float* d_wide, uint16_t* d_fp16, cudaStream_t s, double* stats,
-                      uint32_t* d_work, uint32_t* d_counters) {
+                      uint32_t* d_work, uint32_t* d_counters, unsigned long long* d_ops) {
   R2_REQUIRE(d_out, R2_ERR_INVALID_ARGUMENT, "null output");
   R2_REQUIRE(p.samples_per_voxel >= 1 && p.samples_per_voxel <= kFilterMaxSpv, R2_ERR_UNSUPPORTED,
              "samples_per_voxel must be in [1, 1024]");
@@ -170,6 +170,7 @@ void FilterScene::run(const r2_filter_grid& g, const r2_filter_params& p, uint32
     L.work = work_.get();
   }
   L.counters = d_counters ? d_counters : counters_.get();
+  L.ops = d_ops;
   R2_CUDA(cudaMemsetAsync(L.counters, 0, 2 * sizeof(uint32_t), s));
   launch_filter_classify(L, s);
   R2_CUDA(cudaEventRecord(ev0_, s));

@@ -252,7 +252,14 @@ void RenderScene::commit() {
   committed_ = true;
 }
 
+uint32_t RenderContext::capacity_for(uint32_t n) {
+  uint64_t c = 1u << 16;
+  while (c < n) c <<= 1;
+  return (uint32_t)std::min<uint64_t>(c, 0x80000000ull);
+}
+
 void RenderContext::ensure(uint32_t n, bool media) {
+  n = capacity_for(n);
   if (n > cap_) {
     rayO_.alloc(n); rayD_.alloc(n); T_.alloc(n); L_.alloc(n); hit_.alloc(n);
     shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
@@ -273,6 +280,7 @@ void RenderContext::ensure(uint32_t n, bool media) {
 }
 
 size_t RenderContext::bytes_for(uint32_t n, bool media) {
+  n = capacity_for(n);
   // per path: 5 float4 state + 3 x 2 float4 records + float4 throughput + 3 queue ids + 2 transmittances
   size_t b = (size_t)n * (5 * 16 + 6 * 16 + 16 + 12 + 8) + kCountsSize * 4;
   // media: records (4 float4 + float2), shadow tmax/medium, round queues and walk state
@@ -312,8 +320,9 @@ void RenderScene::check_params(const r2_camera& c, const r2_render_params& p, co
   R2_REQUIRE((p.flags & ~R2_RENDER_BRICK_GRID) == 0, R2_ERR_INVALID_ARGUMENT, "unknown render flags");
 }
 
-uint32_t RenderScene::wave_spp(uint32_t npix, uint32_t spp) const {
-  const uint64_t target = tuning_.wave_paths ? tuning_.wave_paths : kDefaultWavePaths;
+uint32_t RenderScene::wave_spp(uint32_t npix, uint32_t spp, uint32_t maxWavePaths) const {
+  uint64_t target = tuning_.wave_paths ? tuning_.wave_paths : kDefaultWavePaths;
+  if (maxWavePaths && maxWavePaths < target) target = maxWavePaths;
   uint32_t best = 1;
   for (uint32_t k = 2; k <= spp; ++k)
     if (spp % k == 0 && (uint64_t)k * npix <= target && (uint64_t)k * npix < (1ull << 31)) best = k;
@@ -396,9 +405,9 @@ void RenderScene::render(const r2_camera& c, const r2_render_params& p, float* d
 }
 
 void RenderScene::render_graph(RenderContext& ctx, const r2_camera& c, const r2_render_params& p, float* d_frame,
-                               cudaStream_t s) {
+                               cudaStream_t s, uint32_t maxWavePaths) {
   const uint32_t npix = c.width * c.height;
-  const uint32_t S = wave_spp(npix, p.spp);
+  const uint32_t S = wave_spp(npix, p.spp, maxWavePaths);
   RenderLaunch L = prepare(ctx, c, p, d_frame, S);
   R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
   R2_CUDA(cudaMemsetAsync(ctx.sampleDev.get(), 0, sizeof(uint32_t), s));

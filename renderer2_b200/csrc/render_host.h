@@ -35,11 +35,13 @@ class RenderContext {
   RenderContext(const RenderContext&) = delete;
   RenderContext& operator=(const RenderContext&) = delete;
 
-  // Buffers for npix paths (media: the tracking-round state too).
+  // Buffers for at least npix paths (media: the tracking-round state too),
+  // grown to a power of two so that renders of varying size reallocate rarely.
   void ensure(uint32_t npix, bool media);
   void fill(PathState* st) const;
-  // Device bytes a render of npix paths needs (buffers + frame).
+  // Device bytes a render of npix paths needs (buffers as ensure grows them + frame).
   static size_t bytes_for(uint32_t npix, bool media);
+  static uint32_t capacity_for(uint32_t npix);
   // Paths and shadow rays of the last render that a loop bound ended (waits for s).
   uint32_t bound_hits(cudaStream_t s);
 
@@ -86,15 +88,17 @@ class RenderScene {
   void render(const r2_camera& cam, const r2_render_params& p, float* d_frame, cudaStream_t s, double* stats);
   // The same frame on a caller's context and stream, one wave captured as a
   // CUDA graph and replayed spp / wave_spp times (the scene must be committed).
+  // maxWavePaths (0: the tuning's) caps the paths per wave.
   void render_graph(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame,
-                    cudaStream_t s);
+                    cudaStream_t s, uint32_t maxWavePaths = 0);
   // The launch description of a frame on ctx with waveSpp samples per wave
   // (a divisor of p.spp; the context's buffers grown to fit).
   RenderLaunch prepare(RenderContext& ctx, const r2_camera& cam, const r2_render_params& p, float* d_frame,
                        uint32_t waveSpp);
   // Samples per wave of a frame: the largest divisor of spp whose wave stays
-  // within the tuning's paths per wave (at least one).
-  uint32_t wave_spp(uint32_t npix, uint32_t spp) const;
+  // within the tuning's paths per wave, or maxWavePaths if smaller and nonzero
+  // (at least one sample).
+  uint32_t wave_spp(uint32_t npix, uint32_t spp, uint32_t maxWavePaths = 0) const;
   // Launch tuning (0 fields: the defaults) and the autotuner that sets it.
   void set_tuning(const r2_render_tuning& t);
   r2_render_tuning tuning() const { return tuning_; }

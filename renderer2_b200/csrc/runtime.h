@@ -59,6 +59,14 @@ class DBuf {
   }
   // Grow-only reallocation (contents are not preserved).
   void reserve(size_t n) { if (n > n_) alloc(n); }
+  // Grows to a power of two at least n, so that buffers reused for jobs of
+  // varying size reallocate rarely (each cudaFree/cudaMalloc waits for the device).
+  void reserve_grow(size_t n) {
+    if (n <= n_) return;
+    size_t c = 1;
+    while (c < n) c <<= 1;
+    alloc(c);
+  }
   void release() {
     if (p_) cudaFree(p_);
     p_ = nullptr;

@@ -7,6 +7,17 @@
 
 namespace r2 {
 
+// Render jobs run waves of at most this many paths: concurrent jobs fill the
+// GPU together, and small waves keep each slot's buffers small.
+constexpr uint32_t kServeWavePaths = 1u << 20;
+
+// Bytes of a buffer grown to a power of two (DBuf::reserve_grow).
+static size_t grow_bytes(size_t n) {
+  size_t c = 1;
+  while (c < n) c <<= 1;
+  return c;
+}
+
 struct Server::Slot {
   RenderContext ctx;  // wave buffers + the slot's stream
   DBuf<float> frame;
@@ -30,12 +41,14 @@ struct Server::Slot {
     if (done) cudaEventDestroy(done);
   }
   void* staging(size_t bytes) {
-    if (bytes > pinnedBytes) {
+    if (bytes > pinnedBytes) {  // grown to a power of two: pinned allocation is slow and synchronous
       if (pinned) cudaFreeHost(pinned);
       pinned = nullptr;
       pinnedBytes = 0;
-      R2_CUDA(cudaHostAlloc(&pinned, bytes, cudaHostAllocDefault));
-      pinnedBytes = bytes;
+      size_t c = 1 << 16;
+      while (c < bytes) c <<= 1;
+      R2_CUDA(cudaHostAlloc(&pinned, c, cudaHostAllocDefault));
+      pinnedBytes = c;
     }
     return pinned;
   }
@@ -65,6 +78,12 @@ double Server::now() const {
   return duration<double>(steady_clock::now().time_since_epoch()).count() - t0_;
 }
 
+size_t Server::render_bytes(const RenderScene& scene, const r2_camera& cam, const r2_render_params& rp) {
+  const uint32_t npix = cam.width * cam.height;
+  return RenderContext::bytes_for(npix * scene.wave_spp(npix, rp.spp, kServeWavePaths), scene.has_media()) +
+         grow_bytes((size_t)npix * 12);
+}
+
 uint64_t Server::submit(std::unique_ptr<ServerJob> job) {
   ServerJob* j = job.get();
   if (j->kind == 0) {
@@ -72,14 +91,14 @@ uint64_t Server::submit(std::unique_ptr<ServerJob> job) {
     const uint32_t npix = j->cam.width * j->cam.height;
     R2_REQUIRE(npix > 0 && j->rp.spp > 0 && j->rp.max_depth > 0 && j->rp.max_depth <= 60, R2_ERR_INVALID_ARGUMENT,
                "bad render job");
+    j->bytes = render_bytes(*j->scene, j->cam, j->rp);
     j->outBytes = (size_t)npix * 12;
-    j->bytes = RenderContext::bytes_for(npix * j->scene->wave_spp(npix, j->rp.spp), j->scene->has_media());
   } else {
     R2_REQUIRE(j->fscene, R2_ERR_INVALID_ARGUMENT, "filter job needs a filter scene");
     const size_t nvox = (size_t)j->grid.num_voxels[0] * j->grid.num_voxels[1] * j->grid.num_voxels[2];
     R2_REQUIRE(nvox > 0 && nvox < (1ull << 32), R2_ERR_INVALID_ARGUMENT, "bad filter grid");
     j->outBytes = nvox * sizeof(r2_voxel);
-    j->bytes = nvox * (sizeof(r2_voxel) + 4) + 64;
+    j->bytes = grow_bytes(nvox * sizeof(r2_voxel)) + grow_bytes(nvox * 4) + 64;
   }
   R2_REQUIRE(j->bytes <= budget_, R2_ERR_ADMISSION_REJECTED, "job needs more device memory than the HBM budget");
   uint64_t id;
@@ -129,14 +148,14 @@ bool Server::start(Slot& s, ServerJob* j) {
     cudaStream_t st = s.ctx.stream;
     if (j->kind == 0) {
       const uint32_t npix = j->cam.width * j->cam.height;
-      s.frame.reserve((size_t)npix * 3);
-      j->scene->render_graph(s.ctx, j->cam, j->rp, s.frame.get(), st);
+      s.frame.reserve_grow((size_t)npix * 3);
+      j->scene->render_graph(s.ctx, j->cam, j->rp, s.frame.get(), st, kServeWavePaths);
       R2_CUDA(cudaMemcpyAsync(s.staging(j->outBytes), s.frame.get(), j->outBytes, cudaMemcpyDeviceToHost, st));
       R2_CUDA(cudaMemcpyAsync(s.pinnedBound, s.ctx.bound.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     } else {
       const size_t nvox = (size_t)j->grid.num_voxels[0] * j->grid.num_voxels[1] * j->grid.num_voxels[2];
-      s.vox.reserve(nvox);
-      s.work.reserve(nvox);
+      s.vox.reserve_grow(nvox);
+      s.work.reserve_grow(nvox);
       s.counters.reserve(2);
       j->fscene->run(j->grid, j->fp, j->lod, s.vox.get(), nullptr, nullptr, st, nullptr, s.work.get(),
                      s.counters.get());

@@ -53,6 +53,8 @@ struct ServerJob {
 class Server {
  public:
   Server(uint32_t slots, uint64_t hbmBudget);
+  // Device bytes a render job is admitted with (its slot's wave buffers and frame).
+  static size_t render_bytes(const RenderScene& scene, const r2_camera& cam, const r2_render_params& rp);
   ~Server();  // finishes the admitted and queued jobs, then stops
   Server(const Server&) = delete;
   Server& operator=(const Server&) = delete;

@@ -100,6 +100,12 @@ class FilterScene:
         if stats is not None:
             stats[:] = st[:3]
 
+    def count(self, grid, prm, d_out: int):
+        """Counting build of the same LOD: (rays traced, inner nodes visited, triangles tested)."""
+        c = np.zeros(3, np.uint64)
+        N.check(N.lib.r2_filter_scene_count(self.handle, C.byref(grid), C.byref(prm), C.c_void_p(d_out), N.ptr(c)))
+        return tuple(int(x) for x in c)
+
     def bvh(self):
         nn = C.c_uint32()
         ht = C.c_uint32()

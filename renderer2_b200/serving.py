@@ -35,6 +35,13 @@ class Server:
         except Exception:
             pass
 
+    @staticmethod
+    def render_bytes(scene, camera, params) -> int:
+        """Device bytes a render job is admitted with (r2_server_render_bytes)."""
+        b = C.c_uint64()
+        N.check(N.lib.r2_server_render_bytes(scene.handle, C.byref(camera), C.byref(params), C.byref(b)))
+        return b.value
+
     def submit_render(self, scene, camera, params) -> Job:
         out = np.zeros((camera.height, camera.width, 3), np.float32)
         jid = C.c_uint64()

@@ -171,6 +171,27 @@ def test_host_entry_matches_device_entry():
     assert np.array_equal(wide.astype(np.float64), gw)
 
 
+def test_counting_build_gives_the_same_payload_and_consistent_counts():
+    """The counting build of the sampling kernel writes the same voxels and
+    counts spv rays per candidate voxel, at least one node visit per ray."""
+    leaves = scenes.foliage(20_000, 6, 0.7, 5)
+    mat = F.material(diffuse=(0.1, 0.6, 0.1), alpha=0.5)
+    prm = F.params(samples_per_voxel=48, iterations=4)
+    sc = F.FilterScene(leaves, mat)
+    g = sc.grid(scenes.voxel_size_for(leaves, 24))
+    nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+    a = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    b = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    st = np.zeros(3)
+    sc.run(g, prm, a.data_ptr(), stats=st)
+    rays, nodes, tris = sc.count(g, prm, b.data_ptr())
+    torch.cuda.synchronize()
+    sc.close()
+    assert torch.equal(a, b)
+    assert rays == int(st[1]) * 48 and rays > 0
+    assert nodes >= rays and tris > 0
+
+
 def test_fp16_payload_error_stated():
     mesh = scenes.icosphere(4, 0.05, 1)
     mat = F.material()

@@ -92,8 +92,8 @@ def test_budget_serialises_and_rejects(world):
     cam = R.camera(128, 128, 45.0, (0, 0, 3))
     prm = R.params(2, 6, 7)
     ref = world["sc1"].render(cam, prm)
-    paths = 128 * 128 * world["sc1"].wave_samples(cam, prm)  # a wave's paths
-    one_job = paths * (5 * 16 + 6 * 16 + 16 + 12 + 8 + 12) + 4096
+    one_job = S.Server.render_bytes(world["sc1"], cam, prm)
+    assert one_job >= 128 * 128 * (5 * 16 + 6 * 16 + 16 + 12 + 8 + 12)  # at least the wave state of one sample
     srv = S.Server(slots=4, hbm_budget=int(one_job * 1.5))  # at most one such job admitted at a time
     hs = [srv.submit_render(world["sc1"], cam, prm) for _ in range(4)]
     for h in hs:
