@@ -384,6 +384,11 @@ r2_status r2_write_png(const char* path, const uint8_t* rgb, uint32_t width, uin
 r2_status r2_write_jpg(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical,
                        int quality);
 r2_status r2_read_hdr(const char* path, float* rgb, size_t capacity, uint32_t* width, uint32_t* height);
+/* PNG texture (any colour type, 1-16 bits, non-interlaced) as 8-bit RGBA, row 0 = top,
+ * as stb_image loads the reference's texture maps (texture.cu:64-97).  rgba may be
+ * null to query the size; channels_out: the file's channel count (1-4). */
+r2_status r2_read_png(const char* path, uint8_t* rgba, size_t capacity, uint32_t* width, uint32_t* height,
+                      int* channels_out);
 r2_status r2_write_hdr(const char* path, const float* rgb, uint32_t width, uint32_t height);
 /* OBJ/MTL import summary (CAssetManager::loadWithAssimp, asset_manager.cu:25-84). */
 r2_status r2_obj_info(const char* directory, const char* filename, uint32_t* n_submeshes, uint32_t* n_vertices,

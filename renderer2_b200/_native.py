@@ -105,6 +105,7 @@ def _load():
         "r2_tonemap": (C.c_int, [P, u32, u32, f32, P, P]),
         "r2_write_png": (C.c_int, [C.c_char_p, P, u32, u32, C.c_int]),
         "r2_write_jpg": (C.c_int, [C.c_char_p, P, u32, u32, C.c_int, C.c_int]),
+        "r2_read_png": (C.c_int, [C.c_char_p, P, sz, P, P, P]),
         "r2_read_hdr": (C.c_int, [C.c_char_p, P, sz, P, P]),
         "r2_write_hdr": (C.c_int, [C.c_char_p, P, u32, u32]),
         "r2_obj_info": (C.c_int, [C.c_char_p, C.c_char_p, P, P, P, P]),

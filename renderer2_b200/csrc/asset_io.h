@@ -41,6 +41,14 @@ struct RgbImage {
   std::vector<float> rgb;  // row 0 = top
 };
 RgbImage read_hdr(const std::string& path);
+
+// 8-bit RGBA texels (row 0 = top) and the source's channel count (1-4).
+struct RgbaImage8 {
+  uint32_t width = 0, height = 0;
+  int channels = 0;
+  std::vector<uint8_t> rgba;
+};
+RgbaImage8 read_png(const std::string& path);  // png_reader.cpp
 void write_hdr(const std::string& path, const float* rgb, uint32_t width, uint32_t height);
 
 void write_png(const std::string& path, const uint8_t* rgb, uint32_t width, uint32_t height, bool flipVertical);

@@ -220,6 +220,21 @@ r2_status r2_tonemap(const float* linear_rgb, uint32_t width, uint32_t height, f
   R2_API_END
 }
 
+r2_status r2_read_png(const char* path, uint8_t* rgba, size_t capacity, uint32_t* width, uint32_t* height,
+                      int* channels_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(path, R2_ERR_INVALID_ARGUMENT, "null argument");
+  r2::RgbaImage8 img = r2::read_png(path);
+  if (width) *width = img.width;
+  if (height) *height = img.height;
+  if (channels_out) *channels_out = img.channels;
+  if (rgba) {
+    R2_REQUIRE(capacity >= img.rgba.size(), R2_ERR_INVALID_ARGUMENT, "PNG larger than the output buffer");
+    memcpy(rgba, img.rgba.data(), img.rgba.size());
+  }
+  R2_API_END
+}
+
 r2_status r2_write_jpg(const char* path, const uint8_t* rgb, uint32_t width, uint32_t height, int flip_vertical,
                        int quality) {
   R2_API_BEGIN

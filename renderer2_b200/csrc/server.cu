@@ -7,9 +7,11 @@
 
 namespace r2 {
 
-// Render jobs run waves of at most this many paths: concurrent jobs fill the
-// GPU together, and small waves keep each slot's buffers small.
-constexpr uint32_t kServeWavePaths = 1u << 20;
+// Paths per wave of a render job: 0 keeps the scene's tuning.  A wave of a
+// few million paths fills the GPU by itself (capping waves at 1M paths so that
+// concurrent jobs would share the GPU made single jobs 1.7x slower), so slots
+// mainly overlap one job's host work and copies with another's kernels.
+constexpr uint32_t kServeWavePaths = 0;
 
 // Bytes of a buffer grown to a power of two (DBuf::reserve_grow).
 static size_t grow_bytes(size_t n) {

@@ -89,6 +89,15 @@ def write_jpg(path, rgb: np.ndarray, flip_vertical=False, quality=100):
                                int(quality)))
 
 
+def read_png(path):
+    """(H, W, 4) uint8 RGBA texels and the file's channel count."""
+    w, h, c = C.c_uint32(), C.c_uint32(), C.c_int()
+    N.check(N.lib.r2_read_png(str(path).encode(), None, 0, C.byref(w), C.byref(h), C.byref(c)))
+    out = np.zeros((h.value, w.value, 4), np.uint8)
+    N.check(N.lib.r2_read_png(str(path).encode(), N.ptr(out), out.size, None, None, None))
+    return out, c.value
+
+
 def read_hdr(path) -> np.ndarray:
     w, h = C.c_uint32(), C.c_uint32()
     N.check(N.lib.r2_read_hdr(str(path).encode(), None, 0, C.byref(w), C.byref(h)))

@@ -150,6 +150,49 @@ def test_jpg_writer_decodes(tmp_path, w, h):
         P.write_jpg(tmp_path / "bad.jpg", smooth, quality=0)
 
 
+@pytest.mark.parametrize("mode,kw", [("RGB", {}), ("RGBA", {}), ("L", {}), ("LA", {}), ("P", {}), ("1", {}),
+                                     ("RGB", {"compress_level": 0}), ("RGBA", {"compress_level": 1}),
+                                     ("I;16", {}), ("P4", {"bits": 4})])
+def test_png_reader_matches_pillow(tmp_path, mode, kw):
+    """Texture maps: every PNG colour type and filter Pillow writes decodes to
+    the same RGBA bytes Pillow reads (16-bit samples: the high byte)."""
+    Image = pytest.importorskip("PIL.Image")
+    rng = np.random.default_rng(7)
+    h, w = 37, 53
+    base = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+    base[:, :20] = np.linspace(0, 255, 20, dtype=np.uint8)[None, :, None]  # smooth part: the filters matter
+    if mode == "P4":
+        im = Image.fromarray(base[..., :3]).quantize(16)
+        mode = "P"
+    elif mode == "I;16":
+        im = Image.fromarray((base[..., 0].astype(np.uint16) * 257 + 3).astype(np.uint16))
+    elif mode == "1":
+        im = Image.fromarray(base[..., 0] > 127)
+    elif mode == "P":
+        im = Image.fromarray(base[..., :3]).quantize(200)
+    else:
+        im = Image.fromarray(base[..., :len(mode)] if len(mode) > 1 else base[..., 0], mode)
+    im.save(tmp_path / "t.png", **{k: v for k, v in kw.items() if k != "bits"}, **({"bits": 4} if "bits" in kw else {}))
+    got, ch = P.read_png(tmp_path / "t.png")
+    with Image.open(tmp_path / "t.png") as ref:
+        if ref.mode == "I;16" or ref.mode == "I":
+            exp = np.asarray(ref).astype(np.uint32) >> 8
+            exp = np.stack([exp, exp, exp, np.full_like(exp, 255)], -1).astype(np.uint8)
+        else:
+            exp = np.asarray(ref.convert("RGBA"))
+    assert got.shape == (h, w, 4)
+    assert np.array_equal(got, exp)
+    assert ch == {"RGB": 3, "RGBA": 4, "L": 1, "LA": 2, "P": 3, "1": 1, "I;16": 1}[mode]
+
+
+def test_png_reader_rejects_bad_files(tmp_path):
+    (tmp_path / "x.png").write_bytes(b"not a png")
+    with pytest.raises(N.R2Error):
+        P.read_png(tmp_path / "x.png")
+    with pytest.raises(N.R2Error):
+        P.read_png(tmp_path / "missing.png")
+
+
 def _pipeline_files(tmp_path, mesh_mask=("RENDER",), filter_active=False):
     mesh = scenes.icosphere(2, 0.05, 1)
     P.write_obj(tmp_path / "assets", "sphere", [(mesh, (0.8, 0.8, 0.8), (1, 1, 1), 2.0 / 0.3 ** 2 - 2.0, 1.5)])
