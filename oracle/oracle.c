@@ -367,7 +367,38 @@ static int slab(const rpre_t* r, const float* b, int slot, float tmax, float* te
 }
 
 
-static int tri_test(const rpre_t* r, f3 p0, f3 p1, f3 p2, int tri, hit_t* best) {
+void oi_tex_lookup(const oi_tex* t, float u, float v, float out[4]) {
+  u = u - floorf(u);
+  v = v - floorf(v);
+  const float xb = u * (float)t->W - 0.5f, yb = v * (float)t->H - 0.5f;
+  const float fx = floorf(xb), fy = floorf(yb);
+  const float a = xb - fx, b = yb - fy;
+  const int x0 = (int)fx, y0 = (int)fy;
+  const float* tx[4];
+  for (int k = 0; k < 4; ++k) {
+    int x = x0 + (k & 1), y = y0 + (k >> 1);
+    x %= t->W;
+    if (x < 0) x += t->W;
+    y %= t->H;
+    if (y < 0) y += t->H;
+    tx[k] = &t->texels[4 * ((size_t)y * t->W + x)];
+  }
+  const float w00 = (1.0f - a) * (1.0f - b), w10 = a * (1.0f - b), w01 = (1.0f - a) * b, w11 = a * b;
+  for (int c = 0; c < 4; ++c) out[c] = w00 * tx[0][c] + w10 * tx[1][c] + w01 * tx[2][c] + w11 * tx[3][c];
+}
+
+static int alpha_opaque(const oi_alpha* a, int tri, float b1, float b2) {
+  const int k = a->alpha_tex[tri];
+  if (k < 0) return 1;
+  const float* uv = &a->uv[6 * (size_t)tri];
+  const float b0 = (1.0f - b1) - b2;
+  const float u = b0 * uv[0] + b1 * uv[2] + b2 * uv[4], v = b0 * uv[1] + b1 * uv[3] + b2 * uv[5];
+  float c[4];
+  oi_tex_lookup(&a->tex[k], u, v, c);
+  return c[0] > 0.0f;
+}
+
+static int tri_test(const rpre_t* r, f3 p0, f3 p1, f3 p2, int tri, hit_t* best, const oi_alpha* alpha) {
   f3 A = sub3(p0, r->o), B = sub3(p1, r->o), C = sub3(p2, r->o);
   float Az0 = comp3(A, r->kz), Bz0 = comp3(B, r->kz), Cz0 = comp3(C, r->kz);
   float Ax = comp3(A, r->kx) - r->Sx * Az0, Ay = comp3(A, r->ky) - r->Sy * Az0;
@@ -393,9 +424,11 @@ static int tri_test(const rpre_t* r, f3 p0, f3 p1, f3 p2, int tri, hit_t* best) 
   float t = T * rcp;
   if (!(t > 0.0f)) return 0;
   if (t < best->t || (t == best->t && tri < best->tri)) {
+    const float b1 = V * rcp, b2 = W * rcp;
+    if (alpha && !alpha_opaque(alpha, tri, b1, b2)) return 0;
     best->t = t;
-    best->b1 = V * rcp;
-    best->b2 = W * rcp;
+    best->b1 = b1;
+    best->b2 = b2;
     best->tri = tri;
     return 1;
   }
@@ -403,6 +436,11 @@ static int tri_test(const rpre_t* r, f3 p0, f3 p1, f3 p2, int tri, hit_t* best) 
 }
 
 hit_t oi_trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, int any_hit) {
+  return oi_trace_alpha(nodes, tris, o, d, tmax, any_hit, NULL);
+}
+
+hit_t oi_trace_alpha(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, int any_hit,
+                     const oi_alpha* alpha) {
   hit_t best;
   best.t = tmax;
   best.b1 = best.b2 = 0.0f;
@@ -434,7 +472,8 @@ hit_t oi_trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, 
       for (int i = 0; i < count; ++i) {
         int tri = first + i;
         const float* tv = &tris[12 * (size_t)tri];
-        if (tri_test(&r, F3(tv[0], tv[1], tv[2]), F3(tv[4], tv[5], tv[6]), F3(tv[8], tv[9], tv[10]), tri, &best)) {
+        if (tri_test(&r, F3(tv[0], tv[1], tv[2]), F3(tv[4], tv[5], tv[6]), F3(tv[8], tv[9], tv[10]), tri, &best,
+                     alpha)) {
           found = 1;
           if (any_hit) return best;
         }

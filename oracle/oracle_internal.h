@@ -41,6 +41,24 @@ typedef struct { float t, b1, b2; int tri; } hit_t;
 /* Closest (any_hit = 0) or first found (any_hit = 1) hit in (0, tmax]. */
 hit_t oi_trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, int any_hit);
 
+/* Texture maps: float RGBA texels (4 per texel, row 0 = top), looked up at
+ * normalized coordinates with wrap addressing and bilinear weights (the
+ * reference's cudaAddressModeWrap + cudaFilterModeLinear texture objects,
+ * raytracer/src/texture/texture.cu:176-189, with float weights). */
+typedef struct { int W, H; float* texels; } oi_tex;
+void oi_tex_lookup(const oi_tex* t, float u, float v, float out[4]);
+
+/* Alpha test of triangles (__anyhit__mesh, shaders.optix.cu:132-152): per
+ * BVH-order triangle its opacity map (-1: opaque) and 3 texture coordinates;
+ * a hit where the map's red channel is 0 is ignored. */
+typedef struct {
+  const int* alpha_tex;
+  const float* uv;  /* 6 per triangle */
+  const oi_tex* tex;
+} oi_alpha;
+hit_t oi_trace_alpha(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, int any_hit,
+                     const oi_alpha* alpha);
+
 static inline float oi_u01(uint32_t b) { return (float)(b >> 8) * (1.0f / 16777216.0f); }
 
 /* 4x4 helpers (m[col][row]) */

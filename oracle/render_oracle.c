@@ -123,6 +123,7 @@ typedef struct {
   float onA, onB;
   ggx_t ggx;
   float etaI, etaT;
+  int tex[4]; /* albedo, glossy, normal, opacity texture (-1: none) */
 } mat_t;
 
 static mat_t make_mat(const orc_material* m) {
@@ -136,6 +137,7 @@ static mat_t make_mat(const orc_material* m) {
   r.ggx.ay = m->alpha_y;
   r.etaI = m->eta_i;
   r.etaT = m->eta_t;
+  for (int k = 0; k < 4; ++k) r.tex[k] = -1;
   return r;
 }
 
@@ -1029,6 +1031,12 @@ typedef struct {
   uint32_t* idx;    /* global indices */
   uint32_t* triMat; /* per original triangle */
   mat_t* mats;
+  float* uv;        /* per vertex (global), 2 each; null without texture coordinates */
+  oi_tex* tex;      /* texture table */
+  int ntex;
+  oi_alpha alpha;   /* alpha.alpha_tex null: no alpha test */
+  int* triAlpha;    /* per BVH-order triangle */
+  float* triUV;     /* per BVH-order triangle, 6 each */
   uint32_t ntris;
   const orc_shape* shapes;
   mat_t* shapeMats;
@@ -1044,13 +1052,83 @@ typedef struct {
   uint32_t spp, maxDepth, seed;
 } rscene_t;
 
+/* Texel conversions of the reference's CTexture load paths (texture.cu:29-97,
+ * 217-271, asset_manager.cu:165-184): rgb / 255 (a = 1); the alpha channel / 255
+ * in rgb; the luma of rgb / 255 (luma.hpp:4-6). */
+enum { TEX_COLOR = 0, TEX_ALPHA = 1, TEX_LUMA = 2 };
+static int tex_add(rscene_t* S, const orc_texture* src, int kind) {
+  oi_tex* t = &S->tex[S->ntex];
+  t->W = (int)src->width;
+  t->H = (int)src->height;
+  const size_t n = (size_t)t->W * t->H;
+  t->texels = (float*)malloc(sizeof(float) * 4 * n);
+  for (size_t i = 0; i < n; ++i) {
+    const uint8_t* p = &src->rgba[4 * i];
+    const float r = (float)p[0] / 255.0f, g = (float)p[1] / 255.0f, b = (float)p[2] / 255.0f;
+    float* o = &t->texels[4 * i];
+    if (kind == TEX_ALPHA) {
+      const float a = (float)p[3] / 255.0f;
+      o[0] = o[1] = o[2] = a;
+    } else if (kind == TEX_LUMA) {
+      float l = 0.2126f * r;
+      l += 0.7152f * g;
+      l += 0.0722f * b;
+      o[0] = o[1] = o[2] = l;
+    } else {
+      o[0] = r; o[1] = g; o[2] = b;
+    }
+    o[3] = 1.0f;
+  }
+  return S->ntex++;
+}
+
+/* Texture maps of a textured triangle's material at the hit (shaders.optix.cu:61-103,
+ * material.hpp:111-155): albedo and glossy colours, and the normal-mapped shading
+ * normal with the tangent frame of the world-space triangle (BVH index tri). */
+static void textured_surface(const rscene_t* S, int tri, float b1, float b2, f3* n, mat_t* m) {
+  const float* uv = &S->triUV[6 * (size_t)tri];
+  const float b0 = (1.0f - b1) - b2;
+  const float tcx = b0 * uv[0] + b1 * uv[2] + b2 * uv[4], tcy = b0 * uv[1] + b1 * uv[3] + b2 * uv[5];
+  float c[4];
+  if (m->tex[0] >= 0) {
+    oi_tex_lookup(&S->tex[m->tex[0]], tcx, tcy, c);
+    m->diffuse = F3(c[0], c[1], c[2]);
+  }
+  if (m->tex[1] >= 0) {
+    oi_tex_lookup(&S->tex[m->tex[1]], tcx, tcy, c);
+    m->specular = F3(c[0], c[1], c[2]);
+  }
+  if (m->tex[2] >= 0) {
+    const float* tv = &S->tris[12 * (size_t)tri];
+    const f3 P0 = F3(tv[0], tv[1], tv[2]), P1 = F3(tv[4], tv[5], tv[6]), P2 = F3(tv[8], tv[9], tv[10]);
+    const f3 P = add3(add3(mul3s(P0, b0), mul3s(P1, b1)), mul3s(P2, b2));
+    const f3 e1 = sub3(P1, P), e2 = sub3(P2, P);
+    const float du1 = uv[2] - tcx, dv1 = uv[3] - tcy, du2 = uv[4] - tcx, dv2 = uv[5] - tcy;
+    const float den = du1 * dv2 - du2 * dv1;
+    if (den != 0.0f) {
+      const float f = 1.0f / den;
+      const f3 T = F3(f * (dv2 * e1.x - dv1 * e2.x), f * (dv2 * e1.y - dv1 * e2.y), f * (dv2 * e1.z - dv1 * e2.z));
+      const f3 B = F3(f * (-du2 * e1.x + du1 * e2.x), f * (-du2 * e1.y + du1 * e2.y), f * (-du2 * e1.z + du1 * e2.z));
+      const int tz = T.x == 0.0f && T.y == 0.0f && T.z == 0.0f, bz = B.x == 0.0f && B.y == 0.0f && B.z == 0.0f;
+      if (!tz && !bz) {
+        oi_tex_lookup(&S->tex[m->tex[2]], tcx, tcy, c);
+        const f3 nt = F3(c[0] * 2.0f - 1.0f, c[1] * 2.0f - 1.0f, c[2] * 2.0f - 1.0f);
+        if (!(nt.x == 0.0f && nt.y == 0.0f && nt.z == 0.0f)) {
+          const f3 v = norm3(nt);
+          *n = norm3(add3(add3(mul3s(norm3(T), v.x), mul3s(norm3(neg3(B)), v.y)), mul3s(*n, v.z)));
+        }
+      }
+    }
+  }
+}
+
 /* closest: code >= 0 BVH-order triangle, -1 miss, -2 - i shape i */
 static int scene_closest(const rscene_t* S, f3 o, f3 d, float tmax, float* tOut, float* b1, float* b2) {
   float t = tmax;
   int code = -1;
   *b1 = *b2 = 0.0f;
   if (S->ntris > 0) {
-    hit_t h = oi_trace(S->nodes, S->tris, o, d, tmax, 0);
+    hit_t h = oi_trace_alpha(S->nodes, S->tris, o, d, tmax, 0, S->alpha.alpha_tex ? &S->alpha : NULL);
     if (h.tri >= 0) { t = h.t; *b1 = h.b1; *b2 = h.b2; code = h.tri; }
   }
   for (uint32_t i = 0; i < S->nshapes; ++i) {
@@ -1106,7 +1184,7 @@ static int scene_closest_media(const rscene_t* S, f3 o, f3 d, float tmax, float*
 
 static int scene_occluded(const rscene_t* S, f3 o, f3 d, float tmax) {
   if (S->ntris > 0) {
-    hit_t h = oi_trace(S->nodes, S->tris, o, d, tmax, 1);
+    hit_t h = oi_trace_alpha(S->nodes, S->tris, o, d, tmax, 1, S->alpha.alpha_tex ? &S->alpha : NULL);
     if (h.tri >= 0) return 1;
   }
   if (S->nshapes > 0) {
@@ -1289,6 +1367,7 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
     f3 pos = add3(o, mul3s(d, t));
     f3 n;
     const mat_t* m;
+    mat_t mt;
     if (code >= 0) {
       uint32_t prim = S->order[code];
       const uint32_t* tv = &S->idx[3 * (size_t)prim];
@@ -1298,6 +1377,11 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
       float b0 = (1.0f - hb1) - hb2;
       n = norm3(add3(add3(mul3s(n0, b0), mul3s(n1, hb1)), mul3s(n2, hb2)));
       m = &S->mats[S->triMat[prim]];
+      if (S->triUV && (m->tex[0] >= 0 || m->tex[1] >= 0 || m->tex[2] >= 0)) {
+        mt = *m;
+        textured_surface(S, code, hb1, hb2, &n, &mt);
+        m = &mt;
+      }
     } else {
       const orc_shape* sh = &S->shapes[-2 - code];
       n = sh->type == 1 ? norm3(F3(sh->normal[0], sh->normal[1], sh->normal[2]))
@@ -1472,9 +1556,22 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   S.triMat = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)(nt + 1));
   S.mats = (mat_t*)malloc(sizeof(mat_t) * (size_t)(nmeshes + 1));
   uint32_t vb = 0, tb = 0;
+  int anyUV = 0;
+  for (uint32_t i = 0; i < nmeshes; ++i) anyUV = anyUV || meshes[i].uvs != NULL;
+  if (anyUV) S.uv = (float*)calloc(2 * (size_t)(nv + 1), sizeof(float));
+  S.tex = (oi_tex*)calloc(5 * (size_t)(nmeshes + 1), sizeof(oi_tex));
   for (uint32_t i = 0; i < nmeshes; ++i) {
     const orc_mesh* M = &meshes[i];
     S.mats[i] = make_mat(&M->material);
+    if (M->uvs) memcpy(&S.uv[2 * (size_t)vb], M->uvs, sizeof(float) * 2 * (size_t)M->nverts);
+    /* CMaterial(aiMaterial*) (material.cu:110-143) */
+    const float* ks = M->material.specular;
+    if (M->albedo) S.mats[i].tex[0] = tex_add(&S, M->albedo, TEX_COLOR);
+    if (M->albedo && (ks[0] <= 0.02f || ks[1] <= 0.02f || ks[2] <= 0.02f)) S.mats[i].tex[1] = tex_add(&S, M->albedo, TEX_LUMA);
+    else if (M->specular) S.mats[i].tex[1] = tex_add(&S, M->specular, TEX_COLOR);
+    if (M->normal) S.mats[i].tex[2] = tex_add(&S, M->normal, TEX_COLOR);
+    if (M->alpha) S.mats[i].tex[3] = tex_add(&S, M->alpha, TEX_COLOR);
+    else if (M->albedo && M->albedo->channels == 4) S.mats[i].tex[3] = tex_add(&S, M->albedo, TEX_ALPHA);
     for (uint32_t v = 0; v < M->nverts; ++v) {
       f3 pp = xpoint(M->model_to_world, F3(M->positions[3 * v], M->positions[3 * v + 1], M->positions[3 * v + 2]));
       f3 nn = xvec(M->model_to_world, F3(M->normals[3 * v], M->normals[3 * v + 1], M->normals[3 * v + 2]));
@@ -1495,6 +1592,26 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
     S.tris = (float*)malloc(48 * (size_t)nt);
     int h = orc_build_bvh(wpos, nv, S.idx, nt, S.nodes, S.order, S.tris);
     if (h < 0 || h > 96) return -2;
+    if (anyUV) {  /* per BVH-order triangle: texture coordinates and opacity map */
+      S.triUV = (float*)malloc(sizeof(float) * 6 * (size_t)nt);
+      S.triAlpha = (int*)malloc(sizeof(int) * (size_t)nt);
+      int anyAlpha = 0;
+      for (uint32_t i = 0; i < nt; ++i) {
+        const uint32_t prim = S.order[i];
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t v = S.idx[3 * (size_t)prim + k];
+          S.triUV[6 * (size_t)i + 2 * k] = S.uv[2 * (size_t)v];
+          S.triUV[6 * (size_t)i + 2 * k + 1] = S.uv[2 * (size_t)v + 1];
+        }
+        S.triAlpha[i] = S.mats[S.triMat[prim]].tex[3];
+        anyAlpha = anyAlpha || S.triAlpha[i] >= 0;
+      }
+      if (anyAlpha) {
+        S.alpha.alpha_tex = S.triAlpha;
+        S.alpha.uv = S.triUV;
+        S.alpha.tex = S.tex;
+      }
+    }
   }
   S.shapes = shapes;
   S.nshapes = nshapes;
@@ -1521,6 +1638,9 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   free(jobs); free(th);
   env_free(&S.env);
   free(wpos); free(S.wnrm); free(S.idx); free(S.triMat); free(S.mats); free(S.shapeMats);
+  free(S.uv); free(S.triUV); free(S.triAlpha);
+  for (int k = 0; k < S.ntex; ++k) free(S.tex[k].texels);
+  free(S.tex);
   if (nt > 0) { free(S.nodes); free(S.order); free(S.tris); }
   for (uint32_t i = 0; i < nmedia; ++i) med_free(&meds[i]);
   free(meds);

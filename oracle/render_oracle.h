@@ -21,6 +21,14 @@
 extern "C" {
 #endif
 
+/* A texture map as decoded from its file: 8-bit RGBA, row 0 = top, and the
+ * file's channel count. */
+typedef struct orc_texture {
+  uint32_t width, height;
+  int channels;
+  const uint8_t* rgba;
+} orc_texture;
+
 typedef struct orc_mesh {
   const float* positions; /* model space, 3 per vertex */
   uint32_t nverts;
@@ -29,6 +37,13 @@ typedef struct orc_mesh {
   const float* normals;
   float model_to_world[12];
   orc_material material;
+  const float* uvs;  /* nullable: 2 texture coordinates per vertex */
+  /* texture maps of the material (nullable), CMaterial(aiMaterial*)
+   * (material.cu:110-143): map_Kd, map_Ks, map_Bump, map_d */
+  const orc_texture* albedo;
+  const orc_texture* specular;
+  const orc_texture* normal;
+  const orc_texture* alpha;
 } orc_mesh;
 
 typedef struct orc_shape {

@@ -39,6 +39,10 @@ class Material(C.Structure):
                 ("diffuse_roughness", C.c_float), ("pad", C.c_float)]
 
 
+class MaterialMaps(C.Structure):
+    _fields_ = [("albedo", C.c_char_p), ("specular", C.c_char_p), ("normal", C.c_char_p), ("alpha", C.c_char_p)]
+
+
 class FilterParams(C.Structure):
     _fields_ = [("min_voxel_size", C.c_float), ("lods", C.c_uint32), ("samples_per_voxel", C.c_uint32),
                 ("sigma_t", C.c_float), ("estimation_iterations", C.c_uint32), ("alpha", C.c_float),
@@ -75,6 +79,7 @@ def _load():
         "r2_scene_create": (C.c_int, [P]),
         "r2_scene_destroy": (C.c_int, [P]),
         "r2_scene_add_mesh": (C.c_int, [P, P, u32, P, u32, P, P, P, u32]),
+        "r2_scene_add_mesh_textured": (C.c_int, [P, P, u32, P, u32, P, P, P, P, P, u32]),
         "r2_scene_add_shape": (C.c_int, [P, C.c_int, P, f32, P, P, u32]),
         "r2_scene_set_envmap": (C.c_int, [P, P, u32, u32]),
         "r2_scene_add_medium": (C.c_int, [P, C.c_char_p, P, P, P, P, P, u32]),

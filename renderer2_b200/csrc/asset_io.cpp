@@ -24,7 +24,15 @@ struct MtlEntry {
   float ks[3] = {0.0f, 0.0f, 0.0f};
   float ns = 0.0f;
   float ni = 1.0f;
+  std::string mapKd, mapKs, mapBump, mapD;
 };
+
+// The file name of a map_* statement: its last token (options such as -bm come first).
+std::string map_file(std::istringstream& ls) {
+  std::string tok, last;
+  while (ls >> tok) last = tok;
+  return last;
+}
 
 r2_material material_from_mtl(const MtlEntry& m) {
   r2_material r;
@@ -67,13 +75,17 @@ void parse_mtl(const std::string& path, std::map<std::string, MtlEntry>* out) {
       else if (key == "Ks") ls >> m.ks[0] >> m.ks[1] >> m.ks[2];
       else if (key == "Ns") ls >> m.ns;
       else if (key == "Ni") ls >> m.ni;
+      else if (key == "map_Kd") m.mapKd = map_file(ls);
+      else if (key == "map_Ks") m.mapKs = map_file(ls);
+      else if (key == "map_Bump" || key == "map_bump" || key == "bump") m.mapBump = map_file(ls);
+      else if (key == "map_d") m.mapD = map_file(ls);
     }
   }
 }
 
-// one corner of a face: 0-based position / normal index (-1: none)
+// one corner of a face: 0-based position / texture coordinate / normal index (-1: none)
 struct Corner {
-  int64_t v, vn;
+  int64_t v, vt, vn;
 };
 
 int64_t resolve(long long i, size_t count, const std::string& path) {
@@ -87,11 +99,12 @@ int64_t resolve(long long i, size_t count, const std::string& path) {
 std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string& filename) {
   const std::string path = directory + "/" + filename;
   std::istringstream in(read_text_file(path));
-  std::vector<float> v, vn;
+  std::vector<float> v, vn, vt;
   std::map<std::string, MtlEntry> mtl;
   std::vector<ObjSubmesh> subs;
   std::map<std::string, size_t> subIndex;
-  std::vector<std::map<std::pair<int64_t, int64_t>, uint32_t>> dedup;
+  std::vector<std::map<std::tuple<int64_t, int64_t, int64_t>, uint32_t>> dedup;
+  std::vector<bool> anyUv;
   size_t cur = (size_t)-1;
   auto select = [&](const std::string& name) {
     auto it = subIndex.find(name);
@@ -101,6 +114,7 @@ std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string
       subIndex[name] = subs.size();
       subs.push_back(s);
       dedup.emplace_back();
+      anyUv.push_back(false);
       cur = subs.size() - 1;
     } else {
       cur = it->second;
@@ -121,6 +135,10 @@ std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string
       float x = 0, y = 0, z = 0;
       ls >> x >> y >> z;
       vn.push_back(x); vn.push_back(y); vn.push_back(z);
+    } else if (key == "vt") {
+      float x = 0, y = 0;
+      ls >> x >> y;
+      vt.push_back(x); vt.push_back(y);
     } else if (key == "mtllib") {
       std::string rest;
       std::getline(ls, rest);
@@ -136,30 +154,39 @@ std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string
       while (ls >> tok) {
         long long iv = 0, it = 0, in2 = 0;
         int n = 0;
-        Corner c = {-1, -1};
-        if (sscanf(tok.c_str(), "%lld/%lld/%lld", &iv, &it, &in2) == 3) n = 3;
+        Corner c = {-1, -1, -1};
+        bool hasT = false;
+        if (sscanf(tok.c_str(), "%lld/%lld/%lld", &iv, &it, &in2) == 3) n = 3, hasT = true;
         else if (sscanf(tok.c_str(), "%lld//%lld", &iv, &in2) == 2) n = 2;
-        else if (sscanf(tok.c_str(), "%lld/%lld", &iv, &it) == 2) n = 1;
+        else if (sscanf(tok.c_str(), "%lld/%lld", &iv, &it) == 2) n = 1, hasT = true;
         else if (sscanf(tok.c_str(), "%lld", &iv) == 1) n = 1;
         R2_REQUIRE(n > 0, R2_ERR_IO, "bad OBJ face corner '" + tok + "' in " + path);
         c.v = resolve(iv, v.size() / 3, path);
         if (n >= 2) c.vn = resolve(in2, vn.size() / 3, path);
+        if (hasT && !vt.empty()) c.vt = resolve(it, vt.size() / 2, path);  // without vt lines the index is ignored
         face.push_back(c);
       }
       R2_REQUIRE(face.size() >= 3, R2_ERR_IO, "OBJ face with fewer than 3 corners in " + path);
       ObjSubmesh& s = subs[cur];
       bool hasN = true;
       for (const Corner& c : face) hasN = hasN && c.vn >= 0;
+      for (const Corner& c : face) anyUv[cur] = anyUv[cur] || c.vt >= 0;
+      // texture coordinates of every vertex so far (0 where a corner has none)
+      auto push_uv = [&](const Corner& c) {
+        s.uvs.push_back(c.vt >= 0 ? vt[2 * c.vt] : 0.0f);
+        s.uvs.push_back(c.vt >= 0 ? vt[2 * c.vt + 1] : 0.0f);
+      };
       for (size_t k = 1; k + 1 < face.size(); ++k) {  // fan triangulation
         const Corner tri[3] = {face[0], face[k], face[k + 1]};
         if (hasN) {
           for (const Corner& c : tri) {
-            auto key = std::make_pair(c.v, c.vn);
+            auto key = std::make_tuple(c.v, c.vt, c.vn);
             auto it2 = dedup[cur].find(key);
             if (it2 == dedup[cur].end()) {
               const uint32_t id = (uint32_t)(s.positions.size() / 3);
               for (int a = 0; a < 3; ++a) s.positions.push_back(v[3 * c.v + a]);
               for (int a = 0; a < 3; ++a) s.normals.push_back(vn[3 * c.vn + a]);
+              push_uv(c);
               dedup[cur][key] = id;
               s.indices.push_back(id);
             } else {
@@ -180,6 +207,7 @@ std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string
             const uint32_t id = (uint32_t)(s.positions.size() / 3);
             for (int a = 0; a < 3; ++a) s.positions.push_back(p[i][a]);
             for (int a = 0; a < 3; ++a) s.normals.push_back(nn[a]);
+            push_uv(tri[i]);
             s.indices.push_back(id);
           }
         }
@@ -187,10 +215,18 @@ std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string
     }
   }
   std::vector<ObjSubmesh> out;
-  for (ObjSubmesh& s : subs) {
+  for (size_t k = 0; k < subs.size(); ++k) {
+    ObjSubmesh& s = subs[k];
     if (s.indices.empty()) continue;
+    if (!anyUv[k]) s.uvs.clear();
     auto it = mtl.find(s.materialName);
-    s.material = material_from_mtl(it == mtl.end() ? MtlEntry() : it->second);
+    const MtlEntry m = it == mtl.end() ? MtlEntry() : it->second;
+    s.material = material_from_mtl(m);
+    auto joined = [&](const std::string& f) { return f.empty() ? f : directory + "/" + f; };
+    s.texAlbedo = joined(m.mapKd);
+    s.texSpecular = joined(m.mapKs);
+    s.texNormal = joined(m.mapBump);
+    s.texAlpha = joined(m.mapD);
     out.push_back(std::move(s));
   }
   R2_REQUIRE(!out.empty(), R2_ERR_IO, "no triangles in " + path);

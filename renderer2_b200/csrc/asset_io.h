@@ -29,11 +29,16 @@ struct ObjSubmesh {
   std::string materialName;
   std::vector<float> positions;  // 3 per vertex
   std::vector<float> normals;    // 3 per vertex
+  std::vector<float> uvs;        // 2 per vertex, empty when no face has texture coordinates
   std::vector<uint32_t> indices; // 3 per triangle
   r2_material material;
+  // texture maps of the material (paths joined to the OBJ's directory, empty: none):
+  // map_Kd (albedo), map_Ks (specular), map_Bump / bump (normal map), map_d (opacity)
+  std::string texAlbedo, texSpecular, texNormal, texAlpha;
 };
 
-// Submeshes of <directory>/<filename> in order of first use of their material.
+// Submeshes of <directory>/<filename> in order of first use of their material
+// (vertices joined on identical position, texture coordinate and normal).
 std::vector<ObjSubmesh> load_obj(const std::string& directory, const std::string& filename);
 
 struct RgbImage {

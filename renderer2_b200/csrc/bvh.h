@@ -12,6 +12,7 @@
 // ch.w its depth (build bookkeeping; traversal ignores them).
 #pragma once
 #include "r2_core.h"
+#include "texture.h"
 
 namespace r2 {
 
@@ -26,11 +27,36 @@ static_assert(sizeof(BvhNode) == 64, "BvhNode must be 64 bytes");
 // Marker for an absent second child (a BVH over a single leaf).
 #define R2_BVH_NONE ((int)0x80000000)
 
+// Alpha-tested triangles: the reference's __anyhit__mesh
+// (shaders.optix.cu:132-152) ignores a hit where the material's opacity
+// texture reads 0 at the hit's texture coordinates (CMaterial::opaque,
+// material.hpp:134-141).  Per BVH-order triangle.
+struct BvhAlpha {
+  const int* alphaTex;    // texture index of the triangle's opacity map, -1: opaque; null: no alpha test
+  const float2* uv;       // 3 texture coordinates per triangle
+  const float4* texels;
+  const TexInfo* texInfo;
+};
+
 struct BvhView {
   const BvhNode* nodes;
   const float4* tris;  // 3 per triangle, BVH order
   uint32_t ntris;
+  BvhAlpha alpha;      // zero: every triangle opaque
 };
+
+R2_HD bool alpha_opaque(const BvhAlpha& a, int tri, float b1, float b2) {
+#if defined(__CUDA_ARCH__)
+  const int k = __ldg(&a.alphaTex[tri]);
+  if (k < 0) return true;
+  const float2 tc = tex_coord(__ldg(&a.uv[3 * tri]), __ldg(&a.uv[3 * tri + 1]), __ldg(&a.uv[3 * tri + 2]), b1, b2);
+#else
+  const int k = a.alphaTex[tri];
+  if (k < 0) return true;
+  const float2 tc = tex_coord(a.uv[3 * tri], a.uv[3 * tri + 1], a.uv[3 * tri + 2], b1, b2);
+#endif
+  return tex_lookup(a.texels, a.texInfo[k], tc.x, tc.y).x > 0.0f;
+}
 
 struct Hit {
   float t;
@@ -79,8 +105,10 @@ R2_HD bool slab(const RayPre& r, float lox, float hix, float loy, float hiy, flo
 }
 
 // Watertight test.  Accepts 0 < t and (t, tri) lexicographically below the
-// current best (t, tri) so the closest hit is independent of visiting order.
-R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, Hit* best) {
+// current best (t, tri) so the closest hit is independent of visiting order;
+// kAlpha: and only where the triangle is opaque.
+template <bool kAlpha = false>
+R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, Hit* best, const BvhAlpha* alpha = nullptr) {
   V3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
   float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
   float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
@@ -106,9 +134,11 @@ R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, Hit* best) {
   float t = T * rcp;
   if (!(t > 0.0f)) return false;
   if (t < best->t || (t == best->t && tri < best->tri)) {
+    const float b1 = V * rcp, b2 = W * rcp;
+    if (kAlpha && !alpha_opaque(*alpha, tri, b1, b2)) return false;
     best->t = t;
-    best->b1 = V * rcp;
-    best->b2 = W * rcp;
+    best->b1 = b1;
+    best->b2 = b2;
     best->tri = tri;
     return true;
   }
@@ -178,7 +208,7 @@ R2_HD bool trace_all_have_leaf(bool mine) {
 // entry distance.  The builder bounds the tree depth by R2_BVH_STACK so the
 // stack cannot overflow.  The closest hit does not depend on the visiting
 // order (ties go to the lower triangle index).
-template <bool kAnyHit, bool kCount = false>
+template <bool kAnyHit, bool kCount = false, bool kAlpha = false>
 R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* stackT, int maxVisits) {
   int budget = maxVisits;
   while (budget > 0) {
@@ -239,7 +269,8 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
         const float4 b = bvh.tris[3 * tri + 1];
         const float4 c = bvh.tris[3 * tri + 2];
 #endif
-        if (tri_test(s.r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &s.best)) {
+        if (tri_test<kAlpha>(s.r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &s.best,
+                             &bvh.alpha)) {
           s.found = 1;
           if (kAnyHit) {
             s.leaf = 0;
@@ -271,7 +302,12 @@ R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax, uint32_t* nodes 
   trace_begin(s, o, d, tmax);
   int stack[R2_BVH_STACK];
   float stackT[R2_BVH_STACK];
-  while (!trace_advance<kAnyHit, kCount>(bvh, s, stack, stackT, 1 << 30)) {
+  if (bvh.alpha.alphaTex) {
+    while (!trace_advance<kAnyHit, kCount, true>(bvh, s, stack, stackT, 1 << 30)) {
+    }
+  } else {
+    while (!trace_advance<kAnyHit, kCount, false>(bvh, s, stack, stackT, 1 << 30)) {
+    }
   }
   if (kCount) {
     *nodes += s.nodes;

@@ -21,6 +21,7 @@ struct DeviceBvh {
   uint32_t height = 0;     // levels of inner nodes on the longest root-leaf path
   BvhView view() const {
     BvhView v;
+    memset(&v, 0, sizeof(v));
     v.nodes = nodes.get();
     v.tris = tris.get();
     v.ntris = ntris;

@@ -50,9 +50,13 @@ void build_scene(r2_config* c) {
       case r2::SceneObjectDesc::kMesh: {
         float m43[12];
         r2::m43_to_floats(r2::m4_to_m43(object_transform(o)), m43);
-        for (const r2::ObjSubmesh& s : c->meshes[mi])
+        for (const r2::ObjSubmesh& s : c->meshes[mi]) {
+          const r2_material_maps maps = {s.texAlbedo.c_str(), s.texSpecular.c_str(), s.texNormal.c_str(),
+                                         s.texAlpha.c_str()};
           sc->add_mesh(s.positions.data(), (uint32_t)(s.positions.size() / 3), s.indices.data(),
-                       (uint32_t)(s.indices.size() / 3), s.normals.data(), s.material, m43, o.mask);
+                       (uint32_t)(s.indices.size() / 3), s.normals.data(), s.material, m43, o.mask,
+                       s.uvs.empty() ? nullptr : s.uvs.data(), &maps);
+        }
         ++mi;
         break;
       }

@@ -46,6 +46,16 @@ r2_status r2_scene_add_mesh(r2_scene* scene, const float* positions, uint32_t nv
   R2_API_END
 }
 
+r2_status r2_scene_add_mesh_textured(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
+                                     uint32_t ntris, const float* normals, const float* uvs,
+                                     const r2_material* material, const r2_material_maps* maps,
+                                     const float* model_to_world, uint32_t mask) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && material && uvs, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->add_mesh(positions, nverts, indices, ntris, normals, *material, model_to_world, mask, uvs, maps);
+  R2_API_END
+}
+
 r2_status r2_scene_add_shape(r2_scene* scene, int shape_type, const float* center, float radius, const float* normal,
                              const r2_material* material, uint32_t mask) {
   R2_API_BEGIN

@@ -31,6 +31,9 @@ struct SceneView {
   const MediumView* media;  // medium instances (device array), nullable
   int nmedia;
   EnvMap env;
+  const float2* triUV;      // 3 texture coordinates per BVH-order triangle, nullable
+  const float4* texels;     // texture maps of the materials (TexInfo offsets), nullable
+  const TexInfo* texInfo;
 };
 
 // Per-path SoA state of one wave (one sample of every pixel).

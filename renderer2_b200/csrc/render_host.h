@@ -72,8 +72,11 @@ class RenderScene {
   RenderScene(const RenderScene&) = delete;
   RenderScene& operator=(const RenderScene&) = delete;
 
+  // uv (nullable): 2 texture coordinates per vertex; maps (nullable): the
+  // material's texture files.
   void add_mesh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
-                const r2_material& mat, const float* modelToWorld, uint32_t mask);
+                const r2_material& mat, const float* modelToWorld, uint32_t mask, const float* uv = nullptr,
+                const r2_material_maps* maps = nullptr);
   void add_shape(int type, const float* center, float radius, const float* normal, const r2_material& mat,
                  uint32_t mask);
   void set_envmap(const float* rgb, int W, int H);
@@ -115,7 +118,20 @@ class RenderScene {
   static void check_params(const r2_camera& c, const r2_render_params& p, const float* d_frame);
   RenderContext ctx_;
   bool committed_ = false;
-  std::vector<float> hPos_, hNrm_;
+  // Index of the texture of file `path` converted as `kind` (loaded once per scene).
+  int texture(const std::string& path, int kind);
+  std::vector<float> hPos_, hNrm_, hUV_;
+  bool anyUV_ = false;
+  struct TexHost {
+    std::string path;
+    int kind = 0, W = 0, H = 0, channels = 0;
+    std::vector<float4> texels;
+  };
+  std::vector<TexHost> textures_;
+  DBuf<float2> triUV_;
+  DBuf<int> triAlpha_;
+  DBuf<float4> texels_;
+  DBuf<TexInfo> texInfo_;
   std::vector<uint32_t> hIdx_, hTriMat_;
   std::vector<Material> hMats_;
   std::vector<Shape> hShapes_;

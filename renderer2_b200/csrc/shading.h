@@ -152,6 +152,7 @@ struct Material {
   float onA, onB;        // Oren-Nayar coefficients
   Ggx ggx;
   float etaI, etaT;      // CFresnel of the microfacet BRDF
+  int tex[4];            // texture maps: albedo, glossy, normal, opacity (-1: none)
 };
 
 R2_HD Material make_material(const r2_material& m) {
@@ -165,6 +166,7 @@ R2_HD Material make_material(const r2_material& m) {
   r.ggx.ay = m.alpha_y;
   r.etaI = m.eta_i;
   r.etaT = m.eta_t;
+  for (int k = 0; k < 4; ++k) r.tex[k] = -1;
   return r;
 }
 

@@ -89,6 +89,21 @@ class Scene:
         N.check(N.lib.r2_scene_add_mesh(self.handle, N.ptr(pos), pos.shape[0], N.ptr(idx), idx.shape[0], N.ptr(nrm),
                                         C.byref(material), N.ptr(m2w), mask))
 
+    def add_mesh_textured(self, mesh, material, uv, model_to_world=None, mask=255, albedo=None, specular=None,
+                          normal=None, alpha=None):
+        """Mesh with texture coordinates (n, 2) and PNG texture maps (r2_scene_add_mesh_textured)."""
+        pos = np.ascontiguousarray(mesh.positions, np.float32)
+        idx = np.ascontiguousarray(mesh.indices, np.uint32)
+        nrm = np.ascontiguousarray(mesh.normals, np.float32)
+        uvs = np.ascontiguousarray(uv, np.float32)
+        assert uvs.shape == (pos.shape[0], 2)
+        m2w = np.ascontiguousarray(N.identity43() if model_to_world is None else model_to_world, np.float32)
+        enc = [str(p).encode() if p else None for p in (albedo, specular, normal, alpha)]
+        maps = N.MaterialMaps(*enc)
+        N.check(N.lib.r2_scene_add_mesh_textured(self.handle, N.ptr(pos), pos.shape[0], N.ptr(idx), idx.shape[0],
+                                                 N.ptr(nrm), N.ptr(uvs), C.byref(material), C.byref(maps), N.ptr(m2w),
+                                                 mask))
+
     def add_shape(self, kind, center, radius, normal, material, mask=255):
         c = np.ascontiguousarray(center, np.float32)
         n = np.ascontiguousarray(normal, np.float32)

@@ -84,8 +84,14 @@ def volume_scene(work_dir, index: int = 0, grid: int = 256, n_quads: int = 200_0
 
 def build_scene(desc) -> R.Scene:
     sc = R.Scene()
-    for mesh, mat, m2w in desc.get("meshes", []):
-        sc.add_mesh(mesh, mat, m2w)
+    for entry in desc.get("meshes", []):
+        mesh, mat, m2w = entry[:3]
+        tex = entry[3] if len(entry) > 3 else None
+        if tex is None:
+            sc.add_mesh(mesh, mat, m2w)
+        else:
+            sc.add_mesh_textured(mesh, mat, tex["uv"], m2w, albedo=tex.get("albedo"), specular=tex.get("specular"),
+                                 normal=tex.get("normal"), alpha=tex.get("alpha"))
     for kind, c, r, n, mat in desc.get("shapes", []):
         sc.add_shape(kind, c, r, n, mat)
     for med in desc.get("media", []):

@@ -146,9 +146,15 @@ def filter_voxels(mesh, mat, m2w, grid, prm, v0=0, v1=None, lod=0, threads=0):
 
 # ---------------------------------------------------------------- path tracer oracle
 
+class OTexture(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("channels", C.c_int), ("rgba", C.c_void_p)]
+
+
 class OMesh(C.Structure):
     _fields_ = [("positions", C.c_void_p), ("nverts", C.c_uint32), ("indices", C.c_void_p), ("ntris", C.c_uint32),
-                ("normals", C.c_void_p), ("model_to_world", C.c_float * 12), ("material", Material)]
+                ("normals", C.c_void_p), ("model_to_world", C.c_float * 12), ("material", Material),
+                ("uvs", C.c_void_p), ("albedo", C.c_void_p), ("specular", C.c_void_p), ("normal", C.c_void_p),
+                ("alpha", C.c_void_p)]
 
 
 class OShape(C.Structure):
@@ -196,7 +202,20 @@ def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want
         media[i].orientation[:] = list(map(float, ori))
         media[i].scaling[:] = list(map(float, sc))
     meshes = (OMesh * max(1, len(scene_desc.get("meshes", []))))()
-    for i, (mesh, mat, m2w) in enumerate(scene_desc.get("meshes", [])):
+    for i, entry in enumerate(scene_desc.get("meshes", [])):
+        mesh, mat, m2w = entry[:3]
+        tex = entry[3] if len(entry) > 3 else None
+        if tex is not None:  # texture coordinates and texture maps decoded by the library's PNG reader
+            from renderer2_b200 import pipeline as P
+            uv = np.ascontiguousarray(tex["uv"], np.float32)
+            keep.append(uv)
+            meshes[i].uvs = uv.ctypes.data
+            for key in ("albedo", "specular", "normal", "alpha"):
+                if tex.get(key):
+                    rgba, ch = P.read_png(tex[key])
+                    ot = OTexture(rgba.shape[1], rgba.shape[0], ch, rgba.ctypes.data)
+                    keep += [rgba, ot]
+                    setattr(meshes[i], key, C.addressof(ot))
         pos = np.ascontiguousarray(mesh.positions, np.float32)
         idx = np.ascontiguousarray(mesh.indices, np.uint32)
         nrm = np.ascontiguousarray(mesh.normals, np.float32)
