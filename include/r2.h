@@ -70,6 +70,21 @@ typedef struct r2_material {
   float pad;
 } r2_material;
 
+/* Texture maps of a mesh's material (file paths, nullable or empty: none), as
+ * the reference's CMaterial(aiMaterial*) reads them (material.cu:110-143):
+ * albedo (map_Kd), specular (map_Ks; unused when the albedo map exists and a
+ * specular channel is at most 0.02: the albedo's luma is the glossy colour
+ * then), normal (map_Bump / bump: tangent-space normal map), alpha (map_d;
+ * without it an albedo map with an alpha channel is the opacity).  Opacity 0
+ * makes a triangle invisible to every ray (__anyhit__mesh,
+ * shaders.optix.cu:132-152).  PNG files (any colour type). */
+typedef struct r2_material_maps {
+  const char* albedo;
+  const char* specular;
+  const char* normal;
+  const char* alpha;
+} r2_material_maps;
+
 /* Filter parameters: the "Filtering" block of config.json
  * (raytracer/src/backend/config_loader.cu:75-100) plus build options. */
 typedef struct r2_filter_params {
@@ -127,6 +142,15 @@ r2_status r2_filter_scene_create(const float* positions, uint32_t nverts,
                                  const uint32_t* indices, uint32_t ntris, const float* normals,
                                  const r2_material* material, const float* model_to_world,
                                  r2_filter_scene** out);
+/* The same with texture coordinates (2 per vertex) and the material's texture
+ * maps (see r2_material_maps): each hit contributes diffuse(tc), glossy(tc)
+ * and the normal-mapped normal, and opacity cut-outs hide triangles from the
+ * filter rays (CMeshFilter::run, mesh_filter.hpp:300-371, over the closest-hit
+ * and any-hit programs, shaders.optix.cu:28-152). */
+r2_status r2_filter_scene_create_textured(const float* positions, uint32_t nverts, const uint32_t* indices,
+                                          uint32_t ntris, const float* normals, const float* uvs,
+                                          const r2_material* material, const r2_material_maps* maps,
+                                          const float* model_to_world, r2_filter_scene** out);
 r2_status r2_filter_scene_destroy(r2_filter_scene* scene);
 /* Grid for a voxel size over this scene's bounds. */
 r2_status r2_filter_scene_grid(const r2_filter_scene* scene, float voxel_size,
@@ -274,20 +298,6 @@ r2_status r2_scene_add_medium(r2_scene* scene, const char* path, const float* si
 r2_status r2_scene_add_medium_hg(r2_scene* scene, const char* path, const float* sigma_a, const float* sigma_s,
                                  float g, const float* pos, const float* orientation, const float* scaling,
                                  uint32_t mask);
-/* Texture maps of a mesh's material (file paths, nullable or empty: none), as
- * the reference's CMaterial(aiMaterial*) reads them (material.cu:110-143):
- * albedo (map_Kd), specular (map_Ks; unused when the albedo map exists and a
- * specular channel is at most 0.02: the albedo's luma is the glossy colour
- * then), normal (map_Bump / bump: tangent-space normal map), alpha (map_d;
- * without it an albedo map with an alpha channel is the opacity).  Opacity 0
- * makes a triangle invisible to every ray (__anyhit__mesh,
- * shaders.optix.cu:132-152).  PNG files (any colour type). */
-typedef struct r2_material_maps {
-  const char* albedo;
-  const char* specular;
-  const char* normal;
-  const char* alpha;
-} r2_material_maps;
 /* r2_scene_add_mesh with texture coordinates (uvs: 2 per vertex, v = 0 at the
  * maps' top row as stb_image loads them) and texture maps. */
 r2_status r2_scene_add_mesh_textured(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,

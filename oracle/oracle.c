@@ -387,6 +387,81 @@ void oi_tex_lookup(const oi_tex* t, float u, float v, float out[4]) {
   for (int c = 0; c < 4; ++c) out[c] = w00 * tx[0][c] + w10 * tx[1][c] + w01 * tx[2][c] + w11 * tx[3][c];
 }
 
+void oi_tex_from(const orc_texture* src, int kind, oi_tex* t) {
+  t->W = (int)src->width;
+  t->H = (int)src->height;
+  const size_t n = (size_t)t->W * t->H;
+  t->texels = (float*)malloc(sizeof(float) * 4 * n);
+  for (size_t i = 0; i < n; ++i) {
+    const uint8_t* p = &src->rgba[4 * i];
+    const float r = (float)p[0] / 255.0f, g = (float)p[1] / 255.0f, b = (float)p[2] / 255.0f;
+    float* o = &t->texels[4 * i];
+    if (kind == OI_TEX_ALPHA) {
+      const float a = (float)p[3] / 255.0f;
+      o[0] = o[1] = o[2] = a;
+    } else if (kind == OI_TEX_LUMA) {
+      float l = 0.2126f * r;
+      l += 0.7152f * g;
+      l += 0.0722f * b;
+      o[0] = o[1] = o[2] = l;
+    } else {
+      o[0] = r; o[1] = g; o[2] = b;
+    }
+    o[3] = 1.0f;
+  }
+}
+
+void oi_material_maps(const orc_material* m, const orc_texture* albedo, const orc_texture* specular,
+                      const orc_texture* normal, const orc_texture* alpha, oi_tex* tex, int* ntex, int out[4]) {
+  for (int k = 0; k < 4; ++k) out[k] = -1;
+  const float* ks = m->specular;
+  if (albedo) { oi_tex_from(albedo, OI_TEX_COLOR, &tex[*ntex]); out[0] = (*ntex)++; }
+  if (albedo && (ks[0] <= 0.02f || ks[1] <= 0.02f || ks[2] <= 0.02f)) {
+    oi_tex_from(albedo, OI_TEX_LUMA, &tex[*ntex]); out[1] = (*ntex)++;
+  } else if (specular) {
+    oi_tex_from(specular, OI_TEX_COLOR, &tex[*ntex]); out[1] = (*ntex)++;
+  }
+  if (normal) { oi_tex_from(normal, OI_TEX_COLOR, &tex[*ntex]); out[2] = (*ntex)++; }
+  if (alpha) { oi_tex_from(alpha, OI_TEX_COLOR, &tex[*ntex]); out[3] = (*ntex)++; }
+  else if (albedo && albedo->channels == 4) { oi_tex_from(albedo, OI_TEX_ALPHA, &tex[*ntex]); out[3] = (*ntex)++; }
+}
+
+void oi_textured_surface(const oi_tex* tex, int tAlbedo, int tGlossy, int tNormal, const float* uv,
+                         const float* tv, float b1, float b2, f3* n, f3* diffuse, f3* specular) {
+  const float b0 = (1.0f - b1) - b2;
+  const float tcx = b0 * uv[0] + b1 * uv[2] + b2 * uv[4], tcy = b0 * uv[1] + b1 * uv[3] + b2 * uv[5];
+  float c[4];
+  if (tAlbedo >= 0) {
+    oi_tex_lookup(&tex[tAlbedo], tcx, tcy, c);
+    *diffuse = F3(c[0], c[1], c[2]);
+  }
+  if (tGlossy >= 0) {
+    oi_tex_lookup(&tex[tGlossy], tcx, tcy, c);
+    *specular = F3(c[0], c[1], c[2]);
+  }
+  if (tNormal >= 0) {
+    const f3 P0 = F3(tv[0], tv[1], tv[2]), P1 = F3(tv[4], tv[5], tv[6]), P2 = F3(tv[8], tv[9], tv[10]);
+    const f3 P = add3(add3(mul3s(P0, b0), mul3s(P1, b1)), mul3s(P2, b2));
+    const f3 e1 = sub3(P1, P), e2 = sub3(P2, P);
+    const float du1 = uv[2] - tcx, dv1 = uv[3] - tcy, du2 = uv[4] - tcx, dv2 = uv[5] - tcy;
+    const float den = du1 * dv2 - du2 * dv1;
+    if (den != 0.0f) {
+      const float f = 1.0f / den;
+      const f3 T = F3(f * (dv2 * e1.x - dv1 * e2.x), f * (dv2 * e1.y - dv1 * e2.y), f * (dv2 * e1.z - dv1 * e2.z));
+      const f3 B = F3(f * (-du2 * e1.x + du1 * e2.x), f * (-du2 * e1.y + du1 * e2.y), f * (-du2 * e1.z + du1 * e2.z));
+      const int tz = T.x == 0.0f && T.y == 0.0f && T.z == 0.0f, bz = B.x == 0.0f && B.y == 0.0f && B.z == 0.0f;
+      if (!tz && !bz) {
+        oi_tex_lookup(&tex[tNormal], tcx, tcy, c);
+        const f3 nt = F3(c[0] * 2.0f - 1.0f, c[1] * 2.0f - 1.0f, c[2] * 2.0f - 1.0f);
+        if (!(nt.x == 0.0f && nt.y == 0.0f && nt.z == 0.0f)) {
+          const f3 v = norm3(nt);
+          *n = norm3(add3(add3(mul3s(norm3(T), v.x), mul3s(norm3(neg3(B)), v.y)), mul3s(*n, v.z)));
+        }
+      }
+    }
+  }
+}
+
 static int alpha_opaque(const oi_alpha* a, int tri, float b1, float b2) {
   const int k = a->alpha_tex[tri];
   if (k < 0) return 1;
@@ -685,6 +760,10 @@ typedef struct {
   double* wide;
   uint8_t* compact;
   int tid, nthreads;
+  const float* uvs;      /* per vertex, 2 each; null: untextured */
+  const oi_tex* tex;
+  int mtex[4];           /* albedo, glossy, normal, opacity of the material */
+  const oi_alpha* alpha; /* null: no opacity map */
 } job_t;
 
 static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
@@ -723,7 +802,7 @@ static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
     orc_sincos_turns(u01(r1[0]), &sn, &cs);
     f3 d = F3(rr * cs, rr * sn, zz);
     float tmax = p->clip_rays ? sphere_exit(o, d, center, radius) : tmaxFixed;
-    hit_t h = oi_trace(J->nodes, J->tris, o, d, tmax, 0);
+    hit_t h = oi_trace_alpha(J->nodes, J->tris, o, d, tmax, 0, J->alpha);
     if (h.tri < 0) continue;
     uint32_t prim = J->order[h.tri];
     const uint32_t* tv = &J->idx[3 * (size_t)prim];
@@ -734,6 +813,16 @@ static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
     f3 gn = add3(add3(mul3s(n0, b0), mul3s(n1, h.b1)), mul3s(n2, h.b2));
     gn = norm3(gn);
     f3 n = norm3(xvec(J->obj_m2w, gn));
+    f3 kd = F3(m->diffuse[0], m->diffuse[1], m->diffuse[2]), ksp = F3(m->specular[0], m->specular[1], m->specular[2]);
+    if (J->uvs && (J->mtex[0] >= 0 || J->mtex[1] >= 0 || J->mtex[2] >= 0)) {
+      float uv6[6];
+      for (int k = 0; k < 3; ++k) {
+        uv6[2 * k] = J->uvs[2 * (size_t)tv[k]];
+        uv6[2 * k + 1] = J->uvs[2 * (size_t)tv[k] + 1];
+      }
+      oi_textured_surface(J->tex, J->mtex[0], J->mtex[1], J->mtex[2], uv6, &J->tris[12 * (size_t)h.tri], h.b1, h.b2,
+                          &n, &kd, &ksp);
+    }
     /* FP64 accumulation of buildS(n, alpha) and the other means */
     double nx_ = n.x, ny_ = n.y, nz_ = n.z, a = m->alpha_x;
     double xx = nx_ * nx_, xy = nx_ * ny_, xz = nx_ * nz_, yy = ny_ * ny_, yz = ny_ * nz_, zq = nz_ * nz_;
@@ -743,10 +832,8 @@ static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
     S[3] += xy - a * xy;
     S[4] += xz - a * xz;
     S[5] += yz - a * yz;
-    for (int k = 0; k < 3; ++k) {
-      dif[k] += m->diffuse[k];
-      spe[k] += m->specular[k];
-    }
+    dif[0] += kd.x; dif[1] += kd.y; dif[2] += kd.z;
+    spe[0] += ksp.x; spe[1] += ksp.y; spe[2] += ksp.z;
     nrm[0] += nx_;
     nrm[1] += ny_;
     nrm[2] += nz_;
@@ -811,6 +898,15 @@ static void* filter_worker(void* arg) {
 int orc_filter(const float* positions, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* normals,
                const orc_material* mat, const float* obj_m2w, const orc_grid* g, const orc_filter_params* p,
                uint32_t lod, uint64_t v0, uint64_t v1, double* wide_out, uint8_t* compact_out, int threads) {
+  return orc_filter_tex(positions, nverts, idx, ntris, normals, NULL, mat, NULL, NULL, NULL, NULL, obj_m2w, g, p, lod,
+                        v0, v1, wide_out, compact_out, threads);
+}
+
+int orc_filter_tex(const float* positions, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* normals,
+                   const float* uvs, const orc_material* mat, const orc_texture* albedo, const orc_texture* specular,
+                   const orc_texture* normal, const orc_texture* alpha, const float* obj_m2w, const orc_grid* g,
+                   const orc_filter_params* p, uint32_t lod, uint64_t v0, uint64_t v1, double* wide_out,
+                   uint8_t* compact_out, int threads) {
   if (p->samples_per_voxel == 0 || p->samples_per_voxel > 1024) return -1;
   float* wpos = (float*)malloc(sizeof(float) * 3 * (size_t)nverts);
   for (uint32_t v = 0; v < nverts; ++v) {
@@ -826,17 +922,42 @@ int orc_filter(const float* positions, uint32_t nverts, const uint32_t* idx, uin
     free(wpos); free(nodes); free(order); free(tris);
     return -2;
   }
+  /* texture maps (unused without texture coordinates) and the opacity map per BVH-order triangle */
+  oi_tex tex[4];
+  int ntex = 0, mtex[4] = {-1, -1, -1, -1};
+  if (uvs) oi_material_maps(mat, albedo, specular, normal, alpha, tex, &ntex, mtex);
+  oi_alpha al;
+  int* triAlpha = NULL;
+  float* triUV = NULL;
+  if (mtex[3] >= 0) {
+    triAlpha = (int*)malloc(sizeof(int) * (size_t)ntris);
+    triUV = (float*)malloc(sizeof(float) * 6 * (size_t)ntris);
+    for (uint32_t i = 0; i < ntris; ++i) {
+      const uint32_t prim = order[i];
+      triAlpha[i] = mtex[3];
+      for (int k = 0; k < 3; ++k) {
+        triUV[6 * (size_t)i + 2 * k] = uvs[2 * (size_t)idx[3 * (size_t)prim + k]];
+        triUV[6 * (size_t)i + 2 * k + 1] = uvs[2 * (size_t)idx[3 * (size_t)prim + k] + 1];
+      }
+    }
+    al.alpha_tex = triAlpha;
+    al.uv = triUV;
+    al.tex = tex;
+  }
   if (threads <= 0) threads = (int)sysconf(_SC_NPROCESSORS_ONLN);
   if (threads < 1) threads = 1;
   job_t* jobs = (job_t*)malloc(sizeof(job_t) * (size_t)threads);
   pthread_t* th = (pthread_t*)malloc(sizeof(pthread_t) * (size_t)threads);
   for (int t = 0; t < threads; ++t) {
-    job_t J = {g, p, mat, nodes, tris, order, idx, normals, obj_m2w, lod, v0, v1, wide_out, compact_out, t, threads};
+    job_t J = {g, p, mat, nodes, tris, order, idx, normals, obj_m2w, lod, v0, v1, wide_out, compact_out, t, threads,
+               ntex ? uvs : NULL, tex, {mtex[0], mtex[1], mtex[2], mtex[3]}, triAlpha ? &al : NULL};
     jobs[t] = J;
     pthread_create(&th[t], NULL, filter_worker, &jobs[t]);
   }
   for (int t = 0; t < threads; ++t) pthread_join(th[t], NULL);
   free(jobs); free(th); free(wpos); free(nodes); free(order); free(tris);
+  free(triAlpha); free(triUV);
+  for (int k = 0; k < ntex; ++k) free(tex[k].texels);
   return height;
 }
 

@@ -79,6 +79,14 @@ typedef struct orc_grid {
 void orc_setup_grid(const float* model_lo, const float* model_hi, const float* model_to_world, float voxel_size,
                     orc_grid* g);
 
+/* A texture map as decoded from its file: 8-bit RGBA, row 0 = top, and the
+ * file's channel count. */
+typedef struct orc_texture {
+  uint32_t width, height;
+  int channels;
+  const uint8_t* rgba;
+} orc_texture;
+
 /* Filters voxels [v0, v1) of the grid.  wide_out: 20 doubles per voxel of the
  * range (density, S xx yy zz xy xz yz, diffuse, specular, normal, ior, hits,
  * mean ray length, mean roughness); compact_out: 32 bytes per voxel of the
@@ -90,6 +98,14 @@ int orc_filter(const float* positions, uint32_t nverts, const uint32_t* idx, uin
                const orc_material* mat, const float* obj_model_to_world, const orc_grid* g,
                const orc_filter_params* p, uint32_t lod, uint64_t v0, uint64_t v1, double* wide_out,
                uint8_t* compact_out, int threads);
+/* The same for a textured material: uvs (2 per vertex) and the texture maps
+ * (nullable each; map_Kd, map_Ks, map_Bump, map_d as CMaterial(aiMaterial*)
+ * reads them, material.cu:110-143). */
+int orc_filter_tex(const float* positions, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* normals,
+                   const float* uvs, const orc_material* mat, const orc_texture* albedo, const orc_texture* specular,
+                   const orc_texture* normal, const orc_texture* alpha, const float* obj_model_to_world,
+                   const orc_grid* g, const orc_filter_params* p, uint32_t lod, uint64_t v0, uint64_t v1,
+                   double* wide_out, uint8_t* compact_out, int threads);
 
 /* Encode a wide (double) record to the 32-byte payload (FP64 arithmetic). */
 void orc_encode(const double* wide, uint8_t* out32);

@@ -7,6 +7,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "oracle.h"
+
 typedef struct { float x, y, z; } f3;
 static inline f3 F3(float x, float y, float z) { f3 r = {x, y, z}; return r; }
 static inline f3 add3(f3 a, f3 b) { return F3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -47,6 +49,22 @@ hit_t oi_trace(const int32_t* nodes, const float* tris, f3 o, f3 d, float tmax, 
  * raytracer/src/texture/texture.cu:176-189, with float weights). */
 typedef struct { int W, H; float* texels; } oi_tex;
 void oi_tex_lookup(const oi_tex* t, float u, float v, float out[4]);
+/* Texel conversions of the reference's CTexture load paths (texture.cu:29-97,
+ * 217-271, asset_manager.cu:165-184): rgb / 255 (a = 1); the alpha channel / 255
+ * in rgb; the luma of rgb / 255 (luma.hpp:4-6).  Allocates out->texels. */
+enum { OI_TEX_COLOR = 0, OI_TEX_ALPHA = 1, OI_TEX_LUMA = 2 };
+void oi_tex_from(const orc_texture* src, int kind, oi_tex* out);
+/* The texture indices {albedo, glossy, normal, opacity} (-1: none) of a
+ * material and its maps (CMaterial(aiMaterial*), material.cu:110-143),
+ * appending converted textures to tex[*ntex]. */
+void oi_material_maps(const orc_material* m, const orc_texture* albedo, const orc_texture* specular,
+                      const orc_texture* normal, const orc_texture* alpha, oi_tex* tex, int* ntex, int out[4]);
+/* Albedo, glossy and normal-mapped normal at barycentrics (b1, b2) of a
+ * textured triangle: uv6 its 3 texture coordinates, tri12 its 3 world-space
+ * vertices (x y z w each), n the interpolated world normal
+ * (shaders.optix.cu:61-103, material.hpp:111-155). */
+void oi_textured_surface(const oi_tex* tex, int tAlbedo, int tGlossy, int tNormal, const float* uv6,
+                         const float* tri12, float b1, float b2, f3* n, f3* diffuse, f3* specular);
 
 /* Alpha test of triangles (__anyhit__mesh, shaders.optix.cu:132-152): per
  * BVH-order triangle its opacity map (-1: opaque) and 3 texture coordinates;

@@ -1052,76 +1052,6 @@ typedef struct {
   uint32_t spp, maxDepth, seed;
 } rscene_t;
 
-/* Texel conversions of the reference's CTexture load paths (texture.cu:29-97,
- * 217-271, asset_manager.cu:165-184): rgb / 255 (a = 1); the alpha channel / 255
- * in rgb; the luma of rgb / 255 (luma.hpp:4-6). */
-enum { TEX_COLOR = 0, TEX_ALPHA = 1, TEX_LUMA = 2 };
-static int tex_add(rscene_t* S, const orc_texture* src, int kind) {
-  oi_tex* t = &S->tex[S->ntex];
-  t->W = (int)src->width;
-  t->H = (int)src->height;
-  const size_t n = (size_t)t->W * t->H;
-  t->texels = (float*)malloc(sizeof(float) * 4 * n);
-  for (size_t i = 0; i < n; ++i) {
-    const uint8_t* p = &src->rgba[4 * i];
-    const float r = (float)p[0] / 255.0f, g = (float)p[1] / 255.0f, b = (float)p[2] / 255.0f;
-    float* o = &t->texels[4 * i];
-    if (kind == TEX_ALPHA) {
-      const float a = (float)p[3] / 255.0f;
-      o[0] = o[1] = o[2] = a;
-    } else if (kind == TEX_LUMA) {
-      float l = 0.2126f * r;
-      l += 0.7152f * g;
-      l += 0.0722f * b;
-      o[0] = o[1] = o[2] = l;
-    } else {
-      o[0] = r; o[1] = g; o[2] = b;
-    }
-    o[3] = 1.0f;
-  }
-  return S->ntex++;
-}
-
-/* Texture maps of a textured triangle's material at the hit (shaders.optix.cu:61-103,
- * material.hpp:111-155): albedo and glossy colours, and the normal-mapped shading
- * normal with the tangent frame of the world-space triangle (BVH index tri). */
-static void textured_surface(const rscene_t* S, int tri, float b1, float b2, f3* n, mat_t* m) {
-  const float* uv = &S->triUV[6 * (size_t)tri];
-  const float b0 = (1.0f - b1) - b2;
-  const float tcx = b0 * uv[0] + b1 * uv[2] + b2 * uv[4], tcy = b0 * uv[1] + b1 * uv[3] + b2 * uv[5];
-  float c[4];
-  if (m->tex[0] >= 0) {
-    oi_tex_lookup(&S->tex[m->tex[0]], tcx, tcy, c);
-    m->diffuse = F3(c[0], c[1], c[2]);
-  }
-  if (m->tex[1] >= 0) {
-    oi_tex_lookup(&S->tex[m->tex[1]], tcx, tcy, c);
-    m->specular = F3(c[0], c[1], c[2]);
-  }
-  if (m->tex[2] >= 0) {
-    const float* tv = &S->tris[12 * (size_t)tri];
-    const f3 P0 = F3(tv[0], tv[1], tv[2]), P1 = F3(tv[4], tv[5], tv[6]), P2 = F3(tv[8], tv[9], tv[10]);
-    const f3 P = add3(add3(mul3s(P0, b0), mul3s(P1, b1)), mul3s(P2, b2));
-    const f3 e1 = sub3(P1, P), e2 = sub3(P2, P);
-    const float du1 = uv[2] - tcx, dv1 = uv[3] - tcy, du2 = uv[4] - tcx, dv2 = uv[5] - tcy;
-    const float den = du1 * dv2 - du2 * dv1;
-    if (den != 0.0f) {
-      const float f = 1.0f / den;
-      const f3 T = F3(f * (dv2 * e1.x - dv1 * e2.x), f * (dv2 * e1.y - dv1 * e2.y), f * (dv2 * e1.z - dv1 * e2.z));
-      const f3 B = F3(f * (-du2 * e1.x + du1 * e2.x), f * (-du2 * e1.y + du1 * e2.y), f * (-du2 * e1.z + du1 * e2.z));
-      const int tz = T.x == 0.0f && T.y == 0.0f && T.z == 0.0f, bz = B.x == 0.0f && B.y == 0.0f && B.z == 0.0f;
-      if (!tz && !bz) {
-        oi_tex_lookup(&S->tex[m->tex[2]], tcx, tcy, c);
-        const f3 nt = F3(c[0] * 2.0f - 1.0f, c[1] * 2.0f - 1.0f, c[2] * 2.0f - 1.0f);
-        if (!(nt.x == 0.0f && nt.y == 0.0f && nt.z == 0.0f)) {
-          const f3 v = norm3(nt);
-          *n = norm3(add3(add3(mul3s(norm3(T), v.x), mul3s(norm3(neg3(B)), v.y)), mul3s(*n, v.z)));
-        }
-      }
-    }
-  }
-}
-
 /* closest: code >= 0 BVH-order triangle, -1 miss, -2 - i shape i */
 static int scene_closest(const rscene_t* S, f3 o, f3 d, float tmax, float* tOut, float* b1, float* b2) {
   float t = tmax;
@@ -1379,7 +1309,8 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
       m = &S->mats[S->triMat[prim]];
       if (S->triUV && (m->tex[0] >= 0 || m->tex[1] >= 0 || m->tex[2] >= 0)) {
         mt = *m;
-        textured_surface(S, code, hb1, hb2, &n, &mt);
+        oi_textured_surface(S->tex, mt.tex[0], mt.tex[1], mt.tex[2], &S->triUV[6 * (size_t)code],
+                            &S->tris[12 * (size_t)code], hb1, hb2, &n, &mt.diffuse, &mt.specular);
         m = &mt;
       }
     } else {
@@ -1564,14 +1495,9 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
     const orc_mesh* M = &meshes[i];
     S.mats[i] = make_mat(&M->material);
     if (M->uvs) memcpy(&S.uv[2 * (size_t)vb], M->uvs, sizeof(float) * 2 * (size_t)M->nverts);
-    /* CMaterial(aiMaterial*) (material.cu:110-143) */
-    const float* ks = M->material.specular;
-    if (M->albedo) S.mats[i].tex[0] = tex_add(&S, M->albedo, TEX_COLOR);
-    if (M->albedo && (ks[0] <= 0.02f || ks[1] <= 0.02f || ks[2] <= 0.02f)) S.mats[i].tex[1] = tex_add(&S, M->albedo, TEX_LUMA);
-    else if (M->specular) S.mats[i].tex[1] = tex_add(&S, M->specular, TEX_COLOR);
-    if (M->normal) S.mats[i].tex[2] = tex_add(&S, M->normal, TEX_COLOR);
-    if (M->alpha) S.mats[i].tex[3] = tex_add(&S, M->alpha, TEX_COLOR);
-    else if (M->albedo && M->albedo->channels == 4) S.mats[i].tex[3] = tex_add(&S, M->albedo, TEX_ALPHA);
+    /* CMaterial(aiMaterial*) (material.cu:110-143); maps without texture coordinates are unused */
+    if (M->uvs)
+      oi_material_maps(&M->material, M->albedo, M->specular, M->normal, M->alpha, S.tex, &S.ntex, S.mats[i].tex);
     for (uint32_t v = 0; v < M->nverts; ++v) {
       f3 pp = xpoint(M->model_to_world, F3(M->positions[3 * v], M->positions[3 * v + 1], M->positions[3 * v + 2]));
       f3 nn = xvec(M->model_to_world, F3(M->normals[3 * v], M->normals[3 * v + 1], M->normals[3 * v + 2]));

@@ -21,14 +21,6 @@
 extern "C" {
 #endif
 
-/* A texture map as decoded from its file: 8-bit RGBA, row 0 = top, and the
- * file's channel count. */
-typedef struct orc_texture {
-  uint32_t width, height;
-  int channels;
-  const uint8_t* rgba;
-} orc_texture;
-
 typedef struct orc_mesh {
   const float* positions; /* model space, 3 per vertex */
   uint32_t nverts;

@@ -72,6 +72,7 @@ def _load():
         "r2_filter_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, f32, P, P, P, sz]),
         "r2_filter_scene_create": (C.c_int, [P, u32, P, u32, P, P, P, P]),
         "r2_filter_scene_destroy": (C.c_int, [P]),
+        "r2_filter_scene_create_textured": (C.c_int, [P, u32, P, u32, P, P, P, P, P, P]),
         "r2_filter_scene_grid": (C.c_int, [P, f32, P]),
         "r2_filter_scene_run": (C.c_int, [P, P, P, P, P, P, P, P]),
         "r2_filter_scene_count": (C.c_int, [P, P, P, P, P]),

@@ -116,6 +116,25 @@ r2_status r2_filter_scene_create(const float* positions, uint32_t nverts, const 
   R2_API_END
 }
 
+r2_status r2_filter_scene_create_textured(const float* positions, uint32_t nverts, const uint32_t* indices,
+                                          uint32_t ntris, const float* normals, const float* uvs,
+                                          const r2_material* material, const r2_material_maps* maps,
+                                          const float* model_to_world, r2_filter_scene** out) {
+  R2_API_BEGIN
+  R2_REQUIRE(out && model_to_world && uvs && maps, R2_ERR_INVALID_ARGUMENT, "null argument");
+  r2::require_device();
+  auto sc = new r2_filter_scene;
+  try {
+    sc->impl.reset(new r2::FilterScene(positions, nverts, indices, ntris, normals, material, 1, nullptr,
+                                       model_to_world, uvs, maps));
+  } catch (...) {
+    delete sc;
+    throw;
+  }
+  *out = sc;
+  R2_API_END
+}
+
 r2_status r2_filter_scene_destroy(r2_filter_scene* scene) {
   R2_API_BEGIN
   delete scene;

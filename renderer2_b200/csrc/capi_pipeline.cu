@@ -128,9 +128,11 @@ r2_status r2_filter_run(r2_config* cfg, const char* out_root, double* stats_out)
   // CHostScene::getObjectBBs(FILTER) (scene.cu:281-310): one mesh file, its
   // submeshes merged; the last FILTER object's transform
   std::string meshPath, name;
-  std::vector<float> pos, nrm;
+  std::vector<float> pos, nrm, uvs;
   std::vector<uint32_t> idx, triMat;
   std::vector<r2_material> mats;
+  std::vector<r2_material_maps> maps;
+  bool anyUV = false;
   const r2::SceneObjectDesc* last = nullptr;
   size_t mi = 0;
   for (const r2::SceneObjectDesc& o : cfg->cfg.objects) {
@@ -144,6 +146,10 @@ r2_status r2_filter_run(r2_config* cfg, const char* out_root, double* stats_out)
         const uint32_t base = (uint32_t)(pos.size() / 3);
         pos.insert(pos.end(), s.positions.begin(), s.positions.end());
         nrm.insert(nrm.end(), s.normals.begin(), s.normals.end());
+        if (s.uvs.empty()) uvs.insert(uvs.end(), 2 * (s.positions.size() / 3), 0.0f);
+        else uvs.insert(uvs.end(), s.uvs.begin(), s.uvs.end());
+        anyUV = anyUV || !s.uvs.empty();
+        maps.push_back({s.texAlbedo.c_str(), s.texSpecular.c_str(), s.texNormal.c_str(), s.texAlpha.c_str()});
         for (uint32_t i : s.indices) idx.push_back(base + i);
         for (size_t t = 0; t < s.indices.size() / 3; ++t) triMat.push_back((uint32_t)mats.size());
         mats.push_back(s.material);
@@ -159,7 +165,8 @@ r2_status r2_filter_run(r2_config* cfg, const char* out_root, double* stats_out)
   r2::m43_to_floats(r2::m4_to_m43(object_transform(*last)), m43);
   r2::require_device();
   r2::FilterScene scene(pos.data(), (uint32_t)(pos.size() / 3), idx.data(), (uint32_t)(idx.size() / 3), nrm.data(),
-                        mats.data(), (uint32_t)mats.size(), triMat.data(), m43);
+                        mats.data(), (uint32_t)mats.size(), triMat.data(), m43, anyUV ? uvs.data() : nullptr,
+                        maps.data());
   const r2::V3 orient = r2::v3(last->orientation[0], last->orientation[1], last->orientation[2]);
   r2::FilterRunResult r =
       r2::run_filter_lods(scene, cfg->cfg.filter, orient, out_root ? out_root : "./filtering", name, nullptr);

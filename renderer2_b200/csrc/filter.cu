@@ -19,6 +19,7 @@
 //    density fit runs its iterations as warp reductions.
 #include "filter.cuh"
 #include "filter_math.h"
+#include "texture_shade.cuh"
 
 namespace r2 {
 namespace {
@@ -182,8 +183,20 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
         const float b0 = (1.0f - h.b1) - h.b2;
         V3 gn = v3(n0.x, n0.y, n0.z) * b0 + v3(n1.x, n1.y, n1.z) * h.b1 + v3(n2.x, n2.y, n2.z) * h.b2;
         gn = normalize(gn);
-        const V3 n = normalize(xform_vector(L.objModelToWorld, gn));
-        const r2_material& m = L.mats[__ldg(&L.triMat[h.tri])];
+        V3 n = normalize(xform_vector(L.objModelToWorld, gn));
+        const uint32_t mi = __ldg(&L.triMat[h.tri]);
+        const r2_material& m = L.mats[mi];
+        V3 kd = v3(m.diffuse[0], m.diffuse[1], m.diffuse[2]), ks = v3(m.specular[0], m.specular[1], m.specular[2]);
+        if (L.triUV) {  // diffuse(tc), glossy(tc) and the normal-mapped normal (mesh_filter.hpp:300-371)
+          const int4 mt = L.matTex[mi];
+          if (mt.x >= 0 || mt.y >= 0 || mt.z >= 0) {
+            const TexView tv = {L.triUV, L.texels, L.texInfo, L.bvh.tris};
+            const TexShade ts = textured_surface(tv, mt.x, mt.y, mt.z, h.tri, h.b1, h.b2, n, kd, ks);
+            n = ts.n;
+            kd = ts.diffuse;
+            ks = ts.specular;
+          }
+        }
         float bs[6];
         build_s(n, m.alpha_x, bs);
 #pragma unroll
@@ -192,11 +205,12 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
         cadd(nrm[1], n.y);
         cadd(nrm[2], n.z);
         cadd(dist, tmax);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          dif[k] += m.diffuse[k];
-          spe[k] += m.specular[k];
-        }
+        dif[0] += kd.x;
+        dif[1] += kd.y;
+        dif[2] += kd.z;
+        spe[0] += ks.x;
+        spe[1] += ks.y;
+        spe[2] += ks.z;
         rough += m.alpha_x;
         ior += m.eta_t;
         ++hits;

@@ -29,6 +29,12 @@ struct FilterLaunch {
   uint32_t* work;            // candidate voxel ids
   uint32_t* counters;        // [0] candidates, [1] queue head
   unsigned long long* ops;   // nullable: counting build, [0] rays, [1] inner nodes visited, [2] triangles tested
+  // texture maps (nullable): 3 texture coordinates per BVH-order triangle, the
+  // texels, and per material its {albedo, glossy, normal, opacity} texture (-1: none)
+  const float2* triUV;
+  const float4* texels;
+  const TexInfo* texInfo;
+  const int4* matTex;
 };
 
 // Host launchers.  `classify` writes the empty payload for voxels whose

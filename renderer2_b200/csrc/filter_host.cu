@@ -54,7 +54,8 @@ void world_aabb(V3 mlo, V3 mhi, const M43& modelToWorld, V3* wlo, V3* whi) {
 
 FilterScene::FilterScene(const float* positions, uint32_t nverts, const uint32_t* indices,
                          uint32_t ntris, const float* normals, const r2_material* materials,
-                         uint32_t nmaterials, const uint32_t* triMaterial, const float* modelToWorld) {
+                         uint32_t nmaterials, const uint32_t* triMaterial, const float* modelToWorld,
+                         const float* uvs, const r2_material_maps* maps) {
   R2_REQUIRE(positions && indices && normals && materials, R2_ERR_INVALID_ARGUMENT, "null mesh array");
   R2_REQUIRE(nverts > 0 && ntris > 0, R2_ERR_INVALID_ARGUMENT, "empty mesh");
   R2_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
@@ -102,6 +103,33 @@ FilterScene::FilterScene(const float* positions, uint32_t nverts, const uint32_t
   triN_.upload(triN.data(), triN.size(), stream_);
   triMat_.upload(triMat.data(), triMat.size(), stream_);
   mats_.upload(materials, nmaterials, stream_);
+  if (maps && uvs) {  // texture maps per material (CMaterial(aiMaterial*), material.cu:110-143)
+    std::vector<int4> mt(nmaterials);
+    bool anyTex = false, anyAlpha = false;
+    for (uint32_t m = 0; m < nmaterials; ++m) {
+      int t[4];
+      textures_.material_maps(materials[m], &maps[m], t);
+      mt[m] = make_int4(t[0], t[1], t[2], t[3]);
+      anyTex = anyTex || t[0] >= 0 || t[1] >= 0 || t[2] >= 0 || t[3] >= 0;
+      anyAlpha = anyAlpha || t[3] >= 0;
+    }
+    if (anyTex) {
+      std::vector<float2> triUV((size_t)3 * ntris);
+      std::vector<int> triAlpha(ntris);
+      for (uint32_t i = 0; i < ntris; ++i) {
+        const uint32_t p = order[i];
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t v = indices[3 * p + k];
+          triUV[3 * i + k] = make_float2(uvs[2 * v], uvs[2 * v + 1]);
+        }
+        triAlpha[i] = mt[triMat[i]].w;
+      }
+      triUV_.upload(triUV.data(), triUV.size(), stream_);
+      matTex_.upload(mt.data(), mt.size(), stream_);
+      textures_.upload(&texels_, &texInfo_, stream_);
+      if (anyAlpha) triAlpha_.upload(triAlpha.data(), triAlpha.size(), stream_);
+    }
+  }
   counters_.alloc(2);
   R2_CUDA(cudaEventCreate(&ev0_));
   R2_CUDA(cudaEventCreate(&ev1_));
@@ -157,6 +185,18 @@ void FilterScene::run(const r2_filter_grid& g, const r2_filter_params& p, uint32
   L.sigma_t = p.sigma_t;
   L.alpha = p.alpha;
   L.bvh = bvh_.view();
+  if (triUV_.get()) {
+    L.triUV = triUV_.get();
+    L.texels = texels_.get();
+    L.texInfo = texInfo_.get();
+    L.matTex = matTex_.get();
+    if (triAlpha_.get()) {  // opacity cut-outs hide triangles from the filter rays too
+      L.bvh.alpha.alphaTex = triAlpha_.get();
+      L.bvh.alpha.uv = triUV_.get();
+      L.bvh.alpha.texels = texels_.get();
+      L.bvh.alpha.texInfo = texInfo_.get();
+    }
+  }
   L.triN = triN_.get();
   L.triMat = triMat_.get();
   L.mats = mats_.get();

@@ -3,6 +3,7 @@
 // between LODs (raytracer/filter.hpp:13-44).
 #pragma once
 #include "bvh_build.cuh"
+#include "texture_host.h"
 
 namespace r2 {
 
@@ -11,9 +12,12 @@ void world_aabb(V3 mlo, V3 mhi, const M43& modelToWorld, V3* wlo, V3* whi);
 
 class FilterScene {
  public:
+  // uvs (nullable): 2 texture coordinates per vertex; maps (nullable): the
+  // texture files of each material (nmaterials entries).
   FilterScene(const float* positions, uint32_t nverts, const uint32_t* indices, uint32_t ntris,
               const float* normals, const r2_material* materials, uint32_t nmaterials,
-              const uint32_t* triMaterial, const float* modelToWorld);
+              const uint32_t* triMaterial, const float* modelToWorld, const float* uvs = nullptr,
+              const r2_material_maps* maps = nullptr);
   ~FilterScene();
   FilterScene(const FilterScene&) = delete;
   FilterScene& operator=(const FilterScene&) = delete;
@@ -44,6 +48,12 @@ class FilterScene {
   DBuf<r2_material> mats_;
   DBuf<uint32_t> work_;
   DBuf<uint32_t> counters_;
+  TextureSet textures_;
+  DBuf<float2> triUV_;
+  DBuf<int> triAlpha_;
+  DBuf<float4> texels_;
+  DBuf<TexInfo> texInfo_;
+  DBuf<int4> matTex_;
 };
 
 }  // namespace r2

@@ -122,41 +122,6 @@ RenderScene::RenderScene() {
 
 RenderScene::~RenderScene() {}
 
-int RenderScene::texture(const std::string& path, int kind) {
-  for (size_t i = 0; i < textures_.size(); ++i)
-    if (textures_[i].path == path && textures_[i].kind == kind) return (int)i;
-  const size_t dot = path.find_last_of('.');
-  std::string ext = dot == std::string::npos ? "" : path.substr(dot + 1);
-  for (char& c : ext) c = (char)tolower(c);
-  R2_REQUIRE(ext == "png", R2_ERR_UNSUPPORTED, "texture maps are read from PNG files: " + path);
-  const RgbaImage8 img = read_png(path);
-  TexHost t;
-  t.path = path;
-  t.kind = kind;
-  t.W = (int)img.width;
-  t.H = (int)img.height;
-  t.channels = img.channels;
-  t.texels.resize((size_t)t.W * t.H);
-  for (size_t i = 0; i < t.texels.size(); ++i) {
-    const uint8_t* p = &img.rgba[4 * i];
-    const float r = (float)p[0] / 255.0f, g = (float)p[1] / 255.0f, b = (float)p[2] / 255.0f;
-    if (kind == kTexAlphaChannel) {  // CTexture::loadAlpha: the alpha channel in rgb
-      const float a = (float)p[3] / 255.0f;
-      t.texels[i] = make_float4(a, a, a, 1.0f);
-    } else if (kind == kTexLuma) {  // CAssetManager::specularFromDiffuse: luma (luma.hpp:4-6)
-      float l = 0.2126f * r;
-      l += 0.7152f * g;
-      l += 0.0722f * b;
-      t.texels[i] = make_float4(l, l, l, 1.0f);
-    } else {
-      t.texels[i] = make_float4(r, g, b, 1.0f);
-    }
-  }
-  textures_.push_back(std::move(t));
-  committed_ = false;
-  return (int)textures_.size() - 1;
-}
-
 void RenderScene::add_mesh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
                            const r2_material& mat, const float* m2w, uint32_t mask, const float* uv,
                            const r2_material_maps* maps) {
@@ -169,21 +134,8 @@ void RenderScene::add_mesh(const float* pos, uint32_t nverts, const uint32_t* id
   uint32_t base = (uint32_t)(hPos_.size() / 3);
   uint32_t matId = (uint32_t)hMats_.size();
   Material hm = make_material(mat);
-  if (maps) {
-    // CMaterial(aiMaterial*) (material.cu:110-143): glossy from the albedo's luma when a
-    // specular channel is at most 0.02, else the specular map; opacity from map_d, else
-    // from the albedo's alpha channel when it has one
-    const bool hasAlbedo = maps->albedo && maps->albedo[0];
-    if (hasAlbedo) hm.tex[0] = texture(maps->albedo, kTexColor);
-    if (hasAlbedo && (mat.specular[0] <= 0.02f || mat.specular[1] <= 0.02f || mat.specular[2] <= 0.02f))
-      hm.tex[1] = texture(maps->albedo, kTexLuma);
-    else if (maps->specular && maps->specular[0])
-      hm.tex[1] = texture(maps->specular, kTexColor);
-    if (maps->normal && maps->normal[0]) hm.tex[2] = texture(maps->normal, kTexColor);
-    if (maps->alpha && maps->alpha[0]) hm.tex[3] = texture(maps->alpha, kTexColor);
-    else if (hasAlbedo && textures_[hm.tex[0]].channels == 4) hm.tex[3] = texture(maps->albedo, kTexAlphaChannel);
-    const bool anyTex = hm.tex[0] >= 0 || hm.tex[1] >= 0 || hm.tex[2] >= 0 || hm.tex[3] >= 0;
-    R2_REQUIRE(!anyTex || uv, R2_ERR_INVALID_ARGUMENT, "a textured material needs texture coordinates");
+  if (maps && uv) {  // without texture coordinates the maps are not used (shaders.optix.cu:60-61)
+    textures_.material_maps(mat, maps, hm.tex);
   }
   hMats_.push_back(hm);
   if (uv && !anyUV_) {  // earlier meshes get coordinates (0, 0)
@@ -298,21 +250,7 @@ void RenderScene::commit() {
   }
   mats_.upload(hMats_.data(), hMats_.size(), s);
   view_.mats = mats_.get();
-  if (!textures_.empty()) {
-    std::vector<TexInfo> info;
-    std::vector<float4> all;
-    for (const TexHost& t : textures_) {
-      TexInfo ti;
-      ti.offset = (uint32_t)all.size();
-      ti.W = t.W;
-      ti.H = t.H;
-      ti.pad = 0;
-      info.push_back(ti);
-      all.insert(all.end(), t.texels.begin(), t.texels.end());
-    }
-    R2_REQUIRE(all.size() < (1ull << 32), R2_ERR_UNSUPPORTED, "texture maps larger than 2^32 texels");
-    texels_.upload(all.data(), all.size(), s);
-    texInfo_.upload(info.data(), info.size(), s);
+  if (textures_.upload(&texels_, &texInfo_, s)) {
     view_.texels = texels_.get();
     view_.texInfo = texInfo_.get();
     view_.bvh.alpha.texels = view_.texels;

@@ -7,6 +7,7 @@
 
 #include "medium_host.h"
 #include "render.cuh"
+#include "texture_host.h"
 
 namespace r2 {
 
@@ -73,7 +74,7 @@ class RenderScene {
   RenderScene& operator=(const RenderScene&) = delete;
 
   // uv (nullable): 2 texture coordinates per vertex; maps (nullable): the
-  // material's texture files.
+  // material's texture files (unused without texture coordinates).
   void add_mesh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
                 const r2_material& mat, const float* modelToWorld, uint32_t mask, const float* uv = nullptr,
                 const r2_material_maps* maps = nullptr);
@@ -118,16 +119,9 @@ class RenderScene {
   static void check_params(const r2_camera& c, const r2_render_params& p, const float* d_frame);
   RenderContext ctx_;
   bool committed_ = false;
-  // Index of the texture of file `path` converted as `kind` (loaded once per scene).
-  int texture(const std::string& path, int kind);
   std::vector<float> hPos_, hNrm_, hUV_;
   bool anyUV_ = false;
-  struct TexHost {
-    std::string path;
-    int kind = 0, W = 0, H = 0, channels = 0;
-    std::vector<float4> texels;
-  };
-  std::vector<TexHost> textures_;
+  TextureSet textures_;
   DBuf<float2> triUV_;
   DBuf<int> triAlpha_;
   DBuf<float4> texels_;

@@ -64,7 +64,8 @@ def _c(a, dt):
 class FilterScene:
     """Device-resident FILTER mesh (r2_filter_scene_*)."""
 
-    def __init__(self, mesh: Mesh, mat, model_to_world=None):
+    def __init__(self, mesh: Mesh, mat, model_to_world=None, tex=None):
+        """tex (nullable): dict(uv=(nverts, 2), albedo / specular / normal / alpha = PNG paths)."""
         self.mesh = mesh
         self._pos = _c(mesh.positions, np.float32)
         self._idx = _c(mesh.indices, np.uint32)
@@ -72,8 +73,16 @@ class FilterScene:
         self._m2w = _c(N.identity43() if model_to_world is None else model_to_world, np.float32)
         self._mat = mat
         h = C.c_void_p()
-        N.check(N.lib.r2_filter_scene_create(N.ptr(self._pos), mesh.nverts, N.ptr(self._idx), mesh.ntris,
-                                             N.ptr(self._nrm), C.byref(mat), N.ptr(self._m2w), C.byref(h)))
+        if tex is None:
+            N.check(N.lib.r2_filter_scene_create(N.ptr(self._pos), mesh.nverts, N.ptr(self._idx), mesh.ntris,
+                                                 N.ptr(self._nrm), C.byref(mat), N.ptr(self._m2w), C.byref(h)))
+        else:
+            self._uv = _c(tex["uv"], np.float32)
+            maps = N.MaterialMaps(*[str(tex[k]).encode() if tex.get(k) else None
+                                    for k in ("albedo", "specular", "normal", "alpha")])
+            N.check(N.lib.r2_filter_scene_create_textured(N.ptr(self._pos), mesh.nverts, N.ptr(self._idx), mesh.ntris,
+                                                          N.ptr(self._nrm), N.ptr(self._uv), C.byref(mat),
+                                                          C.byref(maps), N.ptr(self._m2w), C.byref(h)))
         self.handle = h
 
     def close(self):

@@ -55,6 +55,9 @@ def _load():
     lib.orc_filter.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, P, P, C.c_uint32, C.c_uint64, C.c_uint64, P,
                                P, C.c_int]
     lib.orc_filter.restype = C.c_int
+    lib.orc_filter_tex.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, P, P, P, P, P, P, P, C.c_uint32, C.c_uint64,
+                                   C.c_uint64, P, P, C.c_int]
+    lib.orc_filter_tex.restype = C.c_int
     lib.orc_encode.argtypes = [P, P]
     return lib
 
@@ -128,8 +131,9 @@ def grid_from(native_grid) -> Grid:
     return g
 
 
-def filter_voxels(mesh, mat, m2w, grid, prm, v0=0, v1=None, lod=0, threads=0):
-    """Oracle filter of voxels [v0, v1): (wide float64 (n, 20), compact uint8 (n, 32))."""
+def filter_voxels(mesh, mat, m2w, grid, prm, v0=0, v1=None, lod=0, threads=0, tex=None):
+    """Oracle filter of voxels [v0, v1): (wide float64 (n, 20), compact uint8 (n, 32)).
+    tex (nullable): dict(uv=(n, 2), albedo / specular / normal / alpha = PNG path)."""
     nvox = int(np.prod(np.array(grid.num_voxels[:], np.int64)))
     v1 = nvox if v1 is None else v1
     pos = np.ascontiguousarray(mesh.positions, np.float32)
@@ -138,8 +142,18 @@ def filter_voxels(mesh, mat, m2w, grid, prm, v0=0, v1=None, lod=0, threads=0):
     m2w = np.ascontiguousarray(m2w, np.float32)
     wide = np.zeros((v1 - v0, 20), np.float64)
     comp = np.zeros((v1 - v0, 32), np.uint8)
-    r = lib.orc_filter(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), C.byref(mat), _p(m2w),
-                       C.byref(grid), C.byref(prm), lod, v0, v1, _p(wide), _p(comp), threads)
+    keep, maps, uv = [], [None] * 4, None
+    if tex is not None:
+        from renderer2_b200 import pipeline as P
+        uv = np.ascontiguousarray(tex["uv"], np.float32)
+        for k, key in enumerate(("albedo", "specular", "normal", "alpha")):
+            if tex.get(key):
+                rgba, ch = P.read_png(tex[key])
+                ot = OTexture(rgba.shape[1], rgba.shape[0], ch, rgba.ctypes.data)
+                keep += [rgba, ot]
+                maps[k] = C.byref(ot)
+    r = lib.orc_filter_tex(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), _p(uv), C.byref(mat), *maps,
+                           _p(m2w), C.byref(grid), C.byref(prm), lod, v0, v1, _p(wide), _p(comp), threads)
     assert r >= 0, f"oracle filter failed ({r})"
     return wide, comp
 

@@ -51,6 +51,17 @@ def _gpu_filter(mesh, mat, prm, vs, m2w=I43, fp16=False):
     return res
 
 
+def _gpu_filter_scene(sc, prm, vs):
+    """(grid, compact, wide) of one LOD of an existing filter scene."""
+    g = sc.grid(vs)
+    nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+    out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    wide = torch.empty(nvox * 20, dtype=torch.float32, device="cuda")
+    sc.run(g, prm, out.data_ptr(), wide.data_ptr())
+    torch.cuda.synchronize()
+    return g, out.cpu().numpy().reshape(nvox, 32), wide.cpu().numpy().reshape(nvox, 20).astype(np.float64)
+
+
 def _compare(gw, gc, ow, oc):
     # topology and hit counts: bit-exact
     assert np.array_equal(gw[:, 17], ow[:, 17]), "hit counts differ"

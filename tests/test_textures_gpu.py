@@ -161,3 +161,30 @@ def test_obj_with_texture_maps_renders_the_same_frame(tmp_path):
     sc.close()
     assert np.abs(g).sum() > 0
     assert np.array_equal(g, lin)
+
+
+def test_textured_filter_matches_oracle(tmp_path):
+    """The filter over textured leaves: diffuse(tc), glossy(tc) from the
+    albedo's luma, the normal-mapped normal, and the opacity map's holes,
+    against the FP64 oracle on the same texels."""
+    from test_filter_gpu import _compare, _gpu_filter_scene
+    maps = _maps(tmp_path)
+    leaves = scenes.foliage(3000, 6, 0.7, 8)
+    # each leaf quad (4 vertices) spans the texture once
+    q = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    uv = np.tile(q, (leaves.nverts // 4 + 1, 1))[:leaves.nverts]
+    tex = {"uv": uv, "albedo": maps["albedo"], "normal": maps["normal"], "alpha": maps["opacity"]}
+    mat = F.material(diffuse=(0.1, 0.6, 0.1), specular=(0.01, 0.3, 0.3), alpha=0.5, ior=1.5)
+    prm = F.params(samples_per_voxel=64, iterations=10)
+    vs = scenes.voxel_size_for(leaves, 16)
+    sc = F.FilterScene(leaves, mat, None, tex)
+    g, gc, gw = _gpu_filter_scene(sc, prm, vs)
+    sc.close()
+    ow, oc = O.filter_voxels(leaves, O.material_from(mat), N.identity43(), O.grid_from(g), O.params_from(prm),
+                             tex=tex)
+    _compare(gw, gc, ow, oc)
+    # the holes matter: fewer hits than the same leaves without the opacity map
+    sc2 = F.FilterScene(leaves, mat, None, {k: v for k, v in tex.items() if k != "alpha"})
+    _, _, gw2 = _gpu_filter_scene(sc2, prm, vs)
+    sc2.close()
+    assert gw[:, 17].sum() < gw2[:, 17].sum()
