@@ -476,8 +476,8 @@ def bench_volume(args, world, local):
            "roofline": roofline,
            "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms},
-           # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, shade, 3 shadow resolve, accum
-           "gpu_launches": (prm.spp // S) * (2 + 13 * prm.max_depth) * args.steps}
+           # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, events, shade, 3 shadow resolve, accum
+           "gpu_launches": (prm.spp // S) * (2 + 14 * prm.max_depth) * args.steps}
     return out, (desc, cam, prm)
 
 
@@ -561,7 +561,7 @@ def bench_volume_batch(args, world, local):
             "speedup_vs_one_at_a_time": ms_seq / ms_batch,
             "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(sum(npix) * 12), "ms_per_step": e2e_ms},
-            "gpu_launches": c["spp"] * c["scenes"] * (3 + 13 * c["depth"]) * args.steps}
+            "gpu_launches": c["spp"] * c["scenes"] * (3 + 14 * c["depth"]) * args.steps}
 
 
 def serving_jobs(seed=11):

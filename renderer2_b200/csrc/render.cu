@@ -63,6 +63,15 @@ __device__ __forceinline__ V3 xyz(float4 v) { return v3(v.x, v.y, v.z); }
 // whole launch description to local memory.
 __device__ __forceinline__ uint32_t* pick(uint32_t* const (&a)[2], uint32_t i) { return i ? a[1] : a[0]; }
 __device__ __forceinline__ uint32_t* path_queue(const RenderLaunch& L, uint32_t b) { return pick(L.st.q, b & 1u); }
+// Events of the bounce (surface hits, then medium collisions) and the path of event i.
+__device__ __forceinline__ uint32_t event_count(const RenderLaunch& L) {
+  return *(volatile uint32_t*)&L.st.counts[kHitCounters + L.bounce] +
+         *(volatile uint32_t*)&L.st.counts[kScatterCounters + L.bounce];
+}
+__device__ __forceinline__ uint32_t event_path(const RenderLaunch& L, uint32_t i) {
+  const uint32_t nh = *(volatile uint32_t*)&L.st.counts[kHitCounters + L.bounce];
+  return i < nh ? L.st.qh[i] : L.st.qs[i - nh];
+}
 
 // Closest hit over triangles, analytic shapes and (kMedia) medium boxes.
 // Code: >= 0 triangle, -1 miss, -2 - i shape i, kMediumCodeBase - m medium m.
@@ -616,7 +625,7 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
           if (kSample) {
             s.rng = rng_stream(path_pixel(L, owner), L.seed, path_sample(L, owner), L.bounce, kPurposeMedium + jm.y);
           } else {
-            const uint32_t op = path_queue(L, L.bounce)[owner >> 1];
+            const uint32_t op = event_path(L, owner >> 1);
             s.rng = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce,
                                kPurposeShadowTr + (owner & 1u), jm.y);
           }
@@ -829,11 +838,37 @@ __device__ __forceinline__ bool shade_scatter(const RenderLaunch& L, uint32_t i,
   return true;
 }
 
+// Media scenes: sorts the bounce's outcomes after the extension phase.  A miss
+// ends the path with the environment term of the first bounce (the
+// reference's miss rule, path_integrator_impl.hpp:176-182), a path ended by a
+// medium rule is dropped, surface hits and medium collisions go to their own
+// queues, so that shading runs over coherent warps of one kind of event.
+__global__ void __launch_bounds__(256) k_events(RenderLaunch L) {
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
+  const uint32_t* q = path_queue(L, L.bounce);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t nRound = (n + 31u) & ~31u;  // whole warps reach the pushes
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nRound; i += stride) {
+    int code = kEventDead;
+    uint32_t p = 0;
+    if (i < n) {
+      p = q[i];
+      code = __float_as_int(L.st.hit[p].w);
+      if (code == -1 && L.bounce == 0) {
+        const V3 le = env_le_nc(L.scene.env, xyz(L.st.rayD[p])).Le;
+        L.st.L[p] = f4(xyz(L.st.L[p]) + le * xyz(L.st.T[p]), 0.0f);
+      }
+    }
+    push_queue(L.st.qs, &L.st.counts[kScatterCounters + L.bounce], code == kEventScatter, p);
+    push_queue(L.st.qh, &L.st.counts[kHitCounters + L.bounce], code != -1 && code != kEventDead && code != kEventScatter,
+               p);
+  }
+}
+
 template <bool kMedia>
 __global__ void __launch_bounds__(128, kMedia ? 4 : 5) k_shade(RenderLaunch L) {
-  // scenes without media shade the bounce's surface hits (k_extend ended the misses)
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[kMedia ? L.bounce : kHitCounters + L.bounce];
-  const uint32_t* q = kMedia ? path_queue(L, L.bounce) : L.st.qh;
+  // the bounce's events: misses and ended paths were finished by k_extend / k_events
+  const uint32_t n = event_count(L);
   uint32_t* qn = path_queue(L, L.bounce + 1);
   uint32_t* cn = &L.st.counts[L.bounce + 1];
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -843,7 +878,7 @@ __global__ void __launch_bounds__(128, kMedia ? 4 : 5) k_shade(RenderLaunch L) {
     bool cont = false;
     uint32_t p = 0;
     if (i < n) {
-      p = q[i];
+      p = event_path(L, i);
       const float4 hr = L.st.hit[p];
       const int code = __float_as_int(hr.w);
       const float4 ro = L.st.rayO[p];
@@ -869,7 +904,7 @@ __global__ void __launch_bounds__(128, kMedia ? 4 : 5) k_shade(RenderLaunch L) {
 
 // Visibility of every shadow record of a scene without media.
 __global__ void __launch_bounds__(128) k_shadow_surfaces(RenderLaunch L) {
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[kHitCounters + L.bounce];
+  const uint32_t n = event_count(L);
   uint32_t traced = 0;
   if (!L.scene.hasTris) {
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -958,7 +993,7 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
   const V3 p1 = o + d * x.x;
   RngStream rs;
   if (kInline) {
-    const uint32_t op = path_queue(L, L.bounce)[slot >> 1];
+    const uint32_t op = event_path(L, slot >> 1);
     rs = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce, kPurposeShadowTr + (slot & 1u), idx);
   }
   int err = 0;
@@ -1003,7 +1038,7 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
 template <bool kFirst, bool kInline>
 __global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int round) {
   uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce + kShadowCounters;
-  const uint32_t n = kFirst ? 2 * *(volatile uint32_t*)&L.st.counts[L.bounce] : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
+  const uint32_t n = kFirst ? 2 * event_count(L) : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
   const uint32_t* list = kFirst ? nullptr : pick(L.st.sl, (uint32_t)(round - 1));
   uint32_t* jobs = &mc[3 * round];
   const uint32_t stride = gridDim.x * blockDim.x;
@@ -1023,18 +1058,17 @@ __global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int roun
     }
     shadow_walk<kInline>(L, slot, kFirst, jobs);
   }
-  if (kFirst && L.stats && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&L.stats[0], (unsigned long long)(n / 2));
+  if (kFirst && L.stats && blockIdx.x == 0 && threadIdx.x == 0)
+    atomicAdd(&L.stats[0], (unsigned long long)L.st.counts[L.bounce]);
 }
 
 __global__ void __launch_bounds__(256) k_accum(RenderLaunch L) {
-  const bool hitsOnly = L.scene.nmedia == 0;  // shadow records of the hit queue
-  const uint32_t n = *(volatile uint32_t*)&L.st.counts[hitsOnly ? kHitCounters + L.bounce : L.bounce];
-  const uint32_t* q = hitsOnly ? L.st.qh : path_queue(L, L.bounce);
+  const uint32_t n = event_count(L);  // the shadow records of the bounce's events
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const float4 o0 = L.st.shO[2 * i], o1 = L.st.shO[2 * i + 1];
     if (!(o0.w > 0.0f) && !(o1.w > 0.0f)) continue;
-    const uint32_t p = q[i];
+    const uint32_t p = event_path(L, i);
     V3 dl = v3(0.0f);
     if (o0.w > 0.0f) dl = dl + (xyz(L.st.shPre[2 * i]) * L.st.shTr[2 * i]) / o0.w;
     if (o1.w > 0.0f) dl = dl + (xyz(L.st.shPre[2 * i + 1]) * L.st.shTr[2 * i + 1]) / o1.w;
@@ -1130,6 +1164,7 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
       }
       if (L.dda) k_collide<true><<<nblocks * 2, 128, 0, s>>>(L);
       else k_collide<false><<<nblocks * 2, 128, 0, s>>>(L);
+      k_events<<<nblocks, 256, 0, s>>>(L);
       mark(1);
       k_shade<true><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);

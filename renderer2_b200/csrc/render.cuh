@@ -45,7 +45,8 @@ struct PathState {
   float4* hit;      // t, b1, b2, event code (int bits: >= 0 triangle, -1 miss, -2 - i shape i,
                     // kEventScatter medium collision, kEventDead path ended by a medium rule)
   uint32_t* q[2];   // ping-pong queues of live path ids
-  uint32_t* qh;     // scenes without media: paths of the bounce that hit a surface (k_extend)
+  uint32_t* qh;     // paths of the bounce that hit a surface (k_extend, or k_events with media)
+  uint32_t* qs;     // media: paths of the bounce with a medium collision (k_events)
   uint32_t* counts; // [bounce] live path count entering the bounce; from kTravCounters on,
                     // per bounce the rays taken by the persistent surface traversals
   // shadow records, two per queue slot (0: light sample, 1: BSDF sample)
@@ -81,10 +82,13 @@ constexpr uint32_t kDefaultWavePaths = 1u << 22;  // paths per wave a frame's sa
 
 // PathState::counts layout: [0, 64) live paths per bounce, then two counters
 // per bounce (extension rays taken, shadow records taken), then the surface
-// hits per bounce (scenes without media).
+// hits and the medium collisions per bounce.  Shading, shadow records and
+// accumulation run over the bounce's events: item i < hits is qh[i], the
+// others qs[i - hits].
 constexpr int kTravCounters = 64;
 constexpr int kHitCounters = kTravCounters + 2 * 64;
-constexpr int kCountsSize = kHitCounters + 64;
+constexpr int kScatterCounters = kHitCounters + 64;
+constexpr int kCountsSize = kScatterCounters + 64;
 
 constexpr int kEventScatter = -2147483647;  // INT_MIN + 1
 constexpr int kEventDead = -2147483646;     // INT_MIN + 2

@@ -304,7 +304,7 @@ void RenderContext::ensure(uint32_t n, bool media) {
   if (n > cap_) {
     rayO_.alloc(n); rayD_.alloc(n); T_.alloc(n); L_.alloc(n); hit_.alloc(n);
     shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
-    q0_.alloc(n); q1_.alloc(n); qh_.alloc(n); shTr_.alloc(2 * (size_t)n);
+    q0_.alloc(n); q1_.alloc(n); qh_.alloc(n); qs_.alloc(n); shTr_.alloc(2 * (size_t)n);
     counts_.alloc(kCountsSize);
     cap_ = n;
   }
@@ -322,8 +322,8 @@ void RenderContext::ensure(uint32_t n, bool media) {
 
 size_t RenderContext::bytes_for(uint32_t n, bool media) {
   n = capacity_for(n);
-  // per path: 5 float4 state + 3 x 2 float4 records + float4 throughput + 3 queue ids + 2 transmittances
-  size_t b = (size_t)n * (5 * 16 + 6 * 16 + 16 + 12 + 8) + kCountsSize * 4;
+  // per path: 5 float4 state + 3 x 2 float4 records + float4 throughput + 4 queue ids + 2 transmittances
+  size_t b = (size_t)n * (5 * 16 + 6 * 16 + 16 + 16 + 8) + kCountsSize * 4;
   // media: records (4 float4 + float2), shadow tmax/medium, round queues and walk state
   if (media) b += (size_t)n * (16 + 48 + 8 + 16 + 16 + 64 + 16 + 32 + 16) + 16 * 64 * 4;
   return b + (size_t)n * 12;  // frame
@@ -331,7 +331,7 @@ size_t RenderContext::bytes_for(uint32_t n, bool media) {
 
 void RenderContext::fill(PathState* st) const {
   st->rayO = rayO_.get(); st->rayD = rayD_.get(); st->T = T_.get(); st->L = L_.get(); st->hit = hit_.get();
-  st->q[0] = q0_.get(); st->q[1] = q1_.get(); st->qh = qh_.get(); st->counts = counts_.get();
+  st->q[0] = q0_.get(); st->q[1] = q1_.get(); st->qh = qh_.get(); st->qs = qs_.get(); st->counts = counts_.get();
   st->shO = shO_.get(); st->shD = shD_.get(); st->shPre = shPre_.get(); st->shT = shT_.get();
   st->shTr = shTr_.get();
   if (mediaCap_ > 0) {

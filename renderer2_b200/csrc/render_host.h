@@ -56,7 +56,7 @@ class RenderContext {
  private:
   uint32_t cap_ = 0, mediaCap_ = 0;
   DBuf<float4> rayO_, rayD_, T_, L_, hit_, shO_, shD_, shPre_, shT_;
-  DBuf<uint32_t> q0_, q1_, qh_, counts_;
+  DBuf<uint32_t> q0_, q1_, qh_, qs_, counts_;
   DBuf<float> shTr_;
   DBuf<float2> shX_, evD_;
   DBuf<float4> evA_, evB_, evC_;
