@@ -425,6 +425,48 @@ r2_status r2_obj_info(const char* directory, const char* filename, uint32_t* n_s
                       uint32_t* n_triangles, r2_material* first_material);
 
 /* ------------------------------------------------------------------------ */
+/* Screen-space LOD selection for many-instance scenes: the forest generator's
+ * selectLOD (raytracer/src/filtering/generate_random_forest.py:179-225, with
+ * project 73-80, projectLOD 82-101, outsideFrustum 103-105, gamma 132-133,
+ * intersectBB 135-151, approximateNumVoxels2 153-177), one GPU thread per
+ * tree, in double precision like the generator's numpy.
+ *
+ * Per tree: if all 8 projected corners of the model's coarsest LOD lie outside
+ * the frustum the coarsest LOD is chosen; otherwise the convex hull area of
+ * the projected corners gives the covered pixels, and the LODs of voxel size
+ * >= min_lod are walked in the order given (the generator's sorted(lods):
+ * the volume description's keys in string order); each one whose estimated
+ * visible voxel count times covered_pixels exceeds the covered pixels
+ * becomes the choice, the first that does not ends the walk.  The choice -1
+ * means the mesh itself (the generator's "0"). */
+typedef struct r2_lod_camera {
+  double world_to_view[16];    /* row-major 4x4 (common_functions.py lookAt) */
+  double pos[3];
+  double near_plane_distance;  /* sensor_width * pixel_size / (2 tan(fov / 2)) */
+  double pixel_size;           /* 1e-5 in the generator */
+  double pixel_area;           /* pixel_size ** 2 as the host computes it */
+  double sensor_width, sensor_height;
+  double far_scale;            /* intersectBB's far-distance factor 1 + 2 gamma(3) */
+} r2_lod_camera;
+
+/* One LOD of a model: an entry of volume_description.json. */
+typedef struct r2_lod_volume {
+  double voxel_size;     /* the entry's key as a number */
+  double bb_min[3], bb_max[3];
+  double num_voxels[3];
+  double corners[8][3];  /* P0..P7 */
+} r2_lod_volume;
+
+/* lods: all models' LODs, model m's at [model_first[m], model_first[m] +
+ * model_count[m]) in walk order; trees: position (3 doubles), uniform
+ * scaling, model index.  lod_out (ntrees): index into lods, or -1 for the
+ * mesh.  Host buffers; the selection runs on the current device. */
+r2_status r2_select_lods(const r2_lod_camera* camera, const r2_lod_volume* lods, const uint32_t* model_first,
+                         const uint32_t* model_count, uint32_t nmodels, const double* tree_pos,
+                         const double* tree_scaling, const uint32_t* tree_model, uint32_t ntrees, double min_lod,
+                         double covered_pixels, int32_t* lod_out);
+
+/* ------------------------------------------------------------------------ */
 /* Serving: a request loop that overlaps jobs on the device (continuous
  * batching).  This has no counterpart in the reference, which renders one
  * frame at a time (raytracer/pipeline.cu:24-90).

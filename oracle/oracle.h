@@ -110,6 +110,31 @@ int orc_filter_tex(const float* positions, uint32_t nverts, const uint32_t* idx,
 /* Encode a wide (double) record to the 32-byte payload (FP64 arithmetic). */
 void orc_encode(const double* wide, uint8_t* out32);
 
+/* Screen-space LOD selection of the forest generator, selectLOD
+ * (raytracer/src/filtering/generate_random_forest.py:179-225), one tree after
+ * the other in double precision (forest_oracle.c).  The two structs have the
+ * layouts of the library's r2_lod_camera and r2_lod_volume. */
+typedef struct orc_lod_camera {
+  double world_to_view[16];
+  double pos[3];
+  double near_plane_distance, pixel_size, pixel_area;
+  double sensor_width, sensor_height;
+  double far_scale;
+} orc_lod_camera;
+typedef struct orc_lod_volume {
+  double voxel_size;
+  double bb_min[3], bb_max[3];
+  double num_voxels[3];
+  double corners[8][3];
+} orc_lod_volume;
+/* lod_out: index into lods or -1 (the mesh); also the inputs of the decision
+ * per tree when diag is non-null: 3 doubles (covered pixels, -1 when all
+ * corners are outside; the coarsest LOD's projected hull area; 0). */
+int orc_select_lods(const orc_lod_camera* cam, const orc_lod_volume* lods, const uint32_t* model_first,
+                    const uint32_t* model_count, uint32_t nmodels, const double* tree_pos, const double* tree_scaling,
+                    const uint32_t* tree_model, uint32_t ntrees, double min_lod, double covered_pixels,
+                    int32_t* lod_out, double* diag);
+
 #ifdef __cplusplus
 }
 #endif

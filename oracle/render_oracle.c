@@ -493,6 +493,8 @@ typedef struct {
   float hgG;
   oi_nvdb g;
   oi_bricks b;
+  float vsF;  /* voxel size of the filtering, from the path */
+  int owner;  /* 1: g and b belong to this entry (the first instance of its path) */
 } med_t;
 
 typedef struct {
@@ -972,11 +974,29 @@ static int voxel_size_from_path(const char* path, float* out) {
   return 0;
 }
 
+/* Placement of one instance: T(pos) R(orientation) S(scaling), the world box
+   from the model box's two corners, the filter/render voxel ratio
+   (sceneobject.cu:50-65, 108-114; aabb.hpp:9-13). */
+static void med_place(med_t* m, const orc_medium* om) {
+  m4_t T = oi_m4_id(), Sc = oi_m4_id();
+  for (int k = 0; k < 3; ++k) { T.m[3][k] = om->pos[k]; Sc.m[k][k] = om->scaling[k]; }
+  const m4_t m2w = oi_m4_mul(oi_m4_mul(T, rot_from_normal(F3(om->orientation[0], om->orientation[1], om->orientation[2]))), Sc);
+  oi_m4_to43(m2w, m->m2w);
+  oi_m4_to43(oi_m4_inv(m2w), m->w2m);
+  const f3 bmin = F3((float)m->g.worldBBox[0], (float)m->g.worldBBox[1], (float)m->g.worldBBox[2]);
+  const f3 bmax = F3((float)m->g.worldBBox[3], (float)m->g.worldBBox[4], (float)m->g.worldBBox[5]);
+  const f3 a = xpoint(m->m2w, bmin), b = xpoint(m->m2w, bmax);
+  m->bbMin = F3(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z);
+  m->bbMax = F3(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z);
+  m->ratio = m->vsF / ((m->bbMax.x - m->bbMin.x) / (float)m->size[0]);
+}
+
 static int med_load(med_t* m, const orc_medium* om) {
   memset(m, 0, sizeof(*m));
   char buf[4096];
   float vsF;
   if (voxel_size_from_path(om->path, &vsF)) return -1;
+  m->vsF = vsF;
   snprintf(buf, sizeof(buf), "%s.nvdb", om->path);
   if (oi_nvdb_read(buf, &m->g)) return -2;
   snprintf(buf, sizeof(buf), "%s.brickgrid", om->path);
@@ -1004,20 +1024,12 @@ static int med_load(med_t* m, const orc_medium* om) {
   m->sigmaS = F3(om->sigma_s[0], om->sigma_s[1], om->sigma_s[2]);
   m->sigmaT = fmaxf(om->sigma_a[0] + om->sigma_s[0], fmaxf(om->sigma_a[1] + om->sigma_s[1], om->sigma_a[2] + om->sigma_s[2]));
   m->invMax = 1.0f / oi_nvdb_max_density(&m->g);
-  m4_t T = oi_m4_id(), Sc = oi_m4_id();
-  for (int k = 0; k < 3; ++k) { T.m[3][k] = om->pos[k]; Sc.m[k][k] = om->scaling[k]; }
-  const m4_t m2w = oi_m4_mul(oi_m4_mul(T, rot_from_normal(F3(om->orientation[0], om->orientation[1], om->orientation[2]))), Sc);
-  oi_m4_to43(m2w, m->m2w);
-  oi_m4_to43(oi_m4_inv(m2w), m->w2m);
-  const f3 bmin = F3((float)m->g.worldBBox[0], (float)m->g.worldBBox[1], (float)m->g.worldBBox[2]);
-  const f3 bmax = F3((float)m->g.worldBBox[3], (float)m->g.worldBBox[4], (float)m->g.worldBBox[5]);
-  const f3 a = xpoint(m->m2w, bmin), b = xpoint(m->m2w, bmax);
-  m->bbMin = F3(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z);
-  m->bbMax = F3(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z);
-  m->ratio = vsF / ((m->bbMax.x - m->bbMin.x) / (float)m->size[0]);
+  m->owner = 1;
+  med_place(m, om);
   return 0;
 }
 static void med_free(med_t* m) {
+  if (!m->owner) return;
   oi_nvdb_free(&m->g);
   oi_bricks_free(&m->b);
 }
@@ -1470,6 +1482,16 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   if (nmedia > 0) {
     meds = (med_t*)calloc(nmedia, sizeof(med_t));
     for (uint32_t i = 0; i < nmedia; ++i) {
+      /* one load per path; later instances of the path share its grid and
+         its coefficients (CAssetManager::loadMedium, asset_manager.cu:114-137) */
+      uint32_t j = 0;
+      while (j < i && strcmp(media[j].path, media[i].path) != 0) ++j;
+      if (j < i) {
+        meds[i] = meds[j];
+        meds[i].owner = 0;
+        med_place(&meds[i], &media[i]);
+        continue;
+      }
       if (med_load(&meds[i], &media[i]) != 0) {
         for (uint32_t k = 0; k < i; ++k) med_free(&meds[k]);
         free(meds);

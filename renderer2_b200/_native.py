@@ -56,6 +56,15 @@ class FilterGrid(C.Structure):
                 ("world_bb_max", C.c_float * 3), ("voxel_size", C.c_float)]
 
 
+# r2_lod_camera and r2_lod_volume (screen-space LOD selection)
+LOD_CAMERA_DTYPE = np.dtype([("world_to_view", "<f8", 16), ("pos", "<f8", 3), ("near_plane_distance", "<f8"),
+                             ("pixel_size", "<f8"), ("pixel_area", "<f8"), ("sensor_width", "<f8"),
+                             ("sensor_height", "<f8"), ("far_scale", "<f8")])
+LOD_VOLUME_DTYPE = np.dtype([("voxel_size", "<f8"), ("bb_min", "<f8", 3), ("bb_max", "<f8", 3),
+                             ("num_voxels", "<f8", 3), ("corners", "<f8", (8, 3))])
+assert LOD_CAMERA_DTYPE.itemsize == 200 and LOD_VOLUME_DTYPE.itemsize == 272
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"native library missing: {LIB_PATH} (run __graft_entry__.build())")
@@ -115,6 +124,7 @@ def _load():
         "r2_read_hdr": (C.c_int, [C.c_char_p, P, sz, P, P]),
         "r2_write_hdr": (C.c_int, [C.c_char_p, P, u32, u32]),
         "r2_obj_info": (C.c_int, [C.c_char_p, C.c_char_p, P, P, P, P]),
+        "r2_select_lods": (C.c_int, [P, P, P, P, u32, P, P, P, u32, C.c_double, C.c_double, P]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(lib, name)

@@ -28,23 +28,9 @@ __device__ __forceinline__ float ord2f(uint32_t o) {
   return __uint_as_float(b);
 }
 
-__global__ void k_tri_bounds(const float* __restrict__ pos, const uint32_t* __restrict__ idx,
-                             uint32_t n, float4* __restrict__ lo, float4* __restrict__ hi,
-                             uint32_t* __restrict__ cbounds /* 6 ordered words */) {
-  V3 cmin = v3(INFINITY), cmax = v3(-INFINITY);
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    uint32_t i0 = idx[3 * t], i1 = idx[3 * t + 1], i2 = idx[3 * t + 2];
-    V3 a = v3(pos[3 * i0], pos[3 * i0 + 1], pos[3 * i0 + 2]);
-    V3 b = v3(pos[3 * i1], pos[3 * i1 + 1], pos[3 * i1 + 2]);
-    V3 c = v3(pos[3 * i2], pos[3 * i2 + 1], pos[3 * i2 + 2]);
-    V3 l = vmin(vmin(a, b), c), h = vmax(vmax(a, b), c);
-    lo[t] = make_float4(l.x, l.y, l.z, 0.0f);
-    hi[t] = make_float4(h.x, h.y, h.z, 0.0f);
-    V3 cen = (l + h) * 0.5f;
-    cmin = vmin(cmin, cen);
-    cmax = vmax(cmax, cen);
-  }
-  // warp then block reduction of the centroid bounds
+// Block reduction of the threads' centroid bounds into cbounds (6 ordered
+// words: min xyz, -max xyz), one atomicMin per word and block.
+__device__ void reduce_centroid_bounds(V3 cmin, V3 cmax, uint32_t* __restrict__ cbounds) {
   float v[6] = {cmin.x, cmin.y, cmin.z, -cmax.x, -cmax.y, -cmax.z};
 #pragma unroll
   for (int k = 0; k < 6; ++k) {
@@ -66,6 +52,37 @@ __global__ void k_tri_bounds(const float* __restrict__ pos, const uint32_t* __re
       if (lane == 0) atomicMin(&cbounds[k], f2ord(x));
     }
   }
+}
+
+__global__ void k_tri_bounds(const float* __restrict__ pos, const uint32_t* __restrict__ idx,
+                             uint32_t n, float4* __restrict__ lo, float4* __restrict__ hi,
+                             uint32_t* __restrict__ cbounds /* 6 ordered words */) {
+  V3 cmin = v3(INFINITY), cmax = v3(-INFINITY);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    uint32_t i0 = idx[3 * t], i1 = idx[3 * t + 1], i2 = idx[3 * t + 2];
+    V3 a = v3(pos[3 * i0], pos[3 * i0 + 1], pos[3 * i0 + 2]);
+    V3 b = v3(pos[3 * i1], pos[3 * i1 + 1], pos[3 * i1 + 2]);
+    V3 c = v3(pos[3 * i2], pos[3 * i2 + 1], pos[3 * i2 + 2]);
+    V3 l = vmin(vmin(a, b), c), h = vmax(vmax(a, b), c);
+    lo[t] = make_float4(l.x, l.y, l.z, 0.0f);
+    hi[t] = make_float4(h.x, h.y, h.z, 0.0f);
+    V3 cen = (l + h) * 0.5f;
+    cmin = vmin(cmin, cen);
+    cmax = vmax(cmax, cen);
+  }
+  reduce_centroid_bounds(cmin, cmax, cbounds);
+}
+
+__global__ void k_box_bounds(const float4* __restrict__ lo, const float4* __restrict__ hi, uint32_t n,
+                             uint32_t* __restrict__ cbounds) {
+  V3 cmin = v3(INFINITY), cmax = v3(-INFINITY);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const float4 l = lo[t], h = hi[t];
+    const V3 cen = (v3(l.x, l.y, l.z) + v3(h.x, h.y, h.z)) * 0.5f;
+    cmin = vmin(cmin, cen);
+    cmax = vmax(cmax, cen);
+  }
+  reduce_centroid_bounds(cmin, cmax, cbounds);
 }
 
 __device__ __forceinline__ uint64_t expand21(uint32_t v) {
@@ -278,20 +295,15 @@ __global__ void k_init_bounds(uint32_t* cb) {
 
 }  // namespace
 
-void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out,
-               cudaStream_t s) {
-  R2_REQUIRE(ntris > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero triangles");
-  R2_REQUIRE(ntris < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 triangles");
+// Steps 3-7 over primitive boxes whose centroid bounds are in cb; with
+// d_pos/d_idx the BVH-ordered triangle array is gathered too.
+static void build_from_boxes(const float4* triLo, const float4* triHi, const uint32_t* cbw, uint32_t ntris,
+                             const float* d_pos, const uint32_t* d_idx, DeviceBvh* out, cudaStream_t s) {
   const int n = (int)ntris;
-  DBuf<float4> triLo(n), triHi(n);
-  DBuf<uint32_t> cb(6);
-  k_init_bounds<<<1, 32, 0, s>>>(cb.get());
-  int nb = (int)std::min<uint32_t>((ntris + 255) / 256, (uint32_t)sm_count() * 8);
-  k_tri_bounds<<<nb, 256, 0, s>>>(d_pos, d_idx, ntris, triLo.get(), triHi.get(), cb.get());
   DBuf<uint64_t> keys(n), keysSorted(n);
   DBuf<uint32_t> vals(n);
   out->order.alloc(n);
-  k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo.get(), triHi.get(), ntris, cb.get(), keys.get(),
+  k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo, triHi, ntris, cbw, keys.get(),
                                            vals.get());
   size_t tempBytes = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys.get(), keysSorted.get(), vals.get(),
@@ -300,14 +312,16 @@ void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, Device
   R2_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), tempBytes, keys.get(), keysSorted.get(),
                                           vals.get(), out->order.get(), n, 0, 63, s));
   out->ntris = ntris;
-  out->tris.alloc((size_t)3 * n);
-  k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_pos, d_idx, out->order.get(), ntris,
-                                                out->tris.get());
+  if (d_pos) {
+    out->tris.alloc((size_t)3 * n);
+    k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_pos, d_idx, out->order.get(), ntris,
+                                                  out->tris.get());
+  }
   if (n == 1) {
     out->nodes.alloc(1);
     out->nnodes = 1;
     out->height = 1;
-    k_single_leaf<<<1, 1, 0, s>>>(triLo.get(), triHi.get(), out->nodes.get());
+    k_single_leaf<<<1, 1, 0, s>>>(triLo, triHi, out->nodes.get());
     R2_CUDA(cudaGetLastError());
     R2_CUDA(cudaStreamSynchronize(s));
     return;
@@ -323,7 +337,7 @@ void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, Device
   DBuf<float> nodeCost(ni);
   DBuf<int> nodeHeight(ni), collapse(ni), flags(ni);
   R2_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int) * ni, s));
-  k_bottom_up<<<(n + 255) / 256, 256, 0, s>>>(n, out->order.get(), triLo.get(), triHi.get(), left.get(),
+  k_bottom_up<<<(n + 255) / 256, 256, 0, s>>>(n, out->order.get(), triLo, triHi, left.get(),
                                               right.get(), first.get(), last.get(), nodeParent.get(),
                                               leafParent.get(), leafLo.get(), leafHi.get(), nodeLo.get(),
                                               nodeHi.get(), nodeCost.get(), nodeHeight.get(),
@@ -342,6 +356,28 @@ void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, Device
   out->height = rootCollapse ? 1 : (uint32_t)rootHeight;
   R2_REQUIRE(out->height <= R2_BVH_STACK, R2_ERR_UNSUPPORTED,
              "BVH deeper than the traversal stack (" + std::to_string(out->height) + " levels)");
+}
+
+void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out,
+               cudaStream_t s) {
+  R2_REQUIRE(ntris > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero triangles");
+  R2_REQUIRE(ntris < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 triangles");
+  DBuf<float4> triLo(ntris), triHi(ntris);
+  DBuf<uint32_t> cb(6);
+  k_init_bounds<<<1, 32, 0, s>>>(cb.get());
+  int nb = (int)std::min<uint32_t>((ntris + 255) / 256, (uint32_t)sm_count() * 8);
+  k_tri_bounds<<<nb, 256, 0, s>>>(d_pos, d_idx, ntris, triLo.get(), triHi.get(), cb.get());
+  build_from_boxes(triLo.get(), triHi.get(), cb.get(), ntris, d_pos, d_idx, out, s);
+}
+
+void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s) {
+  R2_REQUIRE(nboxes > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero boxes");
+  R2_REQUIRE(nboxes < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 boxes");
+  DBuf<uint32_t> cb(6);
+  k_init_bounds<<<1, 32, 0, s>>>(cb.get());
+  int nb = (int)std::min<uint32_t>((nboxes + 255) / 256, (uint32_t)sm_count() * 8);
+  k_box_bounds<<<nb, 256, 0, s>>>(d_lo, d_hi, nboxes, cb.get());
+  build_from_boxes(d_lo, d_hi, cb.get(), nboxes, nullptr, nullptr, out, s);
 }
 
 }  // namespace r2

@@ -34,4 +34,9 @@ struct DeviceBvh {
 void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out,
                cudaStream_t stream);
 
+// The same hierarchy over boxes (d_lo/d_hi: one float4 per box, xyz used,
+// device): leaves reference BVH positions, order[] maps them to box indices;
+// no triangle array.
+void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t stream);
+
 }  // namespace r2

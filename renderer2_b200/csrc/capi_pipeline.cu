@@ -4,6 +4,7 @@
 // and the asset files of the pipeline.
 #include <string.h>
 
+#include <map>
 #include <memory>
 #include <string>
 
@@ -18,8 +19,9 @@
 struct r2_config {
   r2::PipelineConfig cfg;
   r2::RgbImage env;
-  // per Mesh object (in scene order): its OBJ submeshes
-  std::vector<std::vector<r2::ObjSubmesh>> meshes;
+  // per Mesh object (in scene order): its OBJ submeshes, each file read once
+  // (CAssetManager::loadMesh caches by path, asset_manager.cu:86-112)
+  std::vector<std::shared_ptr<const std::vector<r2::ObjSubmesh>>> meshes;
   std::unique_ptr<r2::RenderScene> scene;  // built at the first render, then resident
   r2::DBuf<float> frame;
   r2::DBuf<uint8_t> bytes;
@@ -50,7 +52,7 @@ void build_scene(r2_config* c) {
       case r2::SceneObjectDesc::kMesh: {
         float m43[12];
         r2::m43_to_floats(r2::m4_to_m43(object_transform(o)), m43);
-        for (const r2::ObjSubmesh& s : c->meshes[mi]) {
+        for (const r2::ObjSubmesh& s : *c->meshes[mi]) {
           const r2_material_maps maps = {s.texAlbedo.c_str(), s.texSpecular.c_str(), s.texNormal.c_str(),
                                          s.texAlpha.c_str()};
           sc->add_mesh(s.positions.data(), (uint32_t)(s.positions.size() / 3), s.indices.data(),
@@ -77,8 +79,13 @@ r2_status r2_config_load(const char* config_json_path, r2_config** out) {
   std::unique_ptr<r2_config> c(new r2_config());
   c->cfg = r2::load_config(config_json_path);
   c->env = r2::read_hdr(c->cfg.envmap);
-  for (const r2::SceneObjectDesc& o : c->cfg.objects)
-    if (o.kind == r2::SceneObjectDesc::kMesh) c->meshes.push_back(r2::load_obj(o.directory, o.filename));
+  std::map<std::string, std::shared_ptr<const std::vector<r2::ObjSubmesh>>> loaded;
+  for (const r2::SceneObjectDesc& o : c->cfg.objects) {
+    if (o.kind != r2::SceneObjectDesc::kMesh) continue;
+    auto& m = loaded[o.directory + "\n" + o.filename];
+    if (!m) m = std::make_shared<const std::vector<r2::ObjSubmesh>>(r2::load_obj(o.directory, o.filename));
+    c->meshes.push_back(m);
+  }
   *out = c.release();
   R2_API_END
 }
@@ -109,7 +116,7 @@ r2_status r2_config_info_get(const r2_config* cfg, r2_config_info* out) {
   for (const r2::SceneObjectDesc& o : c.objects) {
     if (o.kind == r2::SceneObjectDesc::kMedium) ++out->n_media;
     else if (o.kind == r2::SceneObjectDesc::kMesh) {
-      for (const r2::ObjSubmesh& s : cfg->meshes[mi]) {
+      for (const r2::ObjSubmesh& s : *cfg->meshes[mi]) {
         ++out->n_meshes;
         out->n_triangles += (uint32_t)(s.indices.size() / 3);
       }
@@ -142,7 +149,7 @@ r2_status r2_filter_run(r2_config* cfg, const char* out_root, double* stats_out)
       const std::string p = o.directory + "/" + o.filename;
       if (meshPath.empty()) meshPath = p;
       R2_REQUIRE(p == meshPath, R2_ERR_INVALID_CONFIG, "Filtering only available for single mesh");
-      for (const r2::ObjSubmesh& s : cfg->meshes[mi]) {
+      for (const r2::ObjSubmesh& s : *cfg->meshes[mi]) {
         const uint32_t base = (uint32_t)(pos.size() / 3);
         pos.insert(pos.end(), s.positions.begin(), s.positions.end());
         nrm.insert(nrm.end(), s.normals.begin(), s.normals.end());

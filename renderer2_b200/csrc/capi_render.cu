@@ -1,7 +1,9 @@
 // C ABI: path tracer scene and frame entry points.
+#include <algorithm>
 #include <memory>
 
 #include "capi_util.h"
+#include "lod_select.h"
 #include "render_host.h"
 
 struct r2_scene {
@@ -192,6 +194,25 @@ r2_status r2_render_batch_run(r2_render_batch* batch, void* stream, double* ms_o
     const uint32_t b = batch->impl->bound_hits(s);
     R2_REQUIRE(b == 0, R2_ERR_DEVICE_TIMEOUT, std::to_string(b) + " paths or shadow rays ended by a loop bound");
   }
+  R2_API_END
+}
+
+r2_status r2_select_lods(const r2_lod_camera* camera, const r2_lod_volume* lods, const uint32_t* model_first,
+                         const uint32_t* model_count, uint32_t nmodels, const double* tree_pos,
+                         const double* tree_scaling, const uint32_t* tree_model, uint32_t ntrees, double min_lod,
+                         double covered_pixels, int32_t* lod_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(camera && (nmodels == 0 || (lods && model_first && model_count)), R2_ERR_INVALID_ARGUMENT,
+             "null argument");
+  R2_REQUIRE(ntrees == 0 || (tree_pos && tree_scaling && tree_model && lod_out), R2_ERR_INVALID_ARGUMENT,
+             "null argument");
+  if (ntrees == 0) return R2_OK;
+  r2::require_device();
+  uint64_t nlods = 0;
+  for (uint32_t m = 0; m < nmodels; ++m) nlods = std::max<uint64_t>(nlods, (uint64_t)model_first[m] + model_count[m]);
+  R2_REQUIRE(nlods < (1ull << 31), R2_ERR_INVALID_ARGUMENT, "LOD table too large");
+  r2::select_lods(*camera, lods, (uint32_t)nlods, model_first, model_count, nmodels, tree_pos, tree_scaling,
+                  tree_model, ntrees, min_lod, covered_pixels, lod_out, nullptr);
   R2_API_END
 }
 

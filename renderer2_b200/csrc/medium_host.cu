@@ -27,7 +27,7 @@ float voxel_size_from_path(const std::string& path) {
 static M4 affine(const M4& a) { return m43_to_m4(m4_to_m43(a)); }
 
 std::unique_ptr<MediumHost> load_medium(const std::string& path, const float sigmaA[3], const float sigmaS[3],
-                                        V3 pos, V3 orientation, V3 scaling, bool hg, float hgG) {
+                                        bool hg, float hgG) {
   std::unique_ptr<MediumHost> mh(new MediumHost());
   MediumView& v = mh->view;
   memset(&v, 0, sizeof(v));
@@ -107,17 +107,9 @@ std::unique_ptr<MediumHost> load_medium(const std::string& path, const float sig
                       g.begin() + (ptrdiff_t)(offs[0] + offs.size() * sizeof(nvdb::LeafNode)));
   }
   v.invMaxDensity = 1.0f / maxDensity;
-  // scene object: T R S, world box from the model box's two corners (aabb.hpp:9-13)
-  const M4 m2w = model_to_world_transform(pos, orientation, scaling);
-  v.modelToWorld = m4_to_m43(m2w);
-  v.worldToModel = m4_to_m43(m4_inverse(m2w));
-  const V3 bmin = v3((float)G->worldBBox[0], (float)G->worldBBox[1], (float)G->worldBBox[2]);
-  const V3 bmax = v3((float)G->worldBBox[3], (float)G->worldBBox[4], (float)G->worldBBox[5]);
-  const V3 a = xform_point(v.modelToWorld, bmin), b = xform_point(v.modelToWorld, bmax);
-  v.aabbMin = v3(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z);
-  v.aabbMax = v3(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z);
-  const float voxelSizeRendering = (v.aabbMax.x - v.aabbMin.x) / (float)v.size[0];
-  v.filterRenderRatio = voxel_size_from_path(path) / voxelSizeRendering;
+  mh->boxMin = v3((float)G->worldBBox[0], (float)G->worldBBox[1], (float)G->worldBBox[2]);
+  mh->boxMax = v3((float)G->worldBBox[3], (float)G->worldBBox[4], (float)G->worldBBox[5]);
+  mh->voxelSizeFiltering = voxel_size_from_path(path);
   // brick grid
   mh->bricks = read_brick_grid(path + ".brickgrid");
   for (int k = 0; k < 3; ++k) {
@@ -125,6 +117,20 @@ std::unique_ptr<MediumHost> load_medium(const std::string& path, const float sig
     v.ad[k] = (int)mh->bricks.atlasDim[k];
   }
   return mh;
+}
+
+MediumView place_medium(const MediumHost& mh, V3 pos, V3 orientation, V3 scaling) {
+  MediumView v = mh.view;
+  // T R S, world box from the model box's two corners (aabb.hpp:9-13)
+  const M4 m2w = model_to_world_transform(pos, orientation, scaling);
+  v.modelToWorld = m4_to_m43(m2w);
+  v.worldToModel = m4_to_m43(m4_inverse(m2w));
+  const V3 a = xform_point(v.modelToWorld, mh.boxMin), b = xform_point(v.modelToWorld, mh.boxMax);
+  v.aabbMin = v3(a.x < b.x ? a.x : b.x, a.y < b.y ? a.y : b.y, a.z < b.z ? a.z : b.z);
+  v.aabbMax = v3(a.x > b.x ? a.x : b.x, a.y > b.y ? a.y : b.y, a.z > b.z ? a.z : b.z);
+  const float voxelSizeRendering = (v.aabbMax.x - v.aabbMin.x) / (float)v.size[0];
+  v.filterRenderRatio = mh.voxelSizeFiltering / voxelSizeRendering;
+  return v;
 }
 
 void MediumHost::upload(cudaStream_t s) {
@@ -140,6 +146,7 @@ void MediumHost::upload(cudaStream_t s) {
   view.range = dRange.get();
   for (int i = 0; i < 3; ++i) view.mips[i] = dMips[i].get();
   view.atlas = dAtlas.get();
+  uploaded = true;
 }
 
 size_t MediumHost::device_bytes() const {

@@ -73,6 +73,97 @@ __device__ __forceinline__ uint32_t event_path(const RenderLaunch& L, uint32_t i
   return i < nh ? L.st.qh[i] : L.st.qs[i - nh];
 }
 
+// Entry distance of a ray into a BVH node's child box, or INFINITY when the
+// ray misses it: the slab arithmetic and comparisons of medium_box_hit, so
+// with the builder's boxes padded around the instances' boxes an instance
+// the ray hits is never culled and its distance is >= the entry returned here.
+__device__ __forceinline__ float media_box_enter(float lx, float hx, float ly, float hy, float lz, float hz, V3 o,
+                                                 V3 inv) {
+  float t0 = 0.0f, t1 = kDefaultTmax;
+  const float lo[3] = {lx, ly, lz}, hi[3] = {hx, hy, hz};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    float a = (lo[i] - comp(o, i)) * comp(inv, i);
+    float b = (hi[i] - comp(o, i)) * comp(inv, i);
+    if (a > b) {
+      const float t = a;
+      a = b;
+      b = t;
+    }
+    if (a > t0) t0 = a;
+    if (b < t1) t1 = b;
+  }
+  return t0 > t1 ? INFINITY : t0;
+}
+
+// First medium-box boundary along a ray: the smallest medium_box_hit in
+// [0, limit] over the instances, the lowest instance index among equal
+// distances (what a loop over the instances in order with a strict `<`
+// keeps).  Returns the instance (-1: none) and its distance in *tOut.
+__device__ __forceinline__ int media_first(const SceneView& S, V3 o, V3 d, float limit, float* tOut) {
+  float best = INFINITY;
+  int bestM = -1;
+  if (S.mediaNodes == nullptr) {
+    for (int m = 0; m < S.nmedia; ++m) {
+      const float tm = medium_box_hit(S.media[m], o, d);
+      if (tm >= 0.0f && tm <= limit && tm < best) {
+        best = tm;
+        bestM = m;
+      }
+    }
+    *tOut = best;
+    return bestM;
+  }
+  const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  int stack[R2_BVH_STACK];
+  float stackT[R2_BVH_STACK];
+  int sp = 0;
+  int ref = 0;  // the root node
+  float refT = 0.0f;
+  for (;;) {
+    if (refT <= best && refT <= limit) {
+      if (ref < 0) {
+        const int first = bvh_leaf_first(ref), count = bvh_leaf_count(ref);
+        for (int k = 0; k < count; ++k) {
+          const int m = (int)__ldg(&S.mediaOrder[first + k]);
+          const float tm = medium_box_hit(S.media[m], o, d);
+          if (tm >= 0.0f && tm <= limit && (tm < best || (tm == best && m < bestM))) {
+            best = tm;
+            bestM = m;
+          }
+        }
+      } else {
+        const BvhNode* nd = S.mediaNodes + ref;
+        const float4 b0 = __ldg(&nd->b0), b1 = __ldg(&nd->b1), bz = __ldg(&nd->bz);
+        const int4 ch = __ldg(&nd->ch);
+        const float t0 = media_box_enter(b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, o, inv);
+        const float t1 = ch.y == R2_BVH_NONE ? INFINITY : media_box_enter(b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, o, inv);
+        const bool h0 = t0 <= best && t0 <= limit, h1 = t1 <= best && t1 <= limit;
+        if (h0 && h1) {
+          const bool near0 = t0 <= t1;
+          stack[sp] = near0 ? ch.y : ch.x;
+          stackT[sp] = near0 ? t1 : t0;
+          ++sp;
+          ref = near0 ? ch.x : ch.y;
+          refT = near0 ? t0 : t1;
+          continue;
+        }
+        if (h0 || h1) {
+          ref = h0 ? ch.x : ch.y;
+          refT = h0 ? t0 : t1;
+          continue;
+        }
+      }
+    }
+    if (sp == 0) break;
+    --sp;
+    ref = stack[sp];
+    refT = stackT[sp];
+  }
+  *tOut = best;
+  return bestM;
+}
+
 // Closest hit over triangles, analytic shapes and (kMedia) medium boxes.
 // Code: >= 0 triangle, -1 miss, -2 - i shape i, kMediumCodeBase - m medium m.
 // scene_closest_after finishes the query from the triangles' result h.
@@ -121,14 +212,13 @@ __device__ __forceinline__ float4 scene_closest_after(const SceneView& S, V3 o, 
       code = -2 - i;
     }
   }
-  if (kMedia) {
-    for (int m = 0; m < S.nmedia; ++m) {
-      const float tm = medium_box_hit(S.media[m], o, d);
-      if (tm >= 0.0f && tm <= tmax && tm < t) {
-        t = tm;
-        b1 = b2 = 0.0f;
-        code = kMediumCodeBase - m;
-      }
+  if (kMedia && S.nmedia > 0) {
+    float tm;
+    const int m = media_first(S, o, d, tmax, &tm);
+    if (m >= 0 && tm < t) {
+      t = tm;
+      b1 = b2 = 0.0f;
+      code = kMediumCodeBase - m;
     }
   }
   return make_float4(t, b1, b2, __int_as_float(code));
@@ -1001,15 +1091,9 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
     const V3 off = offset_ray_origin(p0, normalize(p1 - p0));
     const float tl = length(p1 - off);
     const V3 dir = (p1 - p0) / tl;
-    float best = tl;
-    int hitM = -1;
-    for (int m = 0; m < S.nmedia; ++m) {
-      const float tm = medium_box_hit(S.media[m], off, dir);
-      if (tm >= 0.0f && tm <= tl && tm < best) {
-        best = tm;
-        hitM = m;
-      }
-    }
+    float best;
+    int hitM = media_first(S, off, dir, tl, &best);
+    if (hitM >= 0 && !(best < tl)) hitM = -1;
     if (hitM < 0) {
       L.st.shTr[slot] = tr;
       if (err) atomicAdd(L.bound, 1u);

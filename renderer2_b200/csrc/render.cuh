@@ -30,6 +30,8 @@ struct SceneView {
   int hasTris;
   const MediumView* media;  // medium instances (device array), nullable
   int nmedia;
+  const BvhNode* mediaNodes;    // BVH over the instances' world boxes (more than kMediaLinearMax), nullable
+  const uint32_t* mediaOrder;   // BVH leaf position -> instance index
   EnvMap env;
   const float2* triUV;      // 3 texture coordinates per BVH-order triangle, nullable
   const float4* texels;     // texture maps of the materials (TexInfo offsets), nullable
@@ -89,6 +91,11 @@ constexpr int kTravCounters = 64;
 constexpr int kHitCounters = kTravCounters + 2 * 64;
 constexpr int kScatterCounters = kHitCounters + 64;
 constexpr int kCountsSize = kScatterCounters + 64;
+
+// Scenes with at most this many medium instances test every box along a ray;
+// larger ones walk the instance BVH (same result either way).
+constexpr int kMediaLinearMax = 8;
+constexpr size_t kMaxMediumInstances = size_t(1) << 22;
 
 constexpr int kEventScatter = -2147483647;  // INT_MIN + 1
 constexpr int kEventDead = -2147483646;     // INT_MIN + 2

@@ -187,12 +187,14 @@ void RenderScene::set_envmap(const float* rgb, int W, int H) {
 void RenderScene::add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
                              const float* orientation, const float* scaling, uint32_t mask, bool hg, float g) {
   R2_REQUIRE(path && sigmaA && sigmaS && pos && orientation && scaling, R2_ERR_INVALID_ARGUMENT, "null medium argument");
-  R2_REQUIRE(media_.size() < 4096, R2_ERR_UNSUPPORTED, "too many media in one scene");
-  std::unique_ptr<MediumHost> m = load_medium(path, sigmaA, sigmaS, v3(pos[0], pos[1], pos[2]),
-                                              v3(orientation[0], orientation[1], orientation[2]),
-                                              v3(scaling[0], scaling[1], scaling[2]), hg, g);
+  R2_REQUIRE(media_.size() < kMaxMediumInstances, R2_ERR_UNSUPPORTED, "too many media in one scene");
+  auto it = mediaByPath_.find(path);
+  if (it == mediaByPath_.end())
+    it = mediaByPath_.emplace(std::string(path), load_medium(path, sigmaA, sigmaS, hg, g)).first;
   if (mask == 0) return;  // render rays (mask 255) never see objects with mask NONE
-  media_.push_back(std::move(m));
+  media_.push_back(MediumInstance{it->second.get(), v3(pos[0], pos[1], pos[2]),
+                                  v3(orientation[0], orientation[1], orientation[2]),
+                                  v3(scaling[0], scaling[1], scaling[2])});
   committed_ = false;
 }
 
@@ -261,11 +263,29 @@ void RenderScene::commit() {
   view_.nshapes = (int)hShapes_.size();
   if (!media_.empty()) {
     std::vector<MediumView> mv;
-    for (auto& m : media_) {
-      m->upload(s);
-      mv.push_back(m->view);
+    mv.reserve(media_.size());
+    for (const MediumInstance& m : media_) {
+      if (!m.medium->uploaded) m.medium->upload(s);
+      mv.push_back(place_medium(*m.medium, m.pos, m.orientation, m.scaling));
     }
     mediaViews_.upload(mv.data(), mv.size(), s);
+    if (mv.size() > (size_t)kMediaLinearMax) {
+      // instance BVH over the world boxes, padded so that rounding in the
+      // node tests never culls a box that a ray hits
+      std::vector<float4> lo(mv.size()), hi(mv.size());
+      for (size_t i = 0; i < mv.size(); ++i) {
+        const V3 a = mv[i].aabbMin, b = mv[i].aabbMax;
+        auto pad = [](float x) { return 1e-5f * (fabsf(x) + 1.0f); };
+        lo[i] = make_float4(a.x - pad(a.x), a.y - pad(a.y), a.z - pad(a.z), 0.0f);
+        hi[i] = make_float4(b.x + pad(b.x), b.y + pad(b.y), b.z + pad(b.z), 0.0f);
+      }
+      DBuf<float4> dlo, dhi;
+      dlo.upload(lo.data(), lo.size(), s);
+      dhi.upload(hi.data(), hi.size(), s);
+      build_box_bvh(dlo.get(), dhi.get(), (uint32_t)mv.size(), &mediaBvh_, s);
+      view_.mediaNodes = mediaBvh_.nodes.get();
+      view_.mediaOrder = mediaBvh_.order.get();
+    }
   }
   view_.media = mediaViews_.get();
   view_.nmedia = (int)media_.size();

@@ -2,6 +2,8 @@
 // space, analytic shapes, media, environment map with the reference's
 // distributions), camera setup, per-render state and the per-sample wave loop.
 #pragma once
+#include <map>
+#include <string>
 #include <memory>
 #include <vector>
 
@@ -129,8 +131,16 @@ class RenderScene {
   std::vector<uint32_t> hIdx_, hTriMat_;
   std::vector<Material> hMats_;
   std::vector<Shape> hShapes_;
-  std::vector<std::unique_ptr<MediumHost>> media_;
+  // media loaded once per path (the first load's coefficients, like
+  // CAssetManager::loadMedium, asset_manager.cu:114-137) and their instances
+  struct MediumInstance {
+    MediumHost* medium;
+    V3 pos, orientation, scaling;
+  };
+  std::map<std::string, std::unique_ptr<MediumHost>> mediaByPath_;
+  std::vector<MediumInstance> media_;
   DBuf<MediumView> mediaViews_;
+  DeviceBvh mediaBvh_;
   EnvHost env_;
   DeviceBvh bvh_;
   DBuf<float4> triN_;

@@ -1,9 +1,14 @@
 """Seeded synthetic render scenes of the benchmark configurations."""
 from __future__ import annotations
 
+import json
+import os
+
 import numpy as np
 
 from . import filter as F
+from . import forest as FO
+from . import pipeline as P
 from . import raytracer as R
 from . import scenes
 
@@ -101,3 +106,113 @@ def build_scene(desc) -> R.Scene:
     sc.set_envmap(desc["env"])
     sc.commit()
     return sc
+
+
+# ---------------------------------------------------------------- forests
+
+# (name, size class, expected height, seed) of the synthetic tree library
+TREE_SPECS = (("FA01", "Large", 20.0, 11), ("FB02", "Medium", 8.0, 12), ("FC03", "Small", 2.5, 13))
+# the forest generator's camera (generate_random_forest.py:257): pos, look-at, up, fov
+FOREST_CAMERA = ((-680.0, 35.1, 680.0), (-675.0, 31.5, 675.0), (0.0, 1.0, 0.0), 90.0)
+FOREST_SIGMA_A = (0.0, 0.0, 0.0)
+FOREST_SIGMA_S = (10.0, 10.0, 10.0)  # the generator's media (toFile, common_functions.py:88-89)
+
+
+def tree_mesh(seed: int, n_quads: int) -> F.Mesh:
+    """A slender synthetic tree: foliage quads squeezed to 0.3 x 1 x 0.3."""
+    m = scenes.foliage(n_quads, 8, 0.7, seed)
+    sc = np.array([0.3, 1.0, 0.3], np.float32)
+    nrm = m.normals / sc
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    return F.Mesh((m.positions * sc).astype(np.float32), m.indices, nrm.astype(np.float32))
+
+
+def forest_library(work_dir, n_quads: int = 20_000, grid: int = 64, lods: int = 4, filter_spv: int = 32,
+                   filter_iters: int = 10) -> dict:
+    """Synthetic tree models for forest scenes: per TREE_SPECS entry a tree
+    mesh written as an OBJ asset and filtered on the GPU into `lods` LODs
+    (finest: grid voxels along the height), with the volume description the
+    filter writes.  Returns {relevant_models, volume_descriptions, assets_root,
+    filtering_root, meshes}."""
+    work_dir = str(work_dir)
+    filtering_root = os.path.join(work_dir, "filtering")
+    assets_root = os.path.join(work_dir, "assets")
+    relevant = {"Large": [], "Medium": [], "Small": []}
+    meshes = {}
+    mat = F.material(diffuse=(0.15, 0.55, 0.1), specular=(0.05, 0.05, 0.05), alpha=0.45, ior=1.5)
+    for name, group, height, seed in TREE_SPECS:
+        mesh = tree_mesh(seed, n_quads)
+        prm = F.params(samples_per_voxel=filter_spv, iterations=filter_iters,
+                       min_voxel_size=scenes.voxel_size_for(mesh, grid), lods=lods)
+        F.run_filtering(mesh, mat, prm, filtering_root, name)
+        P.write_obj(os.path.join(assets_root, "Synthetic", name), name,
+                    [(mesh, (0.15, 0.55, 0.1), (0.05, 0.05, 0.05), 8.0, 1.5)])
+        ext = mesh.positions.max(axis=0) - mesh.positions.min(axis=0)
+        relevant[group].append({"Name": name, "Path": f"Synthetic/{name}", "Dimensions": [float(x) for x in ext],
+                                "ExpectedHeight": height, "Orientation": [0.0, 1.0, 0.0]})
+        meshes[name] = mesh
+    with open(os.path.join(filtering_root, "volume_description.json")) as f:
+        volumes = json.load(f)
+    return {"relevant_models": relevant, "volume_descriptions": volumes, "assets_root": assets_root,
+            "filtering_root": filtering_root, "meshes": meshes}
+
+
+def forest_trees(lib: dict, attempts: int, radius: float, width: int, height: int, min_lod: float = 0.0,
+                 covered_pixels: float = 1.0, camera=FOREST_CAMERA, seed: int = 0) -> list:
+    """The generator's scene list for a forest of the library's trees: dart
+    throwing in a disc of `radius`, LODs chosen on the GPU for a width x height
+    sensor at `camera`."""
+    pos, look, up, fov = camera
+    cam = FO.lod_camera(pos, look, up, width, height, fov)
+    return FO.generate_forest(lib["relevant_models"], lib["volume_descriptions"], cam, False, min_lod,
+                              covered_pixels, attempts, seed, radius, assets_root=lib["assets_root"] + "/",
+                              filtering_root=lib["filtering_root"] + "/")
+
+
+def forest_ground():
+    """The generator's ground disc (toFile, common_functions.py:92-104)."""
+    m = F.material(diffuse=(0.07, 0.07, 0.01), specular=(0.9, 0.9, 0.9), alpha=0.99, ior=1.2,
+                   diffuse_roughness=0.999)
+    m.eta_i = 1.00029
+    return (R.CIRCLE, (0.0, 0.0, 0.0), 3.402823466e+38, (0.0, 1.0, 0.0), m)
+
+
+def forest_desc(lib: dict, trees: list, env_seed: int = 3, media_only: bool = False) -> dict:
+    """Scene description of a forest scene list: a medium instance per
+    medium tree (files shared by path), the tree mesh per mesh tree (or, with
+    media_only, its finest LOD instead), the ground disc and a lognormal
+    environment."""
+    mat = F.material(diffuse=(0.15, 0.55, 0.1), specular=(0.05, 0.05, 0.05), alpha=0.45, ior=1.5)
+    finest = {name: sorted(lods, key=float)[0] for name, lods in lib["volume_descriptions"].items()}
+    desc = {"meshes": [], "media": [], "shapes": [forest_ground()], "env": lognormal_env(512, 256, 1.5, env_seed)}
+    for kind, directory, filename, pos, ori, scl in trees:
+        assert tuple(ori) == (0.0, 1.0, 0.0), "synthetic trees stand upright"
+        if kind == "Mesh":
+            name = filename[:-4]
+            if media_only:
+                kind, directory, filename = "Medium", lib["filtering_root"] + "/" + name + "/", \
+                    "filtered_mesh_" + finest[name]
+            else:
+                m2w = np.zeros(12, np.float32)
+                m2w[0], m2w[4], m2w[8] = scl
+                m2w[9:12] = pos
+                desc["meshes"].append((lib["meshes"][name], mat, m2w))
+                continue
+        desc["media"].append((directory + "/" + filename, FOREST_SIGMA_A, FOREST_SIGMA_S, tuple(pos), tuple(ori),
+                              tuple(scl)))
+    return desc
+
+
+def forest_config(lib: dict, trees: list, work_dir, width: int, height: int, samples: int,
+                  camera=FOREST_CAMERA) -> str:
+    """config.json + scenedescription.json (the generator's object format) and
+    the environment map for a forest scene list; returns the config path."""
+    work_dir = str(work_dir)
+    env = os.path.join(work_dir, "forest_env.hdr")
+    P.write_hdr(env, lognormal_env(512, 256, 1.5, 3))
+    sd = os.path.join(work_dir, "scenedescription_forest.json")
+    cfg = os.path.join(work_dir, "config_forest.json")
+    pos, look, up, fov = camera
+    P.write_config(cfg, FO.scene_objects(trees), env, sd, width, height, samples, fov=fov, cam_pos=pos,
+                   look_at=look, up=up, use_brick_grid=True)
+    return cfg

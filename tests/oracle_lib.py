@@ -274,3 +274,26 @@ def tonemap(linear, gamma):
     by = np.zeros(lin.shape, np.uint8)
     lib.orc_tonemap(lin.ctypes.data, lin.shape[1], lin.shape[0], float(gamma), out.ctypes.data, by.ctypes.data)
     return out, by
+
+
+lib.orc_select_lods.restype = C.c_int
+lib.orc_select_lods.argtypes = [C.c_void_p] * 4 + [C.c_uint32] + [C.c_void_p] * 3 + [C.c_uint32, C.c_double,
+                                                                                      C.c_double, C.c_void_p,
+                                                                                      C.c_void_p]
+
+
+def select_lods(cam_rec, lods, first, count, tree_pos, tree_scaling, tree_model, min_lod, covered_pixels,
+                want_diag=False):
+    """selectLOD per tree (orc_select_lods): LOD index or -1; with want_diag
+    also (covered pixels, hull area, 0) per tree."""
+    pos = np.ascontiguousarray(np.asarray(tree_pos, np.float64).reshape(-1, 3))
+    sc = np.ascontiguousarray(np.asarray(tree_scaling, np.float64).reshape(-1))
+    mdl = np.ascontiguousarray(np.asarray(tree_model, np.uint32).reshape(-1))
+    first = np.ascontiguousarray(first, np.uint32)
+    count = np.ascontiguousarray(count, np.uint32)
+    out = np.zeros(len(sc), np.int32)
+    diag = np.zeros((len(sc), 3)) if want_diag else None
+    rc = lib.orc_select_lods(_p(cam_rec), _p(lods), _p(first), _p(count), len(first), _p(pos), _p(sc), _p(mdl),
+                             len(sc), float(min_lod), float(covered_pixels), _p(out), _p(diag))
+    assert rc == 0
+    return (out, diag) if want_diag else out
