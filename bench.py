@@ -58,6 +58,10 @@ VOLUME_CFG = dict(grid=256, n_quads=200_000, ico_subdiv=6, width=1920, height=10
 VOLUME_BATCH_CFG = dict(scenes=16, grids=(128, 192, 256, 160), quads=(50_000, 150_000, 300_000), ico=(6, 7),
                         width=1920, height=1080, spp=2, depth=16)
 SERVE_CFG = dict(jobs=60, rate=40.0, slots=2, budget=40 << 30)
+# forest leg: the forest generator's disc (radius 1000, 100,000 placement attempts) of three synthetic tree
+# models, each filtered into 4 LODs; LODs chosen on the GPU for the generator's camera at 1920x1080
+FOREST_CFG = dict(n_quads=20_000, grid=64, lods=4, attempts=100_000, radius=1000.0, width=1920, height=1080,
+                  spp=4, depth=16, min_lod=0.0, covered_pixels=1.0, seed=0)
 
 
 def _peaks():
@@ -481,6 +485,105 @@ def bench_volume(args, world, local):
     return out, (desc, cam, prm)
 
 
+def bench_forest(args, world, local):
+    """Forest leg: a many-instance scene as the reference's forest generator
+    makes it (dart-throwing placement, screen-space LOD per tree; the trees
+    nearest the camera stay meshes), medium instances sharing their files and
+    walked through the instance BVH, 1920x1080, depth 16, brick-grid DDA.
+    Also times the LOD selection of all trees (r2_select_lods) against the
+    oracle's restatement on the host cores."""
+    import tempfile
+
+    import oracle_lib as O
+    import torch
+    from renderer2_b200 import forest as FO
+    from renderer2_b200 import raytracer as R
+    from renderer2_b200 import render_scenes as RS
+    c = FOREST_CFG
+    work = tempfile.mkdtemp(prefix="r2forest")
+    lib = RS.forest_library(work, n_quads=c["n_quads"], grid=c["grid"], lods=c["lods"])
+    t0 = time.perf_counter()
+    placed = FO.place_trees(lib["relevant_models"], lib["volume_descriptions"], c["attempts"], c["seed"], c["radius"])
+    place_s = time.perf_counter() - t0
+    pos, look, up, fov = RS.FOREST_CAMERA
+    lcam = FO.lod_camera(pos, look, up, c["width"], c["height"], fov)
+    table = FO.LodTable(lib["volume_descriptions"], sorted(lib["volume_descriptions"]))
+    tp = np.array([p["Pos"] for p in placed])
+    ts = np.array([p["Scaling"] for p in placed])
+    tm = np.array([table.index[p["Model"]["Name"]] for p in placed], np.uint32)
+    sel_ms = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        choice = FO.select_lods(lcam, table, tp, ts, tm, c["min_lod"], c["covered_pixels"])
+        sel_ms.append((time.perf_counter() - t0) * 1e3)
+    t0 = time.perf_counter()
+    n_cpu = min(len(placed), 20_000)
+    ref = O.select_lods(lcam["native"], table.lods, table.first, table.count, tp[:n_cpu], ts[:n_cpu], tm[:n_cpu],
+                        c["min_lod"], c["covered_pixels"])
+    cpu_s = time.perf_counter() - t0
+    assert np.array_equal(ref, choice[:n_cpu]), "LOD selection differs from the oracle"
+    trees = RS.forest_trees(lib, c["attempts"], c["radius"], c["width"], c["height"], c["min_lod"],
+                            c["covered_pixels"], placed=placed)
+    desc = RS.forest_desc(lib, trees)
+    t0 = time.perf_counter()
+    sc = RS.build_scene(desc)
+    build_ms = (time.perf_counter() - t0) * 1e3
+    cam = R.camera(c["width"], c["height"], fov, pos, look, up)
+    prm = R.params(c["spp"], c["depth"], c["seed"], brick_grid=True)
+    tuning = sc.autotune(cam, prm).as_dict()
+    npix = cam.width * cam.height
+    frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup):
+        sc.render_device(cam, prm, frame.data_ptr(), stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    st = np.zeros(8)
+    stats = []
+    ev0.record()
+    for _ in range(args.steps):
+        # wave state (~1 GB at 1080p) exceeds L2; no flush needed
+        sc.render_device(cam, prm, frame.data_ptr(), stream, stats=st)
+        stats.append(st.copy())
+    ev1.record()
+    torch.cuda.synchronize()
+    _barrier(world)
+    total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
+    S = sc.wave_samples(cam, prm)
+    sc.close()
+    st = np.mean(np.array(stats), axis=0)
+    paths = npix * prm.spp
+    kinds = [t[0] for t in trees]
+    lods = {}
+    for t in trees:
+        if t[0] == "Medium":
+            lods[t[2]] = lods.get(t[2], 0) + 1
+    return {"metric": "paths/s", "value": world * paths * args.steps / (total_ms / 1e3), "unit": "paths/s",
+            "ms_per_step": total_ms / args.steps,
+            "config": {"workload": f"forest: {kinds.count('Medium')} medium instances of {len(table.models)} tree "
+                                   f"models x {c['lods']} LODs (finest {c['grid']} voxels tall) + "
+                                   f"{kinds.count('Mesh')} mesh trees ({2 * c['n_quads']} tris each), disc radius "
+                                   f"{c['radius']:g}, {c['width']}x{c['height']}, {c['spp']} spp per step, "
+                                   f"depth {c['depth']}",
+                       "trees": len(trees), "medium_instances": kinds.count("Medium"),
+                       "mesh_trees": kinds.count("Mesh"), "lods": dict(sorted(lods.items())),
+                       "paths_per_step": paths, "segments_per_step": st[2], "shadow_rays_per_step": st[3],
+                       "kernel_ms_per_step": {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]},
+                       "l2": "wave state larger than L2", "tuning": tuning},
+            "lod_selection": {"trees": len(placed), "ms": float(np.median(sel_ms)),
+                              "trees_per_s": len(placed) / (float(np.median(sel_ms)) / 1e3),
+                              "timed": "r2_select_lods with host buffers (upload, kernel, download)",
+                              "cpu_baseline": {"value": n_cpu / cpu_s, "unit": "trees/s", "cores": 1,
+                                               "kind": "port", "sample": f"{n_cpu} trees"},
+                              "placement_s": place_s, "placement_attempts": c["attempts"]},
+            "scene_build_ms": build_ms,
+            # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, events, shade, 3 shadow resolve,
+            # accum
+            "gpu_launches": (prm.spp // S) * (2 + 14 * prm.max_depth) * args.steps}
+
+
 def bench_volume_batch(args, world, local):
     """Batched volume leg: VOLUME_BATCH_CFG['scenes'] scenes (foliage grids of uneven size and
     occupancy filtered on the GPU, icosphere meshes of 82k or 328k triangles), 1920x1080, depth 16,
@@ -724,6 +827,7 @@ def run_native(args):
     f = bench_filter(args, world, local) if not args.skip_filter else None
     vol = bench_volume(args, world, local) if not args.skip_volume else None
     vbatch = bench_volume_batch(args, world, local) if not args.skip_volume else None
+    forest = bench_forest(args, world, local) if not args.skip_volume else None
     serve = bench_serving(args) if (not args.skip_serving and world == 1) else None
     if rank == 0:
         cpu = cpu_render_sample(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
@@ -753,6 +857,9 @@ def run_native(args):
         if vbatch is not None:
             line["volume_batch"] = vbatch
             line["gpu_launches"] += vbatch["gpu_launches"]
+        if forest is not None:
+            line["forest"] = forest
+            line["gpu_launches"] += forest["gpu_launches"]
         if serve is not None:
             line["serving"] = serve
         print(json.dumps(line), flush=True)
@@ -837,6 +944,9 @@ def run_case(args):
         import renderer2_b200  # noqa: F401
         args.steps, args.warmup = 1, 1
         print(json.dumps(bench_volume_batch(args, 1, 0)))
+    elif args.case == "forest":
+        args.steps, args.warmup = 1, 1
+        print(json.dumps(bench_forest(args, 1, 0)))
     elif args.case in ("volume-small", "volume-mid"):
         import tempfile
 
@@ -871,7 +981,8 @@ def main():
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
     ap.add_argument("--case", default=None,
-                    help="profiling case: render-wave | filter-small | volume-small | volume-mid | volume-batch | serving")
+                    help="profiling case: render-wave | filter-small | volume-small | volume-mid | volume-batch | forest | "
+                         "serving")
     ap.add_argument("--case-spp", type=int, default=1, help="render-wave: samples per pixel, all in one wave")
     args = ap.parse_args()
     if args.case:

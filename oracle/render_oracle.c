@@ -415,9 +415,9 @@ static f3 env_le(const env_t* e, f3 d, float* pdf) {
 #define EV_SCATTER (-2147483647)
 #define EV_DEAD (-2147483646)
 #define MAX_TRACKING_STEPS (1 << 20)
-#define MAX_PASS_THROUGH 64
-#define MAX_SHADOW_SEGMENTS 256
-#define PURPOSE_MEDIUM 0x10u
+#define MAX_PASS_THROUGH 4096
+#define MAX_SHADOW_SEGMENTS 4096
+#define PURPOSE_MEDIUM 0x1000u
 #define PURPOSE_SCATTER 0x100u
 #define PURPOSE_SHADOW_TR 0x200u
 

@@ -31,11 +31,11 @@ namespace r2 {
 namespace {
 
 constexpr uint32_t kPurposeCamera = 0xCA3E7Au;
-constexpr uint32_t kPurposeMedium = 0x10u;     // + pass-through index within the bounce
+constexpr uint32_t kPurposeMedium = 0x1000u;   // + pass-through index within the bounce
 constexpr uint32_t kPurposeScatter = 0x100u;   // phase-function and light draws at a collision
 constexpr uint32_t kPurposeShadowTr = 0x200u;  // + shadow slot (0 light, 1 BSDF)
-constexpr int kMaxPassThrough = 64;            // medium boundaries crossed within one bounce
-constexpr int kMaxShadowSegments = 256;        // medium boundaries along one shadow ray (per round)
+constexpr int kMaxPassThrough = 4096;          // medium boundaries crossed within one bounce
+constexpr int kMaxShadowSegments = 4096;       // medium boundaries along one shadow ray (per round)
 constexpr int kMediaRounds = 2;                // queued tracking rounds per bounce before the inline round
 // Media counters of a bounce (PathState::mc): [3r] segments queued in round r,
 // [3r+1] segments taken, [3r+2] entries of list r + 1; path extension at 0,

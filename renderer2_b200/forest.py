@@ -177,6 +177,8 @@ class _ClassSet:
         self.n += 1
 
     def collides(self, c, r):
+        # checkCollision: |c_i - c| <= r_i + r + 0.0001 (the generator takes the
+        # length with np.dot, which may round the last bit of the sum differently)
         if self.n == 0:
             return False
         d = self.c[:self.n] - c
@@ -212,11 +214,13 @@ def place_trees(relevant_models: dict, volume_descriptions: dict, attempts: int 
 def generate_forest(relevant_models: dict, volume_descriptions: dict, camera: dict, generate_gt: bool = False,
                     min_lod: float = 0.1, covered_pixels: float = 1.0, attempts: int = 100_000, seed: int = 0,
                     radius: float = RADIUS, assets_root: str = "../../raytracer/assets/",
-                    filtering_root: str = "./filtering/") -> list:
+                    filtering_root: str = "./filtering/", placed: list = None) -> list:
     """The forest as the generator's scene list: (type, directory, filename,
     pos, orientation, scaling) per tree, a Mesh for LOD "0" and a Medium for
-    the others (getTreeDescription, generate_random_forest.py:19-46)."""
-    placed = place_trees(relevant_models, volume_descriptions, attempts, seed, radius)
+    the others (getTreeDescription, generate_random_forest.py:19-46).
+    `placed` (optional): the trees of an earlier place_trees call."""
+    if placed is None:
+        placed = place_trees(relevant_models, volume_descriptions, attempts, seed, radius)
     names = sorted({p["Model"]["Name"] for p in placed})
     table = LodTable(volume_descriptions, names)
     if generate_gt or not placed:

@@ -158,15 +158,15 @@ def forest_library(work_dir, n_quads: int = 20_000, grid: int = 64, lods: int = 
 
 
 def forest_trees(lib: dict, attempts: int, radius: float, width: int, height: int, min_lod: float = 0.0,
-                 covered_pixels: float = 1.0, camera=FOREST_CAMERA, seed: int = 0) -> list:
+                 covered_pixels: float = 1.0, camera=FOREST_CAMERA, seed: int = 0, placed: list = None) -> list:
     """The generator's scene list for a forest of the library's trees: dart
-    throwing in a disc of `radius`, LODs chosen on the GPU for a width x height
-    sensor at `camera`."""
+    throwing in a disc of `radius` (or the trees `placed` earlier), LODs
+    chosen on the GPU for a width x height sensor at `camera`."""
     pos, look, up, fov = camera
     cam = FO.lod_camera(pos, look, up, width, height, fov)
     return FO.generate_forest(lib["relevant_models"], lib["volume_descriptions"], cam, False, min_lod,
                               covered_pixels, attempts, seed, radius, assets_root=lib["assets_root"] + "/",
-                              filtering_root=lib["filtering_root"] + "/")
+                              filtering_root=lib["filtering_root"] + "/", placed=placed)
 
 
 def forest_ground():
