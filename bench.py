@@ -182,6 +182,13 @@ def filter_workload():
     return mesh, mat, prm, vs
 
 
+def _media_launches(tuning):
+    """Kernel launches per bounce of a media scene: resolve, then per queued round track + resolve (the
+    last one walking the rest), collide, events, shade, and the same rounds for the shadow rays, accum."""
+    r = tuning.get("media_rounds") or 2
+    return 6 + 4 * r
+
+
 def _input_bytes(desc):
     b = desc["env"].nbytes
     for mesh, _, _ in desc["meshes"]:
@@ -480,12 +487,12 @@ def bench_volume(args, world, local):
            "roofline": roofline,
            "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms},
-           # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, events, shade, 3 shadow resolve, accum
-           "gpu_launches": (prm.spp // S) * (2 + 14 * prm.max_depth) * args.steps}
+           # per wave: camera, finish; per bounce: _media_launches
+           "gpu_launches": (prm.spp // S) * (2 + _media_launches(tuning) * prm.max_depth) * args.steps}
     return out, (desc, cam, prm)
 
 
-def bench_forest(args, world, local):
+def bench_forest(args, world, local, cfg=None, autotune=True):
     """Forest leg: a many-instance scene as the reference's forest generator
     makes it (dart-throwing placement, screen-space LOD per tree; the trees
     nearest the camera stay meshes), medium instances sharing their files and
@@ -499,7 +506,7 @@ def bench_forest(args, world, local):
     from renderer2_b200 import forest as FO
     from renderer2_b200 import raytracer as R
     from renderer2_b200 import render_scenes as RS
-    c = FOREST_CFG
+    c = dict(FOREST_CFG, **(cfg or {}))
     work = tempfile.mkdtemp(prefix="r2forest")
     lib = RS.forest_library(work, n_quads=c["n_quads"], grid=c["grid"], lods=c["lods"])
     t0 = time.perf_counter()
@@ -530,7 +537,7 @@ def bench_forest(args, world, local):
     build_ms = (time.perf_counter() - t0) * 1e3
     cam = R.camera(c["width"], c["height"], fov, pos, look, up)
     prm = R.params(c["spp"], c["depth"], c["seed"], brick_grid=True)
-    tuning = sc.autotune(cam, prm).as_dict()
+    tuning = sc.autotune(cam, prm).as_dict() if autotune else sc.get_tuning().as_dict()
     npix = cam.width * cam.height
     frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
@@ -579,9 +586,8 @@ def bench_forest(args, world, local):
                                                "kind": "port", "sample": f"{n_cpu} trees"},
                               "placement_s": place_s, "placement_attempts": c["attempts"]},
             "scene_build_ms": build_ms,
-            # per wave: camera, finish; per bounce: 3 resolve, 4 track, collide, events, shade, 3 shadow resolve,
-            # accum
-            "gpu_launches": (prm.spp // S) * (2 + 14 * prm.max_depth) * args.steps}
+            # per wave: camera, finish; per bounce: _media_launches
+            "gpu_launches": (prm.spp // S) * (2 + _media_launches(tuning) * prm.max_depth) * args.steps}
 
 
 def bench_volume_batch(args, world, local):
@@ -664,7 +670,7 @@ def bench_volume_batch(args, world, local):
             "speedup_vs_one_at_a_time": ms_seq / ms_batch,
             "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(sum(npix) * 12), "ms_per_step": e2e_ms},
-            "gpu_launches": c["spp"] * c["scenes"] * (3 + 14 * c["depth"]) * args.steps}
+            "gpu_launches": c["spp"] * c["scenes"] * (3 + _media_launches(tuned.as_dict()) * c["depth"]) * args.steps}
 
 
 def serving_jobs(seed=11):
@@ -947,6 +953,9 @@ def run_case(args):
     elif args.case == "forest":
         args.steps, args.warmup = 1, 1
         print(json.dumps(bench_forest(args, 1, 0)))
+    elif args.case == "forest-small":  # a quarter of the pixels, 1 spp, default tuning: one wave per step
+        args.steps, args.warmup = 1, 1
+        print(json.dumps(bench_forest(args, 1, 0, dict(width=960, height=540, spp=1), autotune=False)))
     elif args.case in ("volume-small", "volume-mid"):
         import tempfile
 
@@ -982,7 +991,7 @@ def main():
     ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
     ap.add_argument("--case", default=None,
                     help="profiling case: render-wave | filter-small | volume-small | volume-mid | volume-batch | forest | "
-                         "serving")
+                         "forest-small | serving")
     ap.add_argument("--case-spp", type=int, default=1, help="render-wave: samples per pixel, all in one wave")
     args = ap.parse_args()
     if args.case:

@@ -259,6 +259,8 @@ typedef struct r2_render_tuning {
   uint32_t trav_refill; /* finished lanes of a warp (1..32) that make it take new rays */
   uint32_t wave_paths;  /* paths per wave: a wave renders the largest divisor of spp samples of every
                            pixel that keeps width*height*samples within it (at least one sample) */
+  uint32_t media_rounds; /* media: queued rounds of medium boundaries per bounce (1..32) before the
+                            remaining boundaries of a path are walked in one pass */
 } r2_render_tuning;
 
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA

@@ -36,13 +36,6 @@ constexpr uint32_t kPurposeScatter = 0x100u;   // phase-function and light draws
 constexpr uint32_t kPurposeShadowTr = 0x200u;  // + shadow slot (0 light, 1 BSDF)
 constexpr int kMaxPassThrough = 4096;          // medium boundaries crossed within one bounce
 constexpr int kMaxShadowSegments = 4096;       // medium boundaries along one shadow ray (per round)
-constexpr int kMediaRounds = 2;                // queued tracking rounds per bounce before the inline round
-// Media counters of a bounce (PathState::mc): [3r] segments queued in round r,
-// [3r+1] segments taken, [3r+2] entries of list r + 1; path extension at 0,
-// shadows at kShadowCounters.
-constexpr int kCountersPerBounce = 16;
-constexpr int kShadowCounters = 6;
-constexpr int kCollideCounter = 12;  // entries of the collision list
 
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 // Sample index of the wave: a kernel parameter, or the device counter of a
@@ -600,7 +593,7 @@ template <bool kFirst, bool kInline>
 __global__ void __launch_bounds__(128) k_resolve(RenderLaunch L, int round) {
   uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce;
   const uint32_t n = kFirst ? *(volatile uint32_t*)&L.st.counts[L.bounce] : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
-  const uint32_t* list = kFirst ? path_queue(L, L.bounce) : pick(L.st.rl, (uint32_t)(round - 1));
+  const uint32_t* list = kFirst ? path_queue(L, L.bounce) : pick(L.st.rl, (uint32_t)(round - 1) & 1u);
   uint32_t* jobs = &mc[3 * round];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) resolve_path<kInline>(L, list[i], kFirst, jobs);
@@ -690,7 +683,7 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
   const uint32_t njobs = *(volatile uint32_t*)&mc[3 * round];
   uint32_t* taken = &mc[3 * round + 1];
   uint32_t* nextCount = &mc[3 * round + 2];
-  uint32_t* nextList = kSample ? pick(L.st.rl, (uint32_t)round) : pick(L.st.sl, (uint32_t)round);
+  uint32_t* nextList = kSample ? pick(L.st.rl, (uint32_t)round & 1u) : pick(L.st.sl, (uint32_t)round & 1u);
   const int lane = threadIdx.x & 31;
   TrackState s;
   uint32_t owner = 0;
@@ -1123,7 +1116,7 @@ template <bool kFirst, bool kInline>
 __global__ void __launch_bounds__(128) k_shadow_resolve(RenderLaunch L, int round) {
   uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce + kShadowCounters;
   const uint32_t n = kFirst ? 2 * event_count(L) : *(volatile uint32_t*)&mc[3 * (round - 1) + 2];
-  const uint32_t* list = kFirst ? nullptr : pick(L.st.sl, (uint32_t)(round - 1));
+  const uint32_t* list = kFirst ? nullptr : pick(L.st.sl, (uint32_t)(round - 1) & 1u);
   uint32_t* jobs = &mc[3 * round];
   const uint32_t stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -1223,6 +1216,8 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
   if (L.trackSteps == 0) L.trackSteps = kDefaultTrackSteps;
   if (L.travVisits == 0) L.travVisits = kDefaultTravVisits;
   if (L.travRefill == 0) L.travRefill = kDefaultTravRefill;
+  if (L.mediaRounds == 0) L.mediaRounds = kDefaultMediaRounds;
+  const int rounds = (int)std::min<uint32_t>(L.mediaRounds, kMaxMediaRounds);
   query_track_blocks();
   const bool media = L.scene.nmedia > 0;
   int ev = 0;
@@ -1241,9 +1236,9 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
     L.bounce = b;
     if (media) {
       k_resolve<true, false><<<nblocks * 2, 128, 0, s>>>(L, 0);
-      for (int r = 0; r < kMediaRounds; ++r) {
+      for (int r = 0; r < rounds; ++r) {
         launch_track(L, true, r, s);
-        if (r + 1 < kMediaRounds) k_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
+        if (r + 1 < rounds) k_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
         else k_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
       if (L.dda) k_collide<true><<<nblocks * 2, 128, 0, s>>>(L);
@@ -1253,9 +1248,9 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
       k_shade<true><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
       k_shadow_resolve<true, false><<<nblocks * 2, 128, 0, s>>>(L, 0);
-      for (int r = 0; r < kMediaRounds; ++r) {
+      for (int r = 0; r < rounds; ++r) {
         launch_track(L, false, r, s);
-        if (r + 1 < kMediaRounds) k_shadow_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
+        if (r + 1 < rounds) k_shadow_resolve<false, false><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
         else k_shadow_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
     } else {

@@ -68,8 +68,8 @@ struct PathState {
   float4* jO;       // queued segments: origin, tmax
   float4* jD;       //                  direction, medium (int bits)
   uint2* jM;        //                  owner (path or shadow slot), stream purpose / draw index
-  uint32_t* rl[2];  // paths resumed in rounds 1, 2
-  uint32_t* sl[2];  // shadow slots resumed in rounds 1, 2
+  uint32_t* rl[2];  // paths resumed in the next round (round r writes list r & 1)
+  uint32_t* sl[2];  // shadow slots resumed in the next round
   uint32_t* cl;     // paths whose queued segment ended in a collision
   float4* swP;      // shadow walk: next origin, transmittance so far
   int2* swM;        // shadow walk: current medium, draw index of the slot's stream
@@ -81,6 +81,14 @@ constexpr uint32_t kDefaultTrackSteps = 8;   // tracking steps a lane takes betw
 constexpr uint32_t kDefaultTravVisits = 32;  // BVH visits between refill checks
 constexpr uint32_t kDefaultTravRefill = 8;   // finished lanes that trigger a refill
 constexpr uint32_t kDefaultWavePaths = 1u << 22;  // paths per wave a frame's samples are grouped to
+constexpr uint32_t kDefaultMediaRounds = 2;       // queued medium-boundary rounds per bounce
+constexpr uint32_t kMaxMediaRounds = 32;
+// Media counters of a bounce (PathState::mc): [3r] segments queued in round r,
+// [3r+1] segments taken, [3r+2] entries of list r + 1; path extension from 0,
+// shadow rays from kShadowCounters, then the collision list's entries.
+constexpr int kShadowCounters = 3 * (kMaxMediaRounds + 1);
+constexpr int kCollideCounter = 2 * kShadowCounters;
+constexpr int kCountersPerBounce = (kCollideCounter + 4) & ~3;
 
 // PathState::counts layout: [0, 64) live paths per bounce, then two counters
 // per bounce (extension rays taken, shadow records taken), then the surface
@@ -118,6 +126,7 @@ struct RenderLaunch {
   uint32_t trackSteps;  // tracking steps a lane takes between refills (tuning, >= 1)
   uint32_t travVisits;  // BVH visits a lane takes between refill checks of the surface kernels (tuning, >= 1)
   uint32_t travRefill;  // finished lanes of a warp that trigger a refill (tuning, 1..32)
+  uint32_t mediaRounds; // queued medium-boundary rounds per bounce (tuning, 1..kMaxMediaRounds)
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

@@ -118,6 +118,7 @@ RenderScene::RenderScene() {
   tuning_.track_steps = env("R2_TRACK_STEPS", 1, 1024);
   tuning_.trav_visits = env("R2_TRAV_VISITS", 1, 1 << 20);
   tuning_.trav_refill = env("R2_TRAV_REFILL", 1, 32);
+  tuning_.media_rounds = env("R2_MEDIA_ROUNDS", 1, kMaxMediaRounds);
 }
 
 RenderScene::~RenderScene() {}
@@ -331,7 +332,7 @@ void RenderContext::ensure(uint32_t n, bool media) {
   if (media && n > mediaCap_) {
     shX_.alloc(2 * (size_t)n);
     evA_.alloc(n); evB_.alloc(n); evC_.alloc(n); evD_.alloc(n);
-    mc_.alloc(16 * 64);
+    mc_.alloc((size_t)kCountersPerBounce * 64);
     pj_.alloc(n); rl0_.alloc(n); rl1_.alloc(n); cl_.alloc(n);
     sl0_.alloc(2 * (size_t)n); sl1_.alloc(2 * (size_t)n);
     jO_.alloc(2 * (size_t)n); jD_.alloc(2 * (size_t)n); jM_.alloc(2 * (size_t)n);
@@ -408,6 +409,7 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   L.trackSteps = tuning_.track_steps;
   L.travVisits = tuning_.trav_visits;
   L.travRefill = tuning_.trav_refill;
+  L.mediaRounds = tuning_.media_rounds;
   L.bound = ctx.bound.get();
   return L;
 }
@@ -515,8 +517,10 @@ RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const 
 }
 
 void RenderScene::set_tuning(const r2_render_tuning& t) {
-  R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31), R2_ERR_INVALID_ARGUMENT,
-             "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31)");
+  R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31) &&
+                 t.media_rounds <= kMaxMediaRounds,
+             R2_ERR_INVALID_ARGUMENT,
+             "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31, media_rounds <= 32)");
   tuning_ = t;
 }
 
@@ -550,7 +554,8 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     }
     return best / ((float)S * (float)npix);
   };
-  r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths};
+  r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths,
+                       kDefaultMediaRounds};
   try {
     R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
     time_wave(cur);  // warm-up
@@ -577,11 +582,13 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     static const uint32_t refills[] = {2, 4, 16, 32};
     static const uint32_t visits[] = {8, 16, 64, 256};
     static const uint32_t steps[] = {2, 4, 16, 32};
+    static const uint32_t rounds[] = {1, 4, 8, 16};
     sweep(&r2_render_tuning::wave_paths, wavePaths, 4);
     if (media_.empty()) {  // the persistent surface traversals run in scenes without media
       sweep(&r2_render_tuning::trav_refill, refills, 4);
       sweep(&r2_render_tuning::trav_visits, visits, 4);
     } else {
+      sweep(&r2_render_tuning::media_rounds, rounds, 4);
       sweep(&r2_render_tuning::track_steps, steps, 4);
     }
   } catch (...) {

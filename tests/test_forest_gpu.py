@@ -127,6 +127,20 @@ def test_forest_frame_matches_oracle(lib, trees, dda):
     assert np.all(np.abs(g - o) <= 1e-3 * np.maximum(1.0, np.abs(o)))
 
 
+def test_forest_rounds_never_change_the_frame(lib, trees):
+    """Paths crossing many tree boxes: the boundaries a bounce queues in rounds
+    and those it walks in the last pass give the same frame."""
+    desc = RS.forest_desc(lib, trees, media_only=True)
+    cam = _cam(40, 28)
+    prm = R.params(2, 6, 11, brick_grid=True)
+    sc = RS.build_scene(desc)
+    ref = sc.render(cam, prm)
+    for rounds in (1, 3, 12, 32):
+        sc.set_tuning(R.tuning(media_rounds=rounds, track_steps=3))
+        assert np.array_equal(sc.render(cam, prm), ref), rounds
+    sc.close()
+
+
 def test_instances_of_one_path_share_the_first_coefficients(lib, trees):
     desc = RS.forest_desc(lib, trees, media_only=True)
     path = desc["media"][0][0]

@@ -126,17 +126,25 @@ def test_medium_loading_errors(lods, tmp_path):
     sc.close()
 
 
+def test_medium_tuning_out_of_range_is_rejected(lods):
+    sc = RS.build_scene(_desc(lods[0]))
+    with pytest.raises(N.R2Error):
+        sc.set_tuning(R.tuning(media_rounds=33))
+    sc.close()
+
+
 def test_medium_tracking_tuning_never_changes_the_frame(lods):
     desc = _desc(lods[0])
     cam = R.camera(32, 28, 50.0, (0.3, 0.6, 3.2), (0.0, 0.0, 0.0), (0, 1, 0))
     sc = RS.build_scene(desc)
     prm = R.params(3, 8, 17, brick_grid=True)
     ref = sc.render(cam, prm)
-    for steps, visits, refill, wave in [(1, 2, 1, 32 * 28), (64, 7, 32, 3 * 32 * 28)]:
-        sc.set_tuning(R.tuning(steps, visits, refill, wave))
+    for steps, visits, refill, wave, rounds in [(1, 2, 1, 32 * 28, 1), (64, 7, 32, 3 * 32 * 28, 32),
+                                                (8, 32, 8, 32 * 28, 5)]:
+        sc.set_tuning(R.tuning(steps, visits, refill, wave, rounds))
         assert sc.wave_samples(cam, prm) == wave // (32 * 28)
-        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill, wave)
+        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill, wave, rounds)
     t = sc.autotune(cam, prm)
-    assert t.track_steps >= 1
+    assert t.track_steps >= 1 and 1 <= t.media_rounds <= 32
     assert np.array_equal(sc.render(cam, prm), ref)
     sc.close()
