@@ -57,7 +57,7 @@ SHADE_BYTES_PER_SEGMENT = 256.0
 VOLUME_CFG = dict(grid=256, n_quads=200_000, ico_subdiv=6, width=1920, height=1080, spp=16, depth=16, seed=0)
 VOLUME_BATCH_CFG = dict(scenes=16, grids=(128, 192, 256, 160), quads=(50_000, 150_000, 300_000), ico=(6, 7),
                         width=1920, height=1080, spp=2, depth=16)
-SERVE_CFG = dict(jobs=60, rate=40.0, slots=2, budget=40 << 30)
+SERVE_CFG = dict(jobs=60, rate=40.0, slots=4, budget=40 << 30)
 # forest leg: the forest generator's disc (radius 1000, 100,000 placement attempts) of three synthetic tree
 # models, each filtered into 4 LODs; LODs chosen on the GPU for the generator's camera at 1920x1080
 FOREST_CFG = dict(n_quads=20_000, grid=64, lods=4, attempts=100_000, radius=1000.0, width=1920, height=1080,
@@ -742,18 +742,19 @@ def bench_serving(args):
 
     for k in range(min(4, len(jobs))):  # warm-up (BVH and graph code paths, allocations)
         run_alone(k)
-    # one job at a time: FIFO on one queue, each job alone on the GPU
-    t0 = time.perf_counter()
-    done_alone = []
-    for k in range(len(jobs)):
-        now = time.perf_counter() - t0
-        if now < arrivals[k]:
-            time.sleep(arrivals[k] - now)
-        run_alone(k)
-        done_alone.append(time.perf_counter() - t0)
-    span_alone = done_alone[-1] - arrivals[0]
-    lat_alone = np.array(done_alone) - arrivals
-    # served: submit at the arrival times, wait for all
+
+    def one_at_a_time(arr):
+        """FIFO on one queue, each job alone on the GPU; completion times from the first arrival."""
+        t0 = time.perf_counter()
+        done = []
+        for k in range(len(jobs)):
+            now = time.perf_counter() - t0
+            if now < arr[k]:
+                time.sleep(arr[k] - now)
+            run_alone(k)
+            done.append(time.perf_counter() - t0)
+        return done[-1] - arr[0], np.array(done) - arr
+
     srv = S.Server(slots=c["slots"], hbm_budget=c["budget"])
     # warm-up like the one-at-a-time path: the largest jobs of each kind size every slot's buffers once
     big = sorted(range(len(jobs)), key=lambda k: -(work[k][0] + 64 * work[k][1]))
@@ -762,27 +763,57 @@ def bench_serving(args):
         hs = [srv.submit_render(*specs[k]) if jobs[k][0] == "render" else srv.submit_filter(*specs[k]) for k in warm]
         for h in hs:
             srv.wait(h, 600.0)
-    handles = [None] * len(jobs)
-    t0 = time.perf_counter()
 
-    def submitter():
+    def served(arr):
+        """Submitted at the arrival times from another thread, served by the request loop."""
+        handles = [None] * len(jobs)
+        t0 = time.perf_counter()
+
+        def submitter():
+            for k in range(len(jobs)):
+                now = time.perf_counter() - t0
+                if now < arr[k]:
+                    time.sleep(arr[k] - now)
+                s = specs[k]
+                handles[k] = srv.submit_render(*s) if jobs[k][0] == "render" else srv.submit_filter(*s)
+
+        th_sub = th.Thread(target=submitter)
+        th_sub.start()
+        th_sub.join()
+        done = np.zeros(len(jobs))
         for k in range(len(jobs)):
-            now = time.perf_counter() - t0
-            if now < arrivals[k]:
-                time.sleep(arrivals[k] - now)
-            s = specs[k]
-            handles[k] = srv.submit_render(*s) if jobs[k][0] == "render" else srv.submit_filter(*s)
+            srv.wait(handles[k], 600.0)
+            done[k] = handles[k].times[2] - handles[k].times[0] + arr[k]
+        return done.max() - arr[0], done - arr
 
-    th_sub = th.Thread(target=submitter)
-    th_sub.start()
-    done_srv = [0.0] * len(jobs)
-    th_sub.join()
+    descs = [d1, d2]
+
+    def plain(k):
+        """A job as a process that renders one frame does it: build the scene (upload, BVH), run, download."""
+        j = jobs[k]
+        if j[0] == "render":
+            sc = RS.build_scene(descs[j[2]])
+            sc.render(specs[k][1], specs[k][2])
+            sc.close()
+        else:
+            fs = F.FilterScene(meshes[j[2]], fmat)
+            out = torch.empty(work[k][1] * 32, dtype=torch.uint8, device="cuda")
+            fs.run(fs.grid(scenes.voxel_size_for(meshes[j[2]], j[3])), specs[k][2], out.data_ptr())
+            out.cpu()
+            fs.close()
+        torch.cuda.synchronize()
+
+    span_alone, lat_alone = one_at_a_time(arrivals)
+    span_srv, lat_srv = served(arrivals)
+    burst = np.zeros(len(jobs))  # every job waiting at once: the throughput each path sustains
+    span_alone_b, _ = one_at_a_time(burst)
+    span_srv_b, lat_srv_b = served(burst)
+    plain(0)
+    t0 = time.perf_counter()
     for k in range(len(jobs)):
-        srv.wait(handles[k], 600.0)
-        done_srv[k] = handles[k].times[2] - handles[k].times[0] + arrivals[k]
+        plain(k)
+    span_plain_b = time.perf_counter() - t0
     srv.close()
-    span_srv = max(done_srv) - arrivals[0]
-    lat_srv = np.array(done_srv) - arrivals
     for sc in rscenes:
         sc.close()
     for fs in fscenes:
@@ -801,7 +832,19 @@ def bench_serving(args):
             "one_at_a_time": {"paths_per_s": paths / span_alone, "voxels_per_s": voxels / span_alone,
                               "makespan_s": span_alone, "p50_latency_s": pct(lat_alone, 50),
                               "p99_latency_s": pct(lat_alone, 99)},
-            "speedup_makespan": span_alone / span_srv}
+            "speedup_makespan": span_alone / span_srv,
+            "burst": {"workload": f"the same {len(jobs)} jobs all submitted at once",
+                      "served": {"paths_per_s": paths / span_srv_b, "voxels_per_s": voxels / span_srv_b,
+                                 "makespan_s": span_srv_b, "p50_latency_s": pct(lat_srv_b, 50),
+                                 "p99_latency_s": pct(lat_srv_b, 99)},
+                      "one_at_a_time": {"paths_per_s": paths / span_alone_b, "voxels_per_s": voxels / span_alone_b,
+                                        "makespan_s": span_alone_b},
+                      "speedup_makespan": span_alone_b / span_srv_b,
+                      "plain_per_job_scene_build": {
+                          "paths_per_s": paths / span_plain_b, "voxels_per_s": voxels / span_plain_b,
+                          "makespan_s": span_plain_b,
+                          "note": "each job builds its scene (upload, BVH), runs and downloads, one after the other"},
+                      "speedup_vs_plain": span_plain_b / span_srv_b}}
 
 
 def run_native(args):
