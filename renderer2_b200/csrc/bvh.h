@@ -168,13 +168,15 @@ struct TraceState {
 
 constexpr int kTraceDone = 0x7FFFFFFF;  // no node left to visit (never a node index)
 
-R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax) {
+// root: the node the query starts at (0: the tree's root; a child reference
+// whose subtree holds every triangle the ray can hit, a leaf included).
+R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax, int root = 0) {
   s.r = make_ray_pre(o, d);
   s.best.t = tmax;
   s.best.b1 = s.best.b2 = 0.0f;
   s.best.tri = 0x7FFFFFFF;
-  s.cur = 0;  // root is internal node 0
-  s.leaf = 0;
+  s.cur = root < 0 ? kTraceDone : root;
+  s.leaf = root < 0 ? root : 0;
   s.sp = 0;
   s.found = 0;
   s.nodes = s.tris = 0;
@@ -297,9 +299,9 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
 // visited and the triangles tested to *nodes and *tris.
 template <bool kAnyHit, bool kCount = false>
 R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax, uint32_t* nodes = nullptr,
-                    uint32_t* tris = nullptr) {
+                    uint32_t* tris = nullptr, int root = 0) {
   TraceState s;
-  trace_begin(s, o, d, tmax);
+  trace_begin(s, o, d, tmax, root);
   int stack[R2_BVH_STACK];
   float stackT[R2_BVH_STACK];
   if (bvh.alpha.alphaTex) {

@@ -75,6 +75,25 @@ __device__ bool bvh_any_box(const BvhView& bvh, V3 qlo, V3 qhi) {
   }
 }
 
+// The deepest node whose subtree holds every leaf whose box overlaps the
+// query box: descend while exactly one child's box overlaps it.  A leaf that
+// a ray confined to the query box can hit overlaps it, and so does every box
+// above that leaf, so a traversal started here finds the same closest hit as
+// one started at the root.
+__device__ int bvh_local_root(const BvhView& bvh, V3 qlo, V3 qhi) {
+  int cur = 0;
+  for (int depth = 0; depth < R2_BVH_STACK && cur >= 0; ++depth) {
+    const BvhNode* nd = &bvh.nodes[cur];
+    const float4 b0 = __ldg(&nd->b0), b1 = __ldg(&nd->b1), bz = __ldg(&nd->bz);
+    const int4 ch = __ldg(&nd->ch);
+    const bool h0 = box_overlap(b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, qlo, qhi);
+    const bool h1 = ch.y != R2_BVH_NONE && box_overlap(b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, qlo, qhi);
+    if (h0 == h1) return cur;  // both children (or neither): start here
+    cur = h0 ? ch.x : ch.y;
+  }
+  return cur;
+}
+
 __device__ __forceinline__ void write_voxel(r2_voxel* out, size_t vid, const r2_voxel& v) {
   const uint4* src = reinterpret_cast<const uint4*>(&v);
   uint4* dst = reinterpret_cast<uint4*>(out + vid);
@@ -156,6 +175,11 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
     const int z = (int)(vid / ((uint32_t)L.nx * (uint32_t)L.ny));
     const V3 center = voxel_center(L, x, y, z);
     const V3 cv = v3((float)x, (float)y, (float)z);
+    // every sample ray stays within `reach` of the centre (the classification's
+    // radius), padded for rounding: its traversal starts at the local root
+    const float reach = L.clip ? radius : length(L.voxelSize) / 2.0f + tMaxFixed;
+    const float pad = reach * 1.01f + 1e-5f * (fabsf(center.x) + fabsf(center.y) + fabsf(center.z) + 1.0f);
+    const int root = bvh_local_root(L.bvh, center - v3(pad), center + v3(pad));
 
     CSum S[6], nrm[3], dist;
     float dif[3] = {0.f, 0.f, 0.f}, spe[3] = {0.f, 0.f, 0.f}, rough = 0.f, ior = 0.f;
@@ -173,7 +197,7 @@ __global__ void __launch_bounds__(kSampleWarps * 32) k_filter_sample(FilterLaunc
       const V3 o = xform_point(L.indexToWorld, oi);
       const V3 d = uniform_sample_sphere(u01(r0.w), u01(r1.x));
       const float tmax = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
-      const Hit h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris);
+      const Hit h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris, root);
       if (kCount) ++cRays;
       float tsv = -1.0f;
       if (h.tri >= 0) {
