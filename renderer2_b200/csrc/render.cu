@@ -1193,7 +1193,7 @@ void query_track_blocks() {
   g_travBlocks[0] = resident_blocks(k_extend, 128);
   g_travBlocks[1] = resident_blocks(k_shadow_surfaces, 128);
   // the trackers run half the resident blocks: their brick and leaf lookups
-  // hit L1 more often with fewer warps per SM (1080p foliage wave, 1 spp:
+  // hit L1 more often with fewer warps per SM (960x540 foliage wave, 1 spp:
   // 24.8 ms with every resident block, 22.5 with half, 23.5 with a third)
   g_trackBlocks[1] = resident_blocks(k_track<true, false>, 128) / 2;
   g_trackBlocks[2] = resident_blocks(k_track<false, true>, 128) / 2;
