@@ -261,6 +261,8 @@ typedef struct r2_render_tuning {
                            pixel that keeps width*height*samples within it (at least one sample) */
   uint32_t media_rounds; /* media: queued rounds of medium boundaries per bounce (1..32) before the
                             remaining boundaries of a path are walked in one pass */
+  uint32_t track_blocks; /* media: blocks per SM of the persistent trackers (at most the resident
+                            blocks; 0: all of them) */
 } r2_render_tuning;
 
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA

@@ -1192,13 +1192,10 @@ void query_track_blocks() {
   if (g_trackBlocks[0] != 0) return;
   g_travBlocks[0] = resident_blocks(k_extend, 128);
   g_travBlocks[1] = resident_blocks(k_shadow_surfaces, 128);
-  // the trackers run half the resident blocks: their brick and leaf lookups
-  // hit L1 more often with fewer warps per SM (960x540 foliage wave, 1 spp:
-  // 24.8 ms with every resident block, 22.5 with half, 23.5 with a third)
-  g_trackBlocks[1] = resident_blocks(k_track<true, false>, 128) / 2;
-  g_trackBlocks[2] = resident_blocks(k_track<false, true>, 128) / 2;
-  g_trackBlocks[3] = resident_blocks(k_track<true, true>, 128) / 2;
-  g_trackBlocks[0] = resident_blocks(k_track<false, false>, 128) / 2;
+  g_trackBlocks[1] = resident_blocks(k_track<true, false>, 128);
+  g_trackBlocks[2] = resident_blocks(k_track<false, true>, 128);
+  g_trackBlocks[3] = resident_blocks(k_track<true, true>, 128);
+  g_trackBlocks[0] = resident_blocks(k_track<false, false>, 128);
 }
 
 __global__ void k_advance_sample(uint32_t* sample, uint32_t n) { *sample += n; }
@@ -1206,7 +1203,11 @@ __global__ void k_advance_sample(uint32_t* sample, uint32_t n) { *sample += n; }
 void launch_track(const RenderLaunch& L, bool sample, int round, cudaStream_t s) {
   query_track_blocks();
   const int which = (L.dda ? 1 : 0) + (sample ? 2 : 0);
-  const int* b = g_trackBlocks;
+  // all resident blocks, or L.trackBlocks per SM (fewer warps per SM can
+  // reuse L1 better: a tuning choice)
+  int b[4];
+  for (int i = 0; i < 4; ++i)
+    b[i] = L.trackBlocks ? std::max(1, std::min(g_trackBlocks[i], (int)L.trackBlocks * sm_count())) : g_trackBlocks[i];
   switch (which) {
     case 0: k_track<false, false><<<b[0], 128, 0, s>>>(L, round); break;
     case 1: k_track<true, false><<<b[1], 128, 0, s>>>(L, round); break;

@@ -127,6 +127,7 @@ struct RenderLaunch {
   uint32_t travVisits;  // BVH visits a lane takes between refill checks of the surface kernels (tuning, >= 1)
   uint32_t travRefill;  // finished lanes of a warp that trigger a refill (tuning, 1..32)
   uint32_t mediaRounds; // queued medium-boundary rounds per bounce (tuning, 1..kMaxMediaRounds)
+  uint32_t trackBlocks; // persistent tracker blocks per SM (tuning; 0: every resident block)
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

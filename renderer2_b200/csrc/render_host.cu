@@ -119,6 +119,7 @@ RenderScene::RenderScene() {
   tuning_.trav_visits = env("R2_TRAV_VISITS", 1, 1 << 20);
   tuning_.trav_refill = env("R2_TRAV_REFILL", 1, 32);
   tuning_.media_rounds = env("R2_MEDIA_ROUNDS", 1, kMaxMediaRounds);
+  tuning_.track_blocks = env("R2_TRACK_BLOCKS", 1, 64);
 }
 
 RenderScene::~RenderScene() {}
@@ -410,6 +411,7 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   L.travVisits = tuning_.trav_visits;
   L.travRefill = tuning_.trav_refill;
   L.mediaRounds = tuning_.media_rounds;
+  L.trackBlocks = tuning_.track_blocks;
   L.bound = ctx.bound.get();
   return L;
 }
@@ -518,9 +520,10 @@ RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const 
 
 void RenderScene::set_tuning(const r2_render_tuning& t) {
   R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31) &&
-                 t.media_rounds <= kMaxMediaRounds,
+                 t.media_rounds <= kMaxMediaRounds && t.track_blocks <= 64,
              R2_ERR_INVALID_ARGUMENT,
-             "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31, media_rounds <= 32)");
+             "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31, media_rounds <= 32, "
+             "track_blocks <= 64)");
   tuning_ = t;
 }
 
@@ -555,7 +558,7 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     return best / ((float)S * (float)npix);
   };
   r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths,
-                       kDefaultMediaRounds};
+                       kDefaultMediaRounds, 0};
   try {
     R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
     time_wave(cur);  // warm-up
@@ -583,6 +586,7 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     static const uint32_t visits[] = {8, 16, 64, 256};
     static const uint32_t steps[] = {2, 4, 16, 32};
     static const uint32_t rounds[] = {1, 4, 8, 16};
+    static const uint32_t trackBlocks[] = {2, 3, 4, 6};
     sweep(&r2_render_tuning::wave_paths, wavePaths, 4);
     if (media_.empty()) {  // the persistent surface traversals run in scenes without media
       sweep(&r2_render_tuning::trav_refill, refills, 4);
@@ -590,6 +594,7 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     } else {
       sweep(&r2_render_tuning::media_rounds, rounds, 4);
       sweep(&r2_render_tuning::track_steps, steps, 4);
+      sweep(&r2_render_tuning::track_blocks, trackBlocks, 4);
     }
   } catch (...) {
     tuning_ = saved;

@@ -150,7 +150,7 @@ class RenderScene {
   DBuf<float4> envTex_;
   DBuf<float> envBuf_;
   SceneView view_;
-  r2_render_tuning tuning_{0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
+  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
 };
 
 // Frames of several committed scenes rendered by one captured CUDA graph: the

@@ -47,8 +47,8 @@ SPHERE, CIRCLE = 0, 1
 class Tuning(C.Structure):
     """Launch tuning (r2_render_tuning); 0 fields select the defaults; images never depend on it."""
     _fields_ = [("track_steps", C.c_uint32), ("trav_visits", C.c_uint32), ("trav_refill", C.c_uint32),
-                ("wave_paths", C.c_uint32), ("media_rounds", C.c_uint32)]
-    NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths", "media_rounds")
+                ("wave_paths", C.c_uint32), ("media_rounds", C.c_uint32), ("track_blocks", C.c_uint32)]
+    NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths", "media_rounds", "track_blocks")
 
     def as_tuple(self):
         return tuple(getattr(self, n) for n in self.NAMES)
@@ -57,8 +57,8 @@ class Tuning(C.Structure):
         return dict(zip(self.NAMES, self.as_tuple()))
 
 
-def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0, media_rounds=0) -> Tuning:
-    return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds)
+def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0, media_rounds=0, track_blocks=0) -> Tuning:
+    return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds, track_blocks)
 
 
 class Scene:

@@ -139,11 +139,11 @@ def test_medium_tracking_tuning_never_changes_the_frame(lods):
     sc = RS.build_scene(desc)
     prm = R.params(3, 8, 17, brick_grid=True)
     ref = sc.render(cam, prm)
-    for steps, visits, refill, wave, rounds in [(1, 2, 1, 32 * 28, 1), (64, 7, 32, 3 * 32 * 28, 32),
-                                                (8, 32, 8, 32 * 28, 5)]:
-        sc.set_tuning(R.tuning(steps, visits, refill, wave, rounds))
+    for steps, visits, refill, wave, rounds, blocks in [(1, 2, 1, 32 * 28, 1, 1), (64, 7, 32, 3 * 32 * 28, 32, 64),
+                                                        (8, 32, 8, 32 * 28, 5, 3)]:
+        sc.set_tuning(R.tuning(steps, visits, refill, wave, rounds, blocks))
         assert sc.wave_samples(cam, prm) == wave // (32 * 28)
-        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill, wave, rounds)
+        assert np.array_equal(sc.render(cam, prm), ref), (steps, visits, refill, wave, rounds, blocks)
     t = sc.autotune(cam, prm)
     assert t.track_steps >= 1 and 1 <= t.media_rounds <= 32
     assert np.array_equal(sc.render(cam, prm), ref)
