@@ -13,6 +13,7 @@ path decisions).  Both tracking modes are covered: the global majorant
 import numpy as np
 import pytest
 
+import flip
 import oracle_lib as O
 
 torch = pytest.importorskip("torch")
@@ -105,12 +106,17 @@ def test_medium_henyey_greenstein_matches_oracle(lods, g):
 def test_medium_three_sigma_against_high_spp_oracle(lods):
     desc = _desc(lods[0], ground=False)
     cam = R.camera(16, 16, 45.0, (0.0, 0.0, 3.0), (0.0, 0.0, 0.0), (0, 1, 0))
-    spp_g, spp_o = 256, 1024
+    spp_g, spp_o = 256, 4096
     g = _gpu(desc, cam, spp_g, 8, 101, True)
     o, var = O.render(desc, cam, spp_o, 8, 7, want_var=True, flags=1)
     sigma = np.sqrt(var / spp_g + var / spp_o) + 1e-7
     within = (np.abs(g - o) / sigma <= 3.0).mean()
     assert within >= 0.97, f"{within:.4f} of pixel channels within 3 sigma"
+    # mean LDR-FLIP of the 256-spp frame against the 4096-spp estimate (x / (1 + x), gamma 2.2)
+    ldr = lambda f: (np.asarray(f).reshape(16, 16, 3) / (1.0 + np.asarray(f).reshape(16, 16, 3))) ** (1 / 2.2)
+    mf = flip.mean_flip(ldr(o), ldr(g))
+    print(f"mean FLIP 256 spp vs 4096 spp: {mf:.4f}")
+    assert mf < 0.1
 
 
 def test_medium_loading_errors(lods, tmp_path):

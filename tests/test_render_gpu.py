@@ -8,6 +8,7 @@ low-spp GPU frame must lie within 3 sigma of a high-spp oracle estimate.
 import numpy as np
 import pytest
 
+import flip
 import oracle_lib as O
 
 torch = pytest.importorskip("torch")
@@ -84,13 +85,19 @@ def test_three_sigma_against_high_spp_oracle():
     desc = dict(desc)
     desc["env"] = RS.lognormal_env(32, 16, 1.0, 4)
     cam = R.camera(24, 24, 45.0, (0, 0, 3), (0, 0, 0), (0, 1, 0))
-    spp_g, spp_o = 64, 2048
+    spp_g, spp_o = 64, 4096
     g = _gpu_frame(desc, cam, spp_g, 8, 101)
     o, var = O.render(desc, cam, spp_o, 8, 7, want_var=True)
     sigma = np.sqrt(var / spp_g + var / spp_o) + 1e-7
     z = np.abs(g - o) / sigma
     within = (z <= 3.0).mean()
     assert within >= 0.98, f"{within:.4f} of pixel channels within 3 sigma"
+    # mean LDR-FLIP of the 64-spp frame against the 4096-spp estimate
+    # (x / (1 + x), gamma 2.2): Monte Carlo noise only
+    ldr = lambda f: (np.asarray(f).reshape(24, 24, 3) / (1.0 + np.asarray(f).reshape(24, 24, 3))) ** (1 / 2.2)
+    mf = flip.mean_flip(ldr(o), ldr(g))
+    print(f"mean FLIP 64 spp vs 4096 spp: {mf:.4f}")
+    assert mf < 0.1
 
 
 def test_device_entry_matches_host_entry_and_is_deterministic():
