@@ -183,7 +183,11 @@ r2_status r2_filter_scene_count(r2_filter_scene* scene, const r2_filter_grid* gr
  * array's device address (set-up done once per device) and should come
  * before any stream capture.  All calls share the one scratch array and it
  * keeps the last call's contents: calls that overlap on the GPU race and must
- * be serialised by the caller.
+ * be serialised by the caller.  stream NULL means the device's legacy default
+ * stream (not the scene's private stream), so calls given NULL run one after
+ * another, whichever scene each filters.  The current device, and the device
+ * of a given stream, must be the scene's device (R2_ERR_INVALID_ARGUMENT
+ * otherwise).
  * This entry point has no counterpart in the reference. */
 r2_status r2_filter_scene_run_static(r2_filter_scene* scene, const r2_filter_grid* grid,
                                      const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
@@ -506,24 +510,6 @@ r2_status r2_server_wait(r2_server* server, uint64_t job_id, double timeout_s, d
 /* stats_out (5 doubles): jobs done, jobs queued, jobs running, device bytes
  * admitted, seconds since the server started. */
 r2_status r2_server_stats(r2_server* server, double* stats_out);
-
-/* ------------------------------------------------------------------------ */
-/* Synthetic inputs (seeded), used by the configs in the benchmark plan. */
-
-/* Icosphere of subdivision level `subdiv` (20*4^subdiv triangles) of radius 1,
- * displaced radially by 1 + amplitude*valuenoise(4 p) with seed `seed`.
- * Capacities are in elements; counts are returned. Smooth area-weighted normals. */
-r2_status r2_gen_icosphere(uint32_t subdiv, float amplitude, uint32_t seed, float* positions,
-                           size_t pos_capacity, uint32_t* indices, size_t idx_capacity,
-                           float* normals, uint32_t* nverts_out, uint32_t* ntris_out);
-
-/* Leaf quads in the unit cube: n_quads quads (2 triangles each), a fraction
- * `clustered` Gaussian (sigma 0.02) around n_branches cubic Bezier curves,
- * random orientation, edge ~ U[0.005, 0.02]. */
-r2_status r2_gen_foliage(uint32_t n_quads, uint32_t n_branches, float clustered, uint32_t seed,
-                         float* positions, size_t pos_capacity, uint32_t* indices,
-                         size_t idx_capacity, float* normals, uint32_t* nverts_out,
-                         uint32_t* ntris_out);
 
 #ifdef __cplusplus
 }

@@ -445,7 +445,8 @@ static float oi_log(float x) {
 }
 
 /* Sequential uniforms: draw i = word i&3 of Philox((sample, bounce, i>>2, purpose), (pixel, seed)). */
-typedef struct { uint32_t k0, k1, c0, c1, purpose, idx; uint32_t buf[4]; } rng_t;
+/* replay (nullable, test hooks only): the values to return in order instead of Philox draws */
+typedef struct { uint32_t k0, k1, c0, c1, purpose, idx; uint32_t buf[4]; const float* replay; } rng_t;
 static rng_t rng_make(uint32_t pixel, uint32_t seed, uint32_t sample, uint32_t bounce, uint32_t purpose) {
   rng_t r;
   memset(&r, 0, sizeof(r));
@@ -453,6 +454,7 @@ static rng_t rng_make(uint32_t pixel, uint32_t seed, uint32_t sample, uint32_t b
   return r;
 }
 static float rng_next(rng_t* r) {
+  if (r->replay) return r->replay[r->idx++];
   const uint32_t w = r->idx & 3u;
   if (w == 0) {
     uint32_t ctr[4] = {r->c0, r->c1, r->idx >> 2, r->purpose}, key[2] = {r->k0, r->k1};
@@ -1719,6 +1721,37 @@ void orc_t_frame(const float* n, const float* v, float* out) {
 void orc_t_offset(const float* p, const float* d, float* out) { P3(out, offset_origin(L3(p), L3(d))); }
 
 int orc_t_find_interval(const float* cdf, int size, float u) { return find_interval(cdf, size, u); }
+
+/* SGGX microflake distribution of S (xx yy zz xy xz yz) and normal n:
+ * out = D(wi), sigma(wi), sampleVNDF(u1, u2) (3), specular p(wo, wi). */
+void orc_t_sggx(const float* S6, const float* n, const float* wo, const float* wi, float u1, float u2, float* out) {
+  const sggx_t g = make_sggx(S6, L3(n));
+  out[0] = sggx_D(&g, L3(wi));
+  out[1] = sggx_sigma(&g, L3(wi));
+  P3(out + 2, sggx_vndf(&g, u1, u2));
+  out[5] = sggx_p_spec(&g, L3(wo), L3(wi));
+}
+
+/* CSGGXPhaseFunction::sampleP with the uniforms u (consumed in order:
+ * lobe choice, VNDF pair, and for the diffuse lobe the cosine pair):
+ * out = wi (3), p, draws consumed. */
+void orc_t_sggx_sample(const float* S6, const float* n, float ior, const float* wo, const float* u, float* out) {
+  const sggx_t g = make_sggx(S6, L3(n));
+  rng_t r;
+  memset(&r, 0, sizeof(r));
+  r.replay = u;
+  f3 wi;
+  out[3] = sggx_sample_p(&g, ior, L3(wo), &wi, &r);
+  P3(out, wi);
+  out[4] = (float)r.idx;
+}
+
+/* getRotation(n): 16 floats, column major. */
+void orc_t_get_rotation(const float* n, float* out) {
+  const m4_t m = rot_from_normal(L3(n));
+  for (int c = 0; c < 4; ++c)
+    for (int i = 0; i < 4; ++i) out[4 * c + i] = m.m[c][i];
+}
 
 void orc_t_sphere(const float* c, float r, const float* o, const float* d, float tmax, float* out) {
   orc_shape sh;

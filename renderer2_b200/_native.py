@@ -2,7 +2,9 @@
 
 The native library is required: importing this module raises if
 ``_lib/librenderer2.so`` is missing (there is no Python or CPU fallback for
-the hot paths).
+the hot paths).  The library itself is opened on the first use of ``lib``,
+so that modules which only describe inputs (structures, seeded generators)
+can be imported by code that must not load it, such as the CPU baseline.
 """
 from __future__ import annotations
 
@@ -75,8 +77,6 @@ def _load():
         "r2_status_string": (C.c_char_p, [C.c_int]),
         "r2_last_error": (C.c_char_p, []),
         "r2_version": (C.c_int, []),
-        "r2_gen_icosphere": (C.c_int, [u32, f32, u32, P, sz, P, sz, P, P, P]),
-        "r2_gen_foliage": (C.c_int, [u32, u32, f32, u32, P, sz, P, sz, P, P, P]),
         "r2_filter_setup_grid": (C.c_int, [P, P, P, f32, P]),
         "r2_filter_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, f32, P, P, P, sz]),
         "r2_filter_scene_create": (C.c_int, [P, u32, P, u32, P, P, P, P]),
@@ -133,7 +133,16 @@ def _load():
     return lib
 
 
-lib = _load()
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"native library missing: {LIB_PATH} (run __graft_entry__.build())")
+
+
+def __getattr__(name):
+    if name == "lib":
+        loaded = _load()
+        globals()["lib"] = loaded
+        return loaded
+    raise AttributeError(name)
 
 
 def check(status: int) -> None:

@@ -1,4 +1,4 @@
-// C ABI: status handling, synthetic inputs and the filter entry points.
+// C ABI: status handling and the filter entry points.
 #include <string.h>
 
 #include <memory>
@@ -9,7 +9,6 @@
 #include "capi_util.h"
 #include "filter.cuh"
 #include "filter_host.h"
-#include "gen.h"
 #include "host_math.h"
 
 namespace r2 {
@@ -44,45 +43,6 @@ const char* r2_status_string(r2_status s) {
 const char* r2_last_error(void) { return r2::last_error(); }
 
 int r2_version(void) { return 100; }
-
-r2_status r2_gen_icosphere(uint32_t subdiv, float amplitude, uint32_t seed, float* positions,
-                           size_t pos_capacity, uint32_t* indices, size_t idx_capacity, float* normals,
-                           uint32_t* nverts_out, uint32_t* ntris_out) {
-  R2_API_BEGIN
-  R2_REQUIRE(subdiv <= 9, R2_ERR_UNSUPPORTED, "subdivision level above 9");
-  std::vector<float> p, n;
-  std::vector<uint32_t> i;
-  r2::gen_icosphere(subdiv, amplitude, seed, &p, &i, &n);
-  if (nverts_out) *nverts_out = (uint32_t)(p.size() / 3);
-  if (ntris_out) *ntris_out = (uint32_t)(i.size() / 3);
-  if (positions || indices || normals) {
-    R2_REQUIRE(pos_capacity >= p.size() && idx_capacity >= i.size(), R2_ERR_INVALID_ARGUMENT,
-               "output capacity too small");
-    if (positions) memcpy(positions, p.data(), p.size() * sizeof(float));
-    if (normals) memcpy(normals, n.data(), n.size() * sizeof(float));
-    if (indices) memcpy(indices, i.data(), i.size() * sizeof(uint32_t));
-  }
-  R2_API_END
-}
-
-r2_status r2_gen_foliage(uint32_t n_quads, uint32_t n_branches, float clustered, uint32_t seed, float* positions,
-                         size_t pos_capacity, uint32_t* indices, size_t idx_capacity, float* normals,
-                         uint32_t* nverts_out, uint32_t* ntris_out) {
-  R2_API_BEGIN
-  if (nverts_out) *nverts_out = 4 * n_quads;
-  if (ntris_out) *ntris_out = 2 * n_quads;
-  if (positions || indices || normals) {
-    R2_REQUIRE(pos_capacity >= (size_t)12 * n_quads && idx_capacity >= (size_t)6 * n_quads,
-               R2_ERR_INVALID_ARGUMENT, "output capacity too small");
-    std::vector<float> p, n;
-    std::vector<uint32_t> i;
-    r2::gen_foliage(n_quads, n_branches, clustered, seed, &p, &i, &n);
-    if (positions) memcpy(positions, p.data(), p.size() * sizeof(float));
-    if (normals) memcpy(normals, n.data(), n.size() * sizeof(float));
-    if (indices) memcpy(indices, i.data(), i.size() * sizeof(uint32_t));
-  }
-  R2_API_END
-}
 
 r2_status r2_filter_setup_grid(const float* model_bb_min, const float* model_bb_max, const float* model_to_world,
                                float voxel_size, r2_filter_grid* grid_out) {

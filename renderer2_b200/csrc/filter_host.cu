@@ -58,6 +58,7 @@ FilterScene::FilterScene(const float* positions, uint32_t nverts, const uint32_t
                          const float* uvs, const r2_material_maps* maps) {
   R2_REQUIRE(positions && indices && normals && materials, R2_ERR_INVALID_ARGUMENT, "null mesh array");
   R2_REQUIRE(nverts > 0 && ntris > 0, R2_ERR_INVALID_ARGUMENT, "empty mesh");
+  R2_CUDA(cudaGetDevice(&device_));
   R2_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   modelToWorld_ = m43_from_floats(modelToWorld);
   worldToModel_ = m4_to_m43(m4_inverse(m43_to_m4(modelToWorld_)));

@@ -33,11 +33,13 @@ class FilterScene {
 
   const DeviceBvh& bvh() const { return bvh_; }
   cudaStream_t stream() const { return stream_; }
+  int device() const { return device_; }
   V3 worldLo() const { return worldLo_; }
   V3 worldHi() const { return worldHi_; }
 
  private:
   cudaStream_t stream_ = nullptr;
+  int device_ = 0;  // the device current when the scene was created; its buffers live there
   cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
   M43 modelToWorld_, worldToModel_;
   V3 modelLo_, modelHi_, worldLo_, worldHi_;

@@ -136,4 +136,5 @@ def main(ref_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/raytracer/src/filtering")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.environ["R2_REFERENCE_DIR"], "raytracer", "src",
+                                                              "filtering"))

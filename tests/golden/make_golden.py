@@ -5,7 +5,9 @@ host from the reference tree, see oracle/ref_kat.cpp) and evaluates it on
 seeded inputs.  Run in the build container, where the reference tree is
 mounted:
 
-    python tests/golden/make_golden.py [/path/to/reference/raytracer/include]
+    python tests/golden/make_golden.py [<reference>/raytracer/include]
+
+Without an argument the reference tree is $R2_REFERENCE_DIR.
 
 The JSON holds inputs and reference outputs; tests/test_golden.py checks the
 oracle's restatement against it without needing the reference.
@@ -53,6 +55,7 @@ def build(ref_include: str) -> C.CDLL:
     lib.ref_sggx.argtypes = [P, P, P, P, f, f, P]
     lib.ref_sggx_sample.argtypes = [P, P, f, P, P, C.c_int, P]
     lib.ref_get_rotation.argtypes = [P, P]
+    lib.ref_draws_used.restype = C.c_int
     return lib
 
 
@@ -70,7 +73,7 @@ def unit(rng, n):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/raytracer/include"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.environ["R2_REFERENCE_DIR"], "raytracer", "include")
     lib = build(ref)
     rng = np.random.default_rng(20261203)
     g = {"vec2_arg_order": lib.ref_vec2_arg_order()}
@@ -208,6 +211,22 @@ def main():
         rows.append({"S": S6.tolist(), "n": n.tolist(), "wo": wo.tolist(), "wi": wi.tolist(), "u": [u1, u2],
                      "out": out.tolist()})
     g["sggx"] = rows
+
+    rows = []
+    for _ in range(256):
+        n = unit(rng, 1)[0]
+        a = float(rng.uniform(0.05, 1.0))
+        S = np.outer(n, n) + a * (np.eye(3) - np.outer(n, n))
+        S6 = _f32([S[0, 0], S[1, 1], S[2, 2], S[0, 1], S[0, 2], S[1, 2]])
+        wo = unit(rng, 1)[0]
+        ior = float(rng.uniform(1.0, 3.0))
+        c = _f32(rng.uniform(1e-6, 1.0, 5))
+        out = np.zeros(4, np.float32)
+        lib.ref_sggx_sample(_p(S6), _p(n), ior, _p(wo), _p(c), 5, _p(out))
+        used = lib.ref_draws_used()
+        rows.append({"S": S6.tolist(), "n": n.tolist(), "ior": ior, "wo": wo.tolist(),
+                     "draw_u": [lib.ref_u01(float(x)) for x in c], "draws_used": used, "out": out.tolist()})
+    g["sggx_sample"] = rows
 
     rows = []
     for n in [unit(rng, 1)[0] for _ in range(32)] + [_f32([0, 1, 0]), _f32([0, -1, 0]), _f32([1, 0, 0]),

@@ -44,9 +44,15 @@ def test_no_device_reported_without_gpu():
         assert e.name == "R2_ERR_NO_DEVICE"
 
 
-def test_generator_capacity_checked():
-    from renderer2_b200 import _native as N
-    pos = np.zeros(3, np.float32)
-    idx = np.zeros(3, np.uint32)
-    st = N.lib.r2_gen_icosphere(2, 0.0, 1, N.ptr(pos), pos.size, N.ptr(idx), idx.size, None, None, None)
-    assert N.lib.r2_status_string(st) == b"R2_ERR_INVALID_ARGUMENT"
+def test_workload_generators_do_not_load_the_library():
+    """The CPU baseline builds the benchmark's inputs with the seeded numpy
+    generators; the GPU library must stay unloaded in that process."""
+    import subprocess
+    import sys
+    code = ("import bench, sys\n"
+            "desc, cam, prm = bench.render_workload()\n"
+            "mesh, mat, fprm, vs = bench.filter_workload()\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "sys.exit(3 if 'librenderer2' in maps else 0)\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr

@@ -8,7 +8,10 @@ microfacet BRDF and VNDF sampling (microfacet_brdf.hpp:57-100,
 microfacet_distribution.hpp:40-141), Oren-Nayar (oren_nayar_brdf.hpp:36-81),
 CSampler warps (sampler.hpp:39-94), CCoordinateFrame::fromNormal
 (objects.hpp:28-40), CRay::offsetRayOrigin (ray.hpp:73-85), Sphere::intersect
-(sphere.hpp:33-90) and findInterval (functions.hpp:10-27).
+(sphere.hpp:33-90), findInterval (functions.hpp:10-27), the SGGX microflake
+distribution and phase function (sggx_phase_function.hpp:107-233: D, sigma,
+sampleVNDF, the specular lobe's p, sampleP of both lobes) and getRotation
+(functions.hpp:128-142).
 
 Tolerances: exact where the oracle performs the same float operations;
 a few float ulps where the oracle evaluates sampled angles with its own
@@ -41,6 +44,9 @@ L.orc_t_find_interval.restype = C.c_int
 L.orc_t_find_interval.argtypes = [P, C.c_int, f]
 L.orc_t_sphere.argtypes = [P, f, P, P, f, P]
 L.orc_t_build_s.argtypes = [P, f, P]
+L.orc_t_sggx.argtypes = [P, P, P, P, f, f, P]
+L.orc_t_sggx_sample.argtypes = [P, P, f, P, P, P]
+L.orc_t_get_rotation.argtypes = [P, P]
 
 
 def a32(x):
@@ -158,3 +164,45 @@ def test_find_interval_matches_reference():
     for r in G["find_interval"]:
         cdf = a32(r["cdf"])
         assert L.orc_t_find_interval(p(cdf), len(cdf), r["u"]) == r["k"]
+
+
+def test_sggx_distribution_matches_reference():
+    """D(w) = 1/(pi sqrt|det S| (w^T S^-1 w)^2), sigma(w), the VNDF sample and
+    the specular lobe.  The oracle draws the VNDF's disk angle with its own
+    sin/cos of 2 pi u, the reference rounds 2 pi u to float first: a few ulps."""
+    for r in G["sggx"]:
+        out = np.zeros(6, np.float32)
+        L.orc_t_sggx(p(a32(r["S"])), p(a32(r["n"])), p(a32(r["wo"])), p(a32(r["wi"])), r["u"][0], r["u"][1], p(out))
+        ref = np.asarray(r["out"], np.float32)
+        assert close(out[:2], ref[:2], 2e-5, 0.0)      # D, sigma: same float operations up to inversion order
+        assert close(out[2:5], ref[2:5], 0.0, 4e-6)    # VNDF sample (unit vector)
+        assert close(out[5], ref[5], 2e-5, 0.0)        # specular p
+
+
+def test_sggx_phase_sampling_matches_reference():
+    """CSGGXPhaseFunction::sampleP: the lobe choice by Fresnel weight, the
+    specular reflection about a VNDF normal or the cosine lobe around one, and
+    the number of draws each lobe takes (3 specular, 5 diffuse)."""
+    order = G["vec2_arg_order"]
+    lobes = set()
+    for r in G["sggx_sample"]:
+        d = list(r["draw_u"])
+        if order == 1:  # glm::vec2(u(), u()) evaluated right to left in the reference build
+            d[1], d[2] = d[2], d[1]
+        out = np.zeros(5, np.float32)
+        L.orc_t_sggx_sample(p(a32(r["S"])), p(a32(r["n"])), r["ior"], p(a32(r["wo"])), p(a32(d)), p(out))
+        assert int(out[4]) == r["draws_used"]
+        lobes.add(r["draws_used"])
+        ref = np.asarray(r["out"], np.float32)
+        assert close(out[:3], ref[:3], 0.0, 2e-5)
+        assert close(out[3], ref[3], 1e-4, 1e-7)
+    assert lobes == {3, 5}
+
+
+def test_get_rotation_matches_reference():
+    """getRotation(n): the rotation taking +Y to n with every entry rounded
+    (the object orientation of the scene description)."""
+    for r in G["get_rotation"]:
+        out = np.zeros(16, np.float32)
+        L.orc_t_get_rotation(p(a32(r["n"])), p(out))
+        assert np.array_equal(out, np.asarray(r["m"], np.float32) + 0.0)

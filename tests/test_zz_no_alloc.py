@@ -54,6 +54,36 @@ def test_static_scratch_matches_allocating_entry_twice():
     sc.close()
 
 
+def test_static_null_stream_orders_calls_on_different_scenes():
+    """Two scenes filtered back to back with stream NULL: the calls run in
+    order on the legacy default stream, so the second call cannot overwrite
+    the shared work list while the first one still reads it."""
+    meshes = [scenes.icosphere(4, 0.05, 1), scenes.icosphere(3, 0.08, 7)]
+    mat = F.material()
+    scs = [F.FilterScene(m, mat) for m in meshes]
+    grids = [sc.grid(scenes.voxel_size_for(m, n)) for sc, m, n in zip(scs, meshes, (40, 36))]
+    prms = [F.params(samples_per_voxel=64, iterations=10, seed=3), F.params(samples_per_voxel=48, iterations=6)]
+    refs, outs = [], []
+    for sc, g, prm in zip(scs, grids, prms):
+        nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+        ro = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+        rw = torch.empty(nvox * 20, dtype=torch.float32, device="cuda")
+        sc.run(g, prm, ro.data_ptr(), rw.data_ptr())
+        refs.append((ro, rw))
+        outs.append((torch.full((nvox * 32,), 0xCD, dtype=torch.uint8, device="cuda"),
+                     torch.full((nvox * 20,), -3.0, dtype=torch.float32, device="cuda")))
+    torch.cuda.synchronize()
+    for _ in range(2):
+        for sc, g, prm, (o, w) in zip(scs, grids, prms, outs):  # no synchronisation between the calls
+            _run_static(sc, g, prm, o, w)
+        torch.cuda.synchronize()
+        for (ro, rw), (o, w) in zip(refs, outs):
+            assert torch.equal(o, ro)
+            assert torch.equal(w, rw)
+    for sc in scs:
+        sc.close()
+
+
 def test_static_scratch_rejects_oversized_grid():
     mesh = scenes.icosphere(2, 0.05, 1)
     sc = F.FilterScene(mesh, F.material())
