@@ -46,6 +46,9 @@ FILTER_CFG = dict(n_quads=500_000, n_branches=20, clustered=0.7, seed=4, grid=25
 EXTEND_BYTES_PER_SEGMENT = 52.0
 SHADOW_BYTES_PER_RAY = 33.0
 FILTER_BYTES_PER_VOXEL = 36.0
+# kernels of one BVH build + shading gather: bounds 2, Morton 1, radix sort 8 passes x 5, triangle gather 1,
+# hierarchy 1, bottom-up 1, emission 1, shading gather 1
+BVH_BUILD_LAUNCHES = 48
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # no measured FP32 figure on this pool
 # media scenes:
 #   extend phase (k_resolve rounds, k_track, k_collide): queue id 4 + ray in/out 64 + throughput in/out 32 + hit record 16 = 116 B per segment
@@ -162,6 +165,16 @@ def _barrier(world: int):
 
 # ------------------------------------------------------------------ workloads
 
+def headline_config(world: int) -> dict:
+    """The headline workload, printed identically by both arms."""
+    c = RENDER_CFG
+    return {"workload": "surface path tracing: 8x8 displaced icospheres (327,680 tris), 512x256 lognormal(0,1.5) env, "
+                        "1024x1024, 64 spp, max depth 8; a step is the BVH build from the resident triangles + the "
+                        "frame",
+            "paths_per_step": c["width"] * c["height"] * c["spp"], "l2": "inputs + wave state larger than L2",
+            "parallelism": f"replicas x{world}"}
+
+
 def render_workload():
     from renderer2_b200 import render_scenes as RS
     from renderer2_b200 import raytracer as R
@@ -218,7 +231,7 @@ def cpu_render_sample(desc, cam, prm, budget_s=15.0, threads=0):
         rate = done / t_work
         rows = max(1, min(int((budget_s - t_work) * rate / W), H - row))
     paths = done * prm.spp
-    return {"value": paths / t_work, "unit": "paths/s", "cores": cores, "kind": "port",
+    return {"value": paths / t_work, "unit": "paths/s", "cores": cores, "kind": "port", "seconds": t_work,
             "sample": f"{done // W} rows x {W} px x {prm.spp} spp at the frame centre ({paths} paths), "
                       f"BVH build included per call"}
 
@@ -273,9 +286,14 @@ def bench_render(args, world, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     st = np.zeros(8)
     stats = []
+    evb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     ev0.record()
-    for _ in range(args.steps):
+    for k in range(args.steps):
+        # one step = BVH build from the resident triangles + the frame (config "BVH build + trace");
         # inputs (BVH 21 MB nodes + 16 MB tris + state ~200 MB per wave) exceed L2; no flush needed
+        evb[k][0].record()
+        sc.rebuild(stream)
+        evb[k][1].record()
         sc.render_device(cam, prm, frame.data_ptr(), stream, stats=st)
         stats.append(st.copy())
     ev1.record()
@@ -283,6 +301,7 @@ def bench_render(args, world, local):
     _barrier(world)
     ck = clocks.stop()
     total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
+    build_ms = float(np.median([a.elapsed_time(b) for a, b in evb]))
     paths = npix * prm.spp
     value = world * paths * args.steps / (total_ms / 1e3)
     st = np.mean(np.array(stats), axis=0)
@@ -332,10 +351,10 @@ def bench_render(args, world, local):
            "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms,
            "scene_build_ms": parts[k][0], "render_and_download_ms": parts[k][1]}
     sc.close()
-    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth)
+    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth) + BVH_BUILD_LAUNCHES
     return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths, tuning=tuning,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
-                desc=desc, cam=cam, prm=prm)
+                bvh_build_ms=build_ms, render_ms=total_ms / args.steps - build_ms, desc=desc, cam=cam, prm=prm)
 
 
 def bench_filter(args, world, local):
@@ -907,12 +926,11 @@ def run_native(args):
         line = {"metric": "paths/s", "value": r["value"], "unit": "paths/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-                "config": {"workload": "surface path tracing: 8x8 displaced icospheres (327,680 tris), 512x256 "
-                                       "lognormal(0,1.5) env, 1024x1024, 64 spp, max depth 8",
-                           "paths_per_step": r["paths"], "segments_per_step": r["segments_per_frame"],
-                           "shadow_rays_per_step": r["shadow_rays_per_frame"],
-                           "l2": "inputs + wave state larger than L2", "parallelism": f"replicas x{world}",
-                           "tuning": r["tuning"]},
+                "config": headline_config(world),
+                "workload_stats": {"segments_per_step": r["segments_per_frame"],
+                                   "shadow_rays_per_step": r["shadow_rays_per_frame"],
+                                   "bvh_build_ms_per_step": r["bvh_build_ms"], "render_ms_per_step": r["render_ms"],
+                                   "tuning": r["tuning"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"]}
         if f is not None:
@@ -935,10 +953,50 @@ def run_native(args):
             line["gpu_launches"] += forest["gpu_launches"]
         if serve is not None:
             line["serving"] = serve
+        line["legs"] = legs_summary(line)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _short(x, nd=4):
+    return None if x is None else float(f"{x:.{nd}g}")
+
+
+def legs_summary(line: dict) -> dict:
+    """One compact entry per leg (value, e2e, roofline fraction, latency), kept at the end of the line."""
+    out = {}
+
+    def leg(name, d, value_key="value"):
+        if not d:
+            return
+        e = {"value": _short(d.get(value_key)), "unit": d.get("unit")}
+        if isinstance(d.get("e2e"), dict):
+            e["e2e"] = _short(d["e2e"].get("value"))
+        rf = d.get("roofline")
+        if isinstance(rf, dict):
+            e["hbm_frac"] = _short(rf.get("frac"), 3)
+            if isinstance(rf.get("fp32"), dict):
+                e["fp32_frac"] = _short(rf["fp32"].get("frac"), 3)
+        for k in ("p50_latency_s", "p99_latency_s", "speedup", "max_rel_err_fp16_vs_fp64"):
+            if k in d:
+                e[k] = _short(d[k], 3)
+        out[name] = e
+
+    leg("headline", line)
+    for k in ("small", "filter", "filter_512", "volume", "volume_batch", "forest"):
+        leg(k, line.get(k))
+    sv = line.get("serving")
+    if sv:
+        out["serving"] = {"paths_per_s": _short(sv["served"]["paths_per_s"]),
+                          "voxels_per_s": _short(sv["served"]["voxels_per_s"]),
+                          "p50_latency_s": _short(sv["served"]["p50_latency_s"], 3),
+                          "p99_latency_s": _short(sv["served"]["p99_latency_s"], 3),
+                          "speedup_makespan": _short(sv.get("speedup_makespan"), 3)}
+        if isinstance(sv.get("roofline"), dict):
+            out["serving"]["hbm_frac"] = _short(sv["roofline"].get("frac"), 3)
+    return out
 
 
 def run_reference(args):
@@ -954,16 +1012,21 @@ def run_reference(args):
     cpu = dict(vals[-1])
     cpu["value"] = v
     line = {"impl": "reference", "metric": "paths/s", "value": v, "unit": "paths/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * float(np.mean([x["seconds"] for x in vals])),  # a bounded sample per step
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
-            "config": {"workload": "surface path tracing: 8x8 displaced icospheres (327,680 tris), 512x256 "
-                                   "lognormal(0,1.5) env, 1024x1024, 64 spp, max depth 8"},
+            "config": headline_config(world),
             "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if not args.skip_filter:
         mesh, mat, fprm, vs = filter_workload()
         fc = cpu_filter_sample(mesh, mat, fprm, vs, budget_s=max(5.0, args.cpu_budget / 2))
         line["filter"] = {"metric": "filtered voxels/s", "value": fc["value"], "unit": "voxels/s", "cpu_baseline": fc}
+    # the CPU arm runs the oracle alone: the GPU library must not be in this process
+    with open("/proc/self/maps") as fh:
+        assert "librenderer2" not in fh.read(), "the reference arm loaded the GPU library"
+    line["native_libraries"] = "oracle only"
     print(json.dumps(line), flush=True)
 
 

@@ -267,6 +267,11 @@ typedef struct r2_render_tuning {
                             remaining boundaries of a path are walked in one pass */
   uint32_t track_blocks; /* media: blocks per SM of the persistent trackers (at most the resident
                             blocks; 0: all of them) */
+  uint32_t track_limit; /* media: bound on the steps of one tracking loop (delta / ratio tracking of
+                           one medium segment; 0: 2^20, the maximum).  A safety bound, not a tuning:
+                           a path or shadow ray whose loop reaches it ends, and the synchronous
+                           render calls return R2_ERR_DEVICE_TIMEOUT with the frame written.  The
+                           reference's loops have no bound (nvdb_medium_impl.hpp:98-136, 155-186). */
 } r2_render_tuning;
 
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA
@@ -314,6 +319,16 @@ r2_status r2_scene_add_mesh_textured(r2_scene* scene, const float* positions, ui
                                      const float* model_to_world, uint32_t mask);
 /* Uploads the scene and builds the BVH (device-resident until destroyed). */
 r2_status r2_scene_commit(r2_scene* scene);
+/* Rebuilds the committed scene's triangle BVH on the device from its resident
+ * triangles, on `stream` (cudaStream_t; NULL: the scene's own stream), and
+ * re-gathers the per-triangle shading data in the new leaf order: the
+ * acceleration-structure build of CHostScene::buildOptixAccel
+ * (raytracer/src/scene/scene.cu:188-256, mesh.cu:140-168) done per frame,
+ * with the geometry already in device memory.  The tree equals the commit's;
+ * nothing is allocated after the first build; the call returns once the
+ * build has finished on the device.  Frames must not be rendering the scene
+ * on another stream meanwhile. */
+r2_status r2_scene_rebuild(r2_scene* scene, void* stream);
 /* Renders one frame into device memory d_rgb (width*height*3 floats).
  * stats_out (nullable, 8 doubles): [0] paths, [1] milliseconds of the frame on
  * the stream, [2] path segments traced, [3] shadow rays traced, [4..7]

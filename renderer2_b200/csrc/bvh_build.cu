@@ -3,7 +3,8 @@
 // 1. triangle boxes and centroids (box midpoints);
 // 2. centroid bounds (block reduction + ordered-integer atomics; min/max are exact);
 // 3. 63-bit Morton codes (21 bits per axis);
-// 4. stable radix sort of (code, triangle) pairs — ties keep triangle order;
+// 4. stable radix sort of (code, triangle) pairs — ties keep triangle order
+//    (radix_sort.cu);
 // 5. Karras hierarchy ("Maximizing Parallelism in the Construction of BVHs,
 //    Octrees, and k-d Trees", HPG 2012) over the sorted codes;
 // 6. bottom-up pass computing boxes and the SAH cost of each node, collapsing a
@@ -12,8 +13,6 @@
 // 7. emission of the 64-byte nodes and the BVH-ordered triangle array.
 // Every step is a pure function of the input, so the host oracle rebuilds the
 // identical tree (same codes, same splits, same collapse decisions).
-#include <cub/device/device_radix_sort.cuh>
-
 #include "bvh_build.cuh"
 
 namespace r2 {
@@ -295,30 +294,22 @@ __global__ void k_init_bounds(uint32_t* cb) {
 
 }  // namespace
 
-// Steps 3-7 over primitive boxes whose centroid bounds are in cb; with
+// Steps 3-7 over primitive boxes whose centroid bounds are in cb_; with
 // d_pos/d_idx the BVH-ordered triangle array is gathered too.
-static void build_from_boxes(const float4* triLo, const float4* triHi, const uint32_t* cbw, uint32_t ntris,
-                             const float* d_pos, const uint32_t* d_idx, DeviceBvh* out, cudaStream_t s) {
+void BvhBuilder::from_boxes(const float4* triLo, const float4* triHi, uint32_t ntris, const float* d_pos,
+                            const uint32_t* d_idx, DeviceBvh* out, cudaStream_t s) {
   const int n = (int)ntris;
-  DBuf<uint64_t> keys(n), keysSorted(n);
-  DBuf<uint32_t> vals(n);
-  out->order.alloc(n);
-  k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo, triHi, ntris, cbw, keys.get(),
-                                           vals.get());
-  size_t tempBytes = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys.get(), keysSorted.get(), vals.get(),
-                                  out->order.get(), n, 0, 63, s);
-  DBuf<uint8_t> temp(tempBytes);
-  R2_CUDA(cub::DeviceRadixSort::SortPairs(temp.get(), tempBytes, keys.get(), keysSorted.get(),
-                                          vals.get(), out->order.get(), n, 0, 63, s));
+  keys_.reserve(n);
+  out->order.reserve(n);
+  k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo, triHi, ntris, cb_.get(), keys_.get(), out->order.get());
+  radix_sort_pairs(keys_.get(), out->order.get(), ntris, 63, &sort_, s);
   out->ntris = ntris;
   if (d_pos) {
-    out->tris.alloc((size_t)3 * n);
-    k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_pos, d_idx, out->order.get(), ntris,
-                                                  out->tris.get());
+    out->tris.reserve((size_t)3 * n);
+    k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_pos, d_idx, out->order.get(), ntris, out->tris.get());
   }
   if (n == 1) {
-    out->nodes.alloc(1);
+    out->nodes.reserve(1);
     out->nnodes = 1;
     out->height = 1;
     k_single_leaf<<<1, 1, 0, s>>>(triLo, triHi, out->nodes.get());
@@ -327,57 +318,66 @@ static void build_from_boxes(const float4* triLo, const float4* triHi, const uin
     return;
   }
   const int ni = n - 1;
-  DBuf<int> left(ni), right(ni), first(ni), last(ni), nodeParent(ni), leafParent(n);
+  left_.reserve(ni); right_.reserve(ni); first_.reserve(ni); last_.reserve(ni);
+  nodeParent_.reserve(ni); leafParent_.reserve(n);
+  leafLo_.reserve(n); leafHi_.reserve(n); nodeLo_.reserve(ni); nodeHi_.reserve(ni);
+  nodeCost_.reserve(ni); nodeHeight_.reserve(ni); collapse_.reserve(ni); flags_.reserve(ni);
   // parents default to -1 so a malformed hierarchy ends the bottom-up walk
-  R2_CUDA(cudaMemsetAsync(nodeParent.get(), 0xFF, sizeof(int) * ni, s));
-  R2_CUDA(cudaMemsetAsync(leafParent.get(), 0xFF, sizeof(int) * n, s));
-  k_karras<<<(ni + 255) / 256, 256, 0, s>>>(keysSorted.get(), n, left.get(), right.get(), first.get(),
-                                            last.get(), nodeParent.get(), leafParent.get());
-  DBuf<float4> leafLo(n), leafHi(n), nodeLo(ni), nodeHi(ni);
-  DBuf<float> nodeCost(ni);
-  DBuf<int> nodeHeight(ni), collapse(ni), flags(ni);
-  R2_CUDA(cudaMemsetAsync(flags.get(), 0, sizeof(int) * ni, s));
-  k_bottom_up<<<(n + 255) / 256, 256, 0, s>>>(n, out->order.get(), triLo, triHi, left.get(),
-                                              right.get(), first.get(), last.get(), nodeParent.get(),
-                                              leafParent.get(), leafLo.get(), leafHi.get(), nodeLo.get(),
-                                              nodeHi.get(), nodeCost.get(), nodeHeight.get(),
-                                              collapse.get(), flags.get());
-  out->nodes.alloc(ni);
+  R2_CUDA(cudaMemsetAsync(nodeParent_.get(), 0xFF, sizeof(int) * ni, s));
+  R2_CUDA(cudaMemsetAsync(leafParent_.get(), 0xFF, sizeof(int) * n, s));
+  k_karras<<<(ni + 255) / 256, 256, 0, s>>>(keys_.get(), n, left_.get(), right_.get(), first_.get(), last_.get(),
+                                            nodeParent_.get(), leafParent_.get());
+  R2_CUDA(cudaMemsetAsync(flags_.get(), 0, sizeof(int) * ni, s));
+  k_bottom_up<<<(n + 255) / 256, 256, 0, s>>>(n, out->order.get(), triLo, triHi, left_.get(), right_.get(),
+                                              first_.get(), last_.get(), nodeParent_.get(), leafParent_.get(),
+                                              leafLo_.get(), leafHi_.get(), nodeLo_.get(), nodeHi_.get(),
+                                              nodeCost_.get(), nodeHeight_.get(), collapse_.get(), flags_.get());
+  out->nodes.reserve(ni);
   out->nnodes = ni;
-  k_emit<<<(ni + 255) / 256, 256, 0, s>>>(n, left.get(), right.get(), first.get(), last.get(),
-                                          nodeParent.get(), leafLo.get(), leafHi.get(), nodeLo.get(),
-                                          nodeHi.get(), nodeHeight.get(), collapse.get(),
-                                          out->nodes.get());
+  k_emit<<<(ni + 255) / 256, 256, 0, s>>>(n, left_.get(), right_.get(), first_.get(), last_.get(),
+                                          nodeParent_.get(), leafLo_.get(), leafHi_.get(), nodeLo_.get(),
+                                          nodeHi_.get(), nodeHeight_.get(), collapse_.get(), out->nodes.get());
   R2_CUDA(cudaGetLastError());
-  int rootHeight = 0, rootCollapse = 0;
-  R2_CUDA(cudaMemcpyAsync(&rootHeight, nodeHeight.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-  R2_CUDA(cudaMemcpyAsync(&rootCollapse, collapse.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  int root[2] = {0, 0};
+  R2_CUDA(cudaMemcpyAsync(&root[0], nodeHeight_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  R2_CUDA(cudaMemcpyAsync(&root[1], collapse_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
   R2_CUDA(cudaStreamSynchronize(s));
-  out->height = rootCollapse ? 1 : (uint32_t)rootHeight;
+  out->height = root[1] ? 1 : (uint32_t)root[0];
   R2_REQUIRE(out->height <= R2_BVH_STACK, R2_ERR_UNSUPPORTED,
              "BVH deeper than the traversal stack (" + std::to_string(out->height) + " levels)");
 }
 
-void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out,
-               cudaStream_t s) {
+void BvhBuilder::build(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s) {
   R2_REQUIRE(ntris > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero triangles");
   R2_REQUIRE(ntris < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 triangles");
-  DBuf<float4> triLo(ntris), triHi(ntris);
-  DBuf<uint32_t> cb(6);
-  k_init_bounds<<<1, 32, 0, s>>>(cb.get());
+  triLo_.reserve(ntris);
+  triHi_.reserve(ntris);
+  cb_.reserve(6);
+  k_init_bounds<<<1, 32, 0, s>>>(cb_.get());
   int nb = (int)std::min<uint32_t>((ntris + 255) / 256, (uint32_t)sm_count() * 8);
-  k_tri_bounds<<<nb, 256, 0, s>>>(d_pos, d_idx, ntris, triLo.get(), triHi.get(), cb.get());
-  build_from_boxes(triLo.get(), triHi.get(), cb.get(), ntris, d_pos, d_idx, out, s);
+  k_tri_bounds<<<nb, 256, 0, s>>>(d_pos, d_idx, ntris, triLo_.get(), triHi_.get(), cb_.get());
+  from_boxes(triLo_.get(), triHi_.get(), ntris, d_pos, d_idx, out, s);
+}
+
+void BvhBuilder::build_boxes(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out,
+                             cudaStream_t s) {
+  R2_REQUIRE(nboxes > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero boxes");
+  R2_REQUIRE(nboxes < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 boxes");
+  cb_.reserve(6);
+  k_init_bounds<<<1, 32, 0, s>>>(cb_.get());
+  int nb = (int)std::min<uint32_t>((nboxes + 255) / 256, (uint32_t)sm_count() * 8);
+  k_box_bounds<<<nb, 256, 0, s>>>(d_lo, d_hi, nboxes, cb_.get());
+  from_boxes(d_lo, d_hi, nboxes, nullptr, nullptr, out, s);
+}
+
+void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s) {
+  BvhBuilder b;
+  b.build(d_pos, d_idx, ntris, out, s);
 }
 
 void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s) {
-  R2_REQUIRE(nboxes > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero boxes");
-  R2_REQUIRE(nboxes < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 boxes");
-  DBuf<uint32_t> cb(6);
-  k_init_bounds<<<1, 32, 0, s>>>(cb.get());
-  int nb = (int)std::min<uint32_t>((nboxes + 255) / 256, (uint32_t)sm_count() * 8);
-  k_box_bounds<<<nb, 256, 0, s>>>(d_lo, d_hi, nboxes, cb.get());
-  build_from_boxes(d_lo, d_hi, cb.get(), nboxes, nullptr, nullptr, out, s);
+  BvhBuilder b;
+  b.build_boxes(d_lo, d_hi, nboxes, out, s);
 }
 
 }  // namespace r2

@@ -1,6 +1,7 @@
 // GPU LBVH builder (host interface).  See bvh_build.cu.
 #pragma once
 #include "bvh.h"
+#include "radix_sort.cuh"
 #include "runtime.h"
 
 namespace r2 {
@@ -27,6 +28,27 @@ struct DeviceBvh {
     v.ntris = ntris;
     return v;
   }
+};
+
+// Builds BVHs with device scratch kept between builds (grown on demand), so
+// that rebuilding a BVH of the same size allocates nothing and the output's
+// buffers (and the pointers taken from them) stay in place.  The host waits
+// for the build once, at its end, to check the tree height against the
+// traversal stack.
+class BvhBuilder {
+ public:
+  void build(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s);
+  void build_boxes(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s);
+
+ private:
+  void from_boxes(const float4* lo, const float4* hi, uint32_t n, const float* d_pos, const uint32_t* d_idx,
+                  DeviceBvh* out, cudaStream_t s);
+  DBuf<float4> triLo_, triHi_, leafLo_, leafHi_, nodeLo_, nodeHi_;
+  DBuf<uint64_t> keys_;
+  DBuf<int> left_, right_, first_, last_, nodeParent_, leafParent_, nodeHeight_, collapse_, flags_;
+  DBuf<float> nodeCost_;
+  DBuf<uint32_t> cb_;
+  RadixSortScratch sort_;
 };
 
 // Builds the BVH over triangles (d_pos: 3 floats per vertex, d_idx: 3 per

@@ -97,6 +97,14 @@ r2_status r2_scene_commit(r2_scene* scene) {
   R2_API_END
 }
 
+r2_status r2_scene_rebuild(r2_scene* scene, void* stream) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(scene->impl->committed(), R2_ERR_INVALID_ARGUMENT, "scene not committed");
+  scene->impl->rebuild((cudaStream_t)stream);
+  R2_API_END
+}
+
 r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* d_rgb,
                            void* stream, double* stats_out) {
   R2_API_BEGIN

@@ -90,7 +90,7 @@ struct MediumView {
 };
 
 constexpr int kMediumCodeBase = -1000000;  // closest-hit code of medium m: kMediumCodeBase - m
-constexpr int kMaxTrackingSteps = 1 << 20; // bound of every tracking loop (path ends when reached)
+constexpr int kMaxTrackingSteps = 1 << 20; // largest bound of a tracking loop (the path ends when reached)
 
 // ---------------------------------------------------------------- payload decode / interpolation
 // SFilteredData (include/filtering/filtered_data.hpp:10-31; decode 63-89;
@@ -355,13 +355,14 @@ R2_HD void fill_event(MediumEvent* ev, const Ray& w, const FData& fd) {
 R2_HD float inv_majorant(const MediumView& m) { return 1.0f / (m.filterRenderRatio / m.invMaxDensity); }
 
 // CNVDBMedium::sampleInternal (delta tracking against the global majorant),
-// model-space ray; *err is set when the step bound is reached.
-R2_HD V3 medium_sample_internal(const MediumView& m, const Ray& rayModel, RngStream& rng, MediumEvent* ev, int* err) {
+// model-space ray; *err is set when `limit` steps are reached.
+R2_HD V3 medium_sample_internal(const MediumView& m, const Ray& rayModel, RngStream& rng, MediumEvent* ev, int* err,
+                                int limit) {
   Ray ray = ray_transform2(rayModel, m.modelToIndex);
   const float invMax = inv_majorant(m);
   if (!(invMax < INFINITY)) return v3(1.0f);  // empty grid: no collision possible
   float t = 0.0f;
-  for (int it = 0; it < kMaxTrackingSteps; ++it) {
+  for (int it = 0; it < limit; ++it) {
     t -= log_r2(1.0f - rng.next()) * invMax / m.sigmaT;
     if (t >= ray.tmax) return v3(1.0f);
     const V3 pt = ray.o + ray.d * t;
@@ -379,13 +380,14 @@ R2_HD V3 medium_sample_internal(const MediumView& m, const Ray& rayModel, RngStr
 
 // CNVDBMedium::sampleDDA (brick-grid majorants; mip starts at 3, +0.25 per
 // step, -2 after a tentative collision).
-R2_HD V3 medium_sample_dda(const MediumView& m, const Ray& rayModel, RngStream& rng, MediumEvent* ev, int* err) {
+R2_HD V3 medium_sample_dda(const MediumView& m, const Ray& rayModel, RngStream& rng, MediumEvent* ev, int* err,
+                           int limit) {
   Ray iray = ray_transform2(rayModel, m.unitToScaled);
   const V3 ri = v3(1.0f / iray.d.x, 1.0f / iray.d.y, 1.0f / iray.d.z);
   float t = 0.0f;
   float tau = -log_r2(1.0f - rng.next());
   float mip = 3.0f;
-  for (int it = 0; it < kMaxTrackingSteps; ++it) {
+  for (int it = 0; it < limit; ++it) {
     if (!(t < iray.tmax)) return v3(1.0f);
     const V3 curr = iray.o + iray.d * t;
     const int mi = (int)roundf(mip);
@@ -421,12 +423,12 @@ R2_HD V3 medium_sample_dda(const MediumView& m, const Ray& rayModel, RngStream& 
 }
 
 // CNVDBMedium::trInternal (ratio tracking with Russian roulette).
-R2_HD float medium_tr_internal(const MediumView& m, const Ray& rayModel, RngStream& rng, int* err) {
+R2_HD float medium_tr_internal(const MediumView& m, const Ray& rayModel, RngStream& rng, int* err, int limit) {
   const Ray ray = ray_transform2(rayModel, m.modelToIndex);
   const float invMax = inv_majorant(m);
   if (!(invMax < INFINITY)) return 1.0f;
   float tr = 1.0f, t = 0.0f;
-  for (int it = 0; it < kMaxTrackingSteps; ++it) {
+  for (int it = 0; it < limit; ++it) {
     t -= log_r2(1.0f - rng.next()) * invMax / m.sigmaT;
     if (t >= ray.tmax) return tr;
     const float d = medium_density(m, ray.o + ray.d * t);
@@ -442,14 +444,14 @@ R2_HD float medium_tr_internal(const MediumView& m, const Ray& rayModel, RngStre
 }
 
 // CNVDBMedium::trDDA.
-R2_HD float medium_tr_dda(const MediumView& m, const Ray& rayModel, RngStream& rng, int* err) {
+R2_HD float medium_tr_dda(const MediumView& m, const Ray& rayModel, RngStream& rng, int* err, int limit) {
   const Ray iray = ray_transform2(rayModel, m.unitToScaled);
   const V3 ri = v3(1.0f / iray.d.x, 1.0f / iray.d.y, 1.0f / iray.d.z);
   float tr = 1.0f, t = 0.0f;
   const float volMajorant = 1.0f / inv_majorant(m);
   float tau = -log_r2(1.0f - rng.next());
   float mip = 3.0f;
-  for (int it = 0; it < kMaxTrackingSteps; ++it) {
+  for (int it = 0; it < limit; ++it) {
     if (!(t < iray.tmax)) return tr;
     const V3 curr = iray.o + iray.d * t;
     const int mi = (int)roundf(mip);
@@ -484,10 +486,11 @@ R2_HD float medium_tr_dda(const MediumView& m, const Ray& rayModel, RngStream& r
 
 // CMediumInstance::sample: world-space ray; returns the albedo weight (1 when
 // the ray passes) and, on a collision, the event in world space.
-R2_HD V3 instance_sample(const MediumView& m, const Ray& rayWorld, bool dda, RngStream& rng, MediumEvent* ev, int* err) {
+R2_HD V3 instance_sample(const MediumView& m, const Ray& rayWorld, bool dda, RngStream& rng, MediumEvent* ev, int* err,
+                         int limit) {
   const Ray rm = ray_transform2(rayWorld, m.worldToModel);
   ev->hit = 0;
-  const V3 a = dda ? medium_sample_dda(m, rm, rng, ev, err) : medium_sample_internal(m, rm, rng, ev, err);
+  const V3 a = dda ? medium_sample_dda(m, rm, rng, ev, err, limit) : medium_sample_internal(m, rm, rng, ev, err, limit);
   if (ev->hit) {
     ev->pos = xform_point(m.modelToWorld, ev->pos);
     ev->normal = normalize(xform_vector(m.modelToWorld, ev->normal));
@@ -496,9 +499,9 @@ R2_HD V3 instance_sample(const MediumView& m, const Ray& rayWorld, bool dda, Rng
 }
 
 // CMediumInstance::tr.
-R2_HD float instance_tr(const MediumView& m, const Ray& rayWorld, bool dda, RngStream& rng, int* err) {
+R2_HD float instance_tr(const MediumView& m, const Ray& rayWorld, bool dda, RngStream& rng, int* err, int limit) {
   const Ray rm = ray_transform2(rayWorld, m.worldToModel);
-  return dda ? medium_tr_dda(m, rm, rng, err) : medium_tr_internal(m, rm, rng, err);
+  return dda ? medium_tr_dda(m, rm, rng, err, limit) : medium_tr_internal(m, rm, rng, err, limit);
 }
 
 // CNVDBMedium::moveToVoxelBorder (model space): the origin moves to just
@@ -680,11 +683,11 @@ struct TrackState {
 // Start of sampleInternal / sampleDDA (kSample) or trInternal / trDDA for a
 // world-space ray through the instance.
 template <bool kDDA, bool kSample>
-R2_HD int track_init(const MediumView& m, const Ray& rayWorld, TrackState* s) {
+R2_HD int track_init(const MediumView& m, const Ray& rayWorld, TrackState* s, int limit) {
   const Ray rm = ray_transform2(rayWorld, m.worldToModel);
   s->t = 0.0f;
   s->tr = 1.0f;
-  s->steps = 0;
+  s->steps = kMaxTrackingSteps - limit;  // track_step ends the loop at kMaxTrackingSteps: after `limit` steps
   if (kDDA) {
     const Ray iray = ray_transform2(rm, m.unitToScaled);
     s->o = iray.o;

@@ -1,0 +1,23 @@
+// Stable LSD radix sort of (uint64 key, uint32 value) pairs on the device.
+// See radix_sort.cu.
+#pragma once
+#include "runtime.h"
+
+namespace r2 {
+
+// Device scratch of the sort, grown on demand and kept between sorts.
+struct RadixSortScratch {
+  DBuf<uint64_t> keysAlt;
+  DBuf<uint32_t> valsAlt;
+  DBuf<uint32_t> hist;      // digit-major block histograms, then their exclusive prefix
+  DBuf<uint32_t> partials;  // per-partition sums of the prefix pass
+  void reserve(uint32_t n);
+};
+
+// Sorts n pairs ascending by the low `bits` bits of the keys (1..64), stably:
+// equal keys keep their input order.  In place: keys/vals hold the sorted
+// pairs when the stream reaches the end of the sort.
+void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, RadixSortScratch* scratch,
+                      cudaStream_t s);
+
+}  // namespace r2

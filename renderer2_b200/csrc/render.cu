@@ -539,7 +539,7 @@ __device__ __forceinline__ void resolve_path(const RenderLaunch& L, uint32_t p, 
         if (kInline) {
           RngStream rs = rng_stream(path_pixel(L, p), L.seed, path_sample(L, p), L.bounce,
                                     kPurposeMedium + (uint32_t)j);
-          T = T * instance_sample(S.media[segMed], seg, L.dda != 0, rs, &ev, &err);
+          T = T * instance_sample(S.media[segMed], seg, L.dda != 0, rs, &ev, &err, (int)L.trackLimit);
           evMed = segMed;
           if (err) dead = true;
         } else {  // queue the segment; the path waits at this boundary hit
@@ -712,7 +712,8 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
             s.rng = rng_resume(path_pixel(L, op), L.seed, path_sample(L, op), L.bounce,
                                kPurposeShadowTr + (owner & 1u), jm.y);
           }
-          const int st = track_init<kDDA, kSample>(L.scene.media[med], make_ray(xyz(jo), xyz(jd), jo.w), &s);
+          const int st = track_init<kDDA, kSample>(L.scene.media[med], make_ray(xyz(jo), xyz(jd), jo.w), &s,
+                                                     (int)L.trackLimit);
           if (st == kTrackRunning) {
             active = true;
           } else if (kSample) {
@@ -1097,7 +1098,7 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
     }
     if (cur >= 0 && hitM == cur) {
       if (kInline) {
-        tr *= instance_tr(S.media[cur], make_ray(off, dir, best), L.dda != 0, rs, &err);
+        tr *= instance_tr(S.media[cur], make_ray(off, dir, best), L.dda != 0, rs, &err, (int)L.trackLimit);
       } else {
         const uint32_t k2 = warp_reserve(jobCounter);
         L.st.jO[k2] = f4(off, best);

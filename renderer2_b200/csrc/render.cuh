@@ -128,6 +128,7 @@ struct RenderLaunch {
   uint32_t travRefill;  // finished lanes of a warp that trigger a refill (tuning, 1..32)
   uint32_t mediaRounds; // queued medium-boundary rounds per bounce (tuning, 1..kMaxMediaRounds)
   uint32_t trackBlocks; // persistent tracker blocks per SM (tuning; 0: every resident block)
+  uint32_t trackLimit;  // steps of one tracking loop after which the path ends (1..kMaxTrackingSteps)
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

@@ -200,53 +200,72 @@ void RenderScene::add_medium(const char* path, const float* sigmaA, const float*
   committed_ = false;
 }
 
+namespace {
+// Per BVH-order triangle: vertex normals, material, texture coordinates and
+// opacity map of the scene-order triangle order[i].
+__global__ void k_gather_shading(const uint32_t* __restrict__ order, uint32_t n, const uint32_t* __restrict__ idx,
+                                 const float* __restrict__ nrm, const uint32_t* __restrict__ matIn,
+                                 const float* __restrict__ uv, const int* __restrict__ alphaIn,
+                                 float4* __restrict__ triN, uint32_t* __restrict__ triMat,
+                                 float2* __restrict__ triUV, int* __restrict__ triAlpha) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t p = order[i];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const uint32_t v = idx[3 * p + k];
+    triN[3 * i + k] = make_float4(nrm[3 * v], nrm[3 * v + 1], nrm[3 * v + 2], 0.0f);
+    if (triUV) triUV[3 * i + k] = make_float2(uv[2 * v], uv[2 * v + 1]);
+  }
+  triMat[i] = matIn[p];
+  if (triAlpha) triAlpha[i] = alphaIn[p];
+}
+}  // namespace
+
+void RenderScene::rebuild(cudaStream_t s) {
+  if (!s) s = ctx_.stream;
+  const uint32_t nt = (uint32_t)(hIdx_.size() / 3);
+  R2_REQUIRE(nt > 0 && dIdx_.get(), R2_ERR_INVALID_ARGUMENT, "scene has no committed triangles");
+  builder_.build(dPos_.get(), dIdx_.get(), nt, &bvh_, s);
+  triN_.reserve((size_t)3 * nt);
+  triMat_.reserve(nt);
+  if (anyUV_) triUV_.reserve((size_t)3 * nt);
+  if (dTriAlphaIn_.get()) triAlpha_.reserve(nt);
+  k_gather_shading<<<(nt + 255) / 256, 256, 0, s>>>(bvh_.order.get(), nt, dIdx_.get(), dNrm_.get(), dTriMatIn_.get(),
+                                                    anyUV_ ? dUV_.get() : nullptr, dTriAlphaIn_.get(), triN_.get(),
+                                                    triMat_.get(), anyUV_ ? triUV_.get() : nullptr,
+                                                    dTriAlphaIn_.get() ? triAlpha_.get() : nullptr);
+  R2_CUDA(cudaGetLastError());
+  const BvhAlpha alpha = view_.bvh.alpha;
+  view_.bvh = bvh_.view();
+  view_.bvh.alpha = alpha;
+}
+
 void RenderScene::commit() {
   R2_REQUIRE(env_.W > 0, R2_ERR_INVALID_CONFIG, "scene has no environment map");
   cudaStream_t s = ctx_.stream;
   uint32_t nt = (uint32_t)(hIdx_.size() / 3);
   memset(&view_, 0, sizeof(view_));
   if (nt > 0) {
-    DBuf<float> dpos;
-    DBuf<uint32_t> didx;
-    dpos.upload(hPos_.data(), hPos_.size(), s);
-    didx.upload(hIdx_.data(), hIdx_.size(), s);
-    build_bvh(dpos.get(), didx.get(), nt, &bvh_, s);
-    std::vector<uint32_t> order(nt);
-    bvh_.order.download(order.data(), nt, s);
-    R2_CUDA(cudaStreamSynchronize(s));
-    std::vector<float4> triN((size_t)3 * nt);
-    std::vector<uint32_t> triMat(nt);
-    for (uint32_t i = 0; i < nt; ++i) {
-      uint32_t p = order[i];
-      for (int k = 0; k < 3; ++k) {
-        uint32_t v = hIdx_[3 * p + k];
-        triN[3 * i + k] = make_float4(hNrm_[3 * v], hNrm_[3 * v + 1], hNrm_[3 * v + 2], 0.0f);
+    dPos_.upload(hPos_.data(), hPos_.size(), s);
+    dNrm_.upload(hNrm_.data(), hNrm_.size(), s);
+    dIdx_.upload(hIdx_.data(), hIdx_.size(), s);
+    dTriMatIn_.upload(hTriMat_.data(), hTriMat_.size(), s);
+    bool anyAlpha = false;
+    if (anyUV_) {  // texture coordinates and opacity maps per triangle
+      dUV_.upload(hUV_.data(), hUV_.size(), s);
+      std::vector<int> alphaIn(nt);
+      for (uint32_t t = 0; t < nt; ++t) {
+        alphaIn[t] = hMats_[hTriMat_[t]].tex[3];
+        anyAlpha = anyAlpha || alphaIn[t] >= 0;
       }
-      triMat[i] = hTriMat_[p];
+      if (anyAlpha) dTriAlphaIn_.upload(alphaIn.data(), alphaIn.size(), s);
     }
-    triN_.upload(triN.data(), triN.size(), s);
-    triMat_.upload(triMat.data(), triMat.size(), s);
-    view_.bvh = bvh_.view();
-    if (anyUV_) {  // texture coordinates and opacity maps per BVH-order triangle
-      std::vector<float2> triUV((size_t)3 * nt);
-      std::vector<int> triAlpha(nt);
-      bool anyAlpha = false;
-      for (uint32_t i = 0; i < nt; ++i) {
-        const uint32_t p = order[i];
-        for (int k = 0; k < 3; ++k) {
-          const uint32_t v = hIdx_[3 * p + k];
-          triUV[3 * i + k] = make_float2(hUV_[2 * v], hUV_[2 * v + 1]);
-        }
-        triAlpha[i] = hMats_[hTriMat_[p]].tex[3];
-        anyAlpha = anyAlpha || triAlpha[i] >= 0;
-      }
-      triUV_.upload(triUV.data(), triUV.size(), s);
-      view_.triUV = triUV_.get();
-      if (anyAlpha) {
-        triAlpha_.upload(triAlpha.data(), triAlpha.size(), s);
-        view_.bvh.alpha.alphaTex = triAlpha_.get();
-        view_.bvh.alpha.uv = triUV_.get();
-      }
+    rebuild(s);
+    if (anyUV_) view_.triUV = triUV_.get();
+    if (anyAlpha) {
+      view_.bvh.alpha.alphaTex = triAlpha_.get();
+      view_.bvh.alpha.uv = triUV_.get();
     }
     view_.triN = triN_.get();
     view_.triMat = triMat_.get();
@@ -412,6 +431,7 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   L.travRefill = tuning_.trav_refill;
   L.mediaRounds = tuning_.media_rounds;
   L.trackBlocks = tuning_.track_blocks;
+  L.trackLimit = tuning_.track_limit ? tuning_.track_limit : (uint32_t)kMaxTrackingSteps;
   L.bound = ctx.bound.get();
   return L;
 }
@@ -520,10 +540,11 @@ RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const 
 
 void RenderScene::set_tuning(const r2_render_tuning& t) {
   R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31) &&
-                 t.media_rounds <= kMaxMediaRounds && t.track_blocks <= 64,
+                 t.media_rounds <= kMaxMediaRounds && t.track_blocks <= 64 &&
+                 t.track_limit <= (uint32_t)kMaxTrackingSteps,
              R2_ERR_INVALID_ARGUMENT,
              "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31, media_rounds <= 32, "
-             "track_blocks <= 64)");
+             "track_blocks <= 64, track_limit <= 2^20)");
   tuning_ = t;
 }
 
@@ -558,7 +579,7 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     return best / ((float)S * (float)npix);
   };
   r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths,
-                       kDefaultMediaRounds, 0};
+                       kDefaultMediaRounds, 0, saved.track_limit};  // the step bound is kept, never tuned
   try {
     R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
     time_wave(cur);  // warm-up

@@ -87,6 +87,12 @@ class RenderScene {
   void add_medium(const char* path, const float* sigmaA, const float* sigmaS, const float* pos,
                   const float* orientation, const float* scaling, uint32_t mask, bool hg = false, float g = 0.0f);
   void commit();
+  // Rebuilds the triangle BVH from the device-resident triangles and
+  // re-gathers the per-triangle shading data in the new order, on stream s
+  // (the scene's own when null): the per-frame BVH build of a scene whose
+  // geometry stays on the device.  Same tree as the commit's; allocates
+  // nothing after the first build; waits for the build's end.
+  void rebuild(cudaStream_t s);
   bool committed() const { return committed_; }
   bool has_media() const { return !media_.empty(); }
   // One frame: spp / wave_spp waves accumulated into d_frame (W*H*3 floats,
@@ -143,6 +149,11 @@ class RenderScene {
   DeviceBvh mediaBvh_;
   EnvHost env_;
   DeviceBvh bvh_;
+  BvhBuilder builder_;
+  // device-resident triangle inputs in scene order (kept for rebuilds)
+  DBuf<float> dPos_, dNrm_, dUV_;
+  DBuf<uint32_t> dIdx_, dTriMatIn_;
+  DBuf<int> dTriAlphaIn_;
   DBuf<float4> triN_;
   DBuf<uint32_t> triMat_;
   DBuf<Material> mats_;
@@ -150,7 +161,7 @@ class RenderScene {
   DBuf<float4> envTex_;
   DBuf<float> envBuf_;
   SceneView view_;
-  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
+  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
 };
 
 // Frames of several committed scenes rendered by one captured CUDA graph: the

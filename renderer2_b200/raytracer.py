@@ -47,8 +47,10 @@ SPHERE, CIRCLE = 0, 1
 class Tuning(C.Structure):
     """Launch tuning (r2_render_tuning); 0 fields select the defaults; images never depend on it."""
     _fields_ = [("track_steps", C.c_uint32), ("trav_visits", C.c_uint32), ("trav_refill", C.c_uint32),
-                ("wave_paths", C.c_uint32), ("media_rounds", C.c_uint32), ("track_blocks", C.c_uint32)]
-    NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths", "media_rounds", "track_blocks")
+                ("wave_paths", C.c_uint32), ("media_rounds", C.c_uint32), ("track_blocks", C.c_uint32),
+                ("track_limit", C.c_uint32)]
+    NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths", "media_rounds", "track_blocks",
+             "track_limit")
 
     def as_tuple(self):
         return tuple(getattr(self, n) for n in self.NAMES)
@@ -57,8 +59,9 @@ class Tuning(C.Structure):
         return dict(zip(self.NAMES, self.as_tuple()))
 
 
-def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0, media_rounds=0, track_blocks=0) -> Tuning:
-    return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds, track_blocks)
+def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0, media_rounds=0, track_blocks=0,
+           track_limit=0) -> Tuning:
+    return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds, track_blocks, track_limit)
 
 
 class Scene:
@@ -129,6 +132,10 @@ class Scene:
 
     def commit(self):
         N.check(N.lib.r2_scene_commit(self.handle))
+
+    def rebuild(self, stream: int = 0):
+        """Rebuild the triangle BVH on the device from the resident triangles (waits for the build)."""
+        N.check(N.lib.r2_scene_rebuild(self.handle, C.c_void_p(stream or None)))
 
     def render_device(self, cam: Camera, prm: RenderParams, d_rgb: int, stream: int = 0, stats=None):
         st = np.zeros(8, np.float64)

@@ -98,12 +98,14 @@ def _oracle(mesh, mat, prm, g, m2w=I43):
     return O.filter_voxels(mesh, O.material_from(mat), m2w, O.grid_from(g), O.params_from(prm))
 
 
-@pytest.mark.parametrize("mesh_kind", ["ico4", "foliage", "single", "pair", "dupes"])
+@pytest.mark.parametrize("mesh_kind", ["ico4", "foliage", "foliage_big", "single", "pair", "dupes"])
 def test_bvh_bit_exact(mesh_kind):
     if mesh_kind == "ico4":
         mesh = scenes.icosphere(4, 0.05, 1)
     elif mesh_kind == "foliage":
         mesh = scenes.foliage(3000, 5, 0.7, 4)
+    elif mesh_kind == "foliage_big":  # 80k triangles: many sort blocks and two scan partitions per pass
+        mesh = scenes.foliage(40000, 20, 0.7, 9)
     elif mesh_kind == "single":
         mesh = F.Mesh(np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32), np.array([[0, 1, 2]], np.uint32),
                       np.tile(np.array([0, 0, 1], np.float32), (3, 1)))

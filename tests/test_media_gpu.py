@@ -154,3 +154,30 @@ def test_medium_tracking_tuning_never_changes_the_frame(lods):
     assert t.track_steps >= 1 and 1 <= t.media_rounds <= 32
     assert np.array_equal(sc.render(cam, prm), ref)
     sc.close()
+
+
+@pytest.mark.parametrize("dda", [False, True])
+def test_tracking_step_bound_ends_paths_with_timeout_status(lods, dda):
+    """A tracking loop that reaches its step bound ends its path instead of
+    spinning: the kernels return, count the paths they ended, and the
+    synchronous render reports R2_ERR_DEVICE_TIMEOUT with that count (no hang,
+    no trap).  The bound is lowered from 2^20 to 2 steps through the launch
+    tuning; the context stays usable and the default bound renders the same
+    frame as before."""
+    desc = _desc(lods[0])
+    cam = R.camera(32, 28, 50.0, (0.3, 0.6, 3.2), (0.0, 0.0, 0.0), (0, 1, 0))
+    sc = RS.build_scene(desc)
+    prm = R.params(2, 8, 5, brick_grid=dda)
+    ref = sc.render(cam, prm)
+    for rounds in (1, 32):  # the persistent tracker, and the queued rounds walked to the end
+        sc.set_tuning(R.tuning(media_rounds=rounds, track_limit=2))
+        with pytest.raises(N.R2Error) as e:
+            sc.render(cam, prm)
+        assert e.value.name == "R2_ERR_DEVICE_TIMEOUT"
+        ended = int(str(e.value).split(":", 1)[1].split()[0])
+        assert 0 < ended <= 2 * 32 * 28 * 2 * 8 * 3, str(e.value)
+    sc.set_tuning(R.tuning())
+    assert np.array_equal(sc.render(cam, prm), ref)
+    with pytest.raises(N.R2Error):
+        sc.set_tuning(R.tuning(track_limit=(1 << 20) + 1))
+    sc.close()

@@ -115,6 +115,24 @@ def test_device_entry_matches_host_entry_and_is_deterministic():
     assert st[0] == 40 * 30 * 4
 
 
+def test_device_rebuild_gives_the_same_frame():
+    """r2_scene_rebuild rebuilds the triangle BVH from the resident triangles
+    and re-gathers the shading data: the frames before and after, on the
+    scene's stream and on a caller's stream, are bit-identical."""
+    desc, _ = RS.icosphere_grid_scene()
+    cam = R.camera(48, 40, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+    sc = RS.build_scene(desc)
+    prm = R.params(2, 8, 4)
+    a = sc.render(cam, prm)
+    sc.rebuild()
+    b = sc.render(cam, prm)
+    s = torch.cuda.Stream()
+    sc.rebuild(s.cuda_stream)
+    c = sc.render(cam, prm)
+    sc.close()
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+
+
 def test_render_rejects_bad_arguments():
     desc, _ = RS.icosphere_scene()
     sc = RS.build_scene(desc)
