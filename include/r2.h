@@ -96,6 +96,14 @@ typedef struct r2_filter_params {
   float alpha;                 /* Alpha */
   uint32_t clip_rays;          /* ClipRays */
   uint32_t seed;               /* Philox key word 1 */
+  /* Build options without a counterpart in the reference (0: the reference's
+   * plain mean of buildS).  sggx_projection 1: the mean SGGX matrix of every
+   * filtered voxel is eigendecomposed in FP64 (Jacobi rotations) and replaced
+   * by V diag(max(w, sggx_floor * w_max)) V^T, so that near-planar voxels
+   * (one eigenvalue near 1, two near 0) keep det(S) > 0 and a finite
+   * D(w) = 1/(pi sqrt|det S| (w^T S^-1 w)^2) (sggx_phase_function.hpp:107-117). */
+  uint32_t sggx_projection;
+  float sggx_floor;            /* relative eigenvalue floor of the projection (>= 0, < 1) */
 } r2_filter_params;
 
 /* Grid of one LOD: COpenvdbBackend::setupGrid (openvdb_backend.cpp:71-106). */
@@ -163,6 +171,15 @@ r2_status r2_filter_scene_grid(const r2_filter_scene* scene, float voxel_size,
 r2_status r2_filter_scene_run(r2_filter_scene* scene, const r2_filter_grid* grid,
                               const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
                               uint16_t* d_fp16, void* stream, double* stats_out);
+/* The same with the FP64 eigendecomposition of each voxel's SGGX matrix:
+ * d_eig (device, 12 floats per voxel) receives w0 >= w1 >= w2, then the unit
+ * eigenvectors v0, v1, v2 (3 floats each, largest-magnitude entry
+ * non-negative) of the mean S before any projection; zeros for voxels without
+ * hits.  The rest of the output is that of r2_filter_scene_run, bit for bit.
+ * The reference stores S and never decomposes it. */
+r2_status r2_filter_scene_run_eig(r2_filter_scene* scene, const r2_filter_grid* grid,
+                                  const r2_filter_params* params, r2_voxel* d_out, float* d_wide,
+                                  uint16_t* d_fp16, float* d_eig, void* stream, double* stats_out);
 /* The same LOD through the counting build of the sampling kernel (same
  * payloads, slower): counts_out[0] rays traced, [1] inner BVH nodes visited,
  * [2] triangles tested -- the operation counts behind the filter's

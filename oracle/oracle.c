@@ -766,6 +766,57 @@ typedef struct {
   const oi_alpha* alpha; /* null: no opacity map */
 } job_t;
 
+/* Symmetric 3x3 eigendecomposition by cyclic Jacobi rotations (Golub and Van
+ * Loan, Matrix Computations, section 8.5): each rotation in the plane (p, q)
+ * with tan = sign(theta) / (|theta| + sqrt(theta^2 + 1)),
+ * theta = (a_qq - a_pp) / (2 a_pq), zeroes a_pq; sweeps stop once the
+ * off-diagonal sum of squares is below double rounding of the diagonal's. */
+void orc_sym3_eig(const double* S6, double* w, double* V) {
+  double a[3][3] = {{S6[0], S6[3], S6[4]}, {S6[3], S6[1], S6[5]}, {S6[4], S6[5], S6[2]}};
+  double v[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  static const int P[3] = {0, 0, 1}, Q[3] = {1, 2, 2};
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+    const double dg = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+    if (!(off > 4.93e-32 * dg)) break;
+    for (int r = 0; r < 3; ++r) {
+      const int p = P[r], q = Q[r];
+      if (a[p][q] == 0.0) continue;
+      const double th = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+      const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+      const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+      for (int k = 0; k < 3; ++k) {
+        const double x = a[k][p], y = a[k][q];
+        a[k][p] = c * x - sn * y;
+        a[k][q] = sn * x + c * y;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double x = a[p][k], y = a[q][k];
+        a[p][k] = c * x - sn * y;
+        a[q][k] = sn * x + c * y;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double x = v[k][p], y = v[k][q];
+        v[k][p] = c * x - sn * y;
+        v[k][q] = sn * x + c * y;
+      }
+    }
+  }
+  int idx[3] = {0, 1, 2};
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2 - i; ++j)
+      if (a[idx[j]][idx[j]] < a[idx[j + 1]][idx[j + 1]]) { const int t = idx[j]; idx[j] = idx[j + 1]; idx[j + 1] = t; }
+  for (int c = 0; c < 3; ++c) {
+    const int src = idx[c];
+    w[c] = a[src][src];
+    int m = 0;
+    for (int k = 1; k < 3; ++k)
+      if (fabs(v[k][src]) > fabs(v[m][src])) m = k;
+    const double sg = v[m][src] < 0.0 ? -1.0 : 1.0;
+    for (int k = 0; k < 3; ++k) V[3 * k + c] = sg * v[k][src];
+  }
+}
+
 static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
   const orc_grid* g = J->g;
   const orc_filter_params* p = J->p;
@@ -867,6 +918,18 @@ static void filter_voxel(const job_t* J, uint64_t vid, double* w) {
   double inv = 1.0 / hits;
   w[0] = density;
   for (int k = 0; k < 6; ++k) w[1 + k] = S[k] * inv;
+  if (p->sggx_projection) { /* V diag(max(w, floor * w0)) V^T */
+    double ev[3], V[9], l[3];
+    orc_sym3_eig(&w[1], ev, V);
+    const double lo = (double)p->sggx_floor * (ev[0] > 0.0 ? ev[0] : 0.0);
+    for (int k = 0; k < 3; ++k) l[k] = ev[k] > lo ? ev[k] : lo;
+    static const int rr[6] = {0, 1, 2, 0, 0, 1}, cc[6] = {0, 1, 2, 1, 2, 2};
+    for (int e = 0; e < 6; ++e) {
+      double acc = 0.0;
+      for (int k = 0; k < 3; ++k) acc += l[k] * V[3 * rr[e] + k] * V[3 * cc[e] + k];
+      w[1 + e] = acc;
+    }
+  }
   for (int k = 0; k < 3; ++k) {
     w[7 + k] = dif[k] * inv;
     w[10 + k] = spe[k] * inv;

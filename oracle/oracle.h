@@ -62,6 +62,8 @@ typedef struct orc_filter_params {
   float alpha;
   uint32_t clip_rays;
   uint32_t seed;
+  uint32_t sggx_projection; /* 1: S replaced by its eigen-projection with eigenvalues >= sggx_floor * max */
+  float sggx_floor;
 } orc_filter_params;
 
 typedef struct orc_grid {
@@ -106,6 +108,11 @@ int orc_filter_tex(const float* positions, uint32_t nverts, const uint32_t* idx,
                    const orc_texture* normal, const orc_texture* alpha, const float* obj_model_to_world,
                    const orc_grid* g, const orc_filter_params* p, uint32_t lod, uint64_t v0, uint64_t v1,
                    double* wide_out, uint8_t* compact_out, int threads);
+
+/* Eigendecomposition of the symmetric 3x3 S (xx yy zz xy xz yz) in double by
+ * cyclic Jacobi rotations: w descending, V row-major (V[3*row + col]) with
+ * unit eigenvector columns, each with its largest-magnitude entry >= 0. */
+void orc_sym3_eig(const double* S6, double* w3, double* V9);
 
 /* Encode a wide (double) record to the 32-byte payload (FP64 arithmetic). */
 void orc_encode(const double* wide, uint8_t* out32);

@@ -48,7 +48,8 @@ class MaterialMaps(C.Structure):
 class FilterParams(C.Structure):
     _fields_ = [("min_voxel_size", C.c_float), ("lods", C.c_uint32), ("samples_per_voxel", C.c_uint32),
                 ("sigma_t", C.c_float), ("estimation_iterations", C.c_uint32), ("alpha", C.c_float),
-                ("clip_rays", C.c_uint32), ("seed", C.c_uint32)]
+                ("clip_rays", C.c_uint32), ("seed", C.c_uint32), ("sggx_projection", C.c_uint32),
+                ("sggx_floor", C.c_float)]
 
 
 class FilterGrid(C.Structure):
@@ -84,6 +85,7 @@ def _load():
         "r2_filter_scene_create_textured": (C.c_int, [P, u32, P, u32, P, P, P, P, P, P]),
         "r2_filter_scene_grid": (C.c_int, [P, f32, P]),
         "r2_filter_scene_run": (C.c_int, [P, P, P, P, P, P, P, P]),
+        "r2_filter_scene_run_eig": (C.c_int, [P, P, P, P, P, P, P, P, P]),
         "r2_filter_scene_count": (C.c_int, [P, P, P, P, P]),
         "r2_filter_scene_bvh": (C.c_int, [P, P, sz, P, sz, P, P]),
         "r2_scene_create": (C.c_int, [P]),

@@ -131,6 +131,16 @@ r2_status r2_filter_scene_run(r2_filter_scene* scene, const r2_filter_grid* grid
   R2_API_END
 }
 
+r2_status r2_filter_scene_run_eig(r2_filter_scene* scene, const r2_filter_grid* grid, const r2_filter_params* params,
+                                  r2_voxel* d_out, float* d_wide, uint16_t* d_fp16, float* d_eig, void* stream,
+                                  double* stats_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && grid && params && d_out && d_eig, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->run(*grid, *params, 0, d_out, d_wide, d_fp16, (cudaStream_t)stream, stats_out, nullptr, nullptr,
+                   nullptr, d_eig);
+  R2_API_END
+}
+
 r2_status r2_filter_scene_bvh(const r2_filter_scene* scene, int32_t* nodes, size_t node_words, uint32_t* tri_order,
                               size_t ntris, uint32_t* nnodes_out, uint32_t* height_out) {
   R2_API_BEGIN

@@ -112,6 +112,31 @@ __device__ __forceinline__ void write_empty(const FilterLaunch& L, size_t vid) {
     uint4* f = reinterpret_cast<uint4*>(L.fp16 + vid * 8);
     *f = make_uint4(0, 0, 0, 0);
   }
+  if (L.eig) {
+    float4* e = reinterpret_cast<float4*>(L.eig + vid * 12);
+    e[0] = e[1] = e[2] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+}
+
+// FP64 eigendecomposition of the voxel's mean SGGX matrix (compensated FP32
+// sums promoted to double), written to L.eig (lanes 0..11, one float each),
+// and, with the projection on, the projected matrix in wv[1..6].  Every lane
+// computes the same values.  Out of line: only this tail uses double registers.
+__device__ __noinline__ void sggx_eig_tail(const FilterLaunch& L, uint32_t vid, int lane, const CSum* S,
+                                           uint32_t hits, float* wv) {
+  double m[6], w[3], V[3][3];
+  const double inv = 1.0 / (double)hits;
+  for (int k = 0; k < 6; ++k) m[k] = ((double)S[k].s + (double)S[k].c) * inv;
+  sym3_eig_jacobi(m, w, V);
+  if (L.eig && lane < 12) {
+    const double v = lane < 3 ? w[lane] : V[(lane - 3) % 3][(lane - 3) / 3];
+    L.eig[(size_t)vid * 12 + lane] = (float)v;
+  }
+  if (L.project) {
+    double P[6];
+    sym3_project(w, V, (double)L.floor, P);
+    for (int k = 0; k < 6; ++k) wv[1 + k] = (float)P[k];
+  }
 }
 
 __global__ void __launch_bounds__(256) k_filter_classify(FilterLaunch L) {
@@ -159,7 +184,9 @@ __device__ __forceinline__ CSum warp_csum(CSum v) {
 // latency bound, and the extra warps hide more than the few spilled values of
 // the shading tail cost (measured on the 256^3 filter: 96 registers and 5
 // blocks 18.6 M voxels/s, 64 and 8 blocks 21.6 M).
-template <bool kCount>
+// kEig: the build with the FP64 eigendecomposition tail (eigen output or
+// projection requested); the default build carries none of its code.
+template <bool kCount, bool kEig>
 __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLaunch L) {
   __shared__ float ts[kSampleWarps][kFilterMaxSpv];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -305,8 +332,10 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
       wv[17] = (float)hits;
       wv[18] = avgDist;
       wv[19] = cvalue(cr) * inv;
+      if (kEig) sggx_eig_tail(L, vid, lane, S, hits, wv);
     } else {
       wv[16] = 1.0f;
+      if (kEig && L.eig && lane < 12) L.eig[(size_t)vid * 12 + lane] = 0.0f;
     }
     if (lane == 0) {
       write_voxel(L.out, vid, hits > 0 ? encode_voxel(wv) : empty_voxel());
@@ -352,17 +381,26 @@ void launch_filter_classify(const FilterLaunch& L, cudaStream_t s) {
   R2_CUDA(cudaGetLastError());
 }
 
-void launch_filter_sample(const FilterLaunch& L, cudaStream_t s) {
-  static int perSm[2] = {0, 0};
-  const int c = L.ops ? 1 : 0;
-  if (perSm[c] == 0) {
+template <bool kCount, bool kEig>
+static void launch_sample(const FilterLaunch& L, cudaStream_t s) {
+  static int perSm = 0;
+  if (perSm == 0) {
     int n = 0;
-    if (c) R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<true>, kSampleWarps * 32, 0));
-    else R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<false>, kSampleWarps * 32, 0));
-    perSm[c] = n < 1 ? 1 : n;
+    R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<kCount, kEig>, kSampleWarps * 32, 0));
+    perSm = n < 1 ? 1 : n;
   }
-  if (c) k_filter_sample<true><<<sm_count() * perSm[c], kSampleWarps * 32, 0, s>>>(L);
-  else k_filter_sample<false><<<sm_count() * perSm[c], kSampleWarps * 32, 0, s>>>(L);
+  k_filter_sample<kCount, kEig><<<sm_count() * perSm, kSampleWarps * 32, 0, s>>>(L);
+}
+
+void launch_filter_sample(const FilterLaunch& L, cudaStream_t s) {
+  const bool eig = L.eig || L.project;
+  if (L.ops) {
+    if (eig) launch_sample<true, true>(L, s);
+    else launch_sample<true, false>(L, s);
+  } else {
+    if (eig) launch_sample<false, true>(L, s);
+    else launch_sample<false, false>(L, s);
+  }
   R2_CUDA(cudaGetLastError());
 }
 

@@ -19,6 +19,8 @@ struct FilterLaunch {
   V3 voxelSize;       // (worldBB.max - worldBB.min) / numVoxels
   uint32_t spv, iters, clip, seed, lod;
   float sigma_t, alpha;
+  uint32_t project;          // FP64 eigendecomposition + projection of S (r2_filter_params::sggx_projection)
+  float floor;               // relative eigenvalue floor of the projection
   BvhView bvh;
   const float4* triN;        // 3 per BVH-order triangle: model-space vertex normals
   const uint32_t* triMat;    // per BVH-order triangle: material index
@@ -26,6 +28,7 @@ struct FilterLaunch {
   r2_voxel* out;
   float* wide;               // nullable
   uint16_t* fp16;            // nullable
+  float* eig;                // nullable: 12 floats per voxel, eigenvalues and eigenvectors of the mean S
   uint32_t* work;            // candidate voxel ids
   uint32_t* counters;        // [0] candidates, [1] queue head
   unsigned long long* ops;   // nullable: counting build, [0] rays, [1] inner nodes visited, [2] triangles tested

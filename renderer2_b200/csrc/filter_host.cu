@@ -153,8 +153,10 @@ r2_filter_grid FilterScene::grid(float voxelSize) const {
 
 void FilterScene::run(const r2_filter_grid& g, const r2_filter_params& p, uint32_t lod, r2_voxel* d_out,
                       float* d_wide, uint16_t* d_fp16, cudaStream_t s, double* stats,
-                      uint32_t* d_work, uint32_t* d_counters, unsigned long long* d_ops) {
+                      uint32_t* d_work, uint32_t* d_counters, unsigned long long* d_ops, float* d_eig) {
   R2_REQUIRE(d_out, R2_ERR_INVALID_ARGUMENT, "null output");
+  R2_REQUIRE(p.sggx_projection <= 1u && p.sggx_floor >= 0.0f && p.sggx_floor < 1.0f, R2_ERR_INVALID_ARGUMENT,
+             "sggx_projection must be 0 or 1 and sggx_floor in [0, 1)");
   R2_REQUIRE(p.samples_per_voxel >= 1 && p.samples_per_voxel <= kFilterMaxSpv, R2_ERR_UNSUPPORTED,
              "samples_per_voxel must be in [1, 1024]");
   R2_REQUIRE(p.sigma_t > 0.0f, R2_ERR_INVALID_ARGUMENT, "sigma_t must be positive");
@@ -185,6 +187,9 @@ void FilterScene::run(const r2_filter_grid& g, const r2_filter_params& p, uint32
   L.lod = lod;
   L.sigma_t = p.sigma_t;
   L.alpha = p.alpha;
+  L.project = p.sggx_projection;
+  L.floor = p.sggx_floor;
+  L.eig = d_eig;
   L.bvh = bvh_.view();
   if (triUV_.get()) {
     L.triUV = triUV_.get();

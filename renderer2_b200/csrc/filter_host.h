@@ -27,9 +27,11 @@ class FilterScene {
   // (nx*ny*nz words) and counters (2 words).  d_ops (nullable, 3 zeroed words)
   // selects the counting build of the sampling kernel, which adds the rays
   // traced, inner nodes visited and triangles tested.
+  // d_eig (nullable): 12 floats per voxel, the FP64 eigendecomposition of the mean S.
   void run(const r2_filter_grid& g, const r2_filter_params& p, uint32_t lod, r2_voxel* d_out,
            float* d_wide, uint16_t* d_fp16, cudaStream_t s, double* stats,
-           uint32_t* d_work = nullptr, uint32_t* d_counters = nullptr, unsigned long long* d_ops = nullptr);
+           uint32_t* d_work = nullptr, uint32_t* d_counters = nullptr, unsigned long long* d_ops = nullptr,
+           float* d_eig = nullptr);
 
   const DeviceBvh& bvh() const { return bvh_; }
   cudaStream_t stream() const { return stream_; }

@@ -114,6 +114,87 @@ R2_HD r2_voxel encode_voxel(const float* w) {
   return v;
 }
 
+// Eigendecomposition of the symmetric 3x3 matrix S (xx yy zz xy xz yz) in
+// double precision by cyclic Jacobi rotations (Jacobi 1846; Golub and Van
+// Loan, Matrix Computations, 4th ed., section 8.5): S = V diag(w) V^T with
+// w[0] >= w[1] >= w[2] and V's columns (V[row][col]) orthonormal
+// eigenvectors, each with its largest-magnitude entry non-negative.  A
+// rotation in the plane (p, q) zeroes the entry a_pq; sweeps repeat until the
+// off-diagonal mass is below double rounding of the diagonal (four sweeps at
+// most for a 3x3 in practice; eight are allowed).  Near-planar SGGX matrices
+// (one eigenvalue near 1, two near 0) are resolved to full double accuracy
+// because rotations, not a characteristic polynomial, find the eigenvalues.
+R2_HD void sym3_eig_jacobi(const double S[6], double w[3], double V[3][3]) {
+  double a[3][3] = {{S[0], S[3], S[4]}, {S[3], S[1], S[5]}, {S[4], S[5], S[2]}};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) V[r][c] = r == c ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+    const double diag = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+    if (!(off > 4.93e-32 * diag)) break;
+    for (int r = 0; r < 3; ++r) {
+      const int p = r == 2 ? 1 : 0, q = r == 0 ? 1 : 2;  // (0,1), (0,2), (1,2)
+      const double apq = a[p][q];
+      if (apq == 0.0) continue;
+      const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+      const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+      const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+      for (int k = 0; k < 3; ++k) {  // A J
+        const double akp = a[k][p], akq = a[k][q];
+        a[k][p] = c * akp - sn * akq;
+        a[k][q] = sn * akp + c * akq;
+      }
+      for (int k = 0; k < 3; ++k) {  // J^T (A J)
+        const double apk = a[p][k], aqk = a[q][k];
+        a[p][k] = c * apk - sn * aqk;
+        a[q][k] = sn * apk + c * aqk;
+      }
+      for (int k = 0; k < 3; ++k) {  // V J
+        const double vkp = V[k][p], vkq = V[k][q];
+        V[k][p] = c * vkp - sn * vkq;
+        V[k][q] = sn * vkp + c * vkq;
+      }
+    }
+  }
+  for (int k = 0; k < 3; ++k) w[k] = a[k][k];
+  for (int i = 0; i < 2; ++i)  // descending order, columns follow
+    for (int j = 0; j < 2 - i; ++j)
+      if (w[j] < w[j + 1]) {
+        const double tw = w[j];
+        w[j] = w[j + 1];
+        w[j + 1] = tw;
+        for (int k = 0; k < 3; ++k) {
+          const double tv = V[k][j];
+          V[k][j] = V[k][j + 1];
+          V[k][j + 1] = tv;
+        }
+      }
+  for (int c = 0; c < 3; ++c) {
+    int m = 0;
+    for (int k = 1; k < 3; ++k)
+      if (fabs(V[k][c]) > fabs(V[m][c])) m = k;
+    if (V[m][c] < 0.0)
+      for (int k = 0; k < 3; ++k) V[k][c] = -V[k][c];
+  }
+}
+
+// Projection of S onto the SGGX matrices with every eigenvalue at least
+// floor * (largest eigenvalue), floor >= 0: V diag(max(w, floor w0)) V^T.
+// With floor 0 it is the projection onto the positive semidefinite cone; with
+// floor > 0 it regularises near-planar voxels so that det(S) > 0 and the
+// phase function's inverse(S) stays finite.
+R2_HD void sym3_project(const double w[3], const double V[3][3], double floor, double S[6]) {
+  double l[3];
+  const double lo = floor * (w[0] > 0.0 ? w[0] : 0.0);
+  for (int k = 0; k < 3; ++k) l[k] = w[k] > lo ? w[k] : lo;
+  const int rr[6] = {0, 1, 2, 0, 0, 1}, cc[6] = {0, 1, 2, 1, 2, 2};
+  for (int e = 0; e < 6; ++e) {
+    double acc = 0.0;
+    for (int k = 0; k < 3; ++k) acc += l[k] * V[rr[e]][k] * V[cc[e]][k];
+    S[e] = acc;
+  }
+}
+
 // Payload of a voxel without hits (mesh_filter.hpp:112-119): zeros, ior = 1.
 R2_HD r2_voxel empty_voxel() {
   r2_voxel v;

@@ -44,7 +44,9 @@ def material(diffuse=(0.8, 0.8, 0.8), specular=(1.0, 1.0, 1.0), alpha=0.3, ior=1
 
 
 def params(samples_per_voxel=64, iterations=10, sigma_t=10.0, alpha=0.1, clip_rays=True, seed=0,
-           min_voxel_size=1.0, lods=1):
+           min_voxel_size=1.0, lods=1, sggx_projection=False, sggx_floor=0.0):
+    """Filter parameters (r2_filter_params); sggx_projection replaces each voxel's mean S by its FP64
+    eigendecomposition with eigenvalues floored at sggx_floor times the largest."""
     p = N.FilterParams()
     p.min_voxel_size = float(min_voxel_size)
     p.lods = int(lods)
@@ -54,6 +56,8 @@ def params(samples_per_voxel=64, iterations=10, sigma_t=10.0, alpha=0.1, clip_ra
     p.alpha = float(alpha)
     p.clip_rays = 1 if clip_rays else 0
     p.seed = int(seed)
+    p.sggx_projection = 1 if sggx_projection else 0
+    p.sggx_floor = float(sggx_floor)
     return p
 
 
@@ -108,6 +112,12 @@ class FilterScene:
                                           C.c_void_p(stream or None), N.ptr(st) if stats is not None else None))
         if stats is not None:
             stats[:] = st[:3]
+
+    def run_eig(self, grid, prm, d_out: int, d_eig: int, d_wide: int = 0, stream: int = 0):
+        """The same LOD with the FP64 eigendecomposition of each voxel's mean S in d_eig (12 floats per voxel)."""
+        N.check(N.lib.r2_filter_scene_run_eig(self.handle, C.byref(grid), C.byref(prm), C.c_void_p(d_out),
+                                              C.c_void_p(d_wide or None), None, C.c_void_p(d_eig),
+                                              C.c_void_p(stream or None), None))
 
     def count(self, grid, prm, d_out: int):
         """Counting build of the same LOD: (rays traced, inner nodes visited, triangles tested)."""

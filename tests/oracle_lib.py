@@ -39,7 +39,8 @@ class Material(C.Structure):
 class Params(C.Structure):
     _fields_ = [("min_voxel_size", C.c_float), ("lods", C.c_uint32), ("samples_per_voxel", C.c_uint32),
                 ("sigma_t", C.c_float), ("estimation_iterations", C.c_uint32), ("alpha", C.c_float),
-                ("clip_rays", C.c_uint32), ("seed", C.c_uint32)]
+                ("clip_rays", C.c_uint32), ("seed", C.c_uint32), ("sggx_projection", C.c_uint32),
+                ("sggx_floor", C.c_float)]
 
 
 def _load():

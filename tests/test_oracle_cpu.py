@@ -209,3 +209,28 @@ def test_oracle_filter_small_scene_properties():
     assert np.allclose(tr, 1 + 2 * 0.3, atol=1e-9)  # trace(buildS) = 1 + 2a for unit normals
     assert np.allclose(np.linalg.norm(wide[h, 13:16], axis=1), 1.0, atol=1e-12)
     assert (comp[~h, :28] == 0).all()
+
+
+def test_oracle_jacobi_eigendecomposition():
+    """orc_sym3_eig (cyclic Jacobi in FP64) against LAPACK's symmetric solver,
+    on random and near-planar SGGX matrices (eigenvalues 1, a, a with a down to 1e-8)."""
+    import ctypes as C
+    O.lib.orc_sym3_eig.argtypes = [C.c_void_p] * 3
+    rng = np.random.default_rng(7)
+    for i in range(2000):
+        if i % 2:
+            m = rng.normal(size=(3, 3))
+            S = m @ m.T
+        else:
+            n = rng.normal(size=3)
+            n /= np.linalg.norm(n)
+            a = 10.0 ** rng.uniform(-8, 0)
+            S = np.outer(n, n) + a * (np.eye(3) - np.outer(n, n))
+        S6 = np.ascontiguousarray([S[0, 0], S[1, 1], S[2, 2], S[0, 1], S[0, 2], S[1, 2]])
+        w, V = np.zeros(3), np.zeros(9)
+        O.lib.orc_sym3_eig(S6.ctypes.data_as(C.c_void_p), w.ctypes.data_as(C.c_void_p), V.ctypes.data_as(C.c_void_p))
+        V = V.reshape(3, 3)
+        ref = np.linalg.eigvalsh(S)[::-1]
+        assert np.all(np.abs(w - ref) <= 1e-13 * ref[0])
+        assert np.abs(V @ np.diag(w) @ V.T - S).max() <= 1e-13 * ref[0]
+        assert np.abs(V.T @ V - np.eye(3)).max() <= 1e-13

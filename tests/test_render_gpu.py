@@ -155,7 +155,7 @@ def test_launch_tuning_never_changes_the_frame():
     ref = sc.render(cam, prm)
     for visits, refill, wave in [(1, 1, 0), (3, 32, 96 * 80), (1000, 5, 2 * 96 * 80), (64, 16, 1 << 24)]:
         sc.set_tuning(R.tuning(trav_visits=visits, trav_refill=refill, wave_paths=wave))
-        assert sc.get_tuning().as_tuple() == (0, visits, refill, wave, 0, 0)
+        assert sc.get_tuning().as_tuple() == (0, visits, refill, wave, 0, 0, 0)
         assert sc.wave_samples(cam, prm) == (2 if wave != 96 * 80 else 1)
         assert np.array_equal(sc.render(cam, prm), ref), (visits, refill, wave)
     t = sc.autotune(cam, prm)
