@@ -701,7 +701,7 @@ static uint8_t q8(double v) {
 }
 static double clampd(double x, double lo, double hi) { return x < lo ? lo : (x > hi ? hi : x); }
 
-static uint16_t half_bits(float f) {
+uint16_t oi_half_bits(float f) {
   uint32_t x;
   memcpy(&x, &f, 4);
   uint32_t sign = (x >> 16) & 0x8000u, mag = x & 0x7FFFFFFFu;
@@ -741,7 +741,7 @@ void orc_encode(const double* w, uint8_t* out) {
   uint16_t nn[3];
   for (int k = 0; k < 3; ++k) nn[k] = q16(clampd(M16 * 0.5 * (w[13 + k] / nl + 1.0), 0.0, M16));
   memcpy(out + 22, nn, 6);
-  uint16_t h = half_bits((float)w[16]);
+  uint16_t h = oi_half_bits((float)w[16]);
   memcpy(out + 28, &h, 2);
 }
 

@@ -114,6 +114,16 @@ int orc_filter_tex(const float* positions, uint32_t nverts, const uint32_t* idx,
  * unit eigenvector columns, each with its largest-magnitude entry >= 0. */
 void orc_sym3_eig(const double* S6, double* w3, double* V9);
 
+/* CHostBrickGrid construction (brick_oracle.c) from the grid's densities
+ * (nx*ny*nz floats, x fastest, inactive voxels 0): n_bricks in nb (3); with
+ * ind null only nb is computed.  ind, range: nb products; mip0..2:
+ * (nb >> (i+1)) products; atlas: capacity nb*8 per axis (zeroed here); ad:
+ * atlas dims after the z prune; count: bricks with an atlas slot; minmaj: the
+ * grid's density min and max.  Returns -1 beyond 1023 bricks per axis. */
+int orc_build_bricks(const float* dens, int nx, int ny, int nz, uint32_t* nb, uint32_t* ind, uint32_t* range,
+                     uint32_t* mip0, uint32_t* mip1, uint32_t* mip2, uint8_t* atlas, uint32_t* ad,
+                     uint64_t* count, float* minmaj);
+
 /* Encode a wide (double) record to the 32-byte payload (FP64 arithmetic). */
 void orc_encode(const double* wide, uint8_t* out32);
 

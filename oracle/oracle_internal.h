@@ -104,7 +104,12 @@ void oi_nvdb_free(oi_nvdb* g);
 void oi_nvdb_value(const oi_nvdb* g, int x, int y, int z, uint8_t out[32]);
 float oi_nvdb_max_density(const oi_nvdb* g);
 
-/* ".brickgrid" file of the library. */
+/* IEEE binary16 conversions: float to half bits, round to nearest even (as
+ * glm::detail::toFloat16), and half bits to float (exact). */
+uint16_t oi_half_bits(float f);
+float oi_half_to_float(uint16_t h);
+
+/* ".brickgrid" file (the reference's cereal PortableBinary layout). */
 typedef struct {
   uint32_t nb[3], ad[3], count;
   float minorant, majorant;

@@ -506,7 +506,7 @@ typedef struct {
   float ior;
 } fdat;
 
-static float half_to_float(uint16_t h) {
+float oi_half_to_float(uint16_t h) {
   const int e = (h >> 10) & 0x1F, m = h & 0x3FF;
   float v;
   if (e == 0) v = ldexpf((float)m, -24);
@@ -531,7 +531,7 @@ static fdat fd_decode(const uint8_t* c) {
   d.diffuse = mul3s(F3((float)c[16], (float)c[17], (float)c[18]), inv8);
   d.specular = mul3s(F3((float)c[19], (float)c[20], (float)c[21]), inv8);
   d.normal = norm3(sub3(mul3s(mul3s(F3((float)nn[0], (float)nn[1], (float)nn[2]), 2.0f), inv16), F3(1.0f, 1.0f, 1.0f)));
-  d.ior = half_to_float(ior);
+  d.ior = oi_half_to_float(ior);
   return d;
 }
 
@@ -603,7 +603,7 @@ static float brick_majorant(const med_t* m, f3 ip, int mip) {
   uint32_t w;
   if (mip <= 0) w = brick_word(m->b.range, nx, ny, nz, bx, by, bz);
   else w = brick_word(m->b.mips[mip - 1], nx >> mip, ny >> mip, nz >> mip, bx >> mip, by >> mip, bz >> mip);
-  return half_to_float((uint16_t)(w >> 16));
+  return oi_half_to_float((uint16_t)(w >> 16));
 }
 static float brick_density(const med_t* m, f3 ip) {
   const int ix = (int)floorf(ip.x), iy = (int)floorf(ip.y), iz = (int)floorf(ip.z);
@@ -616,7 +616,7 @@ static float brick_density(const med_t* m, f3 ip) {
   uint8_t v = 0;
   if (ax < (int)m->b.ad[0] && ay < (int)m->b.ad[1] && az < (int)m->b.ad[2])
     v = m->b.atlas[(size_t)ax + (size_t)ay * m->b.ad[0] + (size_t)az * m->b.ad[0] * m->b.ad[1]];
-  const float lo = half_to_float((uint16_t)(rw & 0xFFFFu)), hi = half_to_float((uint16_t)(rw >> 16));
+  const float lo = oi_half_to_float((uint16_t)(rw & 0xFFFFu)), hi = oi_half_to_float((uint16_t)(rw >> 16));
   return lo + (float)v * (1.0f / 255.0f) * (hi - lo);
 }
 static float step_dda(f3 pos, f3 inv, int mip) {

@@ -11,9 +11,15 @@
  * reads leaves through a flat block index instead, so the two lookups are
  * independent.
  *
- * Brick grid: the library's own ".brickgrid" format (magic "R2BRICK1", brick
- * counts, atlas size, brick count, minorant, majorant, then the indirection,
- * range, three mip and atlas arrays).
+ * Brick grid: the reference's ".brickgrid" file, a cereal 1.3.2
+ * PortableBinary archive of CHostBrickGrid (serialization.cpp:37-40): one
+ * byte 1 (little-endian payload), the mat4 transform (16 floats), n_bricks
+ * (3 uint32), min_maj (2 floats), brick_counter (uint64), then indirection,
+ * range (uint32) and atlas (uint8), each a Buf3D (stride as 3 uint32, then a
+ * std::vector: uint64 element count and the elements), and range_mipmaps (a
+ * uint64 count of uint32 Buf3Ds).  orc_build_bricks restates the
+ * construction (host_grid_brick.cpp:61-152, common.hpp:23-53) one brick
+ * after the other.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -127,29 +133,37 @@ float oi_nvdb_max_density(const oi_nvdb* g) {
   return m;
 }
 
+/* One Buf3D: its stride and a vector of `esize`-byte elements, whose count
+ * must equal the stride's product; *out receives a malloc'd copy. */
+static int read_buf3d(FILE* f, uint32_t stride[3], size_t esize, void** out) {
+  uint64_t n = 0;
+  if (fread(stride, 4, 3, f) != 3 || fread(&n, 8, 1, f) != 1) return 0;
+  if (n != (uint64_t)stride[0] * stride[1] * stride[2] || n > ((uint64_t)1 << 34)) return 0;
+  *out = malloc(n ? n * esize : 1);
+  return *out && fread(*out, esize, n, f) == n;
+}
+
 int oi_bricks_read(const char* path, oi_bricks* b) {
   memset(b, 0, sizeof(*b));
   FILE* f = fopen(path, "rb");
   if (!f) return -1;
-  char magic[8];
-  int ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "R2BRICK1", 8) == 0;
-  ok = ok && fread(b->nb, 4, 3, f) == 3 && fread(b->ad, 4, 3, f) == 3 && fread(&b->count, 4, 1, f) == 1;
-  ok = ok && fread(&b->minorant, 4, 1, f) == 1 && fread(&b->majorant, 4, 1, f) == 1;
-  for (int k = 0; ok && k < 3; ++k) ok = b->nb[k] > 0 && b->nb[k] < 1024 && (b->nb[k] & 7u) == 0 && b->ad[k] <= 8192;
-  if (ok) {
-    const size_t nB = (size_t)b->nb[0] * b->nb[1] * b->nb[2];
-    b->ind = (uint32_t*)malloc(4 * nB);
-    b->range = (uint32_t*)malloc(4 * nB);
-    ok = b->ind && b->range && fread(b->ind, 4, nB, f) == nB && fread(b->range, 4, nB, f) == nB;
-    for (int i = 0; ok && i < 3; ++i) {
-      const size_t m = (size_t)(b->nb[0] >> (i + 1)) * (b->nb[1] >> (i + 1)) * (b->nb[2] >> (i + 1));
-      b->mips[i] = (uint32_t*)malloc(4 * (m ? m : 1));
-      ok = b->mips[i] && fread(b->mips[i], 4, m, f) == m;
-    }
-    const size_t an = (size_t)b->ad[0] * b->ad[1] * b->ad[2];
-    b->atlas = (uint8_t*)malloc(an ? an : 1);
-    ok = ok && b->atlas && fread(b->atlas, 1, an, f) == an;
-  }
+  uint8_t little = 0;
+  float transform[16];
+  uint64_t count = 0;
+  uint32_t st[3];
+  int ok = fread(&little, 1, 1, f) == 1 && little == 1 && fread(transform, 4, 16, f) == 16;
+  ok = ok && fread(b->nb, 4, 3, f) == 3 && fread(&b->minorant, 4, 1, f) == 1 && fread(&b->majorant, 4, 1, f) == 1;
+  ok = ok && fread(&count, 8, 1, f) == 1;
+  for (int k = 0; ok && k < 3; ++k) ok = b->nb[k] > 0 && b->nb[k] < 1024 && (b->nb[k] & 7u) == 0;
+  b->count = (uint32_t)count;
+  ok = ok && read_buf3d(f, st, 4, (void**)&b->ind) && st[0] == b->nb[0] && st[1] == b->nb[1] && st[2] == b->nb[2];
+  ok = ok && read_buf3d(f, st, 4, (void**)&b->range) && st[0] == b->nb[0] && st[1] == b->nb[1] && st[2] == b->nb[2];
+  ok = ok && read_buf3d(f, b->ad, 1, (void**)&b->atlas);
+  uint64_t nm = 0;
+  ok = ok && fread(&nm, 8, 1, f) == 1 && nm == 3;
+  for (int i = 0; ok && i < 3; ++i)
+    ok = read_buf3d(f, st, 4, (void**)&b->mips[i]) && st[0] == b->nb[0] >> (i + 1) && st[1] == b->nb[1] >> (i + 1) &&
+         st[2] == b->nb[2] >> (i + 1);
   fclose(f);
   if (!ok) {
     oi_bricks_free(b);

@@ -157,6 +157,29 @@ __global__ void k_brick_atlas(const r2_voxel* __restrict__ d, int nx, int ny, in
   }
 }
 
+// Density min / max over the grid's voxels as the grid stores them
+// (getMinorantMajorant, host_grid_brick.cpp:44-57): ordered words [0] min, [1] max.
+__global__ void __launch_bounds__(256) k_density_minmax(const r2_voxel* __restrict__ d, int nx, int ny, int nz,
+                                                        uint32_t* __restrict__ mm) {
+  const size_t n = (size_t)nx * ny * nz;
+  float lo = INFINITY, hi = -INFINITY;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % (size_t)nx), y = (int)((i / (size_t)nx) % (size_t)ny), z = (int)(i / ((size_t)nx * ny));
+    const float v = grid_density(d, x, y, z, nx, ny, nz);
+    lo = fminf(lo, v);
+    hi = fmaxf(hi, v);
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    lo = fminf(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, off));
+    hi = fmaxf(hi, __shfl_xor_sync(0xFFFFFFFFu, hi, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&mm[0], f2ord(lo));
+    atomicMax(&mm[1], f2ord(hi));
+  }
+}
+
 __global__ void k_init_minmax(uint32_t* c) {
   c[0] = 0;
   c[1] = 0xFFFFFFFFu;
@@ -250,8 +273,8 @@ void build_brick_grid(const r2_voxel* d_dense, const int32_t nv[3], cudaStream_t
   R2_CUDA(cudaMemcpyAsync(&lastFlag, nonconst.get() + nB - 1, 4, cudaMemcpyDeviceToHost, s));
   R2_CUDA(cudaStreamSynchronize(s));
   g->brickCount = lastSlot + lastFlag;
-  // atlas pruned in z to ceil(count / (bx*by)) brick slices (host_grid_brick.cpp:126)
-  const uint32_t zSlices = (uint32_t)ceil((double)g->brickCount / (double)(nb[0] * nb[1]));
+  // atlas pruned in z to round(ceil(count / float(bx*by))) brick slices (host_grid_brick.cpp:126)
+  const uint32_t zSlices = (uint32_t)roundf(ceilf((float)g->brickCount / (float)(nb[0] * nb[1])));
   g->atlasDim[0] = nb[0] * kBrickSize;
   g->atlasDim[1] = nb[1] * kBrickSize;
   g->atlasDim[2] = zSlices * kBrickSize;
@@ -262,6 +285,14 @@ void build_brick_grid(const r2_voxel* d_dense, const int32_t nv[3], cudaStream_t
   k_brick_atlas<<<std::max(ab, 1), 512, 0, s>>>(d_dense, nv[0], nv[1], nv[2], nb[0], nb[1], nb[2], range.get(),
                                                  nonconst.get(), slot.get(), indirection.get(), atlas.get(),
                                                  g->atlasDim[0], g->atlasDim[1]);
+  DBuf<uint32_t> mm(2);
+  const uint32_t mmInit[2] = {0xFFFFFFFFu, 0u};
+  R2_CUDA(cudaMemcpyAsync(mm.get(), mmInit, sizeof(mmInit), cudaMemcpyHostToDevice, s));
+  const size_t nvox = (size_t)nv[0] * nv[1] * nv[2];
+  const int mb = (int)std::min<size_t>((nvox + 255) / 256, (size_t)sm_count() * 8);
+  k_density_minmax<<<std::max(mb, 1), 256, 0, s>>>(d_dense, nv[0], nv[1], nv[2], mm.get());
+  uint32_t mmHost[2];
+  R2_CUDA(cudaMemcpyAsync(mmHost, mm.get(), sizeof(mmHost), cudaMemcpyDeviceToHost, s));
   g->range.resize(nB);
   g->indirection.resize(nB);
   g->atlas.resize(atlasN);
@@ -293,33 +324,62 @@ void build_brick_grid(const r2_voxel* d_dense, const int32_t nv[3], cudaStream_t
           dst[(size_t)x + (size_t)y * mx + (size_t)z * mx * my] = encode_range(lo, hi);
         }
   }
-  // global minorant/majorant over the index box
-  float lo = FLT_MAX, hi = -FLT_MAX;
-  for (size_t b = 0; b < nB; ++b) {
-    float a, c;
-    decode_range(g->range[b], &a, &c);
-    lo = std::min(lo, a);
-    hi = std::max(hi, c);
-  }
-  g->minorant = lo;
-  g->majorant = hi;
+  g->minorant = ord2f(mmHost[0]);
+  g->majorant = ord2f(mmHost[1]);
 }
 
-// .brickgrid file: this library's own binary layout (the reference stores
-// cereal PortableBinary archives, grid_brick/serialization.cpp:37-70):
-// "R2BRICK1", nBricks[3], atlasDim[3], brickCount, minorant, majorant, then
-// indirection, range, the three mips (u32 each) and the atlas (u8).
+namespace {
+
+struct Writer {
+  FILE* f;
+  bool ok = true;
+  void bytes(const void* p, size_t n) { ok = ok && (n == 0 || fwrite(p, 1, n, f) == n); }
+  template <typename T> void pod(const T& v) { bytes(&v, sizeof(T)); }
+  template <typename T> void buf3d(const uint32_t stride[3], const std::vector<T>& data) {
+    bytes(stride, 12);
+    pod((uint64_t)data.size());
+    bytes(data.data(), data.size() * sizeof(T));
+  }
+};
+
+struct Reader {
+  FILE* f;
+  bool ok = true;
+  void bytes(void* p, size_t n) { ok = ok && (n == 0 || fread(p, 1, n, f) == n); }
+  template <typename T> void pod(T& v) { bytes(&v, sizeof(T)); }
+  // A Buf3D whose element count must equal its stride's product and stay below `limit`.
+  template <typename T> void buf3d(uint32_t stride[3], std::vector<T>& data, uint64_t limit) {
+    uint64_t n = 0;
+    bytes(stride, 12);
+    pod(n);
+    ok = ok && n == (uint64_t)stride[0] * stride[1] * stride[2] && n <= limit;
+    if (!ok) return;
+    data.resize(n);
+    bytes(data.data(), n * sizeof(T));
+  }
+};
+
+}  // namespace
+
 void write_brick_grid(const std::string& path, const BrickGridHost& g) {
   FILE* f = fopen(path.c_str(), "wb");
   R2_REQUIRE(f, R2_ERR_IO, "cannot open " + path + " for writing");
-  bool ok = fwrite("R2BRICK1", 1, 8, f) == 8;
-  ok = ok && fwrite(g.nBricks, 4, 3, f) == 3 && fwrite(g.atlasDim, 4, 3, f) == 3 && fwrite(&g.brickCount, 4, 1, f) == 1;
-  ok = ok && fwrite(&g.minorant, 4, 1, f) == 1 && fwrite(&g.majorant, 4, 1, f) == 1;
-  ok = ok && fwrite(g.indirection.data(), 4, g.indirection.size(), f) == g.indirection.size();
-  ok = ok && fwrite(g.range.data(), 4, g.range.size(), f) == g.range.size();
-  for (uint32_t i = 0; i < kNumMipmaps; ++i) ok = ok && fwrite(g.mips[i].data(), 4, g.mips[i].size(), f) == g.mips[i].size();
-  ok = ok && fwrite(g.atlas.data(), 1, g.atlas.size(), f) == g.atlas.size();
-  ok = (fclose(f) == 0) && ok;
+  Writer w{f};
+  w.pod((uint8_t)1);  // PortableBinaryOutputArchive: data stored little-endian
+  w.bytes(g.transform, sizeof(g.transform));
+  w.bytes(g.nBricks, 12);
+  w.pod(g.minorant);
+  w.pod(g.majorant);
+  w.pod((uint64_t)g.brickCount);
+  w.buf3d(g.nBricks, g.indirection);
+  w.buf3d(g.nBricks, g.range);
+  w.buf3d(g.atlasDim, g.atlas);
+  w.pod((uint64_t)kNumMipmaps);
+  for (uint32_t i = 0; i < kNumMipmaps; ++i) {
+    const uint32_t ms[3] = {g.nBricks[0] >> (i + 1), g.nBricks[1] >> (i + 1), g.nBricks[2] >> (i + 1)};
+    w.buf3d(ms, g.mips[i]);
+  }
+  const bool ok = (fclose(f) == 0) && w.ok;
   R2_REQUIRE(ok, R2_ERR_IO, "short write to " + path);
 }
 
@@ -327,29 +387,39 @@ BrickGridHost read_brick_grid(const std::string& path) {
   FILE* f = fopen(path.c_str(), "rb");
   R2_REQUIRE(f, R2_ERR_IO, "cannot open " + path);
   BrickGridHost g;
-  char magic[8];
-  bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, "R2BRICK1", 8) == 0;
-  ok = ok && fread(g.nBricks, 4, 3, f) == 3 && fread(g.atlasDim, 4, 3, f) == 3 && fread(&g.brickCount, 4, 1, f) == 1;
-  ok = ok && fread(&g.minorant, 4, 1, f) == 1 && fread(&g.majorant, 4, 1, f) == 1;
-  if (ok) {
-    for (int k = 0; k < 3; ++k) ok = ok && g.nBricks[k] > 0 && g.nBricks[k] < kMaxBricks && g.atlasDim[k] <= 8 * kMaxBricks;
-  }
-  if (ok) {
-    const size_t nB = (size_t)g.nBricks[0] * g.nBricks[1] * g.nBricks[2];
-    g.indirection.resize(nB);
-    g.range.resize(nB);
-    ok = fread(g.indirection.data(), 4, nB, f) == nB && fread(g.range.data(), 4, nB, f) == nB;
-    for (uint32_t i = 0; i < kNumMipmaps && ok; ++i) {
-      const size_t m = (size_t)(g.nBricks[0] >> (i + 1)) * (g.nBricks[1] >> (i + 1)) * (g.nBricks[2] >> (i + 1));
-      g.mips[i].resize(m);
-      ok = fread(g.mips[i].data(), 4, m, f) == m;
-    }
-    const size_t an = (size_t)g.atlasDim[0] * g.atlasDim[1] * g.atlasDim[2];
-    g.atlas.resize(an);
-    ok = ok && fread(g.atlas.data(), 1, an, f) == an;
+  Reader r{f};
+  uint8_t little = 0;
+  r.pod(little);
+  r.ok = r.ok && little == 1;  // big-endian archives are not produced by the reference's x86 builds
+  r.bytes(g.transform, sizeof(g.transform));
+  r.bytes(g.nBricks, 12);
+  r.pod(g.minorant);
+  r.pod(g.majorant);
+  uint64_t count = 0;
+  r.pod(count);
+  for (int k = 0; r.ok && k < 3; ++k) r.ok = g.nBricks[k] > 0 && g.nBricks[k] < kMaxBricks;
+  const uint64_t nB = r.ok ? (uint64_t)g.nBricks[0] * g.nBricks[1] * g.nBricks[2] : 0;
+  r.ok = r.ok && count <= nB;
+  g.brickCount = (uint32_t)count;
+  uint32_t st[3];
+  r.buf3d(st, g.indirection, nB);
+  r.ok = r.ok && st[0] == g.nBricks[0] && st[1] == g.nBricks[1] && st[2] == g.nBricks[2];
+  r.buf3d(st, g.range, nB);
+  r.ok = r.ok && st[0] == g.nBricks[0] && st[1] == g.nBricks[1] && st[2] == g.nBricks[2];
+  r.buf3d(g.atlasDim, g.atlas, nB * kBrickSize * kBrickSize * kBrickSize);
+  r.ok = r.ok && g.atlasDim[0] == g.nBricks[0] * kBrickSize && g.atlasDim[1] == g.nBricks[1] * kBrickSize &&
+         g.atlasDim[2] % kBrickSize == 0 &&
+         (uint64_t)(g.atlasDim[0] / kBrickSize) * (g.atlasDim[1] / kBrickSize) * (g.atlasDim[2] / kBrickSize) >= count;
+  uint64_t nm = 0;
+  r.pod(nm);
+  r.ok = r.ok && nm == kNumMipmaps;
+  for (uint32_t i = 0; r.ok && i < kNumMipmaps; ++i) {
+    r.buf3d(st, g.mips[i], nB);
+    r.ok = r.ok && st[0] == g.nBricks[0] >> (i + 1) && st[1] == g.nBricks[1] >> (i + 1) &&
+           st[2] == g.nBricks[2] >> (i + 1);
   }
   fclose(f);
-  R2_REQUIRE(ok, R2_ERR_IO, "corrupt or truncated brick grid " + path);
+  R2_REQUIRE(r.ok, R2_ERR_IO, "corrupt or truncated brick grid " + path);
   return g;
 }
 

@@ -19,12 +19,13 @@ constexpr uint32_t kBrickBitsPerAxis = 10;
 constexpr uint32_t kMaxBricks = 1u << kBrickBitsPerAxis;
 constexpr uint32_t kNumMipmaps = 3;
 
-// Brick grid on the host (the .brickgrid contents).
+// Brick grid on the host (the .brickgrid contents, CHostBrickGrid's fields).
 struct BrickGridHost {
+  float transform[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};  // glm::mat4, identity when built
   uint32_t nBricks[3] = {0, 0, 0};   // per axis, multiple of 8
   uint32_t atlasDim[3] = {0, 0, 0};  // voxels
   uint32_t brickCount = 0;           // bricks with a non-constant range (atlas slots)
-  float minorant = 0.0f, majorant = 0.0f;
+  float minorant = 0.0f, majorant = 0.0f;  // density min / max over the grid's voxels (getMinorantMajorant)
   std::vector<uint32_t> indirection;  // encode_ptr of the atlas slot, 0 for constant bricks
   std::vector<uint32_t> range;        // two IEEE halves (min, max) of the dilated brick
   std::vector<uint32_t> mips[kNumMipmaps];
@@ -39,6 +40,13 @@ void extract_leaves(const r2_voxel* d_dense, const int32_t numVoxels[3], cudaStr
 // Builds the brick grid of the grid's density (inactive voxels read as 0).
 void build_brick_grid(const r2_voxel* d_dense, const int32_t numVoxels[3], cudaStream_t s, BrickGridHost* out);
 
+// The .brickgrid file in the reference's layout: a cereal PortableBinary
+// archive of CHostBrickGrid (raytracer/src/grid_brick/serialization.cpp:37-40):
+// a leading byte 1 (little-endian data), then transform (16 float, column
+// major), n_bricks (3 uint32), min_maj (2 float), brick_counter (uint64), and
+// the Buf3D fields indirection, range (uint32), atlas (uint8), each as its
+// stride (3 uint32), element count (uint64) and elements, then range_mipmaps
+// as a count (uint64) followed by that many uint32 Buf3Ds.
 void write_brick_grid(const std::string& path, const BrickGridHost& g);
 BrickGridHost read_brick_grid(const std::string& path);
 

@@ -298,3 +298,28 @@ def select_lods(cam_rec, lods, first, count, tree_pos, tree_scaling, tree_model,
                              len(sc), float(min_lod), float(covered_pixels), _p(out), _p(diag))
     assert rc == 0
     return (out, diag) if want_diag else out
+
+
+def build_bricks(dens):
+    """The reference's brick grid (CHostBrickGrid) of a density grid dens[z, y, x] (float32), built by the oracle
+    one brick after the other: dict of the archive's fields."""
+    d = np.ascontiguousarray(dens, np.float32)
+    nz, ny, nx = d.shape
+    nb = np.zeros(3, np.uint32)
+    P = C.c_void_p
+    lib.orc_build_bricks.argtypes = [P, C.c_int, C.c_int, C.c_int] + [P] * 10
+    lib.orc_build_bricks.restype = C.c_int
+    assert lib.orc_build_bricks(_p(d), nx, ny, nz, _p(nb), *([None] * 9)) == 0
+    nB = int(nb[0]) * int(nb[1]) * int(nb[2])
+    ind = np.zeros(nB, np.uint32)
+    rng = np.zeros(nB, np.uint32)
+    mips = [np.zeros(int(nb[0] >> (i + 1)) * int(nb[1] >> (i + 1)) * int(nb[2] >> (i + 1)), np.uint32)
+            for i in range(3)]
+    atlas = np.zeros(nB * 512, np.uint8)
+    ad = np.zeros(3, np.uint32)
+    cnt = np.zeros(1, np.uint64)
+    mm = np.zeros(2, np.float32)
+    assert lib.orc_build_bricks(_p(d), nx, ny, nz, _p(nb), _p(ind), _p(rng), _p(mips[0]), _p(mips[1]), _p(mips[2]),
+                                _p(atlas), _p(ad), _p(cnt), _p(mm)) == 0
+    return {"n_bricks": nb, "min_maj": mm, "brick_counter": int(cnt[0]), "indirection": ind, "range": rng,
+            "atlas_stride": ad, "atlas": atlas[:int(ad[0]) * int(ad[1]) * int(ad[2])], "mips": mips}

@@ -198,3 +198,62 @@ def test_corrupt_grid_file_rejected(tmp_path):
     assert N.lib.r2_status_string(st) == b"R2_ERR_IO"
     st = N.lib.r2_nvdb_info(str(tmp_path / "missing.nvdb").encode(), N.ptr(counts), None, None, None)
     assert N.lib.r2_status_string(st) == b"R2_ERR_IO"
+
+
+def _density_grid_from_nvdb(path, nv):
+    """Densities as the written grid stores them (inactive voxels: background 0), dens[z, y, x]."""
+    leaves, _ = parse_nvdb_leaves(path)
+    nx, ny, nz = nv
+    dens = np.zeros((nz, ny, nx), np.float32)
+    i = np.arange(512)
+    dx, dy, dz = i >> 6, (i >> 3) & 7, i & 7
+    for (ox, oy, oz), (mask, vals) in leaves.items():
+        bits = (mask[i >> 6] >> (i & 63).astype(np.uint64)) & np.uint64(1)
+        d = vals[:, :4].copy().view(np.float32).reshape(-1)
+        x, y, z = ox + dx, oy + dy, oz + dz
+        keep = (bits == 1) & (x < nx) & (y < ny) & (z < nz)
+        dens[z[keep], y[keep], x[keep]] = d[keep]
+    return dens
+
+
+@pytest.mark.parametrize("n", [20, 37])
+def test_brickgrid_archive_matches_reference_construction(tmp_path, n):
+    """The .brickgrid written by the filter is the reference's cereal
+    PortableBinary archive of CHostBrickGrid, parsed here independently, and
+    every field equals the oracle's sequential restatement of the reference's
+    construction (host_grid_brick.cpp:61-152) from the densities of the
+    written NanoVDB grid: transform, n_bricks, min_maj, brick_counter,
+    indirection, range, the atlas bytes and the three range mips, bit for bit.
+    The library's own reader returns the same fields."""
+    import brickgrid_io as BIO
+    mesh = scenes.foliage(4000, 6, 0.7, 12)
+    mat = F.material(diffuse=(0.2, 0.6, 0.1), specular=(0.04, 0.04, 0.04), alpha=0.4, ior=1.5)
+    vs0 = scenes.voxel_size_for(mesh, n)
+    prm = F.params(samples_per_voxel=32, iterations=8, min_voxel_size=vs0, lods=2)
+    run_lods(tmp_path, mesh, mat, prm, model="leaves")
+    vs = np.float32(vs0)
+    for lod in range(2):
+        base = tmp_path / "leaves" / f"filtered_mesh_{'%f' % float(vs)}"
+        g = O.setup_grid(mesh.positions.min(0).astype(np.float32), mesh.positions.max(0).astype(np.float32),
+                         N.identity43(), float(vs))
+        nv = tuple(g.num_voxels[:])
+        dens = _density_grid_from_nvdb(str(base) + ".nvdb", nv)
+        ref = O.build_bricks(dens)
+        got = BIO.parse(str(base) + ".brickgrid")
+        assert np.array_equal(got["transform"], np.eye(4, dtype=np.float32).reshape(-1))
+        assert np.array_equal(got["n_bricks"], ref["n_bricks"])
+        assert np.array_equal(got["indirection_stride"], ref["n_bricks"])
+        assert np.array_equal(got["min_maj"], ref["min_maj"])
+        assert got["brick_counter"] == ref["brick_counter"] > 0
+        assert np.array_equal(got["indirection"], ref["indirection"])
+        assert np.array_equal(got["range"], ref["range"])
+        assert np.array_equal(got["atlas_stride"], ref["atlas_stride"])
+        assert np.array_equal(got["atlas"], ref["atlas"])
+        assert len(got["mips"]) == 3
+        for m, rm in zip(got["mips"], ref["mips"]):
+            assert np.array_equal(m, rm)
+        dims = np.zeros(7, np.uint32)
+        mm = np.zeros(2, np.float32)
+        N.check(N.lib.r2_brickgrid_info((str(base) + ".brickgrid").encode(), N.ptr(dims), N.ptr(mm), None, None, 0))
+        assert list(dims) == list(ref["n_bricks"]) + list(ref["atlas_stride"]) + [ref["brick_counter"]]
+        vs = np.float32(vs * np.float32(2.0))
