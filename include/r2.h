@@ -346,6 +346,15 @@ r2_status r2_scene_commit(r2_scene* scene);
  * build has finished on the device.  Frames must not be rendering the scene
  * on another stream meanwhile. */
 r2_status r2_scene_rebuild(r2_scene* scene, void* stream);
+/* Replaces the committed scene's vertex positions (and, when normals is not
+ * NULL, its vertex normals) with nverts world-space vertices from host memory
+ * (pinned memory makes the copy asynchronous), in the order the meshes were
+ * added: the per-frame geometry upload of a dynamic scene.  Triangles,
+ * materials and the vertex count stay; call r2_scene_rebuild before the next
+ * frame.  stream as in r2_scene_rebuild; the host arrays must stay valid
+ * until the stream has copied them. */
+r2_status r2_scene_set_vertices(r2_scene* scene, const float* positions, const float* normals, uint32_t nverts,
+                                void* stream);
 /* Renders one frame into device memory d_rgb (width*height*3 floats).
  * stats_out (nullable, 8 doubles): [0] paths, [1] milliseconds of the frame on
  * the stream, [2] path segments traced, [3] shadow rays traced, [4..7]
@@ -357,8 +366,9 @@ r2_status r2_scene_rebuild(r2_scene* scene, void* stream);
  * shadow ray (the reference's loops have no bound). */
 r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* d_rgb,
                            void* stream, double* stats_out);
-/* Same through host memory: commits if needed, renders, copies the frame to
- * rgb; loop bounds are reported as in r2_render_device. */
+/* Same through host memory: commits if needed, renders into a device frame
+ * the scene keeps (grown on demand, reused by later calls), copies the frame
+ * to rgb and waits; loop bounds are reported as in r2_render_device. */
 r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* rgb);
 
 /* The scene's launch tuning (initially the defaults, or the environment's

@@ -99,6 +99,7 @@ def _load():
         "r2_filter_run_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, P, P, C.c_char_p, C.c_char_p, P]),
         "r2_scene_commit": (C.c_int, [P]),
         "r2_scene_rebuild": (C.c_int, [P, P]),
+        "r2_scene_set_vertices": (C.c_int, [P, P, P, u32, P]),
         "r2_render_device": (C.c_int, [P, P, P, P, P, P]),
         "r2_render_host": (C.c_int, [P, P, P, P]),
         "r2_scene_set_tuning": (C.c_int, [P, P]),

@@ -105,6 +105,15 @@ r2_status r2_scene_rebuild(r2_scene* scene, void* stream) {
   R2_API_END
 }
 
+r2_status r2_scene_set_vertices(r2_scene* scene, const float* positions, const float* normals, uint32_t nverts,
+                                void* stream) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && positions, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(scene->impl->committed(), R2_ERR_INVALID_ARGUMENT, "scene not committed");
+  scene->impl->set_vertices(positions, normals, nverts, (cudaStream_t)stream);
+  R2_API_END
+}
+
 r2_status r2_render_device(r2_scene* scene, const r2_camera* camera, const r2_render_params* params, float* d_rgb,
                            void* stream, double* stats_out) {
   R2_API_BEGIN
@@ -121,7 +130,8 @@ r2_status r2_render_host(r2_scene* scene, const r2_camera* camera, const r2_rend
   R2_API_BEGIN
   R2_REQUIRE(scene && camera && params && rgb, R2_ERR_INVALID_ARGUMENT, "null argument");
   size_t n = (size_t)camera->width * camera->height * 3;
-  r2::DBuf<float> d(n);
+  r2::DBuf<float>& d = scene->impl->host_frame();
+  d.reserve(n);
   cudaStream_t s = scene->impl->stream();
   scene->impl->render(*camera, *params, d.get(), s, nullptr);
   d.download(rgb, n, s);

@@ -241,6 +241,18 @@ void RenderScene::rebuild(cudaStream_t s) {
   view_.bvh.alpha = alpha;
 }
 
+void RenderScene::set_vertices(const float* pos, const float* nrm, uint32_t nverts, cudaStream_t s) {
+  if (!s) s = ctx_.stream;
+  R2_REQUIRE((size_t)nverts * 3 == hPos_.size() && nverts > 0, R2_ERR_INVALID_ARGUMENT,
+             "vertex count differs from the scene's (" + std::to_string(hPos_.size() / 3) + ")");
+  memcpy(hPos_.data(), pos, hPos_.size() * sizeof(float));
+  R2_CUDA(cudaMemcpyAsync(dPos_.get(), pos, hPos_.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+  if (nrm) {
+    memcpy(hNrm_.data(), nrm, hNrm_.size() * sizeof(float));
+    R2_CUDA(cudaMemcpyAsync(dNrm_.get(), nrm, hNrm_.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+  }
+}
+
 void RenderScene::commit() {
   R2_REQUIRE(env_.W > 0, R2_ERR_INVALID_CONFIG, "scene has no environment map");
   cudaStream_t s = ctx_.stream;

@@ -93,6 +93,11 @@ class RenderScene {
   // geometry stays on the device.  Same tree as the commit's; allocates
   // nothing after the first build; waits for the build's end.
   void rebuild(cudaStream_t s);
+  // Replaces the world-space vertex positions (and normals when given) of the
+  // committed scene from host memory, on stream s (the scene's own when null).
+  void set_vertices(const float* pos, const float* nrm, uint32_t nverts, cudaStream_t s);
+  // Device frame of r2_render_host, kept between calls.
+  DBuf<float>& host_frame() { return hostFrame_; }
   bool committed() const { return committed_; }
   bool has_media() const { return !media_.empty(); }
   // One frame: spp / wave_spp waves accumulated into d_frame (W*H*3 floats,
@@ -160,6 +165,7 @@ class RenderScene {
   DBuf<Shape> shapes_;
   DBuf<float4> envTex_;
   DBuf<float> envBuf_;
+  DBuf<float> hostFrame_;
   SceneView view_;
   r2_render_tuning tuning_{0, 0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
 };

@@ -133,6 +133,20 @@ class Scene:
     def commit(self):
         N.check(N.lib.r2_scene_commit(self.handle))
 
+    def set_vertices(self, positions, normals=None, stream: int = 0, nverts: int = 0):
+        """Replace the world-space vertex positions (and normals) of the committed scene, in mesh order: numpy
+        arrays, or host addresses (e.g. of pinned tensors, which make the copy asynchronous) with nverts."""
+        def addr(a):
+            if a is None:
+                return None
+            if isinstance(a, int):
+                return C.c_void_p(a)
+            assert a.flags["C_CONTIGUOUS"] and a.dtype == np.float32
+            return C.c_void_p(a.ctypes.data)
+        n = nverts or positions.size // 3
+        N.check(N.lib.r2_scene_set_vertices(self.handle, addr(positions), addr(normals), n,
+                                            C.c_void_p(stream or None)))
+
     def rebuild(self, stream: int = 0):
         """Rebuild the triangle BVH on the device from the resident triangles (waits for the build)."""
         N.check(N.lib.r2_scene_rebuild(self.handle, C.c_void_p(stream or None)))
@@ -165,7 +179,12 @@ class Scene:
         N.check(N.lib.r2_scene_autotune(self.handle, C.byref(cam), C.byref(prm), C.byref(t)))
         return t
 
-    def render(self, cam: Camera, prm: RenderParams) -> np.ndarray:
+    def render(self, cam: Camera, prm: RenderParams, out_ptr: int = 0) -> np.ndarray:
+        """Frame in host memory (r2_render_host): a new array, or the width*height*3 floats at host address out_ptr
+        (e.g. a pinned buffer; None is returned then)."""
+        if out_ptr:
+            N.check(N.lib.r2_render_host(self.handle, C.byref(cam), C.byref(prm), C.c_void_p(out_ptr)))
+            return None
         out = np.zeros((cam.height, cam.width, 3), np.float32)
         N.check(N.lib.r2_render_host(self.handle, C.byref(cam), C.byref(prm), N.ptr(out)))
         return out

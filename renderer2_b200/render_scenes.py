@@ -87,6 +87,22 @@ def volume_scene(work_dir, index: int = 0, grid: int = 256, n_quads: int = 200_0
     return desc, cam
 
 
+def world_vertices(desc):
+    """World-space vertex positions and normals of the scene's meshes in the order build_scene adds them (the
+    layout r2_scene_set_vertices takes), transformed with the library's float operation order."""
+    P, Nn = [], []
+    for entry in desc.get("meshes", []):
+        mesh, _, m2w = entry[:3]
+        m = np.asarray(m2w, np.float32).reshape(4, 3)
+        p = mesh.positions.astype(np.float32)
+        n = mesh.normals.astype(np.float32)
+        wp = (((m[0] * p[:, :1] + m[1] * p[:, 1:2]) + m[2] * p[:, 2:3]) + m[3] * np.float32(1.0)).astype(np.float32)
+        wn = (((m[0] * n[:, :1] + m[1] * n[:, 1:2]) + m[2] * n[:, 2:3]) + m[3] * np.float32(0.0)).astype(np.float32)
+        P.append(wp)
+        Nn.append(wn)
+    return np.ascontiguousarray(np.concatenate(P)), np.ascontiguousarray(np.concatenate(Nn))
+
+
 def build_scene(desc) -> R.Scene:
     sc = R.Scene()
     for entry in desc.get("meshes", []):

@@ -133,6 +133,37 @@ def test_device_rebuild_gives_the_same_frame():
     assert np.array_equal(a, b) and np.array_equal(a, c)
 
 
+def test_set_vertices_matches_a_scene_built_from_the_moved_meshes():
+    """r2_scene_set_vertices + r2_scene_rebuild on a committed scene give the
+    frame of a scene built from scratch with the moved geometry, bit for bit;
+    the unmoved vertices give back the original frame."""
+    desc, _ = RS.icosphere_grid_scene()
+    cam = R.camera(48, 40, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+    prm = R.params(2, 8, 9)
+    sc = RS.build_scene(desc)
+    a = sc.render(cam, prm)
+    moved = {"meshes": [(m, mat, RS.translate43(float(t[9]) + 0.7, float(t[10]) - 0.4, 1.5))
+                        for m, mat, t in desc["meshes"]], "shapes": [], "env": desc["env"]}
+    pos, nrm = RS.world_vertices(moved)
+    sc.set_vertices(pos, nrm)
+    sc.rebuild()
+    b = sc.render(cam, prm)
+    ref = RS.build_scene(moved)
+    c = ref.render(cam, prm)
+    ref.close()
+    pos0, nrm0 = RS.world_vertices(desc)
+    sc.set_vertices(pos0, nrm0)
+    sc.rebuild()
+    d = sc.render(cam, prm)
+    from renderer2_b200 import _native as N
+    with pytest.raises(N.R2Error):
+        sc.set_vertices(pos0[:-1], None)  # vertex count must match
+    sc.close()
+    assert not np.array_equal(a, b)
+    assert np.array_equal(b, c)
+    assert np.array_equal(a, d)
+
+
 def test_render_rejects_bad_arguments():
     desc, _ = RS.icosphere_scene()
     sc = RS.build_scene(desc)
