@@ -2,7 +2,9 @@
 //
 // Compiled in place from the reference tree (-I .../raytracer/include) against
 // the from-scratch shims in oracle/refshim/ (glm subset, OptiX/NanoVDB type
-// stand-ins, a cuRAND stand-in that replays queued draws).  The exported
+// stand-ins, a cuRAND stand-in that replays queued draws, and a scene,
+// scene-object and material stand-in whose closest hit is the oracle's BVH
+// trace, so that CMeshFilter::run compiles and runs as written).  The exported
 // functions evaluate the reference implementation on given inputs; the golden
 // vectors they produce (tests/golden/make_golden.py) pin the oracle's
 // restatement.  Nothing of the product links this file.
@@ -29,11 +31,51 @@
 #include "medium/sggx_phase_function.hpp"
 #include "shapes/sphere.hpp"
 #include "utility/functions.hpp"
+// CMeshFilter with the scene, scene object and material shims of refshim/;
+// the oracle's BVH and closest-hit trace stand in for OptiX.
+#include "filtering/mesh_filter.hpp"
+#include "oracle.h"
 
 namespace r2ref {
 static std::vector<float> g_queue;
 static size_t g_pos = 0;
 float next_curand() { return g_pos < g_queue.size() ? g_queue[g_pos++] : 0.5f; }
+
+// Filter scene of the CDeviceScene shim: the oracle's BVH over the
+// world-space triangles, model-space vertex normals, the object's transform
+// and its material.
+struct FilterHookScene {
+  std::vector<int32_t> nodes;
+  std::vector<uint32_t> order, idx;
+  std::vector<float> tris, nrm;
+  glm::mat4x3 m2w{1.f};
+  rt::CMaterial mat;
+  float ior = 1.f;
+  bool ready = false;
+};
+static FilterHookScene g_fs;
+
+// __closesthit__ch (shaders.optix.cu:28-130) for an untextured mesh: the
+// normal interpolated from the vertex normals with the hit's barycentrics,
+// normalised, taken to world space by the object's transform and normalised.
+void scene_intersect(const rt::CRay& ray, rt::SInteraction* si, unsigned int mask) {
+  si->hitInformation.hit = false;
+  if (!(mask & rt::ESceneobjectMask::FILTER) || !g_fs.ready) return;
+  float t = 0.f, b1 = 0.f, b2 = 0.f;
+  const int tri = orc_trace(g_fs.nodes.data(), g_fs.tris.data(), ray.m_origin.x, ray.m_origin.y, ray.m_origin.z,
+                            ray.m_direction.x, ray.m_direction.y, ray.m_direction.z, ray.m_t_max, &t, &b1, &b2);
+  if (tri < 0) return;
+  const uint32_t* v = &g_fs.idx[3 * (size_t)g_fs.order[tri]];
+  auto N = [&](uint32_t k) { return glm::vec3(g_fs.nrm[3 * k], g_fs.nrm[3 * k + 1], g_fs.nrm[3 * k + 2]); };
+  glm::vec3 n = glm::normalize((1.f - b1 - b2) * N(v[0]) + b1 * N(v[1]) + b2 * N(v[2]));
+  n = glm::normalize(g_fs.m2w * glm::vec4(n, 0.f));
+  si->hitInformation.hit = true;
+  si->hitInformation.normal = n;
+  si->hitInformation.tc = glm::vec2(0.f);
+  si->hitInformation.ior = g_fs.ior;
+  si->hitInformation.t = t;
+  si->material = &g_fs.mat;
+}
 }  // namespace r2ref
 
 static void feed(const float* c, int n) {
@@ -214,6 +256,70 @@ void ref_get_rotation(const float* n, float* out) {
   glm::mat4 m = rt::getRotation(V(n));
   for (int c = 0; c < 4; ++c)
     for (int r = 0; r < 4; ++r) out[4 * c + r] = m[c][r];
+}
+
+// Evaluation order of a three-argument constructor's arguments in this build
+// (glm::vec3(a(), b(), c())): 0 = left to right, 1 = right to left.
+int ref_vec3_arg_order() {
+  float c[3] = {0.25f, 0.5f, 0.75f};
+  feed(c, 3);
+  rt::CSampler s;
+  glm::vec3 v(s.uniformSample01(), s.uniformSample01(), s.uniformSample01());
+  return v.x < v.z ? 0 : 1;
+}
+
+static glm::mat4x3 M43(const float* m) {
+  return glm::mat4x3(glm::vec3(m[0], m[1], m[2]), glm::vec3(m[3], m[4], m[5]), glm::vec3(m[6], m[7], m[8]),
+                     glm::vec3(m[9], m[10], m[11]));
+}
+
+// Scene of ref_mesh_filter_voxel: world-space vertices (the oracle's BVH is
+// built over them), indices, model-space vertex normals, the object's
+// model-to-world transform (12 floats, glm mat4x3) and the material (Kd, Ks,
+// GGX alpha, ior).  Returns the BVH height, negative on failure.
+int ref_filter_scene(const float* wpos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
+                     const float* m2w, const float* kd, const float* ks, float alpha, float ior) {
+  r2ref::FilterHookScene& fs = r2ref::g_fs;
+  fs.nodes.assign(16 * (size_t)(ntris > 1 ? ntris - 1 : 1), 0);
+  fs.order.assign(ntris, 0);
+  fs.tris.assign(12 * (size_t)ntris, 0.f);
+  fs.idx.assign(idx, idx + 3 * (size_t)ntris);
+  fs.nrm.assign(nrm, nrm + 3 * (size_t)nverts);
+  fs.m2w = M43(m2w);
+  fs.mat.kd = V(kd);
+  fs.mat.ks = V(ks);
+  fs.mat.alpha = alpha;
+  fs.ior = ior;
+  const int h = orc_build_bvh(wpos, nverts, idx, ntris, fs.nodes.data(), fs.order.data(), fs.tris.data());
+  fs.ready = h >= 0;
+  return h;
+}
+
+// CMeshFilter(voxel, grid...).run(scene, spv) (mesh_filter.hpp:24-122): the
+// reference's sampling, closest-hit accumulation, estimateDensity (:182-204,
+// 216-226) and payload compaction for one voxel, with the queued draws c (nc
+// of them; generateRay takes five per sample).  The grid is the filter's
+// launch description (COpenvdbBackend::setupGrid): indexToModel, modelToIndex,
+// modelToWorld, worldToModel (12 floats each), numVoxels and the world box.
+// out32: the SFilteredDataCompact bytes.  Returns the draws consumed.
+int ref_mesh_filter_voxel(const int32_t* voxel, const float* i2m, const float* m2i, const float* m2w,
+                          const float* w2m, const int32_t* nv, const float* bbmin, const float* bbmax, float sigma_t,
+                          uint32_t iters, float alpha, int clip, uint32_t spv, const float* c, int nc,
+                          unsigned char* out32) {
+  if (spv > 1000) return -1;  // rayTs[1000] of CMeshFilter::run
+  const glm::ivec3 cv(voxel[0], voxel[1], voxel[2]);
+  const glm::mat4x3 indexToModel = M43(i2m), modelToIndex = M43(m2i), modelToWorld = M43(m2w),
+                    worldToModel = M43(w2m);
+  const glm::ivec3 numVoxels(nv[0], nv[1], nv[2]);
+  const rt::SAABB bb{V(bbmin), V(bbmax)};
+  feed(c, nc);
+  rt::CSampler sampler;
+  filter::CMeshFilter f(cv, indexToModel, modelToIndex, modelToWorld, worldToModel, numVoxels, bb, sampler, sigma_t,
+                        iters, alpha, clip != 0, 1.0f);
+  rt::CDeviceScene scene;
+  filter::SFilteredDataCompact out = f.run(scene, spv);
+  std::memcpy(out32, &out, 32);
+  return ref_draws_used();
 }
 
 }  // extern "C"

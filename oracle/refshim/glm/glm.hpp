@@ -223,8 +223,9 @@ struct mat {
   }
   vec<R, T, Q>& operator[](length_t i) { return c[i]; }
   const vec<R, T, Q>& operator[](length_t i) const { return c[i]; }
-  // conversion between sizes: copy the overlap, identity elsewhere
-  template <length_t C2, length_t R2> explicit mat(const mat<C2, R2, T, Q>& o) {
+  // conversion between sizes: copy the overlap, identity elsewhere (implicit,
+  // as glm's conversions are unless GLM_FORCE_EXPLICIT_CTOR is defined)
+  template <length_t C2, length_t R2> mat(const mat<C2, R2, T, Q>& o) {
     for (length_t i = 0; i < C; ++i) {
       c[i] = vec<R, T, Q>(static_cast<T>(0));
       if (i < R) c[i][i] = static_cast<T>(1);

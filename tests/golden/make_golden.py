@@ -56,6 +56,11 @@ def build(ref_include: str) -> C.CDLL:
     lib.ref_sggx_sample.argtypes = [P, P, f, P, P, C.c_int, P]
     lib.ref_get_rotation.argtypes = [P, P]
     lib.ref_draws_used.restype = C.c_int
+    lib.ref_vec3_arg_order.restype = C.c_int
+    lib.ref_filter_scene.restype = C.c_int
+    lib.ref_filter_scene.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, P, f, f]
+    lib.ref_mesh_filter_voxel.restype = C.c_int
+    lib.ref_mesh_filter_voxel.argtypes = [P] * 8 + [f, C.c_uint32, f, C.c_int, C.c_uint32, P, C.c_int, P]
     return lib
 
 
@@ -70,6 +75,84 @@ def _f32(x):
 def unit(rng, n):
     v = rng.normal(size=(n, 3))
     return _f32(v / np.linalg.norm(v, axis=1, keepdims=True))
+
+
+# CMeshFilter::run cases: the mesh is rebuilt by the named seeded generator of
+# renderer2_b200.scenes; the grid has `n` voxels along the longest extent.
+MESH_FILTER_CASES = [
+    dict(mesh="icosphere(2, 0.05, 1)", n=10, spv=64, iters=10, sigma_t=10.0, alpha=0.1, clip=1, seed=0,
+         kd=(0.8, 0.6, 0.4), ks=(0.9, 0.9, 0.9), ggx=0.3, ior=1.5),
+    dict(mesh="foliage(300, 3, 0.7, 5)", n=8, spv=128, iters=20, sigma_t=10.0, alpha=0.1, clip=1, seed=3,
+         kd=(0.1, 0.6, 0.1), ks=(0.04, 0.04, 0.04), ggx=0.02, ior=1.33),
+    dict(mesh="icosphere(1, 0.1, 7)", n=7, spv=48, iters=5, sigma_t=4.0, alpha=0.3, clip=0, seed=1,
+         kd=(0.5, 0.5, 0.5), ks=(1.0, 1.0, 1.0), ggx=0.6, ior=1.2),
+]
+
+
+def curand_values_for(lib, u):
+    """cuRAND values c with CSampler::uniformSample01(c) == u (float32), found next to u * (1 - FLT_EPSILON);
+    NaN where no float maps to u exactly."""
+    u = np.asarray(u, np.float32)
+    eps = np.float32(2.0 ** -23)
+    den = np.float32(np.float32(1.0) - eps) - np.float32(np.finfo(np.float32).tiny)
+    base = (u.astype(np.float64) * float(den)).astype(np.float32)
+    out = np.full(u.shape, np.nan, np.float32)
+    for k in (0, 1, -1, 2, -2, 3, -3):
+        c = np.nextafter(base, np.float32(np.inf) if k > 0 else np.float32(-np.inf)) if k else base
+        for _ in range(abs(k) - 1):
+            c = np.nextafter(c, np.float32(np.inf) if k > 0 else np.float32(-np.inf))
+        got = np.clip((c / den).astype(np.float32) - np.finfo(np.float32).tiny, np.float32(0.0), np.float32(1.0) - eps)
+        ok = np.isnan(out) & (got == u) & (c > 0)
+        out[ok] = c[ok]
+    zero = u == 0.0
+    out[zero] = np.float32(1e-30)  # any c below FLT_MIN * den maps to 0
+    for i in range(0, u.size, max(1, u.size // 64)):  # the numpy mapping agrees with the reference's own
+        if not np.isnan(out.flat[i]):
+            assert np.float32(lib.ref_u01(float(out.flat[i]))) == u.flat[i]
+    return out
+
+
+def mesh_filter_case(lib, mesh, n, spv, iters, sigma_t, alpha, clip, seed, kd, ks, ggx, ior):
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    from renderer2_b200 import scenes
+    m = eval("scenes." + mesh)
+    m2w = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], np.float32)
+    pos = np.ascontiguousarray(m.positions, np.float32)
+    idx = np.ascontiguousarray(m.indices, np.uint32)
+    nrm = np.ascontiguousarray(m.normals, np.float32)
+    assert lib.ref_filter_scene(_p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), _p(m2w), _p(_f32(kd)),
+                                _p(_f32(ks)), ggx, ior) >= 0
+    grid = O.setup_grid(pos.min(0), pos.max(0), m2w, scenes.voxel_size_for(m, n))
+    nx, ny, nz = grid.num_voxels[:]
+    order3 = lib.ref_vec3_arg_order()
+    mats = [_f32(list(getattr(grid, k))) for k in ("index_to_model", "model_to_index", "model_to_world",
+                                                    "world_to_model")]
+    nv = np.array([nx, ny, nz], np.int32)
+    bbmin, bbmax = _f32(list(grid.world_bb_min)), _f32(list(grid.world_bb_max))
+    payload = np.zeros((nx * ny * nz, 32), np.uint8)
+    inexact = 0
+    s_idx = np.arange(spv, dtype=np.uint32)
+    assert np.array_equal(np.array(scenes.philox4x32_10(3, 1, 0, 0, 17, seed)).ravel(), O.philox([3, 1, 0, 0], [17, seed]))
+    for vid in range(nx * ny * nz):
+        x, y, z = vid % nx, (vid // nx) % ny, vid // (nx * ny)
+        r0 = np.stack(scenes.philox4x32_10(s_idx, 0, 0, 0, vid, seed), 1)  # the oracle's streams (voxel, seed)
+        r1 = np.stack(scenes.philox4x32_10(s_idx, 1, 0, 0, vid, seed), 1)
+        u = ((np.stack([r0[:, 0], r0[:, 1], r0[:, 2], r0[:, 3], r1[:, 0]], 1) >> 8).astype(np.float64)
+             * (1.0 / 16777216.0)).astype(np.float32)
+        if order3 == 1:  # glm::vec3(u(), u(), u()): the third component is drawn first in this build
+            u[:, [0, 2]] = u[:, [2, 0]]
+        c = curand_values_for(lib, u.reshape(-1))
+        inexact += int(np.isnan(c).sum())
+        c = np.where(np.isnan(c), np.float32(0.5), c).astype(np.float32)
+        used = lib.ref_mesh_filter_voxel(_p(np.array([x, y, z], np.int32)), *[_p(a) for a in mats], _p(nv),
+                                         _p(bbmin), _p(bbmax), sigma_t, iters, alpha, clip, spv, _p(c), c.size,
+                                         _p(payload[vid]))
+        assert used == 5 * spv, used
+    return {"mesh": mesh, "n": n, "spv": spv, "iters": iters, "sigma_t": sigma_t, "alpha": alpha, "clip": clip,
+            "seed": seed, "kd": list(kd), "ks": list(ks), "ggx": ggx, "ior": ior, "num_voxels": [nx, ny, nz],
+            "draws_not_reproduced": inexact, "payload_hex": payload.tobytes().hex()}
 
 
 def main():
@@ -235,6 +318,9 @@ def main():
         lib.ref_get_rotation(_p(n), _p(out))
         rows.append({"n": n.tolist(), "m": out.tolist()})
     g["get_rotation"] = rows
+
+    g["vec3_arg_order"] = lib.ref_vec3_arg_order()
+    g["mesh_filter"] = [mesh_filter_case(lib, **k) for k in MESH_FILTER_CASES]
 
     with open(OUT, "w") as fh:
         json.dump(g, fh)
