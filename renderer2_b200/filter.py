@@ -136,9 +136,12 @@ class FilterScene:
         return nodes, order, ht.value
 
 
-def filter_mesh(mesh: Mesh, mat, prm, voxel_size: float, model_to_world=None, wide=False):
+def filter_mesh(mesh: Mesh, mat, prm, voxel_size: float, model_to_world=None, wide=False, out_ptr: int = 0,
+                out_capacity: int = 0):
     """One LOD through the host-buffer entry point r2_filter_mesh (upload, BVH
-    build, filter, download).  Returns (grid, voxels[, wide])."""
+    build, filter, download).  Returns (grid, voxels[, wide]); with out_ptr the
+    payloads go to that host address (e.g. a pinned buffer of out_capacity
+    voxels) and (grid, None) is returned."""
     pos = _c(mesh.positions, np.float32)
     idx = _c(mesh.indices, np.uint32)
     nrm = _c(mesh.normals, np.float32)
@@ -149,6 +152,12 @@ def filter_mesh(mesh: Mesh, mat, prm, voxel_size: float, model_to_world=None, wi
     hi = mesh.positions.max(axis=0).astype(np.float32)
     N.check(N.lib.r2_filter_setup_grid(N.ptr(lo), N.ptr(hi), N.ptr(m2w), float(voxel_size), C.byref(g)))
     nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+    if out_ptr:
+        assert out_capacity >= nvox and not wide
+        N.check(N.lib.r2_filter_mesh(N.ptr(pos), mesh.nverts, N.ptr(idx), mesh.ntris, N.ptr(nrm), C.byref(mat),
+                                     N.ptr(m2w), C.byref(prm), float(voxel_size), C.byref(g), C.c_void_p(out_ptr),
+                                     None, out_capacity))
+        return g, None
     out = np.zeros(nvox, N.VOXEL_DTYPE)
     w = np.zeros((nvox, 20), np.float32) if wide else None
     N.check(N.lib.r2_filter_mesh(N.ptr(pos), mesh.nverts, N.ptr(idx), mesh.ntris, N.ptr(nrm), C.byref(mat),
