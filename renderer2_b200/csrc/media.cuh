@@ -671,11 +671,12 @@ R2_HD float sggx_sample_p(const Sggx& g, float ior, V3 wo, V3* wi, RngStream& rn
 // takes the next one from a queue).  Each step is one loop iteration of the
 // corresponding function with the same operations and random draws, so a
 // segment tracked step by step gives the same result as the loop.
-enum TrackStatus : int { kTrackRunning = 0, kTrackDone = 1, kTrackCollide = 2, kTrackError = 3 };
+enum TrackStatus : int { kTrackRunning = 0, kTrackDone = 1, kTrackCollide = 2, kTrackError = 3, kTrackPending = 4 };
 
 struct TrackState {
   V3 o, d, ri;  // ray in the tracking space (unit box, or scaled index box for the DDA), 1/d
   float tmax, t, tau, mip, tr, invMax;
+  float maj;    // DDA: the majorant of a tentative collision waiting for its test
   int steps;
   RngStream rng;
 };
@@ -732,73 +733,94 @@ R2_HD V3 track_collision(const MediumView& m, V3 o, V3 d, float t, MediumEvent* 
   return albedo;
 }
 
+// The DDA iteration in two parts.  track_dda_advance takes one step across
+// the brick grid's majorant cells and returns kTrackPending when the optical
+// depth runs out inside the segment (a tentative collision at s.t, majorant
+// in s.maj); track_dda_collide then tests it against the brick density.  A
+// persistent tracker can hold a pending test while the warp's other lanes
+// step on, and test all pending collisions together: each lane performs the
+// same operations in the same order as track_step.
+template <bool kSample>
+R2_HD int track_dda_advance(const MediumView& m, TrackState& s) {
+  if (s.steps >= kMaxTrackingSteps) return kTrackError;
+  ++s.steps;
+  if (!(s.t < s.tmax)) return kTrackDone;
+  const V3 curr = s.o + s.d * s.t;
+  const int mi = (int)roundf(s.mip);
+  const float majorant = m.filterRenderRatio * brick_majorant(m, curr, mi);
+  const float dt = step_dda(curr, s.ri, mi);
+  const float prevT = s.t;
+  s.t += dt / m.sigmaT;
+  if (s.t == prevT) return kTrackDone;
+  s.tau -= majorant * dt;
+  s.mip = fminf(s.mip + 0.25f, 3.0f);
+  if (s.tau > 0.0f) return kTrackRunning;
+  s.t += s.tau / (majorant * m.sigmaT);
+  if (s.t >= s.tmax) return kTrackDone;
+  s.maj = majorant;
+  return kTrackPending;
+}
+
+template <bool kSample>
+R2_HD int track_dda_collide(const MediumView& m, TrackState& s) {
+  const float majorant = s.maj;
+  // draws: jitter x, y, z, acceptance, then the roulette (transmittance
+  // only, after a real collision that drops tr below 0.1) and the next
+  // free-flight sample, in that order
+  float u[5];
+  U4 w0, w1;
+  s.rng.peek5(u, &w0, &w1);
+  const float d = brick_density(m, s.o + s.d * s.t + v3(u[0], u[1], u[2]) - v3(0.5f));
+  if (u[3] * majorant < d * m.filterRenderRatio) {
+    if (kSample) {
+      s.rng.advance(4, w0, w1);
+      return kTrackCollide;
+    }
+    s.tr *= fmaxf(0.0f, 1.0f - s.invMax / majorant);
+    if (s.tr < 0.1f) {
+      const float prob = 1.0f - s.tr;
+      s.rng.advance(5, w0, w1);
+      if (u[4] < prob) {
+        s.tr = 0.0f;
+        return kTrackDone;
+      }
+      s.tr /= 1.0f - prob;
+      s.tau = -log_r2(1.0f - s.rng.next());
+      s.mip = fmaxf(0.0f, s.mip - 2.0f);
+      return kTrackRunning;
+    }
+  }
+  s.rng.advance(5, w0, w1);
+  s.tau = -log_r2(1.0f - u[4]);
+  s.mip = fmaxf(0.0f, s.mip - 2.0f);
+  return kTrackRunning;
+}
+
 // One iteration.  kSample: kTrackCollide leaves the collision at s.t (see
 // track_collision).  Transmittance: kTrackDone leaves the estimate in s.tr.
 template <bool kDDA, bool kSample>
 R2_HD int track_step(const MediumView& m, TrackState& s) {
+  if (kDDA) {
+    const int st = track_dda_advance<kSample>(m, s);
+    return st == kTrackPending ? track_dda_collide<kSample>(m, s) : st;
+  }
   if (s.steps >= kMaxTrackingSteps) return kTrackError;
   ++s.steps;
-  if (kDDA) {
-    if (!(s.t < s.tmax)) return kTrackDone;
-    const V3 curr = s.o + s.d * s.t;
-    const int mi = (int)roundf(s.mip);
-    const float majorant = m.filterRenderRatio * brick_majorant(m, curr, mi);
-    const float dt = step_dda(curr, s.ri, mi);
-    const float prevT = s.t;
-    s.t += dt / m.sigmaT;
-    if (s.t == prevT) return kTrackDone;
-    s.tau -= majorant * dt;
-    s.mip = fminf(s.mip + 0.25f, 3.0f);
-    if (s.tau > 0.0f) return kTrackRunning;
-    s.t += s.tau / (majorant * m.sigmaT);
-    if (s.t >= s.tmax) return kTrackDone;
-    // draws: jitter x, y, z, acceptance, then the roulette (transmittance
-    // only, after a real collision that drops tr below 0.1) and the next
-    // free-flight sample, in that order
-    float u[5];
-    U4 w0, w1;
-    s.rng.peek5(u, &w0, &w1);
-    const float d = brick_density(m, s.o + s.d * s.t + v3(u[0], u[1], u[2]) - v3(0.5f));
-    if (u[3] * majorant < d * m.filterRenderRatio) {
-      if (kSample) {
-        s.rng.advance(4, w0, w1);
-        return kTrackCollide;
-      }
-      s.tr *= fmaxf(0.0f, 1.0f - s.invMax / majorant);
-      if (s.tr < 0.1f) {
-        const float prob = 1.0f - s.tr;
-        s.rng.advance(5, w0, w1);
-        if (u[4] < prob) {
-          s.tr = 0.0f;
-          return kTrackDone;
-        }
-        s.tr /= 1.0f - prob;
-        s.tau = -log_r2(1.0f - s.rng.next());
-        s.mip = fmaxf(0.0f, s.mip - 2.0f);
-        return kTrackRunning;
-      }
+  s.t -= log_r2(1.0f - s.rng.next()) * s.invMax / m.sigmaT;
+  if (s.t >= s.tmax) return kTrackDone;
+  const V3 pt = s.o + s.d * s.t;
+  const float dens = medium_density(m, pt);
+  if (kSample) return m.filterRenderRatio * dens * s.invMax > s.rng.next() ? kTrackCollide : kTrackRunning;
+  s.tr *= 1.0f - fmaxf(0.0f, m.filterRenderRatio * dens * s.invMax);
+  if (s.tr < 1.0f) {
+    const float p = 1.0f - s.tr;
+    if (s.rng.next() < p) {
+      s.tr = 0.0f;
+      return kTrackDone;
     }
-    s.rng.advance(5, w0, w1);
-    s.tau = -log_r2(1.0f - u[4]);
-    s.mip = fmaxf(0.0f, s.mip - 2.0f);
-    return kTrackRunning;
-  } else {
-    s.t -= log_r2(1.0f - s.rng.next()) * s.invMax / m.sigmaT;
-    if (s.t >= s.tmax) return kTrackDone;
-    const V3 pt = s.o + s.d * s.t;
-    const float dens = medium_density(m, pt);
-    if (kSample) return m.filterRenderRatio * dens * s.invMax > s.rng.next() ? kTrackCollide : kTrackRunning;
-    s.tr *= 1.0f - fmaxf(0.0f, m.filterRenderRatio * dens * s.invMax);
-    if (s.tr < 1.0f) {
-      const float p = 1.0f - s.tr;
-      if (s.rng.next() < p) {
-        s.tr = 0.0f;
-        return kTrackDone;
-      }
-      s.tr /= 1.0f - p;
-    }
-    return kTrackRunning;
+    s.tr /= 1.0f - p;
   }
+  return kTrackRunning;
 }
 
 // ---------------------------------------------------------------- Henyey-Greenstein

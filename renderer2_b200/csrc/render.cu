@@ -676,7 +676,12 @@ __device__ __forceinline__ void finish_tr(const RenderLaunch& L, uint32_t slot, 
 
 // Persistent tracking of the queued segments of round `round`: every lane
 // holds one segment, advances it L.trackSteps steps at a time, and takes the
-// next queued segment as soon as its own ends.
+// next queued segment as soon as its own ends.  With the brick-grid DDA a
+// lane that reaches a tentative collision holds it (pending) while the other
+// lanes keep stepping across majorant cells, and the pending collisions are
+// tested together once they are at least half of the warp's running lanes:
+// the test (Philox draws, indirection and atlas lookups) is the long branch
+// of a step, and divergent tests left most lanes idle.
 template <bool kDDA, bool kSample>
 __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
   uint32_t* mc = L.st.mc + kCountersPerBounce * L.bounce + (kSample ? 0 : kShadowCounters);
@@ -688,7 +693,7 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
   TrackState s;
   uint32_t owner = 0;
   int med = 0;
-  bool active = false, drained = false;
+  bool active = false, drained = false, pending = false;
   for (;;) {
     const bool need = !active && !drained;
     const unsigned want = __ballot_sync(0xffffffffu, need);
@@ -728,13 +733,39 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
       if (drained) break;
       continue;
     }
-    for (uint32_t k = 0; k < L.trackSteps && active; ++k) {
-      const int st = track_step<kDDA, kSample>(L.scene.media[med], s);
-      if (st != kTrackRunning) {
-        if (kSample && st == kTrackCollide) finish_collide(L, owner, med, s);
-        else if (kSample) finish_pass(L, owner, st, nextCount, nextList);
-        else finish_tr(L, owner, st, s, nextCount, nextList);
-        active = false;
+    if (kDDA) {
+      for (uint32_t k = 0; k < L.trackSteps; ++k) {
+        if (!__any_sync(0xffffffffu, active)) break;
+        int st = kTrackRunning;
+        if (active && !pending) {
+          st = track_dda_advance<kSample>(L.scene.media[med], s);
+          if (st == kTrackPending) {
+            pending = true;
+            st = kTrackRunning;
+          }
+        }
+        const unsigned held = __ballot_sync(0xffffffffu, pending);
+        const unsigned running = __ballot_sync(0xffffffffu, active && st == kTrackRunning);
+        if (held && 2 * __popc(held) >= __popc(running) && pending) {
+          st = track_dda_collide<kSample>(L.scene.media[med], s);
+          pending = false;
+        }
+        if (active && st != kTrackRunning) {
+          if (kSample && st == kTrackCollide) finish_collide(L, owner, med, s);
+          else if (kSample) finish_pass(L, owner, st, nextCount, nextList);
+          else finish_tr(L, owner, st, s, nextCount, nextList);
+          active = false;
+        }
+      }
+    } else {
+      for (uint32_t k = 0; k < L.trackSteps && active; ++k) {
+        const int st = track_step<kDDA, kSample>(L.scene.media[med], s);
+        if (st != kTrackRunning) {
+          if (kSample && st == kTrackCollide) finish_collide(L, owner, med, s);
+          else if (kSample) finish_pass(L, owner, st, nextCount, nextList);
+          else finish_tr(L, owner, st, s, nextCount, nextList);
+          active = false;
+        }
       }
     }
   }

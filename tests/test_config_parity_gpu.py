@@ -101,9 +101,19 @@ def test_surface_config_band_matches_oracle():
     row0 = 480
     p0, p1 = row0 * 1024, (row0 + 64) * 1024
     o = O.render(desc, cam, 64, 8, 0, p0, p1)
-    frac = _agree(g[p0:p1], o)
-    print(f"1024x1024 64 spp, rows {row0}..{row0 + 63}: {frac:.5f} of pixels within 1e-4")
-    assert frac >= PIX_FRAC
+    gb = g[p0:p1]
+    rel = (np.abs(gb - o) / np.maximum(1.0, np.abs(o))).max(axis=1)
+    q = {t: float((rel <= t).mean()) for t in (1e-4, 1e-3, 1e-2)}
+    print(f"1024x1024 64 spp, rows {row0}..{row0 + 63}: fraction of pixels within 1e-4 / 1e-3 / 1e-2: "
+          f"{q[1e-4]:.5f} / {q[1e-3]:.5f} / {q[1e-2]:.5f}, max {rel.max():.2e}")
+    # The environment here is lognormal(0, 1.5): neighbouring texels differ by
+    # orders of magnitude, so the last-bit differences of CUDA's and libm's
+    # acos/atan2/sin in the environment lookup move a bilinear lookup by more
+    # than 1e-4 of the pixel in a few tenths of a percent of the pixels.
+    assert q[1e-4] >= 0.995
+    assert q[1e-3] >= 0.9995
+    band = np.abs(gb.mean(0) - o.mean(0)) / np.abs(o.mean(0))
+    assert band.max() <= 1e-4
 
 
 def test_three_sigma_small_config_64x64():
