@@ -58,8 +58,12 @@ VOLUME_EXTEND_BYTES_PER_SEGMENT = 116.0
 SHADOW_MEDIA_BYTES_PER_SLOT = 48.0
 SHADE_BYTES_PER_SEGMENT = 256.0
 VOLUME_CFG = dict(grid=256, n_quads=200_000, ico_subdiv=6, width=1920, height=1080, spp=16, depth=16, seed=0)
-VOLUME_BATCH_CFG = dict(scenes=16, grids=(128, 192, 256, 160), quads=(50_000, 150_000, 300_000), ico=(6, 7),
-                        width=1920, height=1080, spp=2, depth=16)
+# one grid size per scene, 128^3 to 512^3 (config: "128^3-512^3")
+VOLUME_BATCH_CFG = dict(scenes=16, grids=(128, 192, 256, 384, 512, 160, 224, 320, 128, 192, 256, 384, 144, 176, 208,
+                                          288),
+                        quads=(50_000, 150_000, 300_000), ico=(6, 7), width=1920, height=1080, spp=4, depth=16,
+                        frame_spp=256)
+SMALL_CFG = dict(grid=32, spv=64, iters=10, width=256, height=256, spp=16, depth=8)
 SERVE_CFG = dict(jobs=60, rate=40.0, slots=4, budget=40 << 30)
 # forest leg: the forest generator's disc (radius 1000, 100,000 placement attempts) of three synthetic tree
 # models, each filtered into 4 LODs; LODs chosen on the GPU for the generator's camera at 1920x1080
@@ -185,6 +189,12 @@ def render_workload():
     return desc, cam, prm
 
 
+def filter_workload_params():
+    from renderer2_b200 import filter as F
+    c = FILTER_CFG
+    return (F.params(samples_per_voxel=c["spv"], iterations=c["iters"]), None)
+
+
 def filter_workload():
     from renderer2_b200 import filter as F
     from renderer2_b200 import scenes
@@ -236,8 +246,9 @@ def cpu_render_sample(desc, cam, prm, budget_s=15.0, threads=0):
                       f"BVH build included per call"}
 
 
-def cpu_filter_sample(mesh, mat, prm, vs, budget_s=15.0, threads=0):
-    """Oracle voxels/s on contiguous z-slices at the grid centre (BVH build subtracted)."""
+def cpu_filter_sample(mesh, mat, prm, vs, budget_s=15.0, threads=0, keep=None):
+    """Oracle voxels/s on contiguous z-slices at the grid centre (BVH build subtracted).  keep (a dict):
+    receives the first slab's voxel range and the oracle's FP64 records of it ("v0", "v1", "wide")."""
     import oracle_lib as O
     from renderer2_b200 import _native as N
     m2w = N.identity43()
@@ -252,8 +263,10 @@ def cpu_filter_sample(mesh, mat, prm, vs, budget_s=15.0, threads=0):
     while True:
         v0, v1 = z * slab, min((z + nsl) * slab, nx * ny * nz)
         t0 = time.perf_counter()
-        O.filter_voxels(mesh, O.material_from(mat), m2w, g, O.params_from(prm), v0, v1, 0, cores)
+        ow, _ = O.filter_voxels(mesh, O.material_from(mat), m2w, g, O.params_from(prm), v0, v1, 0, cores)
         t_work += max(time.perf_counter() - t0 - t_build, 1e-9)
+        if keep is not None and "wide" not in keep:
+            keep.update(v0=v0, v1=v1, wide=ow)
         done += v1 - v0
         z += nsl
         if t_work >= budget_s or z >= nz:
@@ -265,6 +278,33 @@ def cpu_filter_sample(mesh, mat, prm, vs, budget_s=15.0, threads=0):
 
 
 # ------------------------------------------------------------------ native legs
+
+def filter_accuracy(gw, gh, ow):
+    """Largest relative errors of the FP32 records (gw) and the FP16 payload (gh) against the oracle's FP64 ones
+    (ow) over the voxels with hits: density relative to itself, S entries relative to the voxel's largest
+    diagonal entry."""
+    h = (ow[:, 17] > 0) & np.isfinite(ow[:, 0])
+    scale = np.max(np.abs(ow[h, 1:4]), axis=1, keepdims=True)
+    out = {"voxels_compared": int(h.sum()), "hits_bit_exact": bool(np.array_equal(gw[:, 17], ow[:, 17]))}
+    for name, rec in (("fp32", gw), ("fp16", gh)):
+        out[name] = {"density": float((np.abs(rec[h, 0] - ow[h, 0]) / np.abs(ow[h, 0])).max(initial=0.0)),
+                     "S": float((np.abs(rec[h, 1:7] - ow[h, 1:7]) / scale).max(initial=0.0))}
+    return out
+
+
+def gpu_filter_records(sc, g, prm, v0, v1):
+    """FP32 records and FP16 payloads of voxels [v0, v1) from one untimed GPU pass."""
+    import torch
+    nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+    out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    wide = torch.empty(nvox * 20, dtype=torch.float32, device="cuda")
+    f16 = torch.empty(nvox * 8, dtype=torch.float16, device="cuda")
+    sc.run(g, prm, out.data_ptr(), wide.data_ptr(), f16.data_ptr())
+    torch.cuda.synchronize()
+    gw = wide.view(nvox, 20)[v0:v1].cpu().numpy().astype(np.float64)
+    gh = f16.view(nvox, 8)[v0:v1].cpu().numpy().astype(np.float64)
+    return gw, gh
+
 
 def bench_render(args, world, local):
     import torch
@@ -371,10 +411,16 @@ def bench_render(args, world, local):
                 bvh_build_ms=build_ms, render_ms=total_ms / args.steps - build_ms, desc=desc, cam=cam, prm=prm)
 
 
-def bench_filter(args, world, local):
+def bench_filter(args, world, local, grid=None, steps=None, warmup=None, e2e_run=True, mesh_mat=None):
+    """Filter at scale (500k leaf quads, 256 spv, 20 iterations) on the 256^3 grid, or `grid`^3."""
     import torch
     from renderer2_b200 import filter as F
-    mesh, mat, prm, vs = filter_workload()
+    from renderer2_b200 import scenes
+    mesh, mat, prm, vs = filter_workload() if mesh_mat is None else (mesh_mat + filter_workload_params())
+    if grid is not None:
+        vs = scenes.voxel_size_for(mesh, grid)
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     sc = F.FilterScene(mesh, mat)
     g = sc.grid(vs)
     nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
@@ -382,7 +428,7 @@ def bench_filter(args, world, local):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
     st = np.zeros(3)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         flush.fill_(1)
         sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
     torch.cuda.synchronize()
@@ -390,7 +436,7 @@ def bench_filter(args, world, local):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     step_ms, kernel_ms, cand = 0.0, [], []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.fill_(1)  # 256 MiB write evicts L2 between steps
         ev0.record()
         sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
@@ -401,19 +447,29 @@ def bench_filter(args, world, local):
         cand.append(st[1])
     _barrier(world)
     total_ms = _max_over_ranks(step_ms, world)
-    value = world * nvox * args.steps / (total_ms / 1e3)
+    value = world * nvox * steps / (total_ms / 1e3)
     h2d = mesh.positions.nbytes + mesh.indices.nbytes + mesh.normals.nbytes
-    # end to end: r2_filter_mesh with the mesh in host memory and the payloads copied into a pinned host buffer
-    # (upload, BVH build, classification, sampling, download, every step)
-    hout = torch.empty(nvox * 32, dtype=torch.uint8).pin_memory()
-    e2e_ms = []
-    for k in range(max(2, min(args.steps, 3))):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        F.filter_mesh(mesh, mat, prm, vs, out_ptr=hout.data_ptr(), out_capacity=nvox)
-        if k:  # the first call warms the host buffer and the device allocations
-            e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    del out, flush
+    # the central z-slice's FP32 records and FP16 payloads (untimed), for the accuracy against the oracle
+    nx, ny, nz = g.num_voxels[:]
+    slab = (nz // 2 * nx * ny, (nz // 2 + 1) * nx * ny)
+    gpu_slab = gpu_filter_records(sc, g, prm, *slab)
+    e2e = None
+    if e2e_run:
+        # end to end: r2_filter_mesh with the mesh in host memory and the payloads copied into a pinned host
+        # buffer (upload, BVH build, classification, sampling, download, every step)
+        hout = torch.empty(nvox * 32, dtype=torch.uint8).pin_memory()
+        e2e_ms = []
+        for k in range(max(2, min(steps, 3))):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            F.filter_mesh(mesh, mat, prm, vs, out_ptr=hout.data_ptr(), out_capacity=nvox)
+            if k:  # the first call warms the host buffer and the device allocations
+                e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+        del hout
+        e2e = {"value": world * nvox / (e2e_ms / 1e3), "unit": "voxels/s", "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(nvox * 32), "ms_per_step": e2e_ms}
     kms = float(np.mean(kernel_ms))
     peak, peak_kind = _peaks()
     alg = FILTER_BYTES_PER_VOXEL * nvox
@@ -422,12 +478,16 @@ def bench_filter(args, world, local):
     rays = float(np.mean(cand)) * FILTER_CFG["spv"]
     # arithmetic figure from the counting build of the same kernel (untimed):
     # 24 FLOPs per inner node visited, 30 per triangle tested, 40 per ray
-    n_rays, n_nodes, n_tris = sc.count(g, prm, out.data_ptr())
+    cnt_out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    n_rays, n_nodes, n_tris = sc.count(g, prm, cnt_out.data_ptr())
+    del cnt_out
     flops = 24.0 * n_nodes + 30.0 * n_tris + 40.0 * n_rays
     fp32_peak = FP32_NOMINAL_TFLOPS
     sc.close()
-    return {"metric": "filtered voxels/s", "value": value, "unit": "voxels/s", "ms_per_step": total_ms / args.steps,
-            "config": {"workload": "filter at scale: 500k leaf quads (1M tris), 256^3, 256 spv, 20 iters",
+    n = grid or FILTER_CFG["grid"]
+    return {"metric": "filtered voxels/s", "value": value, "unit": "voxels/s", "ms_per_step": total_ms / steps,
+            "steps": steps,
+            "config": {"workload": f"filter at scale: 500k leaf quads (1M tris), {n}^3, 256 spv, 20 iters",
                        "voxels": nvox, "candidate_voxels": float(np.mean(cand)),
                        "l2": "256 MiB flush write between steps"},
             "roofline": {"bound": "hbm", "kernel": "k_filter_sample", "achieved": achieved, "peak": peak,
@@ -441,9 +501,140 @@ def bench_filter(args, world, local):
                                   "flops_per_launch": flops, "rays": n_rays, "inner_nodes_visited": n_nodes,
                                   "triangles_tested": n_tris,
                                   "formula": "24 per inner node visited + 30 per triangle tested + 40 per ray"}},
-            "e2e": {"value": world * nvox / (e2e_ms / 1e3), "unit": "voxels/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(nvox * 32), "ms_per_step": e2e_ms},
-            "gpu_launches": 2 * args.steps, "_mesh": (mesh, mat, prm, vs)}
+            "e2e": e2e,
+            "gpu_launches": 2 * steps, "_mesh": (mesh, mat, prm, vs), "_gpu_slab": (slab, gpu_slab)}
+
+
+def surface_roofline(st, S, spp, launches):
+    """HBM roofline of the dominant surface traversal kernel from r2_render_device's stats of a frame: per-wave
+    kernel times, segments and shadow rays of the frame, S samples per wave."""
+    seg_wave, sh_wave = st[2] * S / spp, st[3] * S / spp
+    ext, shd = st[4], st[6]
+    dom_ext = ext >= shd
+    alg = EXTEND_BYTES_PER_SEGMENT * seg_wave if dom_ext else SHADOW_BYTES_PER_RAY * sh_wave
+    kms = ext if dom_ext else shd
+    peak, kind = _peaks()
+    achieved = alg / (kms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "k_extend" if dom_ext else "k_shadow_surfaces", "achieved": achieved,
+            "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": kind,
+            "alg_bytes_per_launch": alg / launches, "avg_launch_ms": kms / launches, "samples_per_wave": S}
+
+
+def bench_small(args, world, local):
+    """Plain method, small: icosphere subdivision 4 (5,120 triangles) displaced by value noise 0.05, GGX
+    roughness 0.3, albedo 0.8; SGGX filter to 32^3 (64 spv, 10 iterations) and a 256x256 frame (16 spp, depth
+    8, constant white environment).  A step filters the grid and renders the frame (BVH build from the resident
+    triangles + trace), on resident scenes; each part is timed on the stream."""
+    import torch
+    import oracle_lib as O
+    from renderer2_b200 import filter as F
+    from renderer2_b200 import raytracer as R
+    from renderer2_b200 import render_scenes as RS
+    from renderer2_b200 import scenes
+    c = SMALL_CFG
+    desc, cam = RS.icosphere_scene()
+    mesh, mat, m2w = desc["meshes"][0]
+    fprm = F.params(samples_per_voxel=c["spv"], iterations=c["iters"])
+    fsc = F.FilterScene(mesh, mat)
+    g = fsc.grid(scenes.voxel_size_for(mesh, c["grid"]))
+    nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+    out = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+    sc = RS.build_scene(desc)
+    prm = R.params(c["spp"], c["depth"], 0)
+    tuning = sc.autotune(cam, prm).as_dict()
+    npix = cam.width * cam.height
+    frame = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    fst, rst = np.zeros(3), np.zeros(8)
+    for _ in range(args.warmup):
+        fsc.run(g, fprm, out.data_ptr(), stream=stream)
+        sc.rebuild(stream)
+        sc.render_device(cam, prm, frame.data_ptr(), stream)
+    torch.cuda.synchronize()
+    _barrier(world)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    fk, rs = [], []
+    for k in range(args.steps):
+        ev[k][0].record()
+        fsc.run(g, fprm, out.data_ptr(), stream=stream, stats=fst)
+        ev[k][1].record()
+        sc.rebuild(stream)
+        sc.render_device(cam, prm, frame.data_ptr(), stream, stats=rst)
+        ev[k][2].record()
+        fk.append(fst[2])
+        rs.append(rst.copy())
+    torch.cuda.synchronize()
+    _barrier(world)
+    f_ms = _max_over_ranks(sum(e[0].elapsed_time(e[1]) for e in ev), world)
+    r_ms = _max_over_ranks(sum(e[1].elapsed_time(e[2]) for e in ev), world)
+    paths = npix * c["spp"]
+    S = sc.wave_samples(cam, prm)
+    rst = np.mean(np.array(rs), axis=0)
+    peak, kind = _peaks()
+    kms = float(np.mean(fk))
+    fachieved = FILTER_BYTES_PER_VOXEL * nvox / (kms / 1e3) / 1e9
+    # end to end, host buffers: the filter through r2_filter_mesh into pinned memory; the frame through the
+    # vertex upload from pinned memory, the BVH rebuild and r2_render_host into pinned memory
+    hv = torch.empty(nvox * 32, dtype=torch.uint8).pin_memory()
+    pos, nrm = RS.world_vertices(desc)
+    hp, hn = torch.from_numpy(pos).pin_memory(), torch.from_numpy(nrm).pin_memory()
+    hf = torch.empty(npix * 3, dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        F.filter_mesh(mesh, mat, fprm, scenes.voxel_size_for(mesh, c["grid"]), out_ptr=hv.data_ptr(),
+                      out_capacity=nvox)
+        sc.set_vertices(hp.data_ptr(), hn.data_ptr(), nverts=pos.shape[0])
+        sc.rebuild()
+        sc.render(cam, prm, out_ptr=hf.data_ptr())
+
+    e2e_step()
+    e2e_ms = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    # accuracy at this configuration: the whole grid against the FP64 oracle, the frame against the oracle's
+    gw, gh = gpu_filter_records(fsc, g, fprm, 0, nvox)
+    acc, cpu = None, None
+    gframe = hf.numpy().reshape(-1, 3).copy()
+    if world == 1:
+        t0 = time.perf_counter()
+        ow, _ = O.filter_voxels(mesh, O.material_from(mat), m2w, O.grid_from(g), O.params_from(fprm))
+        t_f = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        of = O.render(desc, cam, c["spp"], c["depth"], 0)
+        t_r = time.perf_counter() - t0
+        rel = (np.abs(gframe - of) / np.maximum(1.0, np.abs(of))).max(axis=1)
+        acc = {"filter": filter_accuracy(gw, gh, ow),
+               "frame_pixels_within_1e-4_of_oracle": float((rel <= 1e-4).mean())}
+        cores = os.cpu_count() or 1
+        cpu = {"filter": {"value": nvox / t_f, "unit": "voxels/s", "cores": cores, "kind": "port",
+                          "sample": f"the whole {c['grid']}^3 grid (BVH build included)"},
+               "render": {"value": paths / t_r, "unit": "paths/s", "cores": cores, "kind": "port",
+                          "sample": f"the whole {cam.width}x{cam.height} frame at {c['spp']} spp (BVH build included)"}}
+    fsc.close()
+    sc.close()
+    total_ms = f_ms + r_ms
+    return {"metric": "filtered voxels/s; paths/s", "value": world * nvox * args.steps / (f_ms / 1e3),
+            "unit": "voxels/s", "paths_per_s": world * paths * args.steps / (r_ms / 1e3),
+            "ms_per_step": total_ms / args.steps, "filter_ms_per_step": f_ms / args.steps,
+            "render_ms_per_step": r_ms / args.steps,
+            "config": {"workload": "plain method, small: icosphere subdivision 4 (5,120 tris) displaced 0.05, GGX 0.3 "
+                                   "albedo 0.8; SGGX filter to 32^3, 64 spv, 10 iterations; 256x256, 16 spp, depth 8, "
+                                   "constant white environment", "voxels": nvox, "paths_per_step": paths,
+                       "tuning": tuning, "l2": "small inputs: L2-resident (reported as such)"},
+            "roofline": {"filter": {"bound": "hbm", "kernel": "k_filter_sample", "achieved": fachieved, "peak": peak,
+                                    "unit": "GB/s", "frac": fachieved / peak, "peak_source": kind,
+                                    "kernel_ms": kms},
+                         "render": surface_roofline(rst, S, c["spp"], c["depth"])},
+            "e2e": {"value": world * nvox / (e2e_ms / 1e3), "unit": "voxels/s",
+                    "paths_per_s": world * paths / (e2e_ms / 1e3), "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": int(mesh.positions.nbytes + mesh.indices.nbytes + mesh.normals.nbytes
+                                              + pos.nbytes + nrm.nbytes),
+                    "d2h_bytes_per_step": int(nvox * 32 + npix * 12)},
+            "accuracy": acc, "cpu_baseline": cpu,
+            "gpu_launches": (2 + BVH_BUILD_LAUNCHES + (c["spp"] // S) * (2 + 4 * c["depth"])) * args.steps}
 
 
 def bench_volume(args, world, local):
@@ -720,7 +911,7 @@ def bench_volume_batch(args, world, local):
     shutil.rmtree(work, ignore_errors=True)
     return {"metric": "paths/s", "value": world * paths * args.steps / (ms_batch / 1e3), "unit": "paths/s",
             "ms_per_step": ms_batch / args.steps,
-            "config": {"workload": f"{c['scenes']} batched volume scenes: foliage grids {c['grids']}^3 of "
+            "config": {"workload": f"{c['scenes']} batched volume scenes: foliage grids {sorted(set(c['grids']))}^3 of "
                                    f"{c['quads']} quads (SGGX media, brick-grid DDA) + icosphere meshes "
                                    f"(81,920 / 327,680 tris), {c['width']}x{c['height']}, {c['spp']} spp per step, "
                                    f"depth {c['depth']}, one captured graph per sample",
@@ -729,6 +920,10 @@ def bench_volume_batch(args, world, local):
             "one_scene_at_a_time": {"value": world * paths * args.steps / (ms_seq / 1e3),
                                     "ms_per_step": ms_seq / args.steps},
             "speedup_vs_one_at_a_time": ms_seq / ms_batch,
+            "frames_256spp_ms": ms_batch / args.steps / c["spp"] * c["frame_spp"],
+            "frames_256spp_note": "the 16 frames at the configuration's 256 spp: the graph replays one sample of every "
+                                  "scene per replay, so a full frame set is 256 replays; time per replay measured "
+                                  f"over {args.steps} steps of {c['spp']} replays",
             "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(sum(npix) * 12), "ms_per_step": e2e_ms},
             "gpu_launches": c["spp"] * c["scenes"] * (3 + _media_launches(tuned.as_dict()) * c["depth"]) * args.steps}
@@ -924,6 +1119,7 @@ def run_native(args):
         f = bench_filter(args, world, local)
         if rank == 0:
             mesh, mat, prm, vs = f.pop("_mesh")
+            f.pop("_gpu_slab")
             f.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                       "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)"})
             if world == 1:
@@ -934,7 +1130,12 @@ def run_native(args):
             dist.destroy_process_group()
         return
     r = bench_render(args, world, local)
+    small = bench_small(args, world, local) if not args.skip_small else None
     f = bench_filter(args, world, local) if not args.skip_filter else None
+    f512 = None
+    if f is not None and not args.skip_512:
+        mesh1m, mat1m = f["_mesh"][0], f["_mesh"][1]
+        f512 = bench_filter(args, world, local, grid=512, steps=1, warmup=1, e2e_run=False, mesh_mat=(mesh1m, mat1m))
     vol = bench_volume(args, world, local) if not args.skip_volume else None
     vbatch = bench_volume_batch(args, world, local) if not args.skip_volume else None
     forest = bench_forest(args, world, local) if not args.skip_volume else None
@@ -951,12 +1152,23 @@ def run_native(args):
                                    "tuning": r["tuning"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"]}
-        if f is not None:
-            mesh, mat, prm, vs = f.pop("_mesh")
+        if small is not None:
+            line["small"] = small
+            line["gpu_launches"] += small["gpu_launches"]
+        for key, leg in (("filter", f), ("filter_512", f512)):
+            if leg is None:
+                continue
+            mesh, mat, prm, vs = leg.pop("_mesh")
+            (v0, v1), (gw, gh) = leg.pop("_gpu_slab")
             if world == 1:
-                f["cpu_baseline"] = cpu_filter_sample(mesh, mat, prm, vs, budget_s=args.cpu_budget)
-            line["filter"] = f
-            line["gpu_launches"] += f["gpu_launches"]
+                keep = {}
+                budget = args.cpu_budget if key == "filter" else max(5.0, args.cpu_budget / 2)
+                leg["cpu_baseline"] = cpu_filter_sample(mesh, mat, prm, vs, budget_s=budget, keep=keep)
+                if keep.get("v0") == v0 and keep.get("v1") == v1:
+                    leg["accuracy"] = filter_accuracy(gw, gh, keep["wide"])
+                    leg["accuracy"]["sample"] = "the central z-slice, FP32 records and FP16 payload vs the FP64 oracle"
+            line[key] = leg
+            line["gpu_launches"] += leg["gpu_launches"]
         if vol is not None:
             v, (vdesc, vcam, vprm) = vol
             if world == 1:
@@ -997,9 +1209,17 @@ def legs_summary(line: dict) -> dict:
             e["hbm_frac"] = _short(rf.get("frac"), 3)
             if isinstance(rf.get("fp32"), dict):
                 e["fp32_frac"] = _short(rf["fp32"].get("frac"), 3)
-        for k in ("p50_latency_s", "p99_latency_s", "speedup", "max_rel_err_fp16_vs_fp64"):
+        for k in ("paths_per_s", "p50_latency_s", "p99_latency_s", "speedup_vs_one_at_a_time"):
             if k in d:
-                e[k] = _short(d[k], 3)
+                e[k] = _short(d[k], 4)
+        if isinstance(rf, dict) and "filter" in rf and "render" in rf:
+            e["hbm_frac"] = {"filter": _short(rf["filter"]["frac"], 3), "render": _short(rf["render"]["frac"], 3)}
+        acc = d.get("accuracy")
+        if isinstance(acc, dict):
+            fa = acc.get("filter", acc)
+            if "fp16" in fa:
+                e["fp16_vs_fp64"] = _short(max(fa["fp16"]["density"], fa["fp16"]["S"]), 3)
+                e["fp32_vs_fp64"] = _short(max(fa["fp32"]["density"], fa["fp32"]["S"]), 3)
         out[name] = e
 
     leg("headline", line)
@@ -1137,6 +1357,8 @@ def main():
     ap.add_argument("--skip-volume", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--skip-render", action="store_true", help="run only the filter leg")
+    ap.add_argument("--skip-small", action="store_true", help="skip the small configuration's leg")
+    ap.add_argument("--skip-512", action="store_true", help="skip the 512^3 filter leg")
     ap.add_argument("--case", default=None,
                     help="profiling case: render-wave | filter-small | volume-small | volume-mid | volume-batch | forest | "
                          "forest-small | serving")
