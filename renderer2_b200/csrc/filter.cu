@@ -25,9 +25,6 @@ namespace r2 {
 namespace {
 
 constexpr int kSampleWarps = 4;  // warps per block of the sampling kernel
-constexpr int kFilterVisits = 32;  // BVH visits a lane makes between sample hand-outs
-constexpr int kFilterRefill = 8;   // free lanes of a warp that trigger a hand-out
-constexpr int kFilterMaxVisits = 1 << 26;  // visits after which a ray is ended (a correct traversal visits each node once)
 
 __device__ __forceinline__ V3 voxel_center(const FilterLaunch& L, int x, int y, int z) {
   V3 pm = xform_point(L.indexToModel, v3((float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f));
@@ -198,8 +195,6 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
   const float radius = 1.1f * length(L.voxelSize) / 2.0f;
   const float tMaxFixed = L.voxelSize.x;
   uint32_t cRays = 0, cNodes = 0, cTris = 0;  // counting build only
-  int stack[R2_BVH_STACK];
-  float stackT[R2_BVH_STACK];
   while (true) {
     uint32_t w = 0;
     if (lane == 0) w = atomicAdd(&L.counters[1], 1u);
@@ -226,60 +221,15 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
     dist = csum0();
     uint32_t hits = 0;
 
-    // Samples are handed out within the warp as lanes become free: a lane
-    // whose ray has finished takes the voxel's next sample (once kFilterRefill
-    // lanes are free), so rays of very different traversal lengths do not
-    // leave most lanes waiting for the slowest.  Sample s reads its own Philox
-    // streams whichever lane traces it.
-    uint32_t next = 0;  // warp-uniform: the next sample to hand out
-    bool busy = false;
-    uint32_t smp = 0;
-    float smpT = 0.0f;
-    int spent = 0;
-    TraceState tr;
-    const bool alphaTest = L.bvh.alpha.alphaTex != nullptr;
-    while (true) {
-      if (next < L.spv) {
-        const unsigned idle = __ballot_sync(0xFFFFFFFFu, !busy);
-        const int nIdle = __popc(idle);
-        if (nIdle >= kFilterRefill || idle == 0xFFFFFFFFu) {
-          const uint32_t k = next + (uint32_t)__popc(idle & ((1u << lane) - 1u));
-          if (!busy && k < L.spv) {
-            const U4 r0 = philox4x32_10(u4(k, 0u, L.lod, 0u), vid, L.seed);
-            const U4 r1 = philox4x32_10(u4(k, 1u, L.lod, 0u), vid, L.seed);
-            const V3 oi = cv + v3(u01(r0.x), u01(r0.y), u01(r0.z));
-            const V3 o = xform_point(L.indexToWorld, oi);
-            const V3 d = uniform_sample_sphere(u01(r0.w), u01(r1.x));
-            smpT = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
-            trace_begin(tr, o, d, smpT, root);
-            smp = k;
-            spent = 0;
-            busy = true;
-          }
-          next += (uint32_t)nIdle;
-        }
-      }
-      if (__ballot_sync(0xFFFFFFFFu, busy) == 0) {
-        if (next >= L.spv) break;
-        continue;
-      }
-      if (!busy) continue;
-      bool done = alphaTest ? trace_advance<false, kCount, true>(L.bvh, tr, stack, stackT, kFilterVisits)
-                            : trace_advance<false, kCount, false>(L.bvh, tr, stack, stackT, kFilterVisits);
-      spent += kFilterVisits;
-      if (!done && spent >= kFilterMaxVisits) {  // a corrupted tree: the ray ends as a miss
-        tr.best.tri = -1;
-        done = true;
-      }
-      if (!done) continue;
-      busy = false;
-      if (kCount) {
-        ++cRays;
-        cNodes += tr.nodes;
-        cTris += tr.tris;
-      }
-      const Hit h = tr.best;
-      const float tmax = smpT;
+    for (uint32_t s = lane; s < L.spv; s += 32) {
+      const U4 r0 = philox4x32_10(u4(s, 0u, L.lod, 0u), vid, L.seed);
+      const U4 r1 = philox4x32_10(u4(s, 1u, L.lod, 0u), vid, L.seed);
+      const V3 oi = cv + v3(u01(r0.x), u01(r0.y), u01(r0.z));
+      const V3 o = xform_point(L.indexToWorld, oi);
+      const V3 d = uniform_sample_sphere(u01(r0.w), u01(r1.x));
+      const float tmax = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
+      const Hit h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris, root);
+      if (kCount) ++cRays;
       float tsv = -1.0f;
       if (h.tri >= 0) {
         const float4 n0 = __ldg(&L.triN[3 * h.tri]);
@@ -321,7 +271,7 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
         ++hits;
         tsv = tmax;
       }
-      myTs[smp] = tsv;
+      myTs[s] = tsv;
     }
 
     // warp reductions (butterfly: every lane ends with the same totals)
