@@ -11,9 +11,11 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
+#include "r2_host_texfetch.h"
 #include <cuda_runtime.h>
 #include <glm/glm.hpp>
 #include "utility/qualifiers.hpp"
@@ -31,52 +33,97 @@
 #include "medium/sggx_phase_function.hpp"
 #include "shapes/sphere.hpp"
 #include "utility/functions.hpp"
-// CMeshFilter with the scene, scene object and material shims of refshim/;
-// the oracle's BVH and closest-hit trace stand in for OptiX.
+// CMeshFilter and CPathIntegrator with the scene and scene-object shims of
+// refshim/; the oracle's BVH and closest-hit trace stand in for OptiX, the
+// oracle's environment map for CEnvironmentMap (whose CDistribution2D g++
+// cannot compile), and camera.cu is compiled from the reference's sources.
 #include "filtering/mesh_filter.hpp"
+#include "integrators/path_integrator_impl.hpp"
+#include "camera/camera.cu"
 #include "oracle.h"
+#include "render_oracle.h"
+
+// The CMaterial constructors and destructor live in material.cu with the
+// assimp material import; the plain ones initialise the members as written
+// there (material.cu:8-53, 68-72), and nothing here owns a mesh path.
+namespace rt {
+CMaterial::CMaterial(const glm::vec3& diffuseColor, const glm::vec3& glossyColor, const COrenNayarBRDF& diffuse,
+                     const CMicrofacetBRDF& glossy)
+    : m_deviceObject(false), m_Le(0.f), m_diffuseColor(diffuseColor), m_glossyColor(glossyColor),
+      m_orenNayarBRDF(diffuse), m_microfacetBRDF(glossy), m_albedoTexture(nullptr), m_glossyTexture(nullptr),
+      m_normalTexture(nullptr), m_alphaTexture(nullptr), m_pathLength(0), m_meshPath(nullptr), m_submeshId(0) {}
+CMaterial::~CMaterial() {}
+}  // namespace rt
 
 namespace r2ref {
 static std::vector<float> g_queue;
 static size_t g_pos = 0;
 float next_curand() { return g_pos < g_queue.size() ? g_queue[g_pos++] : 0.5f; }
 
-// Filter scene of the CDeviceScene shim: the oracle's BVH over the
-// world-space triangles, model-space vertex normals, the object's transform
-// and its material.
-struct FilterHookScene {
+// Scene of the CDeviceScene shim: the oracle's BVH over world-space
+// triangles, model-space vertex normals, per triangle its object (transform)
+// and material; the environment map (row 0 = top, RGB) for NEE and misses.
+struct HookScene {
   std::vector<int32_t> nodes;
-  std::vector<uint32_t> order, idx;
+  std::vector<uint32_t> order, idx, triObj;
   std::vector<float> tris, nrm;
-  glm::mat4x3 m2w{1.f};
-  rt::CMaterial mat;
-  float ior = 1.f;
+  std::vector<glm::mat4x3> m2w;
+  std::vector<std::unique_ptr<rt::CMaterial>> mats;  // per object
+  std::vector<float> env;
+  int envW = 0, envH = 0;
+  unsigned int mask = 0;  // visibility of the objects (ESceneobjectMask)
   bool ready = false;
 };
-static FilterHookScene g_fs;
+static HookScene g_fs;
 
-// __closesthit__ch (shaders.optix.cu:28-130) for an untextured mesh: the
-// normal interpolated from the vertex normals with the hit's barycentrics,
-// normalised, taken to world space by the object's transform and normalised.
+// __closesthit__ch (shaders.optix.cu:28-130) for untextured meshes: the hit
+// position o + t d, the normal interpolated from the vertex normals with the
+// hit's barycentrics and normalised, taken to world space by the object's
+// transform and normalised; the object's material and its ior.
 void scene_intersect(const rt::CRay& ray, rt::SInteraction* si, unsigned int mask) {
   si->hitInformation.hit = false;
-  if (!(mask & rt::ESceneobjectMask::FILTER) || !g_fs.ready) return;
+  if (!(mask & g_fs.mask) || !g_fs.ready) return;
   float t = 0.f, b1 = 0.f, b2 = 0.f;
   const int tri = orc_trace(g_fs.nodes.data(), g_fs.tris.data(), ray.m_origin.x, ray.m_origin.y, ray.m_origin.z,
                             ray.m_direction.x, ray.m_direction.y, ray.m_direction.z, ray.m_t_max, &t, &b1, &b2);
   if (tri < 0) return;
-  const uint32_t* v = &g_fs.idx[3 * (size_t)g_fs.order[tri]];
+  const uint32_t prim = g_fs.order[tri];
+  const uint32_t* v = &g_fs.idx[3 * (size_t)prim];
+  const uint32_t obj = g_fs.triObj[prim];
   auto N = [&](uint32_t k) { return glm::vec3(g_fs.nrm[3 * k], g_fs.nrm[3 * k + 1], g_fs.nrm[3 * k + 2]); };
   glm::vec3 n = glm::normalize((1.f - b1 - b2) * N(v[0]) + b1 * N(v[1]) + b2 * N(v[2]));
-  n = glm::normalize(g_fs.m2w * glm::vec4(n, 0.f));
+  n = glm::normalize(g_fs.m2w[obj] * glm::vec4(n, 0.f));
   si->hitInformation.hit = true;
+  si->hitInformation.pos = glm::vec3(ray.m_origin.x + t * ray.m_direction.x, ray.m_origin.y + t * ray.m_direction.y,
+                                     ray.m_origin.z + t * ray.m_direction.z);
   si->hitInformation.normal = n;
+  si->hitInformation.normalG = n;
   si->hitInformation.tc = glm::vec2(0.f);
-  si->hitInformation.ior = g_fs.ior;
+  si->hitInformation.ior = g_fs.mats[obj]->ior();
   si->hitInformation.t = t;
-  si->material = &g_fs.mat;
+  si->material = g_fs.mats[obj].get();
+}
+
+glm::vec3 scene_sample_light(float u0, float u1, glm::vec3* dir, float* pdf) {
+  float d[3], le[3];
+  orc_env_sample(g_fs.env.data(), g_fs.envW, g_fs.envH, u0, u1, d, pdf, le);
+  *dir = glm::vec3(d[0], d[1], d[2]);
+  return glm::vec3(le[0], le[1], le[2]);
+}
+
+glm::vec3 scene_le(const glm::vec3& dir, float* pdf) {
+  const float d[3] = {dir.x, dir.y, dir.z};
+  float le[3];
+  orc_env_le(g_fs.env.data(), g_fs.envW, g_fs.envH, d, pdf, le);
+  return glm::vec3(le[0], le[1], le[2]);
 }
 }  // namespace r2ref
+
+glm::vec3 rt::CDeviceScene::sampleLightSources(CSampler& sampler, glm::vec3* direction, float* pdf) const {
+  const float u0 = sampler.uniformSample01();  // CDistribution2D::sampleContinuous: the marginal's draw first
+  const float u1 = sampler.uniformSample01();
+  return r2ref::scene_sample_light(u0, u1, direction, pdf);
+}
 
 static void feed(const float* c, int n) {
   r2ref::g_queue.assign(c, c + n);
@@ -279,20 +326,70 @@ static glm::mat4x3 M43(const float* m) {
 // GGX alpha, ior).  Returns the BVH height, negative on failure.
 int ref_filter_scene(const float* wpos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
                      const float* m2w, const float* kd, const float* ks, float alpha, float ior) {
-  r2ref::FilterHookScene& fs = r2ref::g_fs;
+  r2ref::HookScene& fs = r2ref::g_fs;
   fs.nodes.assign(16 * (size_t)(ntris > 1 ? ntris - 1 : 1), 0);
   fs.order.assign(ntris, 0);
   fs.tris.assign(12 * (size_t)ntris, 0.f);
   fs.idx.assign(idx, idx + 3 * (size_t)ntris);
+  fs.triObj.assign(ntris, 0u);
   fs.nrm.assign(nrm, nrm + 3 * (size_t)nverts);
-  fs.m2w = M43(m2w);
-  fs.mat.kd = V(kd);
-  fs.mat.ks = V(ks);
-  fs.mat.alpha = alpha;
-  fs.ior = ior;
+  fs.m2w.assign(1, M43(m2w));
+  fs.mats.clear();
+  fs.mats.emplace_back(new rt::CMaterial(V(kd), V(ks), rt::COrenNayarBRDF(0.f),
+                                         rt::CMicrofacetBRDF(alpha, alpha, 1.f, ior)));
+  fs.mask = rt::ESceneobjectMask::FILTER;
   const int h = orc_build_bvh(wpos, nverts, idx, ntris, fs.nodes.data(), fs.order.data(), fs.tris.data());
   fs.ready = h >= 0;
   return h;
+}
+
+// Render scene of ref_path_li: world-space vertices and indices of all
+// meshes, model-space vertex normals, the object of each triangle, per object
+// its transform (12 floats) and material (Kd, Ks, GGX alpha, ior; Oren-Nayar
+// roughness 0 as for OBJ materials, material.cu:95), and the environment map.
+int ref_render_scene(const float* wpos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
+                     const uint32_t* triObj, uint32_t nobj, const float* m2w12, const float* mat8, const float* env,
+                     int envW, int envH) {
+  r2ref::HookScene& fs = r2ref::g_fs;
+  fs.nodes.assign(16 * (size_t)(ntris > 1 ? ntris - 1 : 1), 0);
+  fs.order.assign(ntris, 0);
+  fs.tris.assign(12 * (size_t)ntris, 0.f);
+  fs.idx.assign(idx, idx + 3 * (size_t)ntris);
+  fs.triObj.assign(triObj, triObj + ntris);
+  fs.nrm.assign(nrm, nrm + 3 * (size_t)nverts);
+  fs.m2w.clear();
+  fs.mats.clear();
+  for (uint32_t o = 0; o < nobj; ++o) {
+    fs.m2w.push_back(M43(m2w12 + 12 * o));
+    const float* m = mat8 + 8 * o;
+    fs.mats.emplace_back(new rt::CMaterial(V(m), V(m + 3), rt::COrenNayarBRDF(0.f),
+                                           rt::CMicrofacetBRDF(m[6], m[6], 1.f, m[7])));
+  }
+  fs.env.assign(env, env + 3 * (size_t)envW * envH);
+  fs.envW = envW;
+  fs.envH = envH;
+  fs.mask = rt::ESceneobjectMask::ALL;
+  const int h = orc_build_bvh(wpos, nverts, idx, ntris, fs.nodes.data(), fs.order.data(), fs.tris.data());
+  fs.ready = h >= 0;
+  return h;
+}
+
+// One sample of CPathIntegrator::Li (path_integrator_impl.hpp:120-247, with
+// direct(), :23-118) for pixel (px, py) of the camera CCamera(W, H, fov, pos,
+// lookAt, up) (camera.cu:20-31), the pixel sampled by CPixelSampler
+// (pixel_sampler.hpp:36-47), every draw taken from the queued cuRAND values c.
+// L3 receives Li() (NaN or infinite radiance becomes 0; one sample per pixel).
+// Returns the draws consumed.
+int ref_path_li(uint32_t W, uint32_t H, float fov, const float* pos, const float* lookAt, const float* up,
+                uint32_t px, uint32_t py, const float* c, int nc, float* L3) {
+  rt::CCamera cam((uint16_t)W, (uint16_t)H, fov, V(pos), V(lookAt), V(up));
+  feed(c, nc);
+  rt::CSampler sampler;
+  rt::CPixelSampler ps(&cam, (uint16_t)px, (uint16_t)py, &sampler);
+  rt::CDeviceScene scene;
+  rt::CPathIntegrator li(&scene, &ps, &sampler, 1, false, rt::EDebugMode::NONE);
+  put(L3, li.Li());
+  return ref_draws_used();
 }
 
 // CMeshFilter(voxel, grid...).run(scene, spv) (mesh_filter.hpp:24-122): the

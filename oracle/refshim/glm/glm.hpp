@@ -41,7 +41,8 @@ struct vec<3, T, Q> {
   vec(T a, T b_, T c) : x(a), y(b_), z(c) {}
   template <typename U> explicit vec(const vec<3, U, Q>& o)
       : x(static_cast<T>(o.x)), y(static_cast<T>(o.y)), z(static_cast<T>(o.z)) {}
-  template <typename U> explicit vec(const vec<4, U, Q>& o)
+  // implicit, as glm's conversions are unless GLM_FORCE_EXPLICIT_CTOR is defined
+  template <typename U> vec(const vec<4, U, Q>& o)
       : x(static_cast<T>(o.x)), y(static_cast<T>(o.y)), z(static_cast<T>(o.z)) {}
   template <typename U> vec& operator=(const vec<3, U, Q>& o) {
     x = static_cast<T>(o.x); y = static_cast<T>(o.y); z = static_cast<T>(o.z); return *this;
@@ -265,9 +266,12 @@ mat<C, R, T, Q> operator*(const mat<C, R, T, Q>& a, T s) {
   for (length_t i = 0; i < C; ++i) r.c[i] = a.c[i] * s;
   return r;
 }
-// matrix * column vector: sum_k col_k * v[k], left to right
+// matrix * column vector: sum_k col_k * v[k], left to right.  The vector's
+// type is not deduced (glm declares it as the matrix's row_type), so a vec4
+// converts to the vec3 a mat3 takes.
+template <length_t C, typename T, qualifier Q> struct vec_of { typedef vec<C, T, Q> type; };
 template <length_t C, length_t R, typename T, qualifier Q>
-vec<R, T, Q> operator*(const mat<C, R, T, Q>& m, const vec<C, T, Q>& v) {
+vec<R, T, Q> operator*(const mat<C, R, T, Q>& m, const typename vec_of<C, T, Q>::type& v) {
   vec<R, T, Q> r = m.c[0] * v[0];
   for (length_t k = 1; k < C; ++k) r = r + m.c[k] * v[k];
   return r;

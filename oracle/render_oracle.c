@@ -218,23 +218,39 @@ static float mat_pdf(const mat_t* m, f3 wo, f3 wi) {
   float w = fresnel(m->etaI, m->etaT, abs_cos_theta(wo));
   return on_pdf(wo, wi) * (1.0f - w) + mf_pdf(m, wo, wi) * w;
 }
+static int g_replay_swap_lobe = 0;  /* set with the replay: see orc_set_replay */
 static f3 mat_sample_f(const mat_t* m, f3 wo, float uSel, float u1, float u2, f3* wi, float* pdf) {
   float p = fresnel(m->etaI, m->etaT, abs_cos_theta(wo));
-  if (uSel < p) return mul3s(m->specular, mf_sample_f(m, wo, u1, u2, wi, pdf));
+  if (uSel < p) {
+    if (g_replay_swap_lobe) { const float t = u1; u1 = u2; u2 = t; }
+    return mul3s(m->specular, mf_sample_f(m, wo, u1, u2, wi, pdf));
+  }
   return mul3s(m->diffuse, on_sample_f(m, wo, u1, u2, wi, pdf));
 }
 
 /* ------------------------------------------------------------ frame, ray offset */
-typedef struct { f3 T, B, N; } frame_t;
+/* CCoordinateFrame::fromNormal (objects.hpp:31-41): tangentToWorld =
+ * mat3(T, B, N) by columns, worldToTangent = glm::inverse of it (cofactors
+ * over the determinant), kept as columns W0..W2. */
+typedef struct { f3 T, B, N, W0, W1, W2; } frame_t;
 static frame_t frame_from_normal(f3 N) {
   frame_t f;
   f.N = N;
   f.T = fabsf(N.x) > fabsf(N.y) ? div3s(F3(-N.z, 0.0f, N.x), sqrtf(N.x * N.x + N.z * N.z))
                                 : div3s(F3(0.0f, N.z, -N.y), sqrtf(N.y * N.y + N.z * N.z));
   f.B = norm3(cross3(N, f.T));
+  const f3 T = f.T, B = f.B;
+  const float det = T.x * (B.y * N.z - N.y * B.z) - B.x * (T.y * N.z - N.y * T.z) + N.x * (T.y * B.z - B.y * T.z);
+  const float inv = 1.0f / det;
+  f.W0 = F3(+(B.y * N.z - N.y * B.z) * inv, -(T.y * N.z - N.y * T.z) * inv, +(T.y * B.z - B.y * T.z) * inv);
+  f.W1 = F3(-(B.x * N.z - N.x * B.z) * inv, +(T.x * N.z - N.x * T.z) * inv, -(T.x * B.z - B.x * T.z) * inv);
+  f.W2 = F3(+(B.x * N.y - N.x * B.y) * inv, -(T.x * N.y - N.x * T.y) * inv, +(T.x * B.y - B.x * T.y) * inv);
   return f;
 }
-static f3 to_local(const frame_t* f, f3 v) { return F3(dot3(f->T, v), dot3(f->B, v), dot3(f->N, v)); }
+/* worldToTangent * v, summed column by column (glm's matrix-vector order) */
+static f3 to_local(const frame_t* f, f3 v) {
+  return add3(add3(mul3s(f->W0, v.x), mul3s(f->W1, v.y)), mul3s(f->W2, v.z));
+}
 static f3 to_world(const frame_t* f, f3 v) { return add3(add3(mul3s(f->T, v.x), mul3s(f->B, v.y)), mul3s(f->N, v.z)); }
 
 static float next_up(float v) {
@@ -481,6 +497,13 @@ static ray_t ray_off(ray_t r, f3 dir) {
   f3 end = add3(r.o, mul3s(r.d, r.tmax));
   f3 o = offset_origin(r.o, dir);
   return mkray(o, r.d, len3(sub3(end, o)));
+}
+/* CRay::spawnRay(p0, p1) (ray.hpp:62-69): origin offset from p0 towards p1,
+ * direction (p1 - p0) / |p1 - origin|, that length as tmax. */
+static ray_t spawn_ray(f3 p0, f3 p1) {
+  const f3 off = offset_origin(p0, norm3(sub3(p1, p0)));
+  const float tl = len3(sub3(p1, off));
+  return mkray(off, div3s(sub3(p1, p0), tl), tl);
 }
 
 typedef struct {
@@ -1140,7 +1163,28 @@ static int scene_occluded(const rscene_t* S, f3 o, f3 d, float tmax) {
   return 0;
 }
 
+/* Replay of trace_path's draws (test hook, orc_set_replay): while set, each
+ * Philox block of a surface path (camera, per bounce the shading blocks and
+ * the roulette block) is the next four words of the list, in the order the
+ * path asks for them; g_replay_swap exchanges the two direction draws of the
+ * GGX lobe, for a build that evaluates glm::vec2(u(), u()) right to left. */
+static const uint32_t* g_replay = NULL;
+static size_t g_replay_n = 0, g_replay_pos = 0;
+static int g_replay_swap = 0;
+
+void orc_set_replay(const uint32_t* words, size_t n, int vec2_swap) {
+  g_replay = words;
+  g_replay_n = n;
+  g_replay_pos = 0;
+  g_replay_swap = vec2_swap;
+  g_replay_swap_lobe = words ? vec2_swap : 0;
+}
+
 static void philox_u(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1, uint32_t out[4]) {
+  if (g_replay) {
+    for (int k = 0; k < 4; ++k) out[k] = g_replay_pos < g_replay_n ? g_replay[g_replay_pos++] : 0x80000000u;
+    return;
+  }
   uint32_t ctr[4] = {c0, c1, c2, c3}, key[2] = {k0, k1};
   orc_philox4x32_10(ctr, key, out);
 }
@@ -1148,11 +1192,12 @@ static void philox_u(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_
 /* intersectTr as direct() uses it: 0 when the walk ends on a surface, else
  * the product of the media's ratio-tracking estimates along the segments. */
 static float shadow_tr(const rscene_t* S, f3 o, f3 d, float tmax, int med, rng_t* rng, int* err) {
-  if (scene_occluded(S, o, d, tmax)) return 0.0f;
-  float tr = 1.0f;
-  if (S->nmedia == 0) return tr;
   f3 p0 = o;
   const f3 p1 = add3(o, mul3s(d, tmax));
+  const ray_t r0 = spawn_ray(p0, p1);
+  if (scene_occluded(S, r0.o, r0.d, r0.tmax)) return 0.0f;
+  float tr = 1.0f;
+  if (S->nmedia == 0) return tr;
   int cur = med;
   for (int k = 0; k < MAX_SHADOW_SEGMENTS; ++k) {
     const f3 off = offset_origin(p0, norm3(sub3(p1, p0)));
@@ -1353,14 +1398,9 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
         float spdf = mat_pdf(m, woT, lT);
         float mis = (1.0f * lpdf) / (1.0f * lpdf + 1.0f * spdf);
         f3 pre = mul3(mul3s(f, mis), Le);
-        float tr;
-        if (S->nmedia == 0) {
-          tr = scene_occluded(S, offO, ldir, DEFAULT_TMAX) ? 0.0f : 1.0f;
-        } else {
-          const ray_t lr = ray_off(mkray(pos, ldir, DEFAULT_TMAX), n);
-          rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 0u);
-          tr = shadow_tr(S, offO, ldir, lr.tmax, med, &rt, &err);
-        }
+        const ray_t lr = ray_off(mkray(pos, ldir, DEFAULT_TMAX), n);
+        rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 0u);
+        const float tr = shadow_tr(S, offO, ldir, lr.tmax, med, &rt, &err);
         dl = add3(dl, div3s(mul3s(pre, tr), lpdf));
         anyShadow = 1;
       }
@@ -1377,21 +1417,17 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
         f3 Le = env_le(&S->env, wi, &lpdf);
         float mis = (1.0f * spdf) / (1.0f * spdf + 1.0f * lpdf);
         f3 pre = mul3(mul3s(f, mis), Le);
-        float tr;
-        if (S->nmedia == 0) {
-          tr = scene_occluded(S, offO, wi, DEFAULT_TMAX) ? 0.0f : 1.0f;
-        } else {
-          const ray_t br = ray_off(mkray(pos, wi, DEFAULT_TMAX), n);
-          rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 1u);
-          tr = shadow_tr(S, offO, wi, br.tmax, med, &rt, &err);
-        }
+        const ray_t br = ray_off(mkray(pos, wi, DEFAULT_TMAX), n);
+        rng_t rt = rng_make(p, S->seed, s, b, PURPOSE_SHADOW_TR + 1u);
+        const float tr = shadow_tr(S, offO, wi, br.tmax, med, &rt, &err);
         dl = add3(dl, div3s(mul3s(pre, tr), spdf));
         anyShadow = 1;
       }
     }
     if (anyShadow) L = add3(L, mul3(dl, T));
     /* continuation */
-    f3 dT = norm3(to_local(&fr, d));
+    /* CRay::transform through the mat4x3 widening: + 0 * (zero column) */
+    f3 dT = norm3(add3(to_local(&fr, d), F3(0.0f, 0.0f, 0.0f)));
     f3 wi = F3(0.0f, 0.0f, 0.0f);
     float pdf = 0.0f;
     f3 f = mat_sample_f(m, neg3(dT), oi_u01(rB[1]), oi_u01(rB[2]), oi_u01(rB[3]), &wi, &pdf);

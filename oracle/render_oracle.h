@@ -72,6 +72,12 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
                uint32_t seed, uint32_t p0, uint32_t p1, float* rgb_out, double* var_out, int threads,
                const orc_medium* media, uint32_t nmedia, uint32_t flags);
 
+/* Test hook: while words is not NULL, the Philox blocks of a surface path are
+ * taken from words in the order the path asks for them (render one pixel,
+ * one sample, one thread); vec2_swap exchanges the GGX lobe's two direction
+ * draws.  NULL restores the Philox streams. */
+void orc_set_replay(const uint32_t* words, size_t n, int vec2_swap);
+
 /* Natural logarithm of the tracking code (exposed for unit tests). */
 float orc_t_log(float x);
 

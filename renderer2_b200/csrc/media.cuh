@@ -249,6 +249,14 @@ R2_HD Ray ray_offset(const Ray& r, V3 dir) {
   return make_ray(o, r.d, length(end - o));
 }
 
+// CRay::spawnRay(p0, p1) (ray.hpp:62-69): the origin offset from p0 towards
+// p1, the direction (p1 - p0) / |p1 - offset origin| and that length.
+R2_HD Ray spawn_ray(V3 p0, V3 p1) {
+  const V3 off = offset_ray_origin(p0, normalize(p1 - p0));
+  const float tl = length(p1 - off);
+  return make_ray(off, (p1 - p0) / tl, tl);
+}
+
 // __intersection__volume: nanovdb::Ray::intersects against the world box
 // (t0 = 0, t1 = 1e12), reporting the exit when the origin is strictly inside
 // and the entry otherwise.  Returns -1 when there is no report.

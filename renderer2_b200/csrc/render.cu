@@ -819,13 +819,11 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
       const V3 f = be.f * fabsf(dot(n, ldir));
       const float spdf = be.pdf;
       const float mis = balance_heuristic(lpdf, spdf);
+      const Ray lr = ray_offset(make_ray(pos, ldir, kDefaultTmax), n);
       shO0 = f4(offO, lpdf);
-      shD0 = f4(ldir, 0.0f);
+      shD0 = f4(ldir, lr.tmax);  // intersectTr walks towards offO + ldir * tmax
       pre0 = f4((f * mis) * Le, 0.0f);
-      if (kMedia) {
-        const Ray lr = ray_offset(make_ray(pos, ldir, kDefaultTmax), n);
-        L.st.shX[2 * i] = make_float2(lr.tmax, __int_as_float(med));
-      }
+      if (kMedia) L.st.shX[2 * i] = make_float2(lr.tmax, __int_as_float(med));
     }
   }
   // --- direct(): BSDF sample (path_integrator_impl.hpp:74-113)
@@ -840,13 +838,11 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
       const V3 Le = ee.Le;
       const float lpdf = ee.pdf;
       const float mis = balance_heuristic(spdf, lpdf);
+      const Ray br = ray_offset(make_ray(pos, wi, kDefaultTmax), n);
       shO1 = f4(offO, spdf);
-      shD1 = f4(wi, 0.0f);
+      shD1 = f4(wi, br.tmax);
       pre1 = f4((f * mis) * Le, 0.0f);
-      if (kMedia) {
-        const Ray br = ray_offset(make_ray(pos, wi, kDefaultTmax), n);
-        L.st.shX[2 * i + 1] = make_float2(br.tmax, __int_as_float(med));
-      }
+      if (kMedia) L.st.shX[2 * i + 1] = make_float2(br.tmax, __int_as_float(med));
     }
   }
   L.st.shO[2 * i] = shO0;
@@ -857,7 +853,9 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   L.st.shPre[2 * i + 1] = pre1;
   L.st.shT[i] = f4(T, 0.0f);
   // --- continuation (path_integrator_impl.hpp:200-232)
-  const V3 dT = normalize(to_local(fr, d));
+  // CRay::transform(worldToTangent) widens the matrix to mat4x3 with a zero
+  // fourth column: the direction gains a + 0 term (-0 becomes +0).
+  const V3 dT = normalize(to_local(fr, d) + v3(0.0f));
   const BsdfSample cs = bsdf_sample_nc(m, -dT, u01(rB.y), u01(rB.z), u01(rB.w));
   const V3 wi = cs.wi, f = cs.f;
   const float pdf = cs.pdf;
@@ -1020,6 +1018,14 @@ __global__ void __launch_bounds__(128, kMedia ? 6 : 8) k_shade(RenderLaunch L) {
   }
 }
 
+// The first segment of CDeviceScene::intersectTr for a shadow record: the
+// record holds the normal-offset origin o and direction d with the offset
+// ray's length t1, and intersectTr traces CRay::spawnRay(o, o + d * t1).
+__device__ __forceinline__ Ray shadow_ray(float4 o, float4 d) {
+  const V3 p0 = xyz(o);
+  return spawn_ray(p0, p0 + xyz(d) * d.w);
+}
+
 // Visibility of every shadow record of a scene without media.
 __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
   const uint32_t n = event_count(L);
@@ -1030,7 +1036,8 @@ __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
       const float4 o = L.st.shO[j];
       float tr = 0.0f;
       if (o.w > 0.0f) {
-        tr = scene_occluded(L.scene, xyz(o), xyz(L.st.shD[j]), kDefaultTmax) ? 0.0f : 1.0f;
+        const Ray r = shadow_ray(o, L.st.shD[j]);
+        tr = scene_occluded(L.scene, r.o, r.d, r.tmax) ? 0.0f : 1.0f;
         ++traced;
       }
       L.st.shTr[j] = tr;
@@ -1044,7 +1051,8 @@ __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
         return false;
       }
       ++traced;
-      trace_begin(s, xyz(o), xyz(L.st.shD[j]), kDefaultTmax);
+      const Ray r = shadow_ray(o, L.st.shD[j]);
+      trace_begin(s, r.o, r.d, r.tmax);
       return true;
     };
     auto end = [&](uint32_t j, const TraceState& s) {
@@ -1054,7 +1062,7 @@ __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
         noTris.hasTris = 0;
         Hit none;
         none.tri = -1;
-        occluded = __float_as_int(scene_closest_after<false>(noTris, s.r.o, s.r.d, kDefaultTmax, none).w) != -1;
+        occluded = __float_as_int(scene_closest_after<false>(noTris, s.r.o, s.r.d, s.best.t, none).w) != -1;
       }
       L.st.shTr[j] = occluded ? 0.0f : 1.0f;
     };
@@ -1092,7 +1100,8 @@ __device__ __forceinline__ void shadow_walk(const RenderLaunch& L, uint32_t slot
   float tr;
   uint32_t idx;
   if (fresh) {
-    if (scene_occluded(S, o, d, x.x)) {
+    const Ray r0 = spawn_ray(o, o + d * x.x);
+    if (scene_occluded(S, r0.o, r0.d, r0.tmax)) {
       L.st.shTr[slot] = 0.0f;
       return;
     }

@@ -251,8 +251,12 @@ R2_HD V3 mat_sample_f(const Material& m, V3 wo, float uSel, float u1, float u2, 
 }
 
 // ---------------------------------------------------------------- objects.hpp (CCoordinateFrame)
+// tangentToWorld = mat3(T, B, N) (columns); worldToTangent is its inverse as
+// glm::inverse computes it (cofactors over the determinant), columns W0..W2,
+// which differs from the transpose in the last bits.
 struct Frame {
-  V3 T, B, N;  // tangentToWorld columns; worldToTangent is the transpose
+  V3 T, B, N;
+  V3 W0, W1, W2;
 };
 
 R2_HD Frame frame_from_normal(V3 N) {
@@ -261,9 +265,16 @@ R2_HD Frame frame_from_normal(V3 N) {
   f.T = fabsf(N.x) > fabsf(N.y) ? v3(-N.z, 0.0f, N.x) / sqrtf(N.x * N.x + N.z * N.z)
                                 : v3(0.0f, N.z, -N.y) / sqrtf(N.y * N.y + N.z * N.z);
   f.B = normalize(cross(N, f.T));
+  const V3 T = f.T, B = f.B;
+  const float det = T.x * (B.y * N.z - N.y * B.z) - B.x * (T.y * N.z - N.y * T.z) + N.x * (T.y * B.z - B.y * T.z);
+  const float inv = 1.0f / det;
+  f.W0 = v3(+(B.y * N.z - N.y * B.z) * inv, -(T.y * N.z - N.y * T.z) * inv, +(T.y * B.z - B.y * T.z) * inv);
+  f.W1 = v3(-(B.x * N.z - N.x * B.z) * inv, +(T.x * N.z - N.x * T.z) * inv, -(T.x * B.z - B.x * T.z) * inv);
+  f.W2 = v3(+(B.x * N.y - N.x * B.y) * inv, -(T.x * N.y - N.x * T.y) * inv, +(T.x * B.y - B.x * T.y) * inv);
   return f;
 }
-R2_HD V3 to_local(const Frame& f, V3 v) { return v3(dot(f.T, v), dot(f.B, v), dot(f.N, v)); }
+// worldToTangent * v, summed column by column as glm's matrix-vector product.
+R2_HD V3 to_local(const Frame& f, V3 v) { return f.W0 * v.x + f.W1 * v.y + f.W2 * v.z; }
 R2_HD V3 to_world(const Frame& f, V3 v) { return f.T * v.x + f.B * v.y + f.N * v.z; }
 
 // ---------------------------------------------------------------- ray.hpp / functions.hpp

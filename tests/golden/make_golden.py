@@ -59,6 +59,10 @@ def build(ref_include: str) -> C.CDLL:
     lib.ref_vec3_arg_order.restype = C.c_int
     lib.ref_filter_scene.restype = C.c_int
     lib.ref_filter_scene.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, P, f, f]
+    lib.ref_render_scene.restype = C.c_int
+    lib.ref_render_scene.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, C.c_int, C.c_int]
+    lib.ref_path_li.restype = C.c_int
+    lib.ref_path_li.argtypes = [C.c_uint32, C.c_uint32, f, P, P, P, C.c_uint32, C.c_uint32, P, C.c_int, P]
     lib.ref_mesh_filter_voxel.restype = C.c_int
     lib.ref_mesh_filter_voxel.argtypes = [P] * 8 + [f, C.c_uint32, f, C.c_int, C.c_uint32, P, C.c_int, P]
     return lib
@@ -153,6 +157,93 @@ def mesh_filter_case(lib, mesh, n, spv, iters, sigma_t, alpha, clip, seed, kd, k
     return {"mesh": mesh, "n": n, "spv": spv, "iters": iters, "sigma_t": sigma_t, "alpha": alpha, "clip": clip,
             "seed": seed, "kd": list(kd), "ks": list(ks), "ggx": ggx, "ior": ior, "num_voxels": [nx, ny, nz],
             "draws_not_reproduced": inexact, "payload_hex": payload.tobytes().hex()}
+
+
+# CPathIntegrator::Li case: two displaced icospheres (GGX 0.3 and 0.08) under a
+# lognormal environment; one path per pixel, the draws of path k being
+# path_draws(k) (Philox, key (k, PATH_KEY)); the reference has no depth limit
+# below its 50 bounces.
+PATH_CASES = [dict(room=False, width=24, height=20, fov=50.0, pos=(0.3, 0.6, 4.0), look_at=(0.4, 0.0, 0.0),
+                   up=(0.0, 1.0, 0.0), env=(32, 16, 1.0, 9), draws=2 + 50 * 9),
+              dict(room=True, width=24, height=20, fov=70.0, pos=(0.2, 0.4, 2.9), look_at=(0.4, 0.0, 0.0),
+                   up=(0.0, 1.0, 0.0), env=(32, 16, 1.0, 9), draws=2 + 50 * 9)]
+PATH_KEY = 77
+
+
+def open_box(half=(3.0, 2.0, 3.0), n=4):
+    """Floor, ceiling and three walls of a box (the +z side open), n x n quads each, normals facing in."""
+    from renderer2_b200.filter import Mesh
+    hx, hy, hz = half
+    faces = [((0, -hy, 0), (1, 0, 0), (0, 0, 1), (0, 1, 0), (hx, hz)), ((0, hy, 0), (1, 0, 0), (0, 0, -1), (0, -1, 0), (hx, hz)),
+             ((-hx, 0, 0), (0, 0, 1), (0, 1, 0), (1, 0, 0), (hz, hy)), ((hx, 0, 0), (0, 1, 0), (0, 0, 1), (-1, 0, 0), (hy, hz)),
+             ((0, 0, -hz), (0, 1, 0), (1, 0, 0), (0, 0, 1), (hy, hx))]
+    P, Nn, I = [], [], []
+    for c, a, b, nrm, (ea, eb) in faces:
+        c, a, b = np.asarray(c, float), np.asarray(a, float), np.asarray(b, float)
+        g = np.linspace(-1.0, 1.0, n + 1)
+        base = len(P)
+        for j in range(n + 1):
+            for i in range(n + 1):
+                P.append(c + a * ea * g[i] + b * eb * g[j])
+                Nn.append(nrm)
+        for j in range(n):
+            for i in range(n):
+                v = base + j * (n + 1) + i
+                I += [(v, v + 1, v + n + 2), (v, v + n + 2, v + n + 1)]
+    return Mesh(_f32(P), np.asarray(I, np.uint32), _f32(Nn))
+
+
+def path_scene(room=False):
+    """(meshes as (mesh, kd, ks, ggx alpha, ior, translation)) of a Li case; the test rebuilds it."""
+    sys.path.insert(0, ROOT)
+    from renderer2_b200 import scenes
+    spheres = [(scenes.icosphere(3, 0.05, 7), (0.7, 0.4, 0.2), (1.0, 1.0, 1.0), 0.3, 1.5, (0.0, 0.2, 0.0)),
+               (scenes.icosphere(2, 0.1, 3), (0.2, 0.8, 0.3), (0.9, 0.9, 0.9), 0.08, 1.33, (1.6, 0.0, -0.5))]
+    if not room:
+        return spheres
+    return spheres + [(open_box(), (0.85, 0.85, 0.8), (0.6, 0.6, 0.6), 0.5, 1.4, (0.0, 0.0, 0.0))]
+
+
+def path_draws(k, n):
+    """Uniforms k' / 2^24 of path k, as the oracle's 24-bit mapping produces them."""
+    from renderer2_b200 import scenes
+    i = np.arange(n, dtype=np.uint32)
+    w = scenes.philox4x32_10(i, 0, 0, 0, k, PATH_KEY)[0]
+    return ((w >> np.uint32(8)).astype(np.float64) * (1.0 / 16777216.0)).astype(np.float32)
+
+
+def path_li_case(lib, c):
+    sys.path.insert(0, ROOT)
+    from renderer2_b200 import render_scenes as RS
+    meshes = path_scene(c["room"])
+    wpos, nrm, idx, tobj, m2w, mats = [], [], [], [], [], []
+    base = 0
+    for o, (m, kd, ks, a, ior, t) in enumerate(meshes):
+        wpos.append(m.positions.astype(np.float32) + np.asarray(t, np.float32))
+        nrm.append(m.normals.astype(np.float32))
+        idx.append(m.indices.astype(np.uint32) + np.uint32(base))
+        tobj.append(np.full(m.indices.shape[0], o, np.uint32))
+        m2w.append(_f32([1, 0, 0, 0, 1, 0, 0, 0, 1, *t]))
+        mats.append(_f32([*kd, *ks, a, ior]))
+        base += m.positions.shape[0]
+    wpos, nrm, idx = _f32(np.concatenate(wpos)), _f32(np.concatenate(nrm)), np.concatenate(idx)
+    tobj, m2w, mats = np.concatenate(tobj), _f32(np.concatenate(m2w)), _f32(np.concatenate(mats))
+    env = _f32(RS.lognormal_env(*c["env"]))
+    assert lib.ref_render_scene(_p(wpos), wpos.shape[0], _p(idx), idx.shape[0], _p(nrm), _p(tobj), len(meshes),
+                                _p(m2w), _p(mats), _p(env), env.shape[1], env.shape[0]) >= 0
+    L = np.zeros((c["width"] * c["height"], 3), np.float32)
+    used = np.zeros(c["width"] * c["height"], np.int32)
+    inexact = 0
+    for k in range(c["width"] * c["height"]):
+        u = path_draws(k, c["draws"])
+        cv = curand_values_for(lib, u)
+        inexact += int(np.isnan(cv).sum())
+        cv = np.where(np.isnan(cv), np.float32(0.5), cv).astype(np.float32)
+        used[k] = lib.ref_path_li(c["width"], c["height"], c["fov"], _p(_f32(c["pos"])), _p(_f32(c["look_at"])),
+                                  _p(_f32(c["up"])), k % c["width"], k // c["width"], _p(cv), cv.size, _p(L[k]))
+    out = dict(c)
+    out.update(key=PATH_KEY, draws_not_reproduced=inexact, draws_used=used.tolist(), L=L.tolist())
+    return out
 
 
 def main():
@@ -321,6 +412,7 @@ def main():
 
     g["vec3_arg_order"] = lib.ref_vec3_arg_order()
     g["mesh_filter"] = [mesh_filter_case(lib, **k) for k in MESH_FILTER_CASES]
+    g["path_li"] = [path_li_case(lib, c) for c in PATH_CASES]
 
     with open(OUT, "w") as fh:
         json.dump(g, fh)
