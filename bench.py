@@ -48,7 +48,6 @@ SHADOW_BYTES_PER_RAY = 33.0
 FILTER_BYTES_PER_VOXEL = 36.0
 # kernels of one BVH build + shading gather: bounds 2, Morton 1, radix sort 8 passes x 5, triangle gather 1,
 # hierarchy 1, bottom-up 1, emission 1, shading gather 1
-BVH_BUILD_LAUNCHES = 48
 FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # no measured FP32 figure on this pool
 # media scenes:
 #   extend phase (k_resolve rounds, k_track, k_collide): queue id 4 + ray in/out 64 + throughput in/out 32 + hit record 16 = 116 B per segment
@@ -308,6 +307,7 @@ def gpu_filter_records(sc, g, prm, v0, v1):
 
 def bench_render(args, world, local):
     import torch
+    from renderer2_b200 import raytracer as R
     from renderer2_b200 import render_scenes as RS
     desc, cam, prm = render_workload()
     sc = RS.build_scene(desc)
@@ -392,6 +392,7 @@ def bench_render(args, world, local):
         e2e_step()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    bvh_nodes, bvh_height, bvh_launches = sc.bvh_info()
     e2e = {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(pos.nbytes + nrm.nbytes),
            "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms,
            "calls": "r2_scene_set_vertices (pinned) + r2_scene_rebuild + r2_render_host (pinned frame)"}
@@ -405,10 +406,12 @@ def bench_render(args, world, local):
     s2.close()
     e2e["cold_start"] = {"value": world * paths / (t2 - t0), "scene_build_ms": (t1 - t0) * 1e3,
                          "render_and_download_ms": (t2 - t1) * 1e3, "h2d_bytes": int(_input_bytes(desc))}
-    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth) + BVH_BUILD_LAUNCHES
+    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth) + bvh_launches
     return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths, tuning=tuning,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
-                bvh_build_ms=build_ms, render_ms=total_ms / args.steps - build_ms, desc=desc, cam=cam, prm=prm)
+                bvh_build_ms=build_ms, render_ms=total_ms / args.steps - build_ms, desc=desc, cam=cam, prm=prm,
+                bvh={"method": "PLOC" if R.bvh_method() == R.BVH_PLOC else "Karras", "inner_nodes": bvh_nodes,
+                     "height": bvh_height, "build_launches": bvh_launches})
 
 
 def bench_filter(args, world, local, grid=None, steps=None, warmup=None, e2e_run=True, mesh_mat=None):
@@ -594,6 +597,7 @@ def bench_small(args, world, local):
         e2e_step()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_ms = _max_over_ranks(float(np.median(e2e_ms)), world)
+    bvh_launches = sc.bvh_info()[2]
     # accuracy at this configuration: the whole grid against the FP64 oracle, the frame against the oracle's
     gw, gh = gpu_filter_records(fsc, g, fprm, 0, nvox)
     acc, cpu = None, None
@@ -634,7 +638,7 @@ def bench_small(args, world, local):
                                               + pos.nbytes + nrm.nbytes),
                     "d2h_bytes_per_step": int(nvox * 32 + npix * 12)},
             "accuracy": acc, "cpu_baseline": cpu,
-            "gpu_launches": (2 + BVH_BUILD_LAUNCHES + (c["spp"] // S) * (2 + 4 * c["depth"])) * args.steps}
+            "gpu_launches": (2 + bvh_launches + (c["spp"] // S) * (2 + 4 * c["depth"])) * args.steps}
 
 
 def bench_volume(args, world, local):
@@ -1149,7 +1153,7 @@ def run_native(args):
                 "workload_stats": {"segments_per_step": r["segments_per_frame"],
                                    "shadow_rays_per_step": r["shadow_rays_per_frame"],
                                    "bvh_build_ms_per_step": r["bvh_build_ms"], "render_ms_per_step": r["render_ms"],
-                                   "tuning": r["tuning"]},
+                                   "bvh": r["bvh"], "tuning": r["tuning"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
                 "clocks": r["clocks"]}
         if small is not None:

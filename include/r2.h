@@ -44,6 +44,18 @@ const char* r2_last_error(void);
 /* ABI version: major * 10000 + minor * 100 + patch. */
 int r2_version(void);
 
+/* Hierarchy of the BVHs built from now on (scenes, filter scenes, rebuilds),
+ * process-wide.  Both start from the Morton-sorted primitives and end with the
+ * same SAH leaf collapse.  R2_BVH_PLOC (default): parallel locally-ordered
+ * clustering (Meister & Bittner 2018), mutual nearest neighbours by
+ * surface area within 16 sorted positions.  R2_BVH_KARRAS: the radix tree of
+ * the Morton codes (Karras 2012).  Replaces the OptiX builder
+ * (optixAccelBuild, raytracer/src/mesh/mesh.cu:140-166 and
+ * raytracer/src/scene/scene.cu:188-256), which has no such choice. */
+enum { R2_BVH_PLOC = 0, R2_BVH_KARRAS = 1 };
+r2_status r2_set_bvh_method(int method);
+int r2_get_bvh_method(void);
+
 /* Voxel payload, 32 bytes, byte-identical to the reference's
  * filter::SFilteredDataCompact (raytracer/include/filtering/filtered_data.hpp:33-61),
  * which is stored in the NanoVDB Vec4d grid (openvdb_backend.cpp:27). */
@@ -289,6 +301,10 @@ typedef struct r2_render_tuning {
                            a path or shadow ray whose loop reaches it ends, and the synchronous
                            render calls return R2_ERR_DEVICE_TIMEOUT with the frame written.  The
                            reference's loops have no bound (nvdb_medium_impl.hpp:98-136, 155-186). */
+  uint32_t top_nodes;   /* surface scenes: BVH nodes 0 .. top_nodes-1 copied into each traversal block's
+                           shared memory and read from there (0: off; at most 256).  With the PLOC
+                           builder a parent's index is below its children's, so these are the top
+                           levels of the tree (of the top-level tree in two-level scenes). */
 } r2_render_tuning;
 
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA
@@ -311,6 +327,24 @@ r2_status r2_scene_destroy(r2_scene* scene);
 r2_status r2_scene_add_mesh(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
                             uint32_t ntris, const float* normals, const r2_material* material,
                             const float* model_to_world, uint32_t mask);
+/* Instanced meshes (two-level scenes).  r2_scene_add_mesh_asset keeps a mesh
+ * in model space with its own BVH (uvs and maps nullable, as
+ * r2_scene_add_mesh_textured) and returns its index; r2_scene_add_mesh_instance
+ * places it with a T*R*S transform (mask 0: not visible to render rays).
+ * Once a scene has an instance, the BVH becomes two-level: a top level over
+ * the instances' world boxes (the world-space meshes of r2_scene_add_mesh
+ * form one more instance) and one bottom level per asset, each shared by its
+ * instances.  Replaces CAssetManager::loadMesh's per-file mesh with its GAS
+ * and the scene objects' OptiX instances (raytracer/src/scene/scene.cu:188-256,
+ * raytracer/src/scene/sceneobject.cu:330-349): a hit's normal is the
+ * interpolated model-space normal taken to world space by the instance's
+ * transform (__closesthit__ch, shaders.optix.cu:28-130).  Assets do not
+ * change after commit; r2_scene_set_vertices and r2_scene_rebuild act on the
+ * world-space meshes and rebuild the top level. */
+r2_status r2_scene_add_mesh_asset(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
+                                  uint32_t ntris, const float* normals, const float* uvs, const r2_material* material,
+                                  const r2_material_maps* maps, uint32_t* asset_out);
+r2_status r2_scene_add_mesh_instance(r2_scene* scene, uint32_t asset, const float* model_to_world, uint32_t mask);
 r2_status r2_scene_add_shape(r2_scene* scene, int shape_type, const float* center, float radius,
                              const float* normal, const r2_material* material, uint32_t mask);
 /* Environment map: width*height RGB float texels, row 0 = top (+Y). */
@@ -346,6 +380,11 @@ r2_status r2_scene_commit(r2_scene* scene);
  * build has finished on the device.  Frames must not be rendering the scene
  * on another stream meanwhile. */
 r2_status r2_scene_rebuild(r2_scene* scene, void* stream);
+/* The surface BVH of a committed scene: inner nodes, height (levels of inner
+ * nodes on the longest path) and the kernels its last build or rebuild
+ * launched.  Any output may be NULL. */
+r2_status r2_scene_bvh_info(r2_scene* scene, uint32_t* nodes, uint32_t* height, uint32_t* build_launches);
+
 /* Replaces the committed scene's vertex positions (and, when normals is not
  * NULL, its vertex normals) with nverts world-space vertices from host memory
  * (pinned memory makes the copy asynchronous), in the order the meshes were

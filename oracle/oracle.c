@@ -180,6 +180,144 @@ static void put_box(int32_t* w, int slot, const float* l, const float* h) {
   }
 }
 
+/* ------------------------------------------------ PLOC (bvh_ploc.cu) */
+#define PLOC_RADIUS 16
+
+static int g_bvh_method = 0; /* 0 PLOC, 1 Karras */
+void orc_set_bvh_method(int method) { g_bvh_method = method == 1 ? 1 : 0; }
+int orc_get_bvh_method(void) { return g_bvh_method; }
+
+static float union_area(const float* al, const float* ah, const float* bl, const float* bh) {
+  float dx = fmaxf(ah[0], bh[0]) - fminf(al[0], bl[0]);
+  float dy = fmaxf(ah[1], bh[1]) - fminf(al[1], bl[1]);
+  float dz = fmaxf(ah[2], bh[2]) - fminf(al[2], bl[2]);
+  return dx * dy + dy * dz + dz * dx;
+}
+
+typedef struct {
+  int *left, *right, *parent, *leafParent, *count, *height, *collapse, *first, *leafPos;
+  float *lo, *hi, *cost; /* 4 floats per box */
+} ploc_t;
+
+/* A new inner node nd over clusters a and b (boxes al/ah, bl/bh): box, SAH
+ * cost, primitive count, height and the leaf-collapse decision, in the
+ * kernel's float operation order (make_node). */
+static void ploc_node(ploc_t* P, int nd, int a, const float* al, const float* ah, int b, const float* bl,
+                      const float* bh) {
+  float ca = a < 0 ? SAH_TRI : P->cost[a], cb = b < 0 ? SAH_TRI : P->cost[b];
+  int na = a < 0 ? 1 : P->count[a], nb = b < 0 ? 1 : P->count[b];
+  int ha = a < 0 ? 0 : P->height[a], hb = b < 0 ? 0 : P->height[b];
+  float* lo = &P->lo[4 * (size_t)nd];
+  float* hi = &P->hi[4 * (size_t)nd];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = fminf(al[k], bl[k]);
+    hi[k] = fmaxf(ah[k], bh[k]);
+  }
+  lo[3] = hi[3] = 0.0f;
+  float A = box_area(lo, hi), Al = box_area(al, ah), Ar = box_area(bl, bh);
+  float inner = (A > 0.0f) ? SAH_NODE + (Al * ca + Ar * cb) / A : SAH_NODE + ca + cb;
+  int count = na + nb;
+  float leafc = SAH_TRI * (float)count;
+  int col = (count <= LEAF_MAX && leafc <= inner) ? 1 : 0;
+  P->left[nd] = a;
+  P->right[nd] = b;
+  P->cost[nd] = col ? leafc : inner;
+  P->count[nd] = count;
+  P->height[nd] = col ? 0 : 1 + (ha > hb ? ha : hb);
+  P->collapse[nd] = col;
+  if (a < 0) P->leafParent[~a] = nd; else P->parent[a] = nd;
+  if (b < 0) P->leafParent[~b] = nd; else P->parent[b] = nd;
+}
+
+/* Clustering of the n >= 2 sorted leaves (boxes leafLo/leafHi): each
+ * iteration every cluster finds its nearest neighbour within PLOC_RADIUS
+ * positions (smallest enclosing area; then closest position, even lower
+ * position, lower position — the GPU's 64-bit pair key), mutual pairs
+ * merge into a node at the smaller position (numbered downwards from n-2 in
+ * position order), the list is compacted.  Then depth-first positions of the
+ * leaves and the first position of every node. */
+static void ploc_build(ploc_t* P, int n, const float* leafLo, const float* leafHi) {
+  int* ref = (int*)malloc(sizeof(int) * (size_t)n);
+  int* ref2 = (int*)malloc(sizeof(int) * (size_t)n);
+  float* lo = (float*)malloc(sizeof(float) * 4 * (size_t)n);
+  float* hi = (float*)malloc(sizeof(float) * 4 * (size_t)n);
+  float* lo2 = (float*)malloc(sizeof(float) * 4 * (size_t)n);
+  float* hi2 = (float*)malloc(sizeof(float) * 4 * (size_t)n);
+  int* nn = (int*)malloc(sizeof(int) * (size_t)n);
+  for (int i = 0; i < n; ++i) ref[i] = ~i;
+  memcpy(lo, leafLo, sizeof(float) * 4 * (size_t)n);
+  memcpy(hi, leafHi, sizeof(float) * 4 * (size_t)n);
+  for (int i = 0; i < n - 1; ++i) P->parent[i] = -1;
+  int m = n, cursor = n - 1;
+  while (m > 1) {
+    for (int i = 0; i < m; ++i) {
+      int j0 = i - PLOC_RADIUS < 0 ? 0 : i - PLOC_RADIUS, j1 = i + PLOC_RADIUS > m - 1 ? m - 1 : i + PLOC_RADIUS;
+      uint64_t best = UINT64_MAX;
+      for (int j = j0; j <= j1; ++j) {
+        if (j == i) continue;
+        float a = union_area(&lo[4 * (size_t)i], &hi[4 * (size_t)i], &lo[4 * (size_t)j], &hi[4 * (size_t)j]);
+        uint32_t ab;
+        memcpy(&ab, &a, 4);
+        uint32_t d = (uint32_t)(i > j ? i - j : j - i), lo2 = (uint32_t)(i < j ? i : j);
+        uint64_t key = ((uint64_t)ab << 32) | ((uint64_t)d << 27) | ((uint64_t)(lo2 & 1u) << 26) | lo2;
+        if (key < best) best = key;
+      }
+      int blo = (int)(best & 0x03FFFFFFu), bd = (int)((best >> 27) & 31u);
+      nn[i] = blo < i ? blo : i + bd;
+    }
+    int k = 0;
+    for (int i = 0; i < m; ++i)
+      if (nn[nn[i]] == i && i < nn[i]) ++k;
+    int base = cursor - k, rank = 0, pos = 0;
+    for (int i = 0; i < m; ++i) {
+      int j = nn[i];
+      int mutual = nn[j] == i;
+      if (mutual && j < i) continue;
+      if (mutual) {
+        int nd = base + rank++;
+        ploc_node(P, nd, ref[i], &lo[4 * (size_t)i], &hi[4 * (size_t)i], ref[j], &lo[4 * (size_t)j],
+                  &hi[4 * (size_t)j]);
+        ref2[pos] = nd;
+        memcpy(&lo2[4 * (size_t)pos], &P->lo[4 * (size_t)nd], 16);
+        memcpy(&hi2[4 * (size_t)pos], &P->hi[4 * (size_t)nd], 16);
+      } else {
+        ref2[pos] = ref[i];
+        memcpy(&lo2[4 * (size_t)pos], &lo[4 * (size_t)i], 16);
+        memcpy(&hi2[4 * (size_t)pos], &hi[4 * (size_t)i], 16);
+      }
+      ++pos;
+    }
+    cursor = base;
+    m = pos;
+    int* tr = ref; ref = ref2; ref2 = tr;
+    float* tl = lo; lo = lo2; lo2 = tl;
+    float* th = hi; hi = hi2; hi2 = th;
+  }
+  for (int i = 0; i < n; ++i) {
+    int cur = ~i, p = P->leafParent[i], pos = 0;
+    while (p >= 0) {
+      if (P->right[p] == cur) pos += P->left[p] < 0 ? 1 : P->count[P->left[p]];
+      cur = p;
+      p = P->parent[p];
+    }
+    P->leafPos[i] = pos;
+    cur = ~i;
+    p = P->leafParent[i];
+    while (p >= 0 && P->left[p] == cur) {
+      P->first[p] = pos;
+      cur = p;
+      p = P->parent[p];
+    }
+  }
+  free(ref); free(ref2); free(lo); free(hi); free(lo2); free(hi2); free(nn);
+}
+
+static int ploc_child_ref(const ploc_t* P, int c) {
+  if (c < 0) return ~(P->leafPos[~c] | (1 << 26));
+  if (P->collapse[c]) return ~(P->first[c] | (P->count[c] << 26));
+  return c;
+}
+
 int orc_build_bvh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, int32_t* nodes_out,
                   uint32_t* order_out, float* tris_out) {
   (void)nverts;
@@ -222,6 +360,55 @@ int orc_build_bvh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32
     keys[i] = kv[i].key;
     order_out[i] = kv[i].idx;
   }
+  int plocHeight = -1;
+  if (n > 1 && g_bvh_method == 0) {
+    int ni = n - 1;
+    ploc_t P;
+    P.left = (int*)malloc(sizeof(int) * ni); P.right = (int*)malloc(sizeof(int) * ni);
+    P.parent = (int*)malloc(sizeof(int) * ni); P.leafParent = (int*)malloc(sizeof(int) * (size_t)n);
+    P.count = (int*)malloc(sizeof(int) * ni); P.height = (int*)malloc(sizeof(int) * ni);
+    P.collapse = (int*)malloc(sizeof(int) * ni); P.first = (int*)malloc(sizeof(int) * ni);
+    P.leafPos = (int*)malloc(sizeof(int) * (size_t)n);
+    P.lo = (float*)malloc(sizeof(float) * 4 * ni); P.hi = (float*)malloc(sizeof(float) * 4 * ni);
+    P.cost = (float*)malloc(sizeof(float) * ni);
+    float* sLo = (float*)malloc(sizeof(float) * 4 * (size_t)n);
+    float* sHi = (float*)malloc(sizeof(float) * 4 * (size_t)n);
+    uint32_t* sorted = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)n);
+    for (int i = 0; i < n; ++i) {
+      sorted[i] = order_out[i];
+      memcpy(&sLo[4 * (size_t)i], &tlo[4 * (size_t)sorted[i]], 16);
+      memcpy(&sHi[4 * (size_t)i], &thi[4 * (size_t)sorted[i]], 16);
+    }
+    ploc_build(&P, n, sLo, sHi);
+    for (int i = 0; i < n; ++i) order_out[P.leafPos[i]] = sorted[i];
+    for (int i = 0; i < ni; ++i) {
+      int32_t* w = &nodes_out[16 * (size_t)i];
+      memset(w, 0, 64);
+      if (i == 0 && P.collapse[0]) {
+        float el[3] = {INFINITY, INFINITY, INFINITY}, eh[3] = {-INFINITY, -INFINITY, -INFINITY};
+        put_box(w, 0, &P.lo[0], &P.hi[0]);
+        put_box(w, 1, el, eh);
+        w[12] = leaf_ref(0, n);
+        w[13] = BVH_NONE;
+        w[14] = -1;
+        w[15] = 0;
+        continue;
+      }
+      int lc = P.left[i], rc = P.right[i];
+      put_box(w, 0, lc < 0 ? &sLo[4 * (size_t)(~lc)] : &P.lo[4 * (size_t)lc],
+              lc < 0 ? &sHi[4 * (size_t)(~lc)] : &P.hi[4 * (size_t)lc]);
+      put_box(w, 1, rc < 0 ? &sLo[4 * (size_t)(~rc)] : &P.lo[4 * (size_t)rc],
+              rc < 0 ? &sHi[4 * (size_t)(~rc)] : &P.hi[4 * (size_t)rc]);
+      w[12] = ploc_child_ref(&P, lc);
+      w[13] = ploc_child_ref(&P, rc);
+      w[14] = P.parent[i];
+      w[15] = P.height[i];
+    }
+    plocHeight = P.collapse[0] ? 1 : P.height[0];
+    free(P.left); free(P.right); free(P.parent); free(P.leafParent); free(P.count); free(P.height);
+    free(P.collapse); free(P.first); free(P.leafPos); free(P.lo); free(P.hi); free(P.cost);
+    free(sLo); free(sHi); free(sorted);
+  }
   if (tris_out) {
     for (int i = 0; i < n; ++i) {
       uint32_t p = order_out[i];
@@ -237,7 +424,9 @@ int orc_build_bvh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32
     }
   }
   int height = 0;
-  if (n == 1) {
+  if (plocHeight >= 0) {
+    height = plocHeight;
+  } else if (n == 1) {
     int32_t* w = nodes_out;
     memset(w, 0, 64);
     float el[3] = {INFINITY, INFINITY, INFINITY}, eh[3] = {-INFINITY, -INFINITY, -INFINITY};

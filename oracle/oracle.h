@@ -37,11 +37,16 @@ extern "C" {
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void orc_sincos_turns(float u, float* s, float* c);
 
-/* LBVH identical to the GPU builder.  nodes_out: (ntris > 1 ? ntris-1 : 1) * 16
+/* BVH identical to the GPU builder (method: orc_set_bvh_method).  nodes_out: (ntris > 1 ? ntris-1 : 1) * 16
  * int32 words (BvhNode layout), order_out: ntris.  Returns the tree height or
  * -1 on error. */
 int orc_build_bvh(const float* world_pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris,
                   int32_t* nodes_out, uint32_t* order_out, float* tris_out /* 12*ntris or NULL */);
+
+/* Hierarchy of the BVHs built from now on: 0 PLOC clustering (default), 1
+ * the Karras radix tree; the GPU builder's two methods. */
+void orc_set_bvh_method(int method);
+int orc_get_bvh_method(void);
 
 /* Closest hit: returns BVH-order triangle or -1; t/b1/b2 out. */
 int orc_trace(const int32_t* nodes, const float* tris, float ox, float oy, float oz, float dx, float dy,

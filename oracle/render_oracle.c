@@ -1060,6 +1060,27 @@ static void med_free(med_t* m) {
 }
 
 /* ------------------------------------------------------------ scene */
+/* Two-level scenes: a mesh asset in model space with its own BVH and
+ * per-BVH-order shading data, and its instances (the GPU's BvhInstance). */
+typedef struct {
+  int32_t* nodes;
+  uint32_t* order;
+  float* tris;
+  uint32_t ntris;
+  const float* nrm;     /* per vertex, model space */
+  const uint32_t* idx;  /* local vertex indices */
+  int mat;              /* index into the scene's materials */
+  float* triUV;         /* per BVH-order triangle, 6 each; null without coordinates */
+  int* triAlpha;
+  oi_alpha alpha;       /* alpha.alpha_tex null: no alpha test */
+} asset_t;
+typedef struct {
+  int asset;
+  float m2w[12];  /* object -> world, glm mat4x3 column order */
+  float w2o[12];  /* world -> object, three rows of (3x3 | translation) */
+  uint32_t code;  /* hit code of the asset's BVH-order triangle 0 */
+} oinst_t;
+
 typedef struct {
   int32_t* nodes;
   float* tris;
@@ -1075,6 +1096,9 @@ typedef struct {
   int* triAlpha;    /* per BVH-order triangle */
   float* triUV;     /* per BVH-order triangle, 6 each */
   uint32_t ntris;
+  asset_t* assets;  /* two-level: codes from ntris on belong to instances */
+  oinst_t* insts;
+  uint32_t ninst;
   const orc_shape* shapes;
   mat_t* shapeMats;
   uint32_t nshapes;
@@ -1089,14 +1113,68 @@ typedef struct {
   uint32_t spp, maxDepth, seed;
 } rscene_t;
 
+/* The object-space ray of instance I (the GPU's inst_point / inst_vector). */
+static void inst_ray(const oinst_t* I, f3 o, f3 d, f3* oo, f3* od) {
+  const float* w = I->w2o;
+  *oo = F3(w[0] * o.x + w[1] * o.y + w[2] * o.z + w[3], w[4] * o.x + w[5] * o.y + w[6] * o.z + w[7],
+           w[8] * o.x + w[9] * o.y + w[10] * o.z + w[11]);
+  *od = F3(w[0] * d.x + w[1] * d.y + w[2] * d.z, w[4] * d.x + w[5] * d.y + w[6] * d.z,
+           w[8] * d.x + w[9] * d.y + w[10] * d.z);
+}
+
+/* Closest triangle over the world-space meshes and every instance: the hit
+ * code (world: BVH-order triangle; instance: its code + the asset's
+ * BVH-order triangle), -1 on a miss; ties in t go to the lower code. */
+static int tris_closest(const rscene_t* S, f3 o, f3 d, float tmax, hit_t* out) {
+  hit_t best;
+  best.t = tmax;
+  best.b1 = best.b2 = 0.0f;
+  best.tri = -1;
+  if (S->ntris > 0) {
+    hit_t h = oi_trace_alpha(S->nodes, S->tris, o, d, tmax, 0, S->alpha.alpha_tex ? &S->alpha : NULL);
+    if (h.tri >= 0) best = h;
+  }
+  for (uint32_t i = 0; i < S->ninst; ++i) {
+    const oinst_t* I = &S->insts[i];
+    const asset_t* A = &S->assets[I->asset];
+    f3 oo, od;
+    inst_ray(I, o, d, &oo, &od);
+    hit_t h = oi_trace_alpha(A->nodes, A->tris, oo, od, best.t, 0, A->alpha.alpha_tex ? &A->alpha : NULL);
+    if (h.tri < 0) continue;
+    const int code = (int)(I->code + (uint32_t)h.tri);
+    if (best.tri < 0 || h.t < best.t || (h.t == best.t && code < best.tri)) {
+      best = h;
+      best.tri = code;
+    }
+  }
+  *out = best;
+  return best.tri;
+}
+
+static int tris_occluded(const rscene_t* S, f3 o, f3 d, float tmax) {
+  if (S->ntris > 0) {
+    hit_t h = oi_trace_alpha(S->nodes, S->tris, o, d, tmax, 1, S->alpha.alpha_tex ? &S->alpha : NULL);
+    if (h.tri >= 0) return 1;
+  }
+  for (uint32_t i = 0; i < S->ninst; ++i) {
+    const oinst_t* I = &S->insts[i];
+    const asset_t* A = &S->assets[I->asset];
+    f3 oo, od;
+    inst_ray(I, o, d, &oo, &od);
+    hit_t h = oi_trace_alpha(A->nodes, A->tris, oo, od, tmax, 1, A->alpha.alpha_tex ? &A->alpha : NULL);
+    if (h.tri >= 0) return 1;
+  }
+  return 0;
+}
+
 /* closest: code >= 0 BVH-order triangle, -1 miss, -2 - i shape i */
 static int scene_closest(const rscene_t* S, f3 o, f3 d, float tmax, float* tOut, float* b1, float* b2) {
   float t = tmax;
   int code = -1;
   *b1 = *b2 = 0.0f;
-  if (S->ntris > 0) {
-    hit_t h = oi_trace_alpha(S->nodes, S->tris, o, d, tmax, 0, S->alpha.alpha_tex ? &S->alpha : NULL);
-    if (h.tri >= 0) { t = h.t; *b1 = h.b1; *b2 = h.b2; code = h.tri; }
+  if (S->ntris > 0 || S->ninst > 0) {
+    hit_t h;
+    if (tris_closest(S, o, d, tmax, &h) >= 0) { t = h.t; *b1 = h.b1; *b2 = h.b2; code = h.tri; }
   }
   for (uint32_t i = 0; i < S->nshapes; ++i) {
     const orc_shape* sh = &S->shapes[i];
@@ -1150,13 +1228,11 @@ static int scene_closest_media(const rscene_t* S, f3 o, f3 d, float tmax, float*
 }
 
 static int scene_occluded(const rscene_t* S, f3 o, f3 d, float tmax) {
-  if (S->ntris > 0) {
-    hit_t h = oi_trace_alpha(S->nodes, S->tris, o, d, tmax, 1, S->alpha.alpha_tex ? &S->alpha : NULL);
-    if (h.tri >= 0) return 1;
-  }
+  if (tris_occluded(S, o, d, tmax)) return 1;
   if (S->nshapes > 0) {
     rscene_t T = *S;
     T.ntris = 0;
+    T.ninst = 0;
     float t, b1, b2;
     if (scene_closest(&T, o, d, tmax, &t, &b1, &b2) != -1) return 1;
   }
@@ -1357,7 +1433,7 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
     f3 n;
     const mat_t* m;
     mat_t mt;
-    if (code >= 0) {
+    if (code >= 0 && (uint32_t)code < S->ntris) {
       uint32_t prim = S->order[code];
       const uint32_t* tv = &S->idx[3 * (size_t)prim];
       f3 n0 = F3(S->wnrm[3 * tv[0]], S->wnrm[3 * tv[0] + 1], S->wnrm[3 * tv[0] + 2]);
@@ -1372,6 +1448,26 @@ static f3 trace_path(const rscene_t* S, uint32_t p, uint32_t s) {
                             &S->tris[12 * (size_t)code], hb1, hb2, &n, &mt.diffuse, &mt.specular);
         m = &mt;
       }
+    } else if (code >= 0) {  /* an instance: model-space normal, then the instance's transform */
+      uint32_t k = 0;
+      while (k + 1 < S->ninst && S->insts[k + 1].code <= (uint32_t)code) ++k;
+      const oinst_t* I = &S->insts[k];
+      const asset_t* A = &S->assets[I->asset];
+      const uint32_t tri = (uint32_t)code - I->code, prim = A->order[tri];
+      const uint32_t* tv = &A->idx[3 * (size_t)prim];
+      f3 n0 = F3(A->nrm[3 * tv[0]], A->nrm[3 * tv[0] + 1], A->nrm[3 * tv[0] + 2]);
+      f3 n1 = F3(A->nrm[3 * tv[1]], A->nrm[3 * tv[1] + 1], A->nrm[3 * tv[1] + 2]);
+      f3 n2 = F3(A->nrm[3 * tv[2]], A->nrm[3 * tv[2] + 1], A->nrm[3 * tv[2] + 2]);
+      float b0 = (1.0f - hb1) - hb2;
+      n = norm3(add3(add3(mul3s(n0, b0), mul3s(n1, hb1)), mul3s(n2, hb2)));
+      m = &S->mats[A->mat];
+      if (A->triUV && (m->tex[0] >= 0 || m->tex[1] >= 0 || m->tex[2] >= 0)) {
+        mt = *m;
+        oi_textured_surface(S->tex, mt.tex[0], mt.tex[1], mt.tex[2], &A->triUV[6 * (size_t)tri],
+                            &A->tris[12 * (size_t)tri], hb1, hb2, &n, &mt.diffuse, &mt.specular);
+        m = &mt;
+      }
+      n = norm3(xvec(I->m2w, n));
     } else {
       const orc_shape* sh = &S->shapes[-2 - code];
       n = sh->type == 1 ? norm3(F3(sh->normal[0], sh->normal[1], sh->normal[2]))
@@ -1540,7 +1636,8 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   rscene_t S;
   memset(&S, 0, sizeof(S));
   uint32_t nv = 0, nt = 0;
-  for (uint32_t i = 0; i < nmeshes; ++i) { nv += meshes[i].nverts; nt += meshes[i].ntris; }
+  for (uint32_t i = 0; i < nmeshes; ++i)
+    if (meshes[i].asset == 0) { nv += meshes[i].nverts; nt += meshes[i].ntris; }
   float* wpos = (float*)malloc(sizeof(float) * 3 * (size_t)(nv + 1));
   S.wnrm = (float*)malloc(sizeof(float) * 3 * (size_t)(nv + 1));
   S.idx = (uint32_t*)malloc(sizeof(uint32_t) * 3 * (size_t)(nt + 1));
@@ -1548,16 +1645,33 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   S.mats = (mat_t*)malloc(sizeof(mat_t) * (size_t)(nmeshes + 1));
   uint32_t vb = 0, tb = 0;
   int anyUV = 0;
-  for (uint32_t i = 0; i < nmeshes; ++i) anyUV = anyUV || meshes[i].uvs != NULL;
+  for (uint32_t i = 0; i < nmeshes; ++i) anyUV = anyUV || (meshes[i].asset == 0 && meshes[i].uvs != NULL);
   if (anyUV) S.uv = (float*)calloc(2 * (size_t)(nv + 1), sizeof(float));
   S.tex = (oi_tex*)calloc(5 * (size_t)(nmeshes + 1), sizeof(oi_tex));
+  /* asset k's first mesh (its geometry and material) */
+  int* firstOf = (int*)malloc(sizeof(int) * (size_t)(nmeshes + 1));
+  int* assetOf = (int*)malloc(sizeof(int) * (size_t)(nmeshes + 1));
+  uint32_t nassets = 0, ninst = 0;
+  for (uint32_t i = 0; i < nmeshes; ++i) {
+    assetOf[i] = -1;
+    if (meshes[i].asset == 0) continue;
+    ++ninst;
+    for (uint32_t a = 0; a < nassets; ++a)
+      if (meshes[firstOf[a]].asset == meshes[i].asset) assetOf[i] = (int)a;
+    if (assetOf[i] < 0) {
+      firstOf[nassets] = (int)i;
+      assetOf[i] = (int)nassets++;
+    }
+  }
   for (uint32_t i = 0; i < nmeshes; ++i) {
     const orc_mesh* M = &meshes[i];
     S.mats[i] = make_mat(&M->material);
-    if (M->uvs) memcpy(&S.uv[2 * (size_t)vb], M->uvs, sizeof(float) * 2 * (size_t)M->nverts);
+    const int owner = M->asset == 0 || firstOf[assetOf[i]] == (int)i;
     /* CMaterial(aiMaterial*) (material.cu:110-143); maps without texture coordinates are unused */
-    if (M->uvs)
+    if (M->uvs && owner)
       oi_material_maps(&M->material, M->albedo, M->specular, M->normal, M->alpha, S.tex, &S.ntex, S.mats[i].tex);
+    if (M->asset != 0) continue;
+    if (M->uvs) memcpy(&S.uv[2 * (size_t)vb], M->uvs, sizeof(float) * 2 * (size_t)M->nverts);
     for (uint32_t v = 0; v < M->nverts; ++v) {
       f3 pp = xpoint(M->model_to_world, F3(M->positions[3 * v], M->positions[3 * v + 1], M->positions[3 * v + 2]));
       f3 nn = xvec(M->model_to_world, F3(M->normals[3 * v], M->normals[3 * v + 1], M->normals[3 * v + 2]));
@@ -1599,6 +1713,59 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
       }
     }
   }
+  /* two-level: the assets' model-space BVHs and the instances, numbered after the world triangles */
+  S.assets = (asset_t*)calloc((size_t)nassets + 1, sizeof(asset_t));
+  S.insts = (oinst_t*)calloc((size_t)ninst + 1, sizeof(oinst_t));
+  for (uint32_t a = 0; a < nassets; ++a) {
+    const orc_mesh* M = &meshes[firstOf[a]];
+    asset_t* A = &S.assets[a];
+    A->ntris = M->ntris;
+    A->nrm = M->normals;
+    A->idx = M->indices;
+    A->mat = firstOf[a];
+    A->nodes = (int32_t*)malloc(64 * (size_t)(M->ntris > 1 ? M->ntris - 1 : 1));
+    A->order = (uint32_t*)malloc(4 * (size_t)M->ntris);
+    A->tris = (float*)malloc(48 * (size_t)M->ntris);
+    int h = orc_build_bvh(M->positions, M->nverts, M->indices, M->ntris, A->nodes, A->order, A->tris);
+    if (h < 0 || h > 96) return -2;
+    if (M->uvs) {
+      A->triUV = (float*)malloc(sizeof(float) * 6 * (size_t)M->ntris);
+      A->triAlpha = (int*)malloc(sizeof(int) * (size_t)M->ntris);
+      for (uint32_t i = 0; i < M->ntris; ++i) {
+        const uint32_t prim = A->order[i];
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t v = M->indices[3 * (size_t)prim + k];
+          A->triUV[6 * (size_t)i + 2 * k] = M->uvs[2 * (size_t)v];
+          A->triUV[6 * (size_t)i + 2 * k + 1] = M->uvs[2 * (size_t)v + 1];
+        }
+        A->triAlpha[i] = S.mats[A->mat].tex[3];
+      }
+      if (S.mats[A->mat].tex[3] >= 0) {
+        A->alpha.alpha_tex = A->triAlpha;
+        A->alpha.uv = A->triUV;
+        A->alpha.tex = S.tex;
+      }
+    }
+  }
+  {
+    uint32_t code = nt, k = 0;
+    for (uint32_t i = 0; i < nmeshes; ++i) {
+      if (meshes[i].asset == 0) continue;
+      oinst_t* I = &S.insts[k++];
+      I->asset = assetOf[i];
+      memcpy(I->m2w, meshes[i].model_to_world, sizeof(I->m2w));
+      m4_t M4 = oi_m4_id();
+      for (int c = 0; c < 4; ++c)
+        for (int r = 0; r < 3; ++r) M4.m[c][r] = I->m2w[3 * c + r];
+      float w43[12];
+      oi_m4_to43(oi_m4_inv(M4), w43);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) I->w2o[4 * r + c] = w43[3 * c + r];
+      I->code = code;
+      code += S.assets[I->asset].ntris;
+    }
+    S.ninst = ninst;
+  }
   S.shapes = shapes;
   S.nshapes = nshapes;
   S.shapeMats = (mat_t*)malloc(sizeof(mat_t) * (size_t)(nshapes + 1));
@@ -1628,6 +1795,11 @@ int orc_render(const orc_mesh* meshes, uint32_t nmeshes, const orc_shape* shapes
   for (int k = 0; k < S.ntex; ++k) free(S.tex[k].texels);
   free(S.tex);
   if (nt > 0) { free(S.nodes); free(S.order); free(S.tris); }
+  for (uint32_t a = 0; a < nassets; ++a) {
+    free(S.assets[a].nodes); free(S.assets[a].order); free(S.assets[a].tris);
+    free(S.assets[a].triUV); free(S.assets[a].triAlpha);
+  }
+  free(S.assets); free(S.insts); free(firstOf); free(assetOf);
   for (uint32_t i = 0; i < nmedia; ++i) med_free(&meds[i]);
   free(meds);
   return 0;

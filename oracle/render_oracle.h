@@ -36,6 +36,10 @@ typedef struct orc_mesh {
   const orc_texture* specular;
   const orc_texture* normal;
   const orc_texture* alpha;
+  /* 0: a world-space mesh (flattened into the one-level BVH); k > 0: an
+   * instance of mesh asset k, whose geometry, normals, texture coordinates and
+   * material are those of the first mesh with this k (two-level scene). */
+  uint32_t asset;
 } orc_mesh;
 
 typedef struct orc_shape {

@@ -78,6 +78,11 @@ def _load():
         "r2_status_string": (C.c_char_p, [C.c_int]),
         "r2_last_error": (C.c_char_p, []),
         "r2_version": (C.c_int, []),
+        "r2_set_bvh_method": (C.c_int, [C.c_int]),
+        "r2_get_bvh_method": (C.c_int, []),
+        "r2_scene_bvh_info": (C.c_int, [P, P, P, P]),
+        "r2_scene_add_mesh_asset": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, P, P, P, P, P]),
+        "r2_scene_add_mesh_instance": (C.c_int, [P, C.c_uint32, P, C.c_uint32]),
         "r2_filter_setup_grid": (C.c_int, [P, P, P, f32, P]),
         "r2_filter_mesh": (C.c_int, [P, u32, P, u32, P, P, P, P, f32, P, P, P, sz]),
         "r2_filter_scene_create": (C.c_int, [P, u32, P, u32, P, P, P, P]),

@@ -38,11 +38,29 @@ struct BvhAlpha {
   const TexInfo* texInfo;
 };
 
+// A placed bottom-level BVH of a two-level scene (the reference's OptiX
+// instance, sceneobject.cu:330-349).  The top-level BVH's leaves reference
+// instances (leaf references with count 0); entering one transforms the ray
+// into the instance's object space and continues at its root.  A triangle hit
+// inside the instance reports the code tri + vdelta, where tri is the
+// triangle's position in the global BVH-order array: codes number the
+// triangles of every instance consecutively, instance by instance.
+struct __align__(16) BvhInstance {
+  float4 w2o[3];  // world -> object: rows (3x3 part | translation)
+  int root;       // the instance's BLAS root in the global node array
+  int vdelta;     // hit code - global triangle index
+  int identity;   // 1: object space is world space (no transform)
+  int pad;
+};
+
 struct BvhView {
   const BvhNode* nodes;
   const float4* tris;  // 3 per triangle, BVH order
   uint32_t ntris;
   BvhAlpha alpha;      // zero: every triangle opaque
+  const BvhInstance* inst;  // two-level scenes: the instances (nodes start with the top level), else null
+  const BvhNode* top;       // nodes 0 .. ntop-1 staged in shared memory by the caller (kTop traversals)
+  int ntop;
 };
 
 R2_HD bool alpha_opaque(const BvhAlpha& a, int tri, float b1, float b2) {
@@ -104,11 +122,13 @@ R2_HD bool slab(const RayPre& r, float lox, float hix, float loy, float hiy, flo
   return tn <= tf;
 }
 
-// Watertight test.  Accepts 0 < t and (t, tri) lexicographically below the
-// current best (t, tri) so the closest hit is independent of visiting order;
-// kAlpha: and only where the triangle is opaque.
+// Watertight test.  Accepts 0 < t and (t, code) lexicographically below the
+// current best (t, code) so the closest hit is independent of visiting order;
+// kAlpha: and only where the triangle is opaque.  tri is the triangle's
+// BVH-order index, code the hit code reported (tri itself in one-level BVHs).
 template <bool kAlpha = false>
-R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, Hit* best, const BvhAlpha* alpha = nullptr) {
+R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, int code, Hit* best,
+                    const BvhAlpha* alpha = nullptr) {
   V3 A = p0 - r.o, B = p1 - r.o, C = p2 - r.o;
   float Az0 = comp(A, r.kz), Bz0 = comp(B, r.kz), Cz0 = comp(C, r.kz);
   float Ax = comp(A, r.kx) - r.Sx * Az0, Ay = comp(A, r.ky) - r.Sy * Az0;
@@ -133,13 +153,13 @@ R2_HD bool tri_test(const RayPre& r, V3 p0, V3 p1, V3 p2, int tri, Hit* best, co
   float rcp = 1.0f / det;
   float t = T * rcp;
   if (!(t > 0.0f)) return false;
-  if (t < best->t || (t == best->t && tri < best->tri)) {
+  if (t < best->t || (t == best->t && code < best->tri)) {
     const float b1 = V * rcp, b2 = W * rcp;
     if (kAlpha && !alpha_opaque(*alpha, tri, b1, b2)) return false;
     best->t = t;
     best->b1 = b1;
     best->b2 = b2;
-    best->tri = tri;
+    best->tri = code;
     return true;
   }
   return false;
@@ -164,14 +184,20 @@ struct TraceState {
   int sp;
   int found;
   uint32_t nodes, tris;  // visits counted by the counting instantiation (kCount)
+  V3 wo, wd;             // two-level: the world-space ray, restored when an instance is left
+  int vdelta;            // two-level: hit code offset of the instance being traversed (0: top level)
 };
 
 constexpr int kTraceDone = 0x7FFFFFFF;  // no node left to visit (never a node index)
+constexpr int kInstExit = 0x7FFFFFFE;   // stack marker: leave the current instance (never a node index)
 
 // root: the node the query starts at (0: the tree's root; a child reference
 // whose subtree holds every triangle the ray can hit, a leaf included).
 R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax, int root = 0) {
   s.r = make_ray_pre(o, d);
+  s.wo = o;
+  s.wd = d;
+  s.vdelta = 0;
   s.best.t = tmax;
   s.best.b1 = s.best.b2 = 0.0f;
   s.best.tri = 0x7FFFFFFF;
@@ -180,6 +206,18 @@ R2_HD void trace_begin(TraceState& s, V3 o, V3 d, float tmax, int root = 0) {
   s.sp = 0;
   s.found = 0;
   s.nodes = s.tris = 0;
+}
+
+// The object-space origin and direction of a world-space ray.
+R2_HD V3 inst_point(const BvhInstance& in, V3 p) {
+  return v3(in.w2o[0].x * p.x + in.w2o[0].y * p.y + in.w2o[0].z * p.z + in.w2o[0].w,
+            in.w2o[1].x * p.x + in.w2o[1].y * p.y + in.w2o[1].z * p.z + in.w2o[1].w,
+            in.w2o[2].x * p.x + in.w2o[2].y * p.y + in.w2o[2].z * p.z + in.w2o[2].w);
+}
+R2_HD V3 inst_vector(const BvhInstance& in, V3 d) {
+  return v3(in.w2o[0].x * d.x + in.w2o[0].y * d.y + in.w2o[0].z * d.z,
+            in.w2o[1].x * d.x + in.w2o[1].y * d.y + in.w2o[1].z * d.z,
+            in.w2o[2].x * d.x + in.w2o[2].y * d.y + in.w2o[2].z * d.z);
 }
 
 // Next stacked child whose entry distance is not beyond the closest hit.
@@ -210,20 +248,49 @@ R2_HD bool trace_all_have_leaf(bool mine) {
 // entry distance.  The builder bounds the tree depth by R2_BVH_STACK so the
 // stack cannot overflow.  The closest hit does not depend on the visiting
 // order (ties go to the lower triangle index).
-template <bool kAnyHit, bool kCount = false, bool kAlpha = false>
+//
+// kInst (two-level BVHs): a top-level leaf with count 0 is an instance.
+// Entering it pushes the node to resume at (without its entry distance) and
+// the kInstExit marker, transforms the ray and continues at the instance's
+// root; popping the marker restores the world-space ray, after any postponed
+// leaf of the instance has been tested.  The stack then holds the top-level
+// path, the marker and the instance's path: the builder bounds the sum of the
+// two heights plus two by R2_BVH_STACK.
+template <bool kAnyHit, bool kCount = false, bool kAlpha = false, bool kInst = false, bool kTop = false>
 R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* stackT, int maxVisits) {
   int budget = maxVisits;
   while (budget > 0) {
     // inner nodes, the first leaf met postponed
     while (s.cur >= 0 && s.cur != kTraceDone && budget > 0) {
+      if (kInst && s.cur == kInstExit) {
+        if (s.leaf != 0) break;  // the instance's postponed leaf first
+        s.r = make_ray_pre(s.wo, s.wd);
+        s.vdelta = 0;
+        s.cur = trace_pop(s, stack, stackT);
+        if (s.cur < 0 && s.leaf == 0) {
+          s.leaf = s.cur;
+          s.cur = trace_pop(s, stack, stackT);
+        }
+        if (trace_all_have_leaf(s.leaf != 0)) break;
+        continue;
+      }
       --budget;
       if (kCount) ++s.nodes;
       const int cur = s.cur;
 #if defined(__CUDA_ARCH__)
-      const float4 b0 = __ldg(&bvh.nodes[cur].b0);
-      const float4 b1 = __ldg(&bvh.nodes[cur].b1);
-      const float4 bz = __ldg(&bvh.nodes[cur].bz);
-      const int4 ch = __ldg(&bvh.nodes[cur].ch);
+      float4 b0, b1, bz;
+      int4 ch;
+      if (kTop && cur < bvh.ntop) {
+        b0 = bvh.top[cur].b0;
+        b1 = bvh.top[cur].b1;
+        bz = bvh.top[cur].bz;
+        ch = bvh.top[cur].ch;
+      } else {
+        b0 = __ldg(&bvh.nodes[cur].b0);
+        b1 = __ldg(&bvh.nodes[cur].b1);
+        bz = __ldg(&bvh.nodes[cur].bz);
+        ch = __ldg(&bvh.nodes[cur].ch);
+      }
 #else
       const float4 b0 = bvh.nodes[cur].b0;
       const float4 b1 = bvh.nodes[cur].b1;
@@ -258,6 +325,23 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
     while (s.leaf < 0) {
       const int first = bvh_leaf_first(s.leaf);
       const int count = bvh_leaf_count(s.leaf);
+      if (kInst && count == 0) {  // enter instance `first`
+        --budget;
+        s.leaf = 0;
+        const BvhInstance& in = bvh.inst[first];
+        if (s.cur != kTraceDone) {
+          stack[s.sp] = s.cur;
+          stackT[s.sp] = -INFINITY;
+          ++s.sp;
+        }
+        stack[s.sp] = kInstExit;
+        stackT[s.sp] = -INFINITY;
+        ++s.sp;
+        if (!in.identity) s.r = make_ray_pre(inst_point(in, s.wo), inst_vector(in, s.wd));
+        s.vdelta = in.vdelta;
+        s.cur = in.root;
+        break;
+      }
       budget -= count;
       if (kCount) s.tris += (uint32_t)count;
       for (int i = 0; i < count; ++i) {
@@ -271,8 +355,8 @@ R2_HD bool trace_advance(const BvhView& bvh, TraceState& s, int* stack, float* s
         const float4 b = bvh.tris[3 * tri + 1];
         const float4 c = bvh.tris[3 * tri + 2];
 #endif
-        if (tri_test<kAlpha>(s.r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri, &s.best,
-                             &bvh.alpha)) {
+        if (tri_test<kAlpha>(s.r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(c.x, c.y, c.z), tri,
+                             kInst ? tri + s.vdelta : tri, &s.best, &bvh.alpha)) {
           s.found = 1;
           if (kAnyHit) {
             s.leaf = 0;
@@ -304,7 +388,15 @@ R2_HD Hit bvh_trace(const BvhView& bvh, V3 o, V3 d, float tmax, uint32_t* nodes 
   trace_begin(s, o, d, tmax, root);
   int stack[R2_BVH_STACK];
   float stackT[R2_BVH_STACK];
-  if (bvh.alpha.alphaTex) {
+  if (bvh.inst) {
+    if (bvh.alpha.alphaTex) {
+      while (!trace_advance<kAnyHit, kCount, true, true>(bvh, s, stack, stackT, 1 << 30)) {
+      }
+    } else {
+      while (!trace_advance<kAnyHit, kCount, false, true>(bvh, s, stack, stackT, 1 << 30)) {
+      }
+    }
+  } else if (bvh.alpha.alphaTex) {
     while (!trace_advance<kAnyHit, kCount, true>(bvh, s, stack, stackT, 1 << 30)) {
     }
   } else {

@@ -5,14 +5,17 @@
 // 3. 63-bit Morton codes (21 bits per axis);
 // 4. stable radix sort of (code, triangle) pairs — ties keep triangle order
 //    (radix_sort.cu);
-// 5. Karras hierarchy ("Maximizing Parallelism in the Construction of BVHs,
-//    Octrees, and k-d Trees", HPG 2012) over the sorted codes;
-// 6. bottom-up pass computing boxes and the SAH cost of each node, collapsing a
-//    subtree into one leaf when kSahTri*n <= kSahNode + (A_l c_l + A_r c_r)/A
-//    and n <= kLeafMax (the SAH refinement step);
+// 5. the hierarchy over the sorted primitives: PLOC clustering (bvh_ploc.cu,
+//    the default) or the Karras radix tree ("Maximizing Parallelism in the
+//    Construction of BVHs, Octrees, and k-d Trees", HPG 2012);
+// 6. boxes and the SAH cost of each node, collapsing a subtree into one leaf
+//    when kSahTri*n <= kSahNode + (A_l c_l + A_r c_r)/A and n <= kLeafMax
+//    (a bottom-up pass for the Karras tree; PLOC decides at each merge);
 // 7. emission of the 64-byte nodes and the BVH-ordered triangle array.
 // Every step is a pure function of the input, so the host oracle rebuilds the
 // identical tree (same codes, same splits, same collapse decisions).
+#include <atomic>
+
 #include "bvh_build.cuh"
 
 namespace r2 {
@@ -199,7 +202,7 @@ __global__ void k_bottom_up(int n, const uint32_t* __restrict__ order, const flo
                             const int* __restrict__ last, const int* __restrict__ nodeParent,
                             const int* __restrict__ leafParent, float4* leafLo, float4* leafHi,
                             float4* nodeLo, float4* nodeHi, float* nodeCost, int* nodeHeight,
-                            int* collapse, int* flags) {
+                            int* collapse, int* flags, int leafMax) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t prim = order[i];
@@ -219,7 +222,7 @@ __global__ void k_bottom_up(int n, const uint32_t* __restrict__ order, const flo
     float inner = (A > 0.0f) ? kSahNode + (Al * a.cost + Ar * b.cost) / A : kSahNode + a.cost + b.cost;
     int count = last[p] - first[p] + 1;
     float leafc = kSahTri * (float)count;
-    int col = (count <= kLeafMax && leafc <= inner) ? 1 : 0;
+    int col = (count <= leafMax && leafc <= inner) ? 1 : 0;
     nodeLo[p] = lo;
     nodeHi[p] = hi;
     nodeCost[p] = col ? leafc : inner;
@@ -294,6 +297,10 @@ __global__ void k_init_bounds(uint32_t* cb) {
 
 }  // namespace
 
+static std::atomic<int> g_bvhMethod{kBvhPloc};
+int bvh_method() { return g_bvhMethod.load(); }
+void set_bvh_method(int method) { g_bvhMethod.store(method == kBvhKarras ? kBvhKarras : kBvhPloc); }
+
 // Steps 3-7 over primitive boxes whose centroid bounds are in cb_; with
 // d_pos/d_idx the BVH-ordered triangle array is gathered too.
 void BvhBuilder::from_boxes(const float4* triLo, const float4* triHi, uint32_t ntris, const float* d_pos,
@@ -301,18 +308,35 @@ void BvhBuilder::from_boxes(const float4* triLo, const float4* triHi, uint32_t n
   const int n = (int)ntris;
   keys_.reserve(n);
   out->order.reserve(n);
-  k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo, triHi, ntris, cb_.get(), keys_.get(), out->order.get());
-  radix_sort_pairs(keys_.get(), out->order.get(), ntris, 63, &sort_, s);
+  const bool usePloc = n > 1 && bvh_method() == kBvhPloc;
+  if (usePloc) sorted_.reserve(n);
+  uint32_t* sorted = usePloc ? sorted_.get() : out->order.get();
+  k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo, triHi, ntris, cb_.get(), keys_.get(), sorted);
+  const int sortLaunches = radix_sort_pairs(keys_.get(), sorted, ntris, 63, &sort_, s);
+  launches_ += 1 + sortLaunches;
   out->ntris = ntris;
-  if (d_pos) {
+  auto gather = [&]() {
+    if (!d_pos) return;
     out->tris.reserve((size_t)3 * n);
     k_gather_tris<<<(n + 255) / 256, 256, 0, s>>>(d_pos, d_idx, out->order.get(), ntris, out->tris.get());
+    ++launches_;
+  };
+  if (usePloc) {
+    const int h = ploc(triLo, triHi, n, out, s);  // waits for the device
+    gather();
+    R2_CUDA(cudaGetLastError());
+    out->height = h ? (uint32_t)h : 1u;
+    R2_REQUIRE(out->height <= R2_BVH_STACK, R2_ERR_UNSUPPORTED,
+               "BVH deeper than the traversal stack (" + std::to_string(out->height) + " levels)");
+    return;
   }
+  gather();
   if (n == 1) {
     out->nodes.reserve(1);
     out->nnodes = 1;
     out->height = 1;
     k_single_leaf<<<1, 1, 0, s>>>(triLo, triHi, out->nodes.get());
+    ++launches_;
     R2_CUDA(cudaGetLastError());
     R2_CUDA(cudaStreamSynchronize(s));
     return;
@@ -331,12 +355,14 @@ void BvhBuilder::from_boxes(const float4* triLo, const float4* triHi, uint32_t n
   k_bottom_up<<<(n + 255) / 256, 256, 0, s>>>(n, out->order.get(), triLo, triHi, left_.get(), right_.get(),
                                               first_.get(), last_.get(), nodeParent_.get(), leafParent_.get(),
                                               leafLo_.get(), leafHi_.get(), nodeLo_.get(), nodeHi_.get(),
-                                              nodeCost_.get(), nodeHeight_.get(), collapse_.get(), flags_.get());
+                                              nodeCost_.get(), nodeHeight_.get(), collapse_.get(), flags_.get(),
+                                              leafMax_);
   out->nodes.reserve(ni);
   out->nnodes = ni;
   k_emit<<<(ni + 255) / 256, 256, 0, s>>>(n, left_.get(), right_.get(), first_.get(), last_.get(),
                                           nodeParent_.get(), leafLo_.get(), leafHi_.get(), nodeLo_.get(),
                                           nodeHi_.get(), nodeHeight_.get(), collapse_.get(), out->nodes.get());
+  launches_ += 3;  // karras, bottom-up, emit
   R2_CUDA(cudaGetLastError());
   int root[2] = {0, 0};
   R2_CUDA(cudaMemcpyAsync(&root[0], nodeHeight_.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -350,23 +376,28 @@ void BvhBuilder::from_boxes(const float4* triLo, const float4* triHi, uint32_t n
 void BvhBuilder::build(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s) {
   R2_REQUIRE(ntris > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero triangles");
   R2_REQUIRE(ntris < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 triangles");
+  leafMax_ = kLeafMax;
   triLo_.reserve(ntris);
   triHi_.reserve(ntris);
   cb_.reserve(6);
   k_init_bounds<<<1, 32, 0, s>>>(cb_.get());
   int nb = (int)std::min<uint32_t>((ntris + 255) / 256, (uint32_t)sm_count() * 8);
   k_tri_bounds<<<nb, 256, 0, s>>>(d_pos, d_idx, ntris, triLo_.get(), triHi_.get(), cb_.get());
+  launches_ = 2;
   from_boxes(triLo_.get(), triHi_.get(), ntris, d_pos, d_idx, out, s);
 }
 
 void BvhBuilder::build_boxes(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out,
-                             cudaStream_t s) {
+                             cudaStream_t s, int leafMax) {
   R2_REQUIRE(nboxes > 0, R2_ERR_INVALID_ARGUMENT, "BVH over zero boxes");
+  R2_REQUIRE(leafMax >= 1 && leafMax <= kLeafMax, R2_ERR_INVALID_ARGUMENT, "leaf size out of range");
+  leafMax_ = leafMax;
   R2_REQUIRE(nboxes < (1u << 26), R2_ERR_UNSUPPORTED, "BVH supports fewer than 2^26 boxes");
   cb_.reserve(6);
   k_init_bounds<<<1, 32, 0, s>>>(cb_.get());
   int nb = (int)std::min<uint32_t>((nboxes + 255) / 256, (uint32_t)sm_count() * 8);
   k_box_bounds<<<nb, 256, 0, s>>>(d_lo, d_hi, nboxes, cb_.get());
+  launches_ = 2;
   from_boxes(d_lo, d_hi, nboxes, nullptr, nullptr, out, s);
 }
 
@@ -375,9 +406,10 @@ void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, Device
   b.build(d_pos, d_idx, ntris, out, s);
 }
 
-void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s) {
+void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s,
+                   int leafMax) {
   BvhBuilder b;
-  b.build_boxes(d_lo, d_hi, nboxes, out, s);
+  b.build_boxes(d_lo, d_hi, nboxes, out, s, leafMax);
 }
 
 }  // namespace r2

@@ -11,6 +11,15 @@ namespace r2 {
 constexpr float kSahNode = 1.2f;
 constexpr float kSahTri = 1.0f;
 constexpr int kLeafMax = 8;
+// Window of the PLOC nearest-neighbour search: positions i - r .. i + r.
+constexpr int kPlocRadius = 16;
+
+// Hierarchy over the Morton-sorted primitives: PLOC clustering (default) or
+// the Karras radix tree.  Both end with the same SAH leaf collapse.
+enum BvhMethod { kBvhPloc = 0, kBvhKarras = 1 };
+// Process-wide choice for the BVHs built from now on.
+int bvh_method();
+void set_bvh_method(int method);
 
 // A triangle BVH resident in device memory.
 struct DeviceBvh {
@@ -37,18 +46,34 @@ struct DeviceBvh {
 // traversal stack.
 class BvhBuilder {
  public:
+  BvhBuilder() = default;
+  BvhBuilder(const BvhBuilder&) = delete;
+  BvhBuilder& operator=(const BvhBuilder&) = delete;
+  ~BvhBuilder();
   void build(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s);
-  void build_boxes(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s);
+  // leafMax: the most boxes a collapsed leaf may hold (1: no collapse, every
+  // leaf one box).
+  void build_boxes(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t s,
+                   int leafMax = kLeafMax);
+  // Kernels the last build launched.
+  int launches() const { return launches_; }
 
  private:
   void from_boxes(const float4* lo, const float4* hi, uint32_t n, const float* d_pos, const uint32_t* d_idx,
                   DeviceBvh* out, cudaStream_t s);
+  int ploc(const float4* lo, const float4* hi, int n, DeviceBvh* out, cudaStream_t s);
   DBuf<float4> triLo_, triHi_, leafLo_, leafHi_, nodeLo_, nodeHi_;
+  DBuf<float4> cLo_[2], cHi_[2];
   DBuf<uint64_t> keys_;
   DBuf<int> left_, right_, first_, last_, nodeParent_, leafParent_, nodeHeight_, collapse_, flags_;
+  DBuf<int> cRef_[2], nn_, count_, leafPos_, state_;
+  DBuf<int2> blockCounts_;
   DBuf<float> nodeCost_;
-  DBuf<uint32_t> cb_;
+  DBuf<uint32_t> cb_, sorted_;
   RadixSortScratch sort_;
+  void* hostState_ = nullptr;  // pinned copy of the PLOC iteration state
+  int launches_ = 0;
+  int leafMax_ = kLeafMax;
 };
 
 // Builds the BVH over triangles (d_pos: 3 floats per vertex, d_idx: 3 per
@@ -59,6 +84,7 @@ void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, Device
 // The same hierarchy over boxes (d_lo/d_hi: one float4 per box, xyz used,
 // device): leaves reference BVH positions, order[] maps them to box indices;
 // no triangle array.
-void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t stream);
+void build_box_bvh(const float4* d_lo, const float4* d_hi, uint32_t nboxes, DeviceBvh* out, cudaStream_t stream,
+                   int leafMax = kLeafMax);
 
 }  // namespace r2

@@ -6,6 +6,7 @@
 #include <string>
 #include <vector>
 
+#include "bvh_build.cuh"
 #include "capi_util.h"
 #include "filter.cuh"
 #include "filter_host.h"
@@ -43,6 +44,15 @@ const char* r2_status_string(r2_status s) {
 const char* r2_last_error(void) { return r2::last_error(); }
 
 int r2_version(void) { return 100; }
+
+r2_status r2_set_bvh_method(int method) {
+  R2_API_BEGIN
+  R2_REQUIRE(method == R2_BVH_PLOC || method == R2_BVH_KARRAS, R2_ERR_INVALID_ARGUMENT, "unknown BVH method");
+  r2::set_bvh_method(method == R2_BVH_KARRAS ? r2::kBvhKarras : r2::kBvhPloc);
+  R2_API_END
+}
+
+int r2_get_bvh_method(void) { return r2::bvh_method() == r2::kBvhKarras ? R2_BVH_KARRAS : R2_BVH_PLOC; }
 
 r2_status r2_filter_setup_grid(const float* model_bb_min, const float* model_bb_max, const float* model_to_world,
                                float voxel_size, r2_filter_grid* grid_out) {

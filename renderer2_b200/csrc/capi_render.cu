@@ -48,6 +48,22 @@ r2_status r2_scene_add_mesh(r2_scene* scene, const float* positions, uint32_t nv
   R2_API_END
 }
 
+r2_status r2_scene_add_mesh_asset(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
+                                  uint32_t ntris, const float* normals, const float* uvs, const r2_material* material,
+                                  const r2_material_maps* maps, uint32_t* asset_out) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene && material && asset_out, R2_ERR_INVALID_ARGUMENT, "null argument");
+  *asset_out = scene->impl->add_mesh_asset(positions, nverts, indices, ntris, normals, *material, uvs, maps);
+  R2_API_END
+}
+
+r2_status r2_scene_add_mesh_instance(r2_scene* scene, uint32_t asset, const float* model_to_world, uint32_t mask) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  scene->impl->add_mesh_instance(asset, model_to_world, mask);
+  R2_API_END
+}
+
 r2_status r2_scene_add_mesh_textured(r2_scene* scene, const float* positions, uint32_t nverts, const uint32_t* indices,
                                      uint32_t ntris, const float* normals, const float* uvs,
                                      const r2_material* material, const r2_material_maps* maps,
@@ -102,6 +118,16 @@ r2_status r2_scene_rebuild(r2_scene* scene, void* stream) {
   R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
   R2_REQUIRE(scene->impl->committed(), R2_ERR_INVALID_ARGUMENT, "scene not committed");
   scene->impl->rebuild((cudaStream_t)stream);
+  R2_API_END
+}
+
+r2_status r2_scene_bvh_info(r2_scene* scene, uint32_t* nodes, uint32_t* height, uint32_t* build_launches) {
+  R2_API_BEGIN
+  R2_REQUIRE(scene, R2_ERR_INVALID_ARGUMENT, "null argument");
+  R2_REQUIRE(scene->impl->committed(), R2_ERR_INVALID_ARGUMENT, "scene not committed");
+  if (nodes) *nodes = scene->impl->bvh_nodes();
+  if (height) *height = scene->impl->bvh_height();
+  if (build_launches) *build_launches = (uint32_t)scene->impl->bvh_build_launches();
   R2_API_END
 }
 

@@ -190,9 +190,9 @@ void RadixSortScratch::reserve(uint32_t n) {
   partials.reserve((L + kScanPart - 1) / kScanPart);
 }
 
-void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, RadixSortScratch* scr, cudaStream_t s) {
+int radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, RadixSortScratch* scr, cudaStream_t s) {
   R2_REQUIRE(bits >= 1 && bits <= 64, R2_ERR_INVALID_ARGUMENT, "radix sort key bits must be in [1, 64]");
-  if (n <= 1) return;
+  if (n <= 1) return 0;
   const uint32_t nb = rs_blocks(n);
   const size_t L = (size_t)nb * kRsBins;
   const uint32_t np = (uint32_t)((L + kScanPart - 1) / kScanPart);
@@ -220,6 +220,7 @@ void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, Radi
     R2_CUDA(cudaMemcpyAsync(keys, kin, (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
     R2_CUDA(cudaMemcpyAsync(vals, vin, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
   }
+  return 5 * passes;
 }
 
 }  // namespace r2

@@ -16,8 +16,9 @@ struct RadixSortScratch {
 
 // Sorts n pairs ascending by the low `bits` bits of the keys (1..64), stably:
 // equal keys keep their input order.  In place: keys/vals hold the sorted
-// pairs when the stream reaches the end of the sort.
-void radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, RadixSortScratch* scratch,
+// pairs when the stream reaches the end of the sort.  Returns the number of
+// kernels launched.
+int radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, RadixSortScratch* scratch,
                       cudaStream_t s);
 
 }  // namespace r2

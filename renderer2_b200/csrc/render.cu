@@ -24,6 +24,9 @@
 // bounce, block, purpose) — independent of queue position and batching.
 #include <algorithm>
 
+#include <map>
+#include <mutex>
+
 #include "render.cuh"
 #include "texture_shade.cuh"
 
@@ -357,7 +360,7 @@ __device__ __noinline__ Ray voxel_border_nc(const MediumView* M, Ray r) { return
 // visits each node at most once) is ended as a miss and counted in *bound.
 constexpr int kMaxTraceVisits = 1 << 26;
 
-template <bool kAnyHit, bool kAlpha, class Begin, class End>
+template <bool kAnyHit, bool kAlpha, bool kInst, bool kTop, class Begin, class End>
 __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n, uint32_t* taken, int visits,
                                                  int refill, unsigned int* bound, Begin begin, End end) {
   int stack[R2_BVH_STACK];
@@ -391,7 +394,7 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
       continue;
     }
     if (active) {
-      bool done = trace_advance<kAnyHit, false, kAlpha>(bvh, s, stack, stackT, visits);
+      bool done = trace_advance<kAnyHit, false, kAlpha, kInst, kTop>(bvh, s, stack, stackT, visits);
       spent += visits;
       if (!done && spent >= kMaxTraceVisits) {
         s.best.tri = -1;
@@ -399,6 +402,10 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
         done = true;
       }
       if (done) {
+        if (!kInst) {  // one level: the traversal ray is the world ray (keeps wo/wd out of the live state)
+          s.wo = s.r.o;
+          s.wd = s.r.d;
+        }
         end(item, s);
         active = false;
       }
@@ -408,6 +415,39 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
 
 __device__ __forceinline__ int trav_visits(const RenderLaunch& L) { return (int)max(1u, L.travVisits); }
 __device__ __forceinline__ int trav_refill(const RenderLaunch& L) { return (int)min(32u, max(1u, L.travRefill)); }
+
+// The persistent traversal of the scene's BVH with the instantiation it needs
+// (alpha-tested triangles, two levels).  With L.topNodes, the block first
+// copies BVH nodes 0 .. topNodes-1 (the host keeps the count within the tree
+// and kMaxTopNodes) into its dynamic shared memory and reads them from there.
+// Every thread of the block calls this once.
+template <bool kAnyHit, class Begin, class End>
+__device__ __forceinline__ void trace_scene(const RenderLaunch& L, uint32_t n, uint32_t* taken, Begin begin, End end) {
+  extern __shared__ BvhNode sTop[];
+  BvhView bvh = L.scene.bvh;
+  const int ntop = (int)L.topNodes;
+  const int v = trav_visits(L), r = trav_refill(L);
+  const bool alpha = bvh.alpha.alphaTex != nullptr, inst = bvh.inst != nullptr;
+  if (ntop > 0) {
+    for (int k = threadIdx.x; k < ntop; k += blockDim.x) sTop[k] = bvh.nodes[k];
+    __syncthreads();
+    bvh.top = sTop;
+    bvh.ntop = ntop;
+    if (inst) {
+      if (alpha) trace_persistent<kAnyHit, true, true, true>(bvh, n, taken, v, r, L.bound, begin, end);
+      else trace_persistent<kAnyHit, false, true, true>(bvh, n, taken, v, r, L.bound, begin, end);
+    } else {
+      if (alpha) trace_persistent<kAnyHit, true, false, true>(bvh, n, taken, v, r, L.bound, begin, end);
+      else trace_persistent<kAnyHit, false, false, true>(bvh, n, taken, v, r, L.bound, begin, end);
+    }
+  } else if (inst) {
+    if (alpha) trace_persistent<kAnyHit, true, true, false>(bvh, n, taken, v, r, L.bound, begin, end);
+    else trace_persistent<kAnyHit, false, true, false>(bvh, n, taken, v, r, L.bound, begin, end);
+  } else {
+    if (alpha) trace_persistent<kAnyHit, true, false, false>(bvh, n, taken, v, r, L.bound, begin, end);
+    else trace_persistent<kAnyHit, false, false, false>(bvh, n, taken, v, r, L.bound, begin, end);
+  }
+}
 
 // Closest hit of every live path (scenes without media).  A path that hits a
 // surface goes to the bounce's hit queue (shading, shadow rays and
@@ -444,13 +484,9 @@ __global__ void __launch_bounds__(128, 10) k_extend(RenderLaunch L) {
     return true;
   };
   auto end = [&](uint32_t p, const TraceState& s) {
-    extend_result(L, p, s.r.d, scene_closest_after<false>(L.scene, s.r.o, s.r.d, kDefaultTmax, s.best));
+    extend_result(L, p, s.wd, scene_closest_after<false>(L.scene, s.wo, s.wd, kDefaultTmax, s.best));
   };
-  uint32_t* taken = &L.st.counts[kTravCounters + 2 * L.bounce];
-  if (L.scene.bvh.alpha.alphaTex)
-    trace_persistent<false, true>(L.scene.bvh, n, taken, trav_visits(L), trav_refill(L), L.bound, begin, end);
-  else
-    trace_persistent<false, false>(L.scene.bvh, n, taken, trav_visits(L), trav_refill(L), L.bound, begin, end);
+  trace_scene<false>(L, n, &L.st.counts[kTravCounters + 2 * L.bounce], begin, end);
 }
 
 // ------------------------------------------------------------------ media: path extension
@@ -780,18 +816,36 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   V3 n;
   Material m;
   if (code >= 0) {
-    const float4 n0 = __ldg(&L.scene.triN[3 * code]);
-    const float4 n1 = __ldg(&L.scene.triN[3 * code + 1]);
-    const float4 n2 = __ldg(&L.scene.triN[3 * code + 2]);
+    int tri = code, inst = -1;
+    if (L.scene.bvh.inst) {  // the instance of the code, and the triangle's BVH-order index
+      int lo = 0, hi = L.scene.ninst - 1;
+      while (lo < hi) {  // last instance whose first code is <= code
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&L.scene.instCode[mid]) <= code) lo = mid; else hi = mid - 1;
+      }
+      inst = lo;
+      tri = code - __ldg(&L.scene.bvh.inst[inst].vdelta);
+      if (__ldg(&L.scene.bvh.inst[inst].identity)) inst = -1;
+    }
+    const float4 n0 = __ldg(&L.scene.triN[3 * tri]);
+    const float4 n1 = __ldg(&L.scene.triN[3 * tri + 1]);
+    const float4 n2 = __ldg(&L.scene.triN[3 * tri + 2]);
     const float b0 = (1.0f - hr.y) - hr.z;
     n = normalize(xyz(n0) * b0 + xyz(n1) * hr.y + xyz(n2) * hr.z);
-    m = L.scene.mats[__ldg(&L.scene.triMat[code])];
+    m = L.scene.mats[__ldg(&L.scene.triMat[tri])];
     if (L.scene.triUV && (m.tex[0] >= 0 || m.tex[1] >= 0 || m.tex[2] >= 0)) {
       const TexView tv = {L.scene.triUV, L.scene.texels, L.scene.texInfo, L.scene.bvh.tris};
-      const TexShade ts = textured_surface(tv, m.tex[0], m.tex[1], m.tex[2], code, hr.y, hr.z, n, m.diffuse, m.specular);
+      const TexShade ts = textured_surface(tv, m.tex[0], m.tex[1], m.tex[2], tri, hr.y, hr.z, n, m.diffuse, m.specular);
       n = ts.n;
       m.diffuse = ts.diffuse;
       m.specular = ts.specular;
+    }
+    if (inst >= 0) {  // __closesthit__ch: normalize(modelToWorld * vec4(n, 0)) in glm's column order
+      const float4 r0 = __ldg(&L.scene.instO2W[3 * inst]), r1 = __ldg(&L.scene.instO2W[3 * inst + 1]);
+      const float4 r2 = __ldg(&L.scene.instO2W[3 * inst + 2]);
+      n = normalize(v3(r0.x * n.x + r0.y * n.y + r0.z * n.z + r0.w * 0.0f,
+                       r1.x * n.x + r1.y * n.y + r1.z * n.z + r1.w * 0.0f,
+                       r2.x * n.x + r2.y * n.y + r2.z * n.z + r2.w * 0.0f));
     }
   } else {
     const Shape& sh = L.scene.shapes[-2 - code];
@@ -1062,15 +1116,11 @@ __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
         noTris.hasTris = 0;
         Hit none;
         none.tri = -1;
-        occluded = __float_as_int(scene_closest_after<false>(noTris, s.r.o, s.r.d, s.best.t, none).w) != -1;
+        occluded = __float_as_int(scene_closest_after<false>(noTris, s.wo, s.wd, s.best.t, none).w) != -1;
       }
       L.st.shTr[j] = occluded ? 0.0f : 1.0f;
     };
-    uint32_t* taken = &L.st.counts[kTravCounters + 2 * L.bounce + 1];
-    if (L.scene.bvh.alpha.alphaTex)
-      trace_persistent<true, true>(L.scene.bvh, 2 * n, taken, trav_visits(L), trav_refill(L), L.bound, begin, end);
-    else
-      trace_persistent<true, false>(L.scene.bvh, 2 * n, taken, trav_visits(L), trav_refill(L), L.bound, begin, end);
+    trace_scene<true>(L, 2 * n, &L.st.counts[kTravCounters + 2 * L.bounce + 1], begin, end);
   }
   if (L.stats) {
     for (int o = 16; o > 0; o >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, o);
@@ -1219,15 +1269,29 @@ __global__ void __launch_bounds__(256) k_finish(RenderLaunch L) {
 }
 
 template <typename K>
-int resident_blocks(K kernel, int threads) {
+int resident_blocks(K kernel, int threads, size_t smem = 0) {
   int n = 0;
-  R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0));
+  R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem));
   return std::max(1, n) * sm_count();
 }
 
 int g_trackBlocks[4] = {0, 0, 0, 0};  // resident blocks of k_track<dda, sample>, by dda + 2 sample
 
 int g_travBlocks[2] = {0, 0};  // resident blocks of k_extend, k_shadow_surfaces
+
+// Resident blocks of a surface traversal kernel (0: k_extend, 1:
+// k_shadow_surfaces) with topNodes BVH nodes of dynamic shared memory.
+int trav_blocks(int which, uint32_t topNodes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, uint32_t>, int> cache;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({which, topNodes});
+  if (it != cache.end()) return it->second;
+  const size_t smem = topNodes * sizeof(BvhNode);
+  const int n = which == 0 ? resident_blocks(k_extend, 128, smem) : resident_blocks(k_shadow_surfaces, 128, smem);
+  cache[{which, topNodes}] = n;
+  return n;
+}
 
 void query_track_blocks() {
   if (g_trackBlocks[0] != 0) return;
@@ -1302,11 +1366,12 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
         else k_shadow_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
     } else {
-      k_extend<<<std::min(nblocks * 2, g_travBlocks[0]), 128, 0, s>>>(L);
+      k_extend<<<std::min(nblocks * 2, trav_blocks(0, L.topNodes)), 128, L.topNodes * sizeof(BvhNode), s>>>(L);
       mark(1);
       k_shade<false><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
-      k_shadow_surfaces<<<std::min(nblocks * 2, g_travBlocks[1]), 128, 0, s>>>(L);
+      k_shadow_surfaces<<<std::min(nblocks * 2, trav_blocks(1, L.topNodes)), 128, L.topNodes * sizeof(BvhNode),
+                          s>>>(L);
     }
     mark(3);
     k_accum<<<nblocks, 256, 0, s>>>(L);

@@ -36,6 +36,11 @@ struct SceneView {
   const float2* triUV;      // 3 texture coordinates per BVH-order triangle, nullable
   const float4* texels;     // texture maps of the materials (TexInfo offsets), nullable
   const TexInfo* texInfo;
+  // two-level scenes (bvh.inst set): per instance the first hit code (ascending)
+  // and the object-to-world 3x3 | translation rows that take its normals to world space
+  const int* instCode;
+  const float4* instO2W;
+  int ninst;
 };
 
 // Per-path SoA state of one wave (one sample of every pixel).
@@ -75,6 +80,8 @@ struct PathState {
   int2* swM;        // shadow walk: current medium, draw index of the slot's stream
 };
 
+// Most BVH nodes the surface traversals stage in shared memory (16 KB per block).
+constexpr uint32_t kMaxTopNodes = 256;
 // Launch tuning defaults (RenderLaunch::trackSteps, travVisits, travRefill);
 // no result depends on them.
 constexpr uint32_t kDefaultTrackSteps = 8;   // tracking steps a lane takes between refills
@@ -129,6 +136,7 @@ struct RenderLaunch {
   uint32_t mediaRounds; // queued medium-boundary rounds per bounce (tuning, 1..kMaxMediaRounds)
   uint32_t trackBlocks; // persistent tracker blocks per SM (tuning; 0: every resident block)
   uint32_t trackLimit;  // steps of one tracking loop after which the path ends (1..kMaxTrackingSteps)
+  uint32_t topNodes;    // BVH nodes staged in shared memory by the surface traversals (0: none, <= kMaxTopNodes)
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

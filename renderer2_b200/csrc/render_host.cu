@@ -164,6 +164,38 @@ void RenderScene::add_mesh(const float* pos, uint32_t nverts, const uint32_t* id
   committed_ = false;
 }
 
+uint32_t RenderScene::add_mesh_asset(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris,
+                                     const float* nrm, const r2_material& mat, const float* uv,
+                                     const r2_material_maps* maps) {
+  R2_REQUIRE(pos && idx && nrm, R2_ERR_INVALID_ARGUMENT, "null mesh array");
+  R2_REQUIRE(nverts > 0 && ntris > 0, R2_ERR_INVALID_ARGUMENT, "empty mesh");
+  auto a = std::make_unique<MeshAsset>();
+  a->matId = (uint32_t)hMats_.size();
+  Material hm = make_material(mat);
+  if (maps && uv) textures_.material_maps(mat, maps, hm.tex);
+  hMats_.push_back(hm);
+  a->pos.assign(pos, pos + 3 * (size_t)nverts);
+  a->nrm.assign(nrm, nrm + 3 * (size_t)nverts);
+  if (uv) {
+    a->hasUV = true;
+    a->uv.assign(uv, uv + 2 * (size_t)nverts);
+  }
+  a->idx.assign(idx, idx + 3 * (size_t)ntris);
+  for (uint32_t k = 0; k < 3 * ntris; ++k)
+    R2_REQUIRE(idx[k] < nverts, R2_ERR_INVALID_ARGUMENT, "triangle index out of range");
+  assets_.push_back(std::move(a));
+  committed_ = false;
+  return (uint32_t)(assets_.size() - 1);
+}
+
+void RenderScene::add_mesh_instance(uint32_t asset, const float* m2w, uint32_t mask) {
+  R2_REQUIRE(asset < assets_.size(), R2_ERR_INVALID_ARGUMENT, "unknown mesh asset");
+  R2_REQUIRE(m2w, R2_ERR_INVALID_ARGUMENT, "null transform");
+  if (mask == 0) return;  // invisible to render rays, as add_mesh
+  meshInstances_.push_back(MeshInstanceHost{asset, m43_from_floats(m2w)});
+  committed_ = false;
+}
+
 void RenderScene::add_shape(int type, const float* center, float radius, const float* normal, const r2_material& mat,
                             uint32_t mask) {
   R2_REQUIRE(type == kShapeSphere || type == kShapeCircle, R2_ERR_INVALID_ARGUMENT, "unknown shape type");
@@ -220,13 +252,54 @@ __global__ void k_gather_shading(const uint32_t* __restrict__ order, uint32_t n,
   triMat[i] = matIn[p];
   if (triAlpha) triAlpha[i] = alphaIn[p];
 }
+
+// A bottom-level BVH copied into the global node array: inner references
+// move by nodeOff, leaf ranges by triOff, parents by nodeOff.
+__global__ void k_rebase_nodes(const BvhNode* __restrict__ src, uint32_t n, int nodeOff, int triOff,
+                               BvhNode* __restrict__ dst) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BvhNode nd = src[i];
+  auto move = [&](int c) {
+    if (c == R2_BVH_NONE) return c;
+    if (c >= 0) return c + nodeOff;
+    return bvh_leaf_ref(bvh_leaf_first(c) + triOff, bvh_leaf_count(c));
+  };
+  nd.ch.x = move(nd.ch.x);
+  nd.ch.y = move(nd.ch.y);
+  if (nd.ch.z >= 0) nd.ch.z += nodeOff;
+  dst[i] = nd;
+}
+
+// The top level (one box per leaf) with its leaves turned into instance
+// references: ~instance, a leaf reference with count 0.
+__global__ void k_top_level_nodes(const BvhNode* __restrict__ src, uint32_t n, const uint32_t* __restrict__ order,
+                                  BvhNode* __restrict__ dst) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BvhNode nd = src[i];
+  auto inst = [&](int c) {
+    if (c == R2_BVH_NONE || c >= 0) return c;
+    return bvh_leaf_ref((int)order[bvh_leaf_first(c)], 0);
+  };
+  nd.ch.x = inst(nd.ch.x);
+  nd.ch.y = inst(nd.ch.y);
+  dst[i] = nd;
+}
 }  // namespace
 
 void RenderScene::rebuild(cudaStream_t s) {
   if (!s) s = ctx_.stream;
+  if (two_level()) {
+    build_two_level(s);
+    return;
+  }
   const uint32_t nt = (uint32_t)(hIdx_.size() / 3);
   R2_REQUIRE(nt > 0 && dIdx_.get(), R2_ERR_INVALID_ARGUMENT, "scene has no committed triangles");
   builder_.build(dPos_.get(), dIdx_.get(), nt, &bvh_, s);
+  bvhNodes_ = bvh_.nnodes;
+  bvhHeight_ = bvh_.height;
+  buildLaunches_ = builder_.launches() + 1;
   triN_.reserve((size_t)3 * nt);
   triMat_.reserve(nt);
   if (anyUV_) triUV_.reserve((size_t)3 * nt);
@@ -239,6 +312,178 @@ void RenderScene::rebuild(cudaStream_t s) {
   const BvhAlpha alpha = view_.bvh.alpha;
   view_.bvh = bvh_.view();
   view_.bvh.alpha = alpha;
+}
+
+// Device inputs and bottom-level BVHs of the mesh assets (once per commit:
+// their geometry does not change afterwards).
+void RenderScene::upload_assets(cudaStream_t s) {
+  for (auto& ap : assets_) {
+    MeshAsset& a = *ap;
+    const uint32_t nt = (uint32_t)(a.idx.size() / 3);
+    a.dPos.upload(a.pos.data(), a.pos.size(), s);
+    a.dNrm.upload(a.nrm.data(), a.nrm.size(), s);
+    a.dIdx.upload(a.idx.data(), a.idx.size(), s);
+    std::vector<uint32_t> mat(nt, a.matId);
+    a.dTriMat.upload(mat.data(), mat.size(), s);
+    if (a.hasUV) a.dUV.upload(a.uv.data(), a.uv.size(), s);
+    const int alphaTex = a.hasUV ? hMats_[a.matId].tex[3] : -1;
+    if (alphaTex >= 0) {
+      std::vector<int> al(nt, alphaTex);
+      a.dAlphaIn.upload(al.data(), al.size(), s);
+    }
+    builder_.build(a.dPos.get(), a.dIdx.get(), nt, &a.bvh, s);
+  }
+}
+
+// The two-level structure: the world-space meshes' BVH (rebuilt from the
+// resident triangles), the top level over the instances' world boxes, the
+// global node array [top level | world meshes | assets] and triangle array
+// [world meshes | assets] with per-triangle shading data in the same order.
+// Instance 0 is the world-space meshes (identity) when there are any.
+void RenderScene::build_two_level(cudaStream_t s) {
+  const uint32_t nw = (uint32_t)(hIdx_.size() / 3);
+  int launches = 0;
+  if (nw > 0) {
+    builder_.build(dPos_.get(), dIdx_.get(), nw, &bvh_, s);
+    launches += builder_.launches();
+  }
+  // triangle and node offsets of the pools (0: world meshes, 1 + a: asset a)
+  const size_t npool = 1 + assets_.size();
+  std::vector<uint32_t> triOff(npool), ntri(npool), nnode(npool), height(npool);
+  ntri[0] = nw;
+  nnode[0] = nw ? bvh_.nnodes : 0;
+  height[0] = nw ? bvh_.height : 0;
+  for (size_t a = 0; a < assets_.size(); ++a) {
+    ntri[1 + a] = (uint32_t)(assets_[a]->idx.size() / 3);
+    nnode[1 + a] = assets_[a]->bvh.nnodes;
+    height[1 + a] = assets_[a]->bvh.height;
+  }
+  uint64_t totalTris = 0;
+  for (size_t k = 0; k < npool; ++k) {
+    triOff[k] = (uint32_t)totalTris;
+    totalTris += ntri[k];
+  }
+  R2_REQUIRE(totalTris < (1u << 26), R2_ERR_UNSUPPORTED, "two-level scene with 2^26 or more distinct triangles");
+  // instances: boxes (padded so that rounding never culls a hit), transforms, codes
+  struct Inst {
+    size_t pool;
+    M43 m;
+    bool identity;
+  };
+  std::vector<Inst> insts;
+  if (nw > 0) insts.push_back(Inst{0, M43{}, true});
+  for (const MeshInstanceHost& mi : meshInstances_) insts.push_back(Inst{1 + mi.asset, mi.m2w, false});
+  const uint32_t ninst = (uint32_t)insts.size();
+  std::vector<float4> lo(ninst), hi(ninst), o2w(3 * (size_t)ninst);
+  std::vector<BvhInstance> hin(ninst);
+  std::vector<int> code(ninst);
+  auto pad = [](float x) { return 1e-5f * (fabsf(x) + 1.0f); };
+  uint64_t nextCode = 0;
+  for (uint32_t i = 0; i < ninst; ++i) {
+    const Inst& in = insts[i];
+    const std::vector<float>& P = in.pool == 0 ? hPos_ : assets_[in.pool - 1]->pos;
+    V3 mlo = v3(INFINITY), mhi = v3(-INFINITY);
+    for (size_t v = 0; v < P.size(); v += 3) {
+      const V3 p = v3(P[v], P[v + 1], P[v + 2]);
+      mlo = vmin(mlo, p);
+      mhi = vmax(mhi, p);
+    }
+    V3 wlo = mlo, whi = mhi;
+    BvhInstance& b = hin[i];
+    memset(&b, 0, sizeof(b));
+    if (in.identity) {
+      b.identity = 1;
+      b.w2o[0] = make_float4(1, 0, 0, 0);
+      b.w2o[1] = make_float4(0, 1, 0, 0);
+      b.w2o[2] = make_float4(0, 0, 1, 0);
+      for (int r = 0; r < 3; ++r) o2w[3 * i + r] = b.w2o[r];
+    } else {
+      wlo = v3(INFINITY);
+      whi = v3(-INFINITY);
+      for (int c = 0; c < 8; ++c) {
+        const V3 p = xform_point(in.m, v3(c & 1 ? mhi.x : mlo.x, c & 2 ? mhi.y : mlo.y, c & 4 ? mhi.z : mlo.z));
+        wlo = vmin(wlo, p);
+        whi = vmax(whi, p);
+      }
+      const M4 inv = m4_inverse(m43_to_m4(in.m));  // double elimination, rounded to float
+      for (int r = 0; r < 3; ++r) {
+        b.w2o[r] = make_float4(inv.m[0][r], inv.m[1][r], inv.m[2][r], inv.m[3][r]);
+        o2w[3 * i + r] = make_float4(comp(in.m.c[0], r), comp(in.m.c[1], r), comp(in.m.c[2], r), comp(in.m.c[3], r));
+      }
+    }
+    lo[i] = make_float4(wlo.x - pad(wlo.x), wlo.y - pad(wlo.y), wlo.z - pad(wlo.z), 0.0f);
+    hi[i] = make_float4(whi.x + pad(whi.x), whi.y + pad(whi.y), whi.z + pad(whi.z), 0.0f);
+    code[i] = (int)nextCode;
+    b.vdelta = (int)((int64_t)nextCode - (int64_t)triOff[in.pool]);
+    nextCode += ntri[in.pool];
+    R2_REQUIRE(nextCode < 0x7FFFFFFFull, R2_ERR_UNSUPPORTED, "two-level scene with 2^31 or more instanced triangles");
+  }
+  dInstLo_.upload(lo.data(), ninst, s);
+  dInstHi_.upload(hi.data(), ninst, s);
+  builder_.build_boxes(dInstLo_.get(), dInstHi_.get(), ninst, &tlas_, s, 1);
+  launches += builder_.launches();
+  const uint32_t ntl = tlas_.nnodes;
+  std::vector<uint32_t> nodeOff(npool);
+  uint64_t totalNodes = ntl;
+  uint32_t maxHeight = 0;
+  for (size_t k = 0; k < npool; ++k) {
+    nodeOff[k] = (uint32_t)totalNodes;
+    totalNodes += nnode[k];
+    maxHeight = std::max(maxHeight, height[k]);
+  }
+  R2_REQUIRE(tlas_.height + maxHeight + 2 <= R2_BVH_STACK, R2_ERR_UNSUPPORTED,
+             "two-level BVH deeper than the traversal stack");
+  for (uint32_t i = 0; i < ninst; ++i) hin[i].root = (int)nodeOff[insts[i].pool];
+  dInst_.upload(hin.data(), ninst, s);
+  dInstCode_.upload(code.data(), ninst, s);
+  dInstO2W_.upload(o2w.data(), o2w.size(), s);
+  gNodes_.reserve(totalNodes);
+  gTris_.reserve(3 * totalTris);
+  triN_.reserve(3 * totalTris);
+  triMat_.reserve(totalTris);
+  bool sceneUV = anyUV_;
+  for (auto& a : assets_) sceneUV = sceneUV || a->hasUV;
+  if (sceneUV) triUV_.reserve(3 * totalTris);
+  if (anyAlpha_) triAlpha_.reserve(totalTris);
+  k_top_level_nodes<<<(ntl + 255) / 256, 256, 0, s>>>(tlas_.nodes.get(), ntl, tlas_.order.get(), gNodes_.get());
+  ++launches;
+  for (size_t k = 0; k < npool; ++k) {
+    if (ntri[k] == 0) continue;
+    const DeviceBvh& b = k == 0 ? bvh_ : assets_[k - 1]->bvh;
+    k_rebase_nodes<<<(nnode[k] + 255) / 256, 256, 0, s>>>(b.nodes.get(), nnode[k], (int)nodeOff[k], (int)triOff[k],
+                                                          gNodes_.get() + nodeOff[k]);
+    R2_CUDA(cudaMemcpyAsync(gTris_.get() + 3 * (size_t)triOff[k], b.tris.get(), sizeof(float4) * 3 * ntri[k],
+                            cudaMemcpyDeviceToDevice, s));
+    const uint32_t o = triOff[k], n = ntri[k];
+    if (k == 0) {
+      k_gather_shading<<<(n + 255) / 256, 256, 0, s>>>(
+          b.order.get(), n, dIdx_.get(), dNrm_.get(), dTriMatIn_.get(), sceneUV ? dUV_.get() : nullptr,
+          anyAlpha_ ? dTriAlphaIn_.get() : nullptr, triN_.get() + 3 * (size_t)o, triMat_.get() + o,
+          sceneUV ? triUV_.get() + 3 * (size_t)o : nullptr, anyAlpha_ ? triAlpha_.get() + o : nullptr);
+    } else {
+      MeshAsset& a = *assets_[k - 1];
+      k_gather_shading<<<(n + 255) / 256, 256, 0, s>>>(
+          b.order.get(), n, a.dIdx.get(), a.dNrm.get(), a.dTriMat.get(), sceneUV ? a.dUV.get() : nullptr,
+          anyAlpha_ ? a.dAlphaIn.get() : nullptr, triN_.get() + 3 * (size_t)o, triMat_.get() + o,
+          sceneUV ? triUV_.get() + 3 * (size_t)o : nullptr, anyAlpha_ ? triAlpha_.get() + o : nullptr);
+    }
+    launches += 2;
+  }
+  R2_CUDA(cudaGetLastError());
+  const BvhAlpha alpha = view_.bvh.alpha;
+  memset(&view_.bvh, 0, sizeof(view_.bvh));
+  view_.bvh.nodes = gNodes_.get();
+  view_.bvh.tris = gTris_.get();
+  view_.bvh.ntris = (uint32_t)totalTris;
+  view_.bvh.alpha = alpha;
+  view_.bvh.inst = dInst_.get();
+  view_.instCode = dInstCode_.get();
+  view_.instO2W = dInstO2W_.get();
+  view_.ninst = (int)ninst;
+  bvhNodes_ = (uint32_t)totalNodes;
+  bvhHeight_ = tlas_.height + maxHeight;
+  buildLaunches_ = launches;
+  R2_CUDA(cudaStreamSynchronize(s));  // the host vectors above are freed on return
 }
 
 void RenderScene::set_vertices(const float* pos, const float* nrm, uint32_t nverts, cudaStream_t s) {
@@ -258,24 +503,50 @@ void RenderScene::commit() {
   cudaStream_t s = ctx_.stream;
   uint32_t nt = (uint32_t)(hIdx_.size() / 3);
   memset(&view_, 0, sizeof(view_));
+  const bool twoLevel = two_level();
+  bool sceneUV = anyUV_;
+  if (twoLevel)
+    for (auto& a : assets_) sceneUV = sceneUV || a->hasUV;
+  if (sceneUV && !anyUV_) hUV_.assign(2 * (hPos_.size() / 3), 0.0f);  // world meshes without coordinates: (0, 0)
+  anyAlpha_ = false;
   if (nt > 0) {
     dPos_.upload(hPos_.data(), hPos_.size(), s);
     dNrm_.upload(hNrm_.data(), hNrm_.size(), s);
     dIdx_.upload(hIdx_.data(), hIdx_.size(), s);
     dTriMatIn_.upload(hTriMat_.data(), hTriMat_.size(), s);
-    bool anyAlpha = false;
-    if (anyUV_) {  // texture coordinates and opacity maps per triangle
+    if (sceneUV) {  // texture coordinates and opacity maps per triangle
       dUV_.upload(hUV_.data(), hUV_.size(), s);
       std::vector<int> alphaIn(nt);
       for (uint32_t t = 0; t < nt; ++t) {
         alphaIn[t] = hMats_[hTriMat_[t]].tex[3];
-        anyAlpha = anyAlpha || alphaIn[t] >= 0;
+        anyAlpha_ = anyAlpha_ || alphaIn[t] >= 0;
       }
-      if (anyAlpha) dTriAlphaIn_.upload(alphaIn.data(), alphaIn.size(), s);
+      if (anyAlpha_ || twoLevel) dTriAlphaIn_.upload(alphaIn.data(), alphaIn.size(), s);
     }
+  }
+  if (twoLevel) {
+    for (auto& a : assets_) anyAlpha_ = anyAlpha_ || (a->hasUV && hMats_[a->matId].tex[3] >= 0);
+    if (anyAlpha_)  // every pool needs its opacity-map input
+      for (auto& a : assets_)
+        if (!(a->hasUV && hMats_[a->matId].tex[3] >= 0)) {
+          std::vector<int> al(a->idx.size() / 3, -1);
+          a->dAlphaIn.upload(al.data(), al.size(), s);
+        }
+    for (auto& a : assets_)
+      if (sceneUV && !a->hasUV) {
+        std::vector<float> z(2 * (a->pos.size() / 3), 0.0f);
+        a->dUV.upload(z.data(), z.size(), s);
+      }
+    if (anyAlpha_ && nt > 0 && !dTriAlphaIn_.get()) {
+      std::vector<int> al(nt, -1);
+      dTriAlphaIn_.upload(al.data(), al.size(), s);
+    }
+    upload_assets(s);
+  }
+  if (nt > 0 || twoLevel) {
     rebuild(s);
-    if (anyUV_) view_.triUV = triUV_.get();
-    if (anyAlpha) {
+    if (sceneUV) view_.triUV = triUV_.get();
+    if (anyAlpha_) {
       view_.bvh.alpha.alphaTex = triAlpha_.get();
       view_.bvh.alpha.uv = triUV_.get();
     }
@@ -444,6 +715,8 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   L.mediaRounds = tuning_.media_rounds;
   L.trackBlocks = tuning_.track_blocks;
   L.trackLimit = tuning_.track_limit ? tuning_.track_limit : (uint32_t)kMaxTrackingSteps;
+  // shared-memory top nodes: surface scenes only, within the tree
+  L.topNodes = media_.empty() && view_.hasTris ? std::min(tuning_.top_nodes, bvhNodes_) : 0u;
   L.bound = ctx.bound.get();
   return L;
 }
@@ -553,10 +826,10 @@ RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const 
 void RenderScene::set_tuning(const r2_render_tuning& t) {
   R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31) &&
                  t.media_rounds <= kMaxMediaRounds && t.track_blocks <= 64 &&
-                 t.track_limit <= (uint32_t)kMaxTrackingSteps,
+                 t.track_limit <= (uint32_t)kMaxTrackingSteps && t.top_nodes <= kMaxTopNodes,
              R2_ERR_INVALID_ARGUMENT,
              "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31, media_rounds <= 32, "
-             "track_blocks <= 64, track_limit <= 2^20)");
+             "track_blocks <= 64, track_limit <= 2^20, top_nodes <= 256)");
   tuning_ = t;
 }
 
@@ -591,7 +864,7 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     return best / ((float)S * (float)npix);
   };
   r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths,
-                       kDefaultMediaRounds, 0, saved.track_limit};  // the step bound is kept, never tuned
+                       kDefaultMediaRounds, 0, saved.track_limit, 0};  // the step bound is kept, never tuned
   try {
     R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
     time_wave(cur);  // warm-up
@@ -620,10 +893,12 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     static const uint32_t steps[] = {2, 4, 16, 32};
     static const uint32_t rounds[] = {1, 4, 8, 16};
     static const uint32_t trackBlocks[] = {2, 3, 4, 6};
+    static const uint32_t topNodes[] = {64, 128, 256};
     sweep(&r2_render_tuning::wave_paths, wavePaths, 4);
     if (media_.empty()) {  // the persistent surface traversals run in scenes without media
       sweep(&r2_render_tuning::trav_refill, refills, 4);
       sweep(&r2_render_tuning::trav_visits, visits, 4);
+      sweep(&r2_render_tuning::top_nodes, topNodes, 3);
     } else {
       sweep(&r2_render_tuning::media_rounds, rounds, 4);
       sweep(&r2_render_tuning::track_steps, steps, 4);

@@ -80,6 +80,12 @@ class RenderScene {
   void add_mesh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
                 const r2_material& mat, const float* modelToWorld, uint32_t mask, const float* uv = nullptr,
                 const r2_material_maps* maps = nullptr);
+  // Two-level scenes (the reference's GAS per mesh asset and IAS over scene
+  // objects, scene.cu:188-256): a mesh kept in model space with its own BVH,
+  // placed by any number of instances.  Returns the asset's index.
+  uint32_t add_mesh_asset(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, const float* nrm,
+                          const r2_material& mat, const float* uv = nullptr, const r2_material_maps* maps = nullptr);
+  void add_mesh_instance(uint32_t asset, const float* modelToWorld, uint32_t mask);
   void add_shape(int type, const float* center, float radius, const float* normal, const r2_material& mat,
                  uint32_t mask);
   void set_envmap(const float* rgb, int W, int H);
@@ -93,6 +99,12 @@ class RenderScene {
   // geometry stays on the device.  Same tree as the commit's; allocates
   // nothing after the first build; waits for the build's end.
   void rebuild(cudaStream_t s);
+  // The surface BVH: inner nodes, height and the kernels its last build launched
+  // (BVH builds, shading gathers and, two-level, the node copies).
+  uint32_t bvh_nodes() const { return bvhNodes_; }
+  uint32_t bvh_height() const { return bvhHeight_; }
+  int bvh_build_launches() const { return buildLaunches_; }
+  bool two_level() const { return !meshInstances_.empty(); }
   // Replaces the world-space vertex positions (and normals when given) of the
   // committed scene from host memory, on stream s (the scene's own when null).
   void set_vertices(const float* pos, const float* nrm, uint32_t nverts, cudaStream_t s);
@@ -155,6 +167,36 @@ class RenderScene {
   EnvHost env_;
   DeviceBvh bvh_;
   BvhBuilder builder_;
+  // two-level scenes: mesh assets in model space, their instances, the top
+  // level over the instances' world boxes and the concatenated node and
+  // triangle arrays (top level, then the world-space meshes, then the assets)
+  struct MeshAsset {
+    std::vector<float> pos, nrm, uv;
+    std::vector<uint32_t> idx;
+    uint32_t matId = 0;
+    bool hasUV = false;
+    DBuf<float> dPos, dNrm, dUV;
+    DBuf<uint32_t> dIdx, dTriMat;
+    DBuf<int> dAlphaIn;
+    DeviceBvh bvh;
+  };
+  struct MeshInstanceHost {
+    uint32_t asset;
+    M43 m2w;
+  };
+  std::vector<std::unique_ptr<MeshAsset>> assets_;
+  std::vector<MeshInstanceHost> meshInstances_;
+  DeviceBvh tlas_;
+  DBuf<BvhNode> gNodes_;
+  DBuf<float4> gTris_;
+  DBuf<BvhInstance> dInst_;
+  DBuf<int> dInstCode_;
+  DBuf<float4> dInstO2W_, dInstLo_, dInstHi_;
+  uint32_t bvhNodes_ = 0, bvhHeight_ = 0;
+  int buildLaunches_ = 0;
+  bool anyAlpha_ = false;
+  void upload_assets(cudaStream_t s);
+  void build_two_level(cudaStream_t s);
   // device-resident triangle inputs in scene order (kept for rebuilds)
   DBuf<float> dPos_, dNrm_, dUV_;
   DBuf<uint32_t> dIdx_, dTriMatIn_;
@@ -167,7 +209,7 @@ class RenderScene {
   DBuf<float> envBuf_;
   DBuf<float> hostFrame_;
   SceneView view_;
-  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
+  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
 };
 
 // Frames of several committed scenes rendered by one captured CUDA graph: the

@@ -22,6 +22,19 @@ class RenderParams(C.Structure):
     _fields_ = [("spp", C.c_uint32), ("max_depth", C.c_uint32), ("seed", C.c_uint32), ("flags", C.c_uint32)]
 
 
+BVH_PLOC, BVH_KARRAS = 0, 1
+
+
+def set_bvh_method(method: int):
+    """Hierarchy of the BVHs built from now on, process-wide (r2_set_bvh_method):
+    BVH_PLOC (default) or BVH_KARRAS."""
+    N.check(N.lib.r2_set_bvh_method(int(method)))
+
+
+def bvh_method() -> int:
+    return int(N.lib.r2_get_bvh_method())
+
+
 def camera(width, height, fov_deg=45.0, pos=(0, 0, 3), look_at=(0, 0, 0), up=(0, 1, 0)) -> Camera:
     c = Camera()
     c.width, c.height, c.fov_deg = int(width), int(height), float(fov_deg)
@@ -48,9 +61,9 @@ class Tuning(C.Structure):
     """Launch tuning (r2_render_tuning); 0 fields select the defaults; images never depend on it."""
     _fields_ = [("track_steps", C.c_uint32), ("trav_visits", C.c_uint32), ("trav_refill", C.c_uint32),
                 ("wave_paths", C.c_uint32), ("media_rounds", C.c_uint32), ("track_blocks", C.c_uint32),
-                ("track_limit", C.c_uint32)]
+                ("track_limit", C.c_uint32), ("top_nodes", C.c_uint32)]
     NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths", "media_rounds", "track_blocks",
-             "track_limit")
+             "track_limit", "top_nodes")
 
     def as_tuple(self):
         return tuple(getattr(self, n) for n in self.NAMES)
@@ -60,8 +73,9 @@ class Tuning(C.Structure):
 
 
 def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0, media_rounds=0, track_blocks=0,
-           track_limit=0) -> Tuning:
-    return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds, track_blocks, track_limit)
+           track_limit=0, top_nodes=0) -> Tuning:
+    return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds, track_blocks, track_limit,
+                  top_nodes)
 
 
 class Scene:
@@ -107,6 +121,26 @@ class Scene:
                                                  N.ptr(nrm), N.ptr(uvs), C.byref(material), C.byref(maps), N.ptr(m2w),
                                                  mask))
 
+    def add_mesh_asset(self, mesh, material, uv=None, albedo=None, specular=None, normal=None, alpha=None) -> int:
+        """A mesh kept in model space with its own BVH, placed by add_mesh_instance (r2_scene_add_mesh_asset)."""
+        pos = np.ascontiguousarray(mesh.positions, np.float32)
+        idx = np.ascontiguousarray(mesh.indices, np.uint32)
+        nrm = np.ascontiguousarray(mesh.normals, np.float32)
+        uvs = None if uv is None else np.ascontiguousarray(uv, np.float32)
+        maps = None
+        if uvs is not None:
+            assert uvs.shape == (pos.shape[0], 2)
+            maps = N.MaterialMaps(*[str(p).encode() if p else None for p in (albedo, specular, normal, alpha)])
+        a = C.c_uint32()
+        N.check(N.lib.r2_scene_add_mesh_asset(self.handle, N.ptr(pos), pos.shape[0], N.ptr(idx), idx.shape[0],
+                                              N.ptr(nrm), N.ptr(uvs) if uvs is not None else None, C.byref(material),
+                                              C.byref(maps) if maps is not None else None, C.byref(a)))
+        return a.value
+
+    def add_mesh_instance(self, asset: int, model_to_world=None, mask=255):
+        m2w = np.ascontiguousarray(N.identity43() if model_to_world is None else model_to_world, np.float32)
+        N.check(N.lib.r2_scene_add_mesh_instance(self.handle, int(asset), N.ptr(m2w), mask))
+
     def add_shape(self, kind, center, radius, normal, material, mask=255):
         c = np.ascontiguousarray(center, np.float32)
         n = np.ascontiguousarray(normal, np.float32)
@@ -150,6 +184,12 @@ class Scene:
     def rebuild(self, stream: int = 0):
         """Rebuild the triangle BVH on the device from the resident triangles (waits for the build)."""
         N.check(N.lib.r2_scene_rebuild(self.handle, C.c_void_p(stream or None)))
+
+    def bvh_info(self):
+        """(inner nodes, height, kernels launched by the last build) of the surface BVH."""
+        v = [C.c_uint32() for _ in range(3)]
+        N.check(N.lib.r2_scene_bvh_info(self.handle, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def render_device(self, cam: Camera, prm: RenderParams, d_rgb: int, stream: int = 0, stats=None):
         st = np.zeros(8, np.float64)

@@ -58,6 +58,45 @@ def icosphere_grid_scene():
     return desc, cam
 
 
+def trs43(pos, axis_angle=(0.0, 1.0, 0.0, 0.0), scale=(1.0, 1.0, 1.0)):
+    """T * R * S as 12 floats (glm mat4x3 column order); R rotates by angle
+    (radians) about the axis."""
+    ax = np.asarray(axis_angle[:3], np.float64)
+    ax = ax / np.linalg.norm(ax)
+    a = float(axis_angle[3])
+    K = np.array([[0, -ax[2], ax[1]], [ax[2], 0, -ax[0]], [-ax[1], ax[0], 0]])
+    Rm = np.eye(3) + np.sin(a) * K + (1 - np.cos(a)) * K @ K
+    M = Rm @ np.diag(np.asarray(scale, np.float64))
+    m = np.zeros(12, np.float32)
+    m[0:3], m[3:6], m[6:9] = M[:, 0], M[:, 1], M[:, 2]
+    m[9:12] = pos
+    return m
+
+
+def instanced_scene(n_side: int = 3, width: int = 64, height: int = 64):
+    """Two-level scene: one displaced icosphere (sub 3) placed n_side^2 times
+    with rotations and non-uniform scales (one asset, one material), a second
+    icosphere as a world-space mesh, a ground disc and a lognormal(0, 1.5)
+    environment."""
+    ico = scenes.icosphere(3, 0.08, 7)
+    mat = F.material(diffuse=(0.7, 0.5, 0.3), specular=(1.0, 1.0, 1.0), alpha=0.35, ior=1.5)
+    rng = np.random.default_rng(17)
+    meshes = []
+    for k in range(n_side * n_side):
+        i, j = k % n_side, k // n_side
+        axis = rng.normal(size=3)
+        meshes.append((ico, mat, trs43((-2.2 * (n_side - 1) / 2 + 2.2 * i, -2.2 * (n_side - 1) / 2 + 2.2 * j, 0.0),
+                                       (*axis, float(rng.uniform(0, np.pi))), tuple(rng.uniform(0.6, 1.1, 3)))))
+    other = scenes.icosphere(2, 0.05, 9)
+    meshes.append((other, F.material(diffuse=(0.2, 0.6, 0.8), specular=(0.5, 0.5, 0.5), alpha=0.2, ior=1.5),
+                   trs43((0.0, 0.0, 2.0), scale=(0.7, 0.7, 0.7))))
+    ground = F.material(diffuse=(0.5, 0.5, 0.5), specular=(0.04, 0.04, 0.04), alpha=0.8, ior=1.5)
+    desc = {"meshes": meshes, "shapes": [(R.CIRCLE, (0.0, -3.6, 0.0), 50.0, (0.0, 1.0, 0.0), ground)],
+            "env": lognormal_env(64, 32, 1.5, 4)}
+    cam = R.camera(width, height, 50.0, (0.5, 1.0, 9.0), (0, 0, 0), (0, 1, 0))
+    return desc, cam
+
+
 def volume_scene(work_dir, index: int = 0, grid: int = 256, n_quads: int = 200_000, ico_subdiv: int = 6,
                  width: int = 1920, height: int = 1080, filter_spv: int = 64, filter_iters: int = 10):
     """Batched-volume scene `index` (seed 5 + index): a foliage grid filtered on the GPU
@@ -103,12 +142,37 @@ def world_vertices(desc):
     return np.ascontiguousarray(np.concatenate(P)), np.ascontiguousarray(np.concatenate(Nn))
 
 
-def build_scene(desc) -> R.Scene:
+def mesh_groups(desc):
+    """Indices of desc["meshes"] entries that share one mesh object and one
+    material object (instances of one asset), for the groups of two or more."""
+    groups = {}
+    for k, entry in enumerate(desc.get("meshes", [])):
+        groups.setdefault((id(entry[0]), id(entry[1])), []).append(k)
+    return [g for g in groups.values() if len(g) > 1]
+
+
+def build_scene(desc, instancing: bool = True) -> R.Scene:
+    """The scene of a description; with instancing, meshes that share their mesh
+    and material objects become one asset with an instance each (two-level BVH)."""
     sc = R.Scene()
-    for entry in desc.get("meshes", []):
+    grouped = {}
+    if instancing:
+        for g in mesh_groups(desc):
+            for k in g:
+                grouped[k] = g[0]
+    assets = {}
+    for k, entry in enumerate(desc.get("meshes", [])):
         mesh, mat, m2w = entry[:3]
         tex = entry[3] if len(entry) > 3 else None
-        if tex is None:
+        if k in grouped:
+            first = grouped[k]
+            if first not in assets:
+                t = tex or {}
+                assets[first] = sc.add_mesh_asset(mesh, mat, uv=t.get("uv"), albedo=t.get("albedo"),
+                                                  specular=t.get("specular"), normal=t.get("normal"),
+                                                  alpha=t.get("alpha"))
+            sc.add_mesh_instance(assets[first], m2w)
+        elif tex is None:
             sc.add_mesh(mesh, mat, m2w)
         else:
             sc.add_mesh_textured(mesh, mat, tex["uv"], m2w, albedo=tex.get("albedo"), specular=tex.get("specular"),

@@ -169,7 +169,7 @@ class OMesh(C.Structure):
     _fields_ = [("positions", C.c_void_p), ("nverts", C.c_uint32), ("indices", C.c_void_p), ("ntris", C.c_uint32),
                 ("normals", C.c_void_p), ("model_to_world", C.c_float * 12), ("material", Material),
                 ("uvs", C.c_void_p), ("albedo", C.c_void_p), ("specular", C.c_void_p), ("normal", C.c_void_p),
-                ("alpha", C.c_void_p)]
+                ("alpha", C.c_void_p), ("asset", C.c_uint32)]
 
 
 class OShape(C.Structure):
@@ -197,11 +197,19 @@ lib.orc_env_sample.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_floa
 lib.orc_env_le.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
 
 
-def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want_var=False, flags=0):
+def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want_var=False, flags=0,
+           instancing=True):
     """scene_desc: dict(meshes=[(Mesh, native material, m2w)], shapes=[(kind, center, radius, normal, material)],
     media=[(path, sigma_a, sigma_s, pos, orientation, scaling)], env=(H, W, 3) float32).
-    Returns rgb (n, 3) [, var (n, 3)] for pixels [p0, p1)."""
+    With instancing, meshes sharing their mesh and material objects are instances of one asset, as the
+    library's scene builder makes them.  Returns rgb (n, 3) [, var (n, 3)] for pixels [p0, p1)."""
     keep = []
+    asset_of = {}
+    if instancing:
+        from renderer2_b200 import render_scenes as RS
+        for a, group in enumerate(RS.mesh_groups(scene_desc)):
+            for k in group:
+                asset_of[k] = a + 1
     media = (OMedium * max(1, len(scene_desc.get("media", []))))()
     for i, med in enumerate(scene_desc.get("media", [])):
         path, sa, ss, pos, ori, sc = med[:6]
@@ -242,6 +250,7 @@ def render(scene_desc, cam, spp, max_depth, seed, p0=0, p1=None, threads=0, want
         meshes[i].normals = nrm.ctypes.data
         meshes[i].model_to_world[:] = [float(x) for x in np.asarray(m2w, np.float32)]
         meshes[i].material = material_from(mat)
+        meshes[i].asset = asset_of.get(i, 0)
     shapes = (OShape * max(1, len(scene_desc.get("shapes", []))))()
     for i, (kind, c, r, n, mat) in enumerate(scene_desc.get("shapes", [])):
         shapes[i].type = kind

@@ -98,8 +98,18 @@ def _oracle(mesh, mat, prm, g, m2w=I43):
     return O.filter_voxels(mesh, O.material_from(mat), m2w, O.grid_from(g), O.params_from(prm))
 
 
+@pytest.fixture(params=[0, 1], ids=["ploc", "karras"])
+def bvh_method(request):
+    """Both hierarchies of the builder, on the GPU and in the oracle."""
+    N.check(N.lib.r2_set_bvh_method(request.param))
+    O.lib.orc_set_bvh_method(request.param)
+    yield request.param
+    N.check(N.lib.r2_set_bvh_method(0))
+    O.lib.orc_set_bvh_method(0)
+
+
 @pytest.mark.parametrize("mesh_kind", ["ico4", "foliage", "foliage_big", "single", "pair", "dupes"])
-def test_bvh_bit_exact(mesh_kind):
+def test_bvh_bit_exact(mesh_kind, bvh_method):
     if mesh_kind == "ico4":
         mesh = scenes.icosphere(4, 0.05, 1)
     elif mesh_kind == "foliage":

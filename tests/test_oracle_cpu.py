@@ -76,8 +76,15 @@ def _brute(pos, idx, o, d, tmax, tris, order):
     return best
 
 
-@pytest.mark.parametrize("n", [1, 2, 7, 64])
-def test_oracle_bvh_matches_brute_force(n):
+@pytest.fixture(params=[0, 1], ids=["ploc", "karras"])
+def bvh_method(request):
+    O.lib.orc_set_bvh_method(request.param)
+    yield request.param
+    O.lib.orc_set_bvh_method(0)
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 64, 600])
+def test_oracle_bvh_matches_brute_force(n, bvh_method):
     pos, idx = _random_mesh(n, n)
     nodes, order, tris, h = O.build_bvh(pos, idx)
     assert h >= 1
@@ -93,6 +100,75 @@ def test_oracle_bvh_matches_brute_force(n):
             assert tri == -1
         else:
             assert tri == bi and t == bt
+
+
+def _sah_cost(nodes):
+    """SAH cost of a node array (inner 1.2, triangle 1.0, areas relative to the root's)."""
+    f = nodes.view(np.float32).astype(np.float64)
+
+    def area(lx, hx, ly, hy, lz, hz):
+        dx, dy, dz = hx - lx, hy - ly, hz - lz
+        return dx * dy + dy * dz + dz * dx
+    a0 = area(f[:, 0], f[:, 1], f[:, 2], f[:, 3], f[:, 8], f[:, 9])
+    a1 = area(f[:, 4], f[:, 5], f[:, 6], f[:, 7], f[:, 10], f[:, 11])
+    b = f[0]
+    root = area(min(b[0], b[4]), max(b[1], b[5]), min(b[2], b[6]), max(b[3], b[7]), min(b[8], b[10]),
+                max(b[9], b[11]))
+    cost = 1.2
+    for a, ch in ((a0, nodes[:, 12]), (a1, nodes[:, 13])):
+        inner = ch >= 0
+        leaf = (ch < 0) & (ch != np.int32(-2 ** 31))
+        cnt = ((~ch.astype(np.int64)) >> 26) & 31
+        cost += (1.2 * a[inner]).sum() / root + (cnt[leaf] * a[leaf]).sum() / root
+    return cost
+
+
+def test_ploc_tree_structure_and_quality():
+    """PLOC over the 8x8 icosphere grid (327,680 triangles): every triangle in
+    exactly one leaf, every child box inside its parent's, parents numbered
+    below their children, and a lower SAH cost than the Karras tree."""
+    from renderer2_b200 import render_scenes as RS
+    desc, _ = RS.icosphere_grid_scene()
+    pos, _ = RS.world_vertices(desc)
+    idx, base = [], 0
+    for m, _, _ in desc["meshes"]:
+        idx.append(m.indices.astype(np.uint32) + np.uint32(base))
+        base += m.positions.shape[0]
+    idx = np.concatenate(idx)
+    cost = {}
+    for meth in (1, 0):
+        O.lib.orc_set_bvh_method(meth)
+        nodes, order, _, h = O.build_bvh(pos, idx)
+        cost[meth] = _sah_cost(nodes)
+    O.lib.orc_set_bvh_method(0)
+    n = idx.shape[0]
+    assert np.array_equal(np.sort(order), np.arange(n))
+    covered = np.zeros(n, np.int32)
+    f = nodes.view(np.float32)
+    reach = np.zeros(nodes.shape[0], bool)  # inner nodes reachable from the root (not inside collapsed leaves)
+    reach[0] = True
+    for i in range(nodes.shape[0]):  # parents have smaller indices than their children
+        if reach[i]:
+            for c in range(2):
+                ch = int(nodes[i, 12 + c])
+                if ch >= 0:
+                    reach[ch] = True
+                elif ch != -2 ** 31:
+                    a, k = (~ch) & 0x03FFFFFF, ((~ch) >> 26) & 31
+                    covered[a:a + k] += 1
+    for c in range(2):
+        ch = nodes[:, 12 + c]
+        inner = np.flatnonzero(ch >= 0)
+        kids = ch[inner]
+        assert np.all(nodes[kids, 14] == inner) and np.all(kids > inner)
+        lo = f[inner][:, [0, 2, 8]] if c == 0 else f[inner][:, [4, 6, 10]]
+        hi = f[inner][:, [1, 3, 9]] if c == 0 else f[inner][:, [5, 7, 11]]
+        klo = np.minimum(f[kids][:, [0, 2, 8]], f[kids][:, [4, 6, 10]])
+        khi = np.maximum(f[kids][:, [1, 3, 9]], f[kids][:, [5, 7, 11]])
+        assert np.all(klo >= lo) and np.all(khi <= hi)
+    assert np.all(covered == 1)
+    print(f"SAH cost: PLOC {cost[0]:.2f}, Karras {cost[1]:.2f}")
+    assert cost[0] < 0.85 * cost[1]
 
 
 def test_build_s_eigenvalues_via_oracle_filter_math():
