@@ -63,7 +63,13 @@ VOLUME_BATCH_CFG = dict(scenes=16, grids=(128, 192, 256, 384, 512, 160, 224, 320
                         quads=(50_000, 150_000, 300_000), ico=(6, 7), width=1920, height=1080, spp=4, depth=16,
                         frame_spp=256)
 SMALL_CFG = dict(grid=32, spv=64, iters=10, width=256, height=256, spp=16, depth=8)
-SERVE_CFG = dict(jobs=60, rate=40.0, slots=4, budget=40 << 30)
+SERVE_CFG = dict(jobs=60, rate=40.0, slots=4, budget=40 << 30, sizes=((256, 256), (384, 384), (512, 512), (1280, 720)),
+                 spp=(4, 64), grids=(64, 96, 128, 192), quads=(10_000, 40_000, 100_000))
+# the serving configuration's own mix (Poisson 20 req/s, 70 % renders 256^2..1920x1080 at spp log-uniform in
+# [16, 1024], 30 % filters 64^3..512^3 over 20k..1M triangles, 150 GB budget), 30 jobs: `--case serving-stated`
+SERVE_CFG_STATED = dict(jobs=30, rate=20.0, slots=6, budget=150 << 30,
+                        sizes=((256, 256), (512, 512), (1280, 720), (1920, 1080)), spp=(16, 1024),
+                        grids=(64, 128, 256, 512), quads=(10_000, 100_000, 500_000))
 # forest leg: the forest generator's disc (radius 1000, 100,000 placement attempts) of three synthetic tree
 # models, each filtered into 4 LODs; LODs chosen on the GPU for the generator's camera at 1920x1080
 FOREST_CFG = dict(n_quads=20_000, grid=64, lods=4, attempts=100_000, radius=1000.0, width=1920, height=1080,
@@ -222,27 +228,147 @@ def _input_bytes(desc):
 # ------------------------------------------------------------------ CPU baselines (oracle port)
 
 def cpu_render_sample(desc, cam, prm, budget_s=15.0, threads=0):
-    """Oracle paths/s on full-spp row bands at the frame centre."""
+    """Oracle paths/s on full-spp row bands at the frame centre; the oracle builds the scene's BVH in every call,
+    so the time of a call over no pixels (the BVH build, done once per frame) is taken off each band."""
     import oracle_lib as O
     cores = threads or os.cpu_count() or 1
     W, H = cam.width, cam.height
+    t0 = time.perf_counter()
+    O.render(desc, cam, prm.spp, prm.max_depth, prm.seed, 0, 0, threads=cores, flags=prm.flags)
+    t_build = time.perf_counter() - t0
     row = H // 2
     rows, done, t_work = 2, 0, 0.0
     while True:
         p0, p1 = row * W, min((row + rows) * W, W * H)
         t0 = time.perf_counter()
         O.render(desc, cam, prm.spp, prm.max_depth, prm.seed, p0, p1, threads=cores, flags=prm.flags)
-        t_work += time.perf_counter() - t0
+        t_work += max(1e-6, time.perf_counter() - t0 - t_build)
         done += (p1 - p0)
         row += rows
         if t_work >= budget_s or row >= H:
             break
         rate = done / t_work
-        rows = max(1, min(int((budget_s - t_work) * rate / W), H - row))
+        rows = max(1, min(int((budget_s - t_work) * rate / W), 4 * rows, H - row))
     paths = done * prm.spp
     return {"value": paths / t_work, "unit": "paths/s", "cores": cores, "kind": "port", "seconds": t_work,
+            "bvh_build_s": t_build,
             "sample": f"{done // W} rows x {W} px x {prm.spp} spp at the frame centre ({paths} paths), "
-                      f"BVH build included per call"}
+                      f"the BVH build ({t_build:.2f} s, once per frame) taken off each band"}
+
+
+def ref_code_render_sample(desc, cam, prm, budget_s=10.0, threads=0):
+    """The reference's own CPathIntegrator::Li, compiled for the host (oracle/_ref/libr2ref.so, built from the
+    reference's sources; the scene's closest hits come from the oracle's BVH and the environment from the
+    oracle's map), timed on full-spp row bands at the frame centre.  Its bounce cap is its own 50 (Russian
+    roulette from bounce 4), not the configuration's depth.  None when the library was not built."""
+    import ctypes as C
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref", "libr2ref.so")
+    if not os.path.exists(path) or desc.get("media") or desc.get("shapes"):
+        return None
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.ref_render_scene.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, C.c_uint32, P, P, P, C.c_int, C.c_int]
+    lib.ref_render_paths.argtypes = [C.c_uint32, C.c_uint32, C.c_float, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                     C.c_uint32, P, C.c_int]
+    from renderer2_b200 import render_scenes as RS
+    wpos, _ = RS.world_vertices(desc)
+    nrm, idx, tobj, m2w, mats = [], [], [], [], []
+    base = 0
+    for o, entry in enumerate(desc["meshes"]):
+        mesh, mat, t = entry[:3]
+        nrm.append(np.asarray(mesh.normals, np.float32))
+        idx.append(np.asarray(mesh.indices, np.uint32) + np.uint32(base))
+        tobj.append(np.full(mesh.indices.shape[0], o, np.uint32))
+        m2w.append(np.asarray(t, np.float32))
+        mats.append(np.array([*mat.diffuse, *mat.specular, mat.alpha_x, mat.eta_t], np.float32))
+        base += mesh.positions.shape[0]
+    arrs = [np.ascontiguousarray(a) for a in (wpos, np.concatenate(nrm), np.concatenate(idx), np.concatenate(tobj),
+                                              np.concatenate(m2w), np.concatenate(mats))]
+    wp, nr, ix, to, mw, ma = arrs
+    env = np.ascontiguousarray(desc["env"], np.float32)
+    assert lib.ref_render_scene(wp.ctypes.data, wp.shape[0], ix.ctypes.data, ix.shape[0], nr.ctypes.data,
+                                to.ctypes.data, len(desc["meshes"]), mw.ctypes.data, ma.ctypes.data, env.ctypes.data,
+                                env.shape[1], env.shape[0]) >= 0
+    cores = threads or os.cpu_count() or 1
+    W, H = cam.width, cam.height
+    f3 = lambda v: np.ascontiguousarray(v, np.float32)  # noqa: E731
+    pos, look, up = f3(cam.pos[:]), f3(cam.look_at[:]), f3(cam.up[:])
+    row, rows, done, t_work = H // 2, 2, 0, 0.0
+    while True:
+        p0, p1 = row * W, min((row + rows) * W, W * H)
+        out = np.zeros((p1 - p0, 3), np.float32)
+        t0 = time.perf_counter()
+        assert lib.ref_render_paths(W, H, cam.fov_deg, pos.ctypes.data, look.ctypes.data, up.ctypes.data, prm.spp,
+                                    prm.seed, p0, p1, out.ctypes.data, cores) == 0
+        t_work += time.perf_counter() - t0
+        done += p1 - p0
+        row += rows
+        if t_work >= budget_s or row >= H:
+            break
+        rows = max(1, min(int((budget_s - t_work) * done / t_work / W), 4 * rows, H - row))
+    paths = done * prm.spp
+    return {"value": paths / t_work, "unit": "paths/s", "cores": cores, "kind": "reference", "seconds": t_work,
+            "sample": f"{done // W} rows x {W} px x {prm.spp} spp at the frame centre ({paths} paths) through the "
+                      "reference's CPathIntegrator::Li compiled for the host (bounce cap 50, its own)"}
+
+
+def ref_code_filter_sample(mesh, mat, prm, vs, budget_s=10.0, threads=0):
+    """The reference's own CMeshFilter::run with estimateDensity, compiled for the host (oracle/_ref/libr2ref.so;
+    closest hits from the oracle's BVH), on contiguous z-slices at the grid centre.  None when not built."""
+    import ctypes as C
+    import oracle_lib as O
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle", "_ref", "libr2ref.so")
+    if not os.path.exists(path) or prm.samples_per_voxel > 1000:
+        return None
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    lib.ref_filter_scene.argtypes = [P, C.c_uint32, P, C.c_uint32, P, P, P, P, C.c_float, C.c_float]
+    lib.ref_filter_voxels.argtypes = [P, P, P, P, P, P, P, C.c_float, C.c_uint32, C.c_float, C.c_int, C.c_uint32,
+                                      C.c_uint32, C.c_uint64, C.c_uint64, P, C.c_int]
+    m2w = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0], np.float32)
+    pos = np.ascontiguousarray(mesh.positions, np.float32)
+    idx = np.ascontiguousarray(mesh.indices, np.uint32)
+    nrm = np.ascontiguousarray(mesh.normals, np.float32)
+    kd = np.ascontiguousarray(mat.diffuse[:], np.float32)
+    ks = np.ascontiguousarray(mat.specular[:], np.float32)
+    t0 = time.perf_counter()
+    assert lib.ref_filter_scene(pos.ctypes.data, pos.shape[0], idx.ctypes.data, idx.shape[0], nrm.ctypes.data,
+                                m2w.ctypes.data, kd.ctypes.data, ks.ctypes.data, mat.alpha_x, mat.eta_t) >= 0
+    t_build = time.perf_counter() - t0
+    g = O.setup_grid(pos.min(0), pos.max(0), m2w, vs)
+    nx, ny, nz = g.num_voxels[:]
+    mats = [np.ascontiguousarray(list(getattr(g, k)), np.float32)
+            for k in ("index_to_model", "model_to_index", "model_to_world", "world_to_model")]
+    nv = np.array([nx, ny, nz], np.int32)
+    bbmin = np.ascontiguousarray(list(g.world_bb_min), np.float32)
+    bbmax = np.ascontiguousarray(list(g.world_bb_max), np.float32)
+    cores = threads or os.cpu_count() or 1
+    slab = nx * ny
+    z, done, t_work, nsl = nz // 2, 0, 0.0, 1
+    while True:
+        v0, v1 = z * slab, min((z + nsl) * slab, nx * ny * nz)
+        out = np.zeros((v1 - v0, 32), np.uint8)
+        t0 = time.perf_counter()
+        assert lib.ref_filter_voxels(*[a.ctypes.data for a in mats], nv.ctypes.data, bbmin.ctypes.data,
+                                     bbmax.ctypes.data, prm.sigma_t, prm.estimation_iterations, prm.alpha,
+                                     int(prm.clip_rays), prm.samples_per_voxel, prm.seed, v0, v1, out.ctypes.data,
+                                     cores) == 0
+        t_work += time.perf_counter() - t0
+        done += v1 - v0
+        z += nsl
+        if t_work >= budget_s or z >= nz:
+            break
+        nsl = max(1, min(int((budget_s - t_work) * (done / t_work) / slab), 4 * nsl, nz - z))
+    return {"value": done / t_work, "unit": "voxels/s", "cores": cores, "kind": "reference", "seconds": t_work,
+            "sample": f"{done // slab} z-slices of {nx}x{ny} at the grid centre, {prm.samples_per_voxel} spv, through "
+                      f"the reference's CMeshFilter::run compiled for the host (BVH build {t_build:.2f}s excluded)"}
+
+
+def cpu_render_baseline(desc, cam, prm, budget_s=15.0):
+    """The CPU baseline of a render: the reference's own integrator compiled for the host where it was built
+    (surface scenes), else the oracle port."""
+    r = ref_code_render_sample(desc, cam, prm, budget_s=budget_s)
+    return r if r is not None else cpu_render_sample(desc, cam, prm, budget_s=budget_s)
 
 
 def cpu_filter_sample(mesh, mat, prm, vs, budget_s=15.0, threads=0, keep=None):
@@ -933,29 +1059,30 @@ def bench_volume_batch(args, world, local):
             "gpu_launches": c["spp"] * c["scenes"] * (3 + _media_launches(tuned.as_dict()) * c["depth"]) * args.steps}
 
 
-def serving_jobs(seed=11):
-    """The serving mix scaled to a bench step: 60 jobs, Poisson arrivals at SERVE_CFG['rate'] per second;
-    70% renders (256^2 .. 1280x720, spp log-uniform in [4, 64], depth 8, on the small icosphere and
-    the icosphere-grid scenes), 30% filter jobs (64^3 .. 192^3 over foliage of 20k .. 200k triangles, 64 spv,
-    10 iterations)."""
+def serving_jobs(c=SERVE_CFG, seed=11):
+    """A serving mix: c['jobs'] jobs, Poisson arrivals at c['rate'] per second; 70% renders (sizes c['sizes'],
+    spp log-uniform in c['spp'], depth 8, on the small icosphere and the icosphere-grid scenes), 30% filter
+    jobs (grids c['grids'] over foliage of c['quads'] leaf quads, 64 spv, 10 iterations).  SERVE_CFG is the
+    mix scaled to a bench step (256^2 .. 1280x720, spp 4 .. 64, 64^3 .. 192^3, 20k .. 200k triangles)."""
     rng = np.random.default_rng(seed)
-    c = SERVE_CFG
     t = 0.0
     jobs = []
-    sizes = [(256, 256), (384, 384), (512, 512), (1280, 720)]
+    sizes = list(c["sizes"])
+    lo, hi = c["spp"]
     for k in range(c["jobs"]):
         t += float(rng.exponential(1.0 / c["rate"]))
         if rng.uniform() < 0.7:
             w, h = sizes[int(rng.integers(len(sizes)))]
-            spp = int(round(np.exp(rng.uniform(np.log(4), np.log(64)))))
+            spp = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
             jobs.append(("render", t, int(rng.integers(2)), w, h, spp, int(rng.integers(1 << 30))))
         else:
-            jobs.append(("filter", t, int(rng.integers(3)), int(rng.choice([64, 96, 128, 192])), int(rng.integers(1 << 30))))
+            jobs.append(("filter", t, int(rng.integers(len(c["quads"]))), int(rng.choice(list(c["grids"]))),
+                         int(rng.integers(1 << 30))))
     return jobs
 
 
-def bench_serving(args):
-    """Served (request loop, SERVE_CFG['slots'] slots) against one job at a time on the same GPU."""
+def bench_serving(args, c=SERVE_CFG):
+    """Served (request loop, c['slots'] slots) against one job at a time on the same GPU."""
     import threading as th
 
     import torch
@@ -964,15 +1091,14 @@ def bench_serving(args):
     from renderer2_b200 import render_scenes as RS
     from renderer2_b200 import scenes
     from renderer2_b200 import serving as S
-    c = SERVE_CFG
     d1, _ = RS.icosphere_scene()
     d2, _ = RS.icosphere_grid_scene()
     rscenes = [RS.build_scene(d1), RS.build_scene(d2)]
     cams = [((0, 0, 3), (0, 0, 0)), ((0, 0, 24), (0, 0, 0))]
     fmat = F.material(diffuse=(0.1, 0.6, 0.1), specular=(0.04, 0.04, 0.04), alpha=0.5, ior=1.5)
-    meshes = [scenes.foliage(n, 10, 0.7, 20 + i) for i, n in enumerate((10_000, 40_000, 100_000))]
+    meshes = [scenes.foliage(n, 10, 0.7, 20 + i) for i, n in enumerate(c["quads"])]
     fscenes = [F.FilterScene(m, fmat) for m in meshes]
-    jobs = serving_jobs()
+    jobs = serving_jobs(c)
 
     def spec(j):
         if j[0] == "render":
@@ -1083,9 +1209,11 @@ def bench_serving(args):
         return float(np.percentile(a, q))
 
     return {"metric": "served paths/s & filtered voxels/s", "unit": "paths/s, voxels/s",
-            "config": {"workload": f"{len(jobs)} jobs, Poisson arrivals at {c['rate']}/s: 70% renders (256^2..1280x720, "
-                                   "spp log-uniform 4..64, depth 8, icosphere / icosphere-grid scenes), 30% filters "
-                                   "(64^3..192^3, foliage 10k..100k quads, 64 spv, 10 iterations)",
+            "config": {"workload": f"{len(jobs)} jobs, Poisson arrivals at {c['rate']}/s: 70% renders "
+                                   f"({c['sizes'][0][0]}x{c['sizes'][0][1]}..{c['sizes'][-1][0]}x{c['sizes'][-1][1]}, "
+                                   f"spp log-uniform {c['spp'][0]}..{c['spp'][1]}, depth 8, icosphere / icosphere-grid "
+                                   f"scenes), 30% filters ({c['grids'][0]}^3..{c['grids'][-1]}^3, foliage "
+                                   f"{c['quads'][0]}..{c['quads'][-1]} quads, 64 spv, 10 iterations)",
                        "slots": c["slots"], "hbm_budget_bytes": c["budget"], "paths": paths, "voxels": voxels},
             "served": {"paths_per_s": paths / span_srv, "voxels_per_s": voxels / span_srv, "makespan_s": span_srv,
                        "p50_latency_s": pct(lat_srv, 50), "p99_latency_s": pct(lat_srv, 99)},
@@ -1145,7 +1273,7 @@ def run_native(args):
     forest = bench_forest(args, world, local) if not args.skip_volume else None
     serve = bench_serving(args) if (not args.skip_serving and world == 1) else None
     if rank == 0:
-        cpu = cpu_render_sample(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
+        cpu = cpu_render_baseline(r["desc"], r["cam"], r["prm"], budget_s=args.cpu_budget) if world == 1 else None
         line = {"metric": "paths/s", "value": r["value"], "unit": "paths/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
@@ -1247,12 +1375,14 @@ def run_reference(args):
         return
     desc, cam, prm = render_workload()
     for _ in range(args.warmup):
-        cpu_render_sample(desc, cam, prm, budget_s=1.0)
-    vals = [cpu_render_sample(desc, cam, prm, budget_s=args.cpu_budget / max(1, args.steps))
+        cpu_render_baseline(desc, cam, prm, budget_s=1.0)
+    vals = [cpu_render_baseline(desc, cam, prm, budget_s=args.cpu_budget / max(1, args.steps))
             for _ in range(args.steps)]
     v = float(np.median([x["value"] for x in vals]))
     cpu = dict(vals[-1])
     cpu["value"] = v
+    # beside it: the oracle port at the configuration's depth (the reference integrator's bounce cap is its own)
+    port = cpu_render_sample(desc, cam, prm, budget_s=max(3.0, args.cpu_budget / 2)) if cpu["kind"] != "port" else None
     line = {"impl": "reference", "metric": "paths/s", "value": v, "unit": "paths/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * float(np.mean([x["seconds"] for x in vals])),  # a bounded sample per step
@@ -1260,12 +1390,18 @@ def run_reference(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
             "config": headline_config(world),
             "cpu_baseline": cpu,
-            "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "oracle_port": port}
     if not args.skip_filter:
         mesh, mat, fprm, vs = filter_workload()
-        fc = cpu_filter_sample(mesh, mat, fprm, vs, budget_s=max(5.0, args.cpu_budget / 2))
-        line["filter"] = {"metric": "filtered voxels/s", "value": fc["value"], "unit": "voxels/s", "cpu_baseline": fc}
-    # the CPU arm runs the oracle alone: the GPU library must not be in this process
+        budget = max(5.0, args.cpu_budget / 2)
+        fc = ref_code_filter_sample(mesh, mat, fprm, vs, budget_s=budget)
+        fport = cpu_filter_sample(mesh, mat, fprm, vs, budget_s=budget)
+        if fc is None:
+            fc, fport = fport, None
+        line["filter"] = {"metric": "filtered voxels/s", "value": fc["value"], "unit": "voxels/s", "cpu_baseline": fc,
+                          "oracle_port": fport}
+    # the CPU arm runs the oracle (and the host-compiled reference) alone: the GPU library must not be in this process
     with open("/proc/self/maps") as fh:
         assert "librenderer2" not in fh.read(), "the reference arm loaded the GPU library"
     line["native_libraries"] = "oracle only"
@@ -1318,6 +1454,9 @@ def run_case(args):
     elif args.case == "serving":
         import renderer2_b200  # noqa: F401
         print(json.dumps(bench_serving(args)))
+    elif args.case == "serving-stated":  # the serving configuration's own mix and sizes
+        import renderer2_b200  # noqa: F401
+        print(json.dumps(bench_serving(args, SERVE_CFG_STATED)))
     elif args.case == "volume-batch":
         import renderer2_b200  # noqa: F401
         args.steps, args.warmup = 1, 1
@@ -1365,7 +1504,7 @@ def main():
     ap.add_argument("--skip-512", action="store_true", help="skip the 512^3 filter leg")
     ap.add_argument("--case", default=None,
                     help="profiling case: render-wave | filter-small | volume-small | volume-mid | volume-batch | forest | "
-                         "forest-small | serving")
+                         "forest-small | serving | serving-stated")
     ap.add_argument("--case-spp", type=int, default=1, help="render-wave: samples per pixel, all in one wave")
     args = ap.parse_args()
     if args.case:

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "r2_host_texfetch.h"
@@ -56,9 +57,39 @@ CMaterial::~CMaterial() {}
 }  // namespace rt
 
 namespace r2ref {
-static std::vector<float> g_queue;
-static size_t g_pos = 0;
-float next_curand() { return g_pos < g_queue.size() ? g_queue[g_pos++] : 0.5f; }
+// Draws of the current thread: the queued cuRAND values first; then, when a
+// generator is started (timing runs), Philox4x32-10 words keyed by the path
+// mapped to (0, 1] as curand_uniform's range; else 0.5.
+struct DrawGen {
+  uint32_t key[2], ctr[4], buf[4];
+  int left;
+  bool on;
+};
+static thread_local std::vector<float> g_queue;
+static thread_local size_t g_pos = 0;
+static thread_local DrawGen g_gen = {};
+float next_curand() {
+  if (g_pos < g_queue.size()) return g_queue[g_pos++];
+  if (g_gen.on) {
+    if (g_gen.left == 0) {
+      orc_philox4x32_10(g_gen.ctr, g_gen.key, g_gen.buf);
+      ++g_gen.ctr[1];
+      g_gen.left = 4;
+    }
+    const uint32_t w = g_gen.buf[4 - g_gen.left--];
+    return (float)((w >> 8) + 1u) * (1.0f / 16777216.0f);
+  }
+  return 0.5f;
+}
+static void gen_start(uint32_t a, uint32_t b, uint32_t c) {
+  g_queue.clear();
+  g_pos = 0;
+  g_gen = DrawGen{};
+  g_gen.on = true;
+  g_gen.key[0] = a;
+  g_gen.key[1] = b;
+  g_gen.ctr[0] = c;
+}
 
 // Scene of the CDeviceScene shim: the oracle's BVH over world-space
 // triangles, model-space vertex normals, per triangle its object (transform)
@@ -71,6 +102,7 @@ struct HookScene {
   std::vector<std::unique_ptr<rt::CMaterial>> mats;  // per object
   std::vector<float> env;
   int envW = 0, envH = 0;
+  void* envH_ = nullptr;  // the oracle's environment map with its distributions, built once
   unsigned int mask = 0;  // visibility of the objects (ESceneobjectMask)
   bool ready = false;
 };
@@ -106,7 +138,7 @@ void scene_intersect(const rt::CRay& ray, rt::SInteraction* si, unsigned int mas
 
 glm::vec3 scene_sample_light(float u0, float u1, glm::vec3* dir, float* pdf) {
   float d[3], le[3];
-  orc_env_sample(g_fs.env.data(), g_fs.envW, g_fs.envH, u0, u1, d, pdf, le);
+  orc_env_sample_h(g_fs.envH_, u0, u1, d, pdf, le);
   *dir = glm::vec3(d[0], d[1], d[2]);
   return glm::vec3(le[0], le[1], le[2]);
 }
@@ -114,7 +146,7 @@ glm::vec3 scene_sample_light(float u0, float u1, glm::vec3* dir, float* pdf) {
 glm::vec3 scene_le(const glm::vec3& dir, float* pdf) {
   const float d[3] = {dir.x, dir.y, dir.z};
   float le[3];
-  orc_env_le(g_fs.env.data(), g_fs.envW, g_fs.envH, d, pdf, le);
+  orc_env_le_h(g_fs.envH_, d, pdf, le);
   return glm::vec3(le[0], le[1], le[2]);
 }
 }  // namespace r2ref
@@ -128,6 +160,7 @@ glm::vec3 rt::CDeviceScene::sampleLightSources(CSampler& sampler, glm::vec3* dir
 static void feed(const float* c, int n) {
   r2ref::g_queue.assign(c, c + n);
   r2ref::g_pos = 0;
+  r2ref::g_gen.on = false;
 }
 static glm::vec3 V(const float* p) { return glm::vec3(p[0], p[1], p[2]); }
 static void put(float* o, const glm::vec3& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; }
@@ -343,6 +376,40 @@ int ref_filter_scene(const float* wpos, uint32_t nverts, const uint32_t* idx, ui
   return h;
 }
 
+// Timing run of the reference's filter on the scene of ref_filter_scene:
+// CMeshFilter::run for voxels [v0, v1) (ids x + y*nx + z*nx*ny) of the grid,
+// draws from a Philox generator per voxel (voxel, seed), `threads` host
+// threads taking every threads-th voxel; out32: the payloads.
+int ref_filter_voxels(const float* i2m, const float* m2i, const float* m2w, const float* w2m, const int32_t* nv,
+                      const float* bbmin, const float* bbmax, float sigma_t, uint32_t iters, float alpha, int clip,
+                      uint32_t spv, uint32_t seed, uint64_t v0, uint64_t v1, unsigned char* out32, int threads) {
+  if (!r2ref::g_fs.ready || v1 <= v0 || spv > 1000) return -1;
+  if (threads < 1) threads = 1;
+  const glm::mat4x3 indexToModel = M43(i2m), modelToIndex = M43(m2i), modelToWorld = M43(m2w),
+                    worldToModel = M43(w2m);
+  const glm::ivec3 numVoxels(nv[0], nv[1], nv[2]);
+  const rt::SAABB bb{V(bbmin), V(bbmax)};
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([=, &bb]() {
+      for (uint64_t v = v0 + (uint64_t)t; v < v1; v += (uint64_t)threads) {
+        const glm::ivec3 cv((int)(v % (uint64_t)nv[0]), (int)((v / (uint64_t)nv[0]) % (uint64_t)nv[1]),
+                            (int)(v / ((uint64_t)nv[0] * (uint64_t)nv[1])));
+        r2ref::gen_start((uint32_t)v, seed, 0u);
+        rt::CSampler sampler;
+        filter::CMeshFilter f(cv, indexToModel, modelToIndex, modelToWorld, worldToModel, numVoxels, bb, sampler,
+                              sigma_t, iters, alpha, clip != 0, 1.0f);
+        rt::CDeviceScene scene;
+        const filter::SFilteredDataCompact out = f.run(scene, spv);
+        std::memcpy(out32 + 32 * (size_t)(v - v0), &out, 32);
+      }
+      r2ref::g_gen.on = false;
+    });
+  }
+  for (auto& th : pool) th.join();
+  return 0;
+}
+
 // Render scene of ref_path_li: world-space vertices and indices of all
 // meshes, model-space vertex normals, the object of each triangle, per object
 // its transform (12 floats) and material (Kd, Ks, GGX alpha, ior; Oren-Nayar
@@ -368,6 +435,8 @@ int ref_render_scene(const float* wpos, uint32_t nverts, const uint32_t* idx, ui
   fs.env.assign(env, env + 3 * (size_t)envW * envH);
   fs.envW = envW;
   fs.envH = envH;
+  orc_env_destroy(fs.envH_);
+  fs.envH_ = orc_env_create(fs.env.data(), envW, envH);
   fs.mask = rt::ESceneobjectMask::ALL;
   const int h = orc_build_bvh(wpos, nverts, idx, ntris, fs.nodes.data(), fs.order.data(), fs.tris.data());
   fs.ready = h >= 0;
@@ -390,6 +459,39 @@ int ref_path_li(uint32_t W, uint32_t H, float fov, const float* pos, const float
   rt::CPathIntegrator li(&scene, &ps, &sampler, 1, false, rt::EDebugMode::NONE);
   put(L3, li.Li());
   return ref_draws_used();
+}
+
+// Timing run of the reference's integrator on the scene of ref_render_scene:
+// for pixels [p0, p1) of the camera, spp samples of CPathIntegrator::Li each
+// (its own bounce cap of 50 and roulette from bounce 4), draws from a Philox
+// generator per path (pixel, seed, sample), `threads` host threads taking
+// every threads-th pixel.  rgb_out: the mean per pixel (3 floats).
+int ref_render_paths(uint32_t W, uint32_t H, float fov, const float* pos, const float* lookAt, const float* up,
+                     uint32_t spp, uint32_t seed, uint32_t p0, uint32_t p1, float* rgb_out, int threads) {
+  if (!r2ref::g_fs.ready || p1 <= p0 || p1 > W * H || spp == 0) return -1;
+  if (threads < 1) threads = 1;
+  const glm::vec3 P = V(pos), A = V(lookAt), U = V(up);
+  std::vector<std::thread> pool;
+  for (int t = 0; t < threads; ++t) {
+    pool.emplace_back([=]() {
+      rt::CCamera cam((uint16_t)W, (uint16_t)H, fov, P, A, U);
+      for (uint32_t p = p0 + (uint32_t)t; p < p1; p += (uint32_t)threads) {
+        glm::vec3 acc(0.f);
+        for (uint32_t s = 0; s < spp; ++s) {
+          r2ref::gen_start(p, seed, s);
+          rt::CSampler sampler;
+          rt::CPixelSampler ps(&cam, (uint16_t)(p % W), (uint16_t)(p / W), &sampler);
+          rt::CDeviceScene scene;
+          rt::CPathIntegrator li(&scene, &ps, &sampler, 1, false, rt::EDebugMode::NONE);
+          acc += li.Li();
+        }
+        put(rgb_out + 3 * (size_t)(p - p0), acc / (float)spp);
+      }
+      r2ref::g_gen.on = false;
+    });
+  }
+  for (auto& th : pool) th.join();
+  return 0;
 }
 
 // CMeshFilter(voxel, grid...).run(scene, spv) (mesh_filter.hpp:24-122): the

@@ -1851,6 +1851,29 @@ int orc_env_le(const float* env_rgb, int W, int H, const float* dir, float* pdf,
   return 0;
 }
 
+/* An environment map with its distributions built once (for callers that
+ * query it per path). */
+void* orc_env_create(const float* env_rgb, int W, int H) {
+  env_t* e = (env_t*)malloc(sizeof(env_t));
+  if (e) env_build(e, env_rgb, W, H);
+  return e;
+}
+void orc_env_destroy(void* h) {
+  if (!h) return;
+  env_free((env_t*)h);
+  free(h);
+}
+void orc_env_sample_h(const void* h, float u0, float u1, float* dir, float* pdf, float* le) {
+  f3 d;
+  f3 l = env_sample((const env_t*)h, u0, u1, &d, pdf);
+  dir[0] = d.x; dir[1] = d.y; dir[2] = d.z;
+  le[0] = l.x; le[1] = l.y; le[2] = l.z;
+}
+void orc_env_le_h(const void* h, const float* dir, float* pdf, float* le) {
+  f3 l = env_le((const env_t*)h, F3(dir[0], dir[1], dir[2]), pdf);
+  le[0] = l.x; le[1] = l.y; le[2] = l.z;
+}
+
 /* ------------------------------------------------------------ unit hooks for the golden-vector tests */
 
 static f3 L3(const float* p) { return F3(p[0], p[1], p[2]); }

@@ -92,6 +92,11 @@ void orc_tonemap(const float* rgb, uint32_t W, uint32_t H, float gamma, float* o
 int orc_env_sample(const float* env_rgb, int env_w, int env_h, float u0, float u1, float* dir_out, float* pdf_out,
                    float* le_out);
 int orc_env_le(const float* env_rgb, int env_w, int env_h, const float* dir, float* pdf_out, float* le_out);
+/* The same with the distributions built once: a handle from orc_env_create. */
+void* orc_env_create(const float* env_rgb, int env_w, int env_h);
+void orc_env_destroy(void* env);
+void orc_env_sample_h(const void* env, float u0, float u1, float* dir_out, float* pdf_out, float* le_out);
+void orc_env_le_h(const void* env, const float* dir, float* pdf_out, float* le_out);
 
 #ifdef __cplusplus
 }
