@@ -416,37 +416,23 @@ __device__ __forceinline__ void trace_persistent(const BvhView& bvh, uint32_t n,
 __device__ __forceinline__ int trav_visits(const RenderLaunch& L) { return (int)max(1u, L.travVisits); }
 __device__ __forceinline__ int trav_refill(const RenderLaunch& L) { return (int)min(32u, max(1u, L.travRefill)); }
 
-// The persistent traversal of the scene's BVH with the instantiation it needs
-// (alpha-tested triangles, two levels).  With L.topNodes, the block first
-// copies BVH nodes 0 .. topNodes-1 (the host keeps the count within the tree
-// and kMaxTopNodes) into its dynamic shared memory and reads them from there.
+// The persistent traversal of the scene's BVH (kAlpha: alpha-tested
+// triangles; kInst: two levels).  kTop: the block first copies BVH nodes
+// 0 .. L.topNodes-1 (the host keeps the count within the tree and
+// kMaxTopNodes) into its dynamic shared memory and reads them from there.
 // Every thread of the block calls this once.
-template <bool kAnyHit, class Begin, class End>
+template <bool kAnyHit, bool kAlpha, bool kInst, bool kTop, class Begin, class End>
 __device__ __forceinline__ void trace_scene(const RenderLaunch& L, uint32_t n, uint32_t* taken, Begin begin, End end) {
-  extern __shared__ BvhNode sTop[];
   BvhView bvh = L.scene.bvh;
-  const int ntop = (int)L.topNodes;
-  const int v = trav_visits(L), r = trav_refill(L);
-  const bool alpha = bvh.alpha.alphaTex != nullptr, inst = bvh.inst != nullptr;
-  if (ntop > 0) {
+  if (kTop) {
+    extern __shared__ BvhNode sTop[];
+    const int ntop = (int)L.topNodes;
     for (int k = threadIdx.x; k < ntop; k += blockDim.x) sTop[k] = bvh.nodes[k];
     __syncthreads();
     bvh.top = sTop;
     bvh.ntop = ntop;
-    if (inst) {
-      if (alpha) trace_persistent<kAnyHit, true, true, true>(bvh, n, taken, v, r, L.bound, begin, end);
-      else trace_persistent<kAnyHit, false, true, true>(bvh, n, taken, v, r, L.bound, begin, end);
-    } else {
-      if (alpha) trace_persistent<kAnyHit, true, false, true>(bvh, n, taken, v, r, L.bound, begin, end);
-      else trace_persistent<kAnyHit, false, false, true>(bvh, n, taken, v, r, L.bound, begin, end);
-    }
-  } else if (inst) {
-    if (alpha) trace_persistent<kAnyHit, true, true, false>(bvh, n, taken, v, r, L.bound, begin, end);
-    else trace_persistent<kAnyHit, false, true, false>(bvh, n, taken, v, r, L.bound, begin, end);
-  } else {
-    if (alpha) trace_persistent<kAnyHit, true, false, false>(bvh, n, taken, v, r, L.bound, begin, end);
-    else trace_persistent<kAnyHit, false, false, false>(bvh, n, taken, v, r, L.bound, begin, end);
   }
+  trace_persistent<kAnyHit, kAlpha, kInst, kTop>(bvh, n, taken, trav_visits(L), trav_refill(L), L.bound, begin, end);
 }
 
 // Closest hit of every live path (scenes without media).  A path that hits a
@@ -465,28 +451,31 @@ __device__ __forceinline__ void extend_result(const RenderLaunch& L, uint32_t p,
   push_queue(L.st.qh, &L.st.counts[kHitCounters + L.bounce], __float_as_int(h.w) != -1, p);
 }
 
+// One instantiation per traversal variant (no triangles; alpha test, two
+// levels, shared top nodes), each with its own register allocation.
+template <bool kTris, bool kAlpha, bool kInst, bool kTop>
 __global__ void __launch_bounds__(128, 10) k_extend(RenderLaunch L) {
   const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
   const uint32_t* q = path_queue(L, L.bounce);
-  if (!L.scene.hasTris) {
+  if constexpr (!kTris) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
       const uint32_t p = q[i];
       const V3 d = xyz(L.st.rayD[p]);
       extend_result(L, p, d, scene_closest<false>(L.scene, xyz(L.st.rayO[p]), d, kDefaultTmax));
     }
-    return;
+  } else {
+    auto begin = [&](uint32_t k, TraceState& s, uint32_t* item) {
+      const uint32_t p = q[k];
+      *item = p;
+      trace_begin(s, xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), kDefaultTmax);
+      return true;
+    };
+    auto end = [&](uint32_t p, const TraceState& s) {
+      extend_result(L, p, s.wd, scene_closest_after<false>(L.scene, s.wo, s.wd, kDefaultTmax, s.best));
+    };
+    trace_scene<false, kAlpha, kInst, kTop>(L, n, &L.st.counts[kTravCounters + 2 * L.bounce], begin, end);
   }
-  auto begin = [&](uint32_t k, TraceState& s, uint32_t* item) {
-    const uint32_t p = q[k];
-    *item = p;
-    trace_begin(s, xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), kDefaultTmax);
-    return true;
-  };
-  auto end = [&](uint32_t p, const TraceState& s) {
-    extend_result(L, p, s.wd, scene_closest_after<false>(L.scene, s.wo, s.wd, kDefaultTmax, s.best));
-  };
-  trace_scene<false>(L, n, &L.st.counts[kTravCounters + 2 * L.bounce], begin, end);
 }
 
 // ------------------------------------------------------------------ media: path extension
@@ -1081,10 +1070,11 @@ __device__ __forceinline__ Ray shadow_ray(float4 o, float4 d) {
 }
 
 // Visibility of every shadow record of a scene without media.
+template <bool kTris, bool kAlpha, bool kInst, bool kTop>
 __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
   const uint32_t n = event_count(L);
   uint32_t traced = 0;
-  if (!L.scene.hasTris) {
+  if constexpr (!kTris) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < 2 * n; j += stride) {
       const float4 o = L.st.shO[j];
@@ -1120,7 +1110,7 @@ __global__ void __launch_bounds__(128, 10) k_shadow_surfaces(RenderLaunch L) {
       }
       L.st.shTr[j] = occluded ? 0.0f : 1.0f;
     };
-    trace_scene<true>(L, 2 * n, &L.st.counts[kTravCounters + 2 * L.bounce + 1], begin, end);
+    trace_scene<true, kAlpha, kInst, kTop>(L, 2 * n, &L.st.counts[kTravCounters + 2 * L.bounce + 1], begin, end);
   }
   if (L.stats) {
     for (int o = 16; o > 0; o >>= 1) traced += __shfl_down_sync(0xffffffffu, traced, o);
@@ -1279,24 +1269,45 @@ int g_trackBlocks[4] = {0, 0, 0, 0};  // resident blocks of k_track<dda, sample>
 
 int g_travBlocks[2] = {0, 0};  // resident blocks of k_extend, k_shadow_surfaces
 
+// The surface traversal kernels by variant: alpha + 2 * two-level + 4 * top
+// nodes; 8: a scene without triangles.
+using RenderKernel = void (*)(RenderLaunch);
+const RenderKernel kExtendVariants[9] = {
+    k_extend<true, false, false, false>, k_extend<true, true, false, false>, k_extend<true, false, true, false>,
+    k_extend<true, true, true, false>,   k_extend<true, false, false, true>, k_extend<true, true, false, true>,
+    k_extend<true, false, true, true>,   k_extend<true, true, true, true>,   k_extend<false, false, false, false>};
+const RenderKernel kShadowVariants[9] = {
+    k_shadow_surfaces<true, false, false, false>, k_shadow_surfaces<true, true, false, false>,
+    k_shadow_surfaces<true, false, true, false>,  k_shadow_surfaces<true, true, true, false>,
+    k_shadow_surfaces<true, false, false, true>,  k_shadow_surfaces<true, true, false, true>,
+    k_shadow_surfaces<true, false, true, true>,   k_shadow_surfaces<true, true, true, true>,
+    k_shadow_surfaces<false, false, false, false>};
+
+int trav_variant(const RenderLaunch& L) {
+  if (!L.scene.hasTris) return 8;
+  return (L.scene.bvh.alpha.alphaTex ? 1 : 0) + (L.scene.bvh.inst ? 2 : 0) + (L.topNodes ? 4 : 0);
+}
+
 // Resident blocks of a surface traversal kernel (0: k_extend, 1:
-// k_shadow_surfaces) with topNodes BVH nodes of dynamic shared memory.
-int trav_blocks(int which, uint32_t topNodes) {
+// k_shadow_surfaces) of a variant with topNodes BVH nodes of dynamic shared memory.
+int trav_blocks(int which, int variant, uint32_t topNodes) {
   static std::mutex mu;
   static std::map<std::pair<int, uint32_t>, int> cache;
   std::lock_guard<std::mutex> lock(mu);
-  auto it = cache.find({which, topNodes});
+  const int key = which * 9 + variant;
+  auto it = cache.find({key, topNodes});
   if (it != cache.end()) return it->second;
   const size_t smem = topNodes * sizeof(BvhNode);
-  const int n = which == 0 ? resident_blocks(k_extend, 128, smem) : resident_blocks(k_shadow_surfaces, 128, smem);
-  cache[{which, topNodes}] = n;
+  const RenderKernel k = which == 0 ? kExtendVariants[variant] : kShadowVariants[variant];
+  const int n = resident_blocks(k, 128, smem);
+  cache[{key, topNodes}] = n;
   return n;
 }
 
 void query_track_blocks() {
   if (g_trackBlocks[0] != 0) return;
-  g_travBlocks[0] = resident_blocks(k_extend, 128);
-  g_travBlocks[1] = resident_blocks(k_shadow_surfaces, 128);
+  g_travBlocks[0] = resident_blocks(kExtendVariants[0], 128);
+  g_travBlocks[1] = resident_blocks(kShadowVariants[0], 128);
   g_trackBlocks[1] = resident_blocks(k_track<true, false>, 128);
   g_trackBlocks[2] = resident_blocks(k_track<false, true>, 128);
   g_trackBlocks[3] = resident_blocks(k_track<true, true>, 128);
@@ -1366,12 +1377,14 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
         else k_shadow_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
     } else {
-      k_extend<<<std::min(nblocks * 2, trav_blocks(0, L.topNodes)), 128, L.topNodes * sizeof(BvhNode), s>>>(L);
+      const int tv = trav_variant(L);
+      kExtendVariants[tv]<<<std::min(nblocks * 2, trav_blocks(0, tv, L.topNodes)), 128,
+                            L.topNodes * sizeof(BvhNode), s>>>(L);
       mark(1);
       k_shade<false><<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
-      k_shadow_surfaces<<<std::min(nblocks * 2, trav_blocks(1, L.topNodes)), 128, L.topNodes * sizeof(BvhNode),
-                          s>>>(L);
+      kShadowVariants[tv]<<<std::min(nblocks * 2, trav_blocks(1, tv, L.topNodes)), 128,
+                            L.topNodes * sizeof(BvhNode), s>>>(L);
     }
     mark(3);
     k_accum<<<nblocks, 256, 0, s>>>(L);
