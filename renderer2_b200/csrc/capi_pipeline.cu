@@ -36,8 +36,15 @@ r2::M4 object_transform(const r2::SceneObjectDesc& o) {
                                       r2::v3(o.scaling[0], o.scaling[1], o.scaling[2]));
 }
 
+// Scene objects of type Mesh whose file is used by one object are flattened
+// into world space; a file placed by several objects becomes one mesh asset
+// per submesh with an instance per object (CAssetManager::loadMesh keeps one
+// CMesh and GAS per file, asset_manager.cu, and every object is an instance).
 void build_scene(r2_config* c) {
   auto sc = std::unique_ptr<r2::RenderScene>(new r2::RenderScene());
+  std::map<const std::vector<r2::ObjSubmesh>*, int> uses;
+  for (const auto& m : c->meshes) ++uses[m.get()];
+  std::map<const r2::ObjSubmesh*, uint32_t> assetOf;
   size_t mi = 0;
   for (const r2::SceneObjectDesc& o : c->cfg.objects) {
     switch (o.kind) {
@@ -52,12 +59,22 @@ void build_scene(r2_config* c) {
       case r2::SceneObjectDesc::kMesh: {
         float m43[12];
         r2::m43_to_floats(r2::m4_to_m43(object_transform(o)), m43);
+        const bool shared = uses[c->meshes[mi].get()] > 1;
         for (const r2::ObjSubmesh& s : *c->meshes[mi]) {
           const r2_material_maps maps = {s.texAlbedo.c_str(), s.texSpecular.c_str(), s.texNormal.c_str(),
                                          s.texAlpha.c_str()};
-          sc->add_mesh(s.positions.data(), (uint32_t)(s.positions.size() / 3), s.indices.data(),
-                       (uint32_t)(s.indices.size() / 3), s.normals.data(), s.material, m43, o.mask,
-                       s.uvs.empty() ? nullptr : s.uvs.data(), &maps);
+          const float* uv = s.uvs.empty() ? nullptr : s.uvs.data();
+          if (!shared) {
+            sc->add_mesh(s.positions.data(), (uint32_t)(s.positions.size() / 3), s.indices.data(),
+                         (uint32_t)(s.indices.size() / 3), s.normals.data(), s.material, m43, o.mask, uv, &maps);
+            continue;
+          }
+          auto it = assetOf.find(&s);
+          if (it == assetOf.end())
+            it = assetOf.emplace(&s, sc->add_mesh_asset(s.positions.data(), (uint32_t)(s.positions.size() / 3),
+                                                        s.indices.data(), (uint32_t)(s.indices.size() / 3),
+                                                        s.normals.data(), s.material, uv, &maps)).first;
+          sc->add_mesh_instance(it->second, m43, o.mask);
         }
         ++mi;
         break;
