@@ -452,7 +452,8 @@ def bench_render(args, world, local):
     ev1 = torch.cuda.Event(enable_timing=True)
     st = np.zeros(8)
     stats = []
-    evb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    evb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     ev0.record()
     for k in range(args.steps):
         # one step = BVH build from the resident triangles + the frame (config "BVH build + trace");
@@ -461,13 +462,15 @@ def bench_render(args, world, local):
         sc.rebuild(stream)
         evb[k][1].record()
         sc.render_device(cam, prm, frame.data_ptr(), stream, stats=st)
+        evb[k][2].record()
         stats.append(st.copy())
     ev1.record()
     torch.cuda.synchronize()
     _barrier(world)
     ck = clocks.stop()
     total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
-    build_ms = float(np.median([a.elapsed_time(b) for a, b in evb]))
+    build_ms = float(np.median([a.elapsed_time(b) for a, b, _ in evb]))
+    latency = step_latency([a.elapsed_time(c) for a, _, c in evb])
     paths = npix * prm.spp
     value = world * paths * args.steps / (total_ms / 1e3)
     st = np.mean(np.array(stats), axis=0)
@@ -534,6 +537,7 @@ def bench_render(args, world, local):
                          "render_and_download_ms": (t2 - t1) * 1e3, "h2d_bytes": int(_input_bytes(desc))}
     launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth) + bvh_launches
     return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths, tuning=tuning,
+                latency=latency,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
                 bvh_build_ms=build_ms, render_ms=total_ms / args.steps - build_ms, desc=desc, cam=cam, prm=prm,
                 bvh={"method": "PLOC" if R.bvh_method() == R.BVH_PLOC else "Karras", "inner_nodes": bvh_nodes,
@@ -564,14 +568,15 @@ def bench_filter(args, world, local, grid=None, steps=None, warmup=None, e2e_run
     _barrier(world)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    step_ms, kernel_ms, cand = 0.0, [], []
+    step_ms, kernel_ms, cand, per_step = 0.0, [], [], []
     for _ in range(steps):
         flush.fill_(1)  # 256 MiB write evicts L2 between steps
         ev0.record()
         sc.run(g, prm, out.data_ptr(), stream=stream, stats=st)
         ev1.record()
         torch.cuda.synchronize()
-        step_ms += ev0.elapsed_time(ev1)
+        per_step.append(ev0.elapsed_time(ev1))
+        step_ms += per_step[-1]
         kernel_ms.append(st[2])
         cand.append(st[1])
     _barrier(world)
@@ -619,6 +624,7 @@ def bench_filter(args, world, local, grid=None, steps=None, warmup=None, e2e_run
             "config": {"workload": f"filter at scale: 500k leaf quads (1M tris), {n}^3, 256 spv, 20 iters",
                        "voxels": nvox, "candidate_voxels": float(np.mean(cand)),
                        "l2": "256 MiB flush write between steps"},
+            "latency": step_latency(per_step),
             "roofline": {"bound": "hbm", "kernel": "k_filter_sample", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": tr["bytes_per_unit"] * nvox if tr else None,
@@ -767,6 +773,34 @@ def bench_small(args, world, local):
             "gpu_launches": (2 + bvh_launches + (c["spp"] // S) * (2 + 4 * c["depth"])) * args.steps}
 
 
+def media_roofline(st, S, spp, depth):
+    """HBM roofline of the dominant phase of a media frame from its render statistics st (the 8 values of
+    r2_render_device) and S samples per wave."""
+    ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
+    seg_wave = st[2] * S / spp
+    dom = max(("extend", "shadow", "shade"), key=lambda k: ms_wave[k])
+    per_unit = {"extend": (VOLUME_EXTEND_BYTES_PER_SEGMENT, seg_wave, "extend phase"),
+                "shadow": (SHADOW_MEDIA_BYTES_PER_SLOT, 2.0 * seg_wave, "shadow phase"),
+                "shade": (SHADE_BYTES_PER_SEGMENT, seg_wave, "k_shade<true>")}[dom]
+    alg = per_unit[0] * per_unit[1]
+    kms = ms_wave[dom]
+    peak, peak_kind = _peaks()
+    achieved = alg / (kms / 1e3) / 1e9
+    tr = _traffic(per_unit[2])
+    return {"bound": "hbm", "kernel": per_unit[2], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": tr["bytes_per_unit"] * per_unit[1] / depth if tr else None,
+            "alg_bytes_per_launch": alg / depth, "avg_launch_ms": kms / depth,
+            "note": "delta/ratio tracking is latency bound on dependent grid lookups",
+            "kernel_ms_per_wave": ms_wave}
+
+
+def step_latency(ms):
+    """p50 / p99 of per-step device times (ms)."""
+    a = np.asarray(ms, np.float64)
+    return {"p50_ms": float(np.percentile(a, 50)), "p99_ms": float(np.percentile(a, 99)), "steps": int(a.size)}
+
+
 def bench_volume(args, world, local):
     """Volume leg: one batched-volume scene (filtered 256^3 foliage medium +
     81,920-tri mesh), 1920x1080, depth 16, brick-grid DDA tracking."""
@@ -803,27 +837,12 @@ def bench_volume(args, world, local):
     _barrier(world)
     total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
     paths = npix * prm.spp
+    latency = step_latency([x[1] for x in stats])
     st = np.mean(np.array(stats), axis=0)
     seg, shadow = st[2], st[3]
-    ms_wave = {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]}
     S = sc.wave_samples(cam, prm)
-    seg_wave = seg * S / prm.spp
-    dom = max(("extend", "shadow", "shade"), key=lambda k: ms_wave[k])
-    per_unit = {"extend": (VOLUME_EXTEND_BYTES_PER_SEGMENT, seg_wave, "extend phase"),
-                "shadow": (SHADOW_MEDIA_BYTES_PER_SLOT, 2.0 * seg_wave, "shadow phase"),
-                "shade": (SHADE_BYTES_PER_SEGMENT, seg_wave, "k_shade<true>")}[dom]
-    alg = per_unit[0] * per_unit[1]
-    kms = ms_wave[dom]
-    peak, peak_kind = _peaks()
-    achieved = alg / (kms / 1e3) / 1e9
-    tr = _traffic(per_unit[2])
-    launches = prm.max_depth
-    roofline = {"bound": "hbm", "kernel": per_unit[2], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": tr["bytes_per_unit"] * per_unit[1] / launches if tr else None,
-                "alg_bytes_per_launch": alg / launches, "avg_launch_ms": kms / launches,
-                "note": "delta/ratio tracking is latency bound on dependent grid lookups",
-                "kernel_ms_per_wave": ms_wave}
+    roofline = media_roofline(st, S, prm.spp, prm.max_depth)
+    ms_wave = roofline["kernel_ms_per_wave"]
     h2d = _input_bytes(desc) + sum(os.path.getsize(m[0] + e) for m in desc["media"] for e in (".nvdb", ".brickgrid"))
     e2e_ms = []
     for _ in range(1):
@@ -843,7 +862,7 @@ def bench_volume(args, world, local):
                       "paths_per_step": paths, "segments_per_step": seg, "shadow_rays_per_step": shadow,
                       "l2": "wave state larger than L2",
                       "tuning": tuning},
-           "roofline": roofline,
+           "roofline": roofline, "latency": latency,
            "e2e": {"value": world * paths / (e2e_ms / 1e3), "unit": "paths/s", "h2d_bytes_per_step": int(h2d),
                    "d2h_bytes_per_step": int(npix * 12), "ms_per_step": e2e_ms},
            # per wave: camera, finish; per bounce: _media_launches
@@ -918,8 +937,11 @@ def bench_forest(args, world, local, cfg=None, autotune=True):
     _barrier(world)
     total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
     S = sc.wave_samples(cam, prm)
+    bvh_nodes, bvh_height, _ = sc.bvh_info()
     sc.close()
     st = np.mean(np.array(stats), axis=0)
+    roofline = media_roofline(st, S, prm.spp, prm.max_depth)
+    latency = step_latency([x[1] for x in stats])
     paths = npix * prm.spp
     kinds = [t[0] for t in trees]
     lods = {}
@@ -937,7 +959,10 @@ def bench_forest(args, world, local, cfg=None, autotune=True):
                        "mesh_trees": kinds.count("Mesh"), "lods": dict(sorted(lods.items())),
                        "paths_per_step": paths, "segments_per_step": st[2], "shadow_rays_per_step": st[3],
                        "kernel_ms_per_step": {"extend": st[4], "shade": st[5], "shadow": st[6], "accum": st[7]},
+                       "bvh": {"two_level": kinds.count("Mesh") > 1, "inner_nodes": bvh_nodes,
+                               "height": bvh_height},
                        "l2": "wave state larger than L2", "tuning": tuning},
+            "roofline": roofline, "latency": latency,
             "lod_selection": {"trees": len(placed), "ms": float(np.median(sel_ms)),
                               "trees_per_s": len(placed) / (float(np.median(sel_ms)) / 1e3),
                               "timed": "r2_select_lods with host buffers (upload, kernel, download)",
@@ -1008,18 +1033,34 @@ def bench_volume_batch(args, world, local):
     _barrier(world)
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
     ev[0].record()
-    for _ in range(args.steps):
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
         # 16 scenes' wave state (~1 GB each) and media exceed L2; no flush needed
+        evs[k][0].record()
         batch.run(stream, timing=False)
+        evs[k][1].record()
     ev[1].record()
+    sst = [np.zeros(8) for _ in scs]
     for _ in range(args.steps):
-        for sc, cm, p, f in zip(scs, cams, prms, frames):
-            sc.render_device(cm, p, f.data_ptr(), stream)
+        for k, (sc, cm, p, f) in enumerate(zip(scs, cams, prms, frames)):
+            st = np.zeros(8)
+            sc.render_device(cm, p, f.data_ptr(), stream, stats=st)
+            sst[k] += st / args.steps
     ev[2].record()
     torch.cuda.synchronize()
     _barrier(world)
     ms_batch = _max_over_ranks(ev[0].elapsed_time(ev[1]), world)
     ms_seq = _max_over_ranks(ev[1].elapsed_time(ev[2]), world)
+    latency = step_latency([a.elapsed_time(b) for a, b in evs])
+    # roofline of the dominant phase, scene by scene (statistics of the one-at-a-time frames)
+    rfs = [media_roofline(st, sc.wave_samples(cm, p), p.spp, p.max_depth) for st, sc, cm, p in zip(sst, scs, cams, prms)]
+    w = np.array([sum(r["kernel_ms_per_wave"].values()) for r in rfs])
+    roofline = dict(rfs[0])
+    roofline["frac"] = float(np.sum(w * np.array([r["frac"] for r in rfs])) / np.sum(w))
+    roofline["achieved"] = roofline["frac"] * roofline["peak"]
+    roofline["note"] = ("time-weighted mean over the 16 scenes of each scene's dominant phase, from its frame rendered "
+                        "alone; " + rfs[0]["note"])
+    roofline["per_scene_frac"] = [round(r["frac"], 5) for r in rfs]
     paths = sum(npix) * c["spp"]
     # end to end: upload every scene (media read from their files), one batch, frames back to the host
     h2d = sum(_input_bytes(d) + sum(os.path.getsize(m[0] + e) for m in d["media"] for e in (".nvdb", ".brickgrid"))
@@ -1050,6 +1091,7 @@ def bench_volume_batch(args, world, local):
             "one_scene_at_a_time": {"value": world * paths * args.steps / (ms_seq / 1e3),
                                     "ms_per_step": ms_seq / args.steps},
             "speedup_vs_one_at_a_time": ms_seq / ms_batch,
+            "roofline": roofline, "latency": latency,
             "frames_256spp_ms": ms_batch / args.steps / c["spp"] * c["frame_spp"],
             "frames_256spp_note": "the 16 frames at the configuration's 256 spp: the graph replays one sample of every "
                                   "scene per replay, so a full frame set is 256 replays; time per replay measured "
@@ -1283,7 +1325,7 @@ def run_native(args):
                                    "bvh_build_ms_per_step": r["bvh_build_ms"], "render_ms_per_step": r["render_ms"],
                                    "bvh": r["bvh"], "tuning": r["tuning"]},
                 "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
-                "clocks": r["clocks"]}
+                "latency": r["latency"], "clocks": r["clocks"]}
         if small is not None:
             line["small"] = small
             line["gpu_launches"] += small["gpu_launches"]
@@ -1344,6 +1386,8 @@ def legs_summary(line: dict) -> dict:
         for k in ("paths_per_s", "p50_latency_s", "p99_latency_s", "speedup_vs_one_at_a_time"):
             if k in d:
                 e[k] = _short(d[k], 4)
+        if isinstance(d.get("latency"), dict):
+            e["p99_step_ms"] = _short(d["latency"]["p99_ms"], 4)
         if isinstance(rf, dict) and "filter" in rf and "render" in rf:
             e["hbm_frac"] = {"filter": _short(rf["filter"]["frac"], 3), "render": _short(rf["render"]["frac"], 3)}
         acc = d.get("accuracy")
@@ -1363,7 +1407,9 @@ def legs_summary(line: dict) -> dict:
                           "voxels_per_s": _short(sv["served"]["voxels_per_s"]),
                           "p50_latency_s": _short(sv["served"]["p50_latency_s"], 3),
                           "p99_latency_s": _short(sv["served"]["p99_latency_s"], 3),
-                          "speedup_makespan": _short(sv.get("speedup_makespan"), 3)}
+                          "speedup_makespan": _short(sv.get("speedup_makespan"), 3),
+                          "burst_speedup_vs_one_at_a_time": _short(sv["burst"].get("speedup_makespan"), 3),
+                          "burst_speedup_vs_plain": _short(sv["burst"].get("speedup_vs_plain"), 3)}
         if isinstance(sv.get("roofline"), dict):
             out["serving"]["hbm_frac"] = _short(sv["roofline"].get("frac"), 3)
     return out
