@@ -862,11 +862,12 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
       const V3 f = be.f * fabsf(dot(n, ldir));
       const float spdf = be.pdf;
       const float mis = balance_heuristic(lpdf, spdf);
-      const Ray lr = ray_offset(make_ray(pos, ldir, kDefaultTmax), n);
+      // offsetRayOrigin(n) of the ray (pos, ldir, DEFAULT_TMAX): origin offO, end point kept
+      const float t1 = length((pos + ldir * kDefaultTmax) - offO);
       shO0 = f4(offO, lpdf);
-      shD0 = f4(ldir, lr.tmax);  // intersectTr walks towards offO + ldir * tmax
+      shD0 = f4(ldir, t1);  // intersectTr walks towards offO + ldir * t1
       pre0 = f4((f * mis) * Le, 0.0f);
-      if (kMedia) L.st.shX[2 * i] = make_float2(lr.tmax, __int_as_float(med));
+      if (kMedia) L.st.shX[2 * i] = make_float2(t1, __int_as_float(med));
     }
   }
   // --- direct(): BSDF sample (path_integrator_impl.hpp:74-113)
@@ -881,11 +882,11 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
       const V3 Le = ee.Le;
       const float lpdf = ee.pdf;
       const float mis = balance_heuristic(spdf, lpdf);
-      const Ray br = ray_offset(make_ray(pos, wi, kDefaultTmax), n);
+      const float t1 = length((pos + wi * kDefaultTmax) - offO);
       shO1 = f4(offO, spdf);
-      shD1 = f4(wi, br.tmax);
+      shD1 = f4(wi, t1);
       pre1 = f4((f * mis) * Le, 0.0f);
-      if (kMedia) L.st.shX[2 * i + 1] = make_float2(br.tmax, __int_as_float(med));
+      if (kMedia) L.st.shX[2 * i + 1] = make_float2(t1, __int_as_float(med));
     }
   }
   L.st.shO[2 * i] = shO0;
