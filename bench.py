@@ -540,7 +540,7 @@ def bench_render(args, world, local):
                 latency=latency,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
                 bvh_build_ms=build_ms, render_ms=total_ms / args.steps - build_ms, desc=desc, cam=cam, prm=prm,
-                bvh={"method": "PLOC" if R.bvh_method() == R.BVH_PLOC else "Karras", "inner_nodes": bvh_nodes,
+                bvh={"method": "Karras" if R.bvh_method() == R.BVH_KARRAS else "PLOC", "inner_nodes": bvh_nodes,
                      "height": bvh_height, "build_launches": bvh_launches})
 
 

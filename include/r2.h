@@ -46,13 +46,14 @@ int r2_version(void);
 
 /* Hierarchy of the BVHs built from now on (scenes, filter scenes, rebuilds),
  * process-wide.  Both start from the Morton-sorted primitives and end with the
- * same SAH leaf collapse.  R2_BVH_PLOC (default): parallel locally-ordered
- * clustering (Meister & Bittner 2018), mutual nearest neighbours by
- * surface area within 16 sorted positions.  R2_BVH_KARRAS: the radix tree of
- * the Morton codes (Karras 2012).  Replaces the OptiX builder
- * (optixAccelBuild, raytracer/src/mesh/mesh.cu:140-166 and
+ * same SAH leaf collapse.  R2_BVH_PLOC: parallel locally-ordered clustering
+ * (Meister & Bittner 2018), mutual nearest neighbours by surface area within
+ * 16 sorted positions.  R2_BVH_KARRAS: the radix tree of the Morton codes
+ * (Karras 2012).  R2_BVH_AUTO (default): PLOC for render scenes, the Karras
+ * tree for filter scenes (the faster of the two for each).  Replaces the OptiX
+ * builder (optixAccelBuild, raytracer/src/mesh/mesh.cu:140-166 and
  * raytracer/src/scene/scene.cu:188-256), which has no such choice. */
-enum { R2_BVH_PLOC = 0, R2_BVH_KARRAS = 1 };
+enum { R2_BVH_AUTO = -1, R2_BVH_PLOC = 0, R2_BVH_KARRAS = 1 };
 r2_status r2_set_bvh_method(int method);
 int r2_get_bvh_method(void);
 

@@ -183,9 +183,10 @@ static void put_box(int32_t* w, int slot, const float* l, const float* h) {
 /* ------------------------------------------------ PLOC (bvh_ploc.cu) */
 #define PLOC_RADIUS 16
 
-static int g_bvh_method = 0; /* 0 PLOC, 1 Karras */
-void orc_set_bvh_method(int method) { g_bvh_method = method == 1 ? 1 : 0; }
+static int g_bvh_method = -1; /* -1 auto (PLOC for render scenes, Karras for filter scenes), 0 PLOC, 1 Karras */
+void orc_set_bvh_method(int method) { g_bvh_method = method == 1 ? 1 : (method == 0 ? 0 : -1); }
 int orc_get_bvh_method(void) { return g_bvh_method; }
+static int bvh_method_for(int filterScene) { return g_bvh_method >= 0 ? g_bvh_method : (filterScene ? 1 : 0); }
 
 static float union_area(const float* al, const float* ah, const float* bl, const float* bh) {
   float dx = fmaxf(ah[0], bh[0]) - fminf(al[0], bl[0]);
@@ -318,8 +319,21 @@ static int ploc_child_ref(const ploc_t* P, int c) {
   return c;
 }
 
+static int build_bvh_impl(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, int32_t* nodes_out,
+                          uint32_t* order_out, float* tris_out, int method);
+
 int orc_build_bvh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, int32_t* nodes_out,
                   uint32_t* order_out, float* tris_out) {
+  return build_bvh_impl(pos, nverts, idx, ntris, nodes_out, order_out, tris_out, bvh_method_for(0));
+}
+
+int orc_build_bvh_filter(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, int32_t* nodes_out,
+                         uint32_t* order_out, float* tris_out) {
+  return build_bvh_impl(pos, nverts, idx, ntris, nodes_out, order_out, tris_out, bvh_method_for(1));
+}
+
+static int build_bvh_impl(const float* pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris, int32_t* nodes_out,
+                          uint32_t* order_out, float* tris_out, int method) {
   (void)nverts;
   if (ntris == 0 || ntris >= (1u << 26)) return -1;
   int n = (int)ntris;
@@ -361,7 +375,7 @@ int orc_build_bvh(const float* pos, uint32_t nverts, const uint32_t* idx, uint32
     order_out[i] = kv[i].idx;
   }
   int plocHeight = -1;
-  if (n > 1 && g_bvh_method == 0) {
+  if (n > 1 && method == 0) {
     int ni = n - 1;
     ploc_t P;
     P.left = (int*)malloc(sizeof(int) * ni); P.right = (int*)malloc(sizeof(int) * ni);
@@ -1169,7 +1183,7 @@ int orc_filter_tex(const float* positions, uint32_t nverts, const uint32_t* idx,
   int32_t* nodes = (int32_t*)malloc(64 * nn);
   uint32_t* order = (uint32_t*)malloc(4 * (size_t)ntris);
   float* tris = (float*)malloc(48 * (size_t)ntris);
-  int height = orc_build_bvh(wpos, nverts, idx, ntris, nodes, order, tris);
+  int height = orc_build_bvh_filter(wpos, nverts, idx, ntris, nodes, order, tris);
   if (height < 0 || height > BVH_STACK) {
     free(wpos); free(nodes); free(order); free(tris);
     return -2;

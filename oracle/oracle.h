@@ -43,10 +43,14 @@ void orc_sincos_turns(float u, float* s, float* c);
 int orc_build_bvh(const float* world_pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris,
                   int32_t* nodes_out, uint32_t* order_out, float* tris_out /* 12*ntris or NULL */);
 
-/* Hierarchy of the BVHs built from now on: 0 PLOC clustering (default), 1
- * the Karras radix tree; the GPU builder's two methods. */
+/* Hierarchy of the BVHs built from now on: 0 PLOC clustering, 1 the Karras
+ * radix tree, -1 (default) PLOC for render scenes and Karras for filter
+ * scenes; the GPU builder's methods. */
 void orc_set_bvh_method(int method);
 int orc_get_bvh_method(void);
+/* orc_build_bvh for a filter scene (its default hierarchy under -1). */
+int orc_build_bvh_filter(const float* world_pos, uint32_t nverts, const uint32_t* idx, uint32_t ntris,
+                         int32_t* nodes_out, uint32_t* order_out, float* tris_out);
 
 /* Closest hit: returns BVH-order triangle or -1; t/b1/b2 out. */
 int orc_trace(const int32_t* nodes, const float* tris, float ox, float oy, float oz, float dx, float dy,

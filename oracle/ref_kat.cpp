@@ -371,7 +371,7 @@ int ref_filter_scene(const float* wpos, uint32_t nverts, const uint32_t* idx, ui
   fs.mats.emplace_back(new rt::CMaterial(V(kd), V(ks), rt::COrenNayarBRDF(0.f),
                                          rt::CMicrofacetBRDF(alpha, alpha, 1.f, ior)));
   fs.mask = rt::ESceneobjectMask::FILTER;
-  const int h = orc_build_bvh(wpos, nverts, idx, ntris, fs.nodes.data(), fs.order.data(), fs.tris.data());
+  const int h = orc_build_bvh_filter(wpos, nverts, idx, ntris, fs.nodes.data(), fs.order.data(), fs.tris.data());
   fs.ready = h >= 0;
   return h;
 }

@@ -297,9 +297,16 @@ __global__ void k_init_bounds(uint32_t* cb) {
 
 }  // namespace
 
-static std::atomic<int> g_bvhMethod{kBvhPloc};
+static std::atomic<int> g_bvhMethod{kBvhAuto};
 int bvh_method() { return g_bvhMethod.load(); }
-void set_bvh_method(int method) { g_bvhMethod.store(method == kBvhKarras ? kBvhKarras : kBvhPloc); }
+void set_bvh_method(int method) {
+  g_bvhMethod.store(method == kBvhKarras ? kBvhKarras : (method == kBvhPloc ? kBvhPloc : kBvhAuto));
+}
+int resolve_bvh_method(bool filterScene) {
+  const int m = bvh_method();
+  if (m != kBvhAuto) return m;
+  return filterScene ? kBvhKarras : kBvhPloc;
+}
 
 // Steps 3-7 over primitive boxes whose centroid bounds are in cb_; with
 // d_pos/d_idx the BVH-ordered triangle array is gathered too.
@@ -308,7 +315,7 @@ void BvhBuilder::from_boxes(const float4* triLo, const float4* triHi, uint32_t n
   const int n = (int)ntris;
   keys_.reserve(n);
   out->order.reserve(n);
-  const bool usePloc = n > 1 && bvh_method() == kBvhPloc;
+  const bool usePloc = n > 1 && resolve_bvh_method(filterScene_) == kBvhPloc;
   if (usePloc) sorted_.reserve(n);
   uint32_t* sorted = usePloc ? sorted_.get() : out->order.get();
   k_morton<<<(n + 255) / 256, 256, 0, s>>>(triLo, triHi, ntris, cb_.get(), keys_.get(), sorted);
@@ -401,8 +408,10 @@ void BvhBuilder::build_boxes(const float4* d_lo, const float4* d_hi, uint32_t nb
   from_boxes(d_lo, d_hi, nboxes, nullptr, nullptr, out, s);
 }
 
-void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s) {
+void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out, cudaStream_t s,
+               bool filterScene) {
   BvhBuilder b;
+  b.set_filter_scene(filterScene);
   b.build(d_pos, d_idx, ntris, out, s);
 }
 

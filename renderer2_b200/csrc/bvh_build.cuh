@@ -14,12 +14,17 @@ constexpr int kLeafMax = 8;
 // Window of the PLOC nearest-neighbour search: positions i - r .. i + r.
 constexpr int kPlocRadius = 16;
 
-// Hierarchy over the Morton-sorted primitives: PLOC clustering (default) or
-// the Karras radix tree.  Both end with the same SAH leaf collapse.
-enum BvhMethod { kBvhPloc = 0, kBvhKarras = 1 };
+// Hierarchy over the Morton-sorted primitives: PLOC clustering or the Karras
+// radix tree, both ending with the same SAH leaf collapse.  kBvhAuto (the
+// default) takes PLOC for render scenes and the Karras tree for filter scenes,
+// the faster choice of each (measured on the C2 scene and the C3 foliage).
+enum BvhMethod { kBvhAuto = -1, kBvhPloc = 0, kBvhKarras = 1 };
 // Process-wide choice for the BVHs built from now on.
 int bvh_method();
 void set_bvh_method(int method);
+// The hierarchy a build uses: the process-wide choice, or under kBvhAuto the
+// default of its purpose.
+int resolve_bvh_method(bool filterScene);
 
 // A triangle BVH resident in device memory.
 struct DeviceBvh {
@@ -57,6 +62,8 @@ class BvhBuilder {
                    int leafMax = kLeafMax);
   // Kernels the last build launched.
   int launches() const { return launches_; }
+  // BVHs of filter scenes (their kBvhAuto default differs).
+  void set_filter_scene(bool f) { filterScene_ = f; }
 
  private:
   void from_boxes(const float4* lo, const float4* hi, uint32_t n, const float* d_pos, const uint32_t* d_idx,
@@ -74,12 +81,13 @@ class BvhBuilder {
   void* hostState_ = nullptr;  // pinned copy of the PLOC iteration state
   int launches_ = 0;
   int leafMax_ = kLeafMax;
+  bool filterScene_ = false;
 };
 
 // Builds the BVH over triangles (d_pos: 3 floats per vertex, d_idx: 3 per
 // triangle, both device).  Deterministic: the result depends only on the input.
 void build_bvh(const float* d_pos, const uint32_t* d_idx, uint32_t ntris, DeviceBvh* out,
-               cudaStream_t stream);
+               cudaStream_t stream, bool filterScene = false);
 
 // The same hierarchy over boxes (d_lo/d_hi: one float4 per box, xyz used,
 // device): leaves reference BVH positions, order[] maps them to box indices;

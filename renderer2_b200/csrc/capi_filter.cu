@@ -47,12 +47,16 @@ int r2_version(void) { return 100; }
 
 r2_status r2_set_bvh_method(int method) {
   R2_API_BEGIN
-  R2_REQUIRE(method == R2_BVH_PLOC || method == R2_BVH_KARRAS, R2_ERR_INVALID_ARGUMENT, "unknown BVH method");
-  r2::set_bvh_method(method == R2_BVH_KARRAS ? r2::kBvhKarras : r2::kBvhPloc);
+  R2_REQUIRE(method == R2_BVH_AUTO || method == R2_BVH_PLOC || method == R2_BVH_KARRAS, R2_ERR_INVALID_ARGUMENT,
+             "unknown BVH method");
+  r2::set_bvh_method(method == R2_BVH_KARRAS ? r2::kBvhKarras : (method == R2_BVH_PLOC ? r2::kBvhPloc : r2::kBvhAuto));
   R2_API_END
 }
 
-int r2_get_bvh_method(void) { return r2::bvh_method() == r2::kBvhKarras ? R2_BVH_KARRAS : R2_BVH_PLOC; }
+int r2_get_bvh_method(void) {
+  const int m = r2::bvh_method();
+  return m == r2::kBvhKarras ? R2_BVH_KARRAS : (m == r2::kBvhPloc ? R2_BVH_PLOC : R2_BVH_AUTO);
+}
 
 r2_status r2_filter_setup_grid(const float* model_bb_min, const float* model_bb_max, const float* model_to_world,
                                float voxel_size, r2_filter_grid* grid_out) {

@@ -84,7 +84,7 @@ FilterScene::FilterScene(const float* positions, uint32_t nverts, const uint32_t
   DBuf<uint32_t> didx;
   dpos.upload(wpos.data(), wpos.size(), stream_);
   didx.upload(indices, (size_t)3 * ntris, stream_);
-  build_bvh(dpos.get(), didx.get(), ntris, &bvh_, stream_);
+  build_bvh(dpos.get(), didx.get(), ntris, &bvh_, stream_, true);
   // per BVH-order triangle: model-space vertex normals and material
   std::vector<uint32_t> order(ntris);
   bvh_.order.download(order.data(), ntris, stream_);

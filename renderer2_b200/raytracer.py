@@ -22,12 +22,12 @@ class RenderParams(C.Structure):
     _fields_ = [("spp", C.c_uint32), ("max_depth", C.c_uint32), ("seed", C.c_uint32), ("flags", C.c_uint32)]
 
 
-BVH_PLOC, BVH_KARRAS = 0, 1
+BVH_AUTO, BVH_PLOC, BVH_KARRAS = -1, 0, 1
 
 
 def set_bvh_method(method: int):
     """Hierarchy of the BVHs built from now on, process-wide (r2_set_bvh_method):
-    BVH_PLOC (default) or BVH_KARRAS."""
+    BVH_AUTO (default: PLOC for render scenes, Karras for filter scenes), BVH_PLOC or BVH_KARRAS."""
     N.check(N.lib.r2_set_bvh_method(int(method)))
 
 

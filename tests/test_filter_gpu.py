@@ -104,8 +104,8 @@ def bvh_method(request):
     N.check(N.lib.r2_set_bvh_method(request.param))
     O.lib.orc_set_bvh_method(request.param)
     yield request.param
-    N.check(N.lib.r2_set_bvh_method(0))
-    O.lib.orc_set_bvh_method(0)
+    N.check(N.lib.r2_set_bvh_method(-1))
+    O.lib.orc_set_bvh_method(-1)
 
 
 @pytest.mark.parametrize("mesh_kind", ["ico4", "foliage", "foliage_big", "single", "pair", "dupes"])

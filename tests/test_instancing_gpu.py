@@ -29,8 +29,8 @@ def test_instanced_scene_matches_oracle(method):
         sc.close()
         o = O.render(desc, cam, 4, 6, 3)
     finally:
-        R.set_bvh_method(R.BVH_PLOC)
-        O.lib.orc_set_bvh_method(0)
+        R.set_bvh_method(R.BVH_AUTO)
+        O.lib.orc_set_bvh_method(-1)
     frac = _agree(g, o)
     print(f"two-level ({nodes} nodes, height {height}, {launches} build launches): {frac:.5f} of pixels within 1e-4")
     assert frac >= 0.999

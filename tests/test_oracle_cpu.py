@@ -80,7 +80,7 @@ def _brute(pos, idx, o, d, tmax, tris, order):
 def bvh_method(request):
     O.lib.orc_set_bvh_method(request.param)
     yield request.param
-    O.lib.orc_set_bvh_method(0)
+    O.lib.orc_set_bvh_method(-1)
 
 
 @pytest.mark.parametrize("n", [1, 2, 7, 64, 600])
@@ -140,7 +140,7 @@ def test_ploc_tree_structure_and_quality():
         O.lib.orc_set_bvh_method(meth)
         nodes, order, _, h = O.build_bvh(pos, idx)
         cost[meth] = _sah_cost(nodes)
-    O.lib.orc_set_bvh_method(0)
+    O.lib.orc_set_bvh_method(-1)
     n = idx.shape[0]
     assert np.array_equal(np.sort(order), np.arange(n))
     covered = np.zeros(n, np.int32)
