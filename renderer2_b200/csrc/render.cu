@@ -798,7 +798,9 @@ __global__ void __launch_bounds__(128) k_track(RenderLaunch L, int round) {
 
 // Surface shading: direct() at a surface and the sampleF continuation
 // (path_integrator_impl.hpp:23-118, 196-222).
-template <bool kMedia>
+// kTex: the scene has texture coordinates; kInst: two levels (otherwise those
+// branches are compiled out of the instantiation).
+template <bool kMedia, bool kTex, bool kInst>
 __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i, uint32_t p, int code, float4 hr,
                                               V3 o, V3 d, int med, V3 T) {
   const V3 pos = o + d * hr.x;
@@ -806,7 +808,7 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
   Material m;
   if (code >= 0) {
     int tri = code, inst = -1;
-    if (L.scene.bvh.inst) {  // the instance of the code, and the triangle's BVH-order index
+    if (kInst && L.scene.bvh.inst) {  // the instance of the code, and the triangle's BVH-order index
       int lo = 0, hi = L.scene.ninst - 1;
       while (lo < hi) {  // last instance whose first code is <= code
         const int mid = (lo + hi + 1) >> 1;
@@ -822,7 +824,7 @@ __device__ __forceinline__ bool shade_surface(const RenderLaunch& L, uint32_t i,
     const float b0 = (1.0f - hr.y) - hr.z;
     n = normalize(xyz(n0) * b0 + xyz(n1) * hr.y + xyz(n2) * hr.z);
     m = L.scene.mats[__ldg(&L.scene.triMat[tri])];
-    if (L.scene.triUV && (m.tex[0] >= 0 || m.tex[1] >= 0 || m.tex[2] >= 0)) {
+    if (kTex && L.scene.triUV && (m.tex[0] >= 0 || m.tex[1] >= 0 || m.tex[2] >= 0)) {
       const TexView tv = {L.scene.triUV, L.scene.texels, L.scene.texInfo, L.scene.bvh.tris};
       const TexShade ts = textured_surface(tv, m.tex[0], m.tex[1], m.tex[2], tri, hr.y, hr.z, n, m.diffuse, m.specular);
       n = ts.n;
@@ -1025,7 +1027,7 @@ __global__ void __launch_bounds__(256) k_events(RenderLaunch L) {
 // Register caps (64 a thread without media): the few spilled values of the
 // rare branches cost less than the warps gained (16-sample wave of the
 // 327,680-triangle scene: shading 5.8 -> 4.7 ms).
-template <bool kMedia>
+template <bool kMedia, bool kTex, bool kInst>
 __global__ void __launch_bounds__(128, kMedia ? 6 : 8) k_shade(RenderLaunch L) {
   // the bounce's events: misses and ended paths were finished by k_extend / k_events
   const uint32_t n = event_count(L);
@@ -1055,7 +1057,7 @@ __global__ void __launch_bounds__(128, kMedia ? 6 : 8) k_shade(RenderLaunch L) {
       } else if (kMedia && code == kEventScatter) {
         cont = shade_scatter(L, i, p, d, T);
       } else {
-        cont = shade_surface<kMedia>(L, i, p, code, hr, o, d, __float_as_int(ro.w), T);
+        cont = shade_surface<kMedia, kTex, kInst>(L, i, p, code, hr, o, d, __float_as_int(ro.w), T);
       }
     }
     push_queue(qn, cn, cont, p);
@@ -1284,6 +1286,16 @@ const RenderKernel kShadowVariants[9] = {
     k_shadow_surfaces<true, false, true, true>,   k_shadow_surfaces<true, true, true, true>,
     k_shadow_surfaces<false, false, false, false>};
 
+// k_shade by variant: 4 * media + textured + 2 * two-level.
+const RenderKernel kShadeVariants[8] = {k_shade<false, false, false>, k_shade<false, true, false>,
+                                        k_shade<false, false, true>,  k_shade<false, true, true>,
+                                        k_shade<true, false, false>,  k_shade<true, true, false>,
+                                        k_shade<true, false, true>,   k_shade<true, true, true>};
+
+int shade_variant(const RenderLaunch& L) {
+  return (L.scene.triUV ? 1 : 0) + (L.scene.bvh.inst ? 2 : 0);
+}
+
 int trav_variant(const RenderLaunch& L) {
   if (!L.scene.hasTris) return 8;
   return (L.scene.bvh.alpha.alphaTex ? 1 : 0) + (L.scene.bvh.inst ? 2 : 0) + (L.topNodes ? 4 : 0);
@@ -1369,7 +1381,7 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
       else k_collide<false><<<nblocks * 2, 128, 0, s>>>(L);
       k_events<<<nblocks, 256, 0, s>>>(L);
       mark(1);
-      k_shade<true><<<nblocks * 2, 128, 0, s>>>(L);
+      kShadeVariants[4 + shade_variant(L)]<<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
       k_shadow_resolve<true, false><<<nblocks * 2, 128, 0, s>>>(L, 0);
       for (int r = 0; r < rounds; ++r) {
@@ -1382,7 +1394,7 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
       kExtendVariants[tv]<<<std::min(nblocks * 2, trav_blocks(0, tv, L.topNodes)), 128,
                             L.topNodes * sizeof(BvhNode), s>>>(L);
       mark(1);
-      k_shade<false><<<nblocks * 2, 128, 0, s>>>(L);
+      kShadeVariants[shade_variant(L)]<<<nblocks * 2, 128, 0, s>>>(L);
       mark(2);
       kShadowVariants[tv]<<<std::min(nblocks * 2, trav_blocks(1, tv, L.topNodes)), 128,
                             L.topNodes * sizeof(BvhNode), s>>>(L);
