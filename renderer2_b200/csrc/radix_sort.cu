@@ -190,6 +190,17 @@ void RadixSortScratch::reserve(uint32_t n) {
   partials.reserve((L + kScanPart - 1) / kScanPart);
 }
 
+void exclusive_scan_inplace(uint32_t* data, uint32_t n, DBuf<uint32_t>* partials, cudaStream_t s) {
+  if (n == 0) return;
+  const uint32_t np = (n + kScanPart - 1) / kScanPart;
+  R2_REQUIRE(np <= (uint32_t)kScanPart, R2_ERR_UNSUPPORTED, "prefix sum of more than 2^24 words");
+  partials->reserve(np);
+  k_rs_reduce<<<np, kScanThreads, 0, s>>>(data, n, partials->get());
+  k_rs_partials<<<1, kScanThreads, 0, s>>>(partials->get(), np);
+  k_rs_down<<<np, kScanThreads, 0, s>>>(data, n, partials->get());
+  R2_CUDA(cudaGetLastError());
+}
+
 int radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint32_t n, int bits, RadixSortScratch* scr, cudaStream_t s) {
   R2_REQUIRE(bits >= 1 && bits <= 64, R2_ERR_INVALID_ARGUMENT, "radix sort key bits must be in [1, 64]");
   if (n <= 1) return 0;

@@ -14,6 +14,10 @@ struct RadixSortScratch {
   void reserve(uint32_t n);
 };
 
+// data[0..n) becomes its exclusive prefix sum (n <= 2^24; partials: scratch,
+// grown as needed), with the sort's reduce-then-scan kernels.
+void exclusive_scan_inplace(uint32_t* data, uint32_t n, DBuf<uint32_t>* partials, cudaStream_t s);
+
 // Sorts n pairs ascending by the low `bits` bits of the keys (1..64), stably:
 // equal keys keep their input order.  In place: keys/vals hold the sorted
 // pairs when the stream reaches the end of the sort.  Returns the number of

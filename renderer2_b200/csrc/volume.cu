@@ -7,9 +7,9 @@
 
 #include <algorithm>
 
-#include <cub/device/device_scan.cuh>
 
 #include "filter_math.h"
+#include "radix_sort.cuh"
 #include "volume.h"
 
 namespace r2 {
@@ -264,10 +264,10 @@ void build_brick_grid(const r2_voxel* d_dense, const int32_t nv[3], cudaStream_t
   int blocks = (int)std::min<size_t>((nB + 127) / 128, (size_t)sm_count() * 16);
   k_brick_range<<<std::max(blocks, 1), 128, 0, s>>>(d_dense, nv[0], nv[1], nv[2], nb[0], nb[1], nb[2], range.get(),
                                                     nonconst.get());
-  size_t tmpBytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tmpBytes, nonconst.get(), slot.get(), (int)nB, s);
-  DBuf<uint8_t> tmp(tmpBytes);
-  R2_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tmpBytes, nonconst.get(), slot.get(), (int)nB, s));
+  R2_REQUIRE(nB <= (1u << 24), R2_ERR_UNSUPPORTED, "brick grid of more than 2^24 bricks");
+  R2_CUDA(cudaMemcpyAsync(slot.get(), nonconst.get(), nB * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  DBuf<uint32_t> partials;
+  exclusive_scan_inplace(slot.get(), (uint32_t)nB, &partials, s);
   uint32_t lastSlot = 0, lastFlag = 0;
   R2_CUDA(cudaMemcpyAsync(&lastSlot, slot.get() + nB - 1, 4, cudaMemcpyDeviceToHost, s));
   R2_CUDA(cudaMemcpyAsync(&lastFlag, nonconst.get() + nB - 1, 4, cudaMemcpyDeviceToHost, s));
