@@ -535,7 +535,8 @@ def bench_render(args, world, local):
     s2.close()
     e2e["cold_start"] = {"value": world * paths / (t2 - t0), "scene_build_ms": (t1 - t0) * 1e3,
                          "render_and_download_ms": (t2 - t1) * 1e3, "h2d_bytes": int(_input_bytes(desc))}
-    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth) + bvh_launches
+    sort_launches = 4 * (prm.max_depth - 1) if tuning.get("sort_rays") else 0  # ray sort before bounces 1..
+    launches_per_step = (prm.spp // S) * (2 + 4 * prm.max_depth + sort_launches) + bvh_launches
     return dict(value=value, total_ms=total_ms, roofline=roofline, e2e=e2e, clocks=ck, paths=paths, tuning=tuning,
                 latency=latency,
                 segments_per_frame=seg, shadow_rays_per_frame=shadow, launches=launches_per_step * args.steps,
@@ -770,7 +771,8 @@ def bench_small(args, world, local):
                                               + pos.nbytes + nrm.nbytes),
                     "d2h_bytes_per_step": int(nvox * 32 + npix * 12)},
             "accuracy": acc, "cpu_baseline": cpu,
-            "gpu_launches": (2 + bvh_launches + (c["spp"] // S) * (2 + 4 * c["depth"])) * args.steps}
+            "gpu_launches": (2 + bvh_launches + (c["spp"] // S) * (2 + 4 * c["depth"] + (
+                4 * (c["depth"] - 1) if tuning.get("sort_rays") else 0))) * args.steps}
 
 
 def media_roofline(st, S, spp, depth):

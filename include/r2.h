@@ -306,6 +306,9 @@ typedef struct r2_render_tuning {
                            shared memory and read from there (0: off; at most 256).  With the PLOC
                            builder a parent's index is below its children's, so these are the top
                            levels of the tree (of the top-level tree in two-level scenes). */
+  uint32_t sort_rays;   /* surface scenes: 1 reorders each bounce's rays after the first by direction
+                           octant, dominant axis and origin cell before tracing them (a counting sort
+                           over 256 keys); 0: off.  The order of rays changes no bit of a frame. */
 } r2_render_tuning;
 
 /* "UseBrickGrid" of config.json: media are tracked with the brick-grid DDA

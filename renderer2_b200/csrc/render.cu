@@ -435,6 +435,95 @@ __device__ __forceinline__ void trace_scene(const RenderLaunch& L, uint32_t n, u
   trace_persistent<kAnyHit, kAlpha, kInst, kTop>(bvh, n, taken, trav_visits(L), trav_refill(L), L.bound, begin, end);
 }
 
+// ------------------------------------------------------------------ ray order
+// Coherence order of a bounce's rays (tuning sort_rays): the path queue is
+// reordered by an 8-bit key — direction octant (3 bits), dominant axis
+// (2 bits) and the origin's octant of the scene box (3 bits) — with a counting
+// sort: block histograms, one scan of the 256 bins, a scatter.  Positions
+// within a bin depend on atomic order; no result depends on the order of the
+// rays (each path keeps its own random streams and the frame adds samples per
+// pixel in sample order).
+__device__ __forceinline__ uint32_t ray_key(V3 o, V3 d, V3 mid) {
+  const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  const V3 a = vabs(d);
+  const uint32_t axis = a.x >= a.y ? (a.x >= a.z ? 0u : 2u) : (a.y >= a.z ? 1u : 2u);
+  const uint32_t cell = (o.x < mid.x ? 0u : 1u) | (o.y < mid.y ? 0u : 2u) | (o.z < mid.z ? 0u : 4u);
+  return (cell << 5) | (axis << 3) | oct;
+}
+
+__device__ __forceinline__ V3 scene_mid(const SceneView& S) {
+  const BvhNode nd = S.bvh.nodes[0];
+  const bool two = nd.ch.y != R2_BVH_NONE;
+  const V3 lo = two ? v3(fminf(nd.b0.x, nd.b1.x), fminf(nd.b0.z, nd.b1.z), fminf(nd.bz.x, nd.bz.z))
+                    : v3(nd.b0.x, nd.b0.z, nd.bz.x);
+  const V3 hi = two ? v3(fmaxf(nd.b0.y, nd.b1.y), fmaxf(nd.b0.w, nd.b1.w), fmaxf(nd.bz.y, nd.bz.w))
+                    : v3(nd.b0.y, nd.b0.w, nd.bz.y);
+  return (lo + hi) * 0.5f;
+}
+
+__global__ void __launch_bounds__(256) k_sort_hist(RenderLaunch L) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
+  const uint32_t* q = path_queue(L, L.bounce);
+  const V3 mid = scene_mid(L.scene);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t p = q[i];
+    atomicAdd(&h[ray_key(xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), mid)], 1u);
+  }
+  __syncthreads();
+  if (h[threadIdx.x]) atomicAdd(&L.st.sortBins[threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void __launch_bounds__(256) k_sort_scan(RenderLaunch L) {
+  __shared__ uint32_t w[8];
+  const uint32_t v = L.st.sortBins[threadIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) w[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  for (int k = 0; k < warp; ++k) before += w[k];
+  L.st.sortBins[threadIdx.x] = before + x - v;  // exclusive: the bin's first position
+}
+
+// Each block takes its keys' positions from the bins' cursors with one atomic
+// per bin, then places its rays with shared-memory cursors.
+__global__ void __launch_bounds__(256) k_sort_scatter(RenderLaunch L) {
+  __shared__ uint32_t h[256], base[256];
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
+  const uint32_t* q = path_queue(L, L.bounce);
+  const V3 mid = scene_mid(L.scene);
+  for (uint32_t b0 = blockIdx.x * blockDim.x; b0 < n; b0 += gridDim.x * blockDim.x) {
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t i = b0 + threadIdx.x;
+    uint32_t p = 0, key = 0, rank = 0;
+    if (i < n) {
+      p = q[i];
+      key = ray_key(xyz(L.st.rayO[p]), xyz(L.st.rayD[p]), mid);
+      rank = atomicAdd(&h[key], 1u);
+    }
+    __syncthreads();
+    if (h[threadIdx.x]) base[threadIdx.x] = atomicAdd(&L.st.sortBins[threadIdx.x], h[threadIdx.x]);
+    __syncthreads();
+    if (i < n) L.st.qs[base[key] + rank] = p;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sort_copy(RenderLaunch L) {
+  const uint32_t n = *(volatile uint32_t*)&L.st.counts[L.bounce];
+  uint32_t* q = path_queue(L, L.bounce);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) q[i] = L.st.qs[i];
+}
+
 // Closest hit of every live path (scenes without media).  A path that hits a
 // surface goes to the bounce's hit queue (shading, shadow rays and
 // accumulation then run over hits only); a miss ends the path here with the
@@ -1390,6 +1479,13 @@ void launch_render_wave(const RenderLaunch& L0, int nblocks, cudaStream_t s, Wav
         else k_shadow_resolve<false, true><<<nblocks * 2, 128, 0, s>>>(L, r + 1);
       }
     } else {
+      if (L.sortRays && b > 0) {
+        R2_CUDA(cudaMemsetAsync(L.st.sortBins, 0, 256 * sizeof(uint32_t), s));
+        k_sort_hist<<<nblocks, 256, 0, s>>>(L);
+        k_sort_scan<<<1, 256, 0, s>>>(L);
+        k_sort_scatter<<<nblocks, 256, 0, s>>>(L);
+        k_sort_copy<<<nblocks, 256, 0, s>>>(L);
+      }
       const int tv = trav_variant(L);
       kExtendVariants[tv]<<<std::min(nblocks * 2, trav_blocks(0, tv, L.topNodes)), 128,
                             L.topNodes * sizeof(BvhNode), s>>>(L);

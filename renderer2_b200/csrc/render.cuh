@@ -53,7 +53,8 @@ struct PathState {
                     // kEventScatter medium collision, kEventDead path ended by a medium rule)
   uint32_t* q[2];   // ping-pong queues of live path ids
   uint32_t* qh;     // paths of the bounce that hit a surface (k_extend, or k_events with media)
-  uint32_t* qs;     // media: paths of the bounce with a medium collision (k_events)
+  uint32_t* qs;     // media: paths of the bounce with a medium collision (k_events); surfaces: ray sort output
+  uint32_t* sortBins;  // 256 key counters of the ray sort
   uint32_t* counts; // [bounce] live path count entering the bounce; from kTravCounters on,
                     // per bounce the rays taken by the persistent surface traversals
   // shadow records, two per queue slot (0: light sample, 1: BSDF sample)
@@ -137,6 +138,7 @@ struct RenderLaunch {
   uint32_t trackBlocks; // persistent tracker blocks per SM (tuning; 0: every resident block)
   uint32_t trackLimit;  // steps of one tracking loop after which the path ends (1..kMaxTrackingSteps)
   uint32_t topNodes;    // BVH nodes staged in shared memory by the surface traversals (0: none, <= kMaxTopNodes)
+  uint32_t sortRays;    // surface scenes: reorder each bounce's rays by a coherence key before k_extend
   unsigned long long* stats;  // nullable: [0] path segments traced, [1] shadow rays traced
   unsigned int* bound;        // paths and shadow rays ended by a loop bound (tracking steps, boundaries)
 };

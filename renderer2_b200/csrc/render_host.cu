@@ -630,6 +630,7 @@ void RenderContext::ensure(uint32_t n, bool media) {
     shO_.alloc(2 * (size_t)n); shD_.alloc(2 * (size_t)n); shPre_.alloc(2 * (size_t)n); shT_.alloc(n);
     q0_.alloc(n); q1_.alloc(n); qh_.alloc(n); qs_.alloc(n); shTr_.alloc(2 * (size_t)n);
     counts_.alloc(kCountsSize);
+    sortBins_.alloc(256);
     cap_ = n;
   }
   if (media && n > mediaCap_) {
@@ -656,6 +657,7 @@ size_t RenderContext::bytes_for(uint32_t n, bool media) {
 void RenderContext::fill(PathState* st) const {
   st->rayO = rayO_.get(); st->rayD = rayD_.get(); st->T = T_.get(); st->L = L_.get(); st->hit = hit_.get();
   st->q[0] = q0_.get(); st->q[1] = q1_.get(); st->qh = qh_.get(); st->qs = qs_.get(); st->counts = counts_.get();
+  st->sortBins = sortBins_.get();
   st->shO = shO_.get(); st->shD = shD_.get(); st->shPre = shPre_.get(); st->shT = shT_.get();
   st->shTr = shTr_.get();
   if (mediaCap_ > 0) {
@@ -717,6 +719,7 @@ RenderLaunch RenderScene::make_launch(const RenderContext& ctx, const r2_camera&
   L.trackLimit = tuning_.track_limit ? tuning_.track_limit : (uint32_t)kMaxTrackingSteps;
   // shared-memory top nodes: surface scenes only, within the tree
   L.topNodes = media_.empty() && view_.hasTris ? std::min(tuning_.top_nodes, bvhNodes_) : 0u;
+  L.sortRays = media_.empty() && view_.hasTris && tuning_.sort_rays ? 1u : 0u;
   L.bound = ctx.bound.get();
   return L;
 }
@@ -826,10 +829,10 @@ RenderLaunch RenderScene::prepare(RenderContext& ctx, const r2_camera& c, const 
 void RenderScene::set_tuning(const r2_render_tuning& t) {
   R2_REQUIRE(t.track_steps <= 1024 && t.trav_refill <= 32 && t.wave_paths < (1u << 31) &&
                  t.media_rounds <= kMaxMediaRounds && t.track_blocks <= 64 &&
-                 t.track_limit <= (uint32_t)kMaxTrackingSteps && t.top_nodes <= kMaxTopNodes,
+                 t.track_limit <= (uint32_t)kMaxTrackingSteps && t.top_nodes <= kMaxTopNodes && t.sort_rays <= 1,
              R2_ERR_INVALID_ARGUMENT,
              "tuning out of range (track_steps <= 1024, trav_refill <= 32, wave_paths < 2^31, media_rounds <= 32, "
-             "track_blocks <= 64, track_limit <= 2^20, top_nodes <= 256)");
+             "track_blocks <= 64, track_limit <= 2^20, top_nodes <= 256, sort_rays <= 1)");
   tuning_ = t;
 }
 
@@ -864,7 +867,7 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     return best / ((float)S * (float)npix);
   };
   r2_render_tuning cur{kDefaultTrackSteps, kDefaultTravVisits, kDefaultTravRefill, kDefaultWavePaths,
-                       kDefaultMediaRounds, 0, saved.track_limit, 0};  // the step bound is kept, never tuned
+                       kDefaultMediaRounds, 0, saved.track_limit, 0, 0};  // the step bound is kept, never tuned
   try {
     R2_CUDA(cudaMemsetAsync(ctx.bound.get(), 0, sizeof(unsigned int), s));
     time_wave(cur);  // warm-up
@@ -894,11 +897,13 @@ r2_render_tuning RenderScene::autotune(const r2_camera& c, const r2_render_param
     static const uint32_t rounds[] = {1, 4, 8, 16};
     static const uint32_t trackBlocks[] = {2, 3, 4, 6};
     static const uint32_t topNodes[] = {64, 128, 256};
+    static const uint32_t sortRays[] = {1};
     sweep(&r2_render_tuning::wave_paths, wavePaths, 4);
     if (media_.empty()) {  // the persistent surface traversals run in scenes without media
       sweep(&r2_render_tuning::trav_refill, refills, 4);
       sweep(&r2_render_tuning::trav_visits, visits, 4);
       sweep(&r2_render_tuning::top_nodes, topNodes, 3);
+      sweep(&r2_render_tuning::sort_rays, sortRays, 1);
     } else {
       sweep(&r2_render_tuning::media_rounds, rounds, 4);
       sweep(&r2_render_tuning::track_steps, steps, 4);

@@ -58,7 +58,7 @@ class RenderContext {
  private:
   uint32_t cap_ = 0, mediaCap_ = 0;
   DBuf<float4> rayO_, rayD_, T_, L_, hit_, shO_, shD_, shPre_, shT_;
-  DBuf<uint32_t> q0_, q1_, qh_, qs_, counts_;
+  DBuf<uint32_t> q0_, q1_, qh_, qs_, counts_, sortBins_;
   DBuf<float> shTr_;
   DBuf<float2> shX_, evD_;
   DBuf<float4> evA_, evB_, evC_;
@@ -209,7 +209,7 @@ class RenderScene {
   DBuf<float> envBuf_;
   DBuf<float> hostFrame_;
   SceneView view_;
-  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
+  r2_render_tuning tuning_{0, 0, 0, 0, 0, 0, 0, 0, 0};  // 0 fields: the kernels' defaults
 };
 
 // Frames of several committed scenes rendered by one captured CUDA graph: the

@@ -61,9 +61,9 @@ class Tuning(C.Structure):
     """Launch tuning (r2_render_tuning); 0 fields select the defaults; images never depend on it."""
     _fields_ = [("track_steps", C.c_uint32), ("trav_visits", C.c_uint32), ("trav_refill", C.c_uint32),
                 ("wave_paths", C.c_uint32), ("media_rounds", C.c_uint32), ("track_blocks", C.c_uint32),
-                ("track_limit", C.c_uint32), ("top_nodes", C.c_uint32)]
+                ("track_limit", C.c_uint32), ("top_nodes", C.c_uint32), ("sort_rays", C.c_uint32)]
     NAMES = ("track_steps", "trav_visits", "trav_refill", "wave_paths", "media_rounds", "track_blocks",
-             "track_limit", "top_nodes")
+             "track_limit", "top_nodes", "sort_rays")
 
     def as_tuple(self):
         return tuple(getattr(self, n) for n in self.NAMES)
@@ -73,9 +73,9 @@ class Tuning(C.Structure):
 
 
 def tuning(track_steps=0, trav_visits=0, trav_refill=0, wave_paths=0, media_rounds=0, track_blocks=0,
-           track_limit=0, top_nodes=0) -> Tuning:
+           track_limit=0, top_nodes=0, sort_rays=0) -> Tuning:
     return Tuning(track_steps, trav_visits, trav_refill, wave_paths, media_rounds, track_blocks, track_limit,
-                  top_nodes)
+                  top_nodes, sort_rays)
 
 
 class Scene:

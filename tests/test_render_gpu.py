@@ -184,12 +184,12 @@ def test_launch_tuning_never_changes_the_frame():
     sc = RS.build_scene(desc)
     sc.set_tuning(R.tuning(wave_paths=96 * 80))  # one sample per wave
     ref = sc.render(cam, prm)
-    for visits, refill, wave, top in [(1, 1, 0, 0), (3, 32, 96 * 80, 64), (1000, 5, 2 * 96 * 80, 256),
-                                      (64, 16, 1 << 24, 7)]:
-        sc.set_tuning(R.tuning(trav_visits=visits, trav_refill=refill, wave_paths=wave, top_nodes=top))
-        assert sc.get_tuning().as_tuple() == (0, visits, refill, wave, 0, 0, 0, top)
+    for visits, refill, wave, top, srt in [(1, 1, 0, 0, 1), (3, 32, 96 * 80, 64, 0), (1000, 5, 2 * 96 * 80, 256, 1),
+                                           (64, 16, 1 << 24, 7, 1)]:
+        sc.set_tuning(R.tuning(trav_visits=visits, trav_refill=refill, wave_paths=wave, top_nodes=top, sort_rays=srt))
+        assert sc.get_tuning().as_tuple() == (0, visits, refill, wave, 0, 0, 0, top, srt)
         assert sc.wave_samples(cam, prm) == (2 if wave != 96 * 80 else 1)
-        assert np.array_equal(sc.render(cam, prm), ref), (visits, refill, wave, top)
+        assert np.array_equal(sc.render(cam, prm), ref), (visits, refill, wave, top, srt)
     t = sc.autotune(cam, prm)
     assert 1 <= t.trav_refill <= 32 and t.trav_visits >= 1
     assert sc.get_tuning().as_tuple() == t.as_tuple()
@@ -199,4 +199,6 @@ def test_launch_tuning_never_changes_the_frame():
         sc.set_tuning(R.tuning(trav_refill=33))
     with pytest.raises(N.R2Error):
         sc.set_tuning(R.tuning(top_nodes=257))
+    with pytest.raises(N.R2Error):
+        sc.set_tuning(R.tuning(sort_rays=2))
     sc.close()
