@@ -13,10 +13,15 @@
 //    warp-aggregated atomics (ballot + popc).
 //  * k_filter_sample: a persistent kernel; each warp pops one voxel at a time
 //    from the work list and its 32 lanes trace the voxel's samples (lane l owns
-//    samples l, l+32, ...), so a warp's rays share one BVH neighbourhood.  Hit
-//    ray lengths live in shared memory (no 4 KB per-thread local array).  Sums
-//    are compensated per lane and across the warp (TwoSum butterfly).  The
-//    density fit runs its iterations as warp reductions.
+//    samples l, l+32, ...), so a warp's rays share one BVH neighbourhood.  The
+//    warp first collects the triangles whose boxes overlap the box that holds
+//    all of the voxel's rays (at most kCandMax, in shared memory); every ray
+//    then tests exactly those, the lanes in step, instead of walking the BVH
+//    on its own.  Voxels with more candidates trace through the BVH from the
+//    deepest node that holds them.  Hit ray lengths live in shared memory (no
+//    4 KB per-thread local array).  Sums are compensated per lane and across
+//    the warp (TwoSum butterfly).  The density fit runs its iterations as warp
+//    reductions.
 #include "filter.cuh"
 #include "filter_math.h"
 #include "texture_shade.cuh"
@@ -25,6 +30,7 @@ namespace r2 {
 namespace {
 
 constexpr int kSampleWarps = 4;  // warps per block of the sampling kernel
+constexpr int kCandMax = 512;    // candidate triangles of a voxel tested without the BVH
 
 __device__ __forceinline__ V3 voxel_center(const FilterLaunch& L, int x, int y, int z) {
   V3 pm = xform_point(L.indexToModel, v3((float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f));
@@ -92,6 +98,80 @@ __device__ int bvh_local_root(const BvhView& bvh, V3 qlo, V3 qhi) {
     cur = h0 ? ch.x : ch.y;
   }
   return cur;
+}
+
+// The candidate triangles of a voxel: every triangle whose box overlaps the
+// query box [qlo, qhi], which holds every sample ray of the voxel, so these
+// are all the triangles its rays can hit.  A depth-first walk from root that
+// every lane of the warp takes in step (same nodes, same branches); the
+// triangles of a leaf are tested one per lane and appended in order to list.
+// Returns their number, or -1 as soon as there are more than kCandMax (the
+// caller then traces the voxel's rays through the BVH).  nodes: inner nodes
+// visited (the counting build; lane 0 counts).
+__device__ int gather_candidates(const BvhView& bvh, int root, V3 qlo, V3 qhi, int* list, int lane,
+                                 uint32_t* nodes) {
+  int stack[R2_BVH_STACK];
+  int sp = 0;
+  int cur = root;
+  int n = 0;
+  while (true) {
+    if (cur >= 0) {
+      if (lane == 0) ++*nodes;
+      const BvhNode* nd = &bvh.nodes[cur];
+      const float4 b0 = __ldg(&nd->b0), b1 = __ldg(&nd->b1), bz = __ldg(&nd->bz);
+      const int4 ch = __ldg(&nd->ch);
+      const bool h0 = box_overlap(b0.x, b0.y, b0.z, b0.w, bz.x, bz.y, qlo, qhi);
+      const bool h1 = ch.y != R2_BVH_NONE && box_overlap(b1.x, b1.y, b1.z, b1.w, bz.z, bz.w, qlo, qhi);
+      if (h0 && h1) {
+        stack[sp++] = ch.y;
+        cur = ch.x;
+        continue;
+      }
+      if (h0 || h1) {
+        cur = h0 ? ch.x : ch.y;
+        continue;
+      }
+    } else {
+      const int first = bvh_leaf_first(cur), count = bvh_leaf_count(cur);  // count <= 31 < 32 lanes
+      bool ov = false;
+      if (lane < count) {
+        const int t = first + lane;
+        const float4 a = __ldg(&bvh.tris[3 * t]), b = __ldg(&bvh.tris[3 * t + 1]), c = __ldg(&bvh.tris[3 * t + 2]);
+        ov = box_overlap(fminf(fminf(a.x, b.x), c.x), fmaxf(fmaxf(a.x, b.x), c.x), fminf(fminf(a.y, b.y), c.y),
+                         fmaxf(fmaxf(a.y, b.y), c.y), fminf(fminf(a.z, b.z), c.z), fmaxf(fmaxf(a.z, b.z), c.z), qlo,
+                         qhi);
+      }
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, ov);
+      const int k = __popc(m);
+      if (n + k > kCandMax) return -1;
+      if (ov) list[n + __popc(m & ((1u << lane) - 1u))] = first + lane;
+      n += k;
+    }
+    if (sp == 0) break;
+    cur = stack[--sp];
+  }
+  return n;
+}
+
+// The closest hit of one ray among the candidate triangles list[0 .. n-1],
+// with the test and the (t, triangle) order of the BVH traversal: the same hit
+// as bvh_trace over the whole scene.  Every lane walks the same list.
+template <bool kAlpha>
+__device__ Hit trace_candidates(const BvhView& bvh, const int* list, int n, V3 o, V3 d, float tmax) {
+  const RayPre r = make_ray_pre(o, d);
+  Hit best;
+  best.t = tmax;
+  best.b1 = best.b2 = 0.0f;
+  best.tri = 0x7FFFFFFF;
+  bool found = false;
+  for (int c = 0; c < n; ++c) {
+    const int tri = list[c];
+    const float4 a = __ldg(&bvh.tris[3 * tri]), b = __ldg(&bvh.tris[3 * tri + 1]), e = __ldg(&bvh.tris[3 * tri + 2]);
+    if (tri_test<kAlpha>(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(e.x, e.y, e.z), tri, tri, &best, &bvh.alpha))
+      found = true;
+  }
+  if (!found) best.tri = -1;
+  return best;
 }
 
 __device__ __forceinline__ void write_voxel(r2_voxel* out, size_t vid, const r2_voxel& v) {
@@ -189,8 +269,10 @@ __device__ __forceinline__ CSum warp_csum(CSum v) {
 template <bool kCount, bool kEig>
 __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLaunch L) {
   __shared__ float ts[kSampleWarps][kFilterMaxSpv];
+  __shared__ int cand[kSampleWarps][kCandMax];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* myTs = ts[warp];
+  int* myCand = cand[warp];
   const uint32_t ncand = *(volatile uint32_t*)&L.counters[0];
   const float radius = 1.1f * length(L.voxelSize) / 2.0f;
   const float tMaxFixed = L.voxelSize.x;
@@ -210,7 +292,12 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
     // radius), padded for rounding: its traversal starts at the local root
     const float reach = L.clip ? radius : length(L.voxelSize) / 2.0f + tMaxFixed;
     const float pad = reach * 1.01f + 1e-5f * (fabsf(center.x) + fabsf(center.y) + fabsf(center.z) + 1.0f);
-    const int root = bvh_local_root(L.bvh, center - v3(pad), center + v3(pad));
+    const V3 qlo = center - v3(pad), qhi = center + v3(pad);
+    const int root = bvh_local_root(L.bvh, qlo, qhi);
+    // few candidate triangles (the usual case): every ray tests them all, the
+    // warp's lanes in step; otherwise the rays traverse the BVH from root
+    const int ncand = gather_candidates(L.bvh, root, qlo, qhi, myCand, lane, &cNodes);
+    __syncwarp();
 
     CSum S[6], nrm[3], dist;
     float dif[3] = {0.f, 0.f, 0.f}, spe[3] = {0.f, 0.f, 0.f}, rough = 0.f, ior = 0.f;
@@ -228,7 +315,14 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
       const V3 o = xform_point(L.indexToWorld, oi);
       const V3 d = uniform_sample_sphere(u01(r0.w), u01(r1.x));
       const float tmax = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
-      const Hit h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris, root);
+      Hit h;
+      if (ncand >= 0) {
+        h = L.bvh.alpha.alphaTex ? trace_candidates<true>(L.bvh, myCand, ncand, o, d, tmax)
+                                 : trace_candidates<false>(L.bvh, myCand, ncand, o, d, tmax);
+        if (kCount) cTris += (uint32_t)ncand;
+      } else {
+        h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris, root);
+      }
       if (kCount) ++cRays;
       float tsv = -1.0f;
       if (h.tri >= 0) {
