@@ -44,6 +44,35 @@ r2_filter_grid setup_grid(V3 minWorld, V3 maxWorld, const M43& worldToModel43, f
   return g;
 }
 
+// World-space vertices of the filter scene (the filter traces in world space);
+// the same single-precision products and sums as the host's xform_point.
+__global__ void k_world_points(const float* model, uint32_t n, M43 m, float* world) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const V3 w = xform_point(m, v3(model[3 * v], model[3 * v + 1], model[3 * v + 2]));
+    world[3 * v] = w.x;
+    world[3 * v + 1] = w.y;
+    world[3 * v + 2] = w.z;
+  }
+}
+
+// Per BVH-order triangle: its model-space vertex normals and its material
+// (triMat null: material 0).
+__global__ void k_order_normals(const uint32_t* order, const uint32_t* idx, const float* nrm, const uint32_t* triMat,
+                                uint32_t n, float4* triN, uint32_t* triMatOut) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t p = order[i];
+    for (int k = 0; k < 3; ++k) {
+      const uint32_t v = idx[3 * p + k];
+      triN[3 * i + k] = make_float4(nrm[3 * v], nrm[3 * v + 1], nrm[3 * v + 2], 0.0f);
+    }
+    triMatOut[i] = triMat ? triMat[p] : 0u;
+  }
+}
+
+static int grid_for(uint32_t n) {
+  return (int)std::max<uint32_t>(1u, std::min<uint32_t>((n + 255) / 256, (uint32_t)sm_count() * 16));
+}
+
 // SAABB::transform (include/intersect/aabb.hpp:9-13): only the min and max
 // corners are transformed.
 void world_aabb(V3 mlo, V3 mhi, const M43& modelToWorld, V3* wlo, V3* whi) {
@@ -62,49 +91,45 @@ FilterScene::FilterScene(const float* positions, uint32_t nverts, const uint32_t
   R2_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   modelToWorld_ = m43_from_floats(modelToWorld);
   worldToModel_ = m4_to_m43(m4_inverse(m43_to_m4(modelToWorld_)));
-  // model bounds and world-space vertices (the filter traces in world space)
+  // model bounds and argument checks on the host; the world-space vertices
+  // (the filter traces in world space) and the per-triangle gathers on the device
   V3 lo = v3(INFINITY), hi = v3(-INFINITY);
-  std::vector<float> wpos((size_t)3 * nverts);
   for (uint32_t v = 0; v < nverts; ++v) {
-    V3 p = v3(positions[3 * v], positions[3 * v + 1], positions[3 * v + 2]);
+    const V3 p = v3(positions[3 * v], positions[3 * v + 1], positions[3 * v + 2]);
     lo = vmin(lo, p);
     hi = vmax(hi, p);
-    V3 w = xform_point(modelToWorld_, p);
-    wpos[3 * v] = w.x;
-    wpos[3 * v + 1] = w.y;
-    wpos[3 * v + 2] = w.z;
   }
   for (size_t i = 0; i < (size_t)3 * ntris; ++i)
     R2_REQUIRE(indices[i] < nverts, R2_ERR_INVALID_ARGUMENT, "triangle index out of range");
+  if (triMaterial)
+    for (uint32_t i = 0; i < ntris; ++i)
+      R2_REQUIRE(triMaterial[i] < nmaterials, R2_ERR_INVALID_ARGUMENT, "material index out of range");
+  R2_REQUIRE(nmaterials > 0, R2_ERR_INVALID_ARGUMENT, "material index out of range");
   modelLo_ = lo;
   modelHi_ = hi;
   world_aabb(lo, hi, modelToWorld_, &worldLo_, &worldHi_);
   ntris_ = ntris;
-  DBuf<float> dpos;
-  DBuf<uint32_t> didx;
-  dpos.upload(wpos.data(), wpos.size(), stream_);
+  DBuf<float> dmodel, dpos, dnrm;
+  DBuf<uint32_t> didx, dmat;
+  dmodel.upload(positions, (size_t)3 * nverts, stream_);
+  dpos.alloc((size_t)3 * nverts);
+  k_world_points<<<grid_for(nverts), 256, 0, stream_>>>(dmodel.get(), nverts, modelToWorld_, dpos.get());
+  R2_CUDA(cudaGetLastError());
   didx.upload(indices, (size_t)3 * ntris, stream_);
   build_bvh(dpos.get(), didx.get(), ntris, &bvh_, stream_, true);
-  // per BVH-order triangle: model-space vertex normals and material
-  std::vector<uint32_t> order(ntris);
-  bvh_.order.download(order.data(), ntris, stream_);
-  R2_CUDA(cudaStreamSynchronize(stream_));
-  std::vector<float4> triN((size_t)3 * ntris);
-  std::vector<uint32_t> triMat(ntris);
-  for (uint32_t i = 0; i < ntris; ++i) {
-    uint32_t p = order[i];
-    for (int k = 0; k < 3; ++k) {
-      uint32_t v = indices[3 * p + k];
-      triN[3 * i + k] = make_float4(normals[3 * v], normals[3 * v + 1], normals[3 * v + 2], 0.0f);
-    }
-    uint32_t m = triMaterial ? triMaterial[p] : 0u;
-    R2_REQUIRE(m < nmaterials, R2_ERR_INVALID_ARGUMENT, "material index out of range");
-    triMat[i] = m;
-  }
-  triN_.upload(triN.data(), triN.size(), stream_);
-  triMat_.upload(triMat.data(), triMat.size(), stream_);
+  dnrm.upload(normals, (size_t)3 * nverts, stream_);
+  if (triMaterial) dmat.upload(triMaterial, ntris, stream_);
+  triN_.alloc((size_t)3 * ntris);
+  triMat_.alloc(ntris);
+  k_order_normals<<<grid_for(ntris), 256, 0, stream_>>>(bvh_.order.get(), didx.get(), dnrm.get(),
+                                                        triMaterial ? dmat.get() : nullptr, ntris, triN_.get(),
+                                                        triMat_.get());
+  R2_CUDA(cudaGetLastError());
   mats_.upload(materials, nmaterials, stream_);
   if (maps && uvs) {  // texture maps per material (CMaterial(aiMaterial*), material.cu:110-143)
+    std::vector<uint32_t> order(ntris);
+    bvh_.order.download(order.data(), ntris, stream_);
+    R2_CUDA(cudaStreamSynchronize(stream_));
     std::vector<int4> mt(nmaterials);
     bool anyTex = false, anyAlpha = false;
     for (uint32_t m = 0; m < nmaterials; ++m) {
@@ -123,7 +148,7 @@ FilterScene::FilterScene(const float* positions, uint32_t nverts, const uint32_t
           const uint32_t v = indices[3 * p + k];
           triUV[3 * i + k] = make_float2(uvs[2 * v], uvs[2 * v + 1]);
         }
-        triAlpha[i] = mt[triMat[i]].w;
+        triAlpha[i] = mt[triMaterial ? triMaterial[p] : 0u].w;
       }
       triUV_.upload(triUV.data(), triUV.size(), stream_);
       matTex_.upload(mt.data(), mt.size(), stream_);
