@@ -215,6 +215,34 @@ def test_counting_build_gives_the_same_payload_and_consistent_counts():
     assert nodes >= rays and tris > 0
 
 
+def test_candidate_lists_and_per_ray_traversal_both_match_the_oracle():
+    """A voxel with at most 512 candidate triangles tests them all with the
+    warp's lanes in step (one BVH walk per voxel); a voxel with more traces
+    every ray through the BVH.  The counting build shows which path ran (inner
+    nodes visited against rays), and both give the oracle's hits bit for bit."""
+    mat = F.material(diffuse=(0.1, 0.6, 0.1), alpha=0.5)
+    prm = F.params(samples_per_voxel=256, iterations=4)
+    cases = [(scenes.icosphere(4, 0.05, 1), 32, False),  # ~10 candidates per voxel
+             (scenes.foliage(20_000, 6, 0.7, 5), 5, True)]  # thousands per voxel
+    for mesh, n, per_ray in cases:
+        vs = scenes.voxel_size_for(mesh, n)
+        g, gc, gw, st = _gpu_filter(mesh, mat, prm, vs)
+        ow, oc = _oracle(mesh, mat, prm, g)
+        _compare(gw, gc, ow, oc)
+        sc = F.FilterScene(mesh, mat)
+        nvox = int(np.prod(np.array(g.num_voxels[:], np.int64)))
+        b = torch.empty(nvox * 32, dtype=torch.uint8, device="cuda")
+        rays, nodes, tris = sc.count(sc.grid(vs), prm, b.data_ptr())
+        torch.cuda.synchronize()
+        sc.close()
+        assert rays == int(st[1]) * 256 and rays > 0
+        if per_ray:
+            assert nodes >= rays, (nodes, rays)
+        else:  # a few dozen nodes per voxel against 256 rays
+            assert nodes * 2 < rays, (nodes, rays)
+            assert tris % 256 == 0  # every ray of a voxel tests the voxel's whole list
+
+
 def test_fp16_payload_error_stated():
     mesh = scenes.icosphere(4, 0.05, 1)
     mat = F.material()
