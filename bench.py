@@ -1186,11 +1186,13 @@ def bench_serving(args, c=SERVE_CFG):
         return done[-1] - arr[0], np.array(done) - arr
 
     srv = S.Server(slots=c["slots"], hbm_budget=c["budget"])
-    # warm-up like the one-at-a-time path: the largest jobs of each kind size every slot's buffers once
+    # warm-up like the one-at-a-time path: the largest job of each kind, submitted once per slot at the same
+    # time so that each slot takes one and sizes its buffers (grow-only) before the timed runs
     big = sorted(range(len(jobs)), key=lambda k: -(work[k][0] + 64 * work[k][1]))
     warm = [big[0]] + [k for k in big if jobs[k][0] != jobs[big[0]][0]][:1]
-    for _ in range(c["slots"]):
-        hs = [srv.submit_render(*specs[k]) if jobs[k][0] == "render" else srv.submit_filter(*specs[k]) for k in warm]
+    for k in warm:
+        hs = [srv.submit_render(*specs[k]) if jobs[k][0] == "render" else srv.submit_filter(*specs[k])
+              for _ in range(c["slots"])]
         for h in hs:
             srv.wait(h, 600.0)
 
