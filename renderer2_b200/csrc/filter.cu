@@ -385,6 +385,21 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) hits += __shfl_xor_sync(0xFFFFFFFFu, hits, off);
 
+    // the hit samples' lengths packed into myTs[0 .. hits-1] in sample order, so
+    // that every iteration of the density fit visits the hits only
+    if (L.clip) {
+      uint32_t packed = 0;
+      for (uint32_t base = 0; base < L.spv; base += 32) {
+        const uint32_t s = base + lane;
+        const float t = s < L.spv ? myTs[s] : -1.0f;
+        const unsigned m = __ballot_sync(0xFFFFFFFFu, t >= 0.0f);
+        __syncwarp();  // every lane has read its entry before any is overwritten
+        if (t >= 0.0f) myTs[packed + __popc(m & ((1u << lane) - 1u))] = t;
+        packed += (uint32_t)__popc(m);
+      }
+      __syncwarp();
+    }
+
     float wv[kWideFloats];
 #pragma unroll
     for (int k = 0; k < kWideFloats; ++k) wv[k] = 0.0f;
@@ -398,10 +413,7 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
         float pVol;
         if (L.clip) {
           CSum p = csum0();
-          for (uint32_t s = lane; s < L.spv; s += 32) {
-            float t = myTs[s];
-            if (t >= 0.0f) cadd(p, expf(-density * L.sigma_t * t));
-          }
+          for (uint32_t s = lane; s < hits; s += 32) cadd(p, expf(-density * L.sigma_t * myTs[s]));
           p = warp_csum(p);
           pVol = 1.0f - cvalue(p) / (float)hits;
         } else {
