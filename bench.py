@@ -105,33 +105,55 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (arrival time, line)
+        self.window = None
 
     def start(self):
+        """Starts nvidia-smi and waits (up to 10 s) for its first sample, so that it is sampling when the
+        timed region begins."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 10.0 and self.proc.poll() is None:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def begin(self):
+        self.window = [time.perf_counter(), None]
+
+    def end(self):
+        if self.window:
+            self.window[1] = time.perf_counter()
 
     def stop(self):
+        """Samples that arrived during the timed region (plus 0.3 s for the pipe); if the region was shorter
+        than the sampling interval, the first sample after it began."""
         if not self.proc:
             return None
+        time.sleep(0.3)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        lines = [ln for _, ln in self.lines]
+        if self.window and self.window[1] is not None:
+            t0, t1 = self.window
+            inside = [ln for t, ln in self.lines if t0 <= t <= t1 + 0.3]
+            after = [ln for t, ln in self.lines if t >= t0]
+            lines = inside or after[:1]
         sm, mx, reasons, power = [], None, set(), []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -454,6 +476,7 @@ def bench_render(args, world, local):
     stats = []
     evb = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
             torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    clocks.begin()
     ev0.record()
     for k in range(args.steps):
         # one step = BVH build from the resident triangles + the frame (config "BVH build + trace");
@@ -466,6 +489,7 @@ def bench_render(args, world, local):
         stats.append(st.copy())
     ev1.record()
     torch.cuda.synchronize()
+    clocks.end()
     _barrier(world)
     ck = clocks.stop()
     total_ms = _max_over_ranks(ev0.elapsed_time(ev1), world)
