@@ -31,6 +31,14 @@ namespace {
 
 constexpr int kSampleWarps = 4;  // warps per block of the sampling kernel
 constexpr int kCandMax = 512;    // candidate triangles of a voxel tested without the BVH
+constexpr int kCandStage = 32;   // candidates whose vertices a warp copies into shared memory
+
+// Dynamic shared memory of a sampling block, per warp: the staged candidate
+// vertices (kCandStage x 3 float4), the candidate list (kCandMax ints), the
+// samples' hit lengths (spv floats).
+__host__ __device__ constexpr size_t sample_smem_per_warp(uint32_t spv) {
+  return (size_t)kCandStage * 3 * sizeof(float4) + (size_t)kCandMax * sizeof(int) + (size_t)spv * sizeof(float);
+}
 
 __device__ __forceinline__ V3 voxel_center(const FilterLaunch& L, int x, int y, int z) {
   V3 pm = xform_point(L.indexToModel, v3((float)x + 0.5f, (float)y + 0.5f, (float)z + 0.5f));
@@ -155,9 +163,12 @@ __device__ int gather_candidates(const BvhView& bvh, int root, V3 qlo, V3 qhi, i
 
 // The closest hit of one ray among the candidate triangles list[0 .. n-1],
 // with the test and the (t, triangle) order of the BVH traversal: the same hit
-// as bvh_trace over the whole scene.  Every lane walks the same list.
+// as bvh_trace over the whole scene.  Every lane walks the same list; the
+// vertices of the first nStaged candidates come from the warp's shared copy
+// `staged`, the others from the BVH's triangle array.
 template <bool kAlpha>
-__device__ Hit trace_candidates(const BvhView& bvh, const int* list, int n, V3 o, V3 d, float tmax) {
+__device__ Hit trace_candidates(const BvhView& bvh, const int* list, int n, const float4* staged, int nStaged, V3 o,
+                                V3 d, float tmax) {
   const RayPre r = make_ray_pre(o, d);
   Hit best;
   best.t = tmax;
@@ -166,7 +177,16 @@ __device__ Hit trace_candidates(const BvhView& bvh, const int* list, int n, V3 o
   bool found = false;
   for (int c = 0; c < n; ++c) {
     const int tri = list[c];
-    const float4 a = __ldg(&bvh.tris[3 * tri]), b = __ldg(&bvh.tris[3 * tri + 1]), e = __ldg(&bvh.tris[3 * tri + 2]);
+    float4 a, b, e;
+    if (c < nStaged) {
+      a = staged[3 * c];
+      b = staged[3 * c + 1];
+      e = staged[3 * c + 2];
+    } else {
+      a = __ldg(&bvh.tris[3 * tri]);
+      b = __ldg(&bvh.tris[3 * tri + 1]);
+      e = __ldg(&bvh.tris[3 * tri + 2]);
+    }
     if (tri_test<kAlpha>(r, v3(a.x, a.y, a.z), v3(b.x, b.y, b.z), v3(e.x, e.y, e.z), tri, tri, &best, &bvh.alpha))
       found = true;
   }
@@ -268,11 +288,12 @@ __device__ __forceinline__ CSum warp_csum(CSum v) {
 // projection requested); the default build carries none of its code.
 template <bool kCount, bool kEig>
 __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLaunch L) {
-  __shared__ float ts[kSampleWarps][kFilterMaxSpv];
-  __shared__ int cand[kSampleWarps][kCandMax];
+  extern __shared__ float4 sSample[];  // sample_smem_per_warp(L.spv) bytes per warp
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* myTs = ts[warp];
-  int* myCand = cand[warp];
+  float4* myV = sSample + warp * kCandStage * 3;
+  int* myCand = reinterpret_cast<int*>(sSample + kSampleWarps * kCandStage * 3) + warp * kCandMax;
+  float* myTs = reinterpret_cast<float*>(reinterpret_cast<int*>(sSample + kSampleWarps * kCandStage * 3) +
+                                         kSampleWarps * kCandMax) + (size_t)warp * L.spv;
   const uint32_t ncand = *(volatile uint32_t*)&L.counters[0];
   const float radius = 1.1f * length(L.voxelSize) / 2.0f;
   const float tMaxFixed = L.voxelSize.x;
@@ -298,6 +319,14 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
     // warp's lanes in step; otherwise the rays traverse the BVH from root
     const int ncand = gather_candidates(L.bvh, root, qlo, qhi, myCand, lane, &cNodes);
     __syncwarp();
+    const int nStaged = ncand < 0 ? 0 : min(ncand, kCandStage);
+    if (lane < nStaged) {
+      const int t = myCand[lane];
+      myV[3 * lane] = __ldg(&L.bvh.tris[3 * t]);
+      myV[3 * lane + 1] = __ldg(&L.bvh.tris[3 * t + 1]);
+      myV[3 * lane + 2] = __ldg(&L.bvh.tris[3 * t + 2]);
+    }
+    __syncwarp();
 
     CSum S[6], nrm[3], dist;
     float dif[3] = {0.f, 0.f, 0.f}, spe[3] = {0.f, 0.f, 0.f}, rough = 0.f, ior = 0.f;
@@ -317,8 +346,8 @@ __global__ void __launch_bounds__(kSampleWarps * 32, 8) k_filter_sample(FilterLa
       const float tmax = L.clip ? sphere_exit(o, d, center, radius) : tMaxFixed;
       Hit h;
       if (ncand >= 0) {
-        h = L.bvh.alpha.alphaTex ? trace_candidates<true>(L.bvh, myCand, ncand, o, d, tmax)
-                                 : trace_candidates<false>(L.bvh, myCand, ncand, o, d, tmax);
+        h = L.bvh.alpha.alphaTex ? trace_candidates<true>(L.bvh, myCand, ncand, myV, nStaged, o, d, tmax)
+                                 : trace_candidates<false>(L.bvh, myCand, ncand, myV, nStaged, o, d, tmax);
         if (kCount) cTris += (uint32_t)ncand;
       } else {
         h = bvh_trace<false, kCount>(L.bvh, o, d, tmax, &cNodes, &cTris, root);
@@ -489,13 +518,10 @@ void launch_filter_classify(const FilterLaunch& L, cudaStream_t s) {
 
 template <bool kCount, bool kEig>
 static void launch_sample(const FilterLaunch& L, cudaStream_t s) {
-  static int perSm = 0;
-  if (perSm == 0) {
-    int n = 0;
-    R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<kCount, kEig>, kSampleWarps * 32, 0));
-    perSm = n < 1 ? 1 : n;
-  }
-  k_filter_sample<kCount, kEig><<<sm_count() * perSm, kSampleWarps * 32, 0, s>>>(L);
+  const size_t smem = kSampleWarps * sample_smem_per_warp(L.spv);  // <= 4 x 30 KB at spv 1024
+  int n = 0;
+  R2_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_filter_sample<kCount, kEig>, kSampleWarps * 32, smem));
+  k_filter_sample<kCount, kEig><<<sm_count() * std::max(n, 1), kSampleWarps * 32, smem, s>>>(L);
 }
 
 void launch_filter_sample(const FilterLaunch& L, cudaStream_t s) {
