@@ -654,7 +654,7 @@ def bench_filter(args, world, local, grid=None, steps=None, warmup=None, e2e_run
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": tr["bytes_per_unit"] * nvox if tr else None,
                          "kernel_ms": kms, "rays_per_s": rays / (kms / 1e3),
-                         "note": "36 B/voxel algorithmic; traversal/issue bound",
+                         "note": "36 B/voxel algorithmic; bound by issue (triangle tests, density fit) and L2 latency",
                          "fp32": {"achieved": flops / (kms / 1e3) / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
                                   "frac": flops / (kms / 1e3) / 1e12 / fp32_peak,
                                   "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 2 x 1.965 GHz",
