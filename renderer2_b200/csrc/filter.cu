@@ -32,6 +32,7 @@ namespace {
 constexpr int kSampleWarps = 4;  // warps per block of the sampling kernel
 constexpr int kCandMax = 512;    // candidate triangles of a voxel tested without the BVH
 constexpr int kCandStage = 32;   // candidates whose vertices a warp copies into shared memory
+static_assert(kCandStage <= 32, "the staging copies one candidate per lane");
 
 // Dynamic shared memory of a sampling block, per warp: the staged candidate
 // vertices (kCandStage x 3 float4), the candidate list (kCandMax ints), the
