@@ -54,3 +54,36 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
         steps, warmup = 3, 3
     bench.run_reference(Args())  # rank 1: no work, no line
     assert capsys.readouterr().out == ""
+
+
+def test_clock_sampler_keeps_the_timed_window_and_reads_throttle_reasons():
+    """bench.ClockSampler keeps the nvidia-smi samples that arrived during the
+    timed region (or, for a region shorter than the sampling interval, the
+    first one after it began) and reports the throttle reasons active there."""
+    import bench
+
+    class FakeProc:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            pass
+
+    def row(mhz, power, cap, thermal="Not Active"):
+        return f"0, {mhz}, 1965, {power}, 0x0, Not Active, Not Active, {thermal}, {cap}"
+
+    c = bench.ClockSampler(0)
+    c.proc = FakeProc()
+    c.lines = [(0.5, row(345, 90.0, "Not Active")),            # idle, before the region
+               (1.05, row(1965, 600.0, "Active")),             # inside
+               (1.15, row(1950, 640.0, "Not Active")),         # inside
+               (2.5, row(1965, 100.0, "Not Active", "Active"))]  # long after
+    c.window = [1.0, 1.2]
+    ck = c.stop()
+    assert ck["samples"] == 2 and ck["sm_mhz"] == (1965 + 1950) / 2
+    assert ck["reasons"] == ["sw_power_cap"] and ck["power_w_max"] == 640.0
+    c.window = [2.0, 2.05]  # shorter than the interval: the first sample after it began
+    ck = c.stop()
+    assert ck["samples"] == 1 and ck["reasons"] == ["sw_thermal_slowdown"]
+    c.lines = []
+    assert c.stop() is None
