@@ -243,6 +243,27 @@ def test_candidate_lists_and_per_ray_traversal_both_match_the_oracle():
             assert tris % 256 == 0  # every ray of a voxel tests the voxel's whole list
 
 
+def test_filter_output_does_not_depend_on_the_bvh_method():
+    """Closest hits do not depend on the hierarchy (ties go to the lower
+    triangle), and neither does anything the filter sums, so the PLOC and the
+    Karras trees give the same payload and records bit for bit, on the
+    candidate-list path (fine grid) and the traversal path (coarse grid)."""
+    mat = F.material(diffuse=(0.1, 0.6, 0.1), specular=(0.04, 0.04, 0.04), alpha=0.5, ior=1.5)
+    prm = F.params(samples_per_voxel=128, iterations=10)
+    leaves = scenes.foliage(20_000, 6, 0.7, 5)
+    try:
+        for n in (48, 6):
+            outs = []
+            for method in (0, 1):
+                N.check(N.lib.r2_set_bvh_method(method))
+                g, gc, gw, _ = _gpu_filter(leaves, mat, prm, scenes.voxel_size_for(leaves, n))
+                outs.append((gc, gw))
+            assert np.array_equal(outs[0][0], outs[1][0]), n
+            assert np.array_equal(outs[0][1], outs[1][1]), n
+    finally:
+        N.check(N.lib.r2_set_bvh_method(-1))
+
+
 def test_fp16_payload_error_stated():
     mesh = scenes.icosphere(4, 0.05, 1)
     mat = F.material()
