@@ -133,6 +133,26 @@ def test_device_rebuild_gives_the_same_frame():
     assert np.array_equal(a, b) and np.array_equal(a, c)
 
 
+def test_frame_does_not_depend_on_the_bvh_method():
+    """Closest hits (ties to the lower triangle) and shadow visibility do not
+    depend on the hierarchy, so scenes built with the PLOC and with the Karras
+    tree render the same frame bit for bit."""
+    desc, _ = RS.icosphere_grid_scene()
+    cam = R.camera(64, 48, 45.0, (0, 0, 24), (0, 0, 0), (0, 1, 0))
+    prm = R.params(4, 8, 9)
+    frames = []
+    try:
+        for method in (R.BVH_PLOC, R.BVH_KARRAS):
+            R.set_bvh_method(method)
+            assert R.bvh_method() == method
+            sc = RS.build_scene(desc)
+            frames.append(sc.render(cam, prm))
+            sc.close()
+    finally:
+        R.set_bvh_method(R.BVH_AUTO)
+    assert np.array_equal(frames[0], frames[1])
+
+
 def test_set_vertices_matches_a_scene_built_from_the_moved_meshes():
     """r2_scene_set_vertices + r2_scene_rebuild on a committed scene give the
     frame of a scene built from scratch with the moved geometry, bit for bit;
